@@ -1,0 +1,144 @@
+/* nnm: B200 (sm_100a) k-NN graph construction, merge and search.
+ *
+ * C ABI of the drop-in for the nn-merge hot path.  Plain pointers and
+ * sizes only.  Every call returns an nnm_status code; nnm_last_error()
+ * gives the message of the last failure on a context.
+ *
+ * Memory: "host" entry points take caller-owned host arrays and copy them
+ * to and from the GPU inside the call; "_dev" entry points take device
+ * pointers (inputs already resident in HBM).  The library owns its device
+ * workspace, which nnm_ctx_destroy frees.  A context is bound to one CUDA
+ * device and one stream and is not thread-safe; separate contexts may run
+ * concurrently.
+ *
+ * Seeding: the reference seeds each phase with std::mt19937(time(NULL)) and
+ * shuffles with std::rand().  Under NNM_RNG_EXACT every such phase here uses
+ * mt19937(opts.seed) and the std::rand() stream starts from srand(opts.seed)
+ * at the start of each call -- the reference run with its clock frozen at
+ * opts.seed -- so ids, distances, flags, distance counts and iteration
+ * counts equal the reference's bit for bit.
+ */
+#ifndef NNM_H
+#define NNM_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    NNM_OK = 0,
+    NNM_ERR_INVALID = 1,            /* bad argument (sizes, null pointers, K limits) */
+    NNM_ERR_UNSUPPORTED_METRIC = 2, /* distance function the device does not implement */
+    NNM_ERR_CUDA = 3,               /* CUDA runtime error */
+    NNM_ERR_OOM = 4,                /* device allocation failed */
+    NNM_ERR_NO_DEVICE = 5,          /* no usable CUDA device */
+    NNM_ERR_CAPACITY = 6            /* a device-side capacity/consistency check failed */
+} nnm_status;
+
+/* Distance functions of the reference (space_lp.h:9-53). */
+typedef enum {
+    NNM_METRIC_L2 = 0,   /* VMath::l2norm: squared L2, vmath.cpp:56-88 */
+    NNM_METRIC_L1 = 1,   /* DistOpt::l1norm, distopt.cpp:82-114 */
+    NNM_METRIC_CHI2 = 2  /* DistOpt::KSquare, distopt.cpp:165-184 */
+} nnm_metric;
+
+typedef enum { NNM_RNG_EXACT = 0 } nnm_rng_mode;
+
+typedef struct {
+    uint32_t seed;        /* clock value the reference's time(NULL) seeding is frozen at */
+    uint32_t rng_mode;    /* nnm_rng_mode */
+    uint32_t metric;      /* nnm_metric */
+    uint32_t sample_cap;  /* smplNum, reverse-list cap (kgraph.cpp:100): 100 */
+    float delta;          /* convergence threshold (abstractgraph.cpp:4): 0.002 */
+    uint32_t max_iter;    /* 0: iterate until converged, as the reference */
+    uint32_t exact_trace; /* nonzero: record the reference's float mean every iteration */
+    uint32_t reserved[9];
+} nnm_opts;
+
+typedef struct {
+    uint64_t ncmps;          /* distance evaluations of the measured phase, as the reference counts */
+    uint64_t sub_ncmps;      /* merges: distance evaluations of the sub-graph builds */
+    uint32_t iterations;     /* NN-Descent iterations, all loops */
+    uint32_t n_trace;        /* entries written to trace */
+    float trace[256];        /* convergence mean per iteration, in order */
+    double device_ms;        /* device time of the call (CUDA events) */
+} nnm_stats;
+
+/* H-Merge search hierarchy: layer g has nrows[g] rows (a prefix of the data
+ * set); row i's neighbours are adj[g][off[g][i] .. off[g][i+1]).  Arrays are
+ * allocated by the library (host memory) and freed by nnm_layers_free. */
+typedef struct {
+    uint32_t nlayers;
+    uint32_t nrows[16];
+    uint64_t *off[16];
+    uint32_t *adj[16];
+} nnm_layers;
+
+typedef struct nnm_ctx nnm_ctx;
+
+void nnm_opts_default(nnm_opts *opts);
+const char *nnm_status_string(int status);
+const char *nnm_last_error(const nnm_ctx *ctx);
+
+/* Creates a context on CUDA device `device`. */
+int nnm_ctx_create(int device, nnm_ctx **out);
+int nnm_ctx_destroy(nnm_ctx *ctx);
+
+/* KGraph::buildKGraph(mata, K, N, D) (kgraph.cpp:217-245) and the pools it
+ * leaves (Neighborx{id,dist,flag}, kgraph.h:24-36).  x: n x d row-major.
+ * ids/dists/flags: n x k outputs (any may be NULL). */
+int nnm_kgraph_build(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, uint32_t k,
+                     const nnm_opts *opts, uint32_t *ids, float *dists, uint8_t *flags,
+                     nnm_stats *stats);
+int nnm_kgraph_build_dev(nnm_ctx *ctx, const float *x_dev, uint64_t n, uint32_t d, uint32_t k,
+                         const nnm_opts *opts, uint32_t *ids_dev, float *dists_dev,
+                         uint8_t *flags_dev, nnm_stats *stats);
+
+/* Smerge::buildKGraph (smerge.cpp:46-91): NN-Descent on the two halves split
+ * at n*5/10, cross sampling, cross-half NN-Descent, merge2one. */
+int nnm_smerge(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, uint32_t k,
+               const nnm_opts *opts, uint32_t *ids, float *dists, uint8_t *flags,
+               nnm_stats *stats);
+
+/* Jmerge::buildKGraph (jmerge.cpp:43-80): NN-Descent on the first half,
+ * joint NN-Descent with the raw second half, merge2one. */
+int nnm_jmerge(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, uint32_t k,
+               const nnm_opts *opts, uint32_t *ids, float *dists, uint8_t *flags,
+               nnm_stats *stats);
+
+/* S-Merge over `nleaf` consecutive leaves of the given sizes (sum = n): every
+ * leaf is built with NN-Descent, every row keeps its best k - k/2 entries
+ * and samples k/2 ids from the other leaves, and the join pairs only rows of
+ * different leaves.  With two leaves of sizes n*5/10 and n - n*5/10 this is
+ * nnm_smerge (Smerge::buildKGraph); the reference has no G > 2 form. */
+int nnm_merge_leaves(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, uint32_t k,
+                     const uint32_t *leaf_sizes, uint32_t nleaf, const nnm_opts *opts,
+                     uint32_t *ids, float *dists, uint8_t *flags, nnm_stats *stats);
+int nnm_merge_leaves_dev(nnm_ctx *ctx, const float *x_dev, uint64_t n, uint32_t d, uint32_t k,
+                         const uint32_t *leaf_sizes, uint32_t nleaf, const nnm_opts *opts,
+                         uint32_t *ids_dev, float *dists_dev, uint8_t *flags_dev,
+                         nnm_stats *stats);
+
+/* LyNNDescent::buildhgraph(src, dst, grd, K, M) (lynndescent.cpp:735-831):
+ * H-Merge from 64 rows by doubling J-Merges; DPG layers at 64, 512, 4096,
+ * 32768 and n (lynndescent.cpp:502-544, :640-713).  layers may be NULL. */
+int nnm_hmerge_build(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, uint32_t k, uint32_t m,
+                     const nnm_opts *opts, uint32_t *ids, float *dists, uint8_t *flags,
+                     nnm_layers *layers, nnm_stats *stats);
+void nnm_layers_free(nnm_layers *layers);
+
+/* LySearch::knnSearch per-query steps (lysearch.cpp:363-437) for a batch of
+ * queries at one beam width `topk` (the reference's result size equals its
+ * beam): entry point rand() % nrows[0] after srand(opts.seed), greedy
+ * descent on layers 0..L-2, best-first beam search on layer L-1
+ * (nndHNSWSrch, lysearch.cpp:236-322).  out_ids/out_dists: nq x topk,
+ * ascending distance; ncmps counts distance evaluations. */
+int nnm_search(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, const nnm_layers *layers,
+               const float *q, uint64_t nq, uint32_t topk, const nnm_opts *opts,
+               uint32_t *out_ids, float *out_dists, uint64_t *ncmps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,519 @@
+// Graph builders on the device: the reference's initial graphs, merges and
+// the H-Merge level scheduler, driving run_nndescent (nndescent.cu).
+//
+//   kgraph_build   KGraph::buildKGraph        (kgraph.cpp:56-96, :217-245)
+//   merge_leaves   Smerge::buildKGraph        (smerge.cpp:46-209) for two
+//                  halves; the same steps over G leaves for G > 2
+//   jmerge_build   Jmerge::buildKGraph        (jmerge.cpp:43-176)
+//   hmerge_build   LyNNDescent::buildhgraph   (lynndescent.cpp:143-187,
+//                  :354-500, :717-831)
+//
+// Random draws: each phase that the reference seeds with
+// std::mt19937(time(NULL)) gets mt19937(seed) here (the reference run with a
+// clock frozen at `seed`); the draws are generated on the host in row order
+// and copied to the device, where each row's kernel warp consumes its fixed
+// share.  std::rand() continues across phases from srand(seed).
+#include <algorithm>
+#include <vector>
+
+#include "nnm_builders.h"
+#include "nnm_scan.h"
+
+namespace nnm {
+namespace {
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int WPB = 8;  // warps per block in the per-row kernels
+
+struct InitArgs {
+    const float* x;
+    uint32_t dp, K;
+    int metric;
+    uint32_t* pid;
+    float* pdist;
+    const uint32_t* draws;   // draws of row0 first
+    uint32_t draws_per_row;  // 0 when getRndSds is the identity
+    uint32_t nseed, range;   // getRndSds(k = nseed, N = range)
+    uint32_t row0, row1;
+    uint32_t gd_split;       // gd = (id >= gd_split); 0xffffffff: gd = 0
+    IterCounters* ctr;
+};
+
+// KGraph::InitialGraph (kgraph.cpp:56-96), Jmerge::InitialGraph new rows
+// (jmerge.cpp:147-171), LyNNDescent::init (lynndescent.cpp:143-187) and the
+// new rows of appdNwSmpl (:418-446): the first K seeds that are not the row
+// itself, their distances, std::sort.
+__global__ void k_init_rows(InitArgs a) {
+    __shared__ uint32_t seeds[WPB][72];
+    __shared__ SortEnt ents[WPB][MAXK];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t row = a.row0 + blockIdx.x * WPB + w;
+    if (row >= a.row1) return;
+    if (lane == 0)
+        rnd_seeds_dev(a.draws + (size_t)(row - a.row0) * a.draws_per_row, a.nseed, a.range, seeds[w]);
+    __syncwarp();
+    uint32_t taken = 0;
+    for (uint32_t b = 0; b < a.nseed && taken < a.K; b += 32) {
+        uint32_t j = b + lane;
+        uint32_t s = j < a.nseed ? seeds[w][j] : row;
+        bool ok = j < a.nseed && s != row;
+        unsigned bal = __ballot_sync(FULL, ok);
+        uint32_t r = taken + __popc(bal & ((1u << lane) - 1u));
+        if (ok && r < a.K) ents[w][r].id = s;
+        taken += __popc(bal);
+    }
+    __syncwarp();
+    if (taken < a.K) {
+        if (lane == 0) atomicOr(&a.ctr->error, (unsigned)DERR_CROSS_SAMPLE);
+        return;
+    }
+    if (lane < (int)a.K) {
+        uint32_t s = ents[w][lane].id;
+        float d = dist_seq_rt(a.metric, a.x + (size_t)row * a.dp, a.x + (size_t)s * a.dp, a.dp);
+        uint32_t gd = (a.gd_split != 0xffffffffu && s >= a.gd_split) ? GD_BIT : 0u;
+        ents[w][lane] = SortEnt{d, s | gd | FLAG_BIT};
+    }
+    __syncwarp();
+    if (lane == 0) std_sort_dev(ents[w], (int)a.K);
+    __syncwarp();
+    if (lane < (int)a.K) {
+        a.pid[(size_t)row * a.K + lane] = ents[w][lane].id;
+        a.pdist[(size_t)row * a.K + lane] = ents[w][lane].dist;
+    }
+}
+
+struct CrossArgs {
+    const float* x;
+    uint32_t dp, K;
+    int metric;
+    uint32_t* pid;
+    float* pdist;
+    uint32_t* cpid;
+    float* cpdist;
+    const uint32_t* draws;
+    uint32_t draws_per_row;
+    uint32_t nseed, cut;
+    uint32_t row0, row1;
+    // seed s of row r maps to the id: own leaf [lo, hi) of r is skipped, i.e.
+    // id = s < lo ? s : s + (hi - lo); range = rows outside the leaf.
+    const uint32_t* leaf_off;  // null: a single other group [base, base+range)
+    uint32_t nleaf;
+    uint32_t base, range;
+    uint32_t gd_new;
+    IterCounters* ctr;
+};
+
+__device__ __forceinline__ uint32_t leaf_index(uint32_t id, const uint32_t* off, uint32_t nleaf) {
+    uint32_t lo = 0, hi = nleaf;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (id >= off[mid]) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Cross sampling of built rows: Smerge::InitialGraph (smerge.cpp:94-209),
+// Jmerge::InitialGraph old rows (jmerge.cpp:90-135), appdNwSmpl old rows
+// (lynndescent.cpp:371-415).  The worst `cut` pool entries move to the
+// compensation list and `cut` random ids of the other group(s) that are not
+// already in the pool take their place; then std::sort.
+__global__ void k_cross_sample(CrossArgs a) {
+    __shared__ uint32_t seeds[WPB][72];
+    __shared__ SortEnt ents[WPB][MAXK];
+    __shared__ uint32_t fresh[WPB][MAXK];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t row = a.row0 + blockIdx.x * WPB + w;
+    if (row >= a.row1) return;
+    const uint32_t K = a.K, remain = K - a.cut;
+    uint32_t lo = a.base, hi = a.base, range = a.range;
+    if (a.leaf_off) {
+        uint32_t g = leaf_index(row, a.leaf_off, a.nleaf);
+        lo = a.leaf_off[g];
+        hi = a.leaf_off[g + 1];
+        range = a.leaf_off[a.nleaf] - (hi - lo);
+    }
+    if (lane == 0)
+        rnd_seeds_dev(a.draws + (size_t)(row - a.row0) * a.draws_per_row, a.nseed, range, seeds[w]);
+    if (lane < (int)K) {
+        ents[w][lane] = SortEnt{a.pdist[(size_t)row * K + lane], a.pid[(size_t)row * K + lane]};
+    }
+    __syncwarp();
+    if (lane < (int)a.cut) {
+        a.cpid[(size_t)row * K + lane] = ents[w][remain + lane].id;
+        a.cpdist[(size_t)row * K + lane] = ents[w][remain + lane].dist;
+    }
+    uint32_t taken = 0;
+    for (uint32_t b = 0; b < a.nseed && taken < a.cut; b += 32) {
+        uint32_t m = b + lane;
+        uint32_t rid = 0;
+        bool ok = false;
+        if (m < a.nseed) {
+            uint32_t s = seeds[w][m];
+            rid = a.leaf_off ? (s < lo ? s : s + (hi - lo)) : s + a.base;
+            ok = true;
+            for (uint32_t l = 0; l < K; l++)
+                if ((ents[w][l].id & ID_MASK) == rid) ok = false;
+        }
+        unsigned bal = __ballot_sync(FULL, ok);
+        uint32_t r = taken + __popc(bal & ((1u << lane) - 1u));
+        if (ok && r < a.cut) fresh[w][r] = rid;
+        taken += __popc(bal);
+    }
+    __syncwarp();
+    if (taken < a.cut) {
+        if (lane == 0) atomicOr(&a.ctr->error, (unsigned)DERR_CROSS_SAMPLE);
+        return;
+    }
+    if (lane < (int)a.cut) {
+        uint32_t id = fresh[w][lane];
+        float d = dist_seq_rt(a.metric, a.x + (size_t)id * a.dp, a.x + (size_t)row * a.dp, a.dp);
+        ents[w][remain + lane] = SortEnt{d, id | (a.gd_new ? GD_BIT : 0u) | FLAG_BIT};
+    }
+    __syncwarp();
+    if (lane == 0) std_sort_dev(ents[w], (int)K);
+    __syncwarp();
+    if (lane < (int)K) {
+        a.pid[(size_t)row * K + lane] = ents[w][lane].id;
+        a.pdist[(size_t)row * K + lane] = ents[w][lane].dist;
+    }
+}
+
+// merge2one (abstractmerge.cpp:232-277, lynndescent.cpp:455-500): merge each
+// pool with its compensation list, pool first on equal distances, keep K.
+__global__ void k_merge2one(uint32_t* pid, float* pdist, const uint32_t* cpid, const float* cpdist, uint32_t K,
+                            uint32_t cut, uint32_t rows) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t row = blockIdx.x * WPB + w;
+    if (row >= rows) return;
+    uint32_t pe = 0, ce = 0;
+    float pd = 0.f, cd = 0.f;
+    if (lane < (int)K) {
+        pe = pid[(size_t)row * K + lane];
+        pd = pdist[(size_t)row * K + lane];
+    }
+    if (lane < (int)cut) {
+        ce = cpid[(size_t)row * K + lane];
+        cd = cpdist[(size_t)row * K + lane];
+    }
+    uint32_t pp = lane, cp = lane;
+    for (uint32_t j = 0; j < K; j++) {
+        float od = __shfl_sync(FULL, pd, j);
+        if (j < cut) {
+            float oc = __shfl_sync(FULL, cd, j);
+            if (oc < pd) pp++;  // compensation entries strictly smaller come first
+        }
+        if (od <= cd) cp++;    // pool entries with equal distance win
+    }
+    __syncwarp();
+    if (lane < (int)K && pp < K) {
+        pid[(size_t)row * K + pp] = pe;
+        pdist[(size_t)row * K + pp] = pd;
+    }
+    if (lane < (int)cut && cp < K) {
+        pid[(size_t)row * K + cp] = ce;
+        pdist[(size_t)row * K + cp] = cd;
+    }
+}
+
+// Sub-graph ids become global ids; every entry is flagged new with the
+// sub-graph's group id (AbstractMerge::InitSGraph, abstractmerge.cpp:55-76;
+// the distances are recomputed there with the same arithmetic, so the
+// sub-graph's own values are kept).
+__global__ void k_rebase(uint32_t* pid, size_t count, uint32_t add, uint32_t gd) {
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    pid[t] = ((pid[t] & ID_MASK) + add) | (gd ? GD_BIT : 0u) | FLAG_BIT;
+}
+
+// setflag (lynndescent.cpp:717-732): all group ids to 0.
+__global__ void k_clear_gd(uint32_t* pid, size_t count) {
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) pid[t] &= ~GD_BIT;
+}
+
+__global__ void k_export(const uint32_t* pid, const float* pdist, size_t count, uint32_t* ids, float* dists,
+                         uint8_t* flags) {
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    uint32_t e = pid[t];
+    if (ids) ids[t] = e & ID_MASK;
+    if (dists) dists[t] = pdist[t];
+    if (flags) flags[t] = (uint8_t)(e >> 31);
+}
+
+__global__ void k_pad_copy(const float* src, float* dst, uint64_t n, uint32_t d, uint32_t dp) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * dp) return;
+    uint64_t r = t / dp;
+    uint32_t c = (uint32_t)(t - r * dp);
+    dst[t] = c < d ? src[r * d + c] : 0.f;
+}
+
+unsigned blocks_for(size_t n, unsigned per) { return (unsigned)((n + per - 1) / per); }
+
+// Host-generated mt19937 stream for `rows` rows of `per_row` draws each.
+int upload_draws(Ctx& ctx, uint32_t seed_or_state_unused, std::vector<uint32_t>& host, size_t count) {
+    (void)seed_or_state_unused;
+    NNM_CUDA_TRY(ctx.ws.draws.ensure(std::max<size_t>(count, 1) * 4));
+    if (count)
+        NNM_CUDA_TRY(cudaMemcpyAsync(ctx.ws.draws.p, host.data(), count * 4, cudaMemcpyHostToDevice, ctx.stream));
+    return 0;
+}
+
+// Draws consumed by one getRndSds(k, N) call.
+inline uint32_t sds_draws(uint32_t k, uint32_t N) { return N == k ? 0u : k + 1u; }
+
+int check_counters(Ctx& ctx) {
+    IterCounters* ctr = ctx.ws.counters.as<IterCounters>();
+    NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, ctx.stream));
+    NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+    if (ctx.h_counters->error) {
+        ctx.last_error = ctx.h_counters->error & DERR_CROSS_SAMPLE
+                             ? "random sampling found too few distinct candidates (graph too small for K)"
+                             : "device capacity check failed";
+        return 6;
+    }
+    return 0;
+}
+
+int reset_counters(Ctx& ctx) {
+    NNM_CUDA_TRY(ctx.ws.counters.ensure(sizeof(IterCounters) + 64));
+    NNM_CUDA_TRY(cudaMemsetAsync(ctx.ws.counters.p, 0, sizeof(IterCounters), ctx.stream));
+    return 0;
+}
+
+}  // namespace
+
+int upload_vectors(Ctx& ctx, GraphStore& s, GraphDev& g, const float* x, bool x_on_device) {
+    g.dp = (g.d + 3) & ~3u;
+    const size_t elems = (size_t)g.n_cap * g.dp;
+    NNM_CUDA_TRY(s.x.ensure(elems * 4));
+    if (g.dp == g.d) {
+        NNM_CUDA_TRY(cudaMemcpyAsync(s.x.p, x, elems * 4, x_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                     ctx.stream));
+    } else {
+        const float* src = x;
+        DevBuf tmp;
+        if (!x_on_device) {
+            NNM_CUDA_TRY(tmp.ensure((size_t)g.n_cap * g.d * 4));
+            NNM_CUDA_TRY(cudaMemcpyAsync(tmp.p, x, (size_t)g.n_cap * g.d * 4, cudaMemcpyHostToDevice, ctx.stream));
+            src = tmp.as<float>();
+        }
+        k_pad_copy<<<blocks_for(elems, 256), 256, 0, ctx.stream>>>(src, s.x.as<float>(), g.n_cap, g.d, g.dp);
+        NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+        tmp.release();
+    }
+    g.x = s.x.as<float>();
+    return 0;
+}
+
+int export_graph(Ctx& ctx, const GraphDev& g, uint32_t* ids, float* dists, uint8_t* flags, bool host_out) {
+    const size_t cnt = (size_t)g.n * g.K;
+    if (!host_out) {
+        k_export<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid, g.pdist, cnt, ids, dists, flags);
+        NNM_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
+    DevBuf& tmp = ctx.ws.misc;
+    NNM_CUDA_TRY(tmp.ensure(cnt * 9 + 64));
+    uint32_t* di = tmp.as<uint32_t>();
+    float* dd = reinterpret_cast<float*>(di + cnt);
+    uint8_t* df = reinterpret_cast<uint8_t*>(dd + cnt);
+    k_export<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid, g.pdist, cnt, di, dd, df);
+    if (ids) NNM_CUDA_TRY(cudaMemcpyAsync(ids, di, cnt * 4, cudaMemcpyDeviceToHost, ctx.stream));
+    if (dists) NNM_CUDA_TRY(cudaMemcpyAsync(dists, dd, cnt * 4, cudaMemcpyDeviceToHost, ctx.stream));
+    if (flags) NNM_CUDA_TRY(cudaMemcpyAsync(flags, df, cnt, cudaMemcpyDeviceToHost, ctx.stream));
+    NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+    return 0;
+}
+
+// KGraph on rows [0, g.n) of g (x, pid, pdist already offset by the caller).
+int kgraph_build(Ctx& ctx, GraphDev& g) {
+    const uint32_t K = g.K, n = g.n;
+    const uint32_t per = sds_draws(K + 1, n);
+    std::vector<uint32_t> h((size_t)n * per);
+    gen_mt19937(g.seed, h.size(), h.data());
+    int rc = upload_draws(ctx, g.seed, h, h.size());
+    if (rc) return rc;
+    if ((rc = reset_counters(ctx))) return rc;
+    InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>(), per, K + 1, n, 0, n,
+                0xffffffffu, ctx.ws.counters.as<IterCounters>()};
+    k_init_rows<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(ia);
+    NNM_CUDA_TRY(cudaGetLastError());
+    if ((rc = check_counters(ctx))) return rc;
+    g.ncmps += (uint64_t)n * K;
+    return run_nndescent(ctx, g, MODE_KGRAPH, 0, 0, nullptr, 0);
+}
+
+// A view of rows [b, e) of parent as a stand-alone graph (shared arrays).
+static GraphDev sub_view(const GraphDev& p, uint32_t b, uint32_t e) {
+    GraphDev s = p;
+    s.n_cap = s.n = e - b;
+    s.x = p.x + (size_t)b * p.dp;
+    s.pid = p.pid + (size_t)b * p.K;
+    s.pdist = p.pdist + (size_t)b * p.K;
+    s.cpid = p.cpid + (size_t)b * p.K;
+    s.cpdist = p.cpdist + (size_t)b * p.K;
+    s.ncmps = 0;
+    s.iters = 0;
+    s.trace.clear();
+    s.carry = false;
+    return s;
+}
+
+static void absorb(GraphDev& p, const GraphDev& s) {
+    p.gpos = s.gpos;
+    p.iters += s.iters;
+    p.trace.insert(p.trace.end(), s.trace.begin(), s.trace.end());
+}
+
+int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, uint64_t* sub_ncmps) {
+    const uint32_t K = g.K, n = g.n, nleaf = (uint32_t)leaf_off.size() - 1;
+    int rc;
+    uint64_t subc = 0;
+    // 1. NN-Descent on every leaf, in place (smerge.cpp:56-68).
+    for (uint32_t l = 0; l < nleaf; l++) {
+        GraphDev s = sub_view(g, leaf_off[l], leaf_off[l + 1]);
+        if ((rc = kgraph_build(ctx, s))) return rc;
+        subc += s.ncmps;
+        absorb(g, s);
+        size_t cnt = (size_t)s.n * K;
+        k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(s.pid, cnt, leaf_off[l], nleaf == 2 ? l : 0u);
+    }
+    if (sub_ncmps) *sub_ncmps = subc;
+    // 2. cross sampling (smerge.cpp:94-209)
+    g.cut = K * 1 / 2;
+    std::vector<uint32_t> h;
+    h.reserve((size_t)n * (2 * g.cut + 1));
+    {
+        std::vector<uint32_t> all;
+        size_t total = 0;
+        std::vector<uint32_t> per(nleaf);
+        for (uint32_t l = 0; l < nleaf; l++) {
+            uint32_t range = n - (leaf_off[l + 1] - leaf_off[l]);
+            per[l] = sds_draws(2 * g.cut, range);
+            total += (size_t)(leaf_off[l + 1] - leaf_off[l]) * per[l];
+        }
+        h.resize(total);
+        gen_mt19937(g.seed, total, h.data());
+        if ((rc = upload_draws(ctx, g.seed, h, total))) return rc;
+        DevBuf& lo = ctx.ws.misc;
+        NNM_CUDA_TRY(lo.ensure(leaf_off.size() * 4 + 64));
+        NNM_CUDA_TRY(cudaMemcpyAsync(lo.p, leaf_off.data(), leaf_off.size() * 4, cudaMemcpyHostToDevice, ctx.stream));
+        if ((rc = reset_counters(ctx))) return rc;
+        size_t off = 0;
+        for (uint32_t l = 0; l < nleaf; l++) {
+            uint32_t r0 = leaf_off[l], r1 = leaf_off[l + 1];
+            CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist,
+                         ctx.ws.draws.as<uint32_t>() + off, per[l], 2 * g.cut, g.cut, r0, r1,
+                         lo.as<uint32_t>(), nleaf, 0, 0, nleaf == 2 ? (l == 0 ? 1u : 0u) : 0u,
+                         ctx.ws.counters.as<IterCounters>()};
+            k_cross_sample<<<blocks_for(r1 - r0, WPB), WPB * 32, 0, ctx.stream>>>(ca);
+            off += (size_t)(r1 - r0) * per[l];
+        }
+        NNM_CUDA_TRY(cudaGetLastError());
+        if ((rc = check_counters(ctx))) return rc;
+        g.ncmps += (uint64_t)n * g.cut;
+        // 3. NN-Descent with the cross-group join, 4. merge2one
+        rc = run_nndescent(ctx, g, MODE_SMERGE, leaf_off[1], 0, lo.as<uint32_t>(), nleaf);
+        if (rc) return rc;
+    }
+    k_merge2one<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, n);
+    NNM_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int jmerge_build(Ctx& ctx, GraphDev& g, uint64_t* sub_ncmps) {
+    const uint32_t K = g.K, n = g.n, pre = n * 5 / 10;  // jmerge.cpp:47
+    int rc;
+    GraphDev s = sub_view(g, 0, pre);
+    if ((rc = kgraph_build(ctx, s))) return rc;
+    if (sub_ncmps) *sub_ncmps = s.ncmps;
+    absorb(g, s);
+    k_rebase<<<blocks_for((size_t)pre * K, 256), 256, 0, ctx.stream>>>(g.pid, (size_t)pre * K, 0, 0);
+    g.cut = K * 3 / 6;                                    // jmerge.cpp:87
+    const uint32_t per_old = sds_draws(2 * g.cut, n - pre), per_new = sds_draws(K + 1, n);
+    size_t total = (size_t)pre * per_old + (size_t)(n - pre) * per_new;
+    std::vector<uint32_t> h(total);
+    gen_mt19937(g.seed, total, h.data());
+    if ((rc = upload_draws(ctx, g.seed, h, total))) return rc;
+    if ((rc = reset_counters(ctx))) return rc;
+    CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist, ctx.ws.draws.as<uint32_t>(), per_old,
+                 2 * g.cut, g.cut, 0, pre, nullptr, 0, pre, n - pre, 1, ctx.ws.counters.as<IterCounters>()};
+    k_cross_sample<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(ca);
+    InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>() + (size_t)pre * per_old,
+                per_new, K + 1, n, pre, n, pre, ctx.ws.counters.as<IterCounters>()};
+    k_init_rows<<<blocks_for(n - pre, WPB), WPB * 32, 0, ctx.stream>>>(ia);
+    NNM_CUDA_TRY(cudaGetLastError());
+    if ((rc = check_counters(ctx))) return rc;
+    g.ncmps += (uint64_t)pre * g.cut + (uint64_t)(n - pre) * K;
+    if ((rc = run_nndescent(ctx, g, MODE_JMERGE, pre, 0, nullptr, 0))) return rc;
+    k_merge2one<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, pre);
+    NNM_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer) {
+    const uint32_t N0 = 64, K = g.K, row = g.n_cap;  // lynndescent.cpp:23
+    int rc;
+    // init: 64 rows, random K-NN (lynndescent.cpp:143-187)
+    {
+        const uint32_t per = sds_draws(K + 1, N0);
+        std::vector<uint32_t> h((size_t)N0 * per);
+        gen_mt19937(g.seed, h.size(), h.data());
+        if ((rc = upload_draws(ctx, g.seed, h, h.size()))) return rc;
+        if ((rc = reset_counters(ctx))) return rc;
+        InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>(), per, K + 1, N0, 0, N0,
+                    0xffffffffu, ctx.ws.counters.as<IterCounters>()};
+        k_init_rows<<<blocks_for(N0, WPB), WPB * 32, 0, ctx.stream>>>(ia);
+        if ((rc = check_counters(ctx))) return rc;
+        g.ncmps += (uint64_t)N0 * K;
+    }
+    g.n = N0;
+    uint32_t last_id = N0, total = row - N0, smpl = N0, count_level = 0;
+    if ((rc = run_nndescent(ctx, g, MODE_LY, N0, 1, nullptr, 0))) return rc;
+    if ((rc = on_layer(ctx, g))) return rc;
+    count_level++;
+    static const uint32_t level[10] = {1, 0, 0, 1, 0, 0, 1, 0, 0, 1};  // lynndescent.cpp:771
+    const uint32_t half = K / 2, hsize = K - half;
+    while (total != 0) {
+        const bool last = !(total > smpl);
+        const uint32_t bnum = last ? total : smpl;
+        const uint32_t sz = g.n, lst = last_id;
+        // appdNwSmpl (lynndescent.cpp:354-452): one mt19937(seed), old rows then new rows
+        const uint32_t per_old = sds_draws(2 * half, bnum), per_new = sds_draws(2 * K, sz + bnum);
+        size_t tot = (size_t)sz * per_old + (size_t)bnum * per_new;
+        std::vector<uint32_t> h(tot);
+        gen_mt19937(g.seed, tot, h.data());
+        if ((rc = upload_draws(ctx, g.seed, h, tot))) return rc;
+        if ((rc = reset_counters(ctx))) return rc;
+        g.cut = hsize;
+        CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist, ctx.ws.draws.as<uint32_t>(), per_old,
+                     2 * half, hsize, 0, sz, nullptr, 0, lst, bnum, 1, ctx.ws.counters.as<IterCounters>()};
+        k_cross_sample<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(ca);
+        InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>() + (size_t)sz * per_old,
+                    per_new, 2 * K, sz + bnum, sz, sz + bnum, lst, ctx.ws.counters.as<IterCounters>()};
+        k_init_rows<<<blocks_for(bnum, WPB), WPB * 32, 0, ctx.stream>>>(ia);
+        NNM_CUDA_TRY(cudaGetLastError());
+        if ((rc = check_counters(ctx))) return rc;
+        g.ncmps += (uint64_t)sz * hsize + (uint64_t)bnum * K;
+        g.n = sz + bnum;
+        last_id = lst + bnum;
+        total -= bnum;
+        if ((rc = run_nndescent(ctx, g, MODE_LY, lst, 0, nullptr, 0))) return rc;
+        k_merge2one<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, hsize, sz);
+        NNM_CUDA_TRY(cudaGetLastError());
+        if (last || (count_level < 10 && level[count_level]))
+            if ((rc = on_layer(ctx, g))) return rc;
+        count_level++;
+        if (!last) {
+            smpl = g.n;
+            size_t cnt = (size_t)g.n * K;
+            k_clear_gd<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid, cnt);  // setflag
+        }
+    }
+    NNM_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace nnm

@@ -1,0 +1,294 @@
+// C ABI (include/nnm.h) over the device engine.
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/nnm.h"
+#include "nnm_builders.h"
+#include "nnm_hier.h"
+
+struct nnm_ctx {
+    nnm::Ctx c;
+};
+
+namespace {
+
+using nnm::Ctx;
+using nnm::GraphDev;
+using nnm::GraphStore;
+
+int fail(nnm_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->c.last_error = msg;
+    return code;
+}
+
+bool opts_ok(nnm_ctx* ctx, const nnm_opts* o, int* rc) {
+    if (o->metric > NNM_METRIC_CHI2) {
+        *rc = fail(ctx, NNM_ERR_UNSUPPORTED_METRIC, "metric must be NNM_METRIC_L2, _L1 or _CHI2");
+        return false;
+    }
+    if (o->rng_mode != NNM_RNG_EXACT) {
+        *rc = fail(ctx, NNM_ERR_INVALID, "unknown rng_mode");
+        return false;
+    }
+    if (o->sample_cap == 0 || o->sample_cap > 4096) {
+        *rc = fail(ctx, NNM_ERR_INVALID, "sample_cap must be in [1, 4096]");
+        return false;
+    }
+    return true;
+}
+
+void setup_graph(GraphDev& g, const nnm_opts& o, uint64_t n, uint32_t d, uint32_t k) {
+    g.n_cap = g.n = (uint32_t)n;
+    g.K = k;
+    g.d = d;
+    g.metric = (int)o.metric;
+    g.seed = o.seed;
+    g.gbase = nnm::glibc_base(o.seed);
+    g.gpos = 0;  // srand(seed) at the start of the call
+    g.smpl = o.sample_cap;
+    g.delta = o.delta;
+    g.max_iter = o.max_iter;
+    g.exact_trace = o.exact_trace != 0;
+}
+
+void fill_stats(nnm_stats* st, const GraphDev& g, uint64_t sub, float ms) {
+    if (!st) return;
+    st->ncmps = g.ncmps;
+    st->sub_ncmps = sub;
+    st->iterations = g.iters;
+    st->n_trace = (uint32_t)std::min<size_t>(g.trace.size(), 256);
+    for (uint32_t i = 0; i < st->n_trace; i++) st->trace[i] = g.trace[i];
+    st->device_ms = ms;
+}
+
+struct EventTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaStream_t s;
+    explicit EventTimer(cudaStream_t st) : s(st) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, s);
+    }
+    float stop() {
+        float ms = 0.f;
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    }
+    ~EventTimer() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+};
+
+enum Kind { KIND_KGRAPH, KIND_LEAVES, KIND_JMERGE };
+
+int build_common(nnm_ctx* ctx, Kind kind, const float* x, bool dev, uint64_t n, uint32_t d, uint32_t k,
+                 const uint32_t* leaf_sizes, uint32_t nleaf, const nnm_opts* opts, uint32_t* ids, float* dists,
+                 uint8_t* flags, nnm_stats* stats) {
+    if (!ctx) return NNM_ERR_INVALID;
+    if (!x || n == 0 || d == 0) return fail(ctx, NNM_ERR_INVALID, "x must be non-null with n, d > 0");
+    if (k == 0 || k > (uint32_t)nnm::MAXK) return fail(ctx, NNM_ERR_INVALID, "k must be in [1, 32]");
+    if (n >= (1ull << 30)) return fail(ctx, NNM_ERR_INVALID, "n must be below 2^30");
+    nnm_opts o;
+    if (opts) o = *opts;
+    else nnm_opts_default(&o);
+    int rc;
+    if (!opts_ok(ctx, &o, &rc)) return rc;
+    std::vector<uint32_t> off;
+    if (kind == KIND_LEAVES) {
+        if (!leaf_sizes || nleaf < 2 || nleaf > 1024) return fail(ctx, NNM_ERR_INVALID, "need 2..1024 leaves");
+        off.push_back(0);
+        for (uint32_t l = 0; l < nleaf; l++) {
+            if (leaf_sizes[l] < k + 2) return fail(ctx, NNM_ERR_INVALID, "every leaf needs at least k+2 rows");
+            off.push_back(off.back() + leaf_sizes[l]);
+        }
+        if (off.back() != n) return fail(ctx, NNM_ERR_INVALID, "leaf sizes must sum to n");
+    } else if (kind == KIND_JMERGE) {
+        if (n * 5 / 10 < k + 2) return fail(ctx, NNM_ERR_INVALID, "n too small for k");
+    } else if (n < k + 2) {
+        return fail(ctx, NNM_ERR_INVALID, "n must be at least k+2");
+    }
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    GraphStore store;
+    GraphDev g;
+    setup_graph(g, o, n, d, k);
+    uint64_t sub = 0;
+    EventTimer tm(c.stream);
+    rc = nnm::upload_vectors(c, store, g, x, dev);
+    if (!rc) rc = nnm::graph_alloc(c, store, g, false);
+    if (!rc) {
+        if (kind == KIND_KGRAPH) rc = nnm::kgraph_build(c, g);
+        else if (kind == KIND_LEAVES) rc = nnm::merge_leaves(c, g, off, &sub);
+        else rc = nnm::jmerge_build(c, g, &sub);
+    }
+    if (!rc) rc = nnm::export_graph(c, g, ids, dists, flags, !dev);
+    float ms = tm.stop();
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(c.stream);
+        if (e != cudaSuccess) rc = fail(ctx, NNM_ERR_CUDA, cudaGetErrorString(e));
+    }
+    store.release();
+    if (!rc) fill_stats(stats, g, sub, ms);
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+void nnm_opts_default(nnm_opts* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->seed = 0;
+    o->rng_mode = NNM_RNG_EXACT;
+    o->metric = NNM_METRIC_L2;
+    o->sample_cap = 100;  // kgraph.cpp:100
+    o->delta = 0.002f;    // abstractgraph.cpp:4
+    o->max_iter = 0;
+    o->exact_trace = 0;
+}
+
+const char* nnm_status_string(int s) {
+    switch (s) {
+    case NNM_OK: return "ok";
+    case NNM_ERR_INVALID: return "invalid argument";
+    case NNM_ERR_UNSUPPORTED_METRIC: return "unsupported metric";
+    case NNM_ERR_CUDA: return "CUDA error";
+    case NNM_ERR_OOM: return "out of device memory";
+    case NNM_ERR_NO_DEVICE: return "no CUDA device";
+    case NNM_ERR_CAPACITY: return "device capacity check failed";
+    default: return "unknown status";
+    }
+}
+
+const char* nnm_last_error(const nnm_ctx* ctx) { return ctx ? ctx->c.last_error.c_str() : "null context"; }
+
+int nnm_ctx_create(int device, nnm_ctx** out) {
+    if (!out) return NNM_ERR_INVALID;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) return NNM_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return NNM_ERR_NO_DEVICE;
+    std::unique_ptr<nnm_ctx> ctx(new nnm_ctx());
+    ctx->c.device = device;
+    if (cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking) != cudaSuccess) return NNM_ERR_CUDA;
+    if (cudaMallocHost(&ctx->c.h_counters, sizeof(nnm::IterCounters) * 2) != cudaSuccess) return NNM_ERR_CUDA;
+    if (nnm::glibc_tables_init() != cudaSuccess) return NNM_ERR_CUDA;
+    *out = ctx.release();
+    return NNM_OK;
+}
+
+int nnm_ctx_destroy(nnm_ctx* ctx) {
+    if (!ctx) return NNM_OK;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    ctx->c.ws.release_all();
+    if (ctx->c.h_counters) cudaFreeHost(ctx->c.h_counters);
+    if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
+    delete ctx;
+    return NNM_OK;
+}
+
+int nnm_kgraph_build(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint32_t k, const nnm_opts* opts,
+                     uint32_t* ids, float* dists, uint8_t* flags, nnm_stats* stats) {
+    return build_common(ctx, KIND_KGRAPH, x, false, n, d, k, nullptr, 0, opts, ids, dists, flags, stats);
+}
+
+int nnm_kgraph_build_dev(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint32_t k, const nnm_opts* opts,
+                         uint32_t* ids, float* dists, uint8_t* flags, nnm_stats* stats) {
+    return build_common(ctx, KIND_KGRAPH, x, true, n, d, k, nullptr, 0, opts, ids, dists, flags, stats);
+}
+
+int nnm_smerge(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint32_t k, const nnm_opts* opts,
+               uint32_t* ids, float* dists, uint8_t* flags, nnm_stats* stats) {
+    uint32_t sizes[2] = {(uint32_t)(n * 5 / 10), (uint32_t)(n - n * 5 / 10)};  // smerge.cpp:53
+    return build_common(ctx, KIND_LEAVES, x, false, n, d, k, sizes, 2, opts, ids, dists, flags, stats);
+}
+
+int nnm_jmerge(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint32_t k, const nnm_opts* opts,
+               uint32_t* ids, float* dists, uint8_t* flags, nnm_stats* stats) {
+    return build_common(ctx, KIND_JMERGE, x, false, n, d, k, nullptr, 0, opts, ids, dists, flags, stats);
+}
+
+int nnm_merge_leaves(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint32_t k, const uint32_t* leaf_sizes,
+                     uint32_t nleaf, const nnm_opts* opts, uint32_t* ids, float* dists, uint8_t* flags,
+                     nnm_stats* stats) {
+    return build_common(ctx, KIND_LEAVES, x, false, n, d, k, leaf_sizes, nleaf, opts, ids, dists, flags, stats);
+}
+
+int nnm_merge_leaves_dev(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint32_t k,
+                         const uint32_t* leaf_sizes, uint32_t nleaf, const nnm_opts* opts, uint32_t* ids,
+                         float* dists, uint8_t* flags, nnm_stats* stats) {
+    return build_common(ctx, KIND_LEAVES, x, true, n, d, k, leaf_sizes, nleaf, opts, ids, dists, flags, stats);
+}
+
+int nnm_hmerge_build(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint32_t k, uint32_t m,
+                     const nnm_opts* opts, uint32_t* ids, float* dists, uint8_t* flags, nnm_layers* layers,
+                     nnm_stats* stats) {
+    if (!ctx) return NNM_ERR_INVALID;
+    if (!x || n <= 64 || d == 0) return fail(ctx, NNM_ERR_INVALID, "need x non-null, n > 64, d > 0");
+    if (k == 0 || k + 1 > 64 || k > (uint32_t)nnm::MAXK) return fail(ctx, NNM_ERR_INVALID, "k must be in [1, 32]");
+    if (m == 0 || m > 64) return fail(ctx, NNM_ERR_INVALID, "m must be in [1, 64]");
+    if (n >= (1ull << 30)) return fail(ctx, NNM_ERR_INVALID, "n must be below 2^30");
+    nnm_opts o;
+    if (opts) o = *opts;
+    else nnm_opts_default(&o);
+    int rc;
+    if (!opts_ok(ctx, &o, &rc)) return rc;
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    GraphStore store;
+    GraphDev g;
+    setup_graph(g, o, n, d, k);
+    nnm::DpgState dpg;
+    if (layers) std::memset(layers, 0, sizeof(*layers));
+    EventTimer tm(c.stream);
+    rc = nnm::upload_vectors(c, store, g, x, false);
+    if (!rc) rc = nnm::graph_alloc(c, store, g, true);
+    if (!rc) rc = nnm::dpg_init(c, dpg, g.n_cap, k, m);
+    if (!rc)
+        rc = nnm::hmerge_build(c, g, [&](Ctx& cc, GraphDev& gg) { return nnm::dpg_layer(cc, dpg, gg, layers); });
+    if (!rc) rc = nnm::export_graph(c, g, ids, dists, flags, true);
+    float ms = tm.stop();
+    dpg.release();
+    store.release();
+    if (!rc) fill_stats(stats, g, 0, ms);
+    else if (layers) nnm_layers_free(layers);
+    return rc;
+}
+
+void nnm_layers_free(nnm_layers* layers) {
+    if (!layers) return;
+    for (uint32_t l = 0; l < layers->nlayers && l < 16; l++) {
+        std::free(layers->off[l]);
+        std::free(layers->adj[l]);
+        layers->off[l] = nullptr;
+        layers->adj[l] = nullptr;
+    }
+    layers->nlayers = 0;
+}
+
+int nnm_search(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, const nnm_layers* layers, const float* q,
+               uint64_t nq, uint32_t topk, const nnm_opts* opts, uint32_t* out_ids, float* out_dists,
+               uint64_t* ncmps) {
+    if (!ctx) return NNM_ERR_INVALID;
+    if (!x || !q || !layers || layers->nlayers < 1 || layers->nlayers > 16 || !out_ids)
+        return fail(ctx, NNM_ERR_INVALID, "x, q, layers and out_ids are required");
+    if (topk == 0 || topk > nnm::SEARCH_MAX_BEAM) return fail(ctx, NNM_ERR_INVALID, "topk must be in [1, 1024]");
+    if (n >= (1ull << 30) || layers->nrows[layers->nlayers - 1] > n)
+        return fail(ctx, NNM_ERR_INVALID, "layers do not match the data set");
+    nnm_opts o;
+    if (opts) o = *opts;
+    else nnm_opts_default(&o);
+    int rc;
+    if (!opts_ok(ctx, &o, &rc)) return rc;
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    return nnm::search_host(c, x, n, d, layers, q, nq, topk, o.seed, (int)o.metric, out_ids, out_dists, ncmps);
+}
+
+}  // extern "C"

@@ -1,0 +1,907 @@
+// NN-Descent iterations on the device, reproducing the reference loop
+// (kgraph.cpp:98-189, abstractmerge.cpp:78-192, lynndescent.cpp:201-310)
+// bit for bit under a fixed seed.
+//
+// One iteration:
+//   1. sampling pass   k_sample_count / k_sample_fill   (kgraph.cpp:105-136)
+//      forward new/old lists from each pool, reverse entries to neighbours
+//      whose K-th distance is below the entry's distance, flags cleared.
+//   2. reverse lists   k_rev_sort_*                    (ascending source row,
+//      the order the reference's sequential pass pushes them in)
+//   3. shuffle         k_shuffle_append                 (kgraph.cpp:139-162)
+//      std::random_shuffle with the std::rand() stream (rng.cu), truncation
+//      to smplNum, appended to the sample lists.
+//   4. local join      k_join<COUNT>, k_join<FILL>      (pvetex.h:111-125 ...)
+//      all valid pairs of a row's lists, exact FP32 distances in the
+//      reference's operation order, proposals filtered by the target's K-th
+//      distance at the start of the iteration and bucketed per target.
+//   5. top-K merge     k_merge                          (pvetex.h:40-85)
+//      Within one iteration the reference's sequential UpdateKnnList calls
+//      leave in each pool the K smallest (dist, first-insert time) entries of
+//      start pool + proposals, with one entry per id (equal ids always have
+//      equal distances because the distances are bitwise symmetric).  The
+//      merge computes exactly that, so the order of the parallel inserts does
+//      not matter.
+//   6. convergence     flags counted on the device, mean decided on the host
+//      with the reference's float arithmetic.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "nnm_engine.h"
+#include "nnm_scan.h"
+
+namespace nnm {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int JOIN_THREADS = 128;
+constexpr int MERGE_WARPS = 8;
+constexpr int SHUF_SMEM = 512;  // reverse-list entries a shuffling warp stages in shared memory
+constexpr int BIGSORT_CH = 4096;
+
+// ---------------------------------------------------------------------------
+// 1. Sampling pass.
+struct SampleArgs {
+    uint32_t* pid;
+    const float* pdist;
+    uint32_t n, K, mode, split;
+    uint32_t *rcnt_new, *rcnt_old;           // reverse-entry counts (start at the carried length)
+    uint32_t *rcur_new, *rcur_old;           // fill cursors (start at the carried length)
+    const uint64_t *roff_new, *roff_old;     // reverse segments
+    uint32_t *rseg_new, *rseg_old;
+    uint32_t *newL, *oldL, *newlen, *oldlen; // sample lists
+    uint32_t capn, capo;
+    const uint32_t *rnewT, *roldT, *rnewTlen, *roldTlen;  // carried reverse lists (or null)
+    uint32_t smpl;
+    IterCounters* ctr;
+};
+
+__global__ void k_sample_count(SampleArgs a) {
+    uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (row >= a.n || lane >= (int)a.K) return;
+    size_t o = (size_t)row * a.K + lane;
+    uint32_t e = a.pid[o];
+    float d = a.pdist[o];
+    uint32_t id = e & ID_MASK;
+    float kth = a.pdist[(size_t)id * a.K + a.K - 1];
+    if (kth < d) atomicAdd((e & FLAG_BIT) ? &a.rcnt_new[id] : &a.rcnt_old[id], 1u);
+}
+
+__global__ void k_sample_fill(SampleArgs a) {
+    uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (row >= a.n) return;
+    const bool act = lane < (int)a.K;
+    size_t o = (size_t)row * a.K + lane;
+    uint32_t e = act ? a.pid[o] : 0;
+    float d = act ? a.pdist[o] : 0.f;
+    uint32_t id = e & ID_MASK;
+    bool isnew = act && (e & FLAG_BIT);
+    unsigned bal = __ballot_sync(FULL, isnew);
+    unsigned actmask = a.K >= 32 ? FULL : ((1u << a.K) - 1u);
+    uint32_t nnf = __popc(bal);
+    uint32_t base_n = a.newlen[row], base_o = a.oldlen[row];
+    if (base_n + nnf > a.capn || base_o + (a.K - nnf) > a.capo) {
+        if (lane == 0) atomicOr(&a.ctr->error, (unsigned)DERR_LIST_CAP);
+        return;
+    }
+    uint32_t entry = id | (((e >> 30) & 1u) << 31);
+    if (act) {
+        unsigned lt = (1u << lane) - 1u;
+        if (isnew) a.newL[(size_t)row * a.capn + base_n + __popc(bal & lt)] = entry;
+        else a.oldL[(size_t)row * a.capo + base_o + __popc(~bal & actmask & lt)] = entry;
+        float kth = a.pdist[(size_t)id * a.K + a.K - 1];
+        if (kth < d) {
+            uint32_t rg = (a.mode == MODE_KGRAPH) ? 0u : (row >= a.split ? 1u : 0u);
+            uint32_t v = row | (rg << 31);
+            if (isnew) a.rseg_new[a.roff_new[id] + atomicAdd(&a.rcur_new[id], 1u)] = v;
+            else a.rseg_old[a.roff_old[id] + atomicAdd(&a.rcur_old[id], 1u)] = v;
+        }
+        if (isnew) a.pid[o] = e & ~FLAG_BIT;
+    }
+    if (lane == 0) {
+        a.newlen[row] = base_n + nnf;
+        a.oldlen[row] = base_o + (a.K - nnf);
+    }
+    if (a.rnewTlen) {  // carried reverse lists go first in this row's segments
+        uint32_t cn = a.rnewTlen[row], co = a.roldTlen[row];
+        for (uint32_t j = lane; j < cn; j += 32) a.rseg_new[a.roff_new[row] + j] = a.rnewT[(size_t)row * a.smpl + j];
+        for (uint32_t j = lane; j < co; j += 32) a.rseg_old[a.roff_old[row] + j] = a.roldT[(size_t)row * a.smpl + j];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2. Reverse lists in ascending source-row order.
+struct RevSortArgs {
+    const uint64_t* roff[2];
+    uint32_t* rseg[2];
+    uint32_t* rscr[2];
+    const uint32_t* carry[2];  // carried prefix length per row (or null)
+    uint32_t n;
+    uint32_t* big;             // (row | list << 31) of segments longer than 32
+    IterCounters* ctr;
+};
+
+__device__ __forceinline__ uint32_t rkey(uint32_t v) { return v == 0xffffffffu ? 0xffffffffu : (v & LID_MASK); }
+
+__global__ void k_rev_sort_small(RevSortArgs a) {
+    uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    int l = blockIdx.y;
+    if (t >= a.n) return;
+    uint64_t lo = a.roff[l][t] + (a.carry[l] ? a.carry[l][t] : 0), hi = a.roff[l][t + 1];
+    uint32_t len = (uint32_t)(hi - lo);
+    if (len <= 1) return;
+    if (len > 32) {
+        if (lane == 0) a.big[atomicAdd(&a.ctr->nbig_rev, 1u)] = t | ((uint32_t)l << 31);
+        return;
+    }
+    uint32_t* seg = a.rseg[l] + lo;
+    uint32_t v = lane < (int)len ? seg[lane] : 0xffffffffu;
+    for (int k = 2; k <= 32; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            uint32_t o = __shfl_xor_sync(FULL, v, j);
+            bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
+            uint32_t kv = rkey(v), ko = rkey(o);
+            if (take_min ? (ko < kv) : (ko > kv)) v = o;
+        }
+    if (lane < (int)len) seg[lane] = v;
+}
+
+__global__ void k_rev_sort_big(RevSortArgs a) {
+    __shared__ uint32_t sh[BIGSORT_CH];
+    uint32_t nbig = a.ctr->nbig_rev;
+    for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
+        uint32_t code = a.big[bi];
+        uint32_t t = code & LID_MASK;
+        int l = code >> 31;
+        uint64_t lo = a.roff[l][t] + (a.carry[l] ? a.carry[l][t] : 0);
+        uint32_t len = (uint32_t)(a.roff[l][t + 1] - lo);
+        uint32_t* seg = a.rseg[l] + lo;
+        uint32_t* scr = a.rscr[l] + lo;
+        // phase 1: bitonic sort of chunks in shared memory
+        for (uint32_t cs = 0; cs < len; cs += BIGSORT_CH) {
+            uint32_t m = min((uint32_t)BIGSORT_CH, len - cs);
+            uint32_t P = 1;
+            while (P < m) P <<= 1;
+            for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) sh[i] = i < m ? seg[cs + i] : 0xffffffffu;
+            __syncthreads();
+            for (uint32_t k = 2; k <= P; k <<= 1)
+                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+                        uint32_t ix = i ^ j;
+                        if (ix > i) {
+                            uint32_t x = sh[i], y = sh[ix];
+                            bool asc = (i & k) == 0;
+                            if (asc ? rkey(x) > rkey(y) : rkey(x) < rkey(y)) {
+                                sh[i] = y;
+                                sh[ix] = x;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) seg[cs + i] = sh[i];
+            __syncthreads();
+        }
+        // phase 2: merge sorted runs pairwise (keys are distinct source rows)
+        uint32_t* src = seg;
+        uint32_t* dst = scr;
+        for (uint32_t w = BIGSORT_CH; w < len; w <<= 1) {
+            for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+                uint32_t run = i / w;
+                uint32_t rs = run * w;
+                uint32_t pb = (run & ~1u) * w;
+                uint32_t os = (run & 1u) ? rs - w : rs + w;
+                uint32_t oe = min(os + w, len);
+                if (os > len) os = len;
+                uint32_t key = rkey(src[i]);
+                uint32_t lo2 = os, hi2 = oe;  // lower bound of key in the other run
+                while (lo2 < hi2) {
+                    uint32_t mid = (lo2 + hi2) >> 1;
+                    if (rkey(src[mid]) < key) lo2 = mid + 1;
+                    else hi2 = mid;
+                }
+                dst[pb + (i - rs) + (lo2 - os)] = src[i];
+            }
+            __syncthreads();
+            uint32_t* tmp = src;
+            src = dst;
+            dst = tmp;
+        }
+        if (src != seg)
+            for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) seg[i] = src[i];
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. Shuffle, truncate and append.
+struct ShufArgs {
+    const uint64_t *roff_new, *roff_old;
+    uint32_t *rseg_new, *rseg_old;
+    const uint64_t* rofs;       // first draw of each row, relative to the generated buffer
+    const int32_t* rbuf;
+    uint32_t *newL, *oldL, *newlen, *oldlen;
+    uint32_t capn, capo, n, smpl;
+    uint32_t *rnewT, *roldT, *rnewTlen, *roldTlen;
+    uint32_t smem_rows;
+    uint32_t* bigjoin;
+    IterCounters* ctr;
+};
+
+__global__ void k_rand_count(const uint64_t* roff_new, const uint64_t* roff_old, uint32_t n, uint32_t* out) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    uint32_t ln = (uint32_t)(roff_new[t + 1] - roff_new[t]);
+    uint32_t lo = (uint32_t)(roff_old[t + 1] - roff_old[t]);
+    out[t] = (ln ? ln - 1 : 0) + (lo ? lo - 1 : 0);
+}
+
+// std::random_shuffle over seg[0..len) with draws[0..len-1), one thread.
+__device__ __forceinline__ void shuffle_seg(uint32_t* seg, uint32_t len, const int32_t* draws) {
+    for (uint32_t i = 1; i < len; i++) {
+        uint32_t j = (uint32_t)(draws[i - 1] % (int32_t)(i + 1));
+        if (j != i) {
+            uint32_t t = seg[i];
+            seg[i] = seg[j];
+            seg[j] = t;
+        }
+    }
+}
+
+// One warp per row: lane 0 shuffles in shared memory, the warp appends.
+__global__ void k_shuffle_append(ShufArgs a) {
+    __shared__ uint32_t stage[8][SHUF_SMEM];
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t t = blockIdx.x * 8 + w;
+    if (t >= a.n) return;
+    const int32_t* draws = a.rbuf + a.rofs[t];
+    uint32_t nl = a.newlen[t], ol = a.oldlen[t];
+    for (int l = 0; l < 2; l++) {
+        uint64_t lo = l ? a.roff_old[t] : a.roff_new[t];
+        uint32_t len = (uint32_t)((l ? a.roff_old[t + 1] : a.roff_new[t + 1]) - lo);
+        uint32_t* seg = (l ? a.rseg_old : a.rseg_new) + lo;
+        uint32_t keep = min(len, a.smpl);
+        uint32_t* sh = stage[w];
+        bool staged = len <= SHUF_SMEM;
+        if (staged) {
+            for (uint32_t j = lane; j < len; j += 32) sh[j] = seg[j];
+            __syncwarp();
+            if (lane == 0) shuffle_seg(sh, len, draws);
+            __syncwarp();
+        } else {
+            if (lane == 0) shuffle_seg(seg, len, draws);
+            __syncwarp();
+            sh = seg;
+        }
+        draws += len ? len - 1 : 0;
+        uint32_t* L = l ? a.oldL + (size_t)t * a.capo : a.newL + (size_t)t * a.capn;
+        uint32_t base = l ? ol : nl;
+        uint32_t cap = l ? a.capo : a.capn;
+        uint32_t* T = l ? a.roldT : a.rnewT;
+        if (base + keep > cap) {
+            if (lane == 0) atomicOr(&a.ctr->error, (unsigned)DERR_LIST_CAP);
+            return;
+        }
+        for (uint32_t j = lane; j < keep; j += 32) {
+            uint32_t v = sh[j];
+            L[base + j] = v;
+            if (T) T[(size_t)t * a.smpl + j] = v;
+        }
+        if (l) ol += keep;
+        else nl += keep;
+        if (lane == 0 && T) (l ? a.roldTlen : a.rnewTlen)[t] = keep;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        a.newlen[t] = nl;
+        a.oldlen[t] = ol;
+        if (nl > 0 && nl + ol > a.smem_rows) a.bigjoin[atomicAdd(&a.ctr->nbig_join, 1u)] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 4. Local join.
+struct JoinArgs {
+    const float* x;
+    uint32_t dp, K, n;
+    const float* pdist;
+    const uint32_t *newL, *oldL, *newlen, *oldlen;
+    uint32_t capn, capo, caps;
+    uint32_t mode, verse;
+    const uint32_t* leaf_off;
+    uint32_t nleaf;
+    uint16_t* cntpos;
+    uint32_t *bcnt, *bcur;
+    const uint64_t* boff;
+    Prop* bucket;
+    const uint32_t* bigrows;
+    uint32_t smem_rows;
+    IterCounters* ctr;
+};
+
+enum { PASS_COUNT = 0, PASS_FILL = 1 };
+
+__device__ __forceinline__ uint32_t leaf_of(uint32_t id, const uint32_t* off, uint32_t nleaf) {
+    uint32_t lo = 0, hi = nleaf;  // off[0] = 0 <= id < off[nleaf]
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (id >= off[mid]) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <int M, bool STAGED, int PASS>
+__device__ void join_row(const JoinArgs& a, uint32_t row, unsigned char* smem) {
+    const uint32_t nn = a.newlen[row], no = a.oldlen[row], S = nn + no;
+    if (nn == 0) return;
+    const uint32_t R = STAGED ? a.smem_rows : a.caps;
+    uint32_t* s_ids = reinterpret_cast<uint32_t*>(smem);
+    float* s_kth = reinterpret_cast<float*>(s_ids + R);
+    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_kth + R);
+    uint32_t* s_grp = s_cnt + R;
+    unsigned long long* s_base = reinterpret_cast<unsigned long long*>(s_grp + R);  // 16R bytes before it
+    float4* s_vec = reinterpret_cast<float4*>(s_base + R);  // 24R bytes before it: 16-byte aligned for even R
+    const uint32_t dq = a.dp >> 2, vstride = dq + 1;
+    const float4* x4 = reinterpret_cast<const float4*>(a.x);
+
+    for (uint32_t q = threadIdx.x; q < S; q += blockDim.x) {
+        uint32_t e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
+        uint32_t id = e & LID_MASK;
+        s_ids[q] = e;
+        s_kth[q] = a.pdist[(size_t)id * a.K + a.K - 1];
+        s_cnt[q] = 0;
+        s_grp[q] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
+    }
+    __syncthreads();
+    if (STAGED) {
+        for (uint32_t i = threadIdx.x; i < S * dq; i += blockDim.x) {
+            uint32_t q = i / dq, c = i - q * dq;
+            s_vec[q * vstride + c] = x4[(size_t)(s_ids[q] & LID_MASK) * dq + c];
+        }
+    }
+    if (PASS == PASS_FILL) {
+        for (uint32_t q = threadIdx.x; q < S; q += blockDim.x) {
+            uint32_t c = a.cntpos[(size_t)row * a.caps + q];
+            if (c) {
+                uint32_t id = s_ids[q] & LID_MASK;
+                s_base[q] = a.boff[id] + atomicAdd(&a.bcur[id], c);
+            }
+        }
+    }
+    __syncthreads();
+
+    const uint32_t ntA = (nn + 3) >> 2, ntB = (S + 3) >> 2;
+    const uint32_t ntiles = ntA * ntB - ntA * (ntA - 1) / 2;
+    uint32_t cmps = 0;
+    for (uint32_t t = threadIdx.x; t < ntiles; t += blockDim.x) {
+        uint32_t ta = 0, rem = t;
+        while (rem >= ntB - ta) {
+            rem -= ntB - ta;
+            ta++;
+        }
+        const uint32_t tb = ta + rem;
+        const float4* pa[4];
+        const float4* pb[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            uint32_t ai = min(ta * 4 + i, nn - 1), bj = min(tb * 4 + i, S - 1);
+            pa[i] = STAGED ? s_vec + ai * vstride : x4 + (size_t)(s_ids[ai] & LID_MASK) * dq;
+            pb[i] = STAGED ? s_vec + bj * vstride : x4 + (size_t)(s_ids[bj] & LID_MASK) * dq;
+        }
+        float acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+        for (uint32_t c = 0; c < dq; c++) {
+            float4 A[4], B[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                A[i] = pa[i][c];
+                B[i] = pb[i][c];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    acc[i][j] = dist_step<M>(acc[i][j], A[i].x, B[j].x);
+                    acc[i][j] = dist_step<M>(acc[i][j], A[i].y, B[j].y);
+                    acc[i][j] = dist_step<M>(acc[i][j], A[i].z, B[j].z);
+                    acc[i][j] = dist_step<M>(acc[i][j], A[i].w, B[j].w);
+                }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t av = ta * 4 + i;
+            if (av >= nn) continue;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint32_t bv = tb * 4 + j;
+                if (bv >= S || (bv < nn && bv <= av)) continue;
+                const uint32_t ea = s_ids[av], eb = s_ids[bv];
+                const uint32_t ida = ea & LID_MASK, idb = eb & LID_MASK;
+                if (ida == idb) continue;
+                uint32_t outer = av, inner = bv;
+                if (a.mode == MODE_KGRAPH) {
+                    if (bv < nn && idb < ida) {  // kgraph.h:112-116 visits it from the smaller id
+                        outer = bv;
+                        inner = av;
+                    }
+                } else if (a.mode == MODE_SMERGE) {
+                    if (s_grp[av] == s_grp[bv]) continue;
+                } else {
+                    uint32_t ga = s_grp[av], gb = s_grp[bv];
+                    if (!(ga != gb || ga == 1 || gb == 1 || a.verse)) continue;
+                }
+                cmps++;
+                const float dd = acc[i][j];
+                const unsigned long long kb =
+                    (1ull << 63) | ((unsigned long long)row << 32) | ((unsigned long long)(outer * S + inner) << 1);
+                if (dd < s_kth[outer]) {
+                    if (PASS == PASS_COUNT) atomicAdd(&s_cnt[outer], 1u);
+                    else {
+                        unsigned long long slot = s_base[outer] + atomicAdd(&s_cnt[outer], 1u);
+                        a.bucket[slot] = Prop{dd, s_ids[inner], kb};
+                    }
+                }
+                if (dd < s_kth[inner]) {
+                    if (PASS == PASS_COUNT) atomicAdd(&s_cnt[inner], 1u);
+                    else {
+                        unsigned long long slot = s_base[inner] + atomicAdd(&s_cnt[inner], 1u);
+                        a.bucket[slot] = Prop{dd, s_ids[outer], kb | 1ull};
+                    }
+                }
+            }
+        }
+    }
+    if (PASS == PASS_COUNT) {
+        for (int o = 16; o > 0; o >>= 1) cmps += __shfl_xor_sync(FULL, cmps, o);
+        if ((threadIdx.x & 31) == 0 && cmps) atomicAdd(&a.ctr->ncmps, (unsigned long long)cmps);
+    }
+    __syncthreads();
+    if (PASS == PASS_COUNT) {
+        for (uint32_t q = threadIdx.x; q < S; q += blockDim.x) {
+            uint32_t c = s_cnt[q];
+            a.cntpos[(size_t)row * a.caps + q] = (uint16_t)c;
+            if (c) atomicAdd(&a.bcnt[s_ids[q] & LID_MASK], c);
+        }
+    }
+    __syncthreads();
+}
+
+template <int M, int PASS>
+__global__ void __launch_bounds__(JOIN_THREADS) k_join_staged(JoinArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t row = blockIdx.x;
+    if (row >= a.n) return;
+    uint32_t S = a.newlen[row] + a.oldlen[row];
+    if (S > a.smem_rows) return;  // handled by k_join_global
+    join_row<M, true, PASS>(a, row, smem);
+}
+
+template <int M, int PASS>
+__global__ void __launch_bounds__(JOIN_THREADS) k_join_global(JoinArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t nbig = a.ctr->nbig_join;
+    for (uint32_t b = blockIdx.x; b < nbig; b += gridDim.x) join_row<M, false, PASS>(a, a.bigrows[b], smem);
+}
+
+// ---------------------------------------------------------------------------
+// 5. Top-K merge per target.
+struct MergeArgs {
+    uint32_t* pid;
+    float* pdist;
+    uint32_t n, K;
+    const uint32_t* bcnt;
+    const uint64_t* boff;
+    const Prop* bucket;
+    uint8_t* nflag;
+    IterCounters* ctr;
+};
+
+struct MEnt {
+    uint32_t d;
+    uint32_t e;
+    unsigned long long k;
+};
+
+__device__ __forceinline__ bool mless(uint32_t d1, unsigned long long k1, uint32_t d2, unsigned long long k2) {
+    return d1 < d2 || (d1 == d2 && k1 < k2);
+}
+
+// Number of entries of a sorted per-lane list (first `cnt` lanes) that are
+// smaller than (d, k).
+__device__ __forceinline__ uint32_t count_less(uint32_t ld, unsigned long long lk, uint32_t cnt, uint32_t d,
+                                               unsigned long long k) {
+    uint32_t lo = 0, hi = cnt;
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+        uint32_t mid = (lo + hi) >> 1;
+        uint32_t md = __shfl_sync(FULL, ld, mid & 31);
+        unsigned long long mk = __shfl_sync(FULL, lk, mid & 31);
+        if (lo < hi) {
+            if (mless(md, mk, d, k)) lo = mid + 1;
+            else hi = mid;
+        }
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(MERGE_WARPS * 32) k_merge(MergeArgs a) {
+    __shared__ MEnt sm[MERGE_WARPS][64];
+    __shared__ MEnt kept[MERGE_WARPS][32];
+    __shared__ unsigned int blk_flags;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) blk_flags = 0;
+    __syncthreads();
+    const uint32_t t = blockIdx.x * MERGE_WARPS + w;
+    uint32_t nfl = 0;
+    if (t < a.n) {
+        const uint32_t K = a.K;
+        const uint32_t c = a.bcnt[t];
+        if (c) {
+            uint32_t cd = 0xffffffffu, ce = 0;
+            unsigned long long ck = ~0ull;
+            if (lane < (int)K) {
+                ce = a.pid[(size_t)t * K + lane];
+                cd = __float_as_uint(a.pdist[(size_t)t * K + lane]);
+                ck = (unsigned long long)lane;  // start entries precede every proposal of equal distance
+            }
+            uint32_t kd = __shfl_sync(FULL, cd, K - 1);
+            unsigned long long kk = __shfl_sync(FULL, ck, K - 1);
+            const Prop* bp = a.bucket + a.boff[t];
+            for (uint32_t b0 = 0; b0 < c; b0 += 32) {
+                uint32_t pd = 0xffffffffu, pe = 0;
+                unsigned long long pk = ~0ull;
+                bool valid = false;
+                if (b0 + lane < c) {
+                    Prop p = bp[b0 + lane];
+                    uint32_t dbits = __float_as_uint(p.dist);
+                    if (mless(dbits, p.key, kd, kk)) {
+                        valid = true;
+                        pd = dbits;
+                        pk = p.key;
+                        pe = (p.idg & LID_MASK) | ((p.idg >> 31) << 30) | FLAG_BIT;
+                    }
+                }
+                unsigned vb = __ballot_sync(FULL, valid);
+                if (!vb) continue;
+                // bitonic sort of the chunk by (dist, key)
+                for (int k = 2; k <= 32; k <<= 1)
+                    for (int j = k >> 1; j > 0; j >>= 1) {
+                        uint32_t od = __shfl_xor_sync(FULL, pd, j);
+                        unsigned long long ok = __shfl_xor_sync(FULL, pk, j);
+                        uint32_t oe = __shfl_xor_sync(FULL, pe, j);
+                        bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
+                        bool swap = take_min ? mless(od, ok, pd, pk) : mless(pd, pk, od, ok);
+                        if (swap) {
+                            pd = od;
+                            pk = ok;
+                            pe = oe;
+                        }
+                    }
+                const uint32_t m = __popc(vb);
+                // merged positions
+                if (lane < (int)K) {
+                    uint32_t pos = lane + count_less(pd, pk, m, cd, ck);
+                    sm[w][pos] = MEnt{cd, ce, ck};
+                } else {
+                    count_less(pd, pk, m, cd, ck);
+                }
+                {
+                    uint32_t pos = lane + count_less(cd, ck, K, pd, pk);
+                    if (lane < (int)m) sm[w][pos] = MEnt{pd, pe, pk};
+                }
+                __syncwarp();
+                const uint32_t tot = K + m;
+                bool keep0 = false, keep1 = false;
+                for (int h = 0; h < 2; h++) {
+                    uint32_t s = lane + 32 * h;
+                    bool keep = false;
+                    if (s < tot) {
+                        keep = true;
+                        MEnt me = sm[w][s];
+                        for (int q = (int)s - 1; q >= 0 && sm[w][q].d == me.d; q--)
+                            if ((sm[w][q].e & ID_MASK) == (me.e & ID_MASK)) {
+                                keep = false;
+                                break;
+                            }
+                    }
+                    if (h == 0) keep0 = keep;
+                    else keep1 = keep;
+                }
+                unsigned b0m = __ballot_sync(FULL, keep0), b1m = __ballot_sync(FULL, keep1);
+                unsigned lt = (1u << lane) - 1u;
+                uint32_t r0 = __popc(b0m & lt), r1 = __popc(b0m) + __popc(b1m & lt);
+                if (keep0 && r0 < K) kept[w][r0] = sm[w][lane];
+                if (keep1 && r1 < K) kept[w][r1] = sm[w][lane + 32];
+                __syncwarp();
+                if (lane < (int)K) {
+                    MEnt me = kept[w][lane];
+                    cd = me.d;
+                    ce = me.e;
+                    ck = me.k;
+                }
+                kd = __shfl_sync(FULL, cd, K - 1);
+                kk = __shfl_sync(FULL, ck, K - 1);
+                __syncwarp();
+            }
+            if (lane < (int)K) {
+                a.pid[(size_t)t * K + lane] = ce;
+                a.pdist[(size_t)t * K + lane] = __uint_as_float(cd);
+            }
+            nfl = __popc(__ballot_sync(FULL, lane < (int)K && (ce & FLAG_BIT)));
+        }
+        if (lane == 0) a.nflag[t] = (uint8_t)nfl;
+    }
+    if (lane == 0 && nfl) atomicAdd(&blk_flags, nfl);
+    __syncthreads();
+    if (threadIdx.x == 0 && blk_flags) atomicAdd(&a.ctr->flags, (unsigned long long)blk_flags);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_clear_lists(uint32_t* newlen, uint32_t* oldlen, uint32_t* tn, uint32_t* to, uint32_t n) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    newlen[t] = 0;
+    oldlen[t] = 0;
+    if (tn) {
+        tn[t] = 0;
+        to[t] = 0;
+    }
+}
+
+__global__ void k_set_u32(uint32_t* dst, const uint32_t* src, uint32_t n) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) dst[t] = src ? src[t] : 0u;
+}
+
+template <typename T> T* P(DevBuf& b) { return b.as<T>(); }
+
+}  // namespace
+
+int graph_alloc(Ctx& ctx, GraphStore& s, GraphDev& g, bool with_carry) {
+    const size_t nk = (size_t)g.n_cap * g.K;
+    NNM_CUDA_TRY(s.pid.ensure(nk * 4));
+    NNM_CUDA_TRY(s.pdist.ensure(nk * 4));
+    NNM_CUDA_TRY(s.cpid.ensure(nk * 4));
+    NNM_CUDA_TRY(s.cpdist.ensure(nk * 4));
+    g.capn = g.capo = (g.K + g.smpl) * (with_carry ? 2 : 1);
+    NNM_CUDA_TRY(s.newL.ensure((size_t)g.n_cap * g.capn * 4));
+    NNM_CUDA_TRY(s.oldL.ensure((size_t)g.n_cap * g.capo * 4));
+    NNM_CUDA_TRY(s.newlen.ensure((size_t)g.n_cap * 4));
+    NNM_CUDA_TRY(s.oldlen.ensure((size_t)g.n_cap * 4));
+    NNM_CUDA_TRY(cudaMemsetAsync(s.newlen.p, 0, (size_t)g.n_cap * 4, ctx.stream));
+    NNM_CUDA_TRY(cudaMemsetAsync(s.oldlen.p, 0, (size_t)g.n_cap * 4, ctx.stream));
+    g.pid = s.pid.as<uint32_t>();
+    g.pdist = s.pdist.as<float>();
+    g.cpid = s.cpid.as<uint32_t>();
+    g.cpdist = s.cpdist.as<float>();
+    g.newL = s.newL.as<uint32_t>();
+    g.oldL = s.oldL.as<uint32_t>();
+    g.newlen = s.newlen.as<uint32_t>();
+    g.oldlen = s.oldlen.as<uint32_t>();
+    g.rnewT = g.roldT = g.rnewTlen = g.roldTlen = nullptr;
+    if (with_carry) {
+        NNM_CUDA_TRY(s.rnewT.ensure((size_t)g.n_cap * g.smpl * 4));
+        NNM_CUDA_TRY(s.roldT.ensure((size_t)g.n_cap * g.smpl * 4));
+        NNM_CUDA_TRY(s.rnewTlen.ensure((size_t)g.n_cap * 4));
+        NNM_CUDA_TRY(s.roldTlen.ensure((size_t)g.n_cap * 4));
+        NNM_CUDA_TRY(cudaMemsetAsync(s.rnewTlen.p, 0, (size_t)g.n_cap * 4, ctx.stream));
+        NNM_CUDA_TRY(cudaMemsetAsync(s.roldTlen.p, 0, (size_t)g.n_cap * 4, ctx.stream));
+        g.rnewT = s.rnewT.as<uint32_t>();
+        g.roldT = s.roldT.as<uint32_t>();
+        g.rnewTlen = s.rnewTlen.as<uint32_t>();
+        g.roldTlen = s.roldTlen.as<uint32_t>();
+    }
+    g.carry = false;
+    return 0;
+}
+
+template <int M>
+static void launch_join(const JoinArgs& ja, size_t smem_staged, size_t smem_global, int pass, cudaStream_t st,
+                        int nsm) {
+    if (pass == PASS_COUNT) {
+        k_join_staged<M, PASS_COUNT><<<ja.n, JOIN_THREADS, smem_staged, st>>>(ja);
+        k_join_global<M, PASS_COUNT><<<nsm * 2, JOIN_THREADS, smem_global, st>>>(ja);
+    } else {
+        k_join_staged<M, PASS_FILL><<<ja.n, JOIN_THREADS, smem_staged, st>>>(ja);
+        k_join_global<M, PASS_FILL><<<nsm * 2, JOIN_THREADS, smem_global, st>>>(ja);
+    }
+}
+
+template <int M>
+static cudaError_t set_join_attrs(size_t smem_staged, size_t smem_global) {
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_join_staged<M, PASS_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_staged)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_join_staged<M, PASS_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_staged)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_join_global<M, PASS_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_global)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_join_global<M, PASS_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_global);
+}
+
+// Sequential float mean of the per-row deltas, as the reference computes it
+// with a Boost float accumulator (EvaluateDelta: float(c)/K per row).
+static float host_mean(const std::vector<uint8_t>& nflag, uint32_t n, uint32_t K) {
+    volatile float sum = 0.f;
+    for (uint32_t i = 0; i < n; i++) sum = sum + (float)nflag[i] / (float)K;
+    return sum / (float)n;
+}
+
+int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t verse,
+                  const uint32_t* d_leaf_off, uint32_t nleaf) {
+    Workspace& ws = ctx.ws;
+    cudaStream_t st = ctx.stream;
+    const uint32_t n = g.n, K = g.K;
+    const size_t n1 = (size_t)n + 1;
+    const bool track = g.rnewT != nullptr;
+    const size_t rev_cap = (size_t)n * K + (track ? (size_t)n * g.smpl : 0);
+    const uint32_t caps = g.capn + g.capo;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx.device);
+
+    NNM_CUDA_TRY(ws.rcnt.ensure(n1 * 2 * 4));
+    NNM_CUDA_TRY(ws.rcur.ensure(n1 * 2 * 4));
+    NNM_CUDA_TRY(ws.roff.ensure(n1 * 2 * 8));
+    NNM_CUDA_TRY(ws.rseg.ensure(rev_cap * 2 * 4));
+    NNM_CUDA_TRY(ws.rscr.ensure(rev_cap * 2 * 4));
+    NNM_CUDA_TRY(ws.rcount.ensure(n1 * 4));
+    NNM_CUDA_TRY(ws.rofs.ensure(n1 * 8));
+    NNM_CUDA_TRY(ws.rbuf.ensure(rev_cap * 2 * 4 + 64));
+    NNM_CUDA_TRY(ws.cntpos.ensure((size_t)n * caps * 2));
+    NNM_CUDA_TRY(ws.bcnt.ensure(n1 * 4));
+    NNM_CUDA_TRY(ws.bcur.ensure(n1 * 4));
+    NNM_CUDA_TRY(ws.boff.ensure(n1 * 8));
+    NNM_CUDA_TRY(ws.bigrev.ensure(n1 * 2 * 4));
+    NNM_CUDA_TRY(ws.bigjoin.ensure(n1 * 4));
+    NNM_CUDA_TRY(ws.nflag.ensure(n1));
+    NNM_CUDA_TRY(ws.scan_tmp.ensure((scan_temp_elems(n1) + 8) * 8));
+    NNM_CUDA_TRY(ws.counters.ensure(sizeof(IterCounters) + 64));
+    if (ws.bucket.bytes < (size_t)n * K * 4 * sizeof(Prop)) NNM_CUDA_TRY(ws.bucket.ensure((size_t)n * K * 4 * sizeof(Prop)));
+
+    uint32_t *rcnt_new = P<uint32_t>(ws.rcnt), *rcnt_old = rcnt_new + n1;
+    uint32_t *rcur_new = P<uint32_t>(ws.rcur), *rcur_old = rcur_new + n1;
+    uint64_t *roff_new = P<uint64_t>(ws.roff), *roff_old = roff_new + n1;
+    uint32_t *rseg_new = P<uint32_t>(ws.rseg), *rseg_old = rseg_new + rev_cap;
+    uint32_t *rscr_new = P<uint32_t>(ws.rscr), *rscr_old = rscr_new + rev_cap;
+    uint64_t* scan_tmp = P<uint64_t>(ws.scan_tmp);
+    uint64_t* d_tot = P<uint64_t>(ws.scan_tmp) + scan_temp_elems(n1) + 4;  // past the scan scratch
+    IterCounters* ctr = P<IterCounters>(ws.counters);
+
+    const uint32_t dq = g.dp / 4, vstride = dq + 1;
+    const uint32_t member_bytes_per_row = 4 + 4 + 4 + 4 + 8;
+    uint32_t smem_rows = std::min<uint32_t>(caps, 120u);
+    while (smem_rows > 16 && (size_t)smem_rows * (vstride * 16 + member_bytes_per_row) + 64 > 100 * 1024) smem_rows -= 4;
+    const size_t smem_staged = (size_t)smem_rows * (vstride * 16 + member_bytes_per_row) + 64;
+    const size_t smem_global = (size_t)caps * member_bytes_per_row + 64;
+    cudaError_t ae = g.metric == L2 ? set_join_attrs<L2>(smem_staged, smem_global)
+                     : g.metric == L1 ? set_join_attrs<L1>(smem_staged, smem_global)
+                                      : set_join_attrs<CHI2>(smem_staged, smem_global);
+    NNM_CUDA_TRY(ae);
+
+    const unsigned warp_blocks = (unsigned)((n + 7) / 8);
+    const unsigned tblocks = (unsigned)((n + 255) / 256);
+    std::vector<uint8_t> h_nflag;
+
+    for (uint32_t it = 0;; it++) {
+        const bool carry_now = (it == 0) && g.carry && track;
+        if (!carry_now) {
+            k_clear_lists<<<tblocks, 256, 0, st>>>(g.newlen, g.oldlen,
+                                                   track ? g.rnewTlen : nullptr,
+                                                   track ? g.roldTlen : nullptr, n);
+        }
+        NNM_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(IterCounters), st));
+        // reverse counts and cursors start at the carried lengths
+        k_set_u32<<<tblocks, 256, 0, st>>>(rcnt_new, track ? g.rnewTlen : nullptr, n);
+        k_set_u32<<<tblocks, 256, 0, st>>>(rcnt_old, track ? g.roldTlen : nullptr, n);
+        k_set_u32<<<tblocks, 256, 0, st>>>(rcur_new, track ? g.rnewTlen : nullptr, n);
+        k_set_u32<<<tblocks, 256, 0, st>>>(rcur_old, track ? g.roldTlen : nullptr, n);
+        SampleArgs sa{g.pid, g.pdist, n, K, (uint32_t)mode, split,
+                      rcnt_new, rcnt_old, rcur_new, rcur_old, roff_new, roff_old, rseg_new, rseg_old,
+                      g.newL, g.oldL, g.newlen, g.oldlen,
+                      g.capn, g.capo,
+                      carry_now ? g.rnewT : nullptr, carry_now ? g.roldT : nullptr,
+                      carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr,
+                      g.smpl, ctr};
+        k_sample_count<<<warp_blocks, 256, 0, st>>>(sa);
+        NNM_CUDA_TRY(exclusive_scan(rcnt_new, roff_new, n, scan_tmp, nullptr, st));
+        NNM_CUDA_TRY(exclusive_scan(rcnt_old, roff_old, n, scan_tmp, nullptr, st));
+        k_sample_fill<<<warp_blocks, 256, 0, st>>>(sa);
+        RevSortArgs ra{{roff_new, roff_old}, {rseg_new, rseg_old}, {rscr_new, rscr_old},
+                       {carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr},
+                       n, P<uint32_t>(ws.bigrev), ctr};
+        k_rev_sort_small<<<dim3(warp_blocks, 2), 256, 0, st>>>(ra);
+        k_rev_sort_big<<<nsm * 2, 512, 0, st>>>(ra);
+        // std::rand() draws of this iteration's shuffles
+        k_rand_count<<<tblocks, 256, 0, st>>>(roff_new, roff_old, n, P<uint32_t>(ws.rcount));
+        NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.rcount), P<uint64_t>(ws.rofs), n, scan_tmp, d_tot, st));
+        NNM_CUDA_TRY(glibc_stream_generate(P<int32_t>(ws.rbuf), g.gbase, g.gpos, d_tot, rev_cap * 2, st));
+        ShufArgs sh{roff_new, roff_old, rseg_new, rseg_old, P<uint64_t>(ws.rofs), P<int32_t>(ws.rbuf),
+                    g.newL, g.oldL, g.newlen, g.oldlen,
+                    g.capn, g.capo, n, g.smpl,
+                    track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
+                    track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
+                    smem_rows, P<uint32_t>(ws.bigjoin), ctr};
+        k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh);
+        // local join, pass 1: count proposals per target
+        NNM_CUDA_TRY(cudaMemsetAsync(ws.bcnt.p, 0, n1 * 4, st));
+        NNM_CUDA_TRY(cudaMemsetAsync(ws.bcur.p, 0, n1 * 4, st));
+        JoinArgs ja{g.x, g.dp, K, n, g.pdist, g.newL, g.oldL,
+                    g.newlen, g.oldlen, g.capn, g.capo, caps, (uint32_t)mode, verse,
+                    d_leaf_off, nleaf, P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
+                    P<uint64_t>(ws.boff), P<Prop>(ws.bucket), P<uint32_t>(ws.bigjoin), smem_rows, ctr};
+        if (g.metric == L2) launch_join<L2>(ja, smem_staged, smem_global, PASS_COUNT, st, nsm);
+        else if (g.metric == L1) launch_join<L1>(ja, smem_staged, smem_global, PASS_COUNT, st, nsm);
+        else launch_join<CHI2>(ja, smem_staged, smem_global, PASS_COUNT, st, nsm);
+        NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff), n, scan_tmp,
+                                    reinterpret_cast<uint64_t*>(&ctr->proposals), st));
+        NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
+        NNM_CUDA_TRY(cudaStreamSynchronize(st));
+        if (ctx.h_counters->error) {
+            ctx.last_error = "device capacity check failed (code " + std::to_string(ctx.h_counters->error) + ")";
+            return 6;
+        }
+        const uint64_t nprop = ctx.h_counters->proposals;
+        if (nprop * sizeof(Prop) > ws.bucket.bytes) {
+            NNM_CUDA_TRY(ws.bucket.ensure((size_t)(nprop * 1.25 + 1024) * sizeof(Prop)));
+            ja.bucket = P<Prop>(ws.bucket);
+        }
+        // pass 2: recompute and fill the buckets
+        if (g.metric == L2) launch_join<L2>(ja, smem_staged, smem_global, PASS_FILL, st, nsm);
+        else if (g.metric == L1) launch_join<L1>(ja, smem_staged, smem_global, PASS_FILL, st, nsm);
+        else launch_join<CHI2>(ja, smem_staged, smem_global, PASS_FILL, st, nsm);
+        MergeArgs ma{g.pid, g.pdist, n, K, P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff),
+                     P<Prop>(ws.bucket), P<uint8_t>(ws.nflag), ctr};
+        k_merge<<<(n + MERGE_WARPS - 1) / MERGE_WARPS, MERGE_WARPS * 32, 0, st>>>(ma);
+        NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
+        NNM_CUDA_TRY(cudaMemcpyAsync(&ctx.h_counters->rand_draws, d_tot, 8, cudaMemcpyDeviceToHost, st));
+        NNM_CUDA_TRY(cudaStreamSynchronize(st));
+        NNM_CUDA_TRY(cudaGetLastError());
+        const IterCounters hc = *ctx.h_counters;
+        if (hc.error) {
+            ctx.last_error = "device capacity check failed (code " + std::to_string(hc.error) + ")";
+            return 6;
+        }
+        g.gpos += hc.rand_draws;
+        g.ncmps += hc.ncmps;
+        g.iters++;
+        // Convergence: the reference sums float(c_i)/K in float row by row and
+        // divides by the row count.  The exact flag total decides unless it is
+        // within the float rounding bound of the threshold; then the host
+        // repeats the reference's float sum.
+        const double exact = (double)hc.flags / ((double)K * (double)n);
+        const double slack = 1.05 * ((double)n + 4.0) * std::ldexp(1.0, -24) * exact + 1e-12;
+        float mean;
+        if (!g.exact_trace && std::fabs(exact - (double)g.delta) > slack + 1e-9 * g.delta) {
+            mean = (float)exact;
+        } else {
+            h_nflag.resize(n);
+            NNM_CUDA_TRY(cudaMemcpy(h_nflag.data(), ws.nflag.p, n, cudaMemcpyDeviceToHost));
+            mean = host_mean(h_nflag, n, K);
+        }
+        g.trace.push_back(mean);
+        const bool converged = (std::fabs(exact - (double)g.delta) > slack + 1e-9 * g.delta)
+                                   ? (exact < (double)g.delta)
+                                   : (mean < g.delta);
+        if (converged || (g.max_iter && it + 1 >= g.max_iter)) {
+            g.carry = track;
+            break;
+        }
+        if (it + 1 >= 100000) {
+            ctx.last_error = "NN-Descent did not converge";
+            return 6;
+        }
+    }
+    return 0;
+}
+
+}  // namespace nnm

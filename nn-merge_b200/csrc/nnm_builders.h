@@ -1,0 +1,27 @@
+// Device graph builders (builders.cu).
+#pragma once
+#include <functional>
+#include <vector>
+
+#include "nnm_engine.h"
+
+namespace nnm {
+
+// Called after each H-Merge level that the reference turns into a DPG
+// layer (lynndescent.cpp:767, :780-785, :797-799).
+using LayerHook = std::function<int(Ctx&, GraphDev&)>;
+
+// Copies n_cap x d vectors (host or device) into zero-padded rows of dp
+// floats owned by `store`; sets g.dp and g.x.
+int upload_vectors(Ctx& ctx, GraphStore& store, GraphDev& g, const float* x, bool x_on_device);
+// Writes ids / distances / flags of rows [0, g.n); host or device outputs.
+int export_graph(Ctx& ctx, const GraphDev& g, uint32_t* ids, float* dists, uint8_t* flags, bool host_out);
+
+int kgraph_build(Ctx& ctx, GraphDev& g);
+// Builds one graph per leaf [leaf_off[l], leaf_off[l+1]) and merges them;
+// with two leaves split at n*5/10 this is Smerge::buildKGraph.
+int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, uint64_t* sub_ncmps);
+int jmerge_build(Ctx& ctx, GraphDev& g, uint64_t* sub_ncmps);
+int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer);
+
+}  // namespace nnm

@@ -1,0 +1,117 @@
+// Host-side engine state shared by the NN-Descent driver (nndescent.cu),
+// the graph builders (builders.cu), DPG (dpg.cu), search (search.cu) and the
+// C ABI (capi.cpp).
+#pragma once
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "nnm_nnd.h"
+#include "nnm_rng.h"
+
+namespace nnm {
+
+// Grow-only device allocation.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t b) {
+        if (b <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b ? b : 16);
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Scratch for one NN-Descent iteration, sized for the largest graph seen.
+struct Workspace {
+    DevBuf rcnt, rcur, rtot, roff, rseg, rscr, rcount, rofs, rbuf;
+    DevBuf cntpos, bcnt, bcur, boff, bucket, bigrev, bigjoin, nflag, scan_tmp;
+    DevBuf draws, counters, misc;
+    void release_all() {
+        DevBuf* all[] = {&rcnt, &rcur, &rtot, &roff, &rseg, &rscr, &rcount, &rofs, &rbuf, &cntpos, &bcnt,
+                         &bcur, &boff, &bucket, &bigrev, &bigjoin, &nflag, &scan_tmp, &draws, &counters, &misc};
+        for (auto* b : all) b->release();
+    }
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Workspace ws;
+    IterCounters* h_counters = nullptr;  // pinned
+    std::string last_error;
+    double last_device_ms = 0.0;
+    uint64_t kernel_launches = 0;
+};
+
+// Device storage of a graph under construction (owned buffers).
+struct GraphStore {
+    DevBuf pid, pdist, cpid, cpdist, newL, oldL, newlen, oldlen, rnewT, roldT, rnewTlen, roldTlen, x;
+    void release() {
+        DevBuf* all[] = {&pid, &pdist, &cpid, &cpdist, &newL, &oldL, &newlen, &oldlen,
+                         &rnewT, &roldT, &rnewTlen, &roldTlen, &x};
+        for (auto* b : all) b->release();
+    }
+};
+
+// A graph under construction: raw device pointers, so that a sub-graph
+// (an S-/J-Merge leaf) can run NN-Descent in place inside its parent's
+// arrays.
+struct GraphDev {
+    uint32_t n_cap = 0, n = 0, K = 0, d = 0, dp = 0;
+    int metric = L2;
+    const float* x = nullptr;       // n_cap x dp on the device
+    uint32_t* pid = nullptr;        // pools, n_cap x K
+    float* pdist = nullptr;
+    uint32_t* cpid = nullptr;       // compensation lists, n_cap x K (cut used)
+    float* cpdist = nullptr;
+    uint32_t cut = 0;
+    uint32_t *newL = nullptr, *oldL = nullptr, *newlen = nullptr, *oldlen = nullptr;  // sample lists
+    uint32_t capn = 0, capo = 0;
+    uint32_t *rnewT = nullptr, *roldT = nullptr, *rnewTlen = nullptr, *roldTlen = nullptr;  // H-Merge carry
+    bool carry = false;        // lists of the last converged iteration are still present
+    GlibcBase gbase;
+    uint64_t gpos = 0;         // std::rand() outputs consumed since srand(seed)
+    uint32_t seed = 0;
+    uint32_t smpl = 100;
+    float delta = 0.002f;
+    uint32_t max_iter = 0;     // 0: iterate until the reference's convergence test passes
+    bool exact_trace = false;  // record the reference's float mean every iteration
+    uint64_t ncmps = 0;
+    uint32_t iters = 0;
+    std::vector<float> trace;
+};
+
+#define NNM_CUDA_TRY(expr)                                                         \
+    do {                                                                           \
+        cudaError_t _e = (expr);                                                   \
+        if (_e != cudaSuccess) {                                                   \
+            ctx.last_error = std::string(#expr) + ": " + cudaGetErrorString(_e);   \
+            return _e == cudaErrorMemoryAllocation ? 4 : 3;                        \
+        }                                                                          \
+    } while (0)
+
+// Allocates pools and list storage for up to n_cap rows into `store` and
+// points g at it.  with_carry sizes the lists for one level of carried-over
+// sample lists and keeps the truncated reverse lists (H-Merge).
+int graph_alloc(Ctx& ctx, GraphStore& store, GraphDev& g, bool with_carry);
+// Runs NN-Descent iterations until the reference's convergence test passes
+// (or max_iter).  split: first row of group 1 for the group id of reverse
+// entries; leaf_off/nleaf: group boundaries for MODE_SMERGE.
+int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t verse,
+                  const uint32_t* d_leaf_off, uint32_t nleaf);
+
+}  // namespace nnm

@@ -1,0 +1,47 @@
+// NN-Descent iteration kernels and the device graph they operate on.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "nnm_common.cuh"
+#include "nnm_rng.h"
+
+namespace nnm {
+
+// Join filters of the reference local joins.
+enum JoinMode : uint32_t {
+    MODE_KGRAPH = 0,  // KGraph::join (kgraph.cpp:191-210): all pairs, new x new by id order
+    MODE_SMERGE = 1,  // Smerge::localJoin (smerge.cpp:212-235): groups differ
+    MODE_JMERGE = 2,  // Jmerge::localJoin (jmerge.cpp:178-203): groups differ or either is 1
+    MODE_LY = 3,      // LyNNDescent::localJoin (lynndescent.cpp:313-342): as J-Merge, or verse
+};
+
+// A proposal "insert id into target's pool with distance dist", ordered by
+// (dist, key); key = 2^63 | row << 32 | pair index << 1 | side reproduces the
+// reference's sequential insert order (row ascending, pairs in join order,
+// first insert into the outer element's pool, then the inner's).
+struct __align__(16) Prop {
+    float dist;
+    uint32_t idg;  // id | group bit << 31
+    unsigned long long key;
+};
+
+// Per-iteration statistics read back by the host.
+struct IterCounters {
+    unsigned long long flags;      // pool entries inserted this iteration
+    unsigned long long ncmps;      // distance evaluations in the join
+    unsigned long long proposals;  // bucketed proposals
+    unsigned long long rand_draws; // std::rand() calls of the shuffles
+    unsigned int error;            // nonzero: a capacity or input check failed
+    unsigned int nbig_rev;         // reverse lists longer than one warp
+    unsigned int nbig_join;        // rows whose sample lists exceed shared memory
+    unsigned int pad;
+};
+
+enum DevError : unsigned int {
+    DERR_NONE = 0,
+    DERR_LIST_CAP = 1,      // a sample list overflowed its row capacity
+    DERR_CROSS_SAMPLE = 2,  // a merge found fewer new ids than it needs
+};
+
+}  // namespace nnm

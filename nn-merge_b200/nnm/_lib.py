@@ -1,0 +1,189 @@
+"""ctypes binding of the C ABI in include/nnm.h (lib/libnnm.so).
+
+There is no fallback: if the shared library is missing or no CUDA device is
+present, the calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libnnm.so")
+
+METRICS = {"l2": 0, "l1": 1, "chi2": 2}
+EXPORTED = (
+    "nnm_opts_default", "nnm_status_string", "nnm_last_error", "nnm_ctx_create", "nnm_ctx_destroy",
+    "nnm_kgraph_build", "nnm_kgraph_build_dev", "nnm_smerge", "nnm_jmerge", "nnm_merge_leaves",
+    "nnm_merge_leaves_dev", "nnm_hmerge_build", "nnm_layers_free", "nnm_search",
+)
+
+
+class NnmError(RuntimeError):
+    """A non-zero nnm_status from the library."""
+
+    def __init__(self, status, message):
+        super().__init__("nnm status %d: %s" % (status, message))
+        self.status = status
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint32), ("rng_mode", ctypes.c_uint32), ("metric", ctypes.c_uint32),
+                ("sample_cap", ctypes.c_uint32), ("delta", ctypes.c_float), ("max_iter", ctypes.c_uint32),
+                ("exact_trace", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 9)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("ncmps", ctypes.c_uint64), ("sub_ncmps", ctypes.c_uint64), ("iterations", ctypes.c_uint32),
+                ("n_trace", ctypes.c_uint32), ("trace", ctypes.c_float * 256), ("device_ms", ctypes.c_double)]
+
+
+class Layers(ctypes.Structure):
+    _fields_ = [("nlayers", ctypes.c_uint32), ("nrows", ctypes.c_uint32 * 16),
+                ("off", ctypes.POINTER(ctypes.c_uint64) * 16), ("adj", ctypes.POINTER(ctypes.c_uint32) * 16)]
+
+
+_lib = None
+
+
+def load():
+    """Loads lib/libnnm.so once; raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("nnm: %s not built (run make -C nn-merge_b200)" % LIB_PATH)
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.nnm_status_string.restype = ctypes.c_char_p
+        lib.nnm_last_error.restype = ctypes.c_char_p
+        lib.nnm_ctx_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        lib.nnm_ctx_destroy.argtypes = [ctypes.c_void_p]
+        lib.nnm_last_error.argtypes = [ctypes.c_void_p]
+        vp, u64, u32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32
+        build_args = [vp, vp, u64, u32, u32, vp, vp, vp, vp, vp]
+        for name in ("nnm_kgraph_build", "nnm_kgraph_build_dev", "nnm_smerge", "nnm_jmerge"):
+            getattr(lib, name).argtypes = build_args
+        for name in ("nnm_merge_leaves", "nnm_merge_leaves_dev"):
+            getattr(lib, name).argtypes = [vp, vp, u64, u32, u32, vp, u32, vp, vp, vp, vp, vp]
+        lib.nnm_hmerge_build.argtypes = [vp, vp, u64, u32, u32, u32, vp, vp, vp, vp, vp, vp]
+        lib.nnm_layers_free.argtypes = [vp]
+        lib.nnm_search.argtypes = [vp, vp, u64, u32, vp, vp, u64, u32, vp, vp, vp, vp]
+        _lib = lib
+    return _lib
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exact_trace=False):
+    lib = load()
+    o = Opts()
+    lib.nnm_opts_default(ctypes.byref(o))
+    o.seed = seed
+    o.metric = METRICS[metric] if isinstance(metric, str) else int(metric)
+    o.sample_cap = sample_cap
+    o.delta = delta
+    o.max_iter = max_iter
+    o.exact_trace = 1 if exact_trace else 0
+    return o
+
+
+def _stats_dict(st):
+    return dict(ncmps=int(st.ncmps), sub_ncmps=int(st.sub_ncmps), iterations=int(st.iterations),
+                trace=np.array(st.trace[: st.n_trace], np.float32), device_ms=float(st.device_ms))
+
+
+class Context:
+    """One CUDA device + stream (nnm_ctx)."""
+
+    def __init__(self, device=0):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        rc = self.lib.nnm_ctx_create(device, ctypes.byref(h))
+        if rc != 0:
+            raise NnmError(rc, self.lib.nnm_status_string(rc).decode())
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.nnm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = self.lib.nnm_last_error(self.h).decode()
+            raise NnmError(rc, "%s: %s" % (self.lib.nnm_status_string(rc).decode(), msg))
+
+    def _build(self, fn, x, k, opts, extra=()):
+        x = np.ascontiguousarray(x, np.float32)
+        n, d = x.shape
+        ids = np.empty((n, k), np.uint32)
+        dists = np.empty((n, k), np.float32)
+        flags = np.empty((n, k), np.uint8)
+        st = Stats()
+        head = [self.h, _ptr(x), n, d, k]
+        tail = [ctypes.byref(opts), _ptr(ids), _ptr(dists), _ptr(flags), ctypes.byref(st)]
+        self._check(fn(*(head + list(extra) + tail)))
+        return dict(ids=ids, dists=dists, flags=flags, **_stats_dict(st))
+
+    def kgraph(self, x, k, **kw):
+        return self._build(self.lib.nnm_kgraph_build, x, k, make_opts(**kw))
+
+    def smerge(self, x, k, **kw):
+        return self._build(self.lib.nnm_smerge, x, k, make_opts(**kw))
+
+    def jmerge(self, x, k, **kw):
+        return self._build(self.lib.nnm_jmerge, x, k, make_opts(**kw))
+
+    def merge_leaves(self, x, k, leaf_sizes, **kw):
+        sizes = np.ascontiguousarray(leaf_sizes, np.uint32)
+        return self._build(self.lib.nnm_merge_leaves, x, k, make_opts(**kw), extra=(_ptr(sizes), len(sizes)))
+
+    def hmerge(self, x, k, m, **kw):
+        x = np.ascontiguousarray(x, np.float32)
+        n, d = x.shape
+        ids = np.empty((n, k), np.uint32)
+        dists = np.empty((n, k), np.float32)
+        flags = np.empty((n, k), np.uint8)
+        st = Stats()
+        lay = Layers()
+        o = make_opts(**kw)
+        self._check(self.lib.nnm_hmerge_build(self.h, _ptr(x), n, d, k, m, ctypes.byref(o), _ptr(ids),
+                                              _ptr(dists), _ptr(flags), ctypes.byref(lay), ctypes.byref(st)))
+        layers = []
+        for g in range(lay.nlayers):
+            nr = lay.nrows[g]
+            off = np.ctypeslib.as_array(lay.off[g], shape=(nr + 1,)).copy()
+            tot = int(off[-1])
+            adj = np.ctypeslib.as_array(lay.adj[g], shape=(max(tot, 1),))[:tot].copy()
+            layers.append((off, adj))
+        self.lib.nnm_layers_free(ctypes.byref(lay))
+        return dict(ids=ids, dists=dists, flags=flags, layers=layers, **_stats_dict(st))
+
+    def search(self, x, layers, q, topk, seed=0, metric="l2"):
+        x = np.ascontiguousarray(x, np.float32)
+        q = np.ascontiguousarray(q, np.float32)
+        lay = Layers()
+        lay.nlayers = len(layers)
+        keep = []
+        for g, (off, adj) in enumerate(layers):
+            off = np.ascontiguousarray(off, np.uint64)
+            adj = np.ascontiguousarray(adj if len(adj) else np.zeros(1, np.uint32), np.uint32)
+            keep += [off, adj]
+            lay.nrows[g] = len(off) - 1
+            lay.off[g] = off.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+            lay.adj[g] = adj.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        nq = q.shape[0]
+        ids = np.empty((nq, topk), np.uint32)
+        ds = np.empty((nq, topk), np.float32)
+        nc = ctypes.c_uint64(0)
+        o = make_opts(seed=seed, metric=metric)
+        self._check(self.lib.nnm_search(self.h, _ptr(x), x.shape[0], x.shape[1], ctypes.byref(lay), _ptr(q), nq,
+                                        topk, ctypes.byref(o), _ptr(ids), _ptr(ds), ctypes.byref(nc)))
+        return dict(ids=ids, dists=ds, ncmps=int(nc.value))
