@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Headline benchmark: build time of a 1M x 128, k=20 k-NN graph.
+
+Workload (one step = one complete build): 1,000,000 x 128 float32 vectors
+from a seeded 256-centre Gaussian mixture (integer values 0-255, the shape of
+SIFT-like descriptors), split into 4 leaves of 250,000 rows; every leaf is
+built with NN-Descent and the leaves are S-Merged (each row keeps its best
+k - k/2 entries, samples k/2 ids from the other leaves, cross-leaf
+NN-Descent, merge2one).  The CUDA path is reference-exact: with two leaves it
+equals Smerge::buildKGraph bit for bit.
+
+Printed JSON (one line, rank 0):
+  value       seconds per build with the vectors already resident in HBM
+              (nnm_merge_leaves_dev), max over ranks;
+  e2e         the same through the host C ABI (nnm_merge_leaves): pinned
+              host vectors copied in, the graph (ids) copied back, per step;
+  roofline    the dominant kernel (the local join) from the library's own
+              CUDA-event timing and algorithmic byte count;
+  cpu_baseline the reference itself (oracle/_ref, built from its sources) on
+              a bounded sample, extrapolated linearly to 1M rows.
+
+--impl reference times the reference's CPU path instead (rank 0 only).
+Multi-GPU (torchrun, N > 1): every rank builds its own 1M graph from its own
+seeded data (independent replicas, weak scaling), timed as the max over ranks.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "nn-merge_b200"))
+
+METRIC = "1M×128 k=20 build s at recall@10≥0.95: learned+BF16 vs plain FP32 GPU"
+HBM_FALLBACK = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="nnm", choices=["nnm", "reference"])
+    p.add_argument("--n", type=int, default=1_000_000)
+    p.add_argument("--d", type=int, default=128)
+    p.add_argument("--k", type=int, default=20)
+    p.add_argument("--leaves", type=int, default=4)
+    p.add_argument("--centres", type=int, default=256)
+    p.add_argument("--seed", type=int, default=1234)
+    p.add_argument("--recall-rows", type=int, default=2000)
+    p.add_argument("--cpu-sample", type=int, default=40_000)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+def leaf_sizes(n, leaves):
+    base = n // leaves
+    sizes = [base] * leaves
+    sizes[-1] += n - base * leaves
+    return sizes
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def recall_at(ids, x_t, rows, atop, torch):
+    """Recall@atop of the graph rows `rows` against exact brute force
+    (FP32 squared L2 without TF32: exact for integer data), counting an
+    entry as a hit when its exact distance is within the atop-th exact
+    distance (ties counted as hits)."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        q = x_t[rows]
+        qn = (q * q).sum(1, keepdim=True)
+        xn = (x_t * x_t).sum(1)
+        hits = 0
+        for b in range(0, len(rows), 256):
+            qb, qnb = q[b:b + 256], qn[b:b + 256]
+            d = qnb + xn[None, :] - 2.0 * (qb @ x_t.T)
+            d[torch.arange(len(qb)), torch.as_tensor(rows[b:b + 256], device=d.device)] = float("inf")
+            kth = torch.topk(d, atop, dim=1, largest=False).values[:, -1:]
+            g = torch.as_tensor(ids[b:b + 256, :atop].astype(np.int64), device=d.device)
+            hits += int((torch.gather(d, 1, g) <= kth).sum())
+        return hits / (len(rows) * atop)
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+def reference_cpu(x, k, seed, sample):
+    """Times the reference on the first `sample` rows: S-Merge with its own
+    split (smerge.cpp:53).  Returns (seconds, kind, cores, note)."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "nnm_ref")
+    xs = np.ascontiguousarray(x[:sample])
+    if os.path.exists(ref):
+        with tempfile.TemporaryDirectory() as td:
+            mat = os.path.join(td, "in.mat")
+            with open(mat, "wb") as f:
+                f.write(np.array(xs.shape, np.uint32).tobytes())
+                f.write(xs.tobytes())
+            t0 = time.perf_counter()
+            subprocess.run([ref, "smerge", "l2", mat, str(k), str(seed), os.path.join(td, "out")],
+                           check=True, capture_output=True, cwd=td)
+            return time.perf_counter() - t0, "reference", 1
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    o = Oracle()
+    t0 = time.perf_counter()
+    o.smerge(xs, k, seed)
+    return time.perf_counter() - t0, "port", 1
+
+
+def run_reference_arm(a, rank):
+    if rank != 0:
+        return
+    from nnm.datasets import gaussian_mixture_u8
+    x = gaussian_mixture_u8(a.n if a.cpu_sample > a.n else a.cpu_sample, d=a.d, n_centres=a.centres, seed=a.seed)
+    times = []
+    kind = "reference"
+    for step in range(min(a.warmup, 1) + a.steps):
+        t, kind, cores = reference_cpu(x, a.k, a.seed, a.cpu_sample)
+        if step >= min(a.warmup, 1):
+            times.append(t)
+    scale = a.n / a.cpu_sample
+    v = statistics.median(times) * scale
+    line = {
+        "metric": METRIC, "impl": "reference", "value": v, "unit": "s", "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": statistics.median(times) * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded %d-centre Gaussian mixture, integers 0-255" % a.centres,
+        "config": {"workload": "S-Merge (smerge.cpp:46-91) of the first %d rows, seconds scaled by %.1f to %d rows "
+                               "(linear in n: a lower bound for NN-Descent)" % (a.cpu_sample, scale, a.n),
+                   "n": a.n, "d": a.d, "k": a.k},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": kind,
+                         "sample": "%d rows, S-Merge, single thread (the reference has no threading)" % a.cpu_sample},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference_arm(a, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import nnm
+    from nnm.datasets import gaussian_mixture_u8
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = True
+
+    def barrier():
+        if pg:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if not pg:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n, d, k = a.n, a.d, a.k
+    sizes = leaf_sizes(n, a.leaves)
+    x = gaussian_mixture_u8(n, d=d, n_centres=a.centres, seed=a.seed + rank)
+    x_dev = torch.from_numpy(x).cuda()
+    ids_dev = torch.empty((n, k), dtype=torch.int32, device="cuda")
+    dists_dev = torch.empty((n, k), dtype=torch.float32, device="cuda")
+    ctx = nnm.Context(local)
+    build_seed = a.seed
+
+    def build_dev():
+        return ctx.merge_leaves_dev(x_dev.data_ptr(), n, d, k, sizes, ids_dev.data_ptr(), dists_dev.data_ptr(), 0,
+                                    seed=build_seed)
+
+    for _ in range(a.warmup):
+        st = build_dev()
+    torch.cuda.synchronize()
+    ctx.profile(True)
+    l0 = ctx.launch_count()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(a.steps):
+            st = build_dev()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    launches = ctx.launch_count() - l0
+    prof = ctx.profile_stats()
+    ctx.profile(False)
+    # builds run on the library's stream and synchronize before returning, so
+    # the events on torch's stream bracket them
+    ms = ev0.elapsed_time(ev1) / a.steps
+    ms = max_over_ranks(ms)
+
+    # end to end through the host C ABI: pinned host input, graph ids back
+    e2e = None
+    if not a.no_e2e:
+        x_pin = torch.from_numpy(x).pin_memory()
+        ids_pin = torch.empty((n, k), dtype=torch.int32).pin_memory()
+        xh, ih = x_pin.numpy(), ids_pin.numpy().view(np.uint32)
+        ctx.merge_leaves_into(xh, k, sizes, ih, seed=build_seed)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            ctx.merge_leaves_into(xh, k, sizes, ih, seed=build_seed)
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / a.steps)
+        e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(x.nbytes),
+               "d2h_bytes_per_step": int(n * k * 4)}
+
+    # quality: recall@10 on a seeded row sample vs exact brute force
+    rng = np.random.default_rng(7)
+    rows = np.sort(rng.choice(n, min(a.recall_rows, n), replace=False))
+    ids_np = ids_dev[torch.as_tensor(rows, device="cuda")].cpu().numpy().view(np.uint32)
+    rec = recall_at(ids_np, x_dev, rows, 10, torch)
+
+    hbm, peak_kind = peaks()
+    j = prof["join"]
+    roof = None
+    if j["launches"]:
+        per_ms = j["ms"] / j["launches"]
+        per_bytes = j["bytes"] / j["launches"]
+        achieved = per_bytes / (per_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "local join (k_join_staged/_global, count+fill passes)",
+                "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "peak_kind": peak_kind, "traffic": None,
+                "fp32_pipe_tflops": j["flops"] / j["launches"] / (per_ms * 1e-3) / 1e12,
+                "join_share_of_step": j["ms"] / (ms * a.steps)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        t, kind, cores = reference_cpu(x, k, build_seed, a.cpu_sample)
+        cpu = {"value": t * n / a.cpu_sample, "unit": "s", "cores": cores, "kind": kind,
+               "sample": "S-Merge of the first %d rows (%.1f s measured), scaled linearly to %d rows"
+                         % (a.cpu_sample, t, n)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded %d-centre Gaussian mixture, integers 0-255 (stand-in for SIFT-like data)"
+                    % a.centres,
+            "config": {"workload": "%dx%d k=%d: NN-Descent on %d leaves of %d rows + S-Merge of the leaves "
+                                   "(plain FP32, reference-exact)" % (n, d, k, a.leaves, sizes[0]),
+                       "n": n, "d": d, "k": k, "leaves": a.leaves, "path": "plain_fp32_exact",
+                       "recall@10": rec, "iterations": st["iterations"], "ncmps_merge": st["ncmps"],
+                       "ncmps_leaves": st["sub_ncmps"],
+                       "l2": "inputs (%d MB) larger than L2 (126 MB)" % (x.nbytes >> 20),
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

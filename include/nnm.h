@@ -138,6 +138,15 @@ int nnm_search(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, const nnm_l
                const float *q, uint64_t nq, uint32_t topk, const nnm_opts *opts,
                uint32_t *out_ids, float *out_dists, uint64_t *ncmps);
 
+/* Profiling (no counterpart in the reference, which times whole builds with
+ * boost::timer): while enabled, the engine records CUDA events around its
+ * local-join and top-K merge kernels and accumulates their device time and
+ * algorithmic bytes / flops.  nnm_profile_get writes them as a JSON object. */
+int nnm_profile_enable(nnm_ctx *ctx, int on);
+int nnm_profile_get(const nnm_ctx *ctx, char *buf, uint64_t buflen);
+/* Kernel launches made by this library in this process so far. */
+uint64_t nnm_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

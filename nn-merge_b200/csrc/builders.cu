@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "nnm_builders.h"
+#include "nnm_launch.h"
 #include "nnm_scan.h"
 
 namespace nnm {
@@ -299,7 +300,7 @@ int upload_vectors(Ctx& ctx, GraphStore& s, GraphDev& g, const float* x, bool x_
             NNM_CUDA_TRY(cudaMemcpyAsync(tmp.p, x, (size_t)g.n_cap * g.d * 4, cudaMemcpyHostToDevice, ctx.stream));
             src = tmp.as<float>();
         }
-        k_pad_copy<<<blocks_for(elems, 256), 256, 0, ctx.stream>>>(src, s.x.as<float>(), g.n_cap, g.d, g.dp);
+        k_pad_copy<<<blocks_for(elems, 256), 256, 0, ctx.stream>>>(src, s.x.as<float>(), g.n_cap, g.d, g.dp); count_launch();
         NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
         tmp.release();
     }
@@ -310,7 +311,7 @@ int upload_vectors(Ctx& ctx, GraphStore& s, GraphDev& g, const float* x, bool x_
 int export_graph(Ctx& ctx, const GraphDev& g, uint32_t* ids, float* dists, uint8_t* flags, bool host_out) {
     const size_t cnt = (size_t)g.n * g.K;
     if (!host_out) {
-        k_export<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid, g.pdist, cnt, ids, dists, flags);
+        k_export<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid, g.pdist, cnt, ids, dists, flags); count_launch();
         NNM_CUDA_TRY(cudaGetLastError());
         return 0;
     }
@@ -319,7 +320,7 @@ int export_graph(Ctx& ctx, const GraphDev& g, uint32_t* ids, float* dists, uint8
     uint32_t* di = tmp.as<uint32_t>();
     float* dd = reinterpret_cast<float*>(di + cnt);
     uint8_t* df = reinterpret_cast<uint8_t*>(dd + cnt);
-    k_export<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid, g.pdist, cnt, di, dd, df);
+    k_export<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid, g.pdist, cnt, di, dd, df); count_launch();
     if (ids) NNM_CUDA_TRY(cudaMemcpyAsync(ids, di, cnt * 4, cudaMemcpyDeviceToHost, ctx.stream));
     if (dists) NNM_CUDA_TRY(cudaMemcpyAsync(dists, dd, cnt * 4, cudaMemcpyDeviceToHost, ctx.stream));
     if (flags) NNM_CUDA_TRY(cudaMemcpyAsync(flags, df, cnt, cudaMemcpyDeviceToHost, ctx.stream));
@@ -338,7 +339,7 @@ int kgraph_build(Ctx& ctx, GraphDev& g) {
     if ((rc = reset_counters(ctx))) return rc;
     InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>(), per, K + 1, n, 0, n,
                 0xffffffffu, ctx.ws.counters.as<IterCounters>()};
-    k_init_rows<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(ia);
+    k_init_rows<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(ia); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     if ((rc = check_counters(ctx))) return rc;
     g.ncmps += (uint64_t)n * K;
@@ -378,7 +379,7 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
         subc += s.ncmps;
         absorb(g, s);
         size_t cnt = (size_t)s.n * K;
-        k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(s.pid, cnt, leaf_off[l], nleaf == 2 ? l : 0u);
+        k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(s.pid, cnt, leaf_off[l], nleaf == 2 ? l : 0u); count_launch();
     }
     if (sub_ncmps) *sub_ncmps = subc;
     // 2. cross sampling (smerge.cpp:94-209)
@@ -408,7 +409,7 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
                          ctx.ws.draws.as<uint32_t>() + off, per[l], 2 * g.cut, g.cut, r0, r1,
                          lo.as<uint32_t>(), nleaf, 0, 0, nleaf == 2 ? (l == 0 ? 1u : 0u) : 0u,
                          ctx.ws.counters.as<IterCounters>()};
-            k_cross_sample<<<blocks_for(r1 - r0, WPB), WPB * 32, 0, ctx.stream>>>(ca);
+            k_cross_sample<<<blocks_for(r1 - r0, WPB), WPB * 32, 0, ctx.stream>>>(ca); count_launch();
             off += (size_t)(r1 - r0) * per[l];
         }
         NNM_CUDA_TRY(cudaGetLastError());
@@ -418,7 +419,7 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
         rc = run_nndescent(ctx, g, MODE_SMERGE, leaf_off[1], 0, lo.as<uint32_t>(), nleaf);
         if (rc) return rc;
     }
-    k_merge2one<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, n);
+    k_merge2one<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, n); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -430,7 +431,7 @@ int jmerge_build(Ctx& ctx, GraphDev& g, uint64_t* sub_ncmps) {
     if ((rc = kgraph_build(ctx, s))) return rc;
     if (sub_ncmps) *sub_ncmps = s.ncmps;
     absorb(g, s);
-    k_rebase<<<blocks_for((size_t)pre * K, 256), 256, 0, ctx.stream>>>(g.pid, (size_t)pre * K, 0, 0);
+    k_rebase<<<blocks_for((size_t)pre * K, 256), 256, 0, ctx.stream>>>(g.pid, (size_t)pre * K, 0, 0); count_launch();
     g.cut = K * 3 / 6;                                    // jmerge.cpp:87
     const uint32_t per_old = sds_draws(2 * g.cut, n - pre), per_new = sds_draws(K + 1, n);
     size_t total = (size_t)pre * per_old + (size_t)(n - pre) * per_new;
@@ -440,15 +441,15 @@ int jmerge_build(Ctx& ctx, GraphDev& g, uint64_t* sub_ncmps) {
     if ((rc = reset_counters(ctx))) return rc;
     CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist, ctx.ws.draws.as<uint32_t>(), per_old,
                  2 * g.cut, g.cut, 0, pre, nullptr, 0, pre, n - pre, 1, ctx.ws.counters.as<IterCounters>()};
-    k_cross_sample<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(ca);
+    k_cross_sample<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(ca); count_launch();
     InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>() + (size_t)pre * per_old,
                 per_new, K + 1, n, pre, n, pre, ctx.ws.counters.as<IterCounters>()};
-    k_init_rows<<<blocks_for(n - pre, WPB), WPB * 32, 0, ctx.stream>>>(ia);
+    k_init_rows<<<blocks_for(n - pre, WPB), WPB * 32, 0, ctx.stream>>>(ia); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     if ((rc = check_counters(ctx))) return rc;
     g.ncmps += (uint64_t)pre * g.cut + (uint64_t)(n - pre) * K;
     if ((rc = run_nndescent(ctx, g, MODE_JMERGE, pre, 0, nullptr, 0))) return rc;
-    k_merge2one<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, pre);
+    k_merge2one<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, pre); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -465,7 +466,7 @@ int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer) {
         if ((rc = reset_counters(ctx))) return rc;
         InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>(), per, K + 1, N0, 0, N0,
                     0xffffffffu, ctx.ws.counters.as<IterCounters>()};
-        k_init_rows<<<blocks_for(N0, WPB), WPB * 32, 0, ctx.stream>>>(ia);
+        k_init_rows<<<blocks_for(N0, WPB), WPB * 32, 0, ctx.stream>>>(ia); count_launch();
         if ((rc = check_counters(ctx))) return rc;
         g.ncmps += (uint64_t)N0 * K;
     }
@@ -490,10 +491,10 @@ int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer) {
         g.cut = hsize;
         CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist, ctx.ws.draws.as<uint32_t>(), per_old,
                      2 * half, hsize, 0, sz, nullptr, 0, lst, bnum, 1, ctx.ws.counters.as<IterCounters>()};
-        k_cross_sample<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(ca);
+        k_cross_sample<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(ca); count_launch();
         InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>() + (size_t)sz * per_old,
                     per_new, 2 * K, sz + bnum, sz, sz + bnum, lst, ctx.ws.counters.as<IterCounters>()};
-        k_init_rows<<<blocks_for(bnum, WPB), WPB * 32, 0, ctx.stream>>>(ia);
+        k_init_rows<<<blocks_for(bnum, WPB), WPB * 32, 0, ctx.stream>>>(ia); count_launch();
         NNM_CUDA_TRY(cudaGetLastError());
         if ((rc = check_counters(ctx))) return rc;
         g.ncmps += (uint64_t)sz * hsize + (uint64_t)bnum * K;
@@ -501,7 +502,7 @@ int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer) {
         last_id = lst + bnum;
         total -= bnum;
         if ((rc = run_nndescent(ctx, g, MODE_LY, lst, 0, nullptr, 0))) return rc;
-        k_merge2one<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, hsize, sz);
+        k_merge2one<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, hsize, sz); count_launch();
         NNM_CUDA_TRY(cudaGetLastError());
         if (last || (count_level < 10 && level[count_level]))
             if ((rc = on_layer(ctx, g))) return rc;
@@ -509,7 +510,7 @@ int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer) {
         if (!last) {
             smpl = g.n;
             size_t cnt = (size_t)g.n * K;
-            k_clear_gd<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid, cnt);  // setflag
+            k_clear_gd<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid, cnt); count_launch();  // setflag
         }
     }
     NNM_CUDA_TRY(cudaGetLastError());

@@ -7,6 +7,7 @@
 #include "../../include/nnm.h"
 #include "nnm_builders.h"
 #include "nnm_hier.h"
+#include "nnm_launch.h"
 
 struct nnm_ctx {
     nnm::Ctx c;
@@ -186,6 +187,8 @@ int nnm_ctx_destroy(nnm_ctx* ctx) {
     if (!ctx) return NNM_OK;
     cudaSetDevice(ctx->c.device);
     cudaStreamSynchronize(ctx->c.stream);
+    for (auto& e : ctx->c.ev)
+        if (e) cudaEventDestroy(e);
     ctx->c.ws.release_all();
     if (ctx->c.h_counters) cudaFreeHost(ctx->c.h_counters);
     if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
@@ -260,6 +263,31 @@ int nnm_hmerge_build(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint3
     else if (layers) nnm_layers_free(layers);
     return rc;
 }
+
+int nnm_profile_enable(nnm_ctx* ctx, int on) {
+    if (!ctx) return NNM_ERR_INVALID;
+    if (on && !ctx->c.ev[0]) {
+        cudaSetDevice(ctx->c.device);
+        for (auto& e : ctx->c.ev)
+            if (cudaEventCreate(&e) != cudaSuccess) return fail(ctx, NNM_ERR_CUDA, "cudaEventCreate failed");
+    }
+    ctx->c.prof = on != 0;
+    ctx->c.kjoin = ctx->c.kmerge = ctx->c.kiter = nnm::KStat();
+    return NNM_OK;
+}
+
+int nnm_profile_get(const nnm_ctx* ctx, char* buf, uint64_t buflen) {
+    if (!ctx || !buf || buflen == 0) return NNM_ERR_INVALID;
+    const nnm::Ctx& c = ctx->c;
+    int w = std::snprintf(buf, buflen,
+                          "{\"join\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f, \"flops\": %.1f}, "
+                          "\"merge\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}}",
+                          (unsigned long long)c.kjoin.launches, c.kjoin.ms, c.kjoin.bytes, c.kjoin.flops,
+                          (unsigned long long)c.kmerge.launches, c.kmerge.ms, c.kmerge.bytes);
+    return (w < 0 || (uint64_t)w >= buflen) ? NNM_ERR_INVALID : NNM_OK;
+}
+
+uint64_t nnm_launch_count(void) { return nnm::launch_counter().load(); }
 
 void nnm_layers_free(nnm_layers* layers) {
     if (!layers) return;

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "nnm_hier.h"
+#include "nnm_launch.h"
 #include "nnm_scan.h"
 
 namespace nnm {
@@ -342,7 +343,7 @@ int dpg_layer(Ctx& ctx, DpgState& s, GraphDev& g, nnm_layers* out) {
     DpgCtr* ctr = s.counters.as<DpgCtr>();
     FwdArgs fa{g.x, g.dp, g.metric, g.pid, g.pdist, g.K, N, C, Mo, s.gid.as<uint32_t>(), s.glen.as<uint32_t>(),
                s.gdist.as<float>(), s.g1id.as<uint32_t>(), s.g1len.as<uint32_t>(), s.g1dist.as<float>()};
-    k_dpg_forward<<<nblk(N, WPB), WPB * 32, 0, st>>>(fa);
+    k_dpg_forward<<<nblk(N, WPB), WPB * 32, 0, st>>>(fa); count_launch();
     // initial guess: snapshots = forward lists
     NNM_CUDA_TRY(cudaMemcpyAsync(s.sid.p, s.g1id.p, (size_t)N * C * 4, cudaMemcpyDeviceToDevice, st));
     NNM_CUDA_TRY(cudaMemcpyAsync(s.sdist.p, s.g1dist.p, (size_t)N * C * 4, cudaMemcpyDeviceToDevice, st));
@@ -355,20 +356,20 @@ int dpg_layer(Ctx& ctx, DpgState& s, GraphDev& g, nnm_layers* out) {
         NNM_CUDA_TRY(cudaMemsetAsync(s.ecnt.p, 0, (size_t)N * 4, st));
         NNM_CUDA_TRY(cudaMemsetAsync(s.ecur.p, 0, (size_t)N * 4, st));
         k_ev_count<<<nblk(N, WPB), WPB * 32, 0, st>>>(s.sid.as<uint32_t>(), s.slen.as<uint32_t>(), N, C,
-                                                         s.ecnt.as<uint32_t>());
+                                                         s.ecnt.as<uint32_t>()); count_launch();
         NNM_CUDA_TRY(exclusive_scan(s.ecnt.as<uint32_t>(), s.eoff.as<uint64_t>(), N, s.tmp.as<uint64_t>(), nullptr, st));
         k_ev_fill<<<nblk(N, WPB), WPB * 32, 0, st>>>(s.sid.as<uint32_t>(), s.sdist.as<float>(), s.slen.as<uint32_t>(),
                                                         N, C, s.eoff.as<uint64_t>(), s.ecur.as<uint32_t>(),
-                                                        s.ev.as<unsigned long long>());
+                                                        s.ev.as<unsigned long long>()); count_launch();
         k_ev_sort_small<<<nblk(N, 8), 256, 0, st>>>(s.eoff.as<uint64_t>(), s.ev.as<unsigned long long>(), N,
-                                                    s.bigseg.as<uint32_t>(), ctr);
+                                                    s.bigseg.as<uint32_t>(), ctr); count_launch();
         k_ev_sort_big<<<296, 512, 0, st>>>(s.eoff.as<uint64_t>(), s.ev.as<unsigned long long>(),
-                                           s.escr.as<unsigned long long>(), s.bigseg.as<uint32_t>(), ctr);
+                                           s.escr.as<unsigned long long>(), s.bigseg.as<uint32_t>(), ctr); count_launch();
         RevArgs ra{g.x, g.dp, g.metric, N, C, maxM, s.g1id.as<uint32_t>(), s.g1len.as<uint32_t>(),
                    s.g1dist.as<float>(), s.eoff.as<uint64_t>(), s.ev.as<unsigned long long>(),
                    s.sid.as<uint32_t>(), s.slen.as<uint32_t>(), s.tid.as<uint32_t>(), s.tlen.as<uint32_t>(),
                    s.tdist.as<float>(), s.gid.as<uint32_t>(), s.glen.as<uint32_t>(), s.gdist.as<float>(), ctr};
-        k_dpg_reverse<<<nblk(N, WPB), WPB * 32, 0, st>>>(ra);
+        k_dpg_reverse<<<nblk(N, WPB), WPB * 32, 0, st>>>(ra); count_launch();
         NNM_CUDA_TRY(cudaMemcpyAsync(&h, ctr, sizeof(DpgCtr), cudaMemcpyDeviceToHost, st));
         NNM_CUDA_TRY(cudaStreamSynchronize(st));
         NNM_CUDA_TRY(cudaGetLastError());

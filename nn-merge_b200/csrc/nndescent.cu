@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "nnm_engine.h"
+#include "nnm_launch.h"
 #include "nnm_scan.h"
 
 namespace nnm {
@@ -376,6 +377,7 @@ __device__ void join_row(const JoinArgs& a, uint32_t row, unsigned char* smem) {
     }
     __syncthreads();
 
+    if (PASS == PASS_COUNT && threadIdx.x == 0) atomicAdd(&a.ctr->sum_s, (unsigned long long)S);
     const uint32_t ntA = (nn + 3) >> 2, ntB = (S + 3) >> 2;
     const uint32_t ntiles = ntA * ntB - ntA * (ntA - 1) / 2;
     uint32_t cmps = 0;
@@ -708,11 +710,11 @@ template <int M>
 static void launch_join(const JoinArgs& ja, size_t smem_staged, size_t smem_global, int pass, cudaStream_t st,
                         int nsm) {
     if (pass == PASS_COUNT) {
-        k_join_staged<M, PASS_COUNT><<<ja.n, JOIN_THREADS, smem_staged, st>>>(ja);
-        k_join_global<M, PASS_COUNT><<<nsm * 2, JOIN_THREADS, smem_global, st>>>(ja);
+        k_join_staged<M, PASS_COUNT><<<ja.n, JOIN_THREADS, smem_staged, st>>>(ja); count_launch();
+        k_join_global<M, PASS_COUNT><<<nsm * 2, JOIN_THREADS, smem_global, st>>>(ja); count_launch();
     } else {
-        k_join_staged<M, PASS_FILL><<<ja.n, JOIN_THREADS, smem_staged, st>>>(ja);
-        k_join_global<M, PASS_FILL><<<nsm * 2, JOIN_THREADS, smem_global, st>>>(ja);
+        k_join_staged<M, PASS_FILL><<<ja.n, JOIN_THREADS, smem_staged, st>>>(ja); count_launch();
+        k_join_global<M, PASS_FILL><<<nsm * 2, JOIN_THREADS, smem_global, st>>>(ja); count_launch();
     }
 }
 
@@ -797,14 +799,14 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         if (!carry_now) {
             k_clear_lists<<<tblocks, 256, 0, st>>>(g.newlen, g.oldlen,
                                                    track ? g.rnewTlen : nullptr,
-                                                   track ? g.roldTlen : nullptr, n);
+                                                   track ? g.roldTlen : nullptr, n); count_launch();
         }
         NNM_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(IterCounters), st));
         // reverse counts and cursors start at the carried lengths
-        k_set_u32<<<tblocks, 256, 0, st>>>(rcnt_new, track ? g.rnewTlen : nullptr, n);
-        k_set_u32<<<tblocks, 256, 0, st>>>(rcnt_old, track ? g.roldTlen : nullptr, n);
-        k_set_u32<<<tblocks, 256, 0, st>>>(rcur_new, track ? g.rnewTlen : nullptr, n);
-        k_set_u32<<<tblocks, 256, 0, st>>>(rcur_old, track ? g.roldTlen : nullptr, n);
+        k_set_u32<<<tblocks, 256, 0, st>>>(rcnt_new, track ? g.rnewTlen : nullptr, n); count_launch();
+        k_set_u32<<<tblocks, 256, 0, st>>>(rcnt_old, track ? g.roldTlen : nullptr, n); count_launch();
+        k_set_u32<<<tblocks, 256, 0, st>>>(rcur_new, track ? g.rnewTlen : nullptr, n); count_launch();
+        k_set_u32<<<tblocks, 256, 0, st>>>(rcur_old, track ? g.roldTlen : nullptr, n); count_launch();
         SampleArgs sa{g.pid, g.pdist, n, K, (uint32_t)mode, split,
                       rcnt_new, rcnt_old, rcur_new, rcur_old, roff_new, roff_old, rseg_new, rseg_old,
                       g.newL, g.oldL, g.newlen, g.oldlen,
@@ -812,17 +814,17 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                       carry_now ? g.rnewT : nullptr, carry_now ? g.roldT : nullptr,
                       carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr,
                       g.smpl, ctr};
-        k_sample_count<<<warp_blocks, 256, 0, st>>>(sa);
+        k_sample_count<<<warp_blocks, 256, 0, st>>>(sa); count_launch();
         NNM_CUDA_TRY(exclusive_scan(rcnt_new, roff_new, n, scan_tmp, nullptr, st));
         NNM_CUDA_TRY(exclusive_scan(rcnt_old, roff_old, n, scan_tmp, nullptr, st));
-        k_sample_fill<<<warp_blocks, 256, 0, st>>>(sa);
+        k_sample_fill<<<warp_blocks, 256, 0, st>>>(sa); count_launch();
         RevSortArgs ra{{roff_new, roff_old}, {rseg_new, rseg_old}, {rscr_new, rscr_old},
                        {carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr},
                        n, P<uint32_t>(ws.bigrev), ctr};
-        k_rev_sort_small<<<dim3(warp_blocks, 2), 256, 0, st>>>(ra);
-        k_rev_sort_big<<<nsm * 2, 512, 0, st>>>(ra);
+        k_rev_sort_small<<<dim3(warp_blocks, 2), 256, 0, st>>>(ra); count_launch();
+        k_rev_sort_big<<<nsm * 2, 512, 0, st>>>(ra); count_launch();
         // std::rand() draws of this iteration's shuffles
-        k_rand_count<<<tblocks, 256, 0, st>>>(roff_new, roff_old, n, P<uint32_t>(ws.rcount));
+        k_rand_count<<<tblocks, 256, 0, st>>>(roff_new, roff_old, n, P<uint32_t>(ws.rcount)); count_launch();
         NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.rcount), P<uint64_t>(ws.rofs), n, scan_tmp, d_tot, st));
         NNM_CUDA_TRY(glibc_stream_generate(P<int32_t>(ws.rbuf), g.gbase, g.gpos, d_tot, rev_cap * 2, st));
         ShufArgs sh{roff_new, roff_old, rseg_new, rseg_old, P<uint64_t>(ws.rofs), P<int32_t>(ws.rbuf),
@@ -831,7 +833,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
                     track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
                     smem_rows, P<uint32_t>(ws.bigjoin), ctr};
-        k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh);
+        k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh); count_launch();
         // local join, pass 1: count proposals per target
         NNM_CUDA_TRY(cudaMemsetAsync(ws.bcnt.p, 0, n1 * 4, st));
         NNM_CUDA_TRY(cudaMemsetAsync(ws.bcur.p, 0, n1 * 4, st));
@@ -839,9 +841,11 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     g.newlen, g.oldlen, g.capn, g.capo, caps, (uint32_t)mode, verse,
                     d_leaf_off, nleaf, P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
                     P<uint64_t>(ws.boff), P<Prop>(ws.bucket), P<uint32_t>(ws.bigjoin), smem_rows, ctr};
+        if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
         if (g.metric == L2) launch_join<L2>(ja, smem_staged, smem_global, PASS_COUNT, st, nsm);
         else if (g.metric == L1) launch_join<L1>(ja, smem_staged, smem_global, PASS_COUNT, st, nsm);
         else launch_join<CHI2>(ja, smem_staged, smem_global, PASS_COUNT, st, nsm);
+        if (ctx.prof) cudaEventRecord(ctx.ev[1], st);
         NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff), n, scan_tmp,
                                     reinterpret_cast<uint64_t*>(&ctr->proposals), st));
         NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
@@ -856,12 +860,15 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             ja.bucket = P<Prop>(ws.bucket);
         }
         // pass 2: recompute and fill the buckets
+        if (ctx.prof) cudaEventRecord(ctx.ev[2], st);
         if (g.metric == L2) launch_join<L2>(ja, smem_staged, smem_global, PASS_FILL, st, nsm);
         else if (g.metric == L1) launch_join<L1>(ja, smem_staged, smem_global, PASS_FILL, st, nsm);
         else launch_join<CHI2>(ja, smem_staged, smem_global, PASS_FILL, st, nsm);
         MergeArgs ma{g.pid, g.pdist, n, K, P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff),
                      P<Prop>(ws.bucket), P<uint8_t>(ws.nflag), ctr};
-        k_merge<<<(n + MERGE_WARPS - 1) / MERGE_WARPS, MERGE_WARPS * 32, 0, st>>>(ma);
+        if (ctx.prof) cudaEventRecord(ctx.ev[3], st);
+        k_merge<<<(n + MERGE_WARPS - 1) / MERGE_WARPS, MERGE_WARPS * 32, 0, st>>>(ma); count_launch();
+        if (ctx.prof) cudaEventRecord(ctx.ev[4], st);
         NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
         NNM_CUDA_TRY(cudaMemcpyAsync(&ctx.h_counters->rand_draws, d_tot, 8, cudaMemcpyDeviceToHost, st));
         NNM_CUDA_TRY(cudaStreamSynchronize(st));
@@ -870,6 +877,24 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         if (hc.error) {
             ctx.last_error = "device capacity check failed (code " + std::to_string(hc.error) + ")";
             return 6;
+        }
+        if (ctx.prof) {
+            float t01 = 0.f, t23 = 0.f, t34 = 0.f;
+            cudaEventElapsedTime(&t01, ctx.ev[0], ctx.ev[1]);
+            cudaEventElapsedTime(&t23, ctx.ev[2], ctx.ev[3]);
+            cudaEventElapsedTime(&t34, ctx.ev[3], ctx.ev[4]);
+            // algorithmic traffic: each joined row gathers its list vectors,
+            // list ids and the K-th distances once per pass; the count pass
+            // writes and the fill pass reads a 2-byte count per list slot;
+            // the fill pass writes every proposal (16 B).
+            const double row_bytes = (double)hc.sum_s * ((double)g.dp * 4.0 + 4.0 + 4.0 + 2.0);
+            ctx.kjoin.launches += 2;
+            ctx.kjoin.ms += (double)t01 + (double)t23;
+            ctx.kjoin.bytes += 2.0 * row_bytes + (double)hc.proposals * 16.0;
+            ctx.kjoin.flops += 2.0 * (double)hc.ncmps * (double)g.d * 3.0;
+            ctx.kmerge.launches += 1;
+            ctx.kmerge.ms += t34;
+            ctx.kmerge.bytes += (double)n * K * 16.0 + (double)hc.proposals * 16.0 + (double)n * 13.0;
         }
         g.gpos += hc.rand_draws;
         g.ncmps += hc.ncmps;

@@ -47,8 +47,18 @@ struct Workspace {
     }
 };
 
+// Device time and algorithmic traffic of one kernel class, accumulated
+// while profiling is on (CUDA events on the engine's stream).
+struct KStat {
+    uint64_t launches = 0;
+    double ms = 0.0, bytes = 0.0, flops = 0.0;
+};
+
 struct Ctx {
     int device = 0;
+    bool prof = false;
+    KStat kjoin, kmerge, kiter;
+    cudaEvent_t ev[8] = {};
     cudaStream_t stream = nullptr;
     Workspace ws;
     IterCounters* h_counters = nullptr;  // pinned

@@ -36,6 +36,7 @@ struct IterCounters {
     unsigned int nbig_rev;         // reverse lists longer than one warp
     unsigned int nbig_join;        // rows whose sample lists exceed shared memory
     unsigned int pad;
+    unsigned long long sum_s;      // sum over joined rows of |new| + |old|
 };
 
 enum DevError : unsigned int {

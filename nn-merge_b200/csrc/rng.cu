@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "nnm_rng.h"
+#include "nnm_launch.h"
 
 namespace nnm {
 
@@ -128,7 +129,7 @@ cudaError_t glibc_stream_generate(int32_t* out, const GlibcBase& base, uint64_t 
     if (count_cap == 0) return cudaSuccess;
     uint64_t threads = (count_cap + CHUNK - 1) / CHUNK;
     unsigned blocks = (unsigned)((threads + 127) / 128);
-    k_glibc_stream<<<blocks, 128, 0, st>>>(out, base, first_output, d_count, count_cap);
+    k_glibc_stream<<<blocks, 128, 0, st>>>(out, base, first_output, d_count, count_cap); count_launch();
     return cudaGetLastError();
 }
 

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "nnm_scan.h"
+#include "nnm_launch.h"
 
 namespace nnm {
 namespace {
@@ -97,9 +98,9 @@ cudaError_t exclusive_scan(const uint32_t* in, uint64_t* out, size_t n, uint64_t
         return e;
     }
     size_t tiles = (n + TILE - 1) / TILE;
-    k_tile_sums<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, n, temp);
-    k_scan_sums<<<1, SCAN_THREADS, 0, st>>>(temp, tiles, d_total);
-    k_tile_scan<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, n, temp, out);
+    k_tile_sums<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, n, temp); count_launch();
+    k_scan_sums<<<1, SCAN_THREADS, 0, st>>>(temp, tiles, d_total); count_launch();
+    k_tile_scan<<<(unsigned)tiles, SCAN_THREADS, 0, st>>>(in, n, temp, out); count_launch();
     return cudaGetLastError();
 }
 

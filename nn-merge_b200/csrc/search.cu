@@ -8,27 +8,75 @@
 //     distances of a node's neighbours are computed in parallel, one
 //     neighbour per lane, and the moves are then applied in list order, as
 //     the reference's loop does;
-//   - best-first beam search on the last layer: the reference's result heap
-//     of size `topk` and candidate heap become one sorted shared-memory list
-//     with an "expanded" mark; the next node expanded is the closest
-//     unexpanded one, and the search ends when none is left (every
-//     candidate the reference could still pop lies beyond its worst result).
-//     Neighbours are visited once per query (a per-warp bitmap in HBM,
-//     cleared through the visited list afterwards) and offered in list
-//     order.
+//   - best-first beam search on the last layer with the reference's two
+//     std::priority_queue<pair<float,unsigned>> heaps (results: max-heap on
+//     distance, size <= topk, in shared memory; candidates: max-heap on
+//     minus the distance, in a per-warp HBM slot).  Lane 0 replays
+//     libstdc++'s push_heap/pop_heap steps exactly, so the order among equal
+//     distances -- which the heaps decide -- is the reference's too.  The
+//     neighbours of an expanded node are checked against a per-warp visited
+//     bitmap and their distances computed in parallel first, then offered in
+//     list order.
 // Distances are the reference's sequential float sums (one lane per
-// distance), so every distance equals vmath.cpp:56-88 bit for bit; only the
-// order among exactly equal distances can differ from the reference's heaps.
+// distance), equal to vmath.cpp:56-88 bit for bit.
 #include <algorithm>
 #include <vector>
 
 #include "nnm_hier.h"
+#include "nnm_launch.h"
 
 namespace nnm {
 namespace {
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int SWARPS = 4;        // warps per block
-constexpr uint32_t VCAP = 16384; // visited-list capacity per warp slot
+constexpr int SWARPS = 4;         // warps per block
+constexpr uint32_t VCAP = 16384;  // visited-list capacity per warp slot
+constexpr uint32_t CCAP = 32768;  // candidate-heap capacity per warp slot
+
+// Element of the reference's priority queues: pair<float, unsigned>,
+// compared on .first only (CompareByFirst, lysearch.h:37-42).
+struct HP {
+    float f;
+    uint32_t id;
+};
+
+// libstdc++ push_heap / pop_heap on a max-heap by .f (one thread).
+__device__ __forceinline__ void heap_push(HP* h, uint32_t& n, HP v) {
+    int hole = (int)n++;
+    int parent = (hole - 1) / 2;
+    while (hole > 0 && h[parent].f < v.f) {
+        h[hole] = h[parent];
+        hole = parent;
+        parent = (hole - 1) / 2;
+    }
+    h[hole] = v;
+}
+__device__ __forceinline__ void heap_pop(HP* h, uint32_t& n) {
+    if (n > 1) {
+        const int len = (int)n - 1;
+        HP v = h[len];
+        h[len] = h[0];
+        int hole = 0, second = 0;
+        while (second < (len - 1) / 2) {
+            second = 2 * (second + 1);
+            if (h[second].f < h[second - 1].f) second--;
+            h[hole] = h[second];
+            hole = second;
+        }
+        if ((len & 1) == 0 && second == (len - 2) / 2) {
+            second = 2 * (second + 1);
+            h[hole] = h[second - 1];
+            hole = second - 1;
+        }
+        int parent = (hole - 1) / 2;
+        while (hole > 0 && h[parent].f < v.f) {
+            h[hole] = h[parent];
+            hole = parent;
+            parent = (hole - 1) / 2;
+        }
+        h[hole] = v;
+    }
+    n--;
+}
 
 struct SearchArgs {
     const float* x;
@@ -45,26 +93,25 @@ struct SearchArgs {
     uint32_t* visited;  // per warp slot: ceil(n/32) words
     uint32_t words;
     uint32_t* vlist;    // per warp slot: VCAP ids
+    HP* cand;           // per warp slot: CCAP entries
     unsigned* next_q;
     unsigned long long* ncmps;
+    unsigned* overflow;
 };
-
-__device__ __forceinline__ float qdist(int metric, const float* qv, const float* xr, uint32_t dp) {
-    return dist_seq_rt(metric, qv, xr, dp);
-}
 
 __global__ void k_search(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t slot = blockIdx.x * SWARPS + w;
-    float* qv = reinterpret_cast<float*>(smem) + (size_t)w * a.dp;
-    const size_t rstride = ((size_t)a.topk * 9 + 15) & ~(size_t)15;  // keeps every warp's arrays aligned
-    unsigned char* rbase = smem + (size_t)SWARPS * a.dp * 4 + (size_t)w * rstride;
-    float* rd = reinterpret_cast<float*>(rbase);
-    uint32_t* rid = reinterpret_cast<uint32_t*>(rbase + (size_t)a.topk * 4);
-    unsigned char* rex = rbase + (size_t)a.topk * 8;
+    const size_t wbytes = (size_t)a.dp * 4 + (size_t)(a.topk + 1) * 8 + 32 * 8;
+    unsigned char* base = smem + (size_t)w * ((wbytes + 15) & ~(size_t)15);
+    float* qv = reinterpret_cast<float*>(base);
+    HP* top = reinterpret_cast<HP*>(base + (size_t)a.dp * 4);
+    float* stage_d = reinterpret_cast<float*>(top + a.topk + 1);
+    uint32_t* stage_i = reinterpret_cast<uint32_t*>(stage_d + 32);
     uint32_t* vis = a.visited + (size_t)slot * a.words;
     uint32_t* vl = a.vlist + (size_t)slot * VCAP;
+    HP* cand = a.cand + (size_t)slot * CCAP;
     unsigned long long cmps = 0;
     for (;;) {
         unsigned qi = 0;
@@ -74,9 +121,9 @@ __global__ void k_search(SearchArgs a) {
         for (uint32_t t = lane; t < a.dp; t += 32) qv[t] = a.q[(size_t)qi * a.dp + t];
         __syncwarp();
         uint32_t cur = a.entry;
-        float cur_d = qdist(a.metric, qv, a.x + (size_t)cur * a.dp, a.dp);
+        float cur_d = dist_seq_rt(a.metric, qv, a.x + (size_t)cur * a.dp, a.dp);
         cmps++;
-        // greedy descent on the upper layers
+        // greedy descent on the upper layers (lysearch.cpp:397-420)
         for (uint32_t g = 0; g + 1 < a.L; g++) {
             const uint64_t* off = a.off_all + a.off_base[g];
             bool moved = true;
@@ -88,13 +135,13 @@ __global__ void k_search(SearchArgs a) {
                     float dd = 0.f;
                     if (c0 + lane < e) {
                         nn = a.adj_all[c0 + lane];
-                        dd = qdist(a.metric, qv, a.x + (size_t)nn * a.dp, a.dp);
+                        dd = dist_seq_rt(a.metric, qv, a.x + (size_t)nn * a.dp, a.dp);
                     }
-                    uint32_t cnt = (uint32_t)(e - c0 < 32 ? e - c0 : 32);
+                    const uint32_t cnt = (uint32_t)(e - c0 < 32 ? e - c0 : 32);
                     cmps += cnt;
                     for (uint32_t j = 0; j < cnt; j++) {
-                        float oj = __shfl_sync(FULL, dd, j);
-                        uint32_t ij = __shfl_sync(FULL, nn, j);
+                        const float oj = __shfl_sync(FULL, dd, j);
+                        const uint32_t ij = __shfl_sync(FULL, nn, j);
                         if (oj < cur_d) {
                             cur_d = oj;
                             cur = ij;
@@ -104,109 +151,83 @@ __global__ void k_search(SearchArgs a) {
                 }
             }
         }
-        // beam search on the last layer
+        // beam search on the last layer (nndHNSWSrch, lysearch.cpp:236-322)
         const uint64_t* off = a.off_all + a.off_base[a.L - 1];
-        uint32_t size = 1, cursor = 0, nvis = 0;
-        bool overflow = false;
+        uint32_t ntop = 0, ncand = 0, nvis = 1;
+        bool vis_overflow = false;
         if (lane == 0) {
-            rd[0] = cur_d;
-            rid[0] = cur;
-            rex[0] = 0;
+            heap_push(cand, ncand, HP{-cur_d, cur});
+            heap_push(top, ntop, HP{cur_d, cur});
             atomicOr(&vis[cur >> 5], 1u << (cur & 31));
             vl[0] = cur;
         }
-        nvis = 1;
+        ncand = __shfl_sync(FULL, ncand, 0);
+        ntop = __shfl_sync(FULL, ntop, 0);
         __syncwarp();
-        for (;;) {
-            // closest unexpanded entry
-            uint32_t u = 0xffffffffu;
-            for (uint32_t c0 = cursor; c0 < size; c0 += 32) {
-                bool un = c0 + lane < size && rex[c0 + lane] == 0;
-                unsigned bal = __ballot_sync(FULL, un);
-                if (bal) {
-                    u = c0 + __ffs(bal) - 1;
-                    break;
-                }
-            }
-            if (u == 0xffffffffu) break;
-            cursor = u;
-            if (lane == 0) rex[u] = 1;
-            const uint32_t c = rid[u];
+        float lwbnd = top[0].f;
+        while (ncand > 0) {
+            const HP c = cand[0];
+            if (-c.f > lwbnd) break;
+            if (lane == 0) heap_pop(cand, ncand);
+            ncand = __shfl_sync(FULL, ncand, 0);
             __syncwarp();
-            const uint64_t b = off[c], e = off[c + 1];
+            const uint64_t b = off[c.id], e = off[c.id + 1];
             for (uint64_t c0 = b; c0 < e; c0 += 32) {
                 uint32_t nn = 0;
-                float dd = 0.f;
                 bool fresh = false;
                 if (c0 + lane < e) {
                     nn = a.adj_all[c0 + lane];
-                    uint32_t old = atomicOr(&vis[nn >> 5], 1u << (nn & 31));
+                    const uint32_t old = atomicOr(&vis[nn >> 5], 1u << (nn & 31));
                     fresh = !(old & (1u << (nn & 31)));
                 }
-                // two lanes cannot claim the same id: a node's list has distinct ids
-                unsigned fb = __ballot_sync(FULL, fresh);
+                const unsigned fb = __ballot_sync(FULL, fresh);
                 if (fresh) {
-                    uint32_t r = nvis + __popc(fb & ((1u << lane) - 1u));
-                    if (r < VCAP) vl[r] = nn;
-                    dd = qdist(a.metric, qv, a.x + (size_t)nn * a.dp, a.dp);
+                    const uint32_t r = __popc(fb & ((1u << lane) - 1u));
+                    if (nvis + r < VCAP) vl[nvis + r] = nn;
+                    stage_d[r] = dist_seq_rt(a.metric, qv, a.x + (size_t)nn * a.dp, a.dp);
+                    stage_i[r] = nn;
                 }
-                nvis += __popc(fb);
-                if (nvis > VCAP) overflow = true;
-                cmps += __popc(fb);
-                // offer the fresh neighbours in list order
-                while (fb) {
-                    const int j = __ffs(fb) - 1;
-                    fb &= fb - 1;
-                    const float dj = __shfl_sync(FULL, dd, j);
-                    const uint32_t ij = __shfl_sync(FULL, nn, j);
-                    const bool full = size >= a.topk;
-                    if (full && !(dj < rd[size - 1])) continue;
-                    // position after all entries with distance <= dj
-                    uint32_t pos = 0;
-                    for (uint32_t c1 = 0; c1 < size; c1 += 32) {
-                        bool le = c1 + lane < size && rd[c1 + lane] <= dj;
-                        pos += __popc(__ballot_sync(FULL, le));
-                    }
-                    const uint32_t nsz = full ? size : size + 1;
-                    // shift [pos, nsz-1) right by one, back to front in lane chunks
-                    for (int c1 = (int)nsz - 2; c1 >= (int)pos; c1 -= 32) {
-                        int i0 = c1 - lane;
-                        float vd = 0.f;
-                        uint32_t vi = 0;
-                        unsigned char ve = 0;
-                        bool act = i0 >= (int)pos;
-                        if (act) {
-                            vd = rd[i0];
-                            vi = rid[i0];
-                            ve = rex[i0];
+                const uint32_t nf = __popc(fb);
+                nvis += nf;
+                if (nvis > VCAP) vis_overflow = true;
+                cmps += nf;
+                __syncwarp();
+                if (lane == 0) {  // offers in list order (lysearch.cpp:284-295)
+                    for (uint32_t r = 0; r < nf; r++) {
+                        const float dj = stage_d[r];
+                        if (top[0].f > dj || ntop < a.topk) {
+                            if (ncand >= CCAP) {
+                                atomicOr(a.overflow, 1u);
+                                continue;
+                            }
+                            heap_push(cand, ncand, HP{-dj, stage_i[r]});
+                            heap_push(top, ntop, HP{dj, stage_i[r]});
+                            if (ntop > a.topk) heap_pop(top, ntop);
                         }
-                        __syncwarp();
-                        if (act) {
-                            rd[i0 + 1] = vd;
-                            rid[i0 + 1] = vi;
-                            rex[i0 + 1] = ve;
-                        }
-                        __syncwarp();
                     }
-                    if (lane == 0) {
-                        rd[pos] = dj;
-                        rid[pos] = ij;
-                        rex[pos] = 0;
-                    }
-                    size = nsz;
-                    if (pos < cursor) cursor = pos;
-                    __syncwarp();
                 }
+                __syncwarp();
+                ncand = __shfl_sync(FULL, ncand, 0);
+                ntop = __shfl_sync(FULL, ntop, 0);
+                lwbnd = top[0].f;
             }
         }
-        for (uint32_t t = lane; t < a.topk; t += 32) {
-            a.out_ids[(size_t)qi * a.topk + t] = t < size ? rid[t] : 0xffffffffu;
-            if (a.out_d) a.out_d[(size_t)qi * a.topk + t] = t < size ? rd[t] : 0.f;
+        // results ascending, popped from the max-heap into place (lysearch.cpp:302-312)
+        if (lane == 0) {
+            for (uint32_t t = ntop; t < a.topk; t++) {
+                a.out_ids[(size_t)qi * a.topk + t] = 0xffffffffu;
+                if (a.out_d) a.out_d[(size_t)qi * a.topk + t] = 0.f;
+            }
+            for (int loc = (int)ntop - 1; loc >= 0; loc--) {
+                a.out_ids[(size_t)qi * a.topk + loc] = top[0].id;
+                if (a.out_d) a.out_d[(size_t)qi * a.topk + loc] = top[0].f;
+                heap_pop(top, ntop);
+            }
         }
         // clear the visited bits of this query
-        if (!overflow) {
+        if (!vis_overflow) {
             for (uint32_t t = lane; t < nvis; t += 32) {
-                uint32_t id = vl[t];
+                const uint32_t id = vl[t];
                 atomicAnd(&vis[id >> 5], ~(1u << (id & 31)));
             }
         } else {
@@ -270,7 +291,7 @@ int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_laye
         adj_total += layers->off[g][layers->nrows[g]];
     }
     // one device buffer: vectors | queries | offsets | adjacency
-    DevBuf xb, qb, ob, ab, ib, db, vb, lb, cb;
+    DevBuf xb, qb, ob, ab, ib, db, vb, lb, cb, hb;
     NNM_CUDA_TRY(xb.ensure((size_t)n * dp * 4));
     NNM_CUDA_TRY(qb.ensure((size_t)nq * dp * 4 + 16));
     NNM_CUDA_TRY(ob.ensure(off_total * 8));
@@ -298,7 +319,8 @@ int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_laye
     }
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx.device);
-    const size_t smem = (size_t)SWARPS * dp * 4 + (size_t)SWARPS * (((size_t)topk * 9 + 15) & ~(size_t)15) + 64;
+    const size_t wbytes = (size_t)dp * 4 + (size_t)(topk + 1) * 8 + 32 * 8;
+    const size_t smem = (size_t)SWARPS * ((wbytes + 15) & ~(size_t)15) + 64;
     if (smem > 200 * 1024) {
         ctx.last_error = "beam too wide for shared memory at this dimension";
         return 1;
@@ -306,11 +328,12 @@ int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_laye
     NNM_CUDA_TRY(cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, SWARPS * 32, smem);
-    const uint32_t blocks = (uint32_t)std::min(std::max(1, per_sm), 8) * (uint32_t)nsm;
+    const uint32_t blocks = (uint32_t)std::min(std::max(1, per_sm), 4) * (uint32_t)nsm;
     const uint32_t words = (uint32_t)((n + 31) / 32);
     const size_t slots = (size_t)blocks * SWARPS;
     NNM_CUDA_TRY(vb.ensure(slots * words * 4));
     NNM_CUDA_TRY(lb.ensure(slots * VCAP * 4));
+    NNM_CUDA_TRY(hb.ensure(slots * CCAP * sizeof(HP)));
     NNM_CUDA_TRY(cudaMemsetAsync(vb.p, 0, slots * words * 4, st));
     NNM_CUDA_TRY(cudaMemsetAsync(cb.p, 0, 64, st));
     a.x = xb.as<float>();
@@ -326,17 +349,24 @@ int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_laye
     a.visited = vb.as<uint32_t>();
     a.words = words;
     a.vlist = lb.as<uint32_t>();
+    a.cand = hb.as<HP>();
     a.next_q = cb.as<unsigned>();
     a.ncmps = reinterpret_cast<unsigned long long*>(cb.as<unsigned char>() + 8);
-    k_search<<<blocks, SWARPS * 32, smem, st>>>(a);
+    a.overflow = cb.as<unsigned>() + 1;  // bytes 4..7; ncmps occupies bytes 8..15
+    k_search<<<blocks, SWARPS * 32, smem, st>>>(a); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     NNM_CUDA_TRY(cudaMemcpyAsync(out_ids, ib.p, (size_t)nq * topk * 4, cudaMemcpyDeviceToHost, st));
     if (out_dists) NNM_CUDA_TRY(cudaMemcpyAsync(out_dists, db.p, (size_t)nq * topk * 4, cudaMemcpyDeviceToHost, st));
-    unsigned long long c = 0;
-    NNM_CUDA_TRY(cudaMemcpyAsync(&c, a.ncmps, 8, cudaMemcpyDeviceToHost, st));
+    unsigned long long c[3] = {0, 0, 0};
+    NNM_CUDA_TRY(cudaMemcpyAsync(c, cb.p, 24, cudaMemcpyDeviceToHost, st));
     NNM_CUDA_TRY(cudaStreamSynchronize(st));
-    if (ncmps) *ncmps = c;
-    DevBuf* all[] = {&xb, &qb, &ob, &ab, &ib, &db, &vb, &lb, &cb};
+    if (ncmps) *ncmps = c[1];
+    DevBuf* all[] = {&xb, &qb, &ob, &ab, &ib, &db, &vb, &lb, &cb, &hb};
+    if (c[0] >> 32) {  // overflow word (bytes 4..7)
+        for (auto* b : all) b->release();
+        ctx.last_error = "candidate heap overflow: beam too wide for the per-query capacity";
+        return 6;
+    }
     for (auto* b : all) b->release();
     return 0;
 }

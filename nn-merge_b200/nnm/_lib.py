@@ -16,6 +16,7 @@ EXPORTED = (
     "nnm_opts_default", "nnm_status_string", "nnm_last_error", "nnm_ctx_create", "nnm_ctx_destroy",
     "nnm_kgraph_build", "nnm_kgraph_build_dev", "nnm_smerge", "nnm_jmerge", "nnm_merge_leaves",
     "nnm_merge_leaves_dev", "nnm_hmerge_build", "nnm_layers_free", "nnm_search",
+    "nnm_profile_enable", "nnm_profile_get", "nnm_launch_count",
 )
 
 
@@ -67,6 +68,9 @@ def load():
         lib.nnm_hmerge_build.argtypes = [vp, vp, u64, u32, u32, u32, vp, vp, vp, vp, vp, vp]
         lib.nnm_layers_free.argtypes = [vp]
         lib.nnm_search.argtypes = [vp, vp, u64, u32, vp, vp, u64, u32, vp, vp, vp, vp]
+        lib.nnm_profile_enable.argtypes = [vp, ctypes.c_int]
+        lib.nnm_profile_get.argtypes = [vp, ctypes.c_char_p, u64]
+        lib.nnm_launch_count.restype = ctypes.c_uint64
         _lib = lib
     return _lib
 
@@ -131,6 +135,39 @@ class Context:
         tail = [ctypes.byref(opts), _ptr(ids), _ptr(dists), _ptr(flags), ctypes.byref(st)]
         self._check(fn(*(head + list(extra) + tail)))
         return dict(ids=ids, dists=dists, flags=flags, **_stats_dict(st))
+
+    def profile(self, on=True):
+        self._check(self.lib.nnm_profile_enable(self.h, 1 if on else 0))
+
+    def profile_stats(self):
+        import json
+        buf = ctypes.create_string_buffer(4096)
+        self._check(self.lib.nnm_profile_get(self.h, buf, 4096))
+        return json.loads(buf.value.decode())
+
+    def launch_count(self):
+        return int(self.lib.nnm_launch_count())
+
+    def merge_leaves_dev(self, x_ptr, n, d, k, leaf_sizes, ids_ptr=0, dists_ptr=0, flags_ptr=0, **kw):
+        """Device-pointer build (inputs resident in HBM, outputs on the device)."""
+        sizes = np.ascontiguousarray(leaf_sizes, np.uint32)
+        st = Stats()
+        o = make_opts(**kw)
+        self._check(self.lib.nnm_merge_leaves_dev(self.h, ctypes.c_void_p(x_ptr), n, d, k, _ptr(sizes), len(sizes),
+                                                  ctypes.byref(o), ctypes.c_void_p(ids_ptr),
+                                                  ctypes.c_void_p(dists_ptr), ctypes.c_void_p(flags_ptr),
+                                                  ctypes.byref(st)))
+        return _stats_dict(st)
+
+    def merge_leaves_into(self, x, k, leaf_sizes, ids, dists=None, flags=None, **kw):
+        """Host-pointer build writing into caller-provided (e.g. pinned) arrays."""
+        sizes = np.ascontiguousarray(leaf_sizes, np.uint32)
+        st = Stats()
+        o = make_opts(**kw)
+        self._check(self.lib.nnm_merge_leaves(self.h, _ptr(x), x.shape[0], x.shape[1], k, _ptr(sizes), len(sizes),
+                                              ctypes.byref(o), _ptr(ids), _ptr(dists), _ptr(flags),
+                                              ctypes.byref(st)))
+        return _stats_dict(st)
 
     def kgraph(self, x, k, **kw):
         return self._build(self.lib.nnm_kgraph_build, x, k, make_opts(**kw))

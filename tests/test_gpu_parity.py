@@ -5,6 +5,7 @@ seed.  All calls go through the C ABI (lib/libnnm.so)."""
 import numpy as np
 import pytest
 
+import golden_lib
 from nnm.datasets import gaussian_mixture_u8, queries_like, vmf_mixture
 
 pytestmark = pytest.mark.gpu
@@ -90,8 +91,29 @@ def test_search_matches_reference(ctx, oracle):
     for topk in (1, 10, 60):
         exp = oracle.search(x, h["layers"], q, topk, 9)
         got = ctx.search(x, h["layers"], q, topk, seed=9)
-        same = (got["ids"] == exp["ids"]).all(1).mean()
-        # distances are bitwise the reference's; only the order of exactly
-        # equal distances inside the reference's heaps can differ
-        assert same >= 0.99, (topk, same)
-        assert abs(got["ncmps"] - exp["ncmps"]) <= 0.01 * exp["ncmps"]
+        assert np.array_equal(got["ids"], exp["ids"]), (topk, (got["ids"] == exp["ids"]).all(1).mean())
+        assert np.array_equal(got["dists"], exp["dists"])
+        assert got["ncmps"] == exp["ncmps"]
+
+
+@pytest.mark.parametrize("name", golden_lib.names())
+def test_cuda_matches_golden(ctx, name):
+    """The CUDA path against the reference's own committed outputs."""
+    fx = golden_lib.load(name)
+    x, k, seed, metric = fx["x"], fx["k"], fx["seed"], fx["metric"]
+    if fx["cmd"] == "hmerge":
+        got = ctx.hmerge(x, k, fx["m"], seed=seed, metric=metric, exact_trace=True)
+        assert len(got["layers"]) == len(fx["layers"])
+        for (go, ga), (eo, ea) in zip(got["layers"], fx["layers"]):
+            assert np.array_equal(go, eo) and np.array_equal(ga, ea)
+    else:
+        got = getattr(ctx, fx["cmd"])(x, k, seed=seed, metric=metric, exact_trace=True)
+    assert golden_lib.same_pools(got, fx)
+    assert got["ncmps"] == fx["ncmps"]
+    assert np.array_equal(got["trace"], fx["trace"])
+    if "q" in fx:
+        for topk in (1, 10, 40):
+            s = ctx.search(x, fx["layers"], fx["q"], topk, seed=seed)
+            assert np.array_equal(s["ids"], fx["search%d_ids" % topk])
+            assert np.array_equal(s["dists"], fx["search%d_dists" % topk])
+            assert s["ncmps"] == int(fx["search%d_ncmps" % topk])
