@@ -123,10 +123,12 @@ __global__ void k_dpg_forward(FwdArgs a) {
     }
     __syncwarp();
     for (uint32_t j = 0; j < a.K; j++) {
-        if (slen[w] > a.Mo) break;
+        const uint32_t len = __shfl_sync(FULL, slen[w], 0);  // one value for the whole warp
+        if (len > a.Mo) break;
         uint32_t nb = a.pid[(size_t)i * a.K + j] & ID_MASK;
         float dst = a.pdist[(size_t)i * a.K + j];  // = distfunc(i, nb): the same exact value
-        bool bad = occluded(a.x, a.dp, a.metric, sid[w], slen[w], nb, dst);
+        bool bad = occluded(a.x, a.dp, a.metric, sid[w], len, nb, dst);
+        __syncwarp();  // every lane has read the list before lane 0 changes it
         if (!bad && lane == 0) list_insert(sid[w], sd[w], &slen[w], nb, dst, a.Mo);
         __syncwarp();
     }
@@ -280,11 +282,11 @@ __global__ void k_dpg_reverse(RevArgs a) {
         const uint32_t s = (uint32_t)(v >> 32);
         if (!snapped && (end || s >= x)) {  // list of row x when the walk reaches row x
             snapped = true;
-            for (uint32_t l = lane; l < slen[w]; l += 32) {
+            const uint32_t L = __shfl_sync(FULL, slen[w], 0);
+            for (uint32_t l = lane; l < L; l += 32) {
                 a.tid[(size_t)x * a.C + l] = sid[w][l];
                 a.tdist[(size_t)x * a.C + l] = sd[w][l];
             }
-            uint32_t L = slen[w];
             bool diff = L != a.slen[x];
             for (uint32_t l = lane; l < L && !diff; l += 32)
                 if (a.sid[(size_t)x * a.C + l] != sid[w][l]) diff = true;
@@ -296,8 +298,10 @@ __global__ void k_dpg_reverse(RevArgs a) {
         }
         if (end) break;
         const float dd = __uint_as_float((uint32_t)(v & 0xffffffffu));
+        const uint32_t len = __shfl_sync(FULL, slen[w], 0);
         bool ok = true;
-        if (slen[w] >= a.maxM) ok = !occluded(a.x, a.dp, a.metric, sid[w], slen[w], s, dd);
+        if (len >= a.maxM) ok = !occluded(a.x, a.dp, a.metric, sid[w], len, s, dd);
+        __syncwarp();  // every lane has read the list before lane 0 changes it
         if (ok && lane == 0) list_insert(sid[w], sd[w], &slen[w], s, dd, a.maxM);
         __syncwarp();
     }

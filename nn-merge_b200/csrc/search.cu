@@ -20,6 +20,7 @@
 // Distances are the reference's sequential float sums (one lane per
 // distance), equal to vmath.cpp:56-88 bit for bit.
 #include <algorithm>
+#include <string>
 #include <vector>
 
 #include "nnm_hier.h"
@@ -51,6 +52,7 @@ __device__ __forceinline__ void heap_push(HP* h, uint32_t& n, HP v) {
     h[hole] = v;
 }
 __device__ __forceinline__ void heap_pop(HP* h, uint32_t& n) {
+    if (n == 0) return;
     if (n > 1) {
         const int len = (int)n - 1;
         HP v = h[len];
@@ -96,7 +98,15 @@ struct SearchArgs {
     HP* cand;           // per warp slot: CCAP entries
     unsigned* next_q;
     unsigned long long* ncmps;
-    unsigned* overflow;
+    unsigned* overflow;     // bit 0: candidate heap full; bits 1..: self-check failures
+    uint32_t nrows[16];     // rows of each layer
+};
+
+enum : unsigned {
+    SERR_HEAP = 1u,        // candidate heap capacity reached
+    SERR_GREEDY_CAP = 2u,  // greedy descent made more moves than the layer has rows
+    SERR_BEAM_CAP = 4u,    // beam search expanded more nodes than the layer has rows
+    SERR_BAD_ID = 8u,      // a node id outside its layer
 };
 
 __global__ void k_search(SearchArgs a) {
@@ -127,8 +137,13 @@ __global__ void k_search(SearchArgs a) {
         for (uint32_t g = 0; g + 1 < a.L; g++) {
             const uint64_t* off = a.off_all + a.off_base[g];
             bool moved = true;
+            uint32_t moves = 0;
             while (moved) {
                 moved = false;
+                if (cur >= a.nrows[g] || ++moves > a.nrows[g]) {
+                    if (lane == 0) atomicOr(a.overflow, cur >= a.nrows[g] ? SERR_BAD_ID : SERR_GREEDY_CAP);
+                    break;
+                }
                 const uint64_t b = off[cur], e = off[cur + 1];  // the list of the node at loop entry
                 for (uint64_t c0 = b; c0 < e; c0 += 32) {
                     uint32_t nn = 0;
@@ -155,7 +170,8 @@ __global__ void k_search(SearchArgs a) {
         const uint64_t* off = a.off_all + a.off_base[a.L - 1];
         uint32_t ntop = 0, ncand = 0, nvis = 1;
         bool vis_overflow = false;
-        if (lane == 0) {
+        const bool start_ok = cur < a.nrows[a.L - 1];  // false only after a failed greedy check
+        if (lane == 0 && start_ok) {
             heap_push(cand, ncand, HP{-cur_d, cur});
             heap_push(top, ntop, HP{cur_d, cur});
             atomicOr(&vis[cur >> 5], 1u << (cur & 31));
@@ -164,21 +180,39 @@ __global__ void k_search(SearchArgs a) {
         ncand = __shfl_sync(FULL, ncand, 0);
         ntop = __shfl_sync(FULL, ntop, 0);
         __syncwarp();
-        float lwbnd = top[0].f;
+        if (!start_ok) nvis = 0;
+        float lwbnd = 0.f;
+        if (lane == 0 && start_ok) lwbnd = top[0].f;
+        lwbnd = __shfl_sync(FULL, lwbnd, 0);
+        const uint32_t nlast = a.nrows[a.L - 1];
+        uint32_t expansions = 0;
         while (ncand > 0) {
-            const HP c = cand[0];
+            // Lane 0 alone reads the heaps and broadcasts through registers:
+            // a value every lane loaded itself could be re-read after lane
+            // 0's next update, and lanes that disagree would diverge.
+            HP c{0.f, 0u};
+            if (lane == 0) c = cand[0];
+            c.f = __shfl_sync(FULL, c.f, 0);
+            c.id = __shfl_sync(FULL, c.id, 0);
             if (-c.f > lwbnd) break;
+            if (c.id >= nlast || ++expansions > nlast + 1) {
+                if (lane == 0) atomicOr(a.overflow, c.id >= nlast ? SERR_BAD_ID : SERR_BEAM_CAP);
+                break;
+            }
             if (lane == 0) heap_pop(cand, ncand);
             ncand = __shfl_sync(FULL, ncand, 0);
-            __syncwarp();
             const uint64_t b = off[c.id], e = off[c.id + 1];
             for (uint64_t c0 = b; c0 < e; c0 += 32) {
                 uint32_t nn = 0;
                 bool fresh = false;
                 if (c0 + lane < e) {
                     nn = a.adj_all[c0 + lane];
-                    const uint32_t old = atomicOr(&vis[nn >> 5], 1u << (nn & 31));
-                    fresh = !(old & (1u << (nn & 31)));
+                    if (nn < nlast) {
+                        const uint32_t old = atomicOr(&vis[nn >> 5], 1u << (nn & 31));
+                        fresh = !(old & (1u << (nn & 31)));
+                    } else {
+                        atomicOr(a.overflow, SERR_BAD_ID);
+                    }
                 }
                 const unsigned fb = __ballot_sync(FULL, fresh);
                 if (fresh) {
@@ -197,7 +231,7 @@ __global__ void k_search(SearchArgs a) {
                         const float dj = stage_d[r];
                         if (top[0].f > dj || ntop < a.topk) {
                             if (ncand >= CCAP) {
-                                atomicOr(a.overflow, 1u);
+                                atomicOr(a.overflow, SERR_HEAP);
                                 continue;
                             }
                             heap_push(cand, ncand, HP{-dj, stage_i[r]});
@@ -209,7 +243,9 @@ __global__ void k_search(SearchArgs a) {
                 __syncwarp();
                 ncand = __shfl_sync(FULL, ncand, 0);
                 ntop = __shfl_sync(FULL, ntop, 0);
-                lwbnd = top[0].f;
+                float lw = 0.f;
+                if (lane == 0) lw = top[0].f;
+                lwbnd = __shfl_sync(FULL, lw, 0);
             }
         }
         // results ascending, popped from the max-heap into place (lysearch.cpp:302-312)
@@ -353,6 +389,7 @@ int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_laye
     a.next_q = cb.as<unsigned>();
     a.ncmps = reinterpret_cast<unsigned long long*>(cb.as<unsigned char>() + 8);
     a.overflow = cb.as<unsigned>() + 1;  // bytes 4..7; ncmps occupies bytes 8..15
+    for (uint32_t g = 0; g < L; g++) a.nrows[g] = layers->nrows[g];
     k_search<<<blocks, SWARPS * 32, smem, st>>>(a); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     NNM_CUDA_TRY(cudaMemcpyAsync(out_ids, ib.p, (size_t)nq * topk * 4, cudaMemcpyDeviceToHost, st));
@@ -362,9 +399,11 @@ int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_laye
     NNM_CUDA_TRY(cudaStreamSynchronize(st));
     if (ncmps) *ncmps = c[1];
     DevBuf* all[] = {&xb, &qb, &ob, &ab, &ib, &db, &vb, &lb, &cb, &hb};
-    if (c[0] >> 32) {  // overflow word (bytes 4..7)
+    const unsigned serr = (unsigned)(c[0] >> 32);  // bytes 4..7
+    if (serr) {
         for (auto* b : all) b->release();
-        ctx.last_error = "candidate heap overflow: beam too wide for the per-query capacity";
+        ctx.last_error = "search self-check failed (code " + std::to_string(serr) +
+                         "; 1: candidate heap full, 2/4: loop bound, 8: id outside its layer)";
         return 6;
     }
     for (auto* b : all) b->release();

@@ -73,10 +73,19 @@ def test_merge_two_leaves_is_smerge(ctx):
     assert np.array_equal(a["ids"], b["ids"]) and np.array_equal(a["dists"], b["dists"])
 
 
+_HM_CACHE = {}
+
+
+def oracle_hmerge(oracle, n):
+    if n not in _HM_CACHE:
+        x = gaussian_mixture_u8(n, seed=5)
+        _HM_CACHE[n] = (x, oracle.hmerge(x, 20, 20, 77))
+    return _HM_CACHE[n]
+
+
 @pytest.mark.parametrize("n", [3000, 34000])
 def test_hmerge_bit_exact(ctx, oracle, n):
-    x = gaussian_mixture_u8(n, seed=5)
-    exp = oracle.hmerge(x, 20, 20, 77)
+    x, exp = oracle_hmerge(oracle, n)
     got = ctx.hmerge(x, 20, 20, seed=77, exact_trace=True)
     assert_same_graph(got, exp)
     assert len(got["layers"]) == len(exp["layers"])
@@ -85,8 +94,7 @@ def test_hmerge_bit_exact(ctx, oracle, n):
 
 
 def test_search_matches_reference(ctx, oracle):
-    x = gaussian_mixture_u8(34000, seed=5)
-    h = oracle.hmerge(x, 20, 20, 77)
+    x, h = oracle_hmerge(oracle, 34000)
     q = queries_like(1000, seed=5, query_seed=3)
     for topk in (1, 10, 60):
         exp = oracle.search(x, h["layers"], q, topk, 9)
