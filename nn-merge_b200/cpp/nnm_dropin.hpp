@@ -1,0 +1,399 @@
+// Drop-in replacements for the reference's hot-path classes, implemented
+// over the C ABI of include/nnm.h.  Include this header instead of the
+// reference's kgraph.h, smerge.h, jmerge.h, lynndescent.h, lysearch.h and
+// space_lp.h; link with -lnnm.  Names, constructors and the virtual
+// interface follow the reference:
+//   AbstractGraph    abstractgraph.h:21-45
+//   KGraph           kgraph.h:126-150   (buildKGraph returns new unsigned[n*k])
+//   Smerge, Jmerge   smerge.h:8-23, jmerge.h:7-22 (buildKGraph returns 0)
+//   LyNNDescent      lynndescent.h:19-86 (buildhgraph(src, dst, grd, K, M))
+//   LySearch         lysearch.h:23-91   (knnSearch is public here)
+//   L2space, L1space, Ksquare  space_lp.h:9-53
+// The reference seeds every phase from time(NULL); so do these classes,
+// unless the environment variable NNM_SEED fixes the seed.  Errors print
+// the library's message and exit, as the reference exits on failures.
+#ifndef NNM_DROPIN_HPP
+#define NNM_DROPIN_HPP
+
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/nnm.h"
+
+template <typename MTYPE>
+using DISTFUNC = MTYPE (*)(const float *, const unsigned long s1, const float *, const unsigned long s2,
+                           const unsigned int d0);
+
+template <typename MTYPE>
+class SpaceInterface {
+public:
+    virtual DISTFUNC<MTYPE> get_dist_func() = 0;
+    // Which device metric this space is; spaces the engine does not
+    // implement return -1 and are rejected with NNM_ERR_UNSUPPORTED_METRIC.
+    virtual int nnm_metric() const { return -1; }
+    virtual ~SpaceInterface() {}
+};
+
+namespace nnm_dropin {
+
+inline float l2norm(const float *v1, const unsigned long s1, const float *v2, const unsigned long s2,
+                    const unsigned int d0) {
+    float res = 0.f;
+    for (unsigned i = 0; i < d0; i++) {
+        float diff = v1[s1 * d0 + i] - v2[s2 * d0 + i];
+        res += diff * diff;
+    }
+    return res;
+}
+inline float l1norm(const float *v1, const unsigned long s1, const float *v2, const unsigned long s2,
+                    const unsigned int d0) {
+    float res = 0.f;
+    for (unsigned i = 0; i < d0; i++) res += std::fabs(v1[s1 * d0 + i] - v2[s2 * d0 + i]);
+    return res;
+}
+inline float ksquare(const float *v1, const unsigned long s1, const float *v2, const unsigned long s2,
+                     const unsigned int d0) {
+    float w2 = 0.f;
+    for (unsigned i = 0; i < d0; i++) {
+        float a = v1[s1 * d0 + i], b = v2[s2 * d0 + i], w1 = a - b;
+        if (a != 0 || b != 0) w2 += w1 * w1 / (a + b);
+    }
+    return w2;
+}
+
+inline nnm_ctx *context() {
+    static nnm_ctx *ctx = nullptr;
+    if (!ctx) {
+        int rc = nnm_ctx_create(0, &ctx);
+        if (rc != NNM_OK) {
+            std::cout << "nnm: " << nnm_status_string(rc) << std::endl;
+            std::exit(0);
+        }
+    }
+    return ctx;
+}
+
+inline void check(int rc) {
+    if (rc != NNM_OK) {
+        std::cout << "nnm: " << nnm_status_string(rc) << ": " << nnm_last_error(context()) << std::endl;
+        std::exit(0);
+    }
+}
+
+inline nnm_opts opts(int metric) {
+    nnm_opts o;
+    nnm_opts_default(&o);
+    const char *env = std::getenv("NNM_SEED");
+    o.seed = env ? (uint32_t)std::strtoul(env, nullptr, 10) : (uint32_t)time(NULL);
+    if (metric < 0) check(NNM_ERR_UNSUPPORTED_METRIC);
+    o.metric = (uint32_t)metric;
+    return o;
+}
+
+// IODelegator::load_refSet (iodelegator.cpp:159-182): .fvecs, .bvecs, .txt.
+inline float *load_refSet(const char *fn, unsigned &d, unsigned &r) {
+    std::string s(fn);
+    auto ends = [&](const char *e) { size_t l = std::strlen(e); return s.size() >= l && s.compare(s.size() - l, l, e) == 0; };
+    if (ends(".txt")) {
+        std::ifstream in(fn);
+        if (!in) { std::cout << "Fail to read " << fn << std::endl; std::exit(0); }
+        float a, b;
+        in >> a >> b;
+        r = (unsigned)std::lround(a);
+        d = (unsigned)std::lround(b);
+        float *m = new float[(size_t)r * d];
+        for (size_t i = 0; i < (size_t)r * d; i++) in >> m[i];
+        return m;
+    }
+    const bool bytes = ends(".bvecs");
+    if (!bytes && !ends(".fvecs")) { std::cout << "unknown format " << fn << std::endl; std::exit(0); }
+    std::ifstream in(fn, std::ios::binary);
+    if (!in) { std::cout << "File '" << fn << "' cannot open for read!" << std::endl; std::exit(0); }
+    uint32_t dim = 0;
+    in.read(reinterpret_cast<char *>(&dim), 4);
+    in.seekg(0, std::ios::end);
+    const size_t rec = 4 + (size_t)dim * (bytes ? 1 : 4);
+    r = (unsigned)((size_t)in.tellg() / rec);
+    d = dim;
+    in.seekg(0);
+    float *m = new float[(size_t)r * d];
+    std::vector<unsigned char> buf(rec);
+    for (unsigned i = 0; i < r; i++) {
+        in.read(reinterpret_cast<char *>(buf.data()), rec);
+        for (unsigned j = 0; j < d; j++) {
+            if (bytes) m[(size_t)i * d + j] = (float)buf[4 + j];
+            else std::memcpy(&m[(size_t)i * d + j], &buf[4 + 4 * (size_t)j], 4);
+        }
+    }
+    return m;
+}
+
+// The k-NN graph text format (abstractmerge.cpp:278-291, kgraph.cpp:247-261).
+inline void save_knn(const char *dst, const std::vector<uint32_t> &ids, unsigned n, unsigned k) {
+    std::ofstream out(dst);
+    out << n << " " << k << std::endl;
+    for (unsigned i = 0; i < n; i++) {
+        out << i << " " << k << " ";
+        for (unsigned j = 0; j < k; j++) out << ids[(size_t)i * k + j] << " ";
+        out << std::endl;
+    }
+}
+
+}  // namespace nnm_dropin
+
+class L2space : public SpaceInterface<float> {
+public:
+    DISTFUNC<float> get_dist_func() override { return nnm_dropin::l2norm; }
+    int nnm_metric() const override { return NNM_METRIC_L2; }
+};
+class L1space : public SpaceInterface<float> {
+public:
+    DISTFUNC<float> get_dist_func() override { return nnm_dropin::l1norm; }
+    int nnm_metric() const override { return NNM_METRIC_L1; }
+};
+class Ksquare : public SpaceInterface<float> {
+public:
+    DISTFUNC<float> get_dist_func() override { return nnm_dropin::ksquare; }
+    int nnm_metric() const override { return NNM_METRIC_CHI2; }
+};
+
+class AbstractGraph {
+protected:
+    unsigned K0 = 0, row = 0, col = 0;
+    float *mat = nullptr;
+    int metric = NNM_METRIC_L2;
+    std::vector<uint32_t> ids_;
+
+public:
+    unsigned long nCmps = 0;
+    AbstractGraph() {}
+    explicit AbstractGraph(SpaceInterface<float> *func) { metric = func->nnm_metric(); }
+    virtual ~AbstractGraph() {
+        delete[] mat;  // the reference frees the caller's matrix too (abstractgraph.cpp:43-47)
+        mat = nullptr;
+    }
+    virtual unsigned InitialMemory(float *mata, const unsigned k, const unsigned n, const unsigned d) {
+        mat = mata;
+        K0 = k;
+        row = n;
+        col = d;
+        nCmps = 0;
+        return 0;
+    }
+    virtual unsigned InitialGraph() { return 0; }  // part of the device build
+    virtual unsigned *buildKGraph(float *mata, const unsigned K, const unsigned N, const unsigned D) = 0;
+    virtual void saveKGraph(const char *dst) { nnm_dropin::save_knn(dst, ids_, row, K0); }
+    virtual void setdisfunc(SpaceInterface<float> *func) { metric = func->nnm_metric(); }
+};
+
+class KGraph : public AbstractGraph {
+public:
+    KGraph() {}
+    explicit KGraph(SpaceInterface<float> *func) : AbstractGraph(func) {}
+    unsigned *buildKGraph(float *mata, const unsigned k, const unsigned n, const unsigned d) override {
+        InitialMemory(mata, k, n, d);
+        nnm_opts o = nnm_dropin::opts(metric);
+        nnm_stats st;
+        ids_.resize((size_t)n * k);
+        auto t0 = std::chrono::steady_clock::now();
+        nnm_dropin::check(nnm_kgraph_build(nnm_dropin::context(), mata, n, d, k, &o, ids_.data(), nullptr, nullptr, &st));
+        std::cout << "Construction time ..............................times = "
+                  << std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() << std::endl;
+        nCmps = st.ncmps;
+        unsigned *out = new unsigned[(size_t)n * k];
+        std::memcpy(out, ids_.data(), sizeof(unsigned) * (size_t)n * k);
+        return out;
+    }
+};
+
+class AbstractMerge : public AbstractGraph {
+public:
+    AbstractMerge() {}
+    explicit AbstractMerge(SpaceInterface<float> *func) : AbstractGraph(func) {}
+};
+
+class Smerge : public AbstractMerge {
+public:
+    Smerge() {}
+    explicit Smerge(SpaceInterface<float> *func) : AbstractMerge(func) {}
+    unsigned *buildKGraph(float *mata, const unsigned K, const unsigned N, const unsigned D) override {
+        InitialMemory(mata, K, N, D);
+        nnm_opts o = nnm_dropin::opts(metric);
+        nnm_stats st;
+        ids_.resize((size_t)N * K);
+        nnm_dropin::check(nnm_smerge(nnm_dropin::context(), mata, N, D, K, &o, ids_.data(), nullptr, nullptr, &st));
+        nCmps = st.ncmps;
+        std::cout << "Merge-Scanning rate:............................rate  = "
+                  << nCmps / ((row / 2.0) * (row - 1.0)) << std::endl;
+        return 0;
+    }
+};
+
+class Jmerge : public AbstractMerge {
+public:
+    Jmerge() {}
+    explicit Jmerge(SpaceInterface<float> *func) : AbstractMerge(func) {}
+    unsigned *buildKGraph(float *mata, const unsigned K, const unsigned N, const unsigned D) override {
+        InitialMemory(mata, K, N, D);
+        nnm_opts o = nnm_dropin::opts(metric);
+        nnm_stats st;
+        ids_.resize((size_t)N * K);
+        nnm_dropin::check(nnm_jmerge(nnm_dropin::context(), mata, N, D, K, &o, ids_.data(), nullptr, nullptr, &st));
+        nCmps = st.ncmps;
+        std::cout << "Merge-Scanning rate:............................rate  = "
+                  << nCmps / ((row / 2.0) * (row - 1.0)) << std::endl;
+        return 0;
+    }
+};
+
+class LyNNDescent {
+protected:
+    int metric = NNM_METRIC_L2;
+    unsigned row = 0, col = 0;
+    float *mat = nullptr;
+    unsigned long nCmps = 0;
+
+public:
+    LyNNDescent() {}
+    explicit LyNNDescent(SpaceInterface<float> *func) : metric(func->nnm_metric()) {}
+    virtual ~LyNNDescent() { delete[] mat; }
+    // Writes <dstFn>.txt (the layers, lynndescent.cpp:625-638) and
+    // <dstFn>_baselayer.txt (the k-NN graph, :847-872).
+    unsigned buildhgraph(const char *srcFn, const char *dstFn, const char *grd, const unsigned topk, const unsigned M) {
+        (void)grd;
+        mat = nnm_dropin::load_refSet(srcFn, col, row);
+        std::cout << "Matrix size .............................. " << row << "x" << col << std::endl;
+        nnm_opts o = nnm_dropin::opts(metric);
+        nnm_stats st;
+        nnm_layers lay;
+        std::vector<uint32_t> ids((size_t)row * topk);
+        auto t0 = std::chrono::steady_clock::now();
+        nnm_dropin::check(nnm_hmerge_build(nnm_dropin::context(), mat, row, col, topk, M, &o, ids.data(), nullptr,
+                                           nullptr, &lay, &st));
+        std::cout << "Construction time ........................ times = "
+                  << std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() << std::endl;
+        nCmps = st.ncmps;
+        std::ofstream out(std::string(dstFn) + ".txt");
+        for (uint32_t g = 0; g < lay.nlayers; g++) {
+            out << lay.nrows[g] << std::endl;
+            for (uint32_t i = 0; i < lay.nrows[g]; i++) {
+                out << i << " " << (lay.off[g][i + 1] - lay.off[g][i]) << " ";
+                for (uint64_t t = lay.off[g][i]; t < lay.off[g][i + 1]; t++) out << lay.adj[g][t] << " ";
+                out << std::endl;
+            }
+        }
+        nnm_layers_free(&lay);
+        std::ofstream base(std::string(dstFn) + "_baselayer.txt");
+        base << row << " " << topk << std::endl;
+        for (unsigned i = 0; i < row; i++) {
+            base << i << " " << topk;
+            for (unsigned j = 0; j < topk; j++) base << " " << ids[(size_t)i * topk + j];
+            base << std::endl;
+        }
+        return 0;
+    }
+};
+
+class LySearch {
+protected:
+    int metric = NNM_METRIC_L2;
+    unsigned row = 0, col = 0;
+    float *mat = nullptr;
+    nnm_layers layers{};
+    std::vector<std::vector<uint64_t>> off_;
+    std::vector<std::vector<uint32_t>> adj_;
+
+    // LySearch::loadGraphs (lysearch.cpp:112-186): consecutive layers of
+    // "rows" followed by "i n ids..." lines.
+    void loadGraphs(const char *fn) {
+        std::ifstream in(fn);
+        if (!in) {
+            std::cout << "Open file '" << fn << "' failed!" << std::endl;
+            std::exit(0);
+        }
+        unsigned rows;
+        while (layers.nlayers < 16 && (in >> rows)) {
+            std::vector<uint64_t> off(rows + 1, 0);
+            std::vector<uint32_t> adj;
+            for (unsigned i = 0; i < rows; i++) {
+                unsigned idx, num, v;
+                in >> idx >> num;
+                for (unsigned j = 0; j < num; j++) {
+                    in >> v;
+                    adj.push_back(v);
+                }
+                off[i + 1] = off[i] + num;
+            }
+            off_.push_back(std::move(off));
+            adj_.push_back(std::move(adj));
+            layers.nrows[layers.nlayers++] = rows;
+        }
+        for (uint32_t g = 0; g < layers.nlayers; g++) {
+            layers.off[g] = off_[g].data();
+            layers.adj[g] = adj_[g].data();
+        }
+    }
+
+public:
+    LySearch(const char *Rsrc, const char *Gsrc, SpaceInterface<float> *func) : metric(func->nnm_metric()) {
+        mat = nnm_dropin::load_refSet(Rsrc, col, row);
+        loadGraphs(Gsrc);
+    }
+    virtual ~LySearch() { delete[] mat; }
+    // knnSearch (lysearch.cpp:363-437): beams 60 .. 2; writes "query id dist"
+    // of each query's nearest result to dstFn and "beam recall time
+    // distances/query" lines to record; recall@1 against grdFn ("query id"
+    // pairs) when it can be read.
+    int knnSearch(const char *qryFn, const char *dstFn, const char *grdFn, const char *record) {
+        unsigned qd = 0, nq = 0;
+        float *q = nnm_dropin::load_refSet(qryFn, qd, nq);
+        if (qd != col) {
+            std::cout << "query dimension " << qd << " != " << col << std::endl;
+            std::exit(0);
+        }
+        std::map<unsigned, unsigned> grd;
+        {
+            std::ifstream g(grdFn);
+            unsigned a, b;
+            while (g >> a >> b) grd[a] = b;
+        }
+        std::ofstream rec(record);
+        static const unsigned beams[17] = {60, 50, 40, 36, 32, 28, 24, 20, 18, 15, 14, 12, 10, 8, 6, 4, 2};
+        nnm_opts o = nnm_dropin::opts(metric);
+        for (unsigned t = 0; t < 17; t++) {
+            const unsigned topk = beams[t];
+            std::vector<uint32_t> ids((size_t)nq * topk);
+            std::vector<float> ds((size_t)nq * topk);
+            uint64_t ncmps = 0;
+            auto t0 = std::chrono::steady_clock::now();
+            nnm_dropin::check(nnm_search(nnm_dropin::context(), mat, row, col, &layers, q, nq, topk, &o, ids.data(),
+                                         ds.data(), &ncmps));
+            double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            std::ofstream out(dstFn);
+            unsigned hits = 0;
+            for (unsigned i = 0; i < nq; i++) {
+                out << i << "\t" << ids[(size_t)i * topk] << "\t" << ds[(size_t)i * topk] << std::endl;
+                auto it = grd.find(i);
+                if (it != grd.end() && it->second == ids[(size_t)i * topk]) hits++;
+            }
+            float r = grd.empty() ? 0.f : (float)hits / (float)grd.size();
+            std::cout << "Top-1 : " << r << "\t" << ncmps / nq << "\t" << secs << std::endl;
+            rec << topk << "\t" << r << "\t" << secs << "\t" << ncmps / nq << std::endl;
+            if (r == 1) break;
+        }
+        delete[] q;
+        return 0;
+    }
+};
+
+#endif  // NNM_DROPIN_HPP

@@ -1,0 +1,28 @@
+// Reference-style caller of the drop-in classes (as smerge.cpp:238-261 and
+// kgraph.cpp:263-285 call the reference's): builds a graph from an .fvecs
+// file and saves it in the reference's text format.
+//   dropin_main kgraph|smerge|jmerge <in.fvecs> <K> <out.txt>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+
+#include "nnm_dropin.hpp"
+
+int main(int argc, char **argv) {
+    if (argc != 5) {
+        std::cerr << "usage: dropin_main kgraph|smerge|jmerge <in.fvecs> <K> <out.txt>\n";
+        return 2;
+    }
+    unsigned d = 0, n = 0, k = (unsigned)std::atoi(argv[3]);
+    float *mat = nnm_dropin::load_refSet(argv[2], d, n);
+    L2space l2;
+    AbstractGraph *g = nullptr;
+    if (!std::strcmp(argv[1], "kgraph")) g = new KGraph(&l2);
+    else if (!std::strcmp(argv[1], "smerge")) g = new Smerge(&l2);
+    else g = new Jmerge(&l2);
+    unsigned *ids = g->buildKGraph(mat, k, n, d);
+    g->saveKGraph(argv[4]);
+    delete[] ids;
+    delete g;
+    return 0;
+}

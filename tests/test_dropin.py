@@ -1,0 +1,59 @@
+"""The C++ drop-in classes (nn-merge_b200/cpp/nnm_dropin.hpp) used the way the
+reference's own test() functions use its classes."""
+import os
+import shutil
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from nnm.datasets import gaussian_mixture_u8
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+needs_gxx = pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+
+
+def build(td):
+    exe = os.path.join(td, "dropin_main")
+    subprocess.run(["g++", "-O2", "-std=c++11", "-I", os.path.join(ROOT, "nn-merge_b200", "cpp"),
+                    os.path.join(ROOT, "tests", "cpp", "dropin_main.cpp"), "-o", exe,
+                    "-L", os.path.join(ROOT, "nn-merge_b200", "lib"), "-lnnm",
+                    "-Wl,-rpath," + os.path.join(ROOT, "nn-merge_b200", "lib")], check=True)
+    return exe
+
+
+def write_fvecs(path, x):
+    with open(path, "wb") as f:
+        for row in x:
+            f.write(np.int32(x.shape[1]).tobytes())
+            f.write(row.astype(np.float32).tobytes())
+
+
+def read_knn(path):
+    lines = open(path).read().split("\n")
+    n, k = map(int, lines[0].split())
+    ids = np.array([[int(t) for t in lines[1 + i].split()[2:2 + k]] for i in range(n)], np.uint32)
+    return ids
+
+
+@needs_gxx
+def test_dropin_compiles_against_the_reference_interface():
+    with tempfile.TemporaryDirectory() as td:
+        assert os.path.exists(build(td))
+
+
+@needs_gxx
+@pytest.mark.gpu
+@pytest.mark.parametrize("cmd", ["kgraph", "smerge", "jmerge"])
+def test_dropin_matches_oracle(oracle, cmd):
+    x = gaussian_mixture_u8(2000, d=64, seed=3)
+    with tempfile.TemporaryDirectory() as td:
+        exe = build(td)
+        src, dst = os.path.join(td, "x.fvecs"), os.path.join(td, "g.txt")
+        write_fvecs(src, x)
+        env = dict(os.environ, NNM_SEED="4242")
+        subprocess.run([exe, cmd, src, "20", dst], check=True, env=env, capture_output=True)
+        got = read_knn(dst)
+    exp = getattr(oracle, cmd)(x, 20, 4242)
+    assert np.array_equal(got, exp["ids"])
