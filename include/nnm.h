@@ -138,6 +138,36 @@ int nnm_search(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, const nnm_l
                const float *q, uint64_t nq, uint32_t topk, const nnm_opts *opts,
                uint32_t *out_ids, float *out_dists, uint64_t *ncmps);
 
+/* The search hierarchy in device memory, for nnm_search_noalloc: the layout
+ * of nnm_layers with device pointers. */
+typedef struct {
+    uint32_t nlayers;
+    uint32_t nrows[16];
+    const uint64_t *off[16];
+    const uint32_t *adj[16];
+} nnm_dev_layers;
+
+/* Search without device allocation.  No counterpart in the reference: it
+ * exists for callers that cannot call cudaMalloc -- code running inside a
+ * memory pool owned by another framework, a serving process whose device
+ * memory budget is fixed at start-up, or a latency path that must not pay
+ * the implicit synchronisation of cudaMalloc/cudaFree.  Same results as
+ * nnm_search.  The caller passes every input and output in device memory
+ * (x: n x d row-major, q: nq x d, out_ids / out_dists: nq x topk) and a CUDA
+ * stream (NULL: the legacy default stream); the call allocates nothing.  Its
+ * scratch is a fixed array of about 16 MiB in the library's device image,
+ * which every GPU that loads the library holds until the process exits.
+ * Limits: the last layer has at most 2^20 rows, topk <= 1024, d <= 4096
+ * (NNM_ERR_INVALID beyond them); a query needing more than 12288 candidate
+ * heap entries fails the call with NNM_ERR_CAPACITY.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) and
+ * caches it, so make that first call before any stream capture.  All calls
+ * share the one array: calls that overlap on the GPU race and must not be
+ * issued.  The call waits for its stream before returning. */
+int nnm_search_noalloc(const float *x_dev, uint64_t n, uint32_t d, const nnm_dev_layers *layers,
+                       const float *q_dev, uint64_t nq, uint32_t topk, uint32_t seed, uint32_t metric,
+                       uint32_t *out_ids_dev, float *out_dists_dev, uint64_t *ncmps, void *stream);
+
 /* Profiling (no counterpart in the reference, which times whole builds with
  * boost::timer): while enabled, the engine records CUDA events around its
  * local-join and top-K merge kernels and accumulates their device time and
