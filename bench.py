@@ -306,11 +306,13 @@ def main():
         per_ms = j["ms"] / j["launches"]
         per_bytes = j["bytes"] / j["launches"]
         achieved = per_bytes / (per_ms * 1e-3) / 1e9
-        roof = {"bound": "hbm", "kernel": "local join (k_join_staged/_global, count+fill passes)",
+        roof = {"bound": "hbm", "kernel": "local-join pair distances (k_pairs, all tiers)",
                 "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "peak_kind": peak_kind, "traffic": None,
                 "fp32_pipe_tflops": j["flops"] / j["launches"] / (per_ms * 1e-3) / 1e12,
-                "join_share_of_step": j["ms"] / (ms * a.steps)}
+                "join_share_of_step": j["ms"] / (ms * a.steps),
+                "emit_share_of_step": prof["emit"]["ms"] / (ms * a.steps),
+                "merge_share_of_step": prof["merge"]["ms"] / (ms * a.steps)}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -115,7 +115,7 @@ int build_common(nnm_ctx* ctx, Kind kind, const float* x, bool dev, uint64_t n, 
     }
     Ctx& c = ctx->c;
     if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
-    GraphStore store;
+    GraphStore& store = c.store;
     GraphDev g;
     setup_graph(g, o, n, d, k);
     uint64_t sub = 0;
@@ -133,7 +133,6 @@ int build_common(nnm_ctx* ctx, Kind kind, const float* x, bool dev, uint64_t n, 
         cudaError_t e = cudaStreamSynchronize(c.stream);
         if (e != cudaSuccess) rc = fail(ctx, NNM_ERR_CUDA, cudaGetErrorString(e));
     }
-    store.release();
     if (!rc) fill_stats(stats, g, sub, ms);
     return rc;
 }
@@ -190,6 +189,7 @@ int nnm_ctx_destroy(nnm_ctx* ctx) {
     for (auto& e : ctx->c.ev)
         if (e) cudaEventDestroy(e);
     ctx->c.ws.release_all();
+    ctx->c.store.release();
     if (ctx->c.h_counters) cudaFreeHost(ctx->c.h_counters);
     if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
     delete ctx;
@@ -244,7 +244,7 @@ int nnm_hmerge_build(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint3
     if (!opts_ok(ctx, &o, &rc)) return rc;
     Ctx& c = ctx->c;
     if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
-    GraphStore store;
+    GraphStore& store = c.store;
     GraphDev g;
     setup_graph(g, o, n, d, k);
     nnm::DpgState dpg;
@@ -258,7 +258,6 @@ int nnm_hmerge_build(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint3
     if (!rc) rc = nnm::export_graph(c, g, ids, dists, flags, true);
     float ms = tm.stop();
     dpg.release();
-    store.release();
     if (!rc) fill_stats(stats, g, 0, ms);
     else if (layers) nnm_layers_free(layers);
     return rc;
@@ -272,7 +271,7 @@ int nnm_profile_enable(nnm_ctx* ctx, int on) {
             if (cudaEventCreate(&e) != cudaSuccess) return fail(ctx, NNM_ERR_CUDA, "cudaEventCreate failed");
     }
     ctx->c.prof = on != 0;
-    ctx->c.kjoin = ctx->c.kmerge = ctx->c.kiter = nnm::KStat();
+    ctx->c.kjoin = ctx->c.kemit = ctx->c.kmerge = nnm::KStat();
     return NNM_OK;
 }
 
@@ -281,8 +280,10 @@ int nnm_profile_get(const nnm_ctx* ctx, char* buf, uint64_t buflen) {
     const nnm::Ctx& c = ctx->c;
     int w = std::snprintf(buf, buflen,
                           "{\"join\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f, \"flops\": %.1f}, "
+                          "\"emit\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}, "
                           "\"merge\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}}",
                           (unsigned long long)c.kjoin.launches, c.kjoin.ms, c.kjoin.bytes, c.kjoin.flops,
+                          (unsigned long long)c.kemit.launches, c.kemit.ms, c.kemit.bytes,
                           (unsigned long long)c.kmerge.launches, c.kmerge.ms, c.kmerge.bytes);
     return (w < 0 || (uint64_t)w >= buflen) ? NNM_ERR_INVALID : NNM_OK;
 }

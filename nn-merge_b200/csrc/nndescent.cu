@@ -37,10 +37,14 @@ namespace nnm {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int JOIN_THREADS = 128;
 constexpr int MERGE_WARPS = 8;
 constexpr int SHUF_SMEM = 512;  // reverse-list entries a shuffling warp stages in shared memory
 constexpr int BIGSORT_CH = 4096;
+// Rows of the local join are binned by list size S = |new| + |old|: three
+// tiers whose vectors are staged in shared memory sized for the tier, and
+// the rest read from global memory (L2).
+constexpr uint32_t TIER_CAP[3] = {32, 64, 128};
+constexpr int TIER_THREADS[4] = {64, 64, 128, 128};
 
 // ---------------------------------------------------------------------------
 // 1. Sampling pass.
@@ -229,8 +233,8 @@ struct ShufArgs {
     uint32_t *newL, *oldL, *newlen, *oldlen;
     uint32_t capn, capo, n, smpl;
     uint32_t *rnewT, *roldT, *rnewTlen, *roldTlen;
-    uint32_t smem_rows;
-    uint32_t* bigjoin;
+    uint32_t* npairs;     // pair-distance slots per row
+    uint32_t* tier_rows;  // 4 lists of n rows: joined rows binned by list size
     IterCounters* ctr;
 };
 
@@ -301,12 +305,24 @@ __global__ void k_shuffle_append(ShufArgs a) {
     if (lane == 0) {
         a.newlen[t] = nl;
         a.oldlen[t] = ol;
-        if (nl > 0 && nl + ol > a.smem_rows) a.bigjoin[atomicAdd(&a.ctr->nbig_join, 1u)] = t;
+        // pairs of the local join: new x new above the diagonal, new x old
+        a.npairs[t] = nl ? nl * (nl - 1) / 2 + nl * ol : 0u;
+        if (nl) {
+            const uint32_t S = nl + ol;
+            const int tier = S <= TIER_CAP[0] ? 0 : S <= TIER_CAP[1] ? 1 : S <= TIER_CAP[2] ? 2 : 3;
+            a.tier_rows[(size_t)tier * a.n + atomicAdd(&a.ctr->ntier[tier], 1u)] = t;
+        }
     }
 }
 
 // ---------------------------------------------------------------------------
-// 4. Local join.
+// 4. Local join, in two kernels.
+//   k_pairs: every pair of a row's lists once -- new x new above the
+//     diagonal and new x old -- with the exact sequential distance, stored
+//     in the row's slice of the pair buffer; per list position, the number
+//     of proposals that pass the K-th-distance filter (for bucket sizes).
+//   k_emit: reads the stored distances and writes the proposals into the
+//     per-target buckets.
 struct JoinArgs {
     const float* x;
     uint32_t dp, K, n;
@@ -316,16 +332,15 @@ struct JoinArgs {
     uint32_t mode, verse;
     const uint32_t* leaf_off;
     uint32_t nleaf;
+    const uint32_t* tier_rows;
+    const uint64_t* poff;  // first pair slot of each row
+    float* pd;             // pair distances
     uint16_t* cntpos;
     uint32_t *bcnt, *bcur;
     const uint64_t* boff;
     Prop* bucket;
-    const uint32_t* bigrows;
-    uint32_t smem_rows;
     IterCounters* ctr;
 };
-
-enum { PASS_COUNT = 0, PASS_FILL = 1 };
 
 __device__ __forceinline__ uint32_t leaf_of(uint32_t id, const uint32_t* off, uint32_t nleaf) {
     uint32_t lo = 0, hi = nleaf;  // off[0] = 0 <= id < off[nleaf]
@@ -337,18 +352,48 @@ __device__ __forceinline__ uint32_t leaf_of(uint32_t id, const uint32_t* off, ui
     return lo;
 }
 
-template <int M, bool STAGED, int PASS>
-__device__ void join_row(const JoinArgs& a, uint32_t row, unsigned char* smem) {
+// Slot of pair (a, b), a < b, a in the new list: row-major over the upper
+// triangle of new x new, then new x old.
+__device__ __forceinline__ uint32_t pair_slot(uint32_t a, uint32_t b, uint32_t nn, uint32_t no) {
+    return b < nn ? a * nn - a * (a + 1) / 2 + (b - a - 1) : nn * (nn - 1) / 2 + a * no + (b - nn);
+}
+
+// The reference's join filter and visiting order for pair (a, b), a < b:
+// returns false if the pair is skipped, else the outer (first-inserted
+// target) and inner positions.
+__device__ __forceinline__ bool pair_order(uint32_t mode, uint32_t verse, uint32_t av, uint32_t bv, uint32_t nn,
+                                           uint32_t ea, uint32_t eb, uint32_t ga, uint32_t gb, uint32_t& outer,
+                                           uint32_t& inner) {
+    const uint32_t ida = ea & LID_MASK, idb = eb & LID_MASK;
+    if (ida == idb) return false;
+    outer = av;
+    inner = bv;
+    if (mode == MODE_KGRAPH) {
+        if (bv < nn && idb < ida) {  // kgraph.h:112-116 visits it from the smaller id
+            outer = bv;
+            inner = av;
+        }
+        return true;
+    }
+    if (mode == MODE_SMERGE) return ga != gb;
+    return ga != gb || ga == 1 || gb == 1 || verse;
+}
+
+// Vectors of a row's lists in shared memory: row q starts at 16-byte unit
+// q * vstride + q / 4 with vstride = 1 mod 8, so that the rows of 4x4 tiles
+// of neighbouring threads (q = 4t + i for consecutive t) fall in different
+// bank groups.
+__device__ __forceinline__ uint32_t vrow(uint32_t q, uint32_t vstride) { return q * vstride + (q >> 2); }
+
+template <int M, bool STAGED>
+__device__ void pairs_row(const JoinArgs& a, uint32_t row, unsigned char* smem, uint32_t R) {
     const uint32_t nn = a.newlen[row], no = a.oldlen[row], S = nn + no;
-    if (nn == 0) return;
-    const uint32_t R = STAGED ? a.smem_rows : a.caps;
     uint32_t* s_ids = reinterpret_cast<uint32_t*>(smem);
     float* s_kth = reinterpret_cast<float*>(s_ids + R);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_kth + R);
     uint32_t* s_grp = s_cnt + R;
-    unsigned long long* s_base = reinterpret_cast<unsigned long long*>(s_grp + R);  // 16R bytes before it
-    float4* s_vec = reinterpret_cast<float4*>(s_base + R);  // 24R bytes before it: 16-byte aligned for even R
-    const uint32_t dq = a.dp >> 2, vstride = dq + 1;
+    float4* s_vec = reinterpret_cast<float4*>(s_grp + R);  // 16R bytes before it
+    const uint32_t dq = a.dp >> 2, vstride = ((dq + 7) & ~7u) + 1;
     const float4* x4 = reinterpret_cast<const float4*>(a.x);
 
     for (uint32_t q = threadIdx.x; q < S; q += blockDim.x) {
@@ -363,23 +408,14 @@ __device__ void join_row(const JoinArgs& a, uint32_t row, unsigned char* smem) {
     if (STAGED) {
         for (uint32_t i = threadIdx.x; i < S * dq; i += blockDim.x) {
             uint32_t q = i / dq, c = i - q * dq;
-            s_vec[q * vstride + c] = x4[(size_t)(s_ids[q] & LID_MASK) * dq + c];
+            s_vec[vrow(q, vstride) + c] = x4[(size_t)(s_ids[q] & LID_MASK) * dq + c];
         }
+        __syncthreads();
     }
-    if (PASS == PASS_FILL) {
-        for (uint32_t q = threadIdx.x; q < S; q += blockDim.x) {
-            uint32_t c = a.cntpos[(size_t)row * a.caps + q];
-            if (c) {
-                uint32_t id = s_ids[q] & LID_MASK;
-                s_base[q] = a.boff[id] + atomicAdd(&a.bcur[id], c);
-            }
-        }
-    }
-    __syncthreads();
-
-    if (PASS == PASS_COUNT && threadIdx.x == 0) atomicAdd(&a.ctr->sum_s, (unsigned long long)S);
+    if (threadIdx.x == 0) atomicAdd(&a.ctr->sum_s, (unsigned long long)S);
     const uint32_t ntA = (nn + 3) >> 2, ntB = (S + 3) >> 2;
     const uint32_t ntiles = ntA * ntB - ntA * (ntA - 1) / 2;
+    float* pd = a.pd + a.poff[row];
     uint32_t cmps = 0;
     for (uint32_t t = threadIdx.x; t < ntiles; t += blockDim.x) {
         uint32_t ta = 0, rem = t;
@@ -393,8 +429,8 @@ __device__ void join_row(const JoinArgs& a, uint32_t row, unsigned char* smem) {
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             uint32_t ai = min(ta * 4 + i, nn - 1), bj = min(tb * 4 + i, S - 1);
-            pa[i] = STAGED ? s_vec + ai * vstride : x4 + (size_t)(s_ids[ai] & LID_MASK) * dq;
-            pb[i] = STAGED ? s_vec + bj * vstride : x4 + (size_t)(s_ids[bj] & LID_MASK) * dq;
+            pa[i] = STAGED ? s_vec + vrow(ai, vstride) : x4 + (size_t)(s_ids[ai] & LID_MASK) * dq;
+            pb[i] = STAGED ? s_vec + vrow(bj, vstride) : x4 + (size_t)(s_ids[bj] & LID_MASK) * dq;
         }
         float acc[4][4];
 #pragma unroll
@@ -426,72 +462,83 @@ __device__ void join_row(const JoinArgs& a, uint32_t row, unsigned char* smem) {
             for (int j = 0; j < 4; j++) {
                 const uint32_t bv = tb * 4 + j;
                 if (bv >= S || (bv < nn && bv <= av)) continue;
-                const uint32_t ea = s_ids[av], eb = s_ids[bv];
-                const uint32_t ida = ea & LID_MASK, idb = eb & LID_MASK;
-                if (ida == idb) continue;
-                uint32_t outer = av, inner = bv;
-                if (a.mode == MODE_KGRAPH) {
-                    if (bv < nn && idb < ida) {  // kgraph.h:112-116 visits it from the smaller id
-                        outer = bv;
-                        inner = av;
-                    }
-                } else if (a.mode == MODE_SMERGE) {
-                    if (s_grp[av] == s_grp[bv]) continue;
-                } else {
-                    uint32_t ga = s_grp[av], gb = s_grp[bv];
-                    if (!(ga != gb || ga == 1 || gb == 1 || a.verse)) continue;
-                }
-                cmps++;
                 const float dd = acc[i][j];
-                const unsigned long long kb =
-                    (1ull << 63) | ((unsigned long long)row << 32) | ((unsigned long long)(outer * S + inner) << 1);
-                if (dd < s_kth[outer]) {
-                    if (PASS == PASS_COUNT) atomicAdd(&s_cnt[outer], 1u);
-                    else {
-                        unsigned long long slot = s_base[outer] + atomicAdd(&s_cnt[outer], 1u);
-                        a.bucket[slot] = Prop{dd, s_ids[inner], kb};
-                    }
-                }
-                if (dd < s_kth[inner]) {
-                    if (PASS == PASS_COUNT) atomicAdd(&s_cnt[inner], 1u);
-                    else {
-                        unsigned long long slot = s_base[inner] + atomicAdd(&s_cnt[inner], 1u);
-                        a.bucket[slot] = Prop{dd, s_ids[outer], kb | 1ull};
-                    }
-                }
+                pd[pair_slot(av, bv, nn, no)] = dd;
+                uint32_t outer, inner;
+                if (!pair_order(a.mode, a.verse, av, bv, nn, s_ids[av], s_ids[bv], s_grp[av], s_grp[bv], outer, inner))
+                    continue;
+                cmps++;
+                if (dd < s_kth[outer]) atomicAdd(&s_cnt[outer], 1u);
+                if (dd < s_kth[inner]) atomicAdd(&s_cnt[inner], 1u);
             }
         }
     }
-    if (PASS == PASS_COUNT) {
-        for (int o = 16; o > 0; o >>= 1) cmps += __shfl_xor_sync(FULL, cmps, o);
-        if ((threadIdx.x & 31) == 0 && cmps) atomicAdd(&a.ctr->ncmps, (unsigned long long)cmps);
+    for (int o = 16; o > 0; o >>= 1) cmps += __shfl_xor_sync(FULL, cmps, o);
+    if ((threadIdx.x & 31) == 0 && cmps) atomicAdd(&a.ctr->ncmps, (unsigned long long)cmps);
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < S; q += blockDim.x) {
+        uint32_t c = s_cnt[q];
+        a.cntpos[(size_t)row * a.caps + q] = (uint16_t)c;
+        if (c) atomicAdd(&a.bcnt[s_ids[q] & LID_MASK], c);
     }
     __syncthreads();
-    if (PASS == PASS_COUNT) {
-        for (uint32_t q = threadIdx.x; q < S; q += blockDim.x) {
-            uint32_t c = s_cnt[q];
-            a.cntpos[(size_t)row * a.caps + q] = (uint16_t)c;
-            if (c) atomicAdd(&a.bcnt[s_ids[q] & LID_MASK], c);
+}
+
+template <int M, int TIER>
+__global__ void __launch_bounds__(TIER_THREADS[TIER]) k_pairs(JoinArgs a, uint32_t R) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t cnt = a.ctr->ntier[TIER];
+    const uint32_t* rows = a.tier_rows + (size_t)TIER * a.n;
+    for (uint32_t b = blockIdx.x; b < cnt; b += gridDim.x) pairs_row<M, (TIER < 3)>(a, rows[b], smem, R);
+}
+
+// One warp per row: proposals from the stored pair distances.
+constexpr int EMIT_WARPS = 4;
+
+__global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t row = blockIdx.x * EMIT_WARPS + w;
+    if (row >= a.n) return;
+    const uint32_t nn = a.newlen[row], no = a.oldlen[row], S = nn + no;
+    if (nn == 0) return;
+    const uint32_t R = a.caps;
+    unsigned char* base = smem + (size_t)w * R * 24;
+    unsigned long long* s_base = reinterpret_cast<unsigned long long*>(base);
+    uint32_t* s_ids = reinterpret_cast<uint32_t*>(s_base + R);
+    float* s_kth = reinterpret_cast<float*>(s_ids + R);
+    uint32_t* s_cur = reinterpret_cast<uint32_t*>(s_kth + R);
+    uint32_t* s_grp = s_cur + R;
+    for (uint32_t q = lane; q < S; q += 32) {
+        uint32_t e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
+        uint32_t id = e & LID_MASK;
+        s_ids[q] = e;
+        s_kth[q] = a.pdist[(size_t)id * a.K + a.K - 1];
+        s_cur[q] = 0;
+        s_grp[q] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
+        uint32_t c = a.cntpos[(size_t)row * a.caps + q];
+        if (c) s_base[q] = a.boff[id] + atomicAdd(&a.bcur[id], c);
+    }
+    __syncwarp();
+    const float* pd = a.pd + a.poff[row];
+    for (uint32_t av = 0; av < nn; av++) {
+        for (uint32_t bv = av + 1 + lane; bv < S; bv += 32) {
+            uint32_t outer, inner;
+            if (!pair_order(a.mode, a.verse, av, bv, nn, s_ids[av], s_ids[bv], s_grp[av], s_grp[bv], outer, inner))
+                continue;
+            const float dd = pd[pair_slot(av, bv, nn, no)];
+            const unsigned long long kb =
+                (1ull << 63) | ((unsigned long long)row << 32) | ((unsigned long long)(outer * S + inner) << 1);
+            if (dd < s_kth[outer]) {
+                unsigned long long slot = s_base[outer] + atomicAdd(&s_cur[outer], 1u);
+                a.bucket[slot] = Prop{dd, s_ids[inner], kb};
+            }
+            if (dd < s_kth[inner]) {
+                unsigned long long slot = s_base[inner] + atomicAdd(&s_cur[inner], 1u);
+                a.bucket[slot] = Prop{dd, s_ids[outer], kb | 1ull};
+            }
         }
     }
-    __syncthreads();
-}
-
-template <int M, int PASS>
-__global__ void __launch_bounds__(JOIN_THREADS) k_join_staged(JoinArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t row = blockIdx.x;
-    if (row >= a.n) return;
-    uint32_t S = a.newlen[row] + a.oldlen[row];
-    if (S > a.smem_rows) return;  // handled by k_join_global
-    join_row<M, true, PASS>(a, row, smem);
-}
-
-template <int M, int PASS>
-__global__ void __launch_bounds__(JOIN_THREADS) k_join_global(JoinArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t nbig = a.ctr->nbig_join;
-    for (uint32_t b = blockIdx.x; b < nbig; b += gridDim.x) join_row<M, false, PASS>(a, a.bigrows[b], smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -706,29 +753,37 @@ int graph_alloc(Ctx& ctx, GraphStore& s, GraphDev& g, bool with_carry) {
     return 0;
 }
 
-template <int M>
-static void launch_join(const JoinArgs& ja, size_t smem_staged, size_t smem_global, int pass, cudaStream_t st,
-                        int nsm) {
-    if (pass == PASS_COUNT) {
-        k_join_staged<M, PASS_COUNT><<<ja.n, JOIN_THREADS, smem_staged, st>>>(ja); count_launch();
-        k_join_global<M, PASS_COUNT><<<nsm * 2, JOIN_THREADS, smem_global, st>>>(ja); count_launch();
-    } else {
-        k_join_staged<M, PASS_FILL><<<ja.n, JOIN_THREADS, smem_staged, st>>>(ja); count_launch();
-        k_join_global<M, PASS_FILL><<<nsm * 2, JOIN_THREADS, smem_global, st>>>(ja); count_launch();
-    }
+// Shared memory of a k_pairs block: member arrays (16 B per list slot) and,
+// for the staged tiers, the swizzled vectors.
+static size_t pairs_smem(uint32_t R, uint32_t dp, bool staged) {
+    const uint32_t dq = dp / 4, vstride = ((dq + 7) & ~7u) + 1;
+    return (size_t)R * 16 + (staged ? ((size_t)R * vstride + R / 4 + 1) * 16 : 0) + 64;
 }
 
 template <int M>
-static cudaError_t set_join_attrs(size_t smem_staged, size_t smem_global) {
+static cudaError_t prep_pairs(uint32_t caps, uint32_t dp, size_t emit_smem) {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_join_staged<M, PASS_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem_staged)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_join_staged<M, PASS_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem_staged)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_join_global<M, PASS_COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem_global)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_join_global<M, PASS_FILL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_global);
+    if ((e = cudaFuncSetAttribute(k_pairs<M, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)pairs_smem(TIER_CAP[0], dp, true))) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_pairs<M, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)pairs_smem(TIER_CAP[1], dp, true))) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_pairs<M, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)pairs_smem(TIER_CAP[2], dp, true))) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_pairs<M, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)pairs_smem(caps, dp, false))) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)emit_smem);
+}
+
+template <int M>
+static void launch_pairs(const JoinArgs& ja, const unsigned* ntier, uint32_t caps, uint32_t dp, int nsm,
+                         cudaStream_t st) {
+    if (ntier[0]) { k_pairs<M, 0><<<ntier[0], TIER_THREADS[0], pairs_smem(TIER_CAP[0], dp, true), st>>>(ja, TIER_CAP[0]); count_launch(); }
+    if (ntier[1]) { k_pairs<M, 1><<<ntier[1], TIER_THREADS[1], pairs_smem(TIER_CAP[1], dp, true), st>>>(ja, TIER_CAP[1]); count_launch(); }
+    if (ntier[2]) { k_pairs<M, 2><<<ntier[2], TIER_THREADS[2], pairs_smem(TIER_CAP[2], dp, true), st>>>(ja, TIER_CAP[2]); count_launch(); }
+    if (ntier[3]) {
+        unsigned g = std::min<unsigned>(ntier[3], (unsigned)nsm * 4);
+        k_pairs<M, 3><<<g, TIER_THREADS[3], pairs_smem(caps, dp, false), st>>>(ja, caps); count_launch();
+    }
 }
 
 // Sequential float mean of the per-row deltas, as the reference computes it
@@ -764,7 +819,6 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     NNM_CUDA_TRY(ws.bcur.ensure(n1 * 4));
     NNM_CUDA_TRY(ws.boff.ensure(n1 * 8));
     NNM_CUDA_TRY(ws.bigrev.ensure(n1 * 2 * 4));
-    NNM_CUDA_TRY(ws.bigjoin.ensure(n1 * 4));
     NNM_CUDA_TRY(ws.nflag.ensure(n1));
     NNM_CUDA_TRY(ws.scan_tmp.ensure((scan_temp_elems(n1) + 8) * 8));
     NNM_CUDA_TRY(ws.counters.ensure(sizeof(IterCounters) + 64));
@@ -779,16 +833,14 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     uint64_t* d_tot = P<uint64_t>(ws.scan_tmp) + scan_temp_elems(n1) + 4;  // past the scan scratch
     IterCounters* ctr = P<IterCounters>(ws.counters);
 
-    const uint32_t dq = g.dp / 4, vstride = dq + 1;
-    const uint32_t member_bytes_per_row = 4 + 4 + 4 + 4 + 8;
-    uint32_t smem_rows = std::min<uint32_t>(caps, 120u);
-    while (smem_rows > 16 && (size_t)smem_rows * (vstride * 16 + member_bytes_per_row) + 64 > 100 * 1024) smem_rows -= 4;
-    const size_t smem_staged = (size_t)smem_rows * (vstride * 16 + member_bytes_per_row) + 64;
-    const size_t smem_global = (size_t)caps * member_bytes_per_row + 64;
-    cudaError_t ae = g.metric == L2 ? set_join_attrs<L2>(smem_staged, smem_global)
-                     : g.metric == L1 ? set_join_attrs<L1>(smem_staged, smem_global)
-                                      : set_join_attrs<CHI2>(smem_staged, smem_global);
+    const size_t emit_smem = (size_t)EMIT_WARPS * caps * 24 + 64;
+    cudaError_t ae = g.metric == L2 ? prep_pairs<L2>(caps, g.dp, emit_smem)
+                     : g.metric == L1 ? prep_pairs<L1>(caps, g.dp, emit_smem)
+                                      : prep_pairs<CHI2>(caps, g.dp, emit_smem);
     NNM_CUDA_TRY(ae);
+    NNM_CUDA_TRY(ws.npairs.ensure(n1 * 4));
+    NNM_CUDA_TRY(ws.poff.ensure(n1 * 8));
+    NNM_CUDA_TRY(ws.tiers.ensure((size_t)n * 4 * 4 + 16));
 
     const unsigned warp_blocks = (unsigned)((n + 7) / 8);
     const unsigned tblocks = (unsigned)((n + 255) / 256);
@@ -832,38 +884,43 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     g.capn, g.capo, n, g.smpl,
                     track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
                     track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
-                    smem_rows, P<uint32_t>(ws.bigjoin), ctr};
+                    P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr};
         k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh); count_launch();
-        // local join, pass 1: count proposals per target
+        NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.npairs), P<uint64_t>(ws.poff), n, scan_tmp,
+                                    reinterpret_cast<uint64_t*>(&ctr->pairs), st));
         NNM_CUDA_TRY(cudaMemsetAsync(ws.bcnt.p, 0, n1 * 4, st));
         NNM_CUDA_TRY(cudaMemsetAsync(ws.bcur.p, 0, n1 * 4, st));
-        JoinArgs ja{g.x, g.dp, K, n, g.pdist, g.newL, g.oldL,
-                    g.newlen, g.oldlen, g.capn, g.capo, caps, (uint32_t)mode, verse,
-                    d_leaf_off, nleaf, P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
-                    P<uint64_t>(ws.boff), P<Prop>(ws.bucket), P<uint32_t>(ws.bigjoin), smem_rows, ctr};
-        if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
-        if (g.metric == L2) launch_join<L2>(ja, smem_staged, smem_global, PASS_COUNT, st, nsm);
-        else if (g.metric == L1) launch_join<L1>(ja, smem_staged, smem_global, PASS_COUNT, st, nsm);
-        else launch_join<CHI2>(ja, smem_staged, smem_global, PASS_COUNT, st, nsm);
-        if (ctx.prof) cudaEventRecord(ctx.ev[1], st);
-        NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff), n, scan_tmp,
-                                    reinterpret_cast<uint64_t*>(&ctr->proposals), st));
         NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
         NNM_CUDA_TRY(cudaStreamSynchronize(st));
         if (ctx.h_counters->error) {
             ctx.last_error = "device capacity check failed (code " + std::to_string(ctx.h_counters->error) + ")";
             return 6;
         }
+        unsigned ntier[4];
+        for (int t = 0; t < 4; t++) ntier[t] = ctx.h_counters->ntier[t];
+        NNM_CUDA_TRY(ws.pd.ensure(std::max<uint64_t>(ctx.h_counters->pairs, 1) * 4));
+        // local join, pass 1: pair distances and per-target proposal counts
+        JoinArgs ja{g.x, g.dp, K, n, g.pdist, g.newL, g.oldL, g.newlen, g.oldlen, g.capn, g.capo, caps,
+                    (uint32_t)mode, verse, d_leaf_off, nleaf, P<uint32_t>(ws.tiers), P<uint64_t>(ws.poff),
+                    P<float>(ws.pd), P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
+                    P<uint64_t>(ws.boff), P<Prop>(ws.bucket), ctr};
+        if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
+        if (g.metric == L2) launch_pairs<L2>(ja, ntier, caps, g.dp, nsm, st);
+        else if (g.metric == L1) launch_pairs<L1>(ja, ntier, caps, g.dp, nsm, st);
+        else launch_pairs<CHI2>(ja, ntier, caps, g.dp, nsm, st);
+        if (ctx.prof) cudaEventRecord(ctx.ev[1], st);
+        NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff), n, scan_tmp,
+                                    reinterpret_cast<uint64_t*>(&ctr->proposals), st));
+        NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
+        NNM_CUDA_TRY(cudaStreamSynchronize(st));
         const uint64_t nprop = ctx.h_counters->proposals;
         if (nprop * sizeof(Prop) > ws.bucket.bytes) {
             NNM_CUDA_TRY(ws.bucket.ensure((size_t)(nprop * 1.25 + 1024) * sizeof(Prop)));
             ja.bucket = P<Prop>(ws.bucket);
         }
-        // pass 2: recompute and fill the buckets
+        // pass 2: proposals from the stored distances
         if (ctx.prof) cudaEventRecord(ctx.ev[2], st);
-        if (g.metric == L2) launch_join<L2>(ja, smem_staged, smem_global, PASS_FILL, st, nsm);
-        else if (g.metric == L1) launch_join<L1>(ja, smem_staged, smem_global, PASS_FILL, st, nsm);
-        else launch_join<CHI2>(ja, smem_staged, smem_global, PASS_FILL, st, nsm);
+        k_emit<<<(n + EMIT_WARPS - 1) / EMIT_WARPS, EMIT_WARPS * 32, emit_smem, st>>>(ja); count_launch();
         MergeArgs ma{g.pid, g.pdist, n, K, P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff),
                      P<Prop>(ws.bucket), P<uint8_t>(ws.nflag), ctr};
         if (ctx.prof) cudaEventRecord(ctx.ev[3], st);
@@ -883,15 +940,18 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             cudaEventElapsedTime(&t01, ctx.ev[0], ctx.ev[1]);
             cudaEventElapsedTime(&t23, ctx.ev[2], ctx.ev[3]);
             cudaEventElapsedTime(&t34, ctx.ev[3], ctx.ev[4]);
-            // algorithmic traffic: each joined row gathers its list vectors,
-            // list ids and the K-th distances once per pass; the count pass
-            // writes and the fill pass reads a 2-byte count per list slot;
-            // the fill pass writes every proposal (16 B).
-            const double row_bytes = (double)hc.sum_s * ((double)g.dp * 4.0 + 4.0 + 4.0 + 2.0);
-            ctx.kjoin.launches += 2;
-            ctx.kjoin.ms += (double)t01 + (double)t23;
-            ctx.kjoin.bytes += 2.0 * row_bytes + (double)hc.proposals * 16.0;
-            ctx.kjoin.flops += 2.0 * (double)hc.ncmps * (double)g.d * 3.0;
+            // algorithmic traffic of the pair kernel: each joined row gathers
+            // its list vectors, list ids and the K-th distances once, writes
+            // one 2-byte count per list slot and one distance per pair; the
+            // emit kernel reads the pair distances and the row's members and
+            // writes every proposal (16 B).
+            ctx.kjoin.launches += (hc.ntier[0] > 0) + (hc.ntier[1] > 0) + (hc.ntier[2] > 0) + (hc.ntier[3] > 0);
+            ctx.kjoin.ms += t01;
+            ctx.kjoin.bytes += (double)hc.sum_s * ((double)g.dp * 4.0 + 4.0 + 4.0 + 2.0) + (double)hc.pairs * 4.0;
+            ctx.kjoin.flops += (double)hc.pairs * (double)g.d * 3.0;
+            ctx.kemit.launches += 1;
+            ctx.kemit.ms += t23;
+            ctx.kemit.bytes += (double)hc.pairs * 4.0 + (double)hc.sum_s * 18.0 + (double)hc.proposals * 16.0;
             ctx.kmerge.launches += 1;
             ctx.kmerge.ms += t34;
             ctx.kmerge.bytes += (double)n * K * 16.0 + (double)hc.proposals * 16.0 + (double)n * 13.0;

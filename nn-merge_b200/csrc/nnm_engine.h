@@ -38,11 +38,23 @@ struct DevBuf {
 // Scratch for one NN-Descent iteration, sized for the largest graph seen.
 struct Workspace {
     DevBuf rcnt, rcur, rtot, roff, rseg, rscr, rcount, rofs, rbuf;
-    DevBuf cntpos, bcnt, bcur, boff, bucket, bigrev, bigjoin, nflag, scan_tmp;
+    DevBuf cntpos, bcnt, bcur, boff, bucket, bigrev, nflag, scan_tmp;
+    DevBuf npairs, poff, pd, tiers;
     DevBuf draws, counters, misc;
     void release_all() {
-        DevBuf* all[] = {&rcnt, &rcur, &rtot, &roff, &rseg, &rscr, &rcount, &rofs, &rbuf, &cntpos, &bcnt,
-                         &bcur, &boff, &bucket, &bigrev, &bigjoin, &nflag, &scan_tmp, &draws, &counters, &misc};
+        DevBuf* all[] = {&rcnt, &rcur, &rtot, &roff, &rseg, &rscr, &rcount, &rofs, &rbuf, &cntpos, &bcnt, &bcur,
+                         &boff, &bucket, &bigrev, &nflag, &scan_tmp, &npairs, &poff, &pd, &tiers, &draws,
+                         &counters, &misc};
+        for (auto* b : all) b->release();
+    }
+};
+
+// Device storage of a graph under construction (owned buffers).
+struct GraphStore {
+    DevBuf pid, pdist, cpid, cpdist, newL, oldL, newlen, oldlen, rnewT, roldT, rnewTlen, roldTlen, x;
+    void release() {
+        DevBuf* all[] = {&pid, &pdist, &cpid, &cpdist, &newL, &oldL, &newlen, &oldlen,
+                         &rnewT, &roldT, &rnewTlen, &roldTlen, &x};
         for (auto* b : all) b->release();
     }
 };
@@ -57,7 +69,8 @@ struct KStat {
 struct Ctx {
     int device = 0;
     bool prof = false;
-    KStat kjoin, kmerge, kiter;
+    GraphStore store;  // graph arrays, reused across calls (grow-only)
+    KStat kjoin, kemit, kmerge;
     cudaEvent_t ev[8] = {};
     cudaStream_t stream = nullptr;
     Workspace ws;
@@ -65,16 +78,6 @@ struct Ctx {
     std::string last_error;
     double last_device_ms = 0.0;
     uint64_t kernel_launches = 0;
-};
-
-// Device storage of a graph under construction (owned buffers).
-struct GraphStore {
-    DevBuf pid, pdist, cpid, cpdist, newL, oldL, newlen, oldlen, rnewT, roldT, rnewTlen, roldTlen, x;
-    void release() {
-        DevBuf* all[] = {&pid, &pdist, &cpid, &cpdist, &newL, &oldL, &newlen, &oldlen,
-                         &rnewT, &roldT, &rnewTlen, &roldTlen, &x};
-        for (auto* b : all) b->release();
-    }
 };
 
 // A graph under construction: raw device pointers, so that a sub-graph

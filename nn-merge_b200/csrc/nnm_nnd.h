@@ -34,9 +34,11 @@ struct IterCounters {
     unsigned long long rand_draws; // std::rand() calls of the shuffles
     unsigned int error;            // nonzero: a capacity or input check failed
     unsigned int nbig_rev;         // reverse lists longer than one warp
-    unsigned int nbig_join;        // rows whose sample lists exceed shared memory
+    unsigned int unused;
     unsigned int pad;
     unsigned long long sum_s;      // sum over joined rows of |new| + |old|
+    unsigned long long pairs;      // pair-distance slots of this iteration
+    unsigned int ntier[4];         // rows per pair-kernel tier (by list size)
 };
 
 enum DevError : unsigned int {
