@@ -59,6 +59,11 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=40_000)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--path", default="exact", choices=["exact", "fast"],
+                   help="exact: the reference's random streams, bit-exact (plain FP32); "
+                        "fast: counter-based draws on the device")
+    p.add_argument("--delta", type=float, default=None, help="convergence threshold (default: the reference's 0.002)")
+    p.add_argument("--smpl", type=int, default=100, help="reverse-sample cap smplNum (reference: 100)")
     return p.parse_args()
 
 
@@ -250,9 +255,12 @@ def main():
     ctx = nnm.Context(local)
     build_seed = a.seed
 
+    bkw = dict(seed=build_seed, rng=a.path, sample_cap=a.smpl,
+               delta=a.delta if a.delta is not None else 0.002)
+
     def build_dev():
         return ctx.merge_leaves_dev(x_dev.data_ptr(), n, d, k, sizes, ids_dev.data_ptr(), dists_dev.data_ptr(), 0,
-                                    seed=build_seed)
+                                    **bkw)
 
     for _ in range(a.warmup):
         st = build_dev()
@@ -284,11 +292,11 @@ def main():
         x_pin = torch.from_numpy(x).pin_memory()
         ids_pin = torch.empty((n, k), dtype=torch.int32).pin_memory()
         xh, ih = x_pin.numpy(), ids_pin.numpy().view(np.uint32)
-        ctx.merge_leaves_into(xh, k, sizes, ih, seed=build_seed)
+        ctx.merge_leaves_into(xh, k, sizes, ih, **bkw)
         barrier()
         t0 = time.perf_counter()
         for _ in range(a.steps):
-            ctx.merge_leaves_into(xh, k, sizes, ih, seed=build_seed)
+            ctx.merge_leaves_into(xh, k, sizes, ih, **bkw)
         e2e_s = max_over_ranks((time.perf_counter() - t0) / a.steps)
         e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(x.nbytes),
                "d2h_bytes_per_step": int(n * k * 4)}
@@ -328,9 +336,12 @@ def main():
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded %d-centre Gaussian mixture, integers 0-255 (stand-in for SIFT-like data)"
                     % a.centres,
-            "config": {"workload": "%dx%d k=%d: NN-Descent on %d leaves of %d rows + S-Merge of the leaves "
-                                   "(plain FP32, reference-exact)" % (n, d, k, a.leaves, sizes[0]),
-                       "n": n, "d": d, "k": k, "leaves": a.leaves, "path": "plain_fp32_exact",
+            "config": {"workload": "%dx%d k=%d: NN-Descent on %d leaves of %d rows + S-Merge of the leaves (%s)"
+                                   % (n, d, k, a.leaves, sizes[0],
+                                      "plain FP32, reference-exact" if a.path == "exact" else "fast tier"),
+                       "n": n, "d": d, "k": k, "leaves": a.leaves,
+                       "path": "plain_fp32_exact" if a.path == "exact" else "fast",
+                       "delta": bkw["delta"], "smpl": a.smpl,
                        "recall@10": rec, "iterations": st["iterations"], "ncmps_merge": st["ncmps"],
                        "ncmps_leaves": st["sub_ncmps"],
                        "l2": "inputs (%d MB) larger than L2 (126 MB)" % (x.nbytes >> 20),

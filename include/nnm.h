@@ -43,7 +43,11 @@ typedef enum {
     NNM_METRIC_CHI2 = 2  /* DistOpt::KSquare, distopt.cpp:165-184 */
 } nnm_metric;
 
-typedef enum { NNM_RNG_EXACT = 0 } nnm_rng_mode;
+typedef enum {
+    NNM_RNG_EXACT = 0, /* the reference's mt19937 / std::rand streams: bit-exact results */
+    NNM_RNG_FAST = 1   /* counter-based draws (Philox) on the device: same algorithm, different
+                          random choices, no host-side streams and no ordering of reverse lists */
+} nnm_rng_mode;
 
 typedef struct {
     uint32_t seed;        /* clock value the reference's time(NULL) seeding is frozen at */

@@ -179,10 +179,98 @@ __global__ void k_cross_sample(CrossArgs a) {
     }
 }
 
+// Fast tier: initial graphs and cross samples from Philox draws.  Per row,
+// keep the best `keep` pool entries (their worst K - keep move to the
+// compensation list), then draw K - keep distinct ids -- not the row itself,
+// not already in the pool -- from the row's id space, compute their
+// distances and sort the pool.  Each lane draws one candidate per round;
+// duplicates within a round are resolved with __match_any_sync.
+struct FastArgs {
+    const float* x;
+    uint32_t dp, K;
+    int metric;
+    uint32_t* pid;
+    float* pdist;
+    uint32_t* cpid;
+    float* cpdist;
+    uint32_t row0, row1;
+    uint32_t keep;
+    uint32_t range, base;      // ids base + [0, range) ...
+    const uint32_t* leaf_off;  // ... or, when set, all rows outside the row's own leaf
+    uint32_t nleaf;
+    uint32_t gd_new;           // 0: gd 0, 1: gd 1, 2: gd = (id >= gd_split)
+    uint32_t gd_split;
+    uint32_t seed, phase;
+    IterCounters* ctr;
+};
+
+__global__ void k_fast_rows(FastArgs a) {
+    __shared__ SortEnt ents[WPB][MAXK];
+    __shared__ uint32_t fresh[WPB][MAXK];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t row = a.row0 + blockIdx.x * WPB + w;
+    if (row >= a.row1) return;
+    const uint32_t K = a.K, need = K - a.keep;
+    uint32_t lo = a.base, span = 0, range = a.range;
+    if (a.leaf_off) {
+        uint32_t g = leaf_index(row, a.leaf_off, a.nleaf);
+        lo = a.leaf_off[g];
+        span = a.leaf_off[g + 1] - lo;
+        range = a.leaf_off[a.nleaf] - span;
+    }
+    if (lane < (int)K && a.keep) ents[w][lane] = SortEnt{a.pdist[(size_t)row * K + lane], a.pid[(size_t)row * K + lane]};
+    __syncwarp();
+    if (a.keep && lane < (int)need) {
+        a.cpid[(size_t)row * K + lane] = ents[w][a.keep + lane].id;
+        a.cpdist[(size_t)row * K + lane] = ents[w][a.keep + lane].dist;
+    }
+    const Philox ph{a.seed, 0x6e6e6d02u};
+    uint32_t taken = 0;
+    for (uint32_t round = 0; taken < need && round < 64; round++) {
+        const uint32_t s = bounded(ph(row, a.phase, round, (uint32_t)lane).x, range);
+        const uint32_t id = a.leaf_off ? (s < lo ? s : s + span) : s + a.base;
+        bool ok = id != row;
+        for (uint32_t l = 0; l < K && ok; l++)
+            if (a.keep && (ents[w][l].id & ID_MASK) == id) ok = false;
+        for (uint32_t l = 0; l < taken && ok; l++)
+            if (fresh[w][l] == id) ok = false;
+        const unsigned same = __match_any_sync(FULL, id);
+        if ((int)(__ffs(same) - 1) != lane) ok = false;  // first lane of equal draws
+        const unsigned bal = __ballot_sync(FULL, ok);
+        const uint32_t r = taken + __popc(bal & ((1u << lane) - 1u));
+        __syncwarp();
+        if (ok && r < need) fresh[w][r] = id;
+        taken += __popc(bal);
+        __syncwarp();
+    }
+    if (taken < need) {
+        if (lane == 0) atomicOr(&a.ctr->error, (unsigned)DERR_CROSS_SAMPLE);
+        return;
+    }
+    if (lane < (int)need) {
+        const uint32_t id = fresh[w][lane];
+        const float d = dist_seq_rt(a.metric, a.x + (size_t)row * a.dp, a.x + (size_t)id * a.dp, a.dp);
+        const uint32_t gd = a.gd_new == 1 ? GD_BIT : (a.gd_new == 2 && id >= a.gd_split ? GD_BIT : 0u);
+        ents[w][a.keep + lane] = SortEnt{d, id | gd | FLAG_BIT};
+    }
+    __syncwarp();
+    if (lane == 0) std_sort_dev(ents[w], (int)K);
+    __syncwarp();
+    if (lane < (int)K) {
+        a.pid[(size_t)row * K + lane] = ents[w][lane].id;
+        a.pdist[(size_t)row * K + lane] = ents[w][lane].dist;
+    }
+}
+
 // merge2one (abstractmerge.cpp:232-277, lynndescent.cpp:455-500): merge each
 // pool with its compensation list, pool first on equal distances, keep K.
+// The reference does not look for ids that are in both lists -- after an
+// H-Merge level a compensation id can be back in the pool, and most rows of
+// the reference's H-Merge output then hold duplicate ids.  The exact path
+// keeps that; with `dedupe` (fast tier) such compensation entries are
+// dropped, so every row keeps K distinct ids.
 __global__ void k_merge2one(uint32_t* pid, float* pdist, const uint32_t* cpid, const float* cpdist, uint32_t K,
-                            uint32_t cut, uint32_t rows) {
+                            uint32_t cut, uint32_t rows, uint32_t dedupe) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t row = blockIdx.x * WPB + w;
     if (row >= rows) return;
@@ -196,21 +284,24 @@ __global__ void k_merge2one(uint32_t* pid, float* pdist, const uint32_t* cpid, c
         ce = cpid[(size_t)row * K + lane];
         cd = cpdist[(size_t)row * K + lane];
     }
-    uint32_t pp = lane, cp = lane;
+    bool keepc = lane < (int)cut;
+    if (dedupe)
+        for (uint32_t j = 0; j < K; j++)
+            if ((__shfl_sync(FULL, pe, j) & ID_MASK) == (ce & ID_MASK)) keepc = false;
+    const unsigned km = __ballot_sync(FULL, keepc);
+    uint32_t pp = lane, cp = __popc(km & ((1u << lane) - 1u));
     for (uint32_t j = 0; j < K; j++) {
         float od = __shfl_sync(FULL, pd, j);
-        if (j < cut) {
-            float oc = __shfl_sync(FULL, cd, j);
-            if (oc < pd) pp++;  // compensation entries strictly smaller come first
-        }
-        if (od <= cd) cp++;    // pool entries with equal distance win
+        float oc = __shfl_sync(FULL, cd, j);
+        if (j < cut && ((km >> j) & 1u) && oc < pd) pp++;  // compensation entries strictly smaller come first
+        if (od <= cd) cp++;                                // pool entries with equal distance win
     }
     __syncwarp();
     if (lane < (int)K && pp < K) {
         pid[(size_t)row * K + pp] = pe;
         pdist[(size_t)row * K + pp] = pd;
     }
-    if (lane < (int)cut && cp < K) {
+    if (keepc && cp < K) {
         pid[(size_t)row * K + cp] = ce;
         pdist[(size_t)row * K + cp] = cd;
     }
@@ -329,8 +420,25 @@ int export_graph(Ctx& ctx, const GraphDev& g, uint32_t* ids, float* dists, uint8
 }
 
 // KGraph on rows [0, g.n) of g (x, pid, pdist already offset by the caller).
+static int fast_rows(Ctx& ctx, GraphDev& g, uint32_t row0, uint32_t row1, uint32_t keep, uint32_t range,
+                     uint32_t base, const uint32_t* leaf_off, uint32_t nleaf, uint32_t gd_new, uint32_t gd_split) {
+    int rc;
+    if ((rc = reset_counters(ctx))) return rc;
+    FastArgs fa{g.x, g.dp, g.K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist, row0, row1, keep, range, base,
+                leaf_off, nleaf, gd_new, gd_split, g.seed, g.phase++, ctx.ws.counters.as<IterCounters>()};
+    k_fast_rows<<<blocks_for(row1 - row0, WPB), WPB * 32, 0, ctx.stream>>>(fa); count_launch();
+    NNM_CUDA_TRY(cudaGetLastError());
+    return check_counters(ctx);
+}
+
 int kgraph_build(Ctx& ctx, GraphDev& g) {
     const uint32_t K = g.K, n = g.n;
+    if (g.fast) {
+        int rc = fast_rows(ctx, g, 0, n, 0, n, 0, nullptr, 0, 0, 0);
+        if (rc) return rc;
+        g.ncmps += (uint64_t)n * K;
+        return run_nndescent(ctx, g, MODE_KGRAPH, 0, 0, nullptr, 0);
+    }
     const uint32_t per = sds_draws(K + 1, n);
     std::vector<uint32_t> h((size_t)n * per);
     gen_mt19937(g.seed, h.size(), h.data());
@@ -384,6 +492,17 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
     if (sub_ncmps) *sub_ncmps = subc;
     // 2. cross sampling (smerge.cpp:94-209)
     g.cut = K * 1 / 2;
+    if (g.fast) {
+        DevBuf& lo = ctx.ws.misc;
+        NNM_CUDA_TRY(lo.ensure(leaf_off.size() * 4 + 64));
+        NNM_CUDA_TRY(cudaMemcpyAsync(lo.p, leaf_off.data(), leaf_off.size() * 4, cudaMemcpyHostToDevice, ctx.stream));
+        if ((rc = fast_rows(ctx, g, 0, n, K - g.cut, 0, 0, lo.as<uint32_t>(), nleaf, 0, 0))) return rc;
+        g.ncmps += (uint64_t)n * g.cut;
+        if ((rc = run_nndescent(ctx, g, MODE_SMERGE, leaf_off[1], 0, lo.as<uint32_t>(), nleaf))) return rc;
+        k_merge2one<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, n, g.fast ? 1u : 0u); count_launch();
+        NNM_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
     std::vector<uint32_t> h;
     h.reserve((size_t)n * (2 * g.cut + 1));
     {
@@ -419,7 +538,7 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
         rc = run_nndescent(ctx, g, MODE_SMERGE, leaf_off[1], 0, lo.as<uint32_t>(), nleaf);
         if (rc) return rc;
     }
-    k_merge2one<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, n); count_launch();
+    k_merge2one<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, n, g.fast ? 1u : 0u); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -433,6 +552,15 @@ int jmerge_build(Ctx& ctx, GraphDev& g, uint64_t* sub_ncmps) {
     absorb(g, s);
     k_rebase<<<blocks_for((size_t)pre * K, 256), 256, 0, ctx.stream>>>(g.pid, (size_t)pre * K, 0, 0); count_launch();
     g.cut = K * 3 / 6;                                    // jmerge.cpp:87
+    if (g.fast) {
+        if ((rc = fast_rows(ctx, g, 0, pre, K - g.cut, n - pre, pre, nullptr, 0, 1, 0))) return rc;
+        if ((rc = fast_rows(ctx, g, pre, n, 0, n, 0, nullptr, 0, 2, pre))) return rc;
+        g.ncmps += (uint64_t)pre * g.cut + (uint64_t)(n - pre) * K;
+        if ((rc = run_nndescent(ctx, g, MODE_JMERGE, pre, 0, nullptr, 0))) return rc;
+        k_merge2one<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, pre, g.fast ? 1u : 0u); count_launch();
+        NNM_CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
     const uint32_t per_old = sds_draws(2 * g.cut, n - pre), per_new = sds_draws(K + 1, n);
     size_t total = (size_t)pre * per_old + (size_t)(n - pre) * per_new;
     std::vector<uint32_t> h(total);
@@ -449,7 +577,7 @@ int jmerge_build(Ctx& ctx, GraphDev& g, uint64_t* sub_ncmps) {
     if ((rc = check_counters(ctx))) return rc;
     g.ncmps += (uint64_t)pre * g.cut + (uint64_t)(n - pre) * K;
     if ((rc = run_nndescent(ctx, g, MODE_JMERGE, pre, 0, nullptr, 0))) return rc;
-    k_merge2one<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, pre); count_launch();
+    k_merge2one<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, pre, g.fast ? 1u : 0u); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -458,7 +586,10 @@ int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer) {
     const uint32_t N0 = 64, K = g.K, row = g.n_cap;  // lynndescent.cpp:23
     int rc;
     // init: 64 rows, random K-NN (lynndescent.cpp:143-187)
-    {
+    if (g.fast) {
+        if ((rc = fast_rows(ctx, g, 0, N0, 0, N0, 0, nullptr, 0, 0, 0))) return rc;
+        g.ncmps += (uint64_t)N0 * K;
+    } else {
         const uint32_t per = sds_draws(K + 1, N0);
         std::vector<uint32_t> h((size_t)N0 * per);
         gen_mt19937(g.seed, h.size(), h.data());
@@ -482,27 +613,34 @@ int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer) {
         const uint32_t bnum = last ? total : smpl;
         const uint32_t sz = g.n, lst = last_id;
         // appdNwSmpl (lynndescent.cpp:354-452): one mt19937(seed), old rows then new rows
-        const uint32_t per_old = sds_draws(2 * half, bnum), per_new = sds_draws(2 * K, sz + bnum);
-        size_t tot = (size_t)sz * per_old + (size_t)bnum * per_new;
-        std::vector<uint32_t> h(tot);
-        gen_mt19937(g.seed, tot, h.data());
-        if ((rc = upload_draws(ctx, g.seed, h, tot))) return rc;
-        if ((rc = reset_counters(ctx))) return rc;
-        g.cut = hsize;
-        CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist, ctx.ws.draws.as<uint32_t>(), per_old,
-                     2 * half, hsize, 0, sz, nullptr, 0, lst, bnum, 1, ctx.ws.counters.as<IterCounters>()};
-        k_cross_sample<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(ca); count_launch();
-        InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>() + (size_t)sz * per_old,
-                    per_new, 2 * K, sz + bnum, sz, sz + bnum, lst, ctx.ws.counters.as<IterCounters>()};
-        k_init_rows<<<blocks_for(bnum, WPB), WPB * 32, 0, ctx.stream>>>(ia); count_launch();
-        NNM_CUDA_TRY(cudaGetLastError());
-        if ((rc = check_counters(ctx))) return rc;
+        if (g.fast) {
+            g.cut = hsize;
+            if ((rc = fast_rows(ctx, g, 0, sz, half, bnum, lst, nullptr, 0, 1, 0))) return rc;
+            if ((rc = fast_rows(ctx, g, sz, sz + bnum, 0, sz + bnum, 0, nullptr, 0, 2, lst))) return rc;
+        }
+        if (!g.fast) {
+            const uint32_t per_old = sds_draws(2 * half, bnum), per_new = sds_draws(2 * K, sz + bnum);
+            size_t tot = (size_t)sz * per_old + (size_t)bnum * per_new;
+            std::vector<uint32_t> h(tot);
+            gen_mt19937(g.seed, tot, h.data());
+            if ((rc = upload_draws(ctx, g.seed, h, tot))) return rc;
+            if ((rc = reset_counters(ctx))) return rc;
+            g.cut = hsize;
+            CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist, ctx.ws.draws.as<uint32_t>(), per_old,
+                         2 * half, hsize, 0, sz, nullptr, 0, lst, bnum, 1, ctx.ws.counters.as<IterCounters>()};
+            k_cross_sample<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(ca); count_launch();
+            InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>() + (size_t)sz * per_old,
+                        per_new, 2 * K, sz + bnum, sz, sz + bnum, lst, ctx.ws.counters.as<IterCounters>()};
+            k_init_rows<<<blocks_for(bnum, WPB), WPB * 32, 0, ctx.stream>>>(ia); count_launch();
+            NNM_CUDA_TRY(cudaGetLastError());
+            if ((rc = check_counters(ctx))) return rc;
+        }
         g.ncmps += (uint64_t)sz * hsize + (uint64_t)bnum * K;
         g.n = sz + bnum;
         last_id = lst + bnum;
         total -= bnum;
         if ((rc = run_nndescent(ctx, g, MODE_LY, lst, 0, nullptr, 0))) return rc;
-        k_merge2one<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, hsize, sz); count_launch();
+        k_merge2one<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, hsize, sz, g.fast ? 1u : 0u); count_launch();
         NNM_CUDA_TRY(cudaGetLastError());
         if (last || (count_level < 10 && level[count_level]))
             if ((rc = on_layer(ctx, g))) return rc;

@@ -29,7 +29,7 @@ bool opts_ok(nnm_ctx* ctx, const nnm_opts* o, int* rc) {
         *rc = fail(ctx, NNM_ERR_UNSUPPORTED_METRIC, "metric must be NNM_METRIC_L2, _L1 or _CHI2");
         return false;
     }
-    if (o->rng_mode != NNM_RNG_EXACT) {
+    if (o->rng_mode != NNM_RNG_EXACT && o->rng_mode != NNM_RNG_FAST) {
         *rc = fail(ctx, NNM_ERR_INVALID, "unknown rng_mode");
         return false;
     }
@@ -52,6 +52,8 @@ void setup_graph(GraphDev& g, const nnm_opts& o, uint64_t n, uint32_t d, uint32_
     g.delta = o.delta;
     g.max_iter = o.max_iter;
     g.exact_trace = o.exact_trace != 0;
+    g.fast = o.rng_mode == NNM_RNG_FAST;
+    g.phase = 0;
 }
 
 void fill_stats(nnm_stats* st, const GraphDev& g, uint64_t sub, float ms) {

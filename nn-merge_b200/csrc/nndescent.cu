@@ -236,6 +236,7 @@ struct ShufArgs {
     uint32_t* npairs;     // pair-distance slots per row
     uint32_t* tier_rows;  // 4 lists of n rows: joined rows binned by list size
     IterCounters* ctr;
+    uint32_t fast, seed, phase;  // fast tier: Philox sample instead of std::random_shuffle
 };
 
 __global__ void k_rand_count(const uint64_t* roff_new, const uint64_t* roff_old, uint32_t n, uint32_t* out) {
@@ -264,7 +265,7 @@ __global__ void k_shuffle_append(ShufArgs a) {
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t t = blockIdx.x * 8 + w;
     if (t >= a.n) return;
-    const int32_t* draws = a.rbuf + a.rofs[t];
+    const int32_t* draws = a.fast ? nullptr : a.rbuf + a.rofs[t];
     uint32_t nl = a.newlen[t], ol = a.oldlen[t];
     for (int l = 0; l < 2; l++) {
         uint64_t lo = l ? a.roff_old[t] : a.roff_new[t];
@@ -273,7 +274,22 @@ __global__ void k_shuffle_append(ShufArgs a) {
         uint32_t keep = min(len, a.smpl);
         uint32_t* sh = stage[w];
         bool staged = len <= SHUF_SMEM;
-        if (staged) {
+        if (a.fast) {
+            // keep a uniform random subset of smplNum entries (partial
+            // Fisher-Yates with Philox draws); order is irrelevant here
+            if (len > a.smpl && lane == 0) {
+                const Philox ph{a.seed, 0x6e6e6d01u};
+                for (uint32_t i = 0; i < keep; i++) {
+                    const uint32_t r = ph(t, a.phase, (uint32_t)l, i).x;
+                    const uint32_t j = i + bounded(r, len - i);
+                    const uint32_t v = seg[i];
+                    seg[i] = seg[j];
+                    seg[j] = v;
+                }
+            }
+            __syncwarp();
+            sh = seg;
+        } else if (staged) {
             for (uint32_t j = lane; j < len; j += 32) sh[j] = seg[j];
             __syncwarp();
             if (lane == 0) shuffle_seg(sh, len, draws);
@@ -873,18 +889,25 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         RevSortArgs ra{{roff_new, roff_old}, {rseg_new, rseg_old}, {rscr_new, rscr_old},
                        {carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr},
                        n, P<uint32_t>(ws.bigrev), ctr};
+        // reverse lists in ascending source order (also in the fast tier: the
+        // atomics fill them in arbitrary order, and the sample must not depend
+        // on it)
         k_rev_sort_small<<<dim3(warp_blocks, 2), 256, 0, st>>>(ra); count_launch();
         k_rev_sort_big<<<nsm * 2, 512, 0, st>>>(ra); count_launch();
-        // std::rand() draws of this iteration's shuffles
-        k_rand_count<<<tblocks, 256, 0, st>>>(roff_new, roff_old, n, P<uint32_t>(ws.rcount)); count_launch();
-        NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.rcount), P<uint64_t>(ws.rofs), n, scan_tmp, d_tot, st));
-        NNM_CUDA_TRY(glibc_stream_generate(P<int32_t>(ws.rbuf), g.gbase, g.gpos, d_tot, rev_cap * 2, st));
+        if (!g.fast) {
+            // std::rand() draws of this iteration's shuffles
+            k_rand_count<<<tblocks, 256, 0, st>>>(roff_new, roff_old, n, P<uint32_t>(ws.rcount)); count_launch();
+            NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.rcount), P<uint64_t>(ws.rofs), n, scan_tmp, d_tot, st));
+            NNM_CUDA_TRY(glibc_stream_generate(P<int32_t>(ws.rbuf), g.gbase, g.gpos, d_tot, rev_cap * 2, st));
+        } else {
+            NNM_CUDA_TRY(cudaMemsetAsync(d_tot, 0, 8, st));
+        }
         ShufArgs sh{roff_new, roff_old, rseg_new, rseg_old, P<uint64_t>(ws.rofs), P<int32_t>(ws.rbuf),
                     g.newL, g.oldL, g.newlen, g.oldlen,
                     g.capn, g.capo, n, g.smpl,
                     track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
                     track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
-                    P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr};
+                    P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, g.phase++};
         k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh); count_launch();
         NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.npairs), P<uint64_t>(ws.poff), n, scan_tmp,
                                     reinterpret_cast<uint64_t*>(&ctr->pairs), st));

@@ -220,3 +220,31 @@ __device__ __forceinline__ uint32_t warp_prefix_count(unsigned mask_bits, int la
 }
 
 }  // namespace nnm
+
+namespace nnm {
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11): a counter-based generator, so every (row, phase,
+// draw) pair gets its own independent value with no shared state.  Used by
+// the fast tier in place of the reference's sequential streams.
+struct Philox {
+    uint32_t k0, k1;
+    __device__ __forceinline__ uint4 operator()(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) const {
+        uint32_t a0 = k0, a1 = k1;
+        uint4 c = make_uint4(c0, c1, c2, c3);
+#pragma unroll
+        for (int r = 0; r < 10; r++) {
+            const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+            const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+            c = make_uint4(hi1 ^ c.y ^ a0, lo1, hi0 ^ c.w ^ a1, lo0);
+            a0 += 0x9E3779B9u;
+            a1 += 0xBB67AE85u;
+        }
+        return c;
+    }
+};
+
+// Uniform integer in [0, m) from a 32-bit draw (multiply-shift).
+__device__ __forceinline__ uint32_t bounded(uint32_t r, uint32_t m) {
+    return (uint32_t)(((unsigned long long)r * m) >> 32);
+}
+}  // namespace nnm

@@ -103,6 +103,11 @@ struct GraphDev {
     float delta = 0.002f;
     uint32_t max_iter = 0;     // 0: iterate until the reference's convergence test passes
     bool exact_trace = false;  // record the reference's float mean every iteration
+    // Fast tier: counter-based random draws (Philox keyed by the seed) in
+    // place of the reference's sequential streams, so the initial graphs and
+    // samples are drawn on the device and reverse lists need no ordering.
+    bool fast = false;
+    uint32_t phase = 0;        // Philox counter of the next sampling phase
     uint64_t ncmps = 0;
     uint32_t iters = 0;
     std::vector<float> trace;

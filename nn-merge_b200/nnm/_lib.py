@@ -79,11 +79,15 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
 
 
-def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exact_trace=False):
+RNG_MODES = {"exact": 0, "fast": 1}
+
+
+def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exact_trace=False, rng="exact"):
     lib = load()
     o = Opts()
     lib.nnm_opts_default(ctypes.byref(o))
     o.seed = seed
+    o.rng_mode = RNG_MODES[rng]
     o.metric = METRICS[metric] if isinstance(metric, str) else int(metric)
     o.sample_cap = sample_cap
     o.delta = delta

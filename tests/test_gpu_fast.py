@@ -1,0 +1,62 @@
+"""The fast tier (counter-based random draws on the device): deterministic
+under a seed, pools well formed (sorted, distinct ids, no self, exact
+distances), and recall@10 against exact brute force."""
+import numpy as np
+import pytest
+
+from nnm.datasets import gaussian_mixture_u8
+
+pytestmark = pytest.mark.gpu
+
+
+def exact_knn(x, k):
+    import torch
+    t = torch.from_numpy(x).cuda()
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        nrm = (t * t).sum(1)
+        d = nrm[:, None] + nrm[None, :] - 2.0 * (t @ t.T)
+        d.fill_diagonal_(float("inf"))
+        return torch.topk(d, k, dim=1, largest=False).values.cpu().numpy()
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+def check_pools(x, g):
+    ids, ds = g["ids"], g["dists"]
+    n, k = ids.shape
+    assert (np.diff(ds, axis=1) >= 0).all()
+    assert (ids < n).all() and (ids != np.arange(n)[:, None]).all()
+    assert all(len(set(r)) == k for r in ids)
+    ref = ((x[:, None, :] - x[ids]) ** 2).sum(-1)
+    assert np.array_equal(ref.astype(np.float32), ds)  # integer data: exact
+
+
+def recall(x, g, k=10):
+    kth = exact_knn(x, k)[:, -1:]
+    return float((g["dists"][:, :k] <= kth).mean())
+
+
+@pytest.mark.parametrize("kind", ["kgraph", "smerge", "jmerge"])
+def test_fast_tier_deterministic_and_well_formed(ctx, kind):
+    x = gaussian_mixture_u8(4000, d=64, seed=9)
+    a = getattr(ctx, kind)(x, 20, seed=3, rng="fast")
+    b = getattr(ctx, kind)(x, 20, seed=3, rng="fast")
+    assert np.array_equal(a["ids"], b["ids"]) and a["ncmps"] == b["ncmps"]
+    check_pools(x, a)
+    assert recall(x, a) >= 0.95
+
+
+def test_fast_tier_merge_of_four_leaves(ctx):
+    x = gaussian_mixture_u8(20000, d=128, n_centres=64, seed=2)
+    g = ctx.merge_leaves(x, 20, [5000] * 4, seed=1, rng="fast")
+    check_pools(x, g)
+    assert recall(x, g) >= 0.95
+
+
+def test_fast_tier_hmerge_layers(ctx):
+    x = gaussian_mixture_u8(5000, d=32, seed=4)
+    g = ctx.hmerge(x, 16, 16, seed=2, rng="fast")
+    check_pools(x, g)
+    assert [len(o) - 1 for o, _ in g["layers"]] == [64, 512, 4096, 5000]
