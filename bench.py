@@ -64,6 +64,9 @@ def parse():
                         "fast: counter-based draws on the device")
     p.add_argument("--delta", type=float, default=None, help="convergence threshold (default: the reference's 0.002)")
     p.add_argument("--smpl", type=int, default=100, help="reverse-sample cap smplNum (reference: 100)")
+    p.add_argument("--join", default="fp32", choices=["auto", "fp32", "tensor"],
+                   help="local-join kernel: FP32 CUDA cores, or u8 Gram matrices on the tensor cores "
+                        "(bit-identical for integer data)")
     return p.parse_args()
 
 
@@ -255,7 +258,7 @@ def main():
     ctx = nnm.Context(local)
     build_seed = a.seed
 
-    bkw = dict(seed=build_seed, rng=a.path, sample_cap=a.smpl,
+    bkw = dict(seed=build_seed, rng=a.path, sample_cap=a.smpl, join=a.join,
                delta=a.delta if a.delta is not None else 0.002)
 
     def build_dev():
@@ -341,7 +344,8 @@ def main():
                                       "plain FP32, reference-exact" if a.path == "exact" else "fast tier"),
                        "n": n, "d": d, "k": k, "leaves": a.leaves,
                        "path": "plain_fp32_exact" if a.path == "exact" else "fast",
-                       "delta": bkw["delta"], "smpl": a.smpl,
+                       "delta": bkw["delta"], "smpl": a.smpl, "join": a.join,
+                       "join_rows": prof["rows"],
                        "recall@10": rec, "iterations": st["iterations"], "ncmps_merge": st["ncmps"],
                        "ncmps_leaves": st["sub_ncmps"],
                        "l2": "inputs (%d MB) larger than L2 (126 MB)" % (x.nbytes >> 20),

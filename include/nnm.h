@@ -49,6 +49,16 @@ typedef enum {
                           random choices, no host-side streams and no ordering of reverse lists */
 } nnm_rng_mode;
 
+/* Kernel of the local join's distance evaluations.  Both give the same
+   graphs bit for bit; the tensor-core join applies when the metric is L2 and
+   every vector component is an integer in [0, 255] (every squared distance
+   then stays below 2^24, where the reference's float sum is exact). */
+typedef enum {
+    NNM_JOIN_AUTO = 0,   /* tensor cores when they apply, else FP32 */
+    NNM_JOIN_FP32 = 1,   /* FP32 CUDA cores: the reference's sequential sums */
+    NNM_JOIN_TENSOR = 2  /* tensor cores (u8 Gram matrices); NNM_ERR_INVALID when they do not apply */
+} nnm_join_kernel;
+
 typedef struct {
     uint32_t seed;        /* clock value the reference's time(NULL) seeding is frozen at */
     uint32_t rng_mode;    /* nnm_rng_mode */
@@ -57,7 +67,8 @@ typedef struct {
     float delta;          /* convergence threshold (abstractgraph.cpp:4): 0.002 */
     uint32_t max_iter;    /* 0: iterate until converged, as the reference */
     uint32_t exact_trace; /* nonzero: record the reference's float mean every iteration */
-    uint32_t reserved[9];
+    uint32_t join_kernel; /* nnm_join_kernel */
+    uint32_t reserved[8];
 } nnm_opts;
 
 typedef struct {

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "nnm_builders.h"
+#include "nnm_join.h"
 #include "nnm_launch.h"
 #include "nnm_scan.h"
 
@@ -396,7 +397,7 @@ int upload_vectors(Ctx& ctx, GraphStore& s, GraphDev& g, const float* x, bool x_
         tmp.release();
     }
     g.x = s.x.as<float>();
-    return 0;
+    return tc_prepare(ctx, s, g);
 }
 
 int export_graph(Ctx& ctx, const GraphDev& g, uint32_t* ids, float* dists, uint8_t* flags, bool host_out) {
@@ -459,6 +460,10 @@ static GraphDev sub_view(const GraphDev& p, uint32_t b, uint32_t e) {
     GraphDev s = p;
     s.n_cap = s.n = e - b;
     s.x = p.x + (size_t)b * p.dp;
+    if (p.xq) {
+        s.xq = p.xq + (size_t)b * p.kq;
+        s.nrm = p.nrm + b;
+    }
     s.pid = p.pid + (size_t)b * p.K;
     s.pdist = p.pdist + (size_t)b * p.K;
     s.cpid = p.cpid + (size_t)b * p.K;

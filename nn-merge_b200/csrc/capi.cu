@@ -37,6 +37,10 @@ bool opts_ok(nnm_ctx* ctx, const nnm_opts* o, int* rc) {
         *rc = fail(ctx, NNM_ERR_INVALID, "sample_cap must be in [1, 4096]");
         return false;
     }
+    if (o->join_kernel > NNM_JOIN_TENSOR) {
+        *rc = fail(ctx, NNM_ERR_INVALID, "unknown join_kernel");
+        return false;
+    }
     return true;
 }
 
@@ -53,6 +57,7 @@ void setup_graph(GraphDev& g, const nnm_opts& o, uint64_t n, uint32_t d, uint32_
     g.max_iter = o.max_iter;
     g.exact_trace = o.exact_trace != 0;
     g.fast = o.rng_mode == NNM_RNG_FAST;
+    g.join_kernel = o.join_kernel;
     g.phase = 0;
 }
 
@@ -274,6 +279,8 @@ int nnm_profile_enable(nnm_ctx* ctx, int on) {
     }
     ctx->c.prof = on != 0;
     ctx->c.kjoin = ctx->c.kemit = ctx->c.kmerge = nnm::KStat();
+    for (auto& r : ctx->c.join_rows) r = 0;
+    ctx->c.join_rows_tc = 0;
     return NNM_OK;
 }
 
@@ -283,10 +290,14 @@ int nnm_profile_get(const nnm_ctx* ctx, char* buf, uint64_t buflen) {
     int w = std::snprintf(buf, buflen,
                           "{\"join\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f, \"flops\": %.1f}, "
                           "\"emit\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}, "
-                          "\"merge\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}}",
+                          "\"merge\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}, "
+                          "\"rows\": {\"tiers\": [%llu, %llu, %llu, %llu, %llu], \"tensor\": %llu}}",
                           (unsigned long long)c.kjoin.launches, c.kjoin.ms, c.kjoin.bytes, c.kjoin.flops,
                           (unsigned long long)c.kemit.launches, c.kemit.ms, c.kemit.bytes,
-                          (unsigned long long)c.kmerge.launches, c.kmerge.ms, c.kmerge.bytes);
+                          (unsigned long long)c.kmerge.launches, c.kmerge.ms, c.kmerge.bytes,
+                          (unsigned long long)c.join_rows[0], (unsigned long long)c.join_rows[1],
+                          (unsigned long long)c.join_rows[2], (unsigned long long)c.join_rows[3],
+                          (unsigned long long)c.join_rows[4], (unsigned long long)c.join_rows_tc);
     return (w < 0 || (uint64_t)w >= buflen) ? NNM_ERR_INVALID : NNM_OK;
 }
 

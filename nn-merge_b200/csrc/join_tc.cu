@@ -1,0 +1,412 @@
+// Local join on the 5th-generation tensor cores (tcgen05, TMEM accumulators).
+//
+// The join evaluates d(a, b) for every pair of a row's sample lists.  For the
+// squared L2 metric d(a, b) = |a|^2 + |b|^2 - 2 a.b, so the distances of a
+// row are its Gram matrix plus norms.  When every vector component is an
+// integer in [0, 255] (checked on upload, k_quantize), the vectors are kept
+// as u8 and the Gram matrix is computed by tcgen05.mma kind::i8 with S32
+// accumulation: every product and sum is an exact integer, every distance is
+// below 2^24, and the reference's sequential float sum (vmath.cpp:56-88) of
+// the same integer terms is exact too -- the two agree bit for bit, so the
+// graphs are identical to the FP32 path's.
+//
+// Tiles.  Rows of list size S <= 16, 32, 64, 128 (tiers 0-3) are packed 8,
+// 4, 2, 1 to a tile of 128 slots; slot s holds list entry s % B of the
+// tile's row s / B (B = 16 << tier).  One MMA chain (M = N = 128, K = 32 per
+// instruction) computes the 128 x 128 slot Gram matrix into 128 TMEM
+// columns; only its diagonal blocks are read.  The epilogue reads TMEM lane
+// b (slot b) with tcgen05.ld; by symmetry column a of that lane is G(a, b),
+// so lane b evaluates the pairs (a, b), a < b, of its row: a thread per
+// "inner" slot, all lanes of a warp on the same "outer" column at a time.
+//
+// Two passes, as the FP32 path: pass 0 counts, per list slot, the proposals
+// that pass the K-th-distance filter (the bucket sizes); pass 1 recomputes
+// the distances and writes the proposals.  Nothing per pair is stored.
+//
+// Synchronisation: persistent CTAs of 128 threads, at most four per SM (the
+// TMEM columns and the shared memory request both allow four), each holding
+// 128 TMEM columns for its lifetime.  Thread 0 issues the MMAs and commits
+// them to an mbarrier.  Every wait on the mbarrier is bounded in time; when
+// the bound runs out the CTA records DERR_TC_WAIT, waits (bounded) once more
+// for its MMA, frees its TMEM and returns.
+#include <algorithm>
+#include <cstdint>
+
+#include "../../include/nnm.h"
+#include "nnm_engine.h"
+#include "nnm_join.h"
+#include "nnm_launch.h"
+
+namespace nnm {
+namespace {
+
+constexpr int TC_THREADS = 128;
+constexpr uint32_t TC_SLOTS = 128;             // M = N = 128: one TMEM lane and one column per slot
+constexpr uint32_t TC_COLS = 128;              // TMEM columns held by a CTA
+constexpr uint32_t TC_SMEM_FLOOR = 50 * 1024;  // keeps residency at <= 4 CTAs per SM (4 x 128 columns)
+constexpr uint32_t TC_MAX_KQ = 1024;
+constexpr uint64_t TC_WAIT_NS = 1000000000ull;  // 1 s
+constexpr uint32_t NO_SLOT = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t now_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Shared-memory matrix descriptor of a K-major operand without swizzle:
+// core matrices of 8 rows x 16 bytes (rows 16 bytes apart); LBO = byte
+// distance between the two 16-byte K chunks of one instruction, SBO = byte
+// distance between 8-row groups; addresses in 16-byte units; version 1 at
+// bit 46 (the sm_100 descriptor format).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3fffu) | ((uint64_t)((lbo >> 4) & 0x3fffu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::i8: D = S32 (bits 4-5 = 2), A = B = u8
+// (bits 7-9 = 0, 10-12 = 0), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t IDESC_U8 = (2u << 4) | ((TC_SLOTS >> 3) << 17) | ((TC_SLOTS >> 4) << 24);
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the given phase of the barrier for at most TC_WAIT_NS.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = now_ns();
+    while (!mbar_try(bar, parity))
+        if (now_ns() - t0 > TC_WAIT_NS) return false;
+    return true;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+
+// 32 lanes x 32 columns of 32-bit TMEM words; the wait is in the same asm
+// statement so that no use of v can be scheduled before it.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr)
+        : "memory");
+}
+
+struct TcShared {
+    uint64_t mbar;
+    uint32_t tmem;
+    uint32_t row[8], nn[8], S[8];
+};
+
+// Shared memory: the slot vectors (128 x kq bytes, canonical K-major
+// layout: 8-slot groups of kq/16 core matrices), then per-slot arrays.
+__host__ __device__ constexpr size_t tc_vec_bytes(uint32_t kq) { return (size_t)TC_SLOTS * kq; }
+__host__ __device__ constexpr size_t tc_smem_bytes(uint32_t kq) {
+    return tc_vec_bytes(kq) + (size_t)TC_SLOTS * (5 * 4 + 8) + 1024;
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ TcShared sh;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t kq = a.kq, nchunk = kq >> 4, gbytes = nchunk * 128;
+    unsigned char* vec = smem;
+    uint32_t* s_ids = reinterpret_cast<uint32_t*>(smem + tc_vec_bytes(kq));
+    float* s_kth = reinterpret_cast<float*>(s_ids + TC_SLOTS);
+    uint32_t* s_nrm = reinterpret_cast<uint32_t*>(s_kth + TC_SLOTS);
+    uint32_t* s_cnt = s_nrm + TC_SLOTS;  // pass 0: counts; pass 1: bucket cursors
+    uint32_t* s_grp = s_cnt + TC_SLOTS;
+    unsigned long long* s_base = reinterpret_cast<unsigned long long*>(s_grp + TC_SLOTS);
+
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sh.mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem)),
+                     "r"(TC_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = sh.tmem;
+    const uint32_t bar = smem_u32(&sh.mbar);
+    const uint32_t vbase = smem_u32(vec);
+
+    uint32_t nt[4];
+    uint32_t total = 0;
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        nt[t] = (a.ctr->ntier[t] + (8u >> t) - 1) >> (3 - t);
+        total += nt[t];
+    }
+    uint32_t phase = 0, cmps = 0;
+    unsigned long long sum_s = 0;
+    bool failed = false;
+
+    for (uint32_t tile = blockIdx.x; tile < total; tile += gridDim.x) {
+        uint32_t t = 0, lt = tile;
+        while (t < 3 && lt >= nt[t]) {
+            lt -= nt[t];
+            t++;
+        }
+        const uint32_t lgB = 4 + t, B = 1u << lgB, RT = 8u >> t;
+        const uint32_t first = lt * RT, nrows = min(RT, a.ctr->ntier[t] - first);
+        if (tid < nrows) {
+            const uint32_t row = a.tier_rows[(size_t)t * a.n + first + tid];
+            const uint32_t nn = a.newlen[row], S = nn + a.oldlen[row];
+            sh.row[tid] = row;
+            sh.nn[tid] = nn;
+            sh.S[tid] = S;
+            sum_s += S;
+        }
+        __syncthreads();
+        // slot metadata, thread = slot
+        {
+            const uint32_t r = tid >> lgB, q = tid & (B - 1);
+            uint32_t e = NO_SLOT;
+            if (r < nrows && q < sh.S[r]) {
+                const uint32_t row = sh.row[r], nn = sh.nn[r];
+                e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
+                const uint32_t id = e & LID_MASK;
+                s_kth[tid] = a.pdist[(size_t)id * a.K + a.K - 1];
+                s_nrm[tid] = a.nrm[id];
+                s_grp[tid] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
+                s_cnt[tid] = 0;
+                if (PASS == 1) {
+                    const uint32_t c = a.cntpos[(size_t)row * a.caps + q];
+                    s_base[tid] = c ? a.boff[id] + atomicAdd(&a.bcur[id], c) : 0ull;
+                }
+            }
+            s_ids[tid] = e;
+        }
+        __syncthreads();
+        // gather: 16-byte chunk c of slot s -> group s/8, core matrix c, row s%8
+        for (uint32_t i = tid; i < TC_SLOTS * nchunk; i += TC_THREADS) {
+            const uint32_t r8 = i & 7, rest = i >> 3, c = rest % nchunk, g = rest / nchunk, s = g * 8 + r8;
+            const uint32_t e = s_ids[s];
+            if (e != NO_SLOT) cp_async16(vbase + g * gbytes + c * 128 + r8 * 16, a.xq + (size_t)(e & LID_MASK) * kq + c * 16);
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // cp.async writes -> tensor core reads
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            for (uint32_t k = 0; k < nchunk / 2; k++) {
+                const uint64_t desc = smem_desc(vbase + k * 256, 128, gbytes);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(desc), "l"(desc), "r"(IDESC_U8), "r"(k), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                         : "memory");
+        }
+        const bool ok_wait = mbar_wait_bounded(bar, phase);
+        if (__syncthreads_or(!ok_wait)) {
+            failed = true;
+            break;
+        }
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+
+        // epilogue: this thread is slot b = tid (TMEM lane tid)
+        const uint32_t e_b = s_ids[tid];
+        const bool valid_b = e_b != NO_SLOT;
+        const uint32_t r_b = tid >> lgB, q_b = tid & (B - 1);
+        const uint32_t nn_b = valid_b ? sh.nn[r_b] : 0u, S_b = valid_b ? sh.S[r_b] : 0u;
+        const uint32_t row_b = valid_b ? sh.row[r_b] : 0u;
+        const float kth_b = s_kth[tid];
+        const uint32_t nrm_b = s_nrm[tid], grp_b = s_grp[tid];
+        const uint32_t blk = tid & ~(B - 1);
+        uint32_t cb = 0;
+        const uint32_t c_first = B >= 32 ? ((warp * 32) & ~(B - 1)) : warp * 32;
+        for (uint32_t c0 = c_first; c0 <= warp * 32; c0 += 32) {
+            uint32_t v[32];
+            tmem_ld32(tmem + ((warp * 32) << 16) + c0, v);
+#pragma unroll
+            for (uint32_t jj = 0; jj < 32; jj++) {
+                const uint32_t av = c0 + jj;
+                const uint32_t q_a = av & (B - 1);
+                const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
+                const uint32_t e_a = s_ids[av];
+                const float dd = (float)((int)(s_nrm[av] + nrm_b) - 2 * (int)v[jj]);
+                uint32_t outer = 0, inner = 0;
+                const bool ok = pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, s_grp[av], grp_b, outer, inner);
+                const float kth_a = s_kth[av];
+                if (PASS == 0) {
+                    cmps += ok;
+                    cb += (ok && dd < kth_b);
+                    const unsigned m = __ballot_sync(0xffffffffu, ok && dd < kth_a);
+                    if (m && lane == 0) atomicAdd(&s_cnt[av], (uint32_t)__popc(m));
+                } else {
+                    const unsigned long long key =
+                        (1ull << 63) | ((unsigned long long)row_b << 32) | ((unsigned long long)(outer * S_b + inner) << 1);
+                    const bool pa = ok && dd < kth_a;
+                    const unsigned m = __ballot_sync(0xffffffffu, pa);
+                    if (m) {
+                        const uint32_t leader = __ffs(m) - 1;
+                        uint32_t base = 0;
+                        if (lane == leader) base = atomicAdd(&s_cnt[av], (uint32_t)__popc(m));
+                        base = __shfl_sync(0xffffffffu, base, leader);
+                        if (pa) {
+                            const unsigned long long slot = s_base[av] + base + __popc(m & ((1u << lane) - 1u));
+                            a.bucket[slot] = Prop{dd, e_b, key | (outer == q_a ? 0ull : 1ull)};
+                        }
+                    }
+                    if (ok && dd < kth_b) {
+                        const unsigned long long slot = s_base[tid] + atomicAdd(&s_cnt[tid], 1u);
+                        a.bucket[slot] = Prop{dd, e_a, key | (outer == q_b ? 0ull : 1ull)};
+                    }
+                }
+            }
+        }
+        if (PASS == 0 && cb) atomicAdd(&s_cnt[tid], cb);
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        if (PASS == 0 && valid_b) {
+            const uint32_t c = s_cnt[tid];
+            a.cntpos[(size_t)row_b * a.caps + q_b] = (uint16_t)c;
+            if (c) atomicAdd(&a.bcnt[e_b & LID_MASK], c);
+        }
+        __syncthreads();
+    }
+
+    if (PASS == 0) {
+        for (int o = 16; o > 0; o >>= 1) {
+            cmps += __shfl_xor_sync(0xffffffffu, cmps, o);
+            sum_s += __shfl_xor_sync(0xffffffffu, sum_s, o);
+        }
+        if (lane == 0 && cmps) atomicAdd(&a.ctr->ncmps, (unsigned long long)cmps);
+        if (lane == 0 && sum_s) {
+            atomicAdd(&a.ctr->sum_s, sum_s);
+            atomicAdd(&a.ctr->sum_s_tc, sum_s);
+        }
+    }
+    if (failed) {
+        if (tid == 0) atomicOr(a.tc_err, (unsigned)DERR_TC_WAIT);
+        mbar_wait_bounded(bar, phase);  // the MMA may still write TMEM
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_COLS));
+    }
+}
+
+// Warp per vector: checks that every component is an integer in [0, 255],
+// writes the u8 copy (zero padded to kq bytes) and the squared norm, and
+// tracks the largest norm.
+__global__ void k_quantize(const float* x, uint32_t n, uint32_t d, uint32_t dp, uint32_t kq, uint8_t* xq,
+                           uint32_t* nrm, unsigned* bad, unsigned* maxnrm) {
+    const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float* src = x + (size_t)row * dp;
+    uint8_t* dst = xq + (size_t)row * kq;
+    uint32_t s = 0;
+    bool ok = true;
+    for (uint32_t k = lane; k < kq; k += 32) {
+        uint32_t u = 0;
+        if (k < d) {
+            const float v = src[k];
+            if (v >= 0.f && v <= 255.f && v == truncf(v)) u = (uint32_t)v;
+            else ok = false;
+        }
+        dst[k] = (uint8_t)u;
+        s += u * u;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const bool all_ok = __all_sync(0xffffffffu, ok);
+    if (lane == 0) {
+        nrm[row] = s;
+        if (!all_ok) atomicOr(bad, 1u);
+        atomicMax(maxnrm, s);
+    }
+}
+
+}  // namespace
+
+int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
+    g.xq = nullptr;
+    g.nrm = nullptr;
+    g.kq = 0;
+    if (g.join_kernel == NNM_JOIN_FP32) return 0;
+    const uint32_t kq = (g.d + 31) & ~31u;
+    const char* why = nullptr;
+    if (g.metric != L2) why = "the tensor-core join needs the L2 metric";
+    else if (kq > TC_MAX_KQ) why = "the tensor-core join takes d <= 1024";
+    if (!why) {
+        NNM_CUDA_TRY(s.xq.ensure((size_t)g.n_cap * kq));
+        NNM_CUDA_TRY(s.nrm.ensure((size_t)g.n_cap * 4));
+        DevBuf& m = ctx.ws.misc;
+        NNM_CUDA_TRY(m.ensure(64));
+        NNM_CUDA_TRY(cudaMemsetAsync(m.p, 0, 16, ctx.stream));
+        unsigned* flags = m.as<unsigned>();
+        k_quantize<<<(g.n_cap + 7) / 8, 256, 0, ctx.stream>>>(g.x, g.n_cap, g.d, g.dp, kq, s.xq.as<uint8_t>(),
+                                                              s.nrm.as<uint32_t>(), flags, flags + 1); count_launch();
+        unsigned h[2] = {0, 0};
+        NNM_CUDA_TRY(cudaMemcpyAsync(h, flags, 8, cudaMemcpyDeviceToHost, ctx.stream));
+        NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+        // every squared distance is at most |a|^2 + |b|^2 for non-negative vectors
+        if (h[0]) why = "the tensor-core join needs integer components in [0, 255]";
+        else if (2ull * h[1] >= (1ull << 24)) why = "the tensor-core join needs squared norms below 2^23";
+    }
+    if (why) {
+        if (g.join_kernel == NNM_JOIN_TENSOR) {
+            ctx.last_error = why;
+            return 1;  // NNM_ERR_INVALID
+        }
+        return 0;
+    }
+    g.xq = s.xq.as<uint8_t>();
+    g.nrm = s.nrm.as<uint32_t>();
+    g.kq = kq;
+    return 0;
+}
+
+cudaError_t tc_set_attributes(uint32_t kq) {
+    const int bytes = (int)std::max<size_t>(tc_smem_bytes(kq), TC_SMEM_FLOOR);
+    cudaError_t e = cudaFuncSetAttribute(k_join_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_join_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, int nsm, cudaStream_t st) {
+    unsigned tiles = 0;
+    for (int t = 0; t < 4; t++) tiles += (ntier[t] + (8u >> t) - 1) >> (3 - t);
+    if (!tiles) return cudaSuccess;
+    const unsigned grid = std::min<unsigned>(tiles, (unsigned)nsm * 4);
+    const size_t bytes = std::max<size_t>(tc_smem_bytes(ja.kq), TC_SMEM_FLOOR);
+    if (pass == 0) k_join_tc<0><<<grid, TC_THREADS, bytes, st>>>(ja);
+    else k_join_tc<1><<<grid, TC_THREADS, bytes, st>>>(ja);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace nnm

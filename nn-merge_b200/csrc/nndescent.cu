@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "nnm_engine.h"
+#include "nnm_join.h"
 #include "nnm_launch.h"
 #include "nnm_scan.h"
 
@@ -40,11 +41,6 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int MERGE_WARPS = 8;
 constexpr int SHUF_SMEM = 512;  // reverse-list entries a shuffling warp stages in shared memory
 constexpr int BIGSORT_CH = 4096;
-// Rows of the local join are binned by list size S = |new| + |old|: three
-// tiers whose vectors are staged in shared memory sized for the tier, and
-// the rest read from global memory (L2).
-constexpr uint32_t TIER_CAP[3] = {32, 64, 128};
-constexpr int TIER_THREADS[4] = {64, 64, 128, 128};
 
 // ---------------------------------------------------------------------------
 // 1. Sampling pass.
@@ -234,9 +230,10 @@ struct ShufArgs {
     uint32_t capn, capo, n, smpl;
     uint32_t *rnewT, *roldT, *rnewTlen, *roldTlen;
     uint32_t* npairs;     // pair-distance slots per row
-    uint32_t* tier_rows;  // 4 lists of n rows: joined rows binned by list size
+    uint32_t* tier_rows;  // NTIER lists of n rows: joined rows binned by list size
     IterCounters* ctr;
     uint32_t fast, seed, phase;  // fast tier: Philox sample instead of std::random_shuffle
+    uint32_t tc_max_s;    // rows with S up to this go to the tensor-core join (no stored pairs)
 };
 
 __global__ void k_rand_count(const uint64_t* roff_new, const uint64_t* roff_old, uint32_t n, uint32_t* out) {
@@ -321,11 +318,11 @@ __global__ void k_shuffle_append(ShufArgs a) {
     if (lane == 0) {
         a.newlen[t] = nl;
         a.oldlen[t] = ol;
-        // pairs of the local join: new x new above the diagonal, new x old
-        a.npairs[t] = nl ? nl * (nl - 1) / 2 + nl * ol : 0u;
+        // stored pairs of the local join: new x new above the diagonal, new x old
+        const uint32_t S = nl + ol;
+        a.npairs[t] = nl && S > a.tc_max_s ? nl * (nl - 1) / 2 + nl * ol : 0u;
         if (nl) {
-            const uint32_t S = nl + ol;
-            const int tier = S <= TIER_CAP[0] ? 0 : S <= TIER_CAP[1] ? 1 : S <= TIER_CAP[2] ? 2 : 3;
+            const int tier = tier_of(S);
             a.tier_rows[(size_t)tier * a.n + atomicAdd(&a.ctr->ntier[tier], 1u)] = t;
         }
     }
@@ -339,62 +336,6 @@ __global__ void k_shuffle_append(ShufArgs a) {
 //     of proposals that pass the K-th-distance filter (for bucket sizes).
 //   k_emit: reads the stored distances and writes the proposals into the
 //     per-target buckets.
-struct JoinArgs {
-    const float* x;
-    uint32_t dp, K, n;
-    const float* pdist;
-    const uint32_t *newL, *oldL, *newlen, *oldlen;
-    uint32_t capn, capo, caps;
-    uint32_t mode, verse;
-    const uint32_t* leaf_off;
-    uint32_t nleaf;
-    const uint32_t* tier_rows;
-    const uint64_t* poff;  // first pair slot of each row
-    float* pd;             // pair distances
-    uint16_t* cntpos;
-    uint32_t *bcnt, *bcur;
-    const uint64_t* boff;
-    Prop* bucket;
-    IterCounters* ctr;
-};
-
-__device__ __forceinline__ uint32_t leaf_of(uint32_t id, const uint32_t* off, uint32_t nleaf) {
-    uint32_t lo = 0, hi = nleaf;  // off[0] = 0 <= id < off[nleaf]
-    while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (id >= off[mid]) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
-// Slot of pair (a, b), a < b, a in the new list: row-major over the upper
-// triangle of new x new, then new x old.
-__device__ __forceinline__ uint32_t pair_slot(uint32_t a, uint32_t b, uint32_t nn, uint32_t no) {
-    return b < nn ? a * nn - a * (a + 1) / 2 + (b - a - 1) : nn * (nn - 1) / 2 + a * no + (b - nn);
-}
-
-// The reference's join filter and visiting order for pair (a, b), a < b:
-// returns false if the pair is skipped, else the outer (first-inserted
-// target) and inner positions.
-__device__ __forceinline__ bool pair_order(uint32_t mode, uint32_t verse, uint32_t av, uint32_t bv, uint32_t nn,
-                                           uint32_t ea, uint32_t eb, uint32_t ga, uint32_t gb, uint32_t& outer,
-                                           uint32_t& inner) {
-    const uint32_t ida = ea & LID_MASK, idb = eb & LID_MASK;
-    if (ida == idb) return false;
-    outer = av;
-    inner = bv;
-    if (mode == MODE_KGRAPH) {
-        if (bv < nn && idb < ida) {  // kgraph.h:112-116 visits it from the smaller id
-            outer = bv;
-            inner = av;
-        }
-        return true;
-    }
-    if (mode == MODE_SMERGE) return ga != gb;
-    return ga != gb || ga == 1 || gb == 1 || verse;
-}
-
 // Vectors of a row's lists in shared memory: row q starts at 16-byte unit
 // q * vstride + q / 4 with vstride = 1 mod 8, so that the rows of 4x4 tiles
 // of neighbouring threads (q = 4t + i for consecutive t) fall in different
@@ -505,17 +446,24 @@ __global__ void __launch_bounds__(TIER_THREADS[TIER]) k_pairs(JoinArgs a, uint32
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t cnt = a.ctr->ntier[TIER];
     const uint32_t* rows = a.tier_rows + (size_t)TIER * a.n;
-    for (uint32_t b = blockIdx.x; b < cnt; b += gridDim.x) pairs_row<M, (TIER < 3)>(a, rows[b], smem, R);
+    for (uint32_t b = blockIdx.x; b < cnt; b += gridDim.x) pairs_row<M, (TIER < NTIER - 1)>(a, rows[b], smem, R);
 }
 
-// One warp per row: proposals from the stored pair distances.
+// One warp per row: proposals from the stored pair distances.  With the
+// tensor-core join active, only the rows of the last tier have stored pairs.
 constexpr int EMIT_WARPS = 4;
 
 __global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t row = blockIdx.x * EMIT_WARPS + w;
-    if (row >= a.n) return;
+    const uint32_t idx = blockIdx.x * EMIT_WARPS + w;
+    uint32_t row = idx;
+    if (a.tc) {
+        if (idx >= a.ctr->ntier[NTIER - 1]) return;
+        row = a.tier_rows[(size_t)(NTIER - 1) * a.n + idx];
+    } else if (row >= a.n) {
+        return;
+    }
     const uint32_t nn = a.newlen[row], no = a.oldlen[row], S = nn + no;
     if (nn == 0) return;
     const uint32_t R = a.caps;
@@ -786,19 +734,26 @@ static cudaError_t prep_pairs(uint32_t caps, uint32_t dp, size_t emit_smem) {
     if ((e = cudaFuncSetAttribute(k_pairs<M, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)pairs_smem(TIER_CAP[2], dp, true))) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_pairs<M, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)pairs_smem(TIER_CAP[3], dp, true))) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_pairs<M, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)pairs_smem(caps, dp, false))) != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)emit_smem);
 }
 
+// FP32 pair kernels: all tiers, or only the last one when the tensor-core
+// join takes the others.
 template <int M>
 static void launch_pairs(const JoinArgs& ja, const unsigned* ntier, uint32_t caps, uint32_t dp, int nsm,
-                         cudaStream_t st) {
-    if (ntier[0]) { k_pairs<M, 0><<<ntier[0], TIER_THREADS[0], pairs_smem(TIER_CAP[0], dp, true), st>>>(ja, TIER_CAP[0]); count_launch(); }
-    if (ntier[1]) { k_pairs<M, 1><<<ntier[1], TIER_THREADS[1], pairs_smem(TIER_CAP[1], dp, true), st>>>(ja, TIER_CAP[1]); count_launch(); }
-    if (ntier[2]) { k_pairs<M, 2><<<ntier[2], TIER_THREADS[2], pairs_smem(TIER_CAP[2], dp, true), st>>>(ja, TIER_CAP[2]); count_launch(); }
-    if (ntier[3]) {
-        unsigned g = std::min<unsigned>(ntier[3], (unsigned)nsm * 4);
-        k_pairs<M, 3><<<g, TIER_THREADS[3], pairs_smem(caps, dp, false), st>>>(ja, caps); count_launch();
+                         bool last_only, cudaStream_t st) {
+    if (!last_only) {
+        if (ntier[0]) { k_pairs<M, 0><<<ntier[0], TIER_THREADS[0], pairs_smem(TIER_CAP[0], dp, true), st>>>(ja, TIER_CAP[0]); count_launch(); }
+        if (ntier[1]) { k_pairs<M, 1><<<ntier[1], TIER_THREADS[1], pairs_smem(TIER_CAP[1], dp, true), st>>>(ja, TIER_CAP[1]); count_launch(); }
+        if (ntier[2]) { k_pairs<M, 2><<<ntier[2], TIER_THREADS[2], pairs_smem(TIER_CAP[2], dp, true), st>>>(ja, TIER_CAP[2]); count_launch(); }
+        if (ntier[3]) { k_pairs<M, 3><<<ntier[3], TIER_THREADS[3], pairs_smem(TIER_CAP[3], dp, true), st>>>(ja, TIER_CAP[3]); count_launch(); }
+    }
+    if (ntier[4]) {
+        unsigned g = std::min<unsigned>(ntier[4], (unsigned)nsm * 4);
+        k_pairs<M, 4><<<g, TIER_THREADS[4], pairs_smem(caps, dp, false), st>>>(ja, caps); count_launch();
     }
 }
 
@@ -856,7 +811,9 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     NNM_CUDA_TRY(ae);
     NNM_CUDA_TRY(ws.npairs.ensure(n1 * 4));
     NNM_CUDA_TRY(ws.poff.ensure(n1 * 8));
-    NNM_CUDA_TRY(ws.tiers.ensure((size_t)n * 4 * 4 + 16));
+    NNM_CUDA_TRY(ws.tiers.ensure((size_t)n * NTIER * 4 + 16));
+    const bool tc = g.xq != nullptr;
+    if (tc) NNM_CUDA_TRY(tc_set_attributes(g.kq));
 
     const unsigned warp_blocks = (unsigned)((n + 7) / 8);
     const unsigned tblocks = (unsigned)((n + 255) / 256);
@@ -907,7 +864,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     g.capn, g.capo, n, g.smpl,
                     track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
                     track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
-                    P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, g.phase++};
+                    P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, g.phase++,
+                    tc ? TC_MAX_S : 0u};
         k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh); count_launch();
         NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.npairs), P<uint64_t>(ws.poff), n, scan_tmp,
                                     reinterpret_cast<uint64_t*>(&ctr->pairs), st));
@@ -919,18 +877,21 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             ctx.last_error = "device capacity check failed (code " + std::to_string(ctx.h_counters->error) + ")";
             return 6;
         }
-        unsigned ntier[4];
-        for (int t = 0; t < 4; t++) ntier[t] = ctx.h_counters->ntier[t];
+        unsigned ntier[NTIER];
+        for (int t = 0; t < NTIER; t++) ntier[t] = ctx.h_counters->ntier[t];
         NNM_CUDA_TRY(ws.pd.ensure(std::max<uint64_t>(ctx.h_counters->pairs, 1) * 4));
-        // local join, pass 1: pair distances and per-target proposal counts
+        // local join, pass 1: per-target proposal counts (and, on the FP32
+        // path, the stored pair distances)
         JoinArgs ja{g.x, g.dp, K, n, g.pdist, g.newL, g.oldL, g.newlen, g.oldlen, g.capn, g.capo, caps,
                     (uint32_t)mode, verse, d_leaf_off, nleaf, P<uint32_t>(ws.tiers), P<uint64_t>(ws.poff),
                     P<float>(ws.pd), P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
-                    P<uint64_t>(ws.boff), P<Prop>(ws.bucket), ctr};
+                    P<uint64_t>(ws.boff), P<Prop>(ws.bucket), ctr,
+                    g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error};
         if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
-        if (g.metric == L2) launch_pairs<L2>(ja, ntier, caps, g.dp, nsm, st);
-        else if (g.metric == L1) launch_pairs<L1>(ja, ntier, caps, g.dp, nsm, st);
-        else launch_pairs<CHI2>(ja, ntier, caps, g.dp, nsm, st);
+        if (tc) NNM_CUDA_TRY(launch_join_tc(0, ja, ntier, nsm, st));
+        if (g.metric == L2) launch_pairs<L2>(ja, ntier, caps, g.dp, nsm, tc, st);
+        else if (g.metric == L1) launch_pairs<L1>(ja, ntier, caps, g.dp, nsm, tc, st);
+        else launch_pairs<CHI2>(ja, ntier, caps, g.dp, nsm, tc, st);
         if (ctx.prof) cudaEventRecord(ctx.ev[1], st);
         NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff), n, scan_tmp,
                                     reinterpret_cast<uint64_t*>(&ctr->proposals), st));
@@ -941,9 +902,14 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             NNM_CUDA_TRY(ws.bucket.ensure((size_t)(nprop * 1.25 + 1024) * sizeof(Prop)));
             ja.bucket = P<Prop>(ws.bucket);
         }
-        // pass 2: proposals from the stored distances
+        // pass 2: proposals, recomputed on the tensor cores or read from the
+        // stored distances
         if (ctx.prof) cudaEventRecord(ctx.ev[2], st);
-        k_emit<<<(n + EMIT_WARPS - 1) / EMIT_WARPS, EMIT_WARPS * 32, emit_smem, st>>>(ja); count_launch();
+        if (tc) NNM_CUDA_TRY(launch_join_tc(1, ja, ntier, nsm, st));
+        const unsigned emit_rows = tc ? ntier[NTIER - 1] : n;
+        if (emit_rows) {
+            k_emit<<<(emit_rows + EMIT_WARPS - 1) / EMIT_WARPS, EMIT_WARPS * 32, emit_smem, st>>>(ja); count_launch();
+        }
         MergeArgs ma{g.pid, g.pdist, n, K, P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff),
                      P<Prop>(ws.bucket), P<uint8_t>(ws.nflag), ctr};
         if (ctx.prof) cudaEventRecord(ctx.ev[3], st);
@@ -963,18 +929,27 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             cudaEventElapsedTime(&t01, ctx.ev[0], ctx.ev[1]);
             cudaEventElapsedTime(&t23, ctx.ev[2], ctx.ev[3]);
             cudaEventElapsedTime(&t34, ctx.ev[3], ctx.ev[4]);
-            // algorithmic traffic of the pair kernel: each joined row gathers
-            // its list vectors, list ids and the K-th distances once, writes
-            // one 2-byte count per list slot and one distance per pair; the
-            // emit kernel reads the pair distances and the row's members and
+            // algorithmic traffic of the count pass: each joined row gathers
+            // its list vectors (FP32, or u8 on the tensor cores, with their
+            // norms), list ids and the K-th distances once and writes one
+            // 2-byte count per list slot; the FP32 path also writes one
+            // distance per pair.  The emit pass gathers the same members
+            // again on the tensor cores (or reads the stored distances) and
             // writes every proposal (16 B).
-            ctx.kjoin.launches += (hc.ntier[0] > 0) + (hc.ntier[1] > 0) + (hc.ntier[2] > 0) + (hc.ntier[3] > 0);
+            for (int t = 0; t < NTIER; t++) ctx.join_rows[t] += hc.ntier[t];
+            if (tc) ctx.join_rows_tc += hc.ntier[0] + hc.ntier[1] + hc.ntier[2] + hc.ntier[3];
+            const double s_tc = (double)hc.sum_s_tc, s_f32 = (double)(hc.sum_s - hc.sum_s_tc);
+            ctx.kjoin.launches += tc ? 1 + (hc.ntier[4] > 0)
+                                     : (hc.ntier[0] > 0) + (hc.ntier[1] > 0) + (hc.ntier[2] > 0) +
+                                           (hc.ntier[3] > 0) + (hc.ntier[4] > 0);
             ctx.kjoin.ms += t01;
-            ctx.kjoin.bytes += (double)hc.sum_s * ((double)g.dp * 4.0 + 4.0 + 4.0 + 2.0) + (double)hc.pairs * 4.0;
+            ctx.kjoin.bytes += s_f32 * ((double)g.dp * 4.0 + 10.0) + s_tc * ((double)g.kq + 14.0) +
+                               (double)hc.pairs * 4.0;
             ctx.kjoin.flops += (double)hc.pairs * (double)g.d * 3.0;
-            ctx.kemit.launches += 1;
+            ctx.kemit.launches += tc ? 1 + (hc.ntier[4] > 0) : 1;
             ctx.kemit.ms += t23;
-            ctx.kemit.bytes += (double)hc.pairs * 4.0 + (double)hc.sum_s * 18.0 + (double)hc.proposals * 16.0;
+            ctx.kemit.bytes += (double)hc.pairs * 4.0 + s_f32 * 18.0 + s_tc * ((double)g.kq + 22.0) +
+                               (double)hc.proposals * 16.0;
             ctx.kmerge.launches += 1;
             ctx.kmerge.ms += t34;
             ctx.kmerge.bytes += (double)n * K * 16.0 + (double)hc.proposals * 16.0 + (double)n * 13.0;

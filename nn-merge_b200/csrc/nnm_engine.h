@@ -52,9 +52,10 @@ struct Workspace {
 // Device storage of a graph under construction (owned buffers).
 struct GraphStore {
     DevBuf pid, pdist, cpid, cpdist, newL, oldL, newlen, oldlen, rnewT, roldT, rnewTlen, roldTlen, x;
+    DevBuf xq, nrm;  // u8 copy of the vectors and their squared norms (tensor-core join)
     void release() {
         DevBuf* all[] = {&pid, &pdist, &cpid, &cpdist, &newL, &oldL, &newlen, &oldlen,
-                         &rnewT, &roldT, &rnewTlen, &roldTlen, &x};
+                         &rnewT, &roldT, &rnewTlen, &roldTlen, &x, &xq, &nrm};
         for (auto* b : all) b->release();
     }
 };
@@ -71,6 +72,8 @@ struct Ctx {
     bool prof = false;
     GraphStore store;  // graph arrays, reused across calls (grow-only)
     KStat kjoin, kemit, kmerge;
+    uint64_t join_rows[5] = {};  // joined rows per list-size tier (while profiling)
+    uint64_t join_rows_tc = 0;   // of which on the tensor cores
     cudaEvent_t ev[8] = {};
     cudaStream_t stream = nullptr;
     Workspace ws;
@@ -87,6 +90,12 @@ struct GraphDev {
     uint32_t n_cap = 0, n = 0, K = 0, d = 0, dp = 0;
     int metric = L2;
     const float* x = nullptr;       // n_cap x dp on the device
+    // Tensor-core join (set by tc_prepare when it applies): n_cap x kq u8
+    // vectors, kq = d rounded up to 32 bytes, zero padded, and squared norms.
+    const uint8_t* xq = nullptr;
+    const uint32_t* nrm = nullptr;
+    uint32_t kq = 0;
+    uint32_t join_kernel = 0;       // nnm_join_kernel
     uint32_t* pid = nullptr;        // pools, n_cap x K
     float* pdist = nullptr;
     uint32_t* cpid = nullptr;       // compensation lists, n_cap x K (cut used)

@@ -38,13 +38,16 @@ struct IterCounters {
     unsigned int pad;
     unsigned long long sum_s;      // sum over joined rows of |new| + |old|
     unsigned long long pairs;      // pair-distance slots of this iteration
-    unsigned int ntier[4];         // rows per pair-kernel tier (by list size)
+    unsigned int ntier[5];         // rows per join tier (by list size)
+    unsigned int pad2;
+    unsigned long long sum_s_tc;   // the part of sum_s joined on the tensor cores
 };
 
 enum DevError : unsigned int {
     DERR_NONE = 0,
     DERR_LIST_CAP = 1,      // a sample list overflowed its row capacity
     DERR_CROSS_SAMPLE = 2,  // a merge found fewer new ids than it needs
+    DERR_TC_WAIT = 4,       // a tensor-core join wait ran out (the kernel gave up)
 };
 
 }  // namespace nnm

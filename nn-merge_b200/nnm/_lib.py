@@ -31,7 +31,8 @@ class NnmError(RuntimeError):
 class Opts(ctypes.Structure):
     _fields_ = [("seed", ctypes.c_uint32), ("rng_mode", ctypes.c_uint32), ("metric", ctypes.c_uint32),
                 ("sample_cap", ctypes.c_uint32), ("delta", ctypes.c_float), ("max_iter", ctypes.c_uint32),
-                ("exact_trace", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 9)]
+                ("exact_trace", ctypes.c_uint32), ("join_kernel", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 8)]
 
 
 class Stats(ctypes.Structure):
@@ -82,7 +83,11 @@ def _ptr(a):
 RNG_MODES = {"exact": 0, "fast": 1}
 
 
-def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exact_trace=False, rng="exact"):
+JOIN_KERNELS = {"auto": 0, "fp32": 1, "tensor": 2}
+
+
+def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exact_trace=False, rng="exact",
+              join="auto"):
     lib = load()
     o = Opts()
     lib.nnm_opts_default(ctypes.byref(o))
@@ -93,6 +98,7 @@ def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exac
     o.delta = delta
     o.max_iter = max_iter
     o.exact_trace = 1 if exact_trace else 0
+    o.join_kernel = JOIN_KERNELS[join]
     return o
 
 
