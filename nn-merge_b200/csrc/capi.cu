@@ -281,24 +281,41 @@ int nnm_profile_enable(nnm_ctx* ctx, int on) {
     ctx->c.kjoin = ctx->c.kemit = ctx->c.kmerge = nnm::KStat();
     for (auto& r : ctx->c.join_rows) r = 0;
     ctx->c.join_rows_tc = 0;
+    ctx->c.iter_log.clear();
     return NNM_OK;
 }
 
 int nnm_profile_get(const nnm_ctx* ctx, char* buf, uint64_t buflen) {
     if (!ctx || !buf || buflen == 0) return NNM_ERR_INVALID;
     const nnm::Ctx& c = ctx->c;
-    int w = std::snprintf(buf, buflen,
-                          "{\"join\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f, \"flops\": %.1f}, "
-                          "\"emit\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}, "
-                          "\"merge\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}, "
-                          "\"rows\": {\"tiers\": [%llu, %llu, %llu, %llu, %llu], \"tensor\": %llu}}",
-                          (unsigned long long)c.kjoin.launches, c.kjoin.ms, c.kjoin.bytes, c.kjoin.flops,
-                          (unsigned long long)c.kemit.launches, c.kemit.ms, c.kemit.bytes,
-                          (unsigned long long)c.kmerge.launches, c.kmerge.ms, c.kmerge.bytes,
-                          (unsigned long long)c.join_rows[0], (unsigned long long)c.join_rows[1],
-                          (unsigned long long)c.join_rows[2], (unsigned long long)c.join_rows[3],
-                          (unsigned long long)c.join_rows[4], (unsigned long long)c.join_rows_tc);
-    return (w < 0 || (uint64_t)w >= buflen) ? NNM_ERR_INVALID : NNM_OK;
+    std::string js;
+    char tmp[512];
+    std::snprintf(tmp, sizeof tmp,
+                  "{\"join\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f, \"flops\": %.1f}, "
+                  "\"emit\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}, "
+                  "\"merge\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}, ",
+                  (unsigned long long)c.kjoin.launches, c.kjoin.ms, c.kjoin.bytes, c.kjoin.flops,
+                  (unsigned long long)c.kemit.launches, c.kemit.ms, c.kemit.bytes,
+                  (unsigned long long)c.kmerge.launches, c.kmerge.ms, c.kmerge.bytes);
+    js += tmp;
+    std::snprintf(tmp, sizeof tmp, "\"rows\": {\"tiers\": [%llu, %llu, %llu, %llu, %llu], \"tensor\": %llu}, \"iters\": [",
+                  (unsigned long long)c.join_rows[0], (unsigned long long)c.join_rows[1],
+                  (unsigned long long)c.join_rows[2], (unsigned long long)c.join_rows[3],
+                  (unsigned long long)c.join_rows[4], (unsigned long long)c.join_rows_tc);
+    js += tmp;
+    for (size_t i = 0; i < c.iter_log.size(); i++) {
+        const auto& L = c.iter_log[i];
+        std::snprintf(tmp, sizeof tmp,
+                      "%s[%u, [%u, %u, %u, %u, %u], %llu, %llu, %llu, %llu, %llu, %.4f, %.4f, %.4f]", i ? ", " : "",
+                      L.n, L.rows[0], L.rows[1], L.rows[2], L.rows[3], L.rows[4], (unsigned long long)L.pairs,
+                      (unsigned long long)L.proposals, (unsigned long long)L.flags, (unsigned long long)L.ncmps,
+                      (unsigned long long)L.sum_s, L.ms_join, L.ms_emit, L.ms_merge);
+        js += tmp;
+    }
+    js += "]}";
+    if (js.size() + 1 > buflen) return NNM_ERR_INVALID;
+    std::memcpy(buf, js.c_str(), js.size() + 1);
+    return NNM_OK;
 }
 
 uint64_t nnm_launch_count(void) { return nnm::launch_counter().load(); }

@@ -116,7 +116,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 struct TcShared {
     uint64_t mbar;
     uint32_t tmem;
-    uint32_t row[8], nn[8], S[8];
+    uint32_t row[8], nn[8], S[8], any[8];
 };
 
 // Shared memory: the slot vectors (128 x kq bytes, canonical K-major
@@ -144,6 +144,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sh.mbar)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if (tid < 8) sh.any[tid] = 0;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem)),
                      "r"(TC_COLS));
@@ -156,11 +157,15 @@ __global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
     const uint32_t bar = smem_u32(&sh.mbar);
     const uint32_t vbase = smem_u32(vec);
 
+    // pass 0 joins every row of tiers 0-3; pass 1 only the rows that pass 0
+    // found to have proposals
+    const uint32_t* rcount = PASS == 0 ? a.ctr->ntier : a.ctr->nemit;
+    const uint32_t* rlist = PASS == 0 ? a.tier_rows : a.emit_rows;
     uint32_t nt[4];
     uint32_t total = 0;
 #pragma unroll
     for (int t = 0; t < 4; t++) {
-        nt[t] = (a.ctr->ntier[t] + (8u >> t) - 1) >> (3 - t);
+        nt[t] = (rcount[t] + (8u >> t) - 1) >> (3 - t);
         total += nt[t];
     }
     uint32_t phase = 0, cmps = 0;
@@ -174,9 +179,9 @@ __global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
             t++;
         }
         const uint32_t lgB = 4 + t, B = 1u << lgB, RT = 8u >> t;
-        const uint32_t first = lt * RT, nrows = min(RT, a.ctr->ntier[t] - first);
+        const uint32_t first = lt * RT, nrows = min(RT, rcount[t] - first);
         if (tid < nrows) {
-            const uint32_t row = a.tier_rows[(size_t)t * a.n + first + tid];
+            const uint32_t row = rlist[(size_t)t * a.n + first + tid];
             const uint32_t nn = a.newlen[row], S = nn + a.oldlen[row];
             sh.row[tid] = row;
             sh.nn[tid] = nn;
@@ -288,10 +293,25 @@ __global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
         if (PASS == 0 && cb) atomicAdd(&s_cnt[tid], cb);
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();
-        if (PASS == 0 && valid_b) {
-            const uint32_t c = s_cnt[tid];
-            a.cntpos[(size_t)row_b * a.caps + q_b] = (uint16_t)c;
-            if (c) atomicAdd(&a.bcnt[e_b & LID_MASK], c);
+        if (PASS == 0) {
+            if (valid_b) {
+                const uint32_t c = s_cnt[tid];
+                a.cntpos[(size_t)row_b * a.caps + q_b] = (uint16_t)c;
+                if (c) {
+                    atomicAdd(&a.bcnt[e_b & LID_MASK], c);
+                    sh.any[r_b] = 1;
+                }
+            }
+            __syncthreads();
+            if (warp == 0) {  // rows with proposals go to the emit pass's list
+                const bool has = lane < nrows && sh.any[lane];
+                const unsigned m = __ballot_sync(0xffffffffu, has);
+                uint32_t base = 0;
+                if (m && lane == 0) base = atomicAdd(&a.ctr->nemit[t], (uint32_t)__popc(m));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (has) a.emit_rows[(size_t)t * a.n + base + __popc(m & ((1u << lane) - 1u))] = sh.row[lane];
+                if (lane < 8) sh.any[lane] = 0;
+            }
         }
         __syncthreads();
     }

@@ -473,6 +473,7 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
     float* s_kth = reinterpret_cast<float*>(s_ids + R);
     uint32_t* s_cur = reinterpret_cast<uint32_t*>(s_kth + R);
     uint32_t* s_grp = s_cur + R;
+    bool any_c = false;
     for (uint32_t q = lane; q < S; q += 32) {
         uint32_t e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
         uint32_t id = e & LID_MASK;
@@ -482,7 +483,9 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
         s_grp[q] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
         uint32_t c = a.cntpos[(size_t)row * a.caps + q];
         if (c) s_base[q] = a.boff[id] + atomicAdd(&a.bcur[id], c);
+        any_c |= c != 0;
     }
+    if (!__any_sync(FULL, any_c)) return;  // no pair of this row passed the filter
     __syncwarp();
     const float* pd = a.pd + a.poff[row];
     for (uint32_t av = 0; av < nn; av++) {
@@ -813,7 +816,10 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     NNM_CUDA_TRY(ws.poff.ensure(n1 * 8));
     NNM_CUDA_TRY(ws.tiers.ensure((size_t)n * NTIER * 4 + 16));
     const bool tc = g.xq != nullptr;
-    if (tc) NNM_CUDA_TRY(tc_set_attributes(g.kq));
+    if (tc) {
+        NNM_CUDA_TRY(tc_set_attributes(g.kq));
+        NNM_CUDA_TRY(ws.erows.ensure((size_t)n * 4 * 4 + 16));
+    }
 
     const unsigned warp_blocks = (unsigned)((n + 7) / 8);
     const unsigned tblocks = (unsigned)((n + 255) / 256);
@@ -886,7 +892,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     (uint32_t)mode, verse, d_leaf_off, nleaf, P<uint32_t>(ws.tiers), P<uint64_t>(ws.poff),
                     P<float>(ws.pd), P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
                     P<uint64_t>(ws.boff), P<Prop>(ws.bucket), ctr,
-                    g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error};
+                    g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error, tc ? P<uint32_t>(ws.erows) : nullptr};
         if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
         if (tc) NNM_CUDA_TRY(launch_join_tc(0, ja, ntier, nsm, st));
         if (g.metric == L2) launch_pairs<L2>(ja, ntier, caps, g.dp, nsm, tc, st);
@@ -937,6 +943,11 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             // again on the tensor cores (or reads the stored distances) and
             // writes every proposal (16 B).
             for (int t = 0; t < NTIER; t++) ctx.join_rows[t] += hc.ntier[t];
+            if (ctx.iter_log.size() < 4096) {
+                Ctx::IterLog L{n, {hc.ntier[0], hc.ntier[1], hc.ntier[2], hc.ntier[3], hc.ntier[4]},
+                               hc.pairs, hc.proposals, hc.flags, hc.ncmps, hc.sum_s, t01, t23, t34};
+                ctx.iter_log.push_back(L);
+            }
             if (tc) ctx.join_rows_tc += hc.ntier[0] + hc.ntier[1] + hc.ntier[2] + hc.ntier[3];
             const double s_tc = (double)hc.sum_s_tc, s_f32 = (double)(hc.sum_s - hc.sum_s_tc);
             ctx.kjoin.launches += tc ? 1 + (hc.ntier[4] > 0)

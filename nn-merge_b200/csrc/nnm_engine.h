@@ -39,11 +39,11 @@ struct DevBuf {
 struct Workspace {
     DevBuf rcnt, rcur, rtot, roff, rseg, rscr, rcount, rofs, rbuf;
     DevBuf cntpos, bcnt, bcur, boff, bucket, bigrev, nflag, scan_tmp;
-    DevBuf npairs, poff, pd, tiers;
+    DevBuf npairs, poff, pd, tiers, erows;
     DevBuf draws, counters, misc;
     void release_all() {
         DevBuf* all[] = {&rcnt, &rcur, &rtot, &roff, &rseg, &rscr, &rcount, &rofs, &rbuf, &cntpos, &bcnt, &bcur,
-                         &boff, &bucket, &bigrev, &nflag, &scan_tmp, &npairs, &poff, &pd, &tiers, &draws,
+                         &boff, &bucket, &bigrev, &nflag, &scan_tmp, &npairs, &poff, &pd, &tiers, &erows, &draws,
                          &counters, &misc};
         for (auto* b : all) b->release();
     }
@@ -74,6 +74,13 @@ struct Ctx {
     KStat kjoin, kemit, kmerge;
     uint64_t join_rows[5] = {};  // joined rows per list-size tier (while profiling)
     uint64_t join_rows_tc = 0;   // of which on the tensor cores
+    // per-iteration record while profiling (the most recent iterations)
+    struct IterLog {
+        uint32_t n, rows[5];
+        uint64_t pairs, proposals, flags, ncmps, sum_s;
+        float ms_join, ms_emit, ms_merge;
+    };
+    std::vector<IterLog> iter_log;
     cudaEvent_t ev[8] = {};
     cudaStream_t stream = nullptr;
     Workspace ws;

@@ -43,6 +43,7 @@ struct JoinArgs {
     const uint32_t* nrm;
     uint32_t kq, tc;
     unsigned* tc_err;
+    uint32_t* emit_rows;  // 4 lists of n rows: rows of tiers 0-3 that have proposals
 };
 
 __device__ __forceinline__ uint32_t leaf_of(uint32_t id, const uint32_t* off, uint32_t nleaf) {

@@ -41,6 +41,7 @@ struct IterCounters {
     unsigned int ntier[5];         // rows per join tier (by list size)
     unsigned int pad2;
     unsigned long long sum_s_tc;   // the part of sum_s joined on the tensor cores
+    unsigned int nemit[4];         // rows of tiers 0-3 with at least one proposal (tensor-core emit pass)
 };
 
 enum DevError : unsigned int {

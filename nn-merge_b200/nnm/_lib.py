@@ -151,8 +151,8 @@ class Context:
 
     def profile_stats(self):
         import json
-        buf = ctypes.create_string_buffer(4096)
-        self._check(self.lib.nnm_profile_get(self.h, buf, 4096))
+        buf = ctypes.create_string_buffer(1 << 20)
+        self._check(self.lib.nnm_profile_get(self.h, buf, 1 << 20))
         return json.loads(buf.value.decode())
 
     def launch_count(self):
