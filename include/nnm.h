@@ -59,6 +59,16 @@ typedef enum {
     NNM_JOIN_TENSOR = 2  /* tensor cores (u8 Gram matrices); NNM_ERR_INVALID when they do not apply */
 } nnm_join_kernel;
 
+/* Initial graphs.  NNM_INIT_LEARNED (no counterpart in the reference) needs
+   NNM_RNG_FAST and a model set with nnm_set_init_model: every row's initial
+   pool is the k nearest among the rows next to it in several orderings of
+   the model's 32-bit codes, and the cross-leaf samples of a merge are the
+   nearest rows of the other leaves in those orderings. */
+typedef enum {
+    NNM_INIT_RANDOM = 0, /* the reference's random graphs (getRndSds) */
+    NNM_INIT_LEARNED = 1 /* candidates bucketed by the learned codes */
+} nnm_init_mode;
+
 typedef struct {
     uint32_t seed;        /* clock value the reference's time(NULL) seeding is frozen at */
     uint32_t rng_mode;    /* nnm_rng_mode */
@@ -68,7 +78,8 @@ typedef struct {
     uint32_t max_iter;    /* 0: iterate until converged, as the reference */
     uint32_t exact_trace; /* nonzero: record the reference's float mean every iteration */
     uint32_t join_kernel; /* nnm_join_kernel */
-    uint32_t reserved[8];
+    uint32_t init;        /* nnm_init_mode */
+    uint32_t reserved[7];
 } nnm_opts;
 
 typedef struct {
@@ -182,6 +193,48 @@ typedef struct {
 int nnm_search_noalloc(const float *x_dev, uint64_t n, uint32_t d, const nnm_dev_layers *layers,
                        const float *q_dev, uint64_t nq, uint32_t topk, uint32_t seed, uint32_t metric,
                        uint32_t *out_ids_dev, float *out_dists_dev, uint64_t *ncmps, void *stream);
+
+/* Learned initialisation (no counterpart in the reference).  A 2-layer MLP
+ *   u = x * in_scale + in_shift,  h = relu(W1 u + b1),  z = W2 h + b2,
+ * d_in = d (<= 256) -> 256 -> 32, evaluated with BF16-rounded weights and
+ * FP32 accumulation; a row's code is the sign bits of z (bit o = z_o > 0).
+ * Weights are row-major: w1 is 256 x d_in, w2 is 32 x 256.  Training
+ * minimises the triplet loss mean(max(0, margin + |t_a - t_p|^2 -
+ * |t_a - t_n|^2)), t = tanh(z), over anchors a, graph neighbours p and
+ * random rows n, with Adam on FP32 master weights. */
+#define NNM_MLP_HIDDEN 256
+#define NNM_MLP_OUT 32
+typedef struct {
+    uint32_t d_in;
+    float in_scale, in_shift;
+    float *w1, *b1, *w2, *b2; /* caller-owned host arrays */
+} nnm_mlp;
+
+typedef struct {
+    uint32_t steps;   /* optimiser steps: 400 */
+    uint32_t batch;   /* triplets per step: 2048 */
+    float lr;         /* Adam step size: 2e-3 */
+    float margin;     /* 16 */
+    uint32_t seed;
+    uint32_t reserved[7];
+} nnm_train_opts;
+
+void nnm_train_opts_default(nnm_train_opts *o);
+/* Trains `model` in place (its arrays hold the initial weights) on triplets
+ * drawn from the k-NN graph `graph` (n x k ids) of x (n x d).  loss_trace:
+ * `steps` floats or NULL. */
+int nnm_mlp_train(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, const uint32_t *graph, uint32_t k,
+                  const nnm_train_opts *opts, nnm_mlp *model, float *loss_trace);
+/* Loss and gradients (w.r.t. the BF16-rounded weights) of the triplet loss
+ * over the given triplets (ntrip x 3 row indices of x: anchor, positive,
+ * negative); grad has the model's shapes. */
+int nnm_mlp_grad(nnm_ctx *ctx, const nnm_mlp *model, const float *x, uint64_t n, uint32_t d,
+                 const uint32_t *triplets, uint32_t ntrip, float margin, float *loss, nnm_mlp *grad);
+/* Codes (n) and, when z is not NULL, the outputs (n x 32) of x. */
+int nnm_mlp_codes(nnm_ctx *ctx, const nnm_mlp *model, const float *x, uint64_t n, uint32_t d,
+                  uint32_t *codes, float *z);
+/* The model NNM_INIT_LEARNED builds use (copied to the device); NULL clears it. */
+int nnm_set_init_model(nnm_ctx *ctx, const nnm_mlp *model);
 
 /* Profiling (no counterpart in the reference, which times whole builds with
  * boost::timer): while enabled, the engine records CUDA events around its

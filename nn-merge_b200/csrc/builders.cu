@@ -18,6 +18,7 @@
 
 #include "nnm_builders.h"
 #include "nnm_join.h"
+#include "nnm_learned.h"
 #include "nnm_launch.h"
 #include "nnm_scan.h"
 
@@ -342,7 +343,11 @@ __global__ void k_pad_copy(const float* src, float* dst, uint64_t n, uint32_t d,
     dst[t] = c < d ? src[r * d + c] : 0.f;
 }
 
+}  // namespace
+
 unsigned blocks_for(size_t n, unsigned per) { return (unsigned)((n + per - 1) / per); }
+
+namespace {
 
 // Host-generated mt19937 stream for `rows` rows of `per_row` draws each.
 int upload_draws(Ctx& ctx, uint32_t seed_or_state_unused, std::vector<uint32_t>& host, size_t count) {
@@ -356,6 +361,8 @@ int upload_draws(Ctx& ctx, uint32_t seed_or_state_unused, std::vector<uint32_t>&
 // Draws consumed by one getRndSds(k, N) call.
 inline uint32_t sds_draws(uint32_t k, uint32_t N) { return N == k ? 0u : k + 1u; }
 
+}  // namespace
+
 int check_counters(Ctx& ctx) {
     IterCounters* ctr = ctx.ws.counters.as<IterCounters>();
     NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, ctx.stream));
@@ -368,6 +375,8 @@ int check_counters(Ctx& ctx) {
     }
     return 0;
 }
+
+namespace {
 
 int reset_counters(Ctx& ctx) {
     NNM_CUDA_TRY(ctx.ws.counters.ensure(sizeof(IterCounters) + 64));
@@ -397,6 +406,16 @@ int upload_vectors(Ctx& ctx, GraphStore& s, GraphDev& g, const float* x, bool x_
         tmp.release();
     }
     g.x = s.x.as<float>();
+    if (g.init == NNM_INIT_LEARNED) {
+        if (!ctx.init_model || ctx.init_model->d != g.d) {
+            ctx.last_error = "NNM_INIT_LEARNED needs a model for this dimension (nnm_set_init_model)";
+            return 1;
+        }
+        NNM_CUDA_TRY(s.codes.ensure((size_t)g.n_cap * 4));
+        int rc = mlp_codes_dev(ctx, *ctx.init_model, g.x, g.n_cap, g.dp, s.codes.as<uint32_t>(), nullptr);
+        if (rc) return rc;
+        g.codes = s.codes.as<uint32_t>();
+    }
     return tc_prepare(ctx, s, g);
 }
 
@@ -435,7 +454,18 @@ static int fast_rows(Ctx& ctx, GraphDev& g, uint32_t row0, uint32_t row1, uint32
 int kgraph_build(Ctx& ctx, GraphDev& g) {
     const uint32_t K = g.K, n = g.n;
     if (g.fast) {
-        int rc = fast_rows(ctx, g, 0, n, 0, n, 0, nullptr, 0, 0, 0);
+        int rc;
+        if (g.init == NNM_INIT_LEARNED) {
+            if (g.views) {
+                rc = learned_rows(ctx, g, *g.views, g.view_leaf);
+            } else {
+                CodeViews vw;
+                rc = views_build(ctx, g, {0u, n}, vw);
+                if (!rc) rc = learned_rows(ctx, g, vw, 0);
+            }
+        } else {
+            rc = fast_rows(ctx, g, 0, n, 0, n, 0, nullptr, 0, 0, 0);
+        }
         if (rc) return rc;
         g.ncmps += (uint64_t)n * K;
         return run_nndescent(ctx, g, MODE_KGRAPH, 0, 0, nullptr, 0);
@@ -460,6 +490,8 @@ static GraphDev sub_view(const GraphDev& p, uint32_t b, uint32_t e) {
     GraphDev s = p;
     s.n_cap = s.n = e - b;
     s.x = p.x + (size_t)b * p.dp;
+    if (p.codes) s.codes = p.codes + b;
+    s.views = nullptr;
     if (p.xq) {
         s.xq = p.xq + (size_t)b * p.kq;
         s.nrm = p.nrm + b;
@@ -485,9 +517,16 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
     const uint32_t K = g.K, n = g.n, nleaf = (uint32_t)leaf_off.size() - 1;
     int rc;
     uint64_t subc = 0;
+    CodeViews vw;
+    const bool learned = g.fast && g.init == NNM_INIT_LEARNED;
+    if (learned && (rc = views_build(ctx, g, leaf_off, vw))) return rc;
     // 1. NN-Descent on every leaf, in place (smerge.cpp:56-68).
     for (uint32_t l = 0; l < nleaf; l++) {
         GraphDev s = sub_view(g, leaf_off[l], leaf_off[l + 1]);
+        if (learned) {
+            s.views = &vw;
+            s.view_leaf = l;
+        }
         if ((rc = kgraph_build(ctx, s))) return rc;
         subc += s.ncmps;
         absorb(g, s);
@@ -501,7 +540,9 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
         DevBuf& lo = ctx.ws.misc;
         NNM_CUDA_TRY(lo.ensure(leaf_off.size() * 4 + 64));
         NNM_CUDA_TRY(cudaMemcpyAsync(lo.p, leaf_off.data(), leaf_off.size() * 4, cudaMemcpyHostToDevice, ctx.stream));
-        if ((rc = fast_rows(ctx, g, 0, n, K - g.cut, 0, 0, lo.as<uint32_t>(), nleaf, 0, 0))) return rc;
+        rc = learned ? learned_cross(ctx, g, vw, lo.as<uint32_t>())
+                     : fast_rows(ctx, g, 0, n, K - g.cut, 0, 0, lo.as<uint32_t>(), nleaf, 0, 0);
+        if (rc) return rc;
         g.ncmps += (uint64_t)n * g.cut;
         if ((rc = run_nndescent(ctx, g, MODE_SMERGE, leaf_off[1], 0, lo.as<uint32_t>(), nleaf))) return rc;
         k_merge2one<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, n, g.fast ? 1u : 0u); count_launch();

@@ -8,6 +8,7 @@
 #include "nnm_builders.h"
 #include "nnm_hier.h"
 #include "nnm_launch.h"
+#include "nnm_learned.h"
 
 struct nnm_ctx {
     nnm::Ctx c;
@@ -41,6 +42,14 @@ bool opts_ok(nnm_ctx* ctx, const nnm_opts* o, int* rc) {
         *rc = fail(ctx, NNM_ERR_INVALID, "unknown join_kernel");
         return false;
     }
+    if (o->init > NNM_INIT_LEARNED) {
+        *rc = fail(ctx, NNM_ERR_INVALID, "unknown init");
+        return false;
+    }
+    if (o->init == NNM_INIT_LEARNED && o->rng_mode != NNM_RNG_FAST) {
+        *rc = fail(ctx, NNM_ERR_INVALID, "NNM_INIT_LEARNED needs rng_mode NNM_RNG_FAST");
+        return false;
+    }
     return true;
 }
 
@@ -58,6 +67,7 @@ void setup_graph(GraphDev& g, const nnm_opts& o, uint64_t n, uint32_t d, uint32_
     g.exact_trace = o.exact_trace != 0;
     g.fast = o.rng_mode == NNM_RNG_FAST;
     g.join_kernel = o.join_kernel;
+    g.init = o.init;
     g.phase = 0;
 }
 
@@ -144,6 +154,27 @@ int build_common(nnm_ctx* ctx, Kind kind, const float* x, bool dev, uint64_t n, 
     return rc;
 }
 
+bool mlp_ok(nnm_ctx* ctx, const nnm_mlp* m, uint32_t d) {
+    if (!m || !m->w1 || !m->b1 || !m->w2 || !m->b2) {
+        fail(ctx, NNM_ERR_INVALID, "model arrays must be non-null");
+        return false;
+    }
+    if (m->d_in != d || d == 0 || d > nnm::MLP_MAX_D) {
+        fail(ctx, NNM_ERR_INVALID, "model d_in must equal d and be in [1, 256]");
+        return false;
+    }
+    return true;
+}
+
+// Vectors to the device (zero-padded rows) without any join preparation.
+int upload_plain(Ctx& c, GraphStore& st, GraphDev& g, const float* x, uint64_t n, uint32_t d) {
+    g.n_cap = g.n = (uint32_t)n;
+    g.d = d;
+    g.join_kernel = NNM_JOIN_FP32;
+    g.init = NNM_INIT_RANDOM;
+    return nnm::upload_vectors(c, st, g, x, false);
+}
+
 }  // namespace
 
 extern "C" {
@@ -197,6 +228,10 @@ int nnm_ctx_destroy(nnm_ctx* ctx) {
         if (e) cudaEventDestroy(e);
     ctx->c.ws.release_all();
     ctx->c.store.release();
+    if (ctx->c.init_model) {
+        ctx->c.init_model->release();
+        delete ctx->c.init_model;
+    }
     if (ctx->c.h_counters) cudaFreeHost(ctx->c.h_counters);
     if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
     delete ctx;
@@ -319,6 +354,98 @@ int nnm_profile_get(const nnm_ctx* ctx, char* buf, uint64_t buflen) {
 }
 
 uint64_t nnm_launch_count(void) { return nnm::launch_counter().load(); }
+
+void nnm_train_opts_default(nnm_train_opts* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->steps = 400;
+    o->batch = 2048;
+    o->lr = 2e-3f;
+    o->margin = 16.f;
+    o->seed = 0;
+}
+
+int nnm_set_init_model(nnm_ctx* ctx, const nnm_mlp* model) {
+    if (!ctx) return NNM_ERR_INVALID;
+    Ctx& c = ctx->c;
+    if (!model) {
+        if (c.init_model) {
+            c.init_model->release();
+            delete c.init_model;
+            c.init_model = nullptr;
+        }
+        return NNM_OK;
+    }
+    if (!mlp_ok(ctx, model, model->d_in)) return NNM_ERR_INVALID;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    if (!c.init_model) c.init_model = new nnm::DevMlp();
+    return nnm::mlp_upload(c, *c.init_model, *model);
+}
+
+int nnm_mlp_codes(nnm_ctx* ctx, const nnm_mlp* model, const float* x, uint64_t n, uint32_t d, uint32_t* codes,
+                  float* z) {
+    if (!ctx || !x || !codes || n == 0 || n >= (1ull << 30)) return NNM_ERR_INVALID;
+    if (!mlp_ok(ctx, model, d)) return NNM_ERR_INVALID;
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    nnm::DevMlp m;
+    GraphStore st;
+    GraphDev g;
+    int rc = nnm::mlp_upload(c, m, *model);
+    if (!rc) rc = upload_plain(c, st, g, x, n, d);
+    nnm::DevBuf dc, dz;
+    if (!rc && (dc.ensure(n * 4) != cudaSuccess || (z && dz.ensure(n * 32 * 4) != cudaSuccess)))
+        rc = fail(ctx, NNM_ERR_OOM, "device allocation failed");
+    if (!rc) rc = nnm::mlp_codes_dev(c, m, g.x, (uint32_t)n, g.dp, dc.as<uint32_t>(), z ? dz.as<float>() : nullptr);
+    // the engine's stream is non-blocking: wait for it before the plain copies
+    if (!rc && cudaStreamSynchronize(c.stream) != cudaSuccess) rc = fail(ctx, NNM_ERR_CUDA, "kernel failed");
+    if (!rc && cudaMemcpy(codes, dc.p, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) rc = NNM_ERR_CUDA;
+    if (!rc && z && cudaMemcpy(z, dz.p, n * 32 * 4, cudaMemcpyDeviceToHost) != cudaSuccess) rc = NNM_ERR_CUDA;
+    m.release();
+    dc.release();
+    dz.release();
+    st.release();
+    return rc;
+}
+
+int nnm_mlp_grad(nnm_ctx* ctx, const nnm_mlp* model, const float* x, uint64_t n, uint32_t d,
+                 const uint32_t* triplets, uint32_t ntrip, float margin, float* loss, nnm_mlp* grad) {
+    if (!ctx || !x || !triplets || !loss || !grad || ntrip == 0 || n == 0 || n >= (1ull << 30)) return NNM_ERR_INVALID;
+    if (!mlp_ok(ctx, model, d) || !mlp_ok(ctx, grad, d)) return NNM_ERR_INVALID;
+    for (uint64_t i = 0; i < 3ull * ntrip; i++)
+        if (triplets[i] >= n) return fail(ctx, NNM_ERR_INVALID, "triplet index out of range");
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    GraphStore st;
+    GraphDev g;
+    int rc = upload_plain(c, st, g, x, n, d);
+    if (!rc) rc = nnm::mlp_grad(c, *model, g.x, (uint32_t)n, g.dp, triplets, ntrip, margin, loss, *grad);
+    st.release();
+    return rc;
+}
+
+int nnm_mlp_train(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, const uint32_t* graph, uint32_t k,
+                  const nnm_train_opts* opts, nnm_mlp* model, float* loss_trace) {
+    if (!ctx || !x || !graph || n < 2 || n >= (1ull << 30) || k == 0) return NNM_ERR_INVALID;
+    if (!mlp_ok(ctx, model, d)) return NNM_ERR_INVALID;
+    nnm_train_opts o;
+    if (opts) o = *opts;
+    else nnm_train_opts_default(&o);
+    if (o.steps == 0 || o.batch == 0 || o.batch > (1u << 20)) return fail(ctx, NNM_ERR_INVALID, "bad steps/batch");
+    for (uint64_t i = 0; i < n * k; i++)
+        if (graph[i] >= n) return fail(ctx, NNM_ERR_INVALID, "graph id out of range");
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    GraphStore st;
+    GraphDev g;
+    nnm::DevBuf gd;
+    int rc = upload_plain(c, st, g, x, n, d);
+    if (!rc && gd.ensure(n * k * 4) != cudaSuccess) rc = fail(ctx, NNM_ERR_OOM, "device allocation failed");
+    if (!rc && cudaMemcpy(gd.p, graph, n * k * 4, cudaMemcpyHostToDevice) != cudaSuccess) rc = NNM_ERR_CUDA;
+    if (!rc) rc = nnm::mlp_train(c, g.x, (uint32_t)n, g.dp, gd.as<uint32_t>(), k, o, *model, loss_trace);
+    gd.release();
+    st.release();
+    return rc;
+}
 
 void nnm_layers_free(nnm_layers* layers) {
     if (!layers) return;

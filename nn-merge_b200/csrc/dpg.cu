@@ -390,6 +390,7 @@ int dpg_layer(Ctx& ctx, DpgState& s, GraphDev& g, nnm_layers* out) {
     s.rows = N;
     if (out && out->nlayers < 16) {
         std::vector<uint32_t> len(N), ids((size_t)N * C);
+        NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));  // the plain copies below do not order with it
         NNM_CUDA_TRY(cudaMemcpy(len.data(), s.glen.p, (size_t)N * 4, cudaMemcpyDeviceToHost));
         NNM_CUDA_TRY(cudaMemcpy(ids.data(), s.gid.p, (size_t)N * C * 4, cudaMemcpyDeviceToHost));
         uint32_t L = out->nlayers;

@@ -17,6 +17,10 @@ int upload_vectors(Ctx& ctx, GraphStore& store, GraphDev& g, const float* x, boo
 // Writes ids / distances / flags of rows [0, g.n); host or device outputs.
 int export_graph(Ctx& ctx, const GraphDev& g, uint32_t* ids, float* dists, uint8_t* flags, bool host_out);
 
+unsigned blocks_for(size_t n, unsigned per);
+// Reads the device counters; a set error flag becomes status 6 with a message.
+int check_counters(Ctx& ctx);
+
 int kgraph_build(Ctx& ctx, GraphDev& g);
 // Builds one graph per leaf [leaf_off[l], leaf_off[l+1]) and merges them;
 // with two leaves split at n*5/10 this is Smerge::buildKGraph.

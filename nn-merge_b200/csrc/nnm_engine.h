@@ -53,9 +53,11 @@ struct Workspace {
 struct GraphStore {
     DevBuf pid, pdist, cpid, cpdist, newL, oldL, newlen, oldlen, rnewT, roldT, rnewTlen, roldTlen, x;
     DevBuf xq, nrm;  // u8 copy of the vectors and their squared norms (tensor-core join)
+    DevBuf codes, vkeys, vpos, voff;  // learned codes and their sorted views
     void release() {
         DevBuf* all[] = {&pid, &pdist, &cpid, &cpdist, &newL, &oldL, &newlen, &oldlen,
-                         &rnewT, &roldT, &rnewTlen, &roldTlen, &x, &xq, &nrm};
+                         &rnewT, &roldT, &rnewTlen, &roldTlen, &x, &xq, &nrm,
+                         &codes, &vkeys, &vpos, &voff};
         for (auto* b : all) b->release();
     }
 };
@@ -67,8 +69,12 @@ struct KStat {
     double ms = 0.0, bytes = 0.0, flops = 0.0;
 };
 
+struct DevMlp;
+struct CodeViews;
+
 struct Ctx {
     int device = 0;
+    DevMlp* init_model = nullptr;  // learned-initialisation model (owned)
     bool prof = false;
     GraphStore store;  // graph arrays, reused across calls (grow-only)
     KStat kjoin, kemit, kmerge;
@@ -103,6 +109,12 @@ struct GraphDev {
     const uint32_t* nrm = nullptr;
     uint32_t kq = 0;
     uint32_t join_kernel = 0;       // nnm_join_kernel
+    // Learned initialisation: codes of rows [0, n_cap) and, inside a merge,
+    // the parent's code views with this graph's leaf index.
+    uint32_t init = 0;              // nnm_init_mode
+    const uint32_t* codes = nullptr;
+    const CodeViews* views = nullptr;
+    uint32_t view_leaf = 0;
     uint32_t* pid = nullptr;        // pools, n_cap x K
     float* pdist = nullptr;
     uint32_t* cpid = nullptr;       // compensation lists, n_cap x K (cut used)

@@ -9,5 +9,5 @@ inline std::atomic<uint64_t>& launch_counter() {
     static std::atomic<uint64_t> c{0};
     return c;
 }
-inline void count_launch() { launch_counter().fetch_add(1, std::memory_order_relaxed); }
+inline void count_launch(uint64_t k = 1) { launch_counter().fetch_add(k, std::memory_order_relaxed); }
 }  // namespace nnm

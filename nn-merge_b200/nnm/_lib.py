@@ -17,7 +17,9 @@ EXPORTED = (
     "nnm_kgraph_build", "nnm_kgraph_build_dev", "nnm_smerge", "nnm_jmerge", "nnm_merge_leaves",
     "nnm_merge_leaves_dev", "nnm_hmerge_build", "nnm_layers_free", "nnm_search",
     "nnm_profile_enable", "nnm_profile_get", "nnm_launch_count",
+    "nnm_train_opts_default", "nnm_mlp_train", "nnm_mlp_grad", "nnm_mlp_codes", "nnm_set_init_model",
 )
+MLP_HIDDEN, MLP_OUT = 256, 32
 
 
 class NnmError(RuntimeError):
@@ -32,7 +34,36 @@ class Opts(ctypes.Structure):
     _fields_ = [("seed", ctypes.c_uint32), ("rng_mode", ctypes.c_uint32), ("metric", ctypes.c_uint32),
                 ("sample_cap", ctypes.c_uint32), ("delta", ctypes.c_float), ("max_iter", ctypes.c_uint32),
                 ("exact_trace", ctypes.c_uint32), ("join_kernel", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 8)]
+                ("init", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 7)]
+
+
+class Mlp(ctypes.Structure):
+    _fields_ = [("d_in", ctypes.c_uint32), ("in_scale", ctypes.c_float), ("in_shift", ctypes.c_float),
+                ("w1", ctypes.c_void_p), ("b1", ctypes.c_void_p), ("w2", ctypes.c_void_p), ("b2", ctypes.c_void_p)]
+
+
+class TrainOpts(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_uint32), ("batch", ctypes.c_uint32), ("lr", ctypes.c_float),
+                ("margin", ctypes.c_float), ("seed", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 7)]
+
+
+def mlp_init(d, seed=0, in_scale=1.0 / 64.0, in_shift=-1.0):
+    """A fresh code model (He-initialised weights, zero biases) as a dict of
+    float32 arrays: w1 (256 x d), b1 (256), w2 (32 x 256), b2 (32)."""
+    rng = np.random.default_rng(seed)
+    return dict(w1=(rng.standard_normal((MLP_HIDDEN, d)) * np.sqrt(2.0 / d)).astype(np.float32),
+                b1=np.zeros(MLP_HIDDEN, np.float32),
+                w2=(rng.standard_normal((MLP_OUT, MLP_HIDDEN)) * np.sqrt(1.0 / MLP_HIDDEN)).astype(np.float32),
+                b2=np.zeros(MLP_OUT, np.float32), in_scale=float(in_scale), in_shift=float(in_shift))
+
+
+def _mlp_struct(m):
+    """C view of a model dict; the dict's arrays must stay alive (and are
+    made contiguous float32 in place)."""
+    for k in ("w1", "b1", "w2", "b2"):
+        m[k] = np.ascontiguousarray(m[k], np.float32)
+    return Mlp(m["w1"].shape[1], m["in_scale"], m["in_shift"], m["w1"].ctypes.data, m["b1"].ctypes.data,
+               m["w2"].ctypes.data, m["b2"].ctypes.data)
 
 
 class Stats(ctypes.Structure):
@@ -72,6 +103,11 @@ def load():
         lib.nnm_profile_enable.argtypes = [vp, ctypes.c_int]
         lib.nnm_profile_get.argtypes = [vp, ctypes.c_char_p, u64]
         lib.nnm_launch_count.restype = ctypes.c_uint64
+        lib.nnm_train_opts_default.argtypes = [vp]
+        lib.nnm_mlp_train.argtypes = [vp, vp, u64, u32, vp, u32, vp, vp, vp]
+        lib.nnm_mlp_grad.argtypes = [vp, vp, vp, u64, u32, vp, u32, ctypes.c_float, vp, vp]
+        lib.nnm_mlp_codes.argtypes = [vp, vp, vp, u64, u32, vp, vp]
+        lib.nnm_set_init_model.argtypes = [vp, vp]
         _lib = lib
     return _lib
 
@@ -84,10 +120,11 @@ RNG_MODES = {"exact": 0, "fast": 1}
 
 
 JOIN_KERNELS = {"auto": 0, "fp32": 1, "tensor": 2}
+INITS = {"random": 0, "learned": 1}
 
 
 def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exact_trace=False, rng="exact",
-              join="auto"):
+              join="auto", init="random"):
     lib = load()
     o = Opts()
     lib.nnm_opts_default(ctypes.byref(o))
@@ -99,6 +136,7 @@ def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exac
     o.max_iter = max_iter
     o.exact_trace = 1 if exact_trace else 0
     o.join_kernel = JOIN_KERNELS[join]
+    o.init = INITS[init]
     return o
 
 
@@ -157,6 +195,53 @@ class Context:
 
     def launch_count(self):
         return int(self.lib.nnm_launch_count())
+
+    # -- learned initialisation ------------------------------------------
+    def mlp_train(self, x, graph, model, steps=400, batch=2048, lr=2e-3, margin=16.0, seed=0):
+        """Trains `model` (dict from mlp_init) in place on triplets of the
+        k-NN graph `graph` (n x k ids of x); returns the per-step losses."""
+        x = np.ascontiguousarray(x, np.float32)
+        graph = np.ascontiguousarray(graph, np.uint32)
+        n, d = x.shape
+        o = TrainOpts()
+        self.lib.nnm_train_opts_default(ctypes.byref(o))
+        o.steps, o.batch, o.lr, o.margin, o.seed = steps, batch, lr, margin, seed
+        ms = _mlp_struct(model)
+        loss = np.empty(steps, np.float32)
+        self._check(self.lib.nnm_mlp_train(self.h, _ptr(x), n, d, _ptr(graph), graph.shape[1], ctypes.byref(o),
+                                           ctypes.byref(ms), _ptr(loss)))
+        return loss
+
+    def mlp_grad(self, model, x, triplets, margin=16.0):
+        """(loss, gradient dict) of the triplet loss over `triplets`
+        (t x 3 row indices: anchor, positive, negative)."""
+        x = np.ascontiguousarray(x, np.float32)
+        tr = np.ascontiguousarray(triplets, np.uint32)
+        n, d = x.shape
+        grad = {k: np.zeros_like(np.asarray(model[k], np.float32)) for k in ("w1", "b1", "w2", "b2")}
+        grad.update(in_scale=model["in_scale"], in_shift=model["in_shift"])
+        ms, gs = _mlp_struct(model), _mlp_struct(grad)
+        loss = ctypes.c_float()
+        self._check(self.lib.nnm_mlp_grad(self.h, ctypes.byref(ms), _ptr(x), n, d, _ptr(tr), tr.shape[0], margin,
+                                          ctypes.byref(loss), ctypes.byref(gs)))
+        return float(loss.value), grad
+
+    def mlp_codes(self, model, x, want_z=False):
+        x = np.ascontiguousarray(x, np.float32)
+        n, d = x.shape
+        codes = np.empty(n, np.uint32)
+        z = np.empty((n, MLP_OUT), np.float32) if want_z else None
+        ms = _mlp_struct(model)
+        self._check(self.lib.nnm_mlp_codes(self.h, ctypes.byref(ms), _ptr(x), n, d, _ptr(codes), _ptr(z)))
+        return (codes, z) if want_z else codes
+
+    def set_init_model(self, model):
+        """The model init="learned" builds use (None clears it)."""
+        if model is None:
+            self._check(self.lib.nnm_set_init_model(self.h, None))
+            return
+        ms = _mlp_struct(model)
+        self._check(self.lib.nnm_set_init_model(self.h, ctypes.byref(ms)))
 
     def merge_leaves_dev(self, x_ptr, n, d, k, leaf_sizes, ids_ptr=0, dists_ptr=0, flags_ptr=0, **kw):
         """Device-pointer build (inputs resident in HBM, outputs on the device)."""
