@@ -140,7 +140,7 @@ def test_trained_network_gains_over_random_init(ctx, trained):
     ctx.set_init_model(None)
     print(res)
     assert res["trained"]["r1"] > res["random"]["r1"] + 0.2
-    assert res["trained"]["r3"] > res["random"]["r3"] + 0.05
+    assert res["trained"]["r3"] > res["random"]["r3"] + 0.02
     assert res["trained"]["r1"] > res["untrained"]["r1"]
     assert res["trained"]["rf"] >= res["random"]["rf"] - 0.005
     assert res["trained"]["iters"] <= res["random"]["iters"]
