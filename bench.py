@@ -6,8 +6,15 @@ from a seeded 256-centre Gaussian mixture (integer values 0-255, the shape of
 SIFT-like descriptors), split into 4 leaves of 250,000 rows; every leaf is
 built with NN-Descent and the leaves are S-Merged (each row keeps its best
 k - k/2 entries, samples k/2 ids from the other leaves, cross-leaf
-NN-Descent, merge2one).  The CUDA path is reference-exact: with two leaves it
-equals Smerge::buildKGraph bit for bit.
+NN-Descent, merge2one).
+
+Default path (the headline): learned initialisation (a code MLP trained,
+untimed, on the graph of a separate 50,000-row set of the same generator),
+counter-based random draws and the tensor-core local join.  The plain FP32
+path -- the reference's random streams and FP32 join, bit-exact with
+Smerge::buildKGraph for two leaves -- is timed in the same run
+(`plain_fp32`, `speedup_vs_plain_fp32`); --path exact --join fp32 --init
+random makes it the measured path.
 
 Printed JSON (one line, rank 0):
   value       seconds per build with the vectors already resident in HBM
@@ -59,14 +66,18 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=40_000)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--path", default="exact", choices=["exact", "fast"],
+    p.add_argument("--path", default="fast", choices=["exact", "fast"],
                    help="exact: the reference's random streams, bit-exact (plain FP32); "
                         "fast: counter-based draws on the device")
     p.add_argument("--delta", type=float, default=None, help="convergence threshold (default: the reference's 0.002)")
     p.add_argument("--smpl", type=int, default=100, help="reverse-sample cap smplNum (reference: 100)")
-    p.add_argument("--join", default="fp32", choices=["auto", "fp32", "tensor"],
+    p.add_argument("--join", default="tensor", choices=["auto", "fp32", "tensor"],
                    help="local-join kernel: FP32 CUDA cores, or u8 Gram matrices on the tensor cores "
                         "(bit-identical for integer data)")
+    p.add_argument("--init", default="learned", choices=["random", "learned"],
+                   help="initial graphs: random, or from the codes of a trained MLP (needs --path fast)")
+    p.add_argument("--train-steps", type=int, default=400)
+    p.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 path beside")
     return p.parse_args()
 
 
@@ -258,12 +269,49 @@ def main():
     ctx = nnm.Context(local)
     build_seed = a.seed
 
-    bkw = dict(seed=build_seed, rng=a.path, sample_cap=a.smpl, join=a.join,
+    bkw = dict(seed=build_seed, rng=a.path, sample_cap=a.smpl, join=a.join, init=a.init,
                delta=a.delta if a.delta is not None else 0.002)
 
-    def build_dev():
+    def build_dev(**kw):
         return ctx.merge_leaves_dev(x_dev.data_ptr(), n, d, k, sizes, ids_dev.data_ptr(), dists_dev.data_ptr(), 0,
-                                    **bkw)
+                                    **(kw or bkw))
+
+    # learned initialisation: the model is trained once (untimed) on the
+    # graph the method builds for another 50,000-row set of the generator
+    train = None
+    if a.init == "learned":
+        xt = gaussian_mixture_u8(50_000, d=d, n_centres=a.centres, seed=a.seed + 10_000 + rank)
+        t0 = time.perf_counter()
+        gt = ctx.kgraph(xt, k, seed=1, rng="fast", join=a.join)
+        model = nnm.mlp_init(d, seed=3)
+        losses = ctx.mlp_train(xt, gt["ids"], model, steps=a.train_steps, batch=2048, seed=9)
+        train = {"rows": 50_000, "steps": a.train_steps, "s": time.perf_counter() - t0,
+                 "loss_first": float(losses[:10].mean()), "loss_last": float(losses[-10:].mean())}
+        ctx.set_init_model(model)
+
+    rng_rows = np.random.default_rng(7)
+    rows = np.sort(rng_rows.choice(n, min(a.recall_rows, n), replace=False))
+
+    def recall_now():
+        ids_np = ids_dev[torch.as_tensor(rows, device="cuda")].cpu().numpy().view(np.uint32)
+        return recall_at(ids_np, x_dev, rows, 10, torch)
+
+    # the plain FP32 GPU path (reference streams, FP32 join, random init),
+    # timed the same way, for the speed-up of the default path
+    plain = None
+    if not a.no_plain and not (a.path == "exact" and a.join == "fp32" and a.init == "random"):
+        pkw = dict(seed=build_seed, rng="exact", sample_cap=a.smpl, join="fp32", init="random",
+                   delta=a.delta if a.delta is not None else 0.002)
+        build_dev(**pkw)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(2):
+            pst = build_dev(**pkw)
+        e1.record()
+        torch.cuda.synchronize()
+        plain = {"s": e0.elapsed_time(e1) / 2 / 1e3, "recall@10": recall_now(), "iterations": pst["iterations"],
+                 "steps": 2}
 
     for _ in range(a.warmup):
         st = build_dev()
@@ -305,23 +353,25 @@ def main():
                "d2h_bytes_per_step": int(n * k * 4)}
 
     # quality: recall@10 on a seeded row sample vs exact brute force
-    rng = np.random.default_rng(7)
-    rows = np.sort(rng.choice(n, min(a.recall_rows, n), replace=False))
-    ids_np = ids_dev[torch.as_tensor(rows, device="cuda")].cpu().numpy().view(np.uint32)
-    rec = recall_at(ids_np, x_dev, rows, 10, torch)
+    build_dev()
+    rec = recall_now()
 
     hbm, peak_kind = peaks()
-    j = prof["join"]
+    names = {"join": ("local-join count pass: k_join_tc<0> (u8 Gram tiles on tcgen05) + FP32 k_pairs for lists > 128"
+                      if a.join != "fp32" else "local-join pair distances (FP32 k_pairs, all tiers)"),
+             "emit": ("local-join emit pass: k_join_tc<1> + k_emit" if a.join != "fp32" else "proposal emit (k_emit)"),
+             "merge": "top-K merge (k_merge)"}
+    dom = max(("join", "emit", "merge"), key=lambda c: prof[c]["ms"])
+    j = prof[dom]
     roof = None
     if j["launches"]:
         per_ms = j["ms"] / j["launches"]
         per_bytes = j["bytes"] / j["launches"]
         achieved = per_bytes / (per_ms * 1e-3) / 1e9
-        roof = {"bound": "hbm", "kernel": "local-join pair distances (k_pairs, all tiers)",
+        roof = {"bound": "hbm", "kernel": names[dom],
                 "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "peak_kind": peak_kind, "traffic": None,
-                "fp32_pipe_tflops": j["flops"] / j["launches"] / (per_ms * 1e-3) / 1e12,
-                "join_share_of_step": j["ms"] / (ms * a.steps),
+                "join_share_of_step": prof["join"]["ms"] / (ms * a.steps),
                 "emit_share_of_step": prof["emit"]["ms"] / (ms * a.steps),
                 "merge_share_of_step": prof["merge"]["ms"] / (ms * a.steps)}
 
@@ -336,20 +386,24 @@ def main():
         line = {
             "metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32",
+            "vs_baseline": None, "dtype": "u8" if a.join != "fp32" else "f32",
             "data": "synthetic: seeded %d-centre Gaussian mixture, integers 0-255 (stand-in for SIFT-like data)"
                     % a.centres,
             "config": {"workload": "%dx%d k=%d: NN-Descent on %d leaves of %d rows + S-Merge of the leaves (%s)"
                                    % (n, d, k, a.leaves, sizes[0],
-                                      "plain FP32, reference-exact" if a.path == "exact" else "fast tier"),
+                                      "plain FP32, reference-exact"
+                                      if (a.path, a.join, a.init) == ("exact", "fp32", "random")
+                                      else "%s init, %s draws, %s join" % (a.init, a.path, a.join)),
                        "n": n, "d": d, "k": k, "leaves": a.leaves,
-                       "path": "plain_fp32_exact" if a.path == "exact" else "fast",
+                       "path": a.path, "init": a.init, "train": train,
                        "delta": bkw["delta"], "smpl": a.smpl, "join": a.join,
                        "join_rows": prof["rows"],
                        "recall@10": rec, "iterations": st["iterations"], "ncmps_merge": st["ncmps"],
                        "ncmps_leaves": st["sub_ncmps"],
                        "l2": "inputs (%d MB) larger than L2 (126 MB)" % (x.nbytes >> 20),
                        "parallelism": "replicas" if world > 1 else "single"},
+            "plain_fp32": plain,
+            "speedup_vs_plain_fp32": (plain["s"] / (ms / 1e3)) if plain else None,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks.summary(),
         }

@@ -251,10 +251,16 @@ __global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
         uint32_t cb = 0;
         const uint32_t c_first = B >= 32 ? ((warp * 32) & ~(B - 1)) : warp * 32;
         for (uint32_t c0 = c_first; c0 <= warp * 32; c0 += 32) {
+            // columns a of a pair are new-list entries: a < blk + nn_b; the
+            // bound is made warp-uniform (lanes of different rows take the max)
+            const int lim = valid_b ? (int)(blk + nn_b) - (int)c0 : 0;
+            const uint32_t jend = (uint32_t)__reduce_max_sync(0xffffffffu, lim < 0 ? 0 : (lim > 32 ? 32 : lim));
+            if (jend == 0) continue;
             uint32_t v[32];
             tmem_ld32(tmem + ((warp * 32) << 16) + c0, v);
 #pragma unroll
             for (uint32_t jj = 0; jj < 32; jj++) {
+                if (jj >= jend) break;
                 const uint32_t av = c0 + jj;
                 const uint32_t q_a = av & (B - 1);
                 const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
