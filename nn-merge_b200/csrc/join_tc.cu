@@ -275,8 +275,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
                     const unsigned m = __ballot_sync(0xffffffffu, ok && dd < kth_a);
                     if (m && lane == 0) atomicAdd(&s_cnt[av], (uint32_t)__popc(m));
                 } else {
-                    const unsigned long long key =
-                        (1ull << 63) | ((unsigned long long)row_b << 32) | ((unsigned long long)(outer * S_b + inner) << 1);
+                    const uint32_t pidx = outer * S_b + inner;
                     const bool pa = ok && dd < kth_a;
                     const unsigned m = __ballot_sync(0xffffffffu, pa);
                     if (m) {
@@ -286,12 +285,14 @@ __global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
                         base = __shfl_sync(0xffffffffu, base, leader);
                         if (pa) {
                             const unsigned long long slot = s_base[av] + base + __popc(m & ((1u << lane) - 1u));
-                            a.bucket[slot] = Prop{dd, e_b, key | (outer == q_a ? 0ull : 1ull)};
+                            a.bucket[slot] =
+                                Prop{dd, e_b, prop_key(a.fast_key, row_b, pidx, e_b & LID_MASK, outer == q_a ? 0u : 1u)};
                         }
                     }
                     if (ok && dd < kth_b) {
                         const unsigned long long slot = s_base[tid] + atomicAdd(&s_cnt[tid], 1u);
-                        a.bucket[slot] = Prop{dd, e_a, key | (outer == q_b ? 0ull : 1ull)};
+                        a.bucket[slot] =
+                            Prop{dd, e_a, prop_key(a.fast_key, row_b, pidx, e_a & LID_MASK, outer == q_b ? 0u : 1u)};
                     }
                 }
             }

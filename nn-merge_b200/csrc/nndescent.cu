@@ -256,9 +256,92 @@ __device__ __forceinline__ void shuffle_seg(uint32_t* seg, uint32_t len, const i
     }
 }
 
+// Fast tier: keeps, in place at seg[0, keep), the `keep` entries of
+// seg[0, len) with the smallest (hash(id), id), the hash a Philox draw keyed
+// by (row, phase, list, id) -- a uniform random subset that depends only on
+// the ids, not on their order.  The keep-th smallest hash is found by an
+// 8-bit radix select (4 rounds over a 256-bin histogram), ties on it by the
+// smallest ids.  Warp-wide; hist is this warp's 256-entry shared scratch.
+__device__ void hash_sample(uint32_t* seg, uint32_t len, uint32_t keep, const Philox& ph, uint32_t t,
+                            uint32_t phase, uint32_t l, uint32_t* hist) {
+    const int lane = threadIdx.x & 31;
+    uint32_t prefix = 0, need = keep;
+    for (int byte = 3; byte >= 0; byte--) {
+        for (uint32_t i = lane; i < 256; i += 32) hist[i] = 0;
+        __syncwarp();
+        const uint32_t hi_mask = byte == 3 ? 0u : (0xffffffffu << (8 * (byte + 1)));
+        for (uint32_t j = lane; j < len; j += 32) {
+            const uint32_t h = ph(t, phase, l, seg[j] & LID_MASK).x;
+            if ((h & hi_mask) == prefix) atomicAdd(&hist[(h >> (8 * byte)) & 255u], 1u);
+        }
+        __syncwarp();
+        // the bin holding the need-th entry: 8 bins per lane, scan over lanes
+        uint32_t c[8], sum = 0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            c[q] = hist[lane * 8 + q];
+            sum += c[q];
+        }
+        uint32_t incl = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t excl = incl - sum;
+        const int src = __ffs(__ballot_sync(FULL, excl < need && need <= incl)) - 1;
+        uint32_t bin = 0, before = 0;
+        if (lane == src) {
+            uint32_t run = excl;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (run + c[q] >= need) {
+                    bin = lane * 8 + q;
+                    before = run;
+                    break;
+                }
+                run += c[q];
+            }
+        }
+        bin = __shfl_sync(FULL, bin, src);
+        before = __shfl_sync(FULL, before, src);
+        need -= before;
+        prefix |= bin << (8 * byte);
+        __syncwarp();
+    }
+    // all hashes below the threshold T, and the `need` smallest ids at T
+    const uint32_t T = prefix;
+    uint32_t idT = 0;
+    for (uint32_t r = 0; r < need; r++) {
+        uint32_t mn = 0xffffffffu;
+        for (uint32_t j = lane; j < len; j += 32) {
+            const uint32_t id = seg[j] & LID_MASK;
+            if ((r == 0 || id > idT) && id < mn && ph(t, phase, l, id).x == T) mn = id;
+        }
+        idT = __reduce_min_sync(FULL, mn);
+    }
+    uint32_t out = 0;
+    for (uint32_t j0 = 0; j0 < len; j0 += 32) {  // stable compaction in place
+        const uint32_t j = j0 + lane;
+        uint32_t v = 0;
+        bool sel = false;
+        if (j < len) {
+            v = seg[j];
+            const uint32_t id = v & LID_MASK, h = ph(t, phase, l, id).x;
+            sel = h < T || (h == T && id <= idT);
+        }
+        __syncwarp();
+        const unsigned m = __ballot_sync(FULL, sel);
+        const uint32_t pos = out + __popc(m & ((1u << lane) - 1u));
+        if (sel && pos < keep) seg[pos] = v;
+        out += __popc(m);
+        __syncwarp();
+    }
+}
+
 // One warp per row: lane 0 shuffles in shared memory, the warp appends.
 __global__ void k_shuffle_append(ShufArgs a) {
     __shared__ uint32_t stage[8][SHUF_SMEM];
+    __shared__ uint32_t hist[8][256];
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t t = blockIdx.x * 8 + w;
     if (t >= a.n) return;
@@ -272,18 +355,8 @@ __global__ void k_shuffle_append(ShufArgs a) {
         uint32_t* sh = stage[w];
         bool staged = len <= SHUF_SMEM;
         if (a.fast) {
-            // keep a uniform random subset of smplNum entries (partial
-            // Fisher-Yates with Philox draws); order is irrelevant here
-            if (len > a.smpl && lane == 0) {
-                const Philox ph{a.seed, 0x6e6e6d01u};
-                for (uint32_t i = 0; i < keep; i++) {
-                    const uint32_t r = ph(t, a.phase, (uint32_t)l, i).x;
-                    const uint32_t j = i + bounded(r, len - i);
-                    const uint32_t v = seg[i];
-                    seg[i] = seg[j];
-                    seg[j] = v;
-                }
-            }
+            // a uniform random subset of smplNum entries, chosen by id
+            if (len > a.smpl) hash_sample(seg, len, keep, Philox{a.seed, 0x6e6e6d01u}, t, a.phase, (uint32_t)l, hist[w]);
             __syncwarp();
             sh = seg;
         } else if (staged) {
@@ -494,15 +567,14 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
             if (!pair_order(a.mode, a.verse, av, bv, nn, s_ids[av], s_ids[bv], s_grp[av], s_grp[bv], outer, inner))
                 continue;
             const float dd = pd[pair_slot(av, bv, nn, no)];
-            const unsigned long long kb =
-                (1ull << 63) | ((unsigned long long)row << 32) | ((unsigned long long)(outer * S + inner) << 1);
+            const uint32_t pidx = outer * S + inner;
             if (dd < s_kth[outer]) {
                 unsigned long long slot = s_base[outer] + atomicAdd(&s_cur[outer], 1u);
-                a.bucket[slot] = Prop{dd, s_ids[inner], kb};
+                a.bucket[slot] = Prop{dd, s_ids[inner], prop_key(a.fast_key, row, pidx, s_ids[inner] & LID_MASK, 0)};
             }
             if (dd < s_kth[inner]) {
                 unsigned long long slot = s_base[inner] + atomicAdd(&s_cur[inner], 1u);
-                a.bucket[slot] = Prop{dd, s_ids[outer], kb | 1ull};
+                a.bucket[slot] = Prop{dd, s_ids[outer], prop_key(a.fast_key, row, pidx, s_ids[outer] & LID_MASK, 1)};
             }
         }
     }
@@ -532,9 +604,13 @@ __device__ __forceinline__ bool mless(uint32_t d1, unsigned long long k1, uint32
 }
 
 // Number of entries of a sorted per-lane list (first `cnt` lanes) that are
-// smaller than (d, k).
+// smaller than (d, k) -- or, with `or_equal`, not greater.  Pool entries
+// count the smaller proposals and proposals count the pool entries that
+// are not greater, so that an entry present on both sides (the same
+// proposal made twice, possible with the fast tier's keys) gets two
+// distinct merged positions, pool first; the duplicate is dropped below.
 __device__ __forceinline__ uint32_t count_less(uint32_t ld, unsigned long long lk, uint32_t cnt, uint32_t d,
-                                               unsigned long long k) {
+                                               unsigned long long k, bool or_equal = false) {
     uint32_t lo = 0, hi = cnt;
 #pragma unroll
     for (int s = 0; s < 6; s++) {
@@ -542,7 +618,8 @@ __device__ __forceinline__ uint32_t count_less(uint32_t ld, unsigned long long l
         uint32_t md = __shfl_sync(FULL, ld, mid & 31);
         unsigned long long mk = __shfl_sync(FULL, lk, mid & 31);
         if (lo < hi) {
-            if (mless(md, mk, d, k)) lo = mid + 1;
+            const bool below = mless(md, mk, d, k) || (or_equal && md == d && mk == k);
+            if (below) lo = mid + 1;
             else hi = mid;
         }
     }
@@ -611,7 +688,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32) k_merge(MergeArgs a) {
                     count_less(pd, pk, m, cd, ck);
                 }
                 {
-                    uint32_t pos = lane + count_less(cd, ck, K, pd, pk);
+                    uint32_t pos = lane + count_less(cd, ck, K, pd, pk, true);
                     if (lane < (int)m) sm[w][pos] = MEnt{pd, pe, pk};
                 }
                 __syncwarp();
@@ -852,11 +929,13 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         RevSortArgs ra{{roff_new, roff_old}, {rseg_new, rseg_old}, {rscr_new, rscr_old},
                        {carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr},
                        n, P<uint32_t>(ws.bigrev), ctr};
-        // reverse lists in ascending source order (also in the fast tier: the
-        // atomics fill them in arbitrary order, and the sample must not depend
-        // on it)
-        k_rev_sort_small<<<dim3(warp_blocks, 2), 256, 0, st>>>(ra); count_launch();
-        k_rev_sort_big<<<nsm * 2, 512, 0, st>>>(ra); count_launch();
+        // reverse lists in ascending source order, as the reference pushes
+        // them; the fast tier keeps them in the (arbitrary) order the atomics
+        // left: its samples and tie-break keys do not depend on list order
+        if (!g.fast) {
+            k_rev_sort_small<<<dim3(warp_blocks, 2), 256, 0, st>>>(ra); count_launch();
+            k_rev_sort_big<<<nsm * 2, 512, 0, st>>>(ra); count_launch();
+        }
         if (!g.fast) {
             // std::rand() draws of this iteration's shuffles
             k_rand_count<<<tblocks, 256, 0, st>>>(roff_new, roff_old, n, P<uint32_t>(ws.rcount)); count_launch();
@@ -892,7 +971,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     (uint32_t)mode, verse, d_leaf_off, nleaf, P<uint32_t>(ws.tiers), P<uint64_t>(ws.poff),
                     P<float>(ws.pd), P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
                     P<uint64_t>(ws.boff), P<Prop>(ws.bucket), ctr,
-                    g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error, tc ? P<uint32_t>(ws.erows) : nullptr};
+                    g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error, tc ? P<uint32_t>(ws.erows) : nullptr,
+                    g.fast ? 1u : 0u};
         if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
         if (tc) NNM_CUDA_TRY(launch_join_tc(0, ja, ntier, nsm, st));
         if (g.metric == L2) launch_pairs<L2>(ja, ntier, caps, g.dp, nsm, tc, st);

@@ -44,7 +44,19 @@ struct JoinArgs {
     uint32_t kq, tc;
     unsigned* tc_err;
     uint32_t* emit_rows;  // 4 lists of n rows: rows of tiers 0-3 that have proposals
+    uint32_t fast_key;    // tie-break keys from ids instead of list positions (fast tier)
 };
+
+// Tie-break key of the proposal "target gets `other`" from the join of
+// `row`.  Exact tier: the reference's sequential insert order (the pair's
+// index in join order, then the side: 0 = into the outer element's pool).
+// Fast tier: the other element's id in place of the pair index, so that the
+// graphs do not depend on the order of the sample lists.
+__device__ __forceinline__ unsigned long long prop_key(uint32_t fast, uint32_t row, uint32_t pair_idx,
+                                                       uint32_t other_id, uint32_t side) {
+    return (1ull << 63) | ((unsigned long long)row << 32) |
+           ((unsigned long long)(fast ? other_id : pair_idx) << 1) | side;
+}
 
 __device__ __forceinline__ uint32_t leaf_of(uint32_t id, const uint32_t* off, uint32_t nleaf) {
     uint32_t lo = 0, hi = nleaf;  // off[0] = 0 <= id < off[nleaf]
