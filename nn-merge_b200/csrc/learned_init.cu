@@ -135,11 +135,82 @@ __device__ uint32_t random_fill(SortEnt* ents, uint32_t cnt, uint32_t want, uint
     return cnt;
 }
 
+// Where candidate distances come from: the u8 copy and norms when the
+// tensor-core join prepared them (exact integer dot products, dp4a), else
+// the FP32 vectors with the reference's sequential sum.  Both give the
+// exact distance of the data.
+struct DistSrc {
+    const float* x;
+    uint32_t dp;
+    int metric;
+    const uint8_t* xq;
+    const uint32_t* nrm;
+    uint32_t kq;
+};
+
+__device__ __forceinline__ float cand_dist(const DistSrc& s, uint32_t r, uint32_t c) {
+    if (s.xq) {
+        const uint4* a = reinterpret_cast<const uint4*>(s.xq + (size_t)r * s.kq);
+        const uint4* b = reinterpret_cast<const uint4*>(s.xq + (size_t)c * s.kq);
+        unsigned dot = 0;
+        for (uint32_t i = 0; i < s.kq / 16; i++) {
+            const uint4 u = a[i], v = b[i];
+            dot = __dp4a(u.x, v.x, dot);
+            dot = __dp4a(u.y, v.y, dot);
+            dot = __dp4a(u.z, v.z, dot);
+            dot = __dp4a(u.w, v.w, dot);
+        }
+        return (float)((int)(s.nrm[r] + s.nrm[c]) - 2 * (int)dot);
+    }
+    return dist_seq_rt(s.metric, s.x + (size_t)r * s.dp, s.x + (size_t)c * s.dp, s.dp);
+}
+
+// Sorts e[0, cnt), cnt <= 64, by (distance, id word): a warp bitonic sort of
+// 64-bit keys, two per lane (lane l holds positions 2l and 2l + 1).
+__device__ void warp_sort64(SortEnt* e, uint32_t cnt) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long v[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const uint32_t i = 2 * lane + h;
+        v[h] = i < cnt ? ((unsigned long long)__float_as_uint(e[i].dist) << 32) | e[i].id : ~0ull;
+    }
+    __syncwarp();
+#pragma unroll
+    for (uint32_t k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j == 1) {
+                const bool asc = ((2 * lane) & k) == 0;
+                if ((v[0] > v[1]) == asc) {
+                    const unsigned long long t = v[0];
+                    v[0] = v[1];
+                    v[1] = t;
+                }
+            } else {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const uint32_t i = 2 * lane + h;
+                    const unsigned long long o = __shfl_xor_sync(FULLM, v[h], j >> 1);
+                    const bool lower = (i & j) == 0, asc = (i & k) == 0;
+                    v[h] = (lower == asc) ? min(v[h], o) : max(v[h], o);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const uint32_t i = 2 * lane + h;
+        if (i < cnt) e[i] = SortEnt{__uint_as_float((uint32_t)(v[h] >> 32)), (uint32_t)v[h]};
+    }
+    __syncwarp();
+}
+
 // Keeps the first of equal ids among the 64 candidate slots (c0 at slot
 // lane, c1 at slot lane + 32) and compacts the kept ones with their exact
-// distances into out[]; returns how many.
-__device__ uint32_t compact_candidates(uint32_t* cid, uint32_t c0, uint32_t c1, SortEnt* out, int metric,
-                                       const float* xr, const float* x, uint32_t dp) {
+// distances to row r into out[]; returns how many.
+__device__ uint32_t compact_candidates(uint32_t* cid, uint32_t c0, uint32_t c1, SortEnt* out, const DistSrc& ds,
+                                       uint32_t r) {
     const int lane = threadIdx.x & 31;
     cid[lane] = c0;
     cid[lane + 32] = c1;
@@ -152,8 +223,8 @@ __device__ uint32_t compact_candidates(uint32_t* cid, uint32_t c0, uint32_t c1, 
     }
     const unsigned b0 = __ballot_sync(FULLM, k0), b1 = __ballot_sync(FULLM, k1);
     const unsigned lt = (1u << lane) - 1u;
-    if (k0) out[__popc(b0 & lt)] = SortEnt{dist_seq_rt(metric, xr, x + (size_t)c0 * dp, dp), c0 | FLAG_BIT};
-    if (k1) out[__popc(b0) + __popc(b1 & lt)] = SortEnt{dist_seq_rt(metric, xr, x + (size_t)c1 * dp, dp), c1 | FLAG_BIT};
+    if (k0) out[__popc(b0 & lt)] = SortEnt{cand_dist(ds, r, c0), c0 | FLAG_BIT};
+    if (k1) out[__popc(b0) + __popc(b1 & lt)] = SortEnt{cand_dist(ds, r, c1), c1 | FLAG_BIT};
     __syncwarp();
     return __popc(b0) + __popc(b1);
 }
@@ -170,6 +241,7 @@ struct RowsArgs {
     uint32_t P, nleaf, leaf, npar;  // npar: rows of the parent (pos stride)
     uint32_t seed, phase;
     IterCounters* ctr;
+    DistSrc ds;
 };
 
 __global__ void __launch_bounds__(IW * 32) k_learned_rows(RowsArgs a) {
@@ -187,7 +259,7 @@ __global__ void __launch_bounds__(IW * 32) k_learned_rows(RowsArgs a) {
     if (p >= o + 1) c0 = (uint32_t)(seg[p - o - 1] & 0xffffffffu) - a.base;
     if (p + o + 1 < a.n) c1 = (uint32_t)(seg[p + o + 1] & 0xffffffffu) - a.base;
     const float* xr = a.x + (size_t)row * a.dp;
-    uint32_t cnt = compact_candidates(cid[w], c0, c1, ents[w], a.metric, xr, a.x, a.dp);
+    uint32_t cnt = compact_candidates(cid[w], c0, c1, ents[w], a.ds, row);
     if (cnt < a.K) {
         const Philox ph{a.seed, 0x6e6e6d03u};
         cnt = random_fill(ents[w], cnt, a.K, row, a.n, 0, 0, ph, row, a.phase, a.x, a.dp, a.metric, xr);
@@ -196,8 +268,7 @@ __global__ void __launch_bounds__(IW * 32) k_learned_rows(RowsArgs a) {
             return;
         }
     }
-    if (lane == 0) std_sort_dev(ents[w], (int)cnt);
-    __syncwarp();
+    warp_sort64(ents[w], cnt);
     if (lane < (int)a.K) {
         a.pid[(size_t)row * a.K + lane] = ents[w][lane].id;
         a.pdist[(size_t)row * a.K + lane] = ents[w][lane].dist;
@@ -217,6 +288,7 @@ struct CrossArgsL {
     uint32_t P, nleaf, nview, npair, win;  // (view, other leaf) pairs used (<= 32), window per pair
     uint32_t seed, phase;
     IterCounters* ctr;
+    DistSrc ds;
 };
 
 __device__ __forceinline__ uint32_t leaf_of_row(uint32_t id, const uint32_t* off, uint32_t nleaf) {
@@ -279,7 +351,7 @@ __global__ void __launch_bounds__(IW * 32) k_learned_cross(CrossArgsL a) {
     // candidates go after the kept entries (they are rows of other leaves,
     // so they cannot repeat a kept id)
     SortEnt* cand = e + keep;
-    uint32_t cnt = compact_candidates(cid[w], c[0], c[1], cand, a.metric, xr, a.x, a.dp);
+    uint32_t cnt = compact_candidates(cid[w], c[0], c[1], cand, a.ds, row);
     if (cnt < need) {
         const Philox ph{a.seed, 0x6e6e6d04u};
         cnt = random_fill(cand, cnt, need, row, a.n, a.leaf_off[leaf], a.leaf_off[leaf + 1], ph, row, a.phase, a.x,
@@ -290,11 +362,8 @@ __global__ void __launch_bounds__(IW * 32) k_learned_cross(CrossArgsL a) {
         }
     }
     // the `need` nearest candidates, then the pool sorted
-    if (lane == 0) {
-        std_sort_dev(cand, (int)cnt);
-        std_sort_dev(e, (int)K);
-    }
-    __syncwarp();
+    warp_sort64(cand, cnt);
+    warp_sort64(e, K);
     if (lane < (int)K) {
         a.pid[(size_t)row * K + lane] = e[lane].id;
         a.pdist[(size_t)row * K + lane] = e[lane].dist;
@@ -347,7 +416,8 @@ int learned_rows(Ctx& ctx, GraphDev& s, const CodeViews& vw, uint32_t leaf) {
     NNM_CUDA_TRY(ctx.ws.counters.ensure(sizeof(IterCounters) + 64));
     NNM_CUDA_TRY(cudaMemsetAsync(ctx.ws.counters.p, 0, sizeof(IterCounters), ctx.stream));
     RowsArgs ra{s.x, s.dp, s.K, s.metric, s.pid, s.pdist, s.n, vw.leaf_off[leaf], vw.keys, vw.pos, vw.P, vw.nleaf,
-                leaf, vw.n, s.seed, s.phase++, ctx.ws.counters.as<IterCounters>()};
+                leaf, vw.n, s.seed, s.phase++, ctx.ws.counters.as<IterCounters>(),
+                DistSrc{s.x, s.dp, s.metric, s.xq, s.nrm, s.kq}};
     k_learned_rows<<<blocks_for(s.n, IW), IW * 32, 0, ctx.stream>>>(ra); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return check_counters(ctx);
@@ -365,7 +435,7 @@ int learned_cross(Ctx& ctx, GraphDev& g, const CodeViews& vw, const uint32_t* d_
     const uint32_t win = std::max<uint32_t>(1, NCAND / (2 * npair));
     CrossArgsL ca{g.x, g.dp, g.K, g.metric, g.pid, g.cpid, g.pdist, g.cpdist, g.n, g.K - g.cut, g.codes, vw.keys,
                   d_leaf_off, vw.P, vw.nleaf, nview, npair, win, g.seed, g.phase++,
-                  ctx.ws.counters.as<IterCounters>()};
+                  ctx.ws.counters.as<IterCounters>(), DistSrc{g.x, g.dp, g.metric, g.xq, g.nrm, g.kq}};
     k_learned_cross<<<blocks_for(g.n, IW), IW * 32, 0, ctx.stream>>>(ca); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return check_counters(ctx);

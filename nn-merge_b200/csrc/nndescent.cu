@@ -626,9 +626,82 @@ __device__ __forceinline__ uint32_t count_less(uint32_t ld, unsigned long long l
     return lo;
 }
 
+// One round of the merge: the sorted chunk (pd, pk, pe; m valid entries in
+// the first lanes) merged with the pool (cd, ce, ck in lanes < K), equal
+// ids dropped (first in (dist, key) order kept), K smallest kept.
+__device__ __forceinline__ void merge_round(uint32_t pd, unsigned long long pk, uint32_t pe, uint32_t m, uint32_t K,
+                                            uint32_t& cd, uint32_t& ce, unsigned long long& ck, MEnt* sm,
+                                            MEnt* kept) {
+    const int lane = threadIdx.x & 31;
+    if (lane < (int)K) {
+        uint32_t pos = lane + count_less(pd, pk, m, cd, ck);
+        sm[pos] = MEnt{cd, ce, ck};
+    } else {
+        count_less(pd, pk, m, cd, ck);
+    }
+    {
+        uint32_t pos = lane + count_less(cd, ck, K, pd, pk, true);
+        if (lane < (int)m) sm[pos] = MEnt{pd, pe, pk};
+    }
+    __syncwarp();
+    const uint32_t tot = K + m;
+    bool keep0 = false, keep1 = false;
+    for (int h = 0; h < 2; h++) {
+        uint32_t s = lane + 32 * h;
+        bool keep = false;
+        if (s < tot) {
+            keep = true;
+            MEnt me = sm[s];
+            for (int q = (int)s - 1; q >= 0 && sm[q].d == me.d; q--)
+                if ((sm[q].e & ID_MASK) == (me.e & ID_MASK)) {
+                    keep = false;
+                    break;
+                }
+        }
+        if (h == 0) keep0 = keep;
+        else keep1 = keep;
+    }
+    unsigned b0m = __ballot_sync(FULL, keep0), b1m = __ballot_sync(FULL, keep1);
+    unsigned lt = (1u << lane) - 1u;
+    uint32_t r0 = __popc(b0m & lt), r1 = __popc(b0m) + __popc(b1m & lt);
+    if (keep0 && r0 < K) kept[r0] = sm[lane];
+    if (keep1 && r1 < K) kept[r1] = sm[lane + 32];
+    __syncwarp();
+    if (lane < (int)K) {
+        MEnt me = kept[lane];
+        cd = me.d;
+        ce = me.e;
+        ck = me.k;
+    }
+    __syncwarp();
+}
+
+// Bitonic sort of one entry per lane by (dist, key).
+__device__ __forceinline__ void warp_sort_ment(uint32_t& pd, unsigned long long& pk, uint32_t& pe) {
+    const int lane = threadIdx.x & 31;
+    for (int k = 2; k <= 32; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            uint32_t od = __shfl_xor_sync(FULL, pd, j);
+            unsigned long long ok = __shfl_xor_sync(FULL, pk, j);
+            uint32_t oe = __shfl_xor_sync(FULL, pe, j);
+            bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
+            bool swap = take_min ? mless(od, ok, pd, pk) : mless(pd, pk, od, ok);
+            if (swap) {
+                pd = od;
+                pk = ok;
+                pe = oe;
+            }
+        }
+}
+
+// One warp per target.  Proposals that pass the current K-th entry are
+// collected in a 32-entry buffer; a full buffer (and the rest at the end)
+// is sorted and merged into the pool, which lowers the K-th entry for the
+// proposals still to come.
 __global__ void __launch_bounds__(MERGE_WARPS * 32) k_merge(MergeArgs a) {
     __shared__ MEnt sm[MERGE_WARPS][64];
     __shared__ MEnt kept[MERGE_WARPS][32];
+    __shared__ MEnt buf[MERGE_WARPS][32];
     __shared__ unsigned int blk_flags;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) blk_flags = 0;
@@ -649,82 +722,53 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32) k_merge(MergeArgs a) {
             uint32_t kd = __shfl_sync(FULL, cd, K - 1);
             unsigned long long kk = __shfl_sync(FULL, ck, K - 1);
             const Prop* bp = a.bucket + a.boff[t];
+            const unsigned lt = (1u << lane) - 1u;
+            uint32_t nb = 0;  // entries in buf
+            auto flush = [&]() {
+                uint32_t pd = 0xffffffffu, pe = 0;
+                unsigned long long pk = ~0ull;
+                if (lane < (int)nb) {
+                    const MEnt me = buf[w][lane];
+                    pd = me.d;
+                    pe = me.e;
+                    pk = me.k;
+                }
+                __syncwarp();
+                warp_sort_ment(pd, pk, pe);
+                merge_round(pd, pk, pe, nb, K, cd, ce, ck, sm[w], kept[w]);
+                kd = __shfl_sync(FULL, cd, K - 1);
+                kk = __shfl_sync(FULL, ck, K - 1);
+                nb = 0;
+            };
             for (uint32_t b0 = 0; b0 < c; b0 += 32) {
                 uint32_t pd = 0xffffffffu, pe = 0;
                 unsigned long long pk = ~0ull;
                 bool valid = false;
                 if (b0 + lane < c) {
                     Prop p = bp[b0 + lane];
-                    uint32_t dbits = __float_as_uint(p.dist);
-                    if (mless(dbits, p.key, kd, kk)) {
-                        valid = true;
-                        pd = dbits;
-                        pk = p.key;
-                        pe = (p.idg & LID_MASK) | ((p.idg >> 31) << 30) | FLAG_BIT;
-                    }
+                    pd = __float_as_uint(p.dist);
+                    pk = p.key;
+                    pe = (p.idg & LID_MASK) | ((p.idg >> 31) << 30) | FLAG_BIT;
+                    valid = mless(pd, pk, kd, kk);
                 }
                 unsigned vb = __ballot_sync(FULL, valid);
                 if (!vb) continue;
-                // bitonic sort of the chunk by (dist, key)
-                for (int k = 2; k <= 32; k <<= 1)
-                    for (int j = k >> 1; j > 0; j >>= 1) {
-                        uint32_t od = __shfl_xor_sync(FULL, pd, j);
-                        unsigned long long ok = __shfl_xor_sync(FULL, pk, j);
-                        uint32_t oe = __shfl_xor_sync(FULL, pe, j);
-                        bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
-                        bool swap = take_min ? mless(od, ok, pd, pk) : mless(pd, pk, od, ok);
-                        if (swap) {
-                            pd = od;
-                            pk = ok;
-                            pe = oe;
-                        }
-                    }
-                const uint32_t m = __popc(vb);
-                // merged positions
-                if (lane < (int)K) {
-                    uint32_t pos = lane + count_less(pd, pk, m, cd, ck);
-                    sm[w][pos] = MEnt{cd, ce, ck};
-                } else {
-                    count_less(pd, pk, m, cd, ck);
-                }
-                {
-                    uint32_t pos = lane + count_less(cd, ck, K, pd, pk, true);
-                    if (lane < (int)m) sm[w][pos] = MEnt{pd, pe, pk};
-                }
+                const uint32_t take = min((uint32_t)__popc(vb), 32u - nb);
+                const uint32_t rank = __popc(vb & lt);
+                if (valid && rank < take) buf[w][nb + rank] = MEnt{pd, pe, pk};
                 __syncwarp();
-                const uint32_t tot = K + m;
-                bool keep0 = false, keep1 = false;
-                for (int h = 0; h < 2; h++) {
-                    uint32_t s = lane + 32 * h;
-                    bool keep = false;
-                    if (s < tot) {
-                        keep = true;
-                        MEnt me = sm[w][s];
-                        for (int q = (int)s - 1; q >= 0 && sm[w][q].d == me.d; q--)
-                            if ((sm[w][q].e & ID_MASK) == (me.e & ID_MASK)) {
-                                keep = false;
-                                break;
-                            }
-                    }
-                    if (h == 0) keep0 = keep;
-                    else keep1 = keep;
+                nb += take;
+                if (nb == 32) {
+                    flush();
+                    // the rest of this chunk, against the new K-th entry
+                    valid = valid && rank >= take && mless(pd, pk, kd, kk);
+                    vb = __ballot_sync(FULL, valid);
+                    if (valid) buf[w][__popc(vb & lt)] = MEnt{pd, pe, pk};
+                    __syncwarp();
+                    nb = __popc(vb);
                 }
-                unsigned b0m = __ballot_sync(FULL, keep0), b1m = __ballot_sync(FULL, keep1);
-                unsigned lt = (1u << lane) - 1u;
-                uint32_t r0 = __popc(b0m & lt), r1 = __popc(b0m) + __popc(b1m & lt);
-                if (keep0 && r0 < K) kept[w][r0] = sm[w][lane];
-                if (keep1 && r1 < K) kept[w][r1] = sm[w][lane + 32];
-                __syncwarp();
-                if (lane < (int)K) {
-                    MEnt me = kept[w][lane];
-                    cd = me.d;
-                    ce = me.e;
-                    ck = me.k;
-                }
-                kd = __shfl_sync(FULL, cd, K - 1);
-                kk = __shfl_sync(FULL, ck, K - 1);
-                __syncwarp();
             }
+            if (nb) flush();
             if (lane < (int)K) {
                 a.pid[(size_t)t * K + lane] = ce;
                 a.pdist[(size_t)t * K + lane] = __uint_as_float(cd);
