@@ -23,12 +23,15 @@
 // that pass the K-th-distance filter (the bucket sizes); pass 1 recomputes
 // the distances and writes the proposals.  Nothing per pair is stored.
 //
-// Synchronisation: persistent CTAs of 128 threads, at most four per SM (the
+// Synchronisation: persistent CTAs of 256 threads, at most four per SM (the
 // TMEM columns and the shared memory request both allow four), each holding
-// 128 TMEM columns for its lifetime.  Thread 0 issues the MMAs and commits
-// them to an mbarrier.  Every wait on the mbarrier is bounded in time; when
-// the bound runs out the CTA records DERR_TC_WAIT, waits (bounded) once more
-// for its MMA, frees its TMEM and returns.
+// 128 TMEM columns for its lifetime.  Producer warps load tile k+1 into one
+// buffer while the consumer warps run tile k from the other (full/empty
+// mbarriers per buffer); consumer thread 0 issues the MMAs and commits them
+// to an mbarrier.  Every mbarrier wait is bounded in time; when a bound runs
+// out the group stops (decided by a barrier-OR over its threads), the CTA
+// records DERR_TC_WAIT, waits (bounded) once more for its MMA, frees its
+// TMEM and returns.
 #include <algorithm>
 #include <cstdint>
 
@@ -40,11 +43,11 @@
 namespace nnm {
 namespace {
 
-constexpr int TC_THREADS = 128;
+constexpr int TC_THREADS = 256;                // consumers (warps 0-3) + producers (warps 4-7)
 constexpr uint32_t TC_SLOTS = 128;             // M = N = 128: one TMEM lane and one column per slot
 constexpr uint32_t TC_COLS = 128;              // TMEM columns held by a CTA
 constexpr uint32_t TC_SMEM_FLOOR = 50 * 1024;  // keeps residency at <= 4 CTAs per SM (4 x 128 columns)
-constexpr uint32_t TC_MAX_KQ = 1024;
+constexpr uint32_t TC_MAX_KQ = 768;              // two tile buffers of 128 x kq bytes fit in shared memory
 constexpr uint64_t TC_WAIT_NS = 1000000000ull;  // 1 s
 constexpr uint32_t NO_SLOT = 0xffffffffu;
 
@@ -113,38 +116,106 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         : "memory");
 }
 
-struct TcShared {
-    uint64_t mbar;
-    uint32_t tmem;
+// Tile header of one buffer, written by the producers, read by the consumers.
+struct TileHdr {
+    uint32_t t, lgB, nrows, pad;
     uint32_t row[8], nn[8], S[8], any[8];
 };
 
-// Shared memory: the slot vectors (128 x kq bytes, canonical K-major
-// layout: 8-slot groups of kq/16 core matrices), then per-slot arrays.
+struct TcShared {
+    uint64_t mma_bar;           // MMA completion (tcgen05.commit)
+    uint64_t full[2], empty[2];  // tile buffer b loaded / released
+    uint32_t tmem;
+    TileHdr hdr[2];
+};
+
+// Shared memory of one tile buffer: the slot vectors (128 x kq bytes,
+// canonical K-major layout: 8-slot groups of kq/16 core matrices), then the
+// per-slot arrays.  Two buffers.
 __host__ __device__ constexpr size_t tc_vec_bytes(uint32_t kq) { return (size_t)TC_SLOTS * kq; }
-__host__ __device__ constexpr size_t tc_smem_bytes(uint32_t kq) {
-    return tc_vec_bytes(kq) + (size_t)TC_SLOTS * (5 * 4 + 8) + 1024;
+__host__ __device__ constexpr size_t tc_buf_bytes(uint32_t kq) {
+    return (tc_vec_bytes(kq) + (size_t)TC_SLOTS * (5 * 4 + 8) + 1023) & ~(size_t)1023;
+}
+__host__ __device__ constexpr size_t tc_smem_bytes(uint32_t kq) { return 2 * tc_buf_bytes(kq) + 1024; }
+
+struct SlotBuf {
+    unsigned char* vec;
+    uint32_t* ids;
+    float* kth;
+    uint32_t* nrm;
+    uint32_t* cnt;  // pass 0: counts; pass 1: bucket cursors
+    uint32_t* grp;
+    unsigned long long* base;
+};
+
+__device__ __forceinline__ SlotBuf slot_buf(unsigned char* smem, uint32_t kq, uint32_t b) {
+    unsigned char* p = smem + b * tc_buf_bytes(kq);
+    SlotBuf s;
+    s.vec = p;
+    s.ids = reinterpret_cast<uint32_t*>(p + tc_vec_bytes(kq));
+    s.kth = reinterpret_cast<float*>(s.ids + TC_SLOTS);
+    s.nrm = reinterpret_cast<uint32_t*>(s.kth + TC_SLOTS);
+    s.cnt = s.nrm + TC_SLOTS;
+    s.grp = s.cnt + TC_SLOTS;
+    s.base = reinterpret_cast<unsigned long long*>(s.grp + TC_SLOTS);
+    return s;
 }
 
+// Barriers of one 128-thread group (producers: 1, consumers: 2).
+constexpr uint32_t BAR_PROD = 1, BAR_CONS = 2;
+
+__device__ __forceinline__ void group_sync(uint32_t id) {
+    asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory");
+}
+
+// Barrier of the group that also ORs a predicate over its 128 threads, so
+// that a decision taken after per-thread bounded waits is the same in every
+// thread of the group.
+__device__ __forceinline__ bool group_any(uint32_t id, bool p) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(id)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    uint64_t state;
+    asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(state) : "r"(bar) : "memory");
+    asm volatile("" ::"l"(state));  // the arrival state is not needed
+}
+
+// Persistent CTAs of 256 threads in two groups over two tile buffers:
+//   producers (warps 4-7): for tile k, wait until buffer k%2 is released,
+//     write its header and slot metadata, gather the slot vectors with
+//     cp.async, then arrive on full[k%2];
+//   consumers (warps 0-3, TMEM lanes 0-127): wait for full[k%2], run the
+//     MMA chain (thread 0) and the epilogue, write the counts, then arrive on
+//     empty[k%2].
+// So the loads of tile k+1 overlap the MMA and epilogue of tile k.  Every
+// mbarrier wait is bounded; a group decides to stop with a barrier-OR over
+// its threads, and the other group then times out on its next wait.
 template <int PASS>
-__global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
+__global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ TcShared sh;
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t kq = a.kq, nchunk = kq >> 4, gbytes = nchunk * 128;
-    unsigned char* vec = smem;
-    uint32_t* s_ids = reinterpret_cast<uint32_t*>(smem + tc_vec_bytes(kq));
-    float* s_kth = reinterpret_cast<float*>(s_ids + TC_SLOTS);
-    uint32_t* s_nrm = reinterpret_cast<uint32_t*>(s_kth + TC_SLOTS);
-    uint32_t* s_cnt = s_nrm + TC_SLOTS;  // pass 0: counts; pass 1: bucket cursors
-    uint32_t* s_grp = s_cnt + TC_SLOTS;
-    unsigned long long* s_base = reinterpret_cast<unsigned long long*>(s_grp + TC_SLOTS);
+    const uint32_t mma_bar = smem_u32(&sh.mma_bar);
 
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sh.mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mma_bar));
+        for (int b = 0; b < 2; b++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(smem_u32(&sh.full[b])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(smem_u32(&sh.empty[b])));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (tid < 8) sh.any[tid] = 0;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sh.tmem)),
                      "r"(TC_COLS));
@@ -154,8 +225,6 @@ __global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = sh.tmem;
-    const uint32_t bar = smem_u32(&sh.mbar);
-    const uint32_t vbase = smem_u32(vec);
 
     // pass 0 joins every row of tiers 0-3; pass 1 only the rows that pass 0
     // found to have proposals
@@ -168,176 +237,215 @@ __global__ void __launch_bounds__(TC_THREADS) k_join_tc(JoinArgs a) {
         nt[t] = (rcount[t] + (8u >> t) - 1) >> (3 - t);
         total += nt[t];
     }
-    uint32_t phase = 0, cmps = 0;
-    unsigned long long sum_s = 0;
-    bool failed = false;
+    bool failed = false, mma_pending = false;
+    uint32_t mma_phase = 0;
 
-    for (uint32_t tile = blockIdx.x; tile < total; tile += gridDim.x) {
-        uint32_t t = 0, lt = tile;
-        while (t < 3 && lt >= nt[t]) {
-            lt -= nt[t];
-            t++;
-        }
-        const uint32_t lgB = 4 + t, B = 1u << lgB, RT = 8u >> t;
-        const uint32_t first = lt * RT, nrows = min(RT, rcount[t] - first);
-        if (tid < nrows) {
-            const uint32_t row = rlist[(size_t)t * a.n + first + tid];
-            const uint32_t nn = a.newlen[row], S = nn + a.oldlen[row];
-            sh.row[tid] = row;
-            sh.nn[tid] = nn;
-            sh.S[tid] = S;
-            sum_s += S;
-        }
-        __syncthreads();
-        // slot metadata, thread = slot
-        {
-            const uint32_t r = tid >> lgB, q = tid & (B - 1);
-            uint32_t e = NO_SLOT;
-            if (r < nrows && q < sh.S[r]) {
-                const uint32_t row = sh.row[r], nn = sh.nn[r];
-                e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
-                const uint32_t id = e & LID_MASK;
-                s_kth[tid] = a.pdist[(size_t)id * a.K + a.K - 1];
-                s_nrm[tid] = a.nrm[id];
-                s_grp[tid] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
-                s_cnt[tid] = 0;
-                if (PASS == 1) {
-                    const uint32_t c = a.cntpos[(size_t)row * a.caps + q];
-                    s_base[tid] = c ? a.boff[id] + atomicAdd(&a.bcur[id], c) : 0ull;
+    if (warp >= 4) {
+        // ---------------- producers ----------------
+        const uint32_t ptid = tid - 128;
+        unsigned long long sum_s = 0;
+        for (uint32_t k = 0;; k++) {
+            const uint32_t tile = blockIdx.x + k * gridDim.x;
+            if (tile >= total) break;
+            const uint32_t b = k & 1, use = k >> 1;
+            if (use > 0) {
+                const bool ok = mbar_wait_bounded(smem_u32(&sh.empty[b]), (use - 1) & 1);
+                if (group_any(BAR_PROD, !ok)) {
+                    failed = true;
+                    break;
                 }
             }
-            s_ids[tid] = e;
-        }
-        __syncthreads();
-        // gather: 16-byte chunk c of slot s -> group s/8, core matrix c, row s%8
-        for (uint32_t i = tid; i < TC_SLOTS * nchunk; i += TC_THREADS) {
-            const uint32_t r8 = i & 7, rest = i >> 3, c = rest % nchunk, g = rest / nchunk, s = g * 8 + r8;
-            const uint32_t e = s_ids[s];
-            if (e != NO_SLOT) cp_async16(vbase + g * gbytes + c * 128 + r8 * 16, a.xq + (size_t)(e & LID_MASK) * kq + c * 16);
-        }
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // cp.async writes -> tensor core reads
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            for (uint32_t k = 0; k < nchunk / 2; k++) {
-                const uint64_t desc = smem_desc(vbase + k * 256, 128, gbytes);
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-                    "l"(desc), "l"(desc), "r"(IDESC_U8), "r"(k), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            uint32_t t = 0, lt = tile;
+            while (t < 3 && lt >= nt[t]) {
+                lt -= nt[t];
+                t++;
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                         : "memory");
+            const uint32_t lgB = 4 + t, B = 1u << lgB, RT = 8u >> t;
+            const uint32_t first = lt * RT, nrows = min(RT, rcount[t] - first);
+            TileHdr& H = sh.hdr[b];
+            const SlotBuf S = slot_buf(smem, kq, b);
+            if (ptid == 0) {
+                H.t = t;
+                H.lgB = lgB;
+                H.nrows = nrows;
+            }
+            if (ptid < 8) H.any[ptid] = 0;
+            if (ptid < nrows) {
+                const uint32_t row = rlist[(size_t)t * a.n + first + ptid];
+                const uint32_t nn = a.newlen[row], Sr = nn + a.oldlen[row];
+                H.row[ptid] = row;
+                H.nn[ptid] = nn;
+                H.S[ptid] = Sr;
+                sum_s += Sr;
+            }
+            group_sync(BAR_PROD);
+            {  // slot metadata, ptid = slot
+                const uint32_t r = ptid >> lgB, q = ptid & (B - 1);
+                uint32_t e = NO_SLOT;
+                if (r < nrows && q < H.S[r]) {
+                    const uint32_t row = H.row[r], nn = H.nn[r];
+                    e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
+                    const uint32_t id = e & LID_MASK;
+                    S.kth[ptid] = a.pdist[(size_t)id * a.K + a.K - 1];
+                    S.nrm[ptid] = a.nrm[id];
+                    S.grp[ptid] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
+                    S.cnt[ptid] = 0;
+                    if (PASS == 1) {
+                        const uint32_t c = a.cntpos[(size_t)row * a.caps + q];
+                        S.base[ptid] = c ? a.boff[id] + atomicAdd(&a.bcur[id], c) : 0ull;
+                    }
+                }
+                S.ids[ptid] = e;
+            }
+            group_sync(BAR_PROD);
+            // gather: 16-byte chunk c of slot s -> group s/8, core matrix c, row s%8
+            const uint32_t vbase = smem_u32(S.vec);
+            for (uint32_t i = ptid; i < TC_SLOTS * nchunk; i += 128) {
+                const uint32_t r8 = i & 7, rest = i >> 3, c = rest % nchunk, g = rest / nchunk, sl = g * 8 + r8;
+                const uint32_t e = S.ids[sl];
+                if (e != NO_SLOT)
+                    cp_async16(vbase + g * gbytes + c * 128 + r8 * 16, a.xq + (size_t)(e & LID_MASK) * kq + c * 16);
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // cp.async writes -> tensor core reads
+            mbar_arrive(smem_u32(&sh.full[b]));
         }
-        const bool ok_wait = mbar_wait_bounded(bar, phase);
-        if (__syncthreads_or(!ok_wait)) {
-            failed = true;
-            break;
+        if (PASS == 0) {
+            for (int o = 16; o > 0; o >>= 1) sum_s += __shfl_xor_sync(0xffffffffu, sum_s, o);
+            if (lane == 0 && sum_s) {
+                atomicAdd(&a.ctr->sum_s, sum_s);
+                atomicAdd(&a.ctr->sum_s_tc, sum_s);
+            }
         }
-        phase ^= 1u;
-        asm volatile("tcgen05.fence::after_thread_sync;");
+    } else {
+        // ---------------- consumers ----------------
+        uint32_t cmps = 0;
+        for (uint32_t k = 0;; k++) {
+            const uint32_t tile = blockIdx.x + k * gridDim.x;
+            if (tile >= total) break;
+            const uint32_t b = k & 1, use = k >> 1;
+            const bool okf = mbar_wait_bounded(smem_u32(&sh.full[b]), use & 1);
+            if (group_any(BAR_CONS, !okf)) {
+                failed = true;
+                break;
+            }
+            const TileHdr& H = sh.hdr[b];
+            const SlotBuf S = slot_buf(smem, kq, b);
+            const uint32_t t = H.t, lgB = H.lgB, nrows = H.nrows, B = 1u << lgB;
+            if (tid == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t vbase = smem_u32(S.vec);
+                for (uint32_t kk = 0; kk < nchunk / 2; kk++) {
+                    const uint64_t desc = smem_desc(vbase + kk * 256, 128, gbytes);
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                        "l"(desc), "l"(desc), "r"(IDESC_U8), "r"(kk), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 mma_bar)
+                             : "memory");
+            }
+            const bool okm = mbar_wait_bounded(mma_bar, mma_phase);
+            if (group_any(BAR_CONS, !okm)) {
+                failed = true;
+                mma_pending = true;
+                break;
+            }
+            mma_phase ^= 1u;
+            asm volatile("tcgen05.fence::after_thread_sync;");
 
-        // epilogue: this thread is slot b = tid (TMEM lane tid)
-        const uint32_t e_b = s_ids[tid];
-        const bool valid_b = e_b != NO_SLOT;
-        const uint32_t r_b = tid >> lgB, q_b = tid & (B - 1);
-        const uint32_t nn_b = valid_b ? sh.nn[r_b] : 0u, S_b = valid_b ? sh.S[r_b] : 0u;
-        const uint32_t row_b = valid_b ? sh.row[r_b] : 0u;
-        const float kth_b = s_kth[tid];
-        const uint32_t nrm_b = s_nrm[tid], grp_b = s_grp[tid];
-        const uint32_t blk = tid & ~(B - 1);
-        uint32_t cb = 0;
-        const uint32_t c_first = B >= 32 ? ((warp * 32) & ~(B - 1)) : warp * 32;
-        for (uint32_t c0 = c_first; c0 <= warp * 32; c0 += 32) {
-            // columns a of a pair are new-list entries: a < blk + nn_b; the
-            // bound is made warp-uniform (lanes of different rows take the max)
-            const int lim = valid_b ? (int)(blk + nn_b) - (int)c0 : 0;
-            const uint32_t jend = (uint32_t)__reduce_max_sync(0xffffffffu, lim < 0 ? 0 : (lim > 32 ? 32 : lim));
-            if (jend == 0) continue;
-            uint32_t v[32];
-            tmem_ld32(tmem + ((warp * 32) << 16) + c0, v);
+            // epilogue: this thread is slot b = tid (TMEM lane tid)
+            const uint32_t e_b = S.ids[tid];
+            const bool valid_b = e_b != NO_SLOT;
+            const uint32_t r_b = tid >> lgB, q_b = tid & (B - 1);
+            const uint32_t nn_b = valid_b ? H.nn[r_b] : 0u, S_b = valid_b ? H.S[r_b] : 0u;
+            const uint32_t row_b = valid_b ? H.row[r_b] : 0u;
+            const float kth_b = S.kth[tid];
+            const uint32_t nrm_b = S.nrm[tid], grp_b = S.grp[tid];
+            const uint32_t blk = tid & ~(B - 1);
+            uint32_t cb = 0;
+            const uint32_t c_first = B >= 32 ? ((warp * 32) & ~(B - 1)) : warp * 32;
+            for (uint32_t c0 = c_first; c0 <= warp * 32; c0 += 32) {
+                // columns a of a pair are new-list entries: a < blk + nn_b; the
+                // bound is made warp-uniform (lanes of different rows take the max)
+                const int lim = valid_b ? (int)(blk + nn_b) - (int)c0 : 0;
+                const uint32_t jend = (uint32_t)__reduce_max_sync(0xffffffffu, lim < 0 ? 0 : (lim > 32 ? 32 : lim));
+                if (jend == 0) continue;
+                uint32_t v[32];
+                tmem_ld32(tmem + ((warp * 32) << 16) + c0, v);
 #pragma unroll
-            for (uint32_t jj = 0; jj < 32; jj++) {
-                if (jj >= jend) break;
-                const uint32_t av = c0 + jj;
-                const uint32_t q_a = av & (B - 1);
-                const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
-                const uint32_t e_a = s_ids[av];
-                const float dd = (float)((int)(s_nrm[av] + nrm_b) - 2 * (int)v[jj]);
-                uint32_t outer = 0, inner = 0;
-                const bool ok = pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, s_grp[av], grp_b, outer, inner);
-                const float kth_a = s_kth[av];
-                if (PASS == 0) {
-                    cmps += ok;
-                    cb += (ok && dd < kth_b);
-                    const unsigned m = __ballot_sync(0xffffffffu, ok && dd < kth_a);
-                    if (m && lane == 0) atomicAdd(&s_cnt[av], (uint32_t)__popc(m));
-                } else {
-                    const uint32_t pidx = outer * S_b + inner;
-                    const bool pa = ok && dd < kth_a;
-                    const unsigned m = __ballot_sync(0xffffffffu, pa);
-                    if (m) {
-                        const uint32_t leader = __ffs(m) - 1;
-                        uint32_t base = 0;
-                        if (lane == leader) base = atomicAdd(&s_cnt[av], (uint32_t)__popc(m));
-                        base = __shfl_sync(0xffffffffu, base, leader);
-                        if (pa) {
-                            const unsigned long long slot = s_base[av] + base + __popc(m & ((1u << lane) - 1u));
-                            a.bucket[slot] =
-                                Prop{dd, e_b, prop_key(a.fast_key, row_b, pidx, e_b & LID_MASK, outer == q_a ? 0u : 1u)};
+                for (uint32_t jj = 0; jj < 32; jj++) {
+                    if (jj >= jend) break;
+                    const uint32_t av = c0 + jj;
+                    const uint32_t q_a = av & (B - 1);
+                    const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
+                    const uint32_t e_a = S.ids[av];
+                    const float dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[jj]);
+                    uint32_t outer = 0, inner = 0;
+                    const bool ok =
+                        pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, S.grp[av], grp_b, outer, inner);
+                    const float kth_a = S.kth[av];
+                    if (PASS == 0) {
+                        cmps += ok;
+                        cb += (ok && dd < kth_b);
+                        const unsigned m = __ballot_sync(0xffffffffu, ok && dd < kth_a);
+                        if (m && lane == 0) atomicAdd(&S.cnt[av], (uint32_t)__popc(m));
+                    } else {
+                        const uint32_t pidx = outer * S_b + inner;
+                        const bool pa = ok && dd < kth_a;
+                        const unsigned m = __ballot_sync(0xffffffffu, pa);
+                        if (m) {
+                            const uint32_t leader = __ffs(m) - 1;
+                            uint32_t base = 0;
+                            if (lane == leader) base = atomicAdd(&S.cnt[av], (uint32_t)__popc(m));
+                            base = __shfl_sync(0xffffffffu, base, leader);
+                            if (pa) {
+                                const unsigned long long slot = S.base[av] + base + __popc(m & ((1u << lane) - 1u));
+                                a.bucket[slot] = Prop{
+                                    dd, e_b, prop_key(a.fast_key, row_b, pidx, e_b & LID_MASK, outer == q_a ? 0u : 1u)};
+                            }
+                        }
+                        if (ok && dd < kth_b) {
+                            const unsigned long long slot = S.base[tid] + atomicAdd(&S.cnt[tid], 1u);
+                            a.bucket[slot] = Prop{
+                                dd, e_a, prop_key(a.fast_key, row_b, pidx, e_a & LID_MASK, outer == q_b ? 0u : 1u)};
                         }
                     }
-                    if (ok && dd < kth_b) {
-                        const unsigned long long slot = s_base[tid] + atomicAdd(&s_cnt[tid], 1u);
-                        a.bucket[slot] =
-                            Prop{dd, e_a, prop_key(a.fast_key, row_b, pidx, e_a & LID_MASK, outer == q_b ? 0u : 1u)};
+                }
+            }
+            if (PASS == 0 && cb) atomicAdd(&S.cnt[tid], cb);
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            group_sync(BAR_CONS);
+            if (PASS == 0) {
+                if (valid_b) {
+                    const uint32_t c = S.cnt[tid];
+                    a.cntpos[(size_t)row_b * a.caps + q_b] = (uint16_t)c;
+                    if (c) {
+                        atomicAdd(&a.bcnt[e_b & LID_MASK], c);
+                        sh.hdr[b].any[r_b] = 1;
                     }
                 }
-            }
-        }
-        if (PASS == 0 && cb) atomicAdd(&s_cnt[tid], cb);
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
-        if (PASS == 0) {
-            if (valid_b) {
-                const uint32_t c = s_cnt[tid];
-                a.cntpos[(size_t)row_b * a.caps + q_b] = (uint16_t)c;
-                if (c) {
-                    atomicAdd(&a.bcnt[e_b & LID_MASK], c);
-                    sh.any[r_b] = 1;
+                group_sync(BAR_CONS);
+                if (warp == 0) {  // rows with proposals go to the emit pass's list
+                    const bool has = lane < nrows && H.any[lane];
+                    const unsigned m = __ballot_sync(0xffffffffu, has);
+                    uint32_t base = 0;
+                    if (m && lane == 0) base = atomicAdd(&a.ctr->nemit[t], (uint32_t)__popc(m));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (has) a.emit_rows[(size_t)t * a.n + base + __popc(m & ((1u << lane) - 1u))] = H.row[lane];
                 }
             }
-            __syncthreads();
-            if (warp == 0) {  // rows with proposals go to the emit pass's list
-                const bool has = lane < nrows && sh.any[lane];
-                const unsigned m = __ballot_sync(0xffffffffu, has);
-                uint32_t base = 0;
-                if (m && lane == 0) base = atomicAdd(&a.ctr->nemit[t], (uint32_t)__popc(m));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (has) a.emit_rows[(size_t)t * a.n + base + __popc(m & ((1u << lane) - 1u))] = sh.row[lane];
-                if (lane < 8) sh.any[lane] = 0;
-            }
+            mbar_arrive(smem_u32(&sh.empty[b]));
         }
-        __syncthreads();
-    }
-
-    if (PASS == 0) {
-        for (int o = 16; o > 0; o >>= 1) {
-            cmps += __shfl_xor_sync(0xffffffffu, cmps, o);
-            sum_s += __shfl_xor_sync(0xffffffffu, sum_s, o);
-        }
-        if (lane == 0 && cmps) atomicAdd(&a.ctr->ncmps, (unsigned long long)cmps);
-        if (lane == 0 && sum_s) {
-            atomicAdd(&a.ctr->sum_s, sum_s);
-            atomicAdd(&a.ctr->sum_s_tc, sum_s);
+        if (PASS == 0) {
+            for (int o = 16; o > 0; o >>= 1) cmps += __shfl_xor_sync(0xffffffffu, cmps, o);
+            if (lane == 0 && cmps) atomicAdd(&a.ctr->ncmps, (unsigned long long)cmps);
         }
     }
-    if (failed) {
-        if (tid == 0) atomicOr(a.tc_err, (unsigned)DERR_TC_WAIT);
-        mbar_wait_bounded(bar, phase);  // the MMA may still write TMEM
-    }
+    if (failed && (tid & 127) == 0) atomicOr(a.tc_err, (unsigned)DERR_TC_WAIT);
+    if (mma_pending) mbar_wait_bounded(mma_bar, mma_phase);  // the MMA may still write TMEM
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 0) {
@@ -387,7 +495,7 @@ int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
     const uint32_t kq = (g.d + 31) & ~31u;
     const char* why = nullptr;
     if (g.metric != L2) why = "the tensor-core join needs the L2 metric";
-    else if (kq > TC_MAX_KQ) why = "the tensor-core join takes d <= 1024";
+    else if (kq > TC_MAX_KQ) why = "the tensor-core join takes d <= 768";
     if (!why) {
         NNM_CUDA_TRY(s.xq.ensure((size_t)g.n_cap * kq));
         NNM_CUDA_TRY(s.nrm.ensure((size_t)g.n_cap * 4));

@@ -702,10 +702,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32) k_merge(MergeArgs a) {
     __shared__ MEnt sm[MERGE_WARPS][64];
     __shared__ MEnt kept[MERGE_WARPS][32];
     __shared__ MEnt buf[MERGE_WARPS][32];
-    __shared__ unsigned int blk_flags;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) blk_flags = 0;
-    __syncthreads();
     const uint32_t t = blockIdx.x * MERGE_WARPS + w;
     uint32_t nfl = 0;
     if (t < a.n) {
@@ -777,9 +774,22 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32) k_merge(MergeArgs a) {
         }
         if (lane == 0) a.nflag[t] = (uint8_t)nfl;
     }
-    if (lane == 0 && nfl) atomicAdd(&blk_flags, nfl);
+}
+
+// Total of the per-row flag counts (the warps of k_merge finish unevenly, so
+// they do not meet at a block barrier to add them up).
+__global__ void k_sum_flags(const uint8_t* nflag, uint32_t n, IterCounters* ctr) {
+    __shared__ unsigned int part[8];
+    unsigned int s = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += nflag[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
     __syncthreads();
-    if (threadIdx.x == 0 && blk_flags) atomicAdd(&a.ctr->flags, (unsigned long long)blk_flags);
+    if (threadIdx.x == 0) {
+        unsigned int b = 0;
+        for (int w = 0; w < 8; w++) b += part[w];
+        if (b) atomicAdd(&ctr->flags, (unsigned long long)b);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1044,6 +1054,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                      P<Prop>(ws.bucket), P<uint8_t>(ws.nflag), ctr};
         if (ctx.prof) cudaEventRecord(ctx.ev[3], st);
         k_merge<<<(n + MERGE_WARPS - 1) / MERGE_WARPS, MERGE_WARPS * 32, 0, st>>>(ma); count_launch();
+        k_sum_flags<<<std::min<unsigned>((n + 255) / 256, (unsigned)nsm * 4), 256, 0, st>>>(P<uint8_t>(ws.nflag), n, ctr); count_launch();
         if (ctx.prof) cudaEventRecord(ctx.ev[4], st);
         NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
         NNM_CUDA_TRY(cudaMemcpyAsync(&ctx.h_counters->rand_draws, d_tot, 8, cudaMemcpyDeviceToHost, st));
