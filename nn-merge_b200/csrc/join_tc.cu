@@ -33,7 +33,10 @@
 // records DERR_TC_WAIT, waits (bounded) once more for its MMA, frees its
 // TMEM and returns.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
+
+#include <cuda_bf16.h>
 
 #include "../../include/nnm.h"
 #include "nnm_engine.h"
@@ -74,6 +77,15 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 // Instruction descriptor of kind::i8: D = S32 (bits 4-5 = 2), A = B = u8
 // (bits 7-9 = 0, 10-12 = 0), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
 constexpr uint32_t IDESC_U8 = (2u << 4) | ((TC_SLOTS >> 3) << 17) | ((TC_SLOTS >> 4) << 24);
+// Instruction descriptor of kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16
+// (bits 7-9 = 1, 10-12 = 1), both K-major.
+constexpr uint32_t IDESC_BF16 = (1u << 4) | (1u << 7) | (1u << 10) | ((TC_SLOTS >> 3) << 17) | ((TC_SLOTS >> 4) << 24);
+
+// The reference's sequential FP32 distance of rows i and j: the BF16 tier's
+// recheck, one non-inlined copy for every call site.
+__device__ __noinline__ float exact_l2(const float* x, uint32_t dp, uint32_t i, uint32_t j) {
+    return dist_seq<L2>(x + (size_t)i * dp, x + (size_t)j * dp, (int)dp);
+}
 
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     uint32_t ok;
@@ -200,7 +212,7 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 // So the loads of tile k+1 overlap the MMA and epilogue of tile k.  Every
 // mbarrier wait is bounded; a group decides to stop with a barrier-OR over
 // its threads, and the other group then times out on its next wait.
-template <int PASS>
+template <int PASS, int KIND>
 __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ TcShared sh;
@@ -335,13 +347,22 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             if (tid == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint32_t vbase = smem_u32(S.vec);
-                for (uint32_t kk = 0; kk < nchunk / 2; kk++) {
+                for (uint32_t kk = 0; kk < nchunk / 2; kk++) {  // 32 bytes of K per instruction
                     const uint64_t desc = smem_desc(vbase + kk * 256, 128, gbytes);
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-                        "l"(desc), "l"(desc), "r"(IDESC_U8), "r"(kk), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                    if (KIND == 0)
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                tmem),
+                            "l"(desc), "l"(desc), "r"(IDESC_U8), "r"(kk), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                    else
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                tmem),
+                            "l"(desc), "l"(desc), "r"(IDESC_BF16), "r"(kk), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  mma_bar)
@@ -382,7 +403,17 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                     const uint32_t q_a = av & (B - 1);
                     const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
                     const uint32_t e_a = S.ids[av];
-                    const float dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[jj]);
+                    float dd;
+                    if (KIND == 0) {
+                        dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[jj]);
+                    } else {
+                        // approximate distance; pairs it cannot rule out get
+                        // the reference's exact sum
+                        const float ns = __uint_as_float(S.nrm[av]) + __uint_as_float(nrm_b);
+                        dd = ns - 2.f * __uint_as_float(v[jj]);
+                        if (pv && dd - a.err_c * ns < fmaxf(S.kth[av], kth_b))
+                            dd = exact_l2(a.x, a.dp, e_a & LID_MASK, e_b & LID_MASK);
+                    }
                     uint32_t outer = 0, inner = 0;
                     const bool ok =
                         pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, S.grp[av], grp_b, outer, inner);
@@ -485,6 +516,37 @@ __global__ void k_quantize(const float* x, uint32_t n, uint32_t d, uint32_t dp, 
     }
 }
 
+// Warp per vector: the BF16 copy (round to nearest even, zero padded to kq
+// bytes) and the squared norm (double sum, rounded to float).  Flags rows
+// the BF16 bound does not cover: non-finite components, or nonzero ones
+// outside [2^-60, 2^50] (products must stay normal and sums finite).
+__global__ void k_to_bf16(const float* x, uint32_t n, uint32_t d, uint32_t dp, uint32_t kq, __nv_bfloat16* xb,
+                          uint32_t* nrm, unsigned* bad) {
+    const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float* src = x + (size_t)row * dp;
+    __nv_bfloat16* dst = xb + (size_t)row * (kq / 2);
+    double s = 0.0;
+    bool ok = true;
+    for (uint32_t k = lane; k < kq / 2; k += 32) {
+        float v = 0.f;
+        if (k < d) {
+            v = src[k];
+            const float m = fabsf(v);
+            if (!(m <= 0x1p50f) || (m != 0.f && m < 0x1p-60f)) ok = false;
+        }
+        dst[k] = __float2bfloat16_rn(v);
+        s += (double)v * (double)v;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const bool all_ok = __all_sync(0xffffffffu, ok);
+    if (lane == 0) {
+        nrm[row] = __float_as_uint((float)s);
+        if (!all_ok) atomicOr(bad, 1u);
+    }
+}
+
 }  // namespace
 
 int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
@@ -509,27 +571,62 @@ int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
         NNM_CUDA_TRY(cudaMemcpyAsync(h, flags, 8, cudaMemcpyDeviceToHost, ctx.stream));
         NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
         // every squared distance is at most |a|^2 + |b|^2 for non-negative vectors
-        if (h[0]) why = "the tensor-core join needs integer components in [0, 255]";
-        else if (2ull * h[1] >= (1ull << 24)) why = "the tensor-core join needs squared norms below 2^23";
-    }
-    if (why) {
-        if (g.join_kernel == NNM_JOIN_TENSOR) {
-            ctx.last_error = why;
-            return 1;  // NNM_ERR_INVALID
+        if (!h[0] && 2ull * h[1] < (1ull << 24)) {
+            g.xq = s.xq.as<uint8_t>();
+            g.nrm = s.nrm.as<uint32_t>();
+            g.kq = kq;
+            g.tc_kind = 0;
+            return 0;
         }
-        return 0;
+        // other data: BF16 Gram matrices with the FP32 recheck
+        const uint32_t kqb = 2 * ((g.d + 15) & ~15u);
+        if (kqb > TC_MAX_KQ) {
+            why = "the BF16 tensor-core join takes d <= 384";
+        } else {
+            NNM_CUDA_TRY(s.xq.ensure((size_t)g.n_cap * kqb));
+            NNM_CUDA_TRY(cudaMemsetAsync(m.p, 0, 16, ctx.stream));
+            k_to_bf16<<<(g.n_cap + 7) / 8, 256, 0, ctx.stream>>>(g.x, g.n_cap, g.d, g.dp, kqb,
+                                                                 s.xq.as<__nv_bfloat16>(), s.nrm.as<uint32_t>(), flags); count_launch();
+            NNM_CUDA_TRY(cudaMemcpyAsync(h, flags, 4, cudaMemcpyDeviceToHost, ctx.stream));
+            NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+            if (h[0]) {
+                why = "the BF16 tensor-core join needs finite components with magnitudes in [2^-60, 2^50]";
+            } else {
+                g.xq = s.xq.as<uint8_t>();
+                g.nrm = s.nrm.as<uint32_t>();
+                g.kq = kqb;
+                g.tc_kind = 1;
+                // |computed - reference| <= err_c (|a|^2 + |b|^2): BF16 inputs
+                // (2 x 2^-9 relative per product), FP32 accumulation of d
+                // terms (d 2^-22, truncating adds allowed), the float norms
+                // and the final two operations (2^-21), and the reference's
+                // own sequential sum ((d + 2) 2^-23 of a distance <= 2(|a|^2 +
+                // |b|^2)); |a||b| <= (|a|^2 + |b|^2) / 2; a 1.25 safety factor
+                const double dd = (double)g.d;
+                g.err_c = (float)(1.25 * (std::ldexp(1.0, -8) + std::ldexp(1.0, -18) + (2 * dd + 4) * std::ldexp(1.0, -22) +
+                                          std::ldexp(1.0, -21)));
+                return 0;
+            }
+        }
     }
-    g.xq = s.xq.as<uint8_t>();
-    g.nrm = s.nrm.as<uint32_t>();
-    g.kq = kq;
+    if (why && g.join_kernel == NNM_JOIN_TENSOR) {
+        ctx.last_error = why;
+        return 1;  // NNM_ERR_INVALID
+    }
     return 0;
 }
 
-cudaError_t tc_set_attributes(uint32_t kq) {
+cudaError_t tc_set_attributes(uint32_t kq, uint32_t kind) {
     const int bytes = (int)std::max<size_t>(tc_smem_bytes(kq), TC_SMEM_FLOOR);
-    cudaError_t e = cudaFuncSetAttribute(k_join_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e;
+    if (kind == 0) {
+        e = cudaFuncSetAttribute(k_join_tc<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+        return cudaFuncSetAttribute(k_join_tc<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    }
+    e = cudaFuncSetAttribute(k_join_tc<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_join_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return cudaFuncSetAttribute(k_join_tc<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, int nsm, cudaStream_t st) {
@@ -538,8 +635,13 @@ cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, 
     if (!tiles) return cudaSuccess;
     const unsigned grid = std::min<unsigned>(tiles, (unsigned)nsm * 4);
     const size_t bytes = std::max<size_t>(tc_smem_bytes(ja.kq), TC_SMEM_FLOOR);
-    if (pass == 0) k_join_tc<0><<<grid, TC_THREADS, bytes, st>>>(ja);
-    else k_join_tc<1><<<grid, TC_THREADS, bytes, st>>>(ja);
+    if (ja.tc_kind == 0) {
+        if (pass == 0) k_join_tc<0, 0><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else k_join_tc<1, 0><<<grid, TC_THREADS, bytes, st>>>(ja);
+    } else {
+        if (pass == 0) k_join_tc<0, 1><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else k_join_tc<1, 1><<<grid, TC_THREADS, bytes, st>>>(ja);
+    }
     count_launch();
     return cudaGetLastError();
 }

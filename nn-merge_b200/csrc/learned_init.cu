@@ -417,7 +417,7 @@ int learned_rows(Ctx& ctx, GraphDev& s, const CodeViews& vw, uint32_t leaf) {
     NNM_CUDA_TRY(cudaMemsetAsync(ctx.ws.counters.p, 0, sizeof(IterCounters), ctx.stream));
     RowsArgs ra{s.x, s.dp, s.K, s.metric, s.pid, s.pdist, s.n, vw.leaf_off[leaf], vw.keys, vw.pos, vw.P, vw.nleaf,
                 leaf, vw.n, s.seed, s.phase++, ctx.ws.counters.as<IterCounters>(),
-                DistSrc{s.x, s.dp, s.metric, s.xq, s.nrm, s.kq}};
+                DistSrc{s.x, s.dp, s.metric, s.tc_kind == 0 ? s.xq : nullptr, s.nrm, s.kq}};
     k_learned_rows<<<blocks_for(s.n, IW), IW * 32, 0, ctx.stream>>>(ra); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return check_counters(ctx);
@@ -435,7 +435,7 @@ int learned_cross(Ctx& ctx, GraphDev& g, const CodeViews& vw, const uint32_t* d_
     const uint32_t win = std::max<uint32_t>(1, NCAND / (2 * npair));
     CrossArgsL ca{g.x, g.dp, g.K, g.metric, g.pid, g.cpid, g.pdist, g.cpdist, g.n, g.K - g.cut, g.codes, vw.keys,
                   d_leaf_off, vw.P, vw.nleaf, nview, npair, win, g.seed, g.phase++,
-                  ctx.ws.counters.as<IterCounters>(), DistSrc{g.x, g.dp, g.metric, g.xq, g.nrm, g.kq}};
+                  ctx.ws.counters.as<IterCounters>(), DistSrc{g.x, g.dp, g.metric, g.tc_kind == 0 ? g.xq : nullptr, g.nrm, g.kq}};
     k_learned_cross<<<blocks_for(g.n, IW), IW * 32, 0, ctx.stream>>>(ca); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return check_counters(ctx);

@@ -948,7 +948,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     NNM_CUDA_TRY(ws.tiers.ensure((size_t)n * NTIER * 4 + 16));
     const bool tc = g.xq != nullptr;
     if (tc) {
-        NNM_CUDA_TRY(tc_set_attributes(g.kq));
+        NNM_CUDA_TRY(tc_set_attributes(g.kq, g.tc_kind));
         NNM_CUDA_TRY(ws.erows.ensure((size_t)n * 4 * 4 + 16));
     }
 
@@ -1026,7 +1026,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     P<float>(ws.pd), P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
                     P<uint64_t>(ws.boff), P<Prop>(ws.bucket), ctr,
                     g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error, tc ? P<uint32_t>(ws.erows) : nullptr,
-                    g.fast ? 1u : 0u};
+                    g.fast ? 1u : 0u, g.tc_kind, g.err_c};
         if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
         if (tc) NNM_CUDA_TRY(launch_join_tc(0, ja, ntier, nsm, st));
         if (g.metric == L2) launch_pairs<L2>(ja, ntier, caps, g.dp, nsm, tc, st);

@@ -103,11 +103,14 @@ struct GraphDev {
     uint32_t n_cap = 0, n = 0, K = 0, d = 0, dp = 0;
     int metric = L2;
     const float* x = nullptr;       // n_cap x dp on the device
-    // Tensor-core join (set by tc_prepare when it applies): n_cap x kq u8
-    // vectors, kq = d rounded up to 32 bytes, zero padded, and squared norms.
+    // Tensor-core join (set by tc_prepare when it applies): n_cap x kq bytes
+    // of u8 vectors (kq = d rounded up to 32) or BF16 vectors (kq = 2 x d
+    // rounded up to 16), zero padded, and squared norms.
     const uint8_t* xq = nullptr;
     const uint32_t* nrm = nullptr;
     uint32_t kq = 0;
+    uint32_t tc_kind = 0;  // 0: u8 copy (exact); 1: BF16 copy, float norms, FP32 recheck
+    float err_c = 0.f;     // BF16 distance error bound coefficient
     uint32_t join_kernel = 0;       // nnm_join_kernel
     // Learned initialisation: codes of rows [0, n_cap) and, inside a merge,
     // the parent's code views with this graph's leaf index.

@@ -37,14 +37,17 @@ struct JoinArgs {
     const uint64_t* boff;
     Prop* bucket;
     IterCounters* ctr;
-    // tensor-core join: u8 copy of the vectors (kq bytes a row, zero
-    // padded) and their squared norms; tc != 0 when it takes tiers 0-3
+    // tensor-core join: the operand copy of the vectors (kq bytes a row,
+    // zero padded; u8 or BF16 by tc_kind) and their squared norms (u32
+    // integers for u8, float bits for BF16); tc != 0 when it takes tiers 0-3
     const uint8_t* xq;
     const uint32_t* nrm;
     uint32_t kq, tc;
     unsigned* tc_err;
     uint32_t* emit_rows;  // 4 lists of n rows: rows of tiers 0-3 that have proposals
     uint32_t fast_key;    // tie-break keys from ids instead of list positions (fast tier)
+    uint32_t tc_kind;     // 0: u8 (exact), 1: BF16 with the FP32 recheck
+    float err_c;          // BF16: |approx - reference distance| <= err_c * (|a|^2 + |b|^2)
 };
 
 // Tie-break key of the proposal "target gets `other`" from the join of
@@ -103,7 +106,7 @@ struct GraphDev;
 // every component an integer in [0, 255], every distance below 2^24) and,
 // if so, builds the u8 copy and the norms.  Returns an engine status.
 int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g);
-cudaError_t tc_set_attributes(uint32_t kq);
+cudaError_t tc_set_attributes(uint32_t kq, uint32_t kind);
 // pass 0: per-slot proposal counts; pass 1: proposals into the buckets.
 cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, int nsm, cudaStream_t st);
 

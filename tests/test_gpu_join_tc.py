@@ -1,7 +1,9 @@
-"""The tensor-core local join (u8 Gram matrices on tcgen05) against the FP32
-join: identical graphs, bit for bit, for every builder, both random-draw
-tiers, every list-size tier and ragged dimensions; the selection rule
-(integer components in [0, 255], L2) and its error when forced."""
+"""The tensor-core local join against the FP32 join: identical graphs, bit
+for bit, for every builder, both random-draw tiers, every list-size tier and
+ragged dimensions -- u8 Gram matrices for integer data, BF16 ones with the
+FP32 recheck for other data; the selection rule (L2; integer components in
+[0, 255] for u8; finite, bounded components and d <= 384 for BF16) and its
+error when forced."""
 import numpy as np
 import pytest
 
@@ -93,31 +95,67 @@ def test_extreme_values(ctx):
     same(t, f)
 
 
-def test_auto_picks_tensor_only_when_exact(ctx):
+def test_auto_picks_the_tensor_cores_for_l2(ctx):
+    # integer data -> u8 tier, other finite data -> BF16 tier with the recheck
     x = gaussian_mixture_u8(3000, seed=39)
-    ctx.profile(True)
-    a = ctx.kgraph(x, 10, seed=1)
-    assert ctx.profile_stats()["rows"]["tensor"] > 0
-    ctx.profile(True)
-    xf = x + 0.5
-    b = ctx.kgraph(xf, 10, seed=1)
-    assert ctx.profile_stats()["rows"]["tensor"] == 0
+    for data in (x, x + 0.5):
+        ctx.profile(True)
+        ctx.kgraph(data, 10, seed=1)
+        assert ctx.profile_stats()["rows"]["tensor"] > 0
     ctx.profile(False)
-    assert a["ids"].shape == b["ids"].shape
 
 
-@pytest.mark.parametrize("bad", ["fraction", "negative", "big", "norm"])
-def test_forced_tensor_rejects_inexact_data(ctx, bad):
-    x = gaussian_mixture_u8(2000, d=64, seed=40)
-    if bad == "fraction":
-        x[5, 3] += 0.25
-    elif bad == "negative":
-        x[7, 1] = -1.0
-    elif bad == "big":
-        x[9, 0] = 256.0
+def float_mixture(n, d, seed, unit=False):
+    rng = np.random.default_rng(seed)
+    c = rng.standard_normal((32, d))
+    x = c[rng.integers(0, 32, n)] + 0.35 * rng.standard_normal((n, d))
+    if unit:
+        x /= np.linalg.norm(x, axis=1, keepdims=True)
+    return x.astype(np.float32)
+
+
+@pytest.mark.parametrize("unit", [False, True])
+@pytest.mark.parametrize("rng", ["exact", "fast"])
+def test_bf16_tier_matches_fp32(ctx, unit, rng):
+    x = float_mixture(5000, 96, 50 + unit, unit)
+    t, f, rows = both(ctx, ctx.kgraph, x, 16, seed=3, rng=rng)
+    same(t, f)
+    assert rows["tensor"] > 0
+
+
+def test_bf16_tier_merges_match_fp32(ctx):
+    x = float_mixture(6000, 64, 61) * 37.0
+    t, f, _ = both(ctx, ctx.merge_leaves, x, 20, [1500] * 4, seed=5)
+    same(t, f)
+    t, f, _ = both(ctx, ctx.jmerge, x[:4000], 12, seed=6)
+    same(t, f)
+    t = ctx.hmerge(x[:3000], 10, 8, seed=9, join="tensor")
+    f = ctx.hmerge(x[:3000], 10, 8, seed=9, join="fp32")
+    same(t, f)
+
+
+def test_bf16_tier_ties_and_scales(ctx):
+    # many exact ties (few distinct values) and mixed magnitudes
+    rng = np.random.default_rng(62)
+    x = (rng.integers(-3, 4, size=(4000, 40)) * 0.25).astype(np.float32)
+    x[::7] *= 1e3
+    t, f, _ = both(ctx, ctx.kgraph, x, 12, seed=7)
+    same(t, f)
+
+
+@pytest.mark.parametrize("bad", ["nan", "inf", "huge", "tiny", "wide"])
+def test_forced_tensor_rejects_uncovered_data(ctx, bad):
+    x = float_mixture(2000, 64, 40)
+    if bad == "nan":
+        x[5, 3] = np.nan
+    elif bad == "inf":
+        x[7, 1] = np.inf
+    elif bad == "huge":
+        x[9, 0] = 2.0 ** 60
+    elif bad == "tiny":
+        x[9, 0] = 2.0 ** -70
     else:
-        x = np.full((2000, 300), 255.0, np.float32)  # 2 * |x|^2 >= 2^24
-        x[:, 0] = np.arange(2000) % 256
+        x = float_mixture(2000, 400, 41)  # BF16 tier: d <= 384
     with pytest.raises(NnmError) as e:
         ctx.kgraph(x, 10, seed=1, join="tensor")
     assert e.value.status == 1
