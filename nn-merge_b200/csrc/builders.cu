@@ -451,23 +451,31 @@ static int fast_rows(Ctx& ctx, GraphDev& g, uint32_t row0, uint32_t row1, uint32
     return check_counters(ctx);
 }
 
+// Fast tier: the initial graph of g's rows (learned or random), local ids.
+static int fast_init(Ctx& ctx, GraphDev& g) {
+    const uint32_t n = g.n;
+    int rc;
+    if (g.init == NNM_INIT_LEARNED) {
+        if (g.views) {
+            rc = learned_rows(ctx, g, *g.views, g.view_leaf);
+        } else {
+            CodeViews vw;
+            rc = views_build(ctx, g, {0u, n}, vw);
+            if (!rc) rc = learned_rows(ctx, g, vw, 0);
+        }
+    } else {
+        rc = fast_rows(ctx, g, 0, n, 0, n, 0, nullptr, 0, 0, 0);
+    }
+    if (rc) return rc;
+    g.ncmps += (uint64_t)n * g.K;
+    return 0;
+}
+
 int kgraph_build(Ctx& ctx, GraphDev& g) {
     const uint32_t K = g.K, n = g.n;
     if (g.fast) {
-        int rc;
-        if (g.init == NNM_INIT_LEARNED) {
-            if (g.views) {
-                rc = learned_rows(ctx, g, *g.views, g.view_leaf);
-            } else {
-                CodeViews vw;
-                rc = views_build(ctx, g, {0u, n}, vw);
-                if (!rc) rc = learned_rows(ctx, g, vw, 0);
-            }
-        } else {
-            rc = fast_rows(ctx, g, 0, n, 0, n, 0, nullptr, 0, 0, 0);
-        }
+        int rc = fast_init(ctx, g);
         if (rc) return rc;
-        g.ncmps += (uint64_t)n * K;
         return run_nndescent(ctx, g, MODE_KGRAPH, 0, 0, nullptr, 0);
     }
     const uint32_t per = sds_draws(K + 1, n);
@@ -520,8 +528,35 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
     CodeViews vw;
     const bool learned = g.fast && g.init == NNM_INIT_LEARNED;
     if (learned && (rc = views_build(ctx, g, leaf_off, vw))) return rc;
-    // 1. NN-Descent on every leaf, in place (smerge.cpp:56-68).
-    for (uint32_t l = 0; l < nleaf; l++) {
+    // 1. NN-Descent on every leaf, in place (smerge.cpp:56-68).  The fast
+    // tier runs all leaves in one NN-Descent: each leaf's initial graph holds
+    // only rows of that leaf, reverse lists come from the pools, so no list
+    // ever mixes leaves -- one launch sequence for leaves of any sizes.
+    if (g.fast) {
+        for (uint32_t l = 0; l < nleaf; l++) {
+            GraphDev s = sub_view(g, leaf_off[l], leaf_off[l + 1]);
+            if (learned) {
+                s.views = &vw;
+                s.view_leaf = l;
+            }
+            s.phase = g.phase + l;  // independent draws per leaf
+            if ((rc = fast_init(ctx, s))) return rc;
+            subc += s.ncmps;
+            const size_t cnt = (size_t)s.n * K;
+            k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(s.pid, cnt, leaf_off[l], 0u); count_launch();
+        }
+        g.phase += nleaf;
+        const uint64_t before = g.ncmps;
+        if ((rc = run_nndescent(ctx, g, MODE_KGRAPH, 0, 0, nullptr, 0))) return rc;
+        subc += g.ncmps - before;
+        g.ncmps = before;
+        for (uint32_t l = 0; l < nleaf; l++) {  // InitSGraph: all entries new, group ids
+            const size_t cnt = (size_t)(leaf_off[l + 1] - leaf_off[l]) * K;
+            k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid + (size_t)leaf_off[l] * K, cnt, 0u,
+                                                                  nleaf == 2 ? l : 0u); count_launch();
+        }
+    }
+    for (uint32_t l = 0; l < nleaf && !g.fast; l++) {
         GraphDev s = sub_view(g, leaf_off[l], leaf_off[l + 1]);
         if (learned) {
             s.views = &vw;
