@@ -238,31 +238,17 @@ def main():
         return
 
     import torch
-    import torch.distributed as dist
     import nnm
     from nnm.datasets import gaussian_mixture_u8
+    from nnm.replicas import Replicas
 
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-        pg = True
-
-    def barrier():
-        if pg:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if not pg:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    reps = Replicas("nccl")
+    barrier, max_over_ranks = reps.barrier, reps.max
 
     n, d, k = a.n, a.d, a.k
     sizes = leaf_sizes(n, a.leaves)
-    x = gaussian_mixture_u8(n, d=d, n_centres=a.centres, seed=a.seed + rank)
+    x = gaussian_mixture_u8(n, d=d, n_centres=a.centres, seed=reps.data_seed(a.seed))
     x_dev = torch.from_numpy(x).cuda()
     ids_dev = torch.empty((n, k), dtype=torch.int32, device="cuda")
     dists_dev = torch.empty((n, k), dtype=torch.float32, device="cuda")
@@ -409,8 +395,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     ctx.close()
-    if pg:
-        dist.destroy_process_group()
+    reps.close()
 
 
 if __name__ == "__main__":
