@@ -578,9 +578,15 @@ int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
             g.tc_kind = 0;
             return 0;
         }
-        // other data: BF16 Gram matrices with the FP32 recheck
+        // other data: BF16 Gram matrices with the FP32 recheck, on request
+        // only -- the rigorous BF16 bound (about 2^-8 of |a|^2 + |b|^2)
+        // leaves most candidate pairs inside the recheck band, and the
+        // per-pair exact sums then cost more than the FP32 join (measured
+        // 3-4x slower per iteration on unit-norm 96-d data)
         const uint32_t kqb = 2 * ((g.d + 15) & ~15u);
-        if (kqb > TC_MAX_KQ) {
+        if (g.join_kernel != NNM_JOIN_TENSOR) {
+            why = "auto: FP32 join for non-integer data";
+        } else if (kqb > TC_MAX_KQ) {
             why = "the BF16 tensor-core join takes d <= 384";
         } else {
             NNM_CUDA_TRY(s.xq.ensure((size_t)g.n_cap * kqb));

@@ -95,13 +95,14 @@ def test_extreme_values(ctx):
     same(t, f)
 
 
-def test_auto_picks_the_tensor_cores_for_l2(ctx):
-    # integer data -> u8 tier, other finite data -> BF16 tier with the recheck
+def test_auto_picks_u8_tensor_cores_for_integer_data(ctx):
+    # auto: integer data -> u8 tensor cores; other data -> FP32 (the BF16
+    # tier only when forced)
     x = gaussian_mixture_u8(3000, seed=39)
-    for data in (x, x + 0.5):
+    for data, on_tc in ((x, True), (x + 0.5, False)):
         ctx.profile(True)
         ctx.kgraph(data, 10, seed=1)
-        assert ctx.profile_stats()["rows"]["tensor"] > 0
+        assert (ctx.profile_stats()["rows"]["tensor"] > 0) == on_tc
     ctx.profile(False)
 
 
