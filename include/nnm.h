@@ -49,14 +49,17 @@ typedef enum {
                           random choices, no host-side streams and no ordering of reverse lists */
 } nnm_rng_mode;
 
-/* Kernel of the local join's distance evaluations.  Both give the same
-   graphs bit for bit; the tensor-core join applies when the metric is L2 and
-   every vector component is an integer in [0, 255] (every squared distance
-   then stays below 2^24, where the reference's float sum is exact). */
+/* Kernel of the local join's distance evaluations.  All give the same
+   graphs bit for bit.  The tensor-core join needs the L2 metric; for data
+   whose components are all integers in [0, 255] it computes u8 Gram matrices
+   exactly (every squared distance stays below 2^24, where the reference's
+   float sum is exact); for other finite data (|components| in [2^-60, 2^50],
+   d <= 384) it computes BF16 Gram matrices, rules pairs out with a rigorous
+   error bound and gives every other pair the reference's exact FP32 sum. */
 typedef enum {
-    NNM_JOIN_AUTO = 0,   /* tensor cores when they apply, else FP32 */
+    NNM_JOIN_AUTO = 0,   /* u8 tensor cores for integer data, else FP32 */
     NNM_JOIN_FP32 = 1,   /* FP32 CUDA cores: the reference's sequential sums */
-    NNM_JOIN_TENSOR = 2  /* tensor cores (u8 Gram matrices); NNM_ERR_INVALID when they do not apply */
+    NNM_JOIN_TENSOR = 2  /* tensor cores (u8, else BF16 with the FP32 recheck); NNM_ERR_INVALID when neither applies */
 } nnm_join_kernel;
 
 /* Initial graphs.  NNM_INIT_LEARNED (no counterpart in the reference) needs
@@ -235,6 +238,88 @@ int nnm_mlp_codes(nnm_ctx *ctx, const nnm_mlp *model, const float *x, uint64_t n
                   uint32_t *codes, float *z);
 /* The model NNM_INIT_LEARNED builds use (copied to the device); NULL clears it. */
 int nnm_set_init_model(nnm_ctx *ctx, const nnm_mlp *model);
+
+/* Serving (LySearch::knnSearch's per-query steps, lysearch.cpp:363-437, on a
+ * resident index).  nnm_index_create copies the vectors and the hierarchy
+ * to the device once; nnm_index_search then runs batches of queries, each
+ * with its own beam width (the reference's topk, lysearch.cpp:236: result
+ * heap size), and returns the best out_k results of every query, ascending
+ * (padded with id 0xffffffff, distance 0 when a beam holds fewer).
+ *
+ * Kernels: NNM_SERVE_EXACT is the kernel of nnm_search (the reference's
+ * heaps and float sums bit for bit; with beams == NULL, beam == out_k and
+ * the default entry it gives nnm_search's results).  NNM_SERVE_FAST
+ * computes each distance with a whole warp (coalesced rows, a different
+ * float summation order) and keeps the beam as a sorted array in shared
+ * memory in place of the two heaps: the same best-first expansion and
+ * stopping rule, ties between equal distances broken by id.
+ *
+ * Entry points: NNM_ENTRY_DEFAULT starts every query at rand() % nrows[0]
+ * after srand(seed) and descends greedily from layer 0, as the reference.
+ * NNM_ENTRY_LEARNED (no counterpart in the reference) runs the entry
+ * network set with nnm_index_set_entry_model: the rows of its layer with
+ * the `probes` largest scores are measured, the nearest of them starts the
+ * greedy descent on that layer. */
+typedef struct nnm_index nnm_index;
+
+typedef enum { NNM_SERVE_EXACT = 0, NNM_SERVE_FAST = 1 } nnm_serve_mode;
+typedef enum { NNM_ENTRY_DEFAULT = 0, NNM_ENTRY_LEARNED = 1 } nnm_entry_mode;
+
+typedef struct {
+    uint64_t ncmps;       /* distance evaluations, all queries (entry probes included) */
+    uint64_t expansions;  /* beam expansions (nodes whose lists were read), all queries */
+    double device_ms;     /* device time of the call's kernels (CUDA events) */
+    double predict_ms;    /* of which the entry network */
+} nnm_search_stats;
+
+/* The index keeps pointers to nothing the caller owns; it belongs to ctx
+ * (its stream and device) and must be freed before ctx is destroyed. */
+int nnm_index_create(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, const nnm_layers *layers,
+                     uint32_t seed, uint32_t metric, nnm_index **out);
+int nnm_index_free(nnm_index *ix);
+/* beams: nq widths (1..1024) or NULL for `beam` everywhere; out_k <= every width.
+ * q, beams, out_ids, out_dists: host arrays (nq x d, nq, nq x out_k). */
+int nnm_index_search(nnm_index *ix, const float *q, uint64_t nq, const uint32_t *beams, uint32_t beam,
+                     uint32_t out_k, uint32_t serve_mode, uint32_t entry_mode, uint32_t *out_ids,
+                     float *out_dists, nnm_search_stats *stats);
+/* The same with q, beams, out_ids and out_dists in device memory. */
+int nnm_index_search_dev(nnm_index *ix, const float *q_dev, uint64_t nq, const uint32_t *beams_dev,
+                         uint32_t beam, uint32_t out_k, uint32_t serve_mode, uint32_t entry_mode,
+                         uint32_t *out_ids_dev, float *out_dists_dev, nnm_search_stats *stats);
+
+/* Entry-point network (no counterpart in the reference): its classes are
+ * rows 0..C-1 of the data set (C <= NNM_ENTRY_MAX_CLASSES), and a learned
+ * search starts its greedy descent on the first layer that holds them all.
+ * nnm_index_entry_layer gives the default: the deepest layer with at most
+ * NNM_ENTRY_MAX_CLASSES rows (C = its rows), else layer 0 with C = 4096.
+ *   u = x * in_scale + in_shift,  h = relu(W1 u + b1),  s = W2 h + b2,
+ * d_in (<= 256) -> 256 -> C, BF16-rounded weights, FP32 accumulation.
+ * Training minimises the softmax cross-entropy of s against the nearest
+ * class row (squared L2) of each training row, with Adam on FP32 master
+ * weights.  w1 is 256 x d_in, w2 is C x 256 (row-major). */
+#define NNM_ENTRY_MAX_CLASSES 4096
+typedef struct {
+    uint32_t d_in, n_classes;
+    float in_scale, in_shift;
+    float *w1, *b1, *w2, *b2; /* caller-owned host arrays */
+} nnm_entry_mlp;
+
+int nnm_index_entry_layer(const nnm_index *ix, uint32_t *layer, uint32_t *n_classes);
+/* Scores (n x C) of x (n x d). */
+int nnm_entry_forward(nnm_ctx *ctx, const nnm_entry_mlp *model, const float *x, uint64_t n, uint32_t d,
+                      float *scores);
+/* Mean cross-entropy over the rows of x against labels (n classes) and its
+ * gradients w.r.t. the BF16-rounded weights; grad has the model's shapes. */
+int nnm_entry_grad(nnm_ctx *ctx, const nnm_entry_mlp *model, const float *x, uint64_t n, uint32_t d,
+                   const uint32_t *labels, float *loss, nnm_entry_mlp *grad);
+/* Trains `model` in place on rows of the index's data set (a seeded sample
+ * of at most 262144 rows, labelled on the device by brute force); steps,
+ * batch, lr and seed come from opts (margin is unused).  loss_trace: `steps`
+ * floats or NULL. */
+int nnm_entry_train(nnm_index *ix, nnm_entry_mlp *model, const nnm_train_opts *opts, float *loss_trace);
+/* The network NNM_ENTRY_LEARNED uses (copied to the device), probes in
+ * 1..min(8, C); NULL clears it. */
+int nnm_index_set_entry_model(nnm_index *ix, const nnm_entry_mlp *model, uint32_t probes);
 
 /* Profiling (no counterpart in the reference, which times whole builds with
  * boost::timer): while enabled, the engine records CUDA events around its

@@ -6,12 +6,18 @@
 
 #include "../../include/nnm.h"
 #include "nnm_builders.h"
+#include "nnm_entry.h"
 #include "nnm_hier.h"
 #include "nnm_launch.h"
 #include "nnm_learned.h"
 
 struct nnm_ctx {
     nnm::Ctx c;
+};
+
+struct nnm_index {
+    nnm_ctx* ctx;
+    nnm::IndexDev ix;
 };
 
 namespace {
@@ -475,6 +481,281 @@ int nnm_search(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, const nnm_l
     Ctx& c = ctx->c;
     if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
     return nnm::search_host(c, x, n, d, layers, q, nq, topk, o.seed, (int)o.metric, out_ids, out_dists, ncmps);
+}
+
+int nnm_index_create(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, const nnm_layers* layers, uint32_t seed,
+                     uint32_t metric, nnm_index** out) {
+    if (!ctx || !out) return NNM_ERR_INVALID;
+    *out = nullptr;
+    if (!x || !layers || n == 0 || d == 0 || layers->nlayers < 1 || layers->nlayers > 16)
+        return fail(ctx, NNM_ERR_INVALID, "x and 1..16 layers are required, n, d > 0");
+    if (n >= (1ull << 30) || layers->nrows[layers->nlayers - 1] > n)
+        return fail(ctx, NNM_ERR_INVALID, "layers do not match the data set");
+    if (metric > NNM_METRIC_CHI2) return fail(ctx, NNM_ERR_UNSUPPORTED_METRIC, "unknown metric");
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    std::unique_ptr<nnm_index> h(new nnm_index());
+    h->ctx = ctx;
+    int rc = nnm::index_upload(c, h->ix, x, n, d, layers, seed, metric);
+    if (!rc && cudaStreamSynchronize(c.stream) != cudaSuccess) rc = fail(ctx, NNM_ERR_CUDA, "index upload failed");
+    if (rc) {
+        h->ix.release();
+        return rc;
+    }
+    *out = h.release();
+    return NNM_OK;
+}
+
+int nnm_index_free(nnm_index* h) {
+    if (!h) return NNM_OK;
+    cudaSetDevice(h->ctx->c.device);
+    cudaStreamSynchronize(h->ctx->c.stream);
+    if (h->ix.net) {
+        h->ix.net->release();
+        delete h->ix.net;
+    }
+    h->ix.release();
+    delete h;
+    return NNM_OK;
+}
+
+namespace {
+int index_search_impl(nnm_index* h, const float* q, uint64_t nq, const uint32_t* beams, uint32_t beam,
+                      uint32_t out_k, uint32_t smode, uint32_t emode, uint32_t* out_ids, float* out_d,
+                      nnm_search_stats* stats, bool dev) {
+    if (!h) return NNM_ERR_INVALID;
+    nnm_ctx* ctx = h->ctx;
+    Ctx& c = ctx->c;
+    nnm::IndexDev& ix = h->ix;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (nq == 0) return NNM_OK;
+    if (!q || !out_ids) return fail(ctx, NNM_ERR_INVALID, "q and out_ids are required");
+    if (nq >= (1ull << 31)) return fail(ctx, NNM_ERR_INVALID, "nq must be below 2^31");
+    if (smode > NNM_SERVE_FAST || emode > NNM_ENTRY_LEARNED) return fail(ctx, NNM_ERR_INVALID, "unknown mode");
+    if (emode == NNM_ENTRY_LEARNED && !ix.net) return fail(ctx, NNM_ERR_INVALID, "no entry model set");
+    if (out_k == 0) return fail(ctx, NNM_ERR_INVALID, "out_k must be positive");
+    uint32_t bmax = beam;
+    if (beams && !dev) {
+        bmax = 0;
+        for (uint64_t i = 0; i < nq; i++) {
+            if (beams[i] < out_k || beams[i] > nnm::SEARCH_MAX_BEAM)
+                return fail(ctx, NNM_ERR_INVALID, "every beam width must be in [out_k, 1024]");
+            bmax = std::max(bmax, beams[i]);
+        }
+    } else if (beam < out_k || beam > nnm::SEARCH_MAX_BEAM) {
+        return fail(ctx, NNM_ERR_INVALID, "beam must be in [out_k, 1024]");
+    }
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    cudaStream_t st = c.stream;
+    const uint32_t d = ix.d, dp = ix.dp;
+    auto cu = [&](cudaError_t e) {
+        if (e == cudaSuccess) return 0;
+        c.last_error = cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? (int)NNM_ERR_OOM : (int)NNM_ERR_CUDA;
+    };
+    int rc = 0;
+    // queries with rows of dp floats
+    const float* qd = q;
+    if (!dev || dp != d) {
+        if ((rc = cu(ix.qpad.ensure((size_t)nq * dp * 4)))) return rc;
+        const cudaMemcpyKind kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        if (dp == d) rc = cu(cudaMemcpyAsync(ix.qpad.p, q, (size_t)nq * d * 4, kind, st));
+        else {
+            rc = cu(cudaMemset2DAsync(ix.qpad.p, dp * 4, 0, dp * 4, nq, st));
+            if (!rc) rc = cu(cudaMemcpy2DAsync(ix.qpad.p, dp * 4, q, d * 4, d * 4, nq, kind, st));
+        }
+        if (rc) return rc;
+        qd = ix.qpad.as<float>();
+    }
+    const uint32_t* bd = beams;
+    if (beams && !dev) {
+        if ((rc = cu(ix.beams.ensure((size_t)nq * 4)))) return rc;
+        if ((rc = cu(cudaMemcpyAsync(ix.beams.p, beams, (size_t)nq * 4, cudaMemcpyHostToDevice, st)))) return rc;
+        bd = ix.beams.as<uint32_t>();
+    }
+    uint32_t* oi = out_ids;
+    float* od = out_d;
+    if (!dev) {
+        if ((rc = cu(ix.out.ensure((size_t)nq * out_k * 8)))) return rc;
+        oi = ix.out.as<uint32_t>();
+        od = out_d ? reinterpret_cast<float*>(oi + (size_t)nq * out_k) : nullptr;
+    }
+    nnm::SearchReq r{};
+    r.q = qd;
+    r.nq = (uint32_t)nq;
+    r.beams = bd;
+    r.beam = beam;
+    r.beam_max = bmax;
+    r.out_k = out_k;
+    r.out_ids = oi;
+    r.out_d = od;
+    cudaEvent_t ev[3];
+    for (auto& e : ev) cudaEventCreate(&e);
+    cudaEventRecord(ev[0], st);
+    if (emode == NNM_ENTRY_LEARNED) {
+        rc = cu(ix.probes.ensure((size_t)nq * ix.nprobe * 4));
+        if (!rc) rc = nnm::entry_predict(c, ix, qd, (uint32_t)nq, ix.probes.as<uint32_t>());
+        r.probes = ix.probes.as<uint32_t>();
+        r.nprobe = ix.nprobe;
+        r.g0 = ix.entry_layer;
+    }
+    cudaEventRecord(ev[1], st);
+    if (!rc) rc = smode == NNM_SERVE_FAST ? nnm::index_run_fast(c, ix, r) : nnm::index_run_exact(c, ix, r);
+    cudaEventRecord(ev[2], st);
+    uint64_t ncmps = 0, nexp = 0;
+    if (!rc) rc = nnm::index_counters(c, ix, &ncmps, &nexp);
+    if (!rc && !dev) {
+        rc = cu(cudaMemcpyAsync(out_ids, oi, (size_t)nq * out_k * 4, cudaMemcpyDeviceToHost, st));
+        if (!rc && out_d) rc = cu(cudaMemcpyAsync(out_d, od, (size_t)nq * out_k * 4, cudaMemcpyDeviceToHost, st));
+        if (!rc) rc = cu(cudaStreamSynchronize(st));
+    }
+    if (!rc && stats) {
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, ev[0], ev[1]);
+        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        stats->ncmps = ncmps;
+        stats->expansions = nexp;
+        stats->predict_ms = a;
+        stats->device_ms = a + b;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return rc;
+}
+
+bool entry_ok(nnm_ctx* ctx, const nnm_entry_mlp* m, uint32_t d) {
+    if (!m || !m->w1 || !m->b1 || !m->w2 || !m->b2) {
+        fail(ctx, NNM_ERR_INVALID, "model arrays must be non-null");
+        return false;
+    }
+    if (m->d_in != d || d == 0 || d > nnm::ENTRY_MAX_D) {
+        fail(ctx, NNM_ERR_INVALID, "model d_in must equal d and be in [1, 256]");
+        return false;
+    }
+    if (m->n_classes == 0 || m->n_classes > nnm::ENTRY_MAX_C) {
+        fail(ctx, NNM_ERR_INVALID, "n_classes must be in [1, 4096]");
+        return false;
+    }
+    return true;
+}
+}  // namespace
+
+int nnm_index_search(nnm_index* ix, const float* q, uint64_t nq, const uint32_t* beams, uint32_t beam, uint32_t out_k,
+                     uint32_t serve_mode, uint32_t entry_mode, uint32_t* out_ids, float* out_dists,
+                     nnm_search_stats* stats) {
+    return index_search_impl(ix, q, nq, beams, beam, out_k, serve_mode, entry_mode, out_ids, out_dists, stats, false);
+}
+
+int nnm_index_search_dev(nnm_index* ix, const float* q, uint64_t nq, const uint32_t* beams, uint32_t beam,
+                         uint32_t out_k, uint32_t serve_mode, uint32_t entry_mode, uint32_t* out_ids,
+                         float* out_dists, nnm_search_stats* stats) {
+    return index_search_impl(ix, q, nq, beams, beam, out_k, serve_mode, entry_mode, out_ids, out_dists, stats, true);
+}
+
+int nnm_index_entry_layer(const nnm_index* h, uint32_t* layer, uint32_t* n_classes) {
+    if (!h || !layer || !n_classes) return NNM_ERR_INVALID;
+    const nnm::IndexDev& ix = h->ix;
+    for (int g = (int)ix.L - 1; g >= 0; g--)
+        if (ix.nrows[g] <= nnm::ENTRY_MAX_C) {
+            *layer = (uint32_t)g;
+            *n_classes = ix.nrows[g];
+            return NNM_OK;
+        }
+    *layer = 0;  // rows 0..4095, a prefix of the top layer
+    *n_classes = nnm::ENTRY_MAX_C;
+    return NNM_OK;
+}
+
+int nnm_entry_forward(nnm_ctx* ctx, const nnm_entry_mlp* model, const float* x, uint64_t n, uint32_t d,
+                      float* scores) {
+    if (!ctx || !x || !scores || n == 0 || n >= (1ull << 30)) return NNM_ERR_INVALID;
+    if (!entry_ok(ctx, model, d)) return NNM_ERR_INVALID;
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    nnm::DevEntry m;
+    GraphStore st;
+    GraphDev g;
+    nnm::DevBuf hb, sb;
+    int rc = nnm::entry_upload(c, m, *model);
+    if (!rc) rc = upload_plain(c, st, g, x, n, d);
+    if (!rc && (hb.ensure(n * nnm::ENTRY_H * 4) != cudaSuccess || sb.ensure(n * model->n_classes * 4) != cudaSuccess))
+        rc = fail(ctx, NNM_ERR_OOM, "device allocation failed");
+    if (!rc) rc = nnm::entry_scores_dev(c, m, g.x, (uint32_t)n, g.dp, hb.as<float>(), sb.as<float>());
+    if (!rc && cudaStreamSynchronize(c.stream) != cudaSuccess) rc = fail(ctx, NNM_ERR_CUDA, "entry forward failed");
+    if (!rc && cudaMemcpy(scores, sb.p, n * model->n_classes * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = NNM_ERR_CUDA;
+    m.release();
+    st.release();
+    hb.release();
+    sb.release();
+    return rc;
+}
+
+int nnm_entry_grad(nnm_ctx* ctx, const nnm_entry_mlp* model, const float* x, uint64_t n, uint32_t d,
+                   const uint32_t* labels, float* loss, nnm_entry_mlp* grad) {
+    if (!ctx || !x || !labels || !loss || !grad || n == 0 || n >= (1ull << 24)) return NNM_ERR_INVALID;
+    if (!entry_ok(ctx, model, d) || !entry_ok(ctx, grad, d)) return NNM_ERR_INVALID;
+    if (grad->n_classes != model->n_classes) return fail(ctx, NNM_ERR_INVALID, "grad must have the model's shapes");
+    for (uint64_t i = 0; i < n; i++)
+        if (labels[i] >= model->n_classes) return fail(ctx, NNM_ERR_INVALID, "label out of range");
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    GraphStore st;
+    GraphDev g;
+    int rc = upload_plain(c, st, g, x, n, d);
+    if (!rc) rc = nnm::entry_grad(c, *model, g.x, (uint32_t)n, g.dp, labels, loss, *grad);
+    st.release();
+    return rc;
+}
+
+int nnm_entry_train(nnm_index* h, nnm_entry_mlp* model, const nnm_train_opts* opts, float* loss_trace) {
+    if (!h) return NNM_ERR_INVALID;
+    nnm_ctx* ctx = h->ctx;
+    nnm::IndexDev& ix = h->ix;
+    if (!entry_ok(ctx, model, ix.d)) return NNM_ERR_INVALID;
+    if (model->n_classes > ix.n) return fail(ctx, NNM_ERR_INVALID, "more classes than rows");
+    if (ix.metric != NNM_METRIC_L2) return fail(ctx, NNM_ERR_UNSUPPORTED_METRIC, "entry training needs L2");
+    nnm_train_opts o;
+    if (opts) o = *opts;
+    else nnm_train_opts_default(&o);
+    if (o.steps == 0 || o.batch == 0 || o.batch > (1u << 16)) return fail(ctx, NNM_ERR_INVALID, "bad training opts");
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    return nnm::entry_train(c, ix, 0, o, *model, loss_trace);
+}
+
+int nnm_index_set_entry_model(nnm_index* h, const nnm_entry_mlp* model, uint32_t probes) {
+    if (!h) return NNM_ERR_INVALID;
+    nnm_ctx* ctx = h->ctx;
+    nnm::IndexDev& ix = h->ix;
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    if (!model) {
+        if (ix.net) {
+            cudaStreamSynchronize(c.stream);
+            ix.net->release();
+            delete ix.net;
+            ix.net = nullptr;
+        }
+        return NNM_OK;
+    }
+    if (!entry_ok(ctx, model, ix.d)) return NNM_ERR_INVALID;
+    if (model->n_classes > ix.n) return fail(ctx, NNM_ERR_INVALID, "more classes than rows");
+    if (probes == 0 || probes > (uint32_t)nnm::ENTRY_MAX_PROBES || probes > model->n_classes)
+        return fail(ctx, NNM_ERR_INVALID, "probes must be in [1, min(8, n_classes)]");
+    if (!ix.net) ix.net = new nnm::DevEntry();
+    int rc = nnm::entry_upload(c, *ix.net, *model);
+    if (rc) return rc;
+    // the descent starts on the first layer that holds every class row
+    uint32_t g0 = ix.L - 1;
+    for (uint32_t g = 0; g < ix.L; g++)
+        if (ix.nrows[g] >= model->n_classes) {
+            g0 = g;
+            break;
+        }
+    ix.entry_layer = g0;
+    ix.n_classes = model->n_classes;
+    ix.nprobe = probes;
+    return NNM_OK;
 }
 
 }  // extern "C"

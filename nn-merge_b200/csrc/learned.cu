@@ -327,6 +327,20 @@ MlpView pass_view(const Pass& p, const Layout& L, const nnm_mlp& m) {
 
 }  // namespace
 
+void launch_grad_w1(const float* dh, const float* x, uint32_t dp, const uint32_t* idx, uint32_t R, uint32_t d,
+                    float scale, float shift, float* gw1, float* gb1, cudaStream_t st) {
+    MlpView m{};
+    m.d = d;
+    m.scale = scale;
+    m.shift = shift;
+    k_grad_w1<<<MLP_H, 256, 0, st>>>(dh, x, dp, idx, R, m, gw1, gb1);
+}
+
+void launch_adam(float* p, float* mo, float* ve, const float* g, uint32_t cnt, float lr, const uint32_t* step,
+                 cudaStream_t st) {
+    k_adam<<<(cnt + 255) / 256, 256, 0, st>>>(p, mo, ve, g, cnt, lr, step);
+}
+
 int mlp_upload(Ctx& ctx, DevMlp& m, const nnm_mlp& h) {
     const uint32_t d = h.d_in;
     const Layout L(d);

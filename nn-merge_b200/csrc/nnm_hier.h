@@ -32,6 +32,42 @@ int dpg_init(Ctx& ctx, DpgState& s, uint32_t n_cap, uint32_t K, uint32_t M);
 // to `out` (host CSR) when out is non-null.
 int dpg_layer(Ctx& ctx, DpgState& s, GraphDev& g, nnm_layers* out);
 
+struct DevEntry;  // entry network (entry.cu)
+
+// A resident search hierarchy (nnm_index): vectors (n x dp), every layer's
+// offsets rebased onto one adjacency array, and the search scratch.
+struct IndexDev {
+    uint32_t n = 0, d = 0, dp = 0, L = 0, metric = 0, seed = 0, entry = 0;
+    uint32_t nrows[16] = {};
+    uint64_t off_base[16] = {};
+    DevBuf x, off, adj;
+    DevBuf visited, vlist, cand, ctr;          // per-warp scratch and counters
+    DevBuf qpad, beams, probes, hid, scores, out;  // per-call staging
+    DevEntry* net = nullptr;                   // entry network, owned
+    uint32_t nprobe = 0, entry_layer = 0, n_classes = 0;
+    void release();
+};
+
+// One batch of queries against an index; every pointer is device memory.
+struct SearchReq {
+    const float* q;           // nq x dp
+    uint32_t nq;
+    const uint32_t* beams;    // nq widths or null: `beam` for all
+    uint32_t beam, beam_max, out_k;
+    const uint32_t* probes;   // nq x nprobe rows of layer g0, or null: default entry
+    uint32_t nprobe, g0;
+    uint32_t* out_ids;        // nq x out_k
+    float* out_d;             // nq x out_k or null
+};
+
+int index_upload(Ctx& ctx, IndexDev& ix, const float* x, uint64_t n, uint32_t d, const nnm_layers* layers,
+                 uint32_t seed, uint32_t metric);
+int index_run_exact(Ctx& ctx, IndexDev& ix, const SearchReq& r);
+int index_run_fast(Ctx& ctx, IndexDev& ix, const SearchReq& r);
+// Waits for the stream, reads the distance and expansion counts of the last
+// run and turns its self-check flags into an error.
+int index_counters(Ctx& ctx, IndexDev& ix, uint64_t* ncmps, uint64_t* nexp);
+
 int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_layers* layers, const float* q,
                 uint64_t nq, uint32_t topk, uint32_t seed, int metric, uint32_t* out_ids, float* out_dists,
                 uint64_t* ncmps);

@@ -47,6 +47,14 @@ int mlp_train(Ctx& ctx, const float* x_dev, uint32_t n, uint32_t dp, const uint3
 int mlp_grad(Ctx& ctx, const nnm_mlp& model, const float* x_dev, uint32_t n, uint32_t dp, const uint32_t* trip_host,
              uint32_t ntrip, float margin, float* loss, nnm_mlp& grad);
 
+// Kernels shared with the entry network (entry.cu); neither counts its launch.
+// dW1 (256 x d) and db1 of dL/dh over rows idx[0..R) of x.
+void launch_grad_w1(const float* dh, const float* x, uint32_t dp, const uint32_t* idx, uint32_t R, uint32_t d,
+                    float scale, float shift, float* gw1, float* gb1, cudaStream_t st);
+// One Adam step over cnt parameters; the step number is read from *step.
+void launch_adam(float* p, float* mo, float* ve, const float* g, uint32_t cnt, float lr, const uint32_t* step,
+                 cudaStream_t st);
+
 // Code orderings of a graph's rows, per leaf: V views (the code rotated by
 // 8v bits), each leaf's rows sorted by (view key, row) into a segment of P
 // slots (padded with all-ones keys).

@@ -90,6 +90,11 @@ struct SearchArgs {
     const uint32_t* adj_all;
     const float* q;
     uint32_t nq, topk, entry, n;
+    const uint32_t* beams;   // per-query beam widths, or null: topk for all
+    uint32_t beam_cap;       // largest beam width (shared-memory sizing)
+    uint32_t out_k;          // results written per query
+    const uint32_t* probes;  // learned entries: nq x nprobe rows of layer g0, or null
+    uint32_t nprobe, g0;
     uint32_t* out_ids;
     float* out_d;
     uint32_t* visited;  // per warp slot: ceil(n/32) words
@@ -98,6 +103,7 @@ struct SearchArgs {
     HP* cand;           // per warp slot: CCAP entries
     unsigned* next_q;
     unsigned long long* ncmps;
+    unsigned long long* nexp;
     unsigned* overflow;     // bit 0: candidate heap full; bits 1..: self-check failures
     uint32_t nrows[16];     // rows of each layer
 };
@@ -107,34 +113,66 @@ enum : unsigned {
     SERR_GREEDY_CAP = 2u,  // greedy descent made more moves than the layer has rows
     SERR_BEAM_CAP = 4u,    // beam search expanded more nodes than the layer has rows
     SERR_BAD_ID = 8u,      // a node id outside its layer
+    SERR_BEAM_RANGE = 32u, // a per-query beam width outside [out_k, beam_cap]
 };
 
 __global__ void k_search(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t slot = blockIdx.x * SWARPS + w;
-    const size_t wbytes = (size_t)a.dp * 4 + (size_t)(a.topk + 1) * 8 + 32 * 8;
+    const size_t wbytes = (size_t)a.dp * 4 + (size_t)(a.beam_cap + 1) * 8 + 32 * 8;
     unsigned char* base = smem + (size_t)w * ((wbytes + 15) & ~(size_t)15);
     float* qv = reinterpret_cast<float*>(base);
     HP* top = reinterpret_cast<HP*>(base + (size_t)a.dp * 4);
-    float* stage_d = reinterpret_cast<float*>(top + a.topk + 1);
+    float* stage_d = reinterpret_cast<float*>(top + a.beam_cap + 1);
     uint32_t* stage_i = reinterpret_cast<uint32_t*>(stage_d + 32);
     uint32_t* vis = a.visited + (size_t)slot * a.words;
     uint32_t* vl = a.vlist + (size_t)slot * VCAP;
     HP* cand = a.cand + (size_t)slot * CCAP;
-    unsigned long long cmps = 0;
+    unsigned long long cmps = 0, nexp = 0;
     for (;;) {
         unsigned qi = 0;
         if (lane == 0) qi = atomicAdd(a.next_q, 1u);
         qi = __shfl_sync(FULL, qi, 0);
         if (qi >= a.nq) break;
+        uint32_t topk = a.beams ? a.beams[qi] : a.topk;
+        if (topk < a.out_k || topk > a.beam_cap) {
+            if (lane == 0) atomicOr(a.overflow, SERR_BEAM_RANGE);
+            topk = min(max(topk, a.out_k), a.beam_cap);
+        }
         for (uint32_t t = lane; t < a.dp; t += 32) qv[t] = a.q[(size_t)qi * a.dp + t];
         __syncwarp();
-        uint32_t cur = a.entry;
-        float cur_d = dist_seq_rt(a.metric, qv, a.x + (size_t)cur * a.dp, a.dp);
-        cmps++;
+        uint32_t cur = a.entry, g0 = 0;
+        float cur_d;
+        if (a.probes) {
+            // learned entries: the first nearest of the probed rows of layer g0,
+            // taken in probe order as the descent takes a list
+            g0 = a.g0;
+            uint32_t pid = 0;
+            float pd = 0.f;
+            if (lane < a.nprobe) {
+                pid = a.probes[(size_t)qi * a.nprobe + lane];
+                if (pid < a.nrows[g0]) pd = dist_seq_rt(a.metric, qv, a.x + (size_t)pid * a.dp, a.dp);
+                else atomicOr(a.overflow, SERR_BAD_ID);
+            }
+            cur = __shfl_sync(FULL, pid, 0);
+            cur_d = __shfl_sync(FULL, pd, 0);
+            for (uint32_t j = 1; j < a.nprobe; j++) {
+                const float oj = __shfl_sync(FULL, pd, j);
+                const uint32_t ij = __shfl_sync(FULL, pid, j);
+                if (oj < cur_d) {
+                    cur_d = oj;
+                    cur = ij;
+                }
+            }
+            cmps += a.nprobe;
+            if (cur >= a.nrows[g0]) cur = 0;
+        } else {
+            cur_d = dist_seq_rt(a.metric, qv, a.x + (size_t)cur * a.dp, a.dp);
+            cmps++;
+        }
         // greedy descent on the upper layers (lysearch.cpp:397-420)
-        for (uint32_t g = 0; g + 1 < a.L; g++) {
+        for (uint32_t g = g0; g + 1 < a.L; g++) {
             const uint64_t* off = a.off_all + a.off_base[g];
             bool moved = true;
             uint32_t moves = 0;
@@ -201,6 +239,7 @@ __global__ void k_search(SearchArgs a) {
             }
             if (lane == 0) heap_pop(cand, ncand);
             ncand = __shfl_sync(FULL, ncand, 0);
+            nexp++;
             const uint64_t b = off[c.id], e = off[c.id + 1];
             for (uint64_t c0 = b; c0 < e; c0 += 32) {
                 uint32_t nn = 0;
@@ -229,14 +268,14 @@ __global__ void k_search(SearchArgs a) {
                 if (lane == 0) {  // offers in list order (lysearch.cpp:284-295)
                     for (uint32_t r = 0; r < nf; r++) {
                         const float dj = stage_d[r];
-                        if (top[0].f > dj || ntop < a.topk) {
+                        if (top[0].f > dj || ntop < topk) {
                             if (ncand >= CCAP) {
                                 atomicOr(a.overflow, SERR_HEAP);
                                 continue;
                             }
                             heap_push(cand, ncand, HP{-dj, stage_i[r]});
                             heap_push(top, ntop, HP{dj, stage_i[r]});
-                            if (ntop > a.topk) heap_pop(top, ntop);
+                            if (ntop > topk) heap_pop(top, ntop);
                         }
                     }
                 }
@@ -248,15 +287,19 @@ __global__ void k_search(SearchArgs a) {
                 lwbnd = __shfl_sync(FULL, lw, 0);
             }
         }
-        // results ascending, popped from the max-heap into place (lysearch.cpp:302-312)
+        // results ascending, popped from the max-heap into place (lysearch.cpp:302-312);
+        // the first out_k are kept
         if (lane == 0) {
-            for (uint32_t t = ntop; t < a.topk; t++) {
-                a.out_ids[(size_t)qi * a.topk + t] = 0xffffffffu;
-                if (a.out_d) a.out_d[(size_t)qi * a.topk + t] = 0.f;
+            const size_t o = (size_t)qi * a.out_k;
+            for (uint32_t t = ntop; t < a.out_k; t++) {
+                a.out_ids[o + t] = 0xffffffffu;
+                if (a.out_d) a.out_d[o + t] = 0.f;
             }
             for (int loc = (int)ntop - 1; loc >= 0; loc--) {
-                a.out_ids[(size_t)qi * a.topk + loc] = top[0].id;
-                if (a.out_d) a.out_d[(size_t)qi * a.topk + loc] = top[0].f;
+                if ((uint32_t)loc < a.out_k) {
+                    a.out_ids[o + loc] = top[0].id;
+                    if (a.out_d) a.out_d[o + loc] = top[0].f;
+                }
                 heap_pop(top, ntop);
             }
         }
@@ -273,23 +316,18 @@ __global__ void k_search(SearchArgs a) {
     }
     for (int o = 16; o > 0; o >>= 1) cmps += __shfl_xor_sync(FULL, cmps, o);
     if (lane == 0 && a.ncmps) atomicAdd(a.ncmps, cmps / 32);
+    if (lane == 0 && a.nexp) atomicAdd(a.nexp, nexp);
 }
 }  // namespace
 
-int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_layers* layers, const float* q,
-                uint64_t nq, uint32_t topk, uint32_t seed, int metric, uint32_t* out_ids, float* out_dists,
-                uint64_t* ncmps) {
+int index_upload(Ctx& ctx, IndexDev& ix, const float* x, uint64_t n, uint32_t d, const nnm_layers* layers,
+                 uint32_t seed, uint32_t metric) {
     cudaStream_t st = ctx.stream;
     const uint32_t dp = (d + 3) & ~3u;
     const uint32_t L = layers->nlayers;
-    // entry point: the first std::rand() after srand(seed) (lysearch.cpp:382)
-    GlibcBase gb = glibc_base(seed);
-    uint32_t r0;
-    {
-        // rand() #0 = s[310] >> 1, s[i] = s[i-3] + s[i-31]
-        std::vector<uint32_t> s(gb.s, gb.s + 62);
-        while (s.size() <= 310) s.push_back(s[s.size() - 3] + s[s.size() - 31]);
-        r0 = s[310] >> 1;
+    if (L == 0 || L > 16) {
+        ctx.last_error = "search needs 1..16 layers";
+        return 1;
     }
     // Layers must be nested prefixes whose ids stay inside their own layer;
     // anything else is rejected here rather than read out of bounds.
@@ -315,47 +353,61 @@ int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_laye
                 return 1;
             }
     }
-    const uint32_t entry = r0 % layers->nrows[0];
-    SearchArgs a{};
-    a.dp = dp;
-    a.metric = metric;
-    a.L = L;
+    // entry point: the first std::rand() after srand(seed) (lysearch.cpp:382)
+    GlibcBase gb = glibc_base(seed);
+    uint32_t r0;
+    {
+        // rand() #0 = s[310] >> 1, s[i] = s[i-3] + s[i-31]
+        std::vector<uint32_t> s(gb.s, gb.s + 62);
+        while (s.size() <= 310) s.push_back(s[s.size() - 3] + s[s.size() - 31]);
+        r0 = s[310] >> 1;
+    }
+    ix.n = (uint32_t)n;
+    ix.d = d;
+    ix.dp = dp;
+    ix.L = L;
+    ix.metric = metric;
+    ix.seed = seed;
+    ix.entry = r0 % layers->nrows[0];
     uint64_t off_total = 0, adj_total = 0;
     for (uint32_t g = 0; g < L; g++) {
-        a.off_base[g] = off_total;
+        ix.nrows[g] = layers->nrows[g];
+        ix.off_base[g] = off_total;
         off_total += (uint64_t)layers->nrows[g] + 1;
         adj_total += layers->off[g][layers->nrows[g]];
     }
-    // one device buffer: vectors | queries | offsets | adjacency
-    DevBuf xb, qb, ob, ab, ib, db, vb, lb, cb, hb;
-    NNM_CUDA_TRY(xb.ensure((size_t)n * dp * 4));
-    NNM_CUDA_TRY(qb.ensure((size_t)nq * dp * 4 + 16));
-    NNM_CUDA_TRY(ob.ensure(off_total * 8));
-    NNM_CUDA_TRY(ab.ensure(std::max<uint64_t>(adj_total, 1) * 4));
-    NNM_CUDA_TRY(ib.ensure((size_t)nq * topk * 4 + 16));
-    NNM_CUDA_TRY(db.ensure((size_t)nq * topk * 4 + 16));
-    NNM_CUDA_TRY(cb.ensure(64));
+    NNM_CUDA_TRY(ix.x.ensure((size_t)n * dp * 4));
+    NNM_CUDA_TRY(ix.off.ensure(off_total * 8));
+    NNM_CUDA_TRY(ix.adj.ensure(std::max<uint64_t>(adj_total, 1) * 4));
+    NNM_CUDA_TRY(ix.ctr.ensure(64));
     if (dp == d) {
-        NNM_CUDA_TRY(cudaMemcpyAsync(xb.p, x, (size_t)n * d * 4, cudaMemcpyHostToDevice, st));
-        NNM_CUDA_TRY(cudaMemcpyAsync(qb.p, q, (size_t)nq * d * 4, cudaMemcpyHostToDevice, st));
+        NNM_CUDA_TRY(cudaMemcpyAsync(ix.x.p, x, (size_t)n * d * 4, cudaMemcpyHostToDevice, st));
     } else {
-        NNM_CUDA_TRY(cudaMemset2DAsync(xb.p, dp * 4, 0, dp * 4, n, st));
-        NNM_CUDA_TRY(cudaMemcpy2DAsync(xb.p, dp * 4, x, d * 4, d * 4, n, cudaMemcpyHostToDevice, st));
-        NNM_CUDA_TRY(cudaMemset2DAsync(qb.p, dp * 4, 0, dp * 4, nq, st));
-        NNM_CUDA_TRY(cudaMemcpy2DAsync(qb.p, dp * 4, q, d * 4, d * 4, nq, cudaMemcpyHostToDevice, st));
+        NNM_CUDA_TRY(cudaMemset2DAsync(ix.x.p, dp * 4, 0, dp * 4, n, st));
+        NNM_CUDA_TRY(cudaMemcpy2DAsync(ix.x.p, dp * 4, x, d * 4, d * 4, n, cudaMemcpyHostToDevice, st));
     }
+    // offsets rebased onto one adjacency array; the copies wait for the
+    // stream's earlier work through the synchronous calls below
+    NNM_CUDA_TRY(cudaStreamSynchronize(st));
     adj_total = 0;
     for (uint32_t g = 0; g < L; g++) {
         std::vector<uint64_t> off(layers->off[g], layers->off[g] + layers->nrows[g] + 1);
         for (auto& v : off) v += adj_total;
-        NNM_CUDA_TRY(cudaMemcpy(ob.as<uint64_t>() + a.off_base[g], off.data(), off.size() * 8, cudaMemcpyHostToDevice));
+        NNM_CUDA_TRY(cudaMemcpy(ix.off.as<uint64_t>() + ix.off_base[g], off.data(), off.size() * 8,
+                                cudaMemcpyHostToDevice));
         uint64_t cnt = layers->off[g][layers->nrows[g]];
-        if (cnt) NNM_CUDA_TRY(cudaMemcpy(ab.as<uint32_t>() + adj_total, layers->adj[g], cnt * 4, cudaMemcpyHostToDevice));
+        if (cnt) NNM_CUDA_TRY(cudaMemcpy(ix.adj.as<uint32_t>() + adj_total, layers->adj[g], cnt * 4, cudaMemcpyHostToDevice));
         adj_total += cnt;
     }
+    return 0;
+}
+
+int index_run_exact(Ctx& ctx, IndexDev& ix, const SearchReq& r) {
+    cudaStream_t st = ctx.stream;
+    const uint32_t dp = ix.dp;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx.device);
-    const size_t wbytes = (size_t)dp * 4 + (size_t)(topk + 1) * 8 + 32 * 8;
+    const size_t wbytes = (size_t)dp * 4 + (size_t)(r.beam_max + 1) * 8 + 32 * 8;
     const size_t smem = (size_t)SWARPS * ((wbytes + 15) & ~(size_t)15) + 64;
     if (smem > 200 * 1024) {
         ctx.last_error = "beam too wide for shared memory at this dimension";
@@ -365,49 +417,124 @@ int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_laye
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, SWARPS * 32, smem);
     const uint32_t blocks = (uint32_t)std::min(std::max(1, per_sm), 4) * (uint32_t)nsm;
-    const uint32_t words = (uint32_t)((n + 31) / 32);
+    const uint32_t words = (uint32_t)((ix.n + 31) / 32);
     const size_t slots = (size_t)blocks * SWARPS;
-    NNM_CUDA_TRY(vb.ensure(slots * words * 4));
-    NNM_CUDA_TRY(lb.ensure(slots * VCAP * 4));
-    NNM_CUDA_TRY(hb.ensure(slots * CCAP * sizeof(HP)));
-    NNM_CUDA_TRY(cudaMemsetAsync(vb.p, 0, slots * words * 4, st));
-    NNM_CUDA_TRY(cudaMemsetAsync(cb.p, 0, 64, st));
-    a.x = xb.as<float>();
-    a.off_all = ob.as<uint64_t>();
-    a.adj_all = ab.as<uint32_t>();
-    a.q = qb.as<float>();
-    a.nq = (uint32_t)nq;
-    a.topk = topk;
-    a.entry = entry;
-    a.n = (uint32_t)n;
-    a.out_ids = ib.as<uint32_t>();
-    a.out_d = db.as<float>();
-    a.visited = vb.as<uint32_t>();
+    if (ix.visited.bytes < slots * words * 4) {
+        NNM_CUDA_TRY(ix.visited.ensure(slots * words * 4));
+        NNM_CUDA_TRY(cudaMemsetAsync(ix.visited.p, 0, slots * words * 4, st));
+    }
+    NNM_CUDA_TRY(ix.vlist.ensure(slots * VCAP * 4));
+    NNM_CUDA_TRY(ix.cand.ensure(slots * CCAP * sizeof(HP)));
+    NNM_CUDA_TRY(cudaMemsetAsync(ix.ctr.p, 0, 64, st));
+    SearchArgs a{};
+    a.x = ix.x.as<float>();
+    a.dp = dp;
+    a.metric = (int)ix.metric;
+    a.L = ix.L;
+    for (uint32_t g = 0; g < ix.L; g++) {
+        a.off_base[g] = ix.off_base[g];
+        a.nrows[g] = ix.nrows[g];
+    }
+    a.off_all = ix.off.as<uint64_t>();
+    a.adj_all = ix.adj.as<uint32_t>();
+    a.q = r.q;
+    a.nq = r.nq;
+    a.topk = r.beam;
+    a.entry = ix.entry;
+    a.n = ix.n;
+    a.beams = r.beams;
+    a.beam_cap = r.beam_max;
+    a.out_k = r.out_k;
+    a.probes = r.probes;
+    a.nprobe = r.nprobe;
+    a.g0 = r.g0;
+    a.out_ids = r.out_ids;
+    a.out_d = r.out_d;
+    a.visited = ix.visited.as<uint32_t>();
     a.words = words;
-    a.vlist = lb.as<uint32_t>();
-    a.cand = hb.as<HP>();
-    a.next_q = cb.as<unsigned>();
-    a.ncmps = reinterpret_cast<unsigned long long*>(cb.as<unsigned char>() + 8);
-    a.overflow = cb.as<unsigned>() + 1;  // bytes 4..7; ncmps occupies bytes 8..15
-    for (uint32_t g = 0; g < L; g++) a.nrows[g] = layers->nrows[g];
+    a.vlist = ix.vlist.as<uint32_t>();
+    a.cand = ix.cand.as<HP>();
+    unsigned char* c = ix.ctr.as<unsigned char>();
+    a.next_q = reinterpret_cast<unsigned*>(c);
+    a.overflow = reinterpret_cast<unsigned*>(c + 4);
+    a.ncmps = reinterpret_cast<unsigned long long*>(c + 8);
+    a.nexp = reinterpret_cast<unsigned long long*>(c + 16);
     k_search<<<blocks, SWARPS * 32, smem, st>>>(a); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
-    NNM_CUDA_TRY(cudaMemcpyAsync(out_ids, ib.p, (size_t)nq * topk * 4, cudaMemcpyDeviceToHost, st));
-    if (out_dists) NNM_CUDA_TRY(cudaMemcpyAsync(out_dists, db.p, (size_t)nq * topk * 4, cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
+int index_counters(Ctx& ctx, IndexDev& ix, uint64_t* ncmps, uint64_t* nexp) {
     unsigned long long c[3] = {0, 0, 0};
-    NNM_CUDA_TRY(cudaMemcpyAsync(c, cb.p, 24, cudaMemcpyDeviceToHost, st));
-    NNM_CUDA_TRY(cudaStreamSynchronize(st));
+    NNM_CUDA_TRY(cudaMemcpyAsync(c, ix.ctr.p, 24, cudaMemcpyDeviceToHost, ctx.stream));
+    NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
     if (ncmps) *ncmps = c[1];
-    DevBuf* all[] = {&xb, &qb, &ob, &ab, &ib, &db, &vb, &lb, &cb, &hb};
+    if (nexp) *nexp = c[2];
     const unsigned serr = (unsigned)(c[0] >> 32);  // bytes 4..7
     if (serr) {
-        for (auto* b : all) b->release();
         ctx.last_error = "search self-check failed (code " + std::to_string(serr) +
-                         "; 1: candidate heap full, 2/4: loop bound, 8: id outside its layer)";
+                         "; 1: candidate heap full, 2/4: loop bound, 8: id outside its layer, "
+                         "32: beam width outside [out_k, beam])";
         return 6;
     }
-    for (auto* b : all) b->release();
     return 0;
+}
+
+void IndexDev::release() {
+    DevBuf* all[] = {&x, &off, &adj, &visited, &vlist, &cand, &ctr, &qpad, &beams, &probes, &hid, &scores, &out};
+    for (auto* b : all) b->release();
+}
+
+int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_layers* layers, const float* q,
+                uint64_t nq, uint32_t topk, uint32_t seed, int metric, uint32_t* out_ids, float* out_dists,
+                uint64_t* ncmps) {
+    cudaStream_t st = ctx.stream;
+    IndexDev ix;
+    int rc = index_upload(ctx, ix, x, n, d, layers, seed, (uint32_t)metric);
+    if (rc) {
+        ix.release();
+        return rc;
+    }
+    const uint32_t dp = ix.dp;
+    DevBuf qb, ib, db;
+    auto fail = [&](int code) {
+        ix.release();
+        qb.release();
+        ib.release();
+        db.release();
+        return code;
+    };
+#define TRY_OR_FREE(call)                                      \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) {                               \
+            ctx.last_error = cudaGetErrorString(e_);           \
+            return fail(e_ == cudaErrorMemoryAllocation ? 4 : 3); \
+        }                                                      \
+    } while (0)
+    TRY_OR_FREE(qb.ensure((size_t)nq * dp * 4 + 16));
+    TRY_OR_FREE(ib.ensure((size_t)nq * topk * 4 + 16));
+    TRY_OR_FREE(db.ensure((size_t)nq * topk * 4 + 16));
+    if (dp == d) {
+        TRY_OR_FREE(cudaMemcpyAsync(qb.p, q, (size_t)nq * d * 4, cudaMemcpyHostToDevice, st));
+    } else {
+        TRY_OR_FREE(cudaMemset2DAsync(qb.p, dp * 4, 0, dp * 4, nq, st));
+        TRY_OR_FREE(cudaMemcpy2DAsync(qb.p, dp * 4, q, d * 4, d * 4, nq, cudaMemcpyHostToDevice, st));
+    }
+    SearchReq r{};
+    r.q = qb.as<float>();
+    r.nq = (uint32_t)nq;
+    r.beam = topk;
+    r.beam_max = topk;
+    r.out_k = topk;
+    r.out_ids = ib.as<uint32_t>();
+    r.out_d = db.as<float>();
+    if ((rc = index_run_exact(ctx, ix, r))) return fail(rc);
+    TRY_OR_FREE(cudaMemcpyAsync(out_ids, ib.p, (size_t)nq * topk * 4, cudaMemcpyDeviceToHost, st));
+    if (out_dists) TRY_OR_FREE(cudaMemcpyAsync(out_dists, db.p, (size_t)nq * topk * 4, cudaMemcpyDeviceToHost, st));
+#undef TRY_OR_FREE
+    rc = index_counters(ctx, ix, ncmps, nullptr);
+    return fail(rc);
 }
 
 }  // namespace nnm

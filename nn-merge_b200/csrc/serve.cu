@@ -1,0 +1,466 @@
+// Fast batched LySearch (NNM_SERVE_FAST): the per-query steps of
+// LySearch::knnSearch (lysearch.cpp:363-437) and nndHNSWSrch (:236-322),
+// laid out for throughput rather than for the reference's float rounding.
+//
+// One warp per query; persistent warps pull queries from a counter, so
+// queries of different beam widths balance.
+//   - distances: a whole warp per distance, lane l holding components
+//     [4l, 4l+4) (+128 per further float4) of the query in registers; a
+//     row is one coalesced 512-byte read for d = 128.  Up to 32 distances
+//     are evaluated together and reduced by a transposing butterfly (31
+//     shuffles for 32 sums), after which lane j holds distance j.  The
+//     summation order differs from the reference's sequential sum.
+//   - greedy descent on the upper layers: the reference's rule (move to the
+//     first strictly nearer neighbour of the minimum distance in list order,
+//     repeat until no move) evaluated a list chunk at a time.
+//   - beam: the reference keeps a result max-heap of size topk and a
+//     candidate heap, and stops when the nearest candidate is farther than
+//     the worst result.  Every candidate that can still be expanded is in
+//     the result set, so both heaps are replaced by one array of at most
+//     `beam` entries in shared memory, sorted by (distance, id), with an
+//     "expanded" bit per entry: expand the first unexpanded entry, merge the
+//     accepted neighbours (distance below the worst entry, or the beam not
+//     full) into place, stop when every entry is expanded.
+//   - visited set: one bitmap per warp slot in HBM, cleared after each query
+//     from the list of ids it set.
+#include <algorithm>
+#include <cmath>
+
+#include "nnm_hier.h"
+#include "nnm_launch.h"
+
+namespace nnm {
+namespace {
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int FW = 4;                    // warps per block
+constexpr uint32_t FVCAP = 65536;        // visited ids recorded per warp slot
+constexpr uint32_t EXP_BIT = 1u << 31;   // beam entry already expanded
+constexpr uint32_t IDM = 0x7fffffffu;
+constexpr uint32_t FAST_MAX_DP = 512;    // 4 float4 per lane
+
+// self-check codes, shared with the exact kernel's report
+enum : unsigned { FERR_LOOP = 4u, FERR_BAD_ID = 8u, FERR_BEAM_RANGE = 32u };
+
+struct ServeArgs {
+    const float* x;
+    uint32_t dp4;  // float4 per row
+    uint32_t L;
+    uint64_t off_base[16];
+    uint32_t nrows[16];
+    const uint64_t* off_all;
+    const uint32_t* adj_all;
+    const float* q;
+    uint32_t nq;
+    const uint32_t* beams;
+    uint32_t beam, cap, out_k;
+    uint32_t entry;
+    const uint32_t* probes;
+    uint32_t nprobe, g0;
+    uint32_t* out_ids;
+    float* out_d;
+    uint32_t* visited;
+    uint32_t words;
+    uint32_t* vlist;
+    unsigned* next_q;
+    unsigned* overflow;
+    unsigned long long* ncmps;
+    unsigned long long* nexp;
+};
+
+template <int M>
+__device__ __forceinline__ float term(float a, float b, float acc) {
+    const float t = a - b;
+    if (M == L2) return fmaf(t, t, acc);
+    if (M == L1) return acc + fabsf(t);
+    return (a != 0.f || b != 0.f) ? acc + t * t / (a + b) : acc;
+}
+template <int M>
+__device__ __forceinline__ float part4(const float4 q, const float4 r, float acc) {
+    acc = term<M>(q.x, r.x, acc);
+    acc = term<M>(q.y, r.y, acc);
+    acc = term<M>(q.z, r.z, acc);
+    return term<M>(q.w, r.w, acc);
+}
+
+// Distances from the query (qr, spread over the warp) to the rows whose ids
+// lanes 0..nf-1 hold in fid (nf <= 32, warp-uniform).  Lane j returns the
+// distance of row j (0 for j >= nf).
+template <int M, int QV>
+__device__ __forceinline__ float warp_dists(const float4 (&qr)[QV], const float4* __restrict__ x4, uint32_t dp4,
+                                            uint32_t fid, uint32_t nf, uint32_t lane) {
+    constexpr int NB = QV == 1 ? 8 : (QV == 2 ? 4 : 2);  // rows in flight per lane
+    float v[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = 0.f;
+#pragma unroll
+    for (int j0 = 0; j0 < 32; j0 += NB) {
+        if ((uint32_t)j0 < nf) {
+            float4 r[NB][QV];
+#pragma unroll
+            for (int b = 0; b < NB; b++) {
+                const uint32_t id = __shfl_sync(FULL, fid, j0 + b);
+#pragma unroll
+                for (int t = 0; t < QV; t++) {
+                    const uint32_t c4 = lane + 32u * t;
+                    r[b][t] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if ((uint32_t)(j0 + b) < nf && c4 < dp4) r[b][t] = __ldg(x4 + (size_t)id * dp4 + c4);
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+#pragma unroll
+                for (int t = 0; t < QV; t++) v[j0 + b] = part4<M>(qr[t], r[b][t], v[j0 + b]);
+        }
+    }
+    // transposing butterfly: after the level of width s, v[i] holds the
+    // partial sum of distance (lane's upper bits) + i over 2x more lanes
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const bool up = (lane & s) != 0;
+#pragma unroll
+        for (int i = 0; i < s; i++) {
+            const float send = up ? v[i] : v[i + s];
+            const float keep = up ? v[i + s] : v[i];
+            v[i] = keep + __shfl_xor_sync(FULL, send, s);
+        }
+    }
+    return v[0];
+}
+
+__device__ __forceinline__ bool key_less(float da, uint32_t ia, float db, uint32_t ib) {
+    return da < db || (da == db && ia < ib);
+}
+
+// Smallest d over lanes < valid, ties to the lowest lane.
+__device__ __forceinline__ void warp_argmin(float d, uint32_t valid, uint32_t lane, float& md, uint32_t& ml) {
+    float m = lane < valid ? d : INFINITY;
+    uint32_t l = lane < valid ? lane : 32u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float om = __shfl_xor_sync(FULL, m, o);
+        const uint32_t ol = __shfl_xor_sync(FULL, l, o);
+        if (om < m || (om == m && ol < l)) {
+            m = om;
+            l = ol;
+        }
+    }
+    md = m;
+    ml = l;
+}
+
+// Bitonic sort of one (d, id) pair per lane, ascending by (d, id).
+__device__ __forceinline__ void warp_sort(float& d, uint32_t& id, uint32_t lane) {
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const float od = __shfl_xor_sync(FULL, d, j);
+            const uint32_t oi = __shfl_xor_sync(FULL, id, j);
+            const bool asc = (lane & k) == 0 || k == 32;
+            const bool low = (lane & j) == 0;
+            const bool other_less = key_less(od, oi, d, id);
+            const bool other_more = key_less(d, id, od, oi);
+            if ((low == asc) ? other_less : other_more) {
+                d = od;
+                id = oi;
+            }
+        }
+    }
+}
+
+template <int M, int QV>
+__global__ void __launch_bounds__(FW * 32) k_serve(ServeArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t slot = blockIdx.x * FW + w;
+    unsigned char* base = smem + (size_t)w * ((size_t)a.cap * 16 + 256);
+    float* bd = reinterpret_cast<float*>(base);
+    uint32_t* bi = reinterpret_cast<uint32_t*>(bd + a.cap);
+    float* td = reinterpret_cast<float*>(bi + a.cap);
+    uint32_t* ti = reinterpret_cast<uint32_t*>(td + a.cap);
+    float* nd = reinterpret_cast<float*>(ti + a.cap);
+    uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 32);
+    uint32_t* vis = a.visited + (size_t)slot * a.words;
+    uint32_t* vl = a.vlist + (size_t)slot * FVCAP;
+    const float4* x4 = reinterpret_cast<const float4*>(a.x);
+    const uint32_t nlast = a.nrows[a.L - 1];
+    unsigned long long cmps = 0, nexp = 0;
+    for (;;) {
+        uint32_t qi = 0;
+        if (lane == 0) qi = atomicAdd(a.next_q, 1u);
+        qi = __shfl_sync(FULL, qi, 0);
+        if (qi >= a.nq) break;
+        uint32_t ef = a.beams ? a.beams[qi] : a.beam;
+        if (ef < a.out_k || ef > a.cap) {
+            if (lane == 0) atomicOr(a.overflow, FERR_BEAM_RANGE);
+            ef = min(max(ef, a.out_k), a.cap);
+        }
+        float4 qr[QV];
+#pragma unroll
+        for (int t = 0; t < QV; t++) {
+            const uint32_t c4 = lane + 32u * t;
+            qr[t] = c4 < a.dp4 ? __ldg(reinterpret_cast<const float4*>(a.q) + (size_t)qi * a.dp4 + c4)
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        // entry
+        uint32_t cur, g0;
+        float cur_d;
+        if (a.probes) {
+            g0 = a.g0;
+            uint32_t pid = 0;
+            if (lane < a.nprobe) {
+                pid = a.probes[(size_t)qi * a.nprobe + lane];
+                if (pid >= a.nrows[g0]) {
+                    atomicOr(a.overflow, FERR_BAD_ID);
+                    pid = 0;
+                }
+            }
+            const float pd = warp_dists<M, QV>(qr, x4, a.dp4, pid, a.nprobe, lane);
+            uint32_t l;
+            warp_argmin(pd, a.nprobe, lane, cur_d, l);
+            cur = __shfl_sync(FULL, pid, l & 31);
+            cmps += a.nprobe;
+        } else {
+            g0 = 0;
+            cur = a.entry;
+            cur_d = __shfl_sync(FULL, warp_dists<M, QV>(qr, x4, a.dp4, cur, 1, lane), 0);
+            cmps++;
+        }
+        // greedy descent (lysearch.cpp:397-420); upper-layer ids were checked
+        // against their layers when the index was made
+        for (uint32_t g = g0; g + 1 < a.L; g++) {
+            const uint64_t* off = a.off_all + a.off_base[g];
+            uint32_t moves = 0;
+            for (;;) {
+                if (cur >= a.nrows[g] || ++moves > a.nrows[g]) {
+                    if (lane == 0) atomicOr(a.overflow, cur >= a.nrows[g] ? FERR_BAD_ID : FERR_LOOP);
+                    cur = 0;
+                    break;
+                }
+                const uint64_t b = off[cur], e = off[cur + 1];
+                float best = cur_d;
+                uint32_t bid = cur;
+                for (uint64_t c0 = b; c0 < e; c0 += 32) {
+                    const uint32_t cnt = (uint32_t)(e - c0 < 32 ? e - c0 : 32);
+                    const uint32_t nn = lane < cnt ? a.adj_all[c0 + lane] : 0u;
+                    const float dd = warp_dists<M, QV>(qr, x4, a.dp4, nn, cnt, lane);
+                    cmps += cnt;
+                    float md;
+                    uint32_t ml;
+                    warp_argmin(dd, cnt, lane, md, ml);
+                    const uint32_t mid = __shfl_sync(FULL, nn, ml & 31);
+                    if (md < best) {
+                        best = md;
+                        bid = mid;
+                    }
+                }
+                if (bid == cur) break;
+                cur = bid;
+                cur_d = best;
+            }
+        }
+        // beam on the last layer
+        const uint64_t* off = a.off_all + a.off_base[a.L - 1];
+        uint32_t m = 0, p = 0, nvis = 0;
+        if (cur < nlast) {
+            if (lane == 0) {
+                bd[0] = cur_d;
+                bi[0] = cur;
+                atomicOr(&vis[cur >> 5], 1u << (cur & 31));
+                vl[0] = cur;
+            }
+            m = 1;
+            nvis = 1;
+        } else if (lane == 0) {
+            atomicOr(a.overflow, FERR_BAD_ID);
+        }
+        __syncwarp();
+        uint32_t expansions = 0;
+        for (;;) {
+            __syncwarp();  // lane 0's expanded mark and the last merge are visible
+            uint32_t pos = m;
+            for (uint32_t s0 = p; s0 < m; s0 += 32) {
+                const bool un = s0 + lane < m && !(bi[s0 + lane] & EXP_BIT);
+                const unsigned bal = __ballot_sync(FULL, un);
+                if (bal) {
+                    pos = s0 + __ffs(bal) - 1;
+                    break;
+                }
+            }
+            if (pos >= m) break;
+            if (++expansions > nlast) {
+                if (lane == 0) atomicOr(a.overflow, FERR_LOOP);
+                break;
+            }
+            p = pos + 1;
+            const uint32_t c = bi[pos] & IDM;
+            __syncwarp();
+            if (lane == 0) bi[pos] = c | EXP_BIT;
+            nexp++;
+            const uint64_t b = off[c], e = off[c + 1];
+            for (uint64_t c0 = b; c0 < e; c0 += 32) {
+                const uint32_t cnt = (uint32_t)(e - c0 < 32 ? e - c0 : 32);
+                bool fresh = false;
+                uint32_t nn = 0;
+                if (lane < cnt) {
+                    nn = a.adj_all[c0 + lane];
+                    const uint32_t old = atomicOr(&vis[nn >> 5], 1u << (nn & 31));
+                    fresh = !(old & (1u << (nn & 31)));
+                }
+                const unsigned fb = __ballot_sync(FULL, fresh);
+                const uint32_t nf = __popc(fb);
+                if (nf == 0) continue;
+                __syncwarp();
+                if (fresh) {
+                    const uint32_t r = __popc(fb & ((1u << lane) - 1u));
+                    ni[r] = nn;
+                    if (nvis + r < FVCAP) vl[nvis + r] = nn;
+                }
+                __syncwarp();
+                const uint32_t fid = lane < nf ? ni[lane] : 0u;
+                nvis += nf;
+                cmps += nf;
+                const float dd = warp_dists<M, QV>(qr, x4, a.dp4, fid, nf, lane);
+                // accepted: below the worst entry of a full beam
+                bool acc = lane < nf;
+                if (m >= ef) acc = acc && key_less(dd, fid, bd[m - 1], bi[m - 1] & IDM);
+                const uint32_t nk = __popc(__ballot_sync(FULL, acc));
+                if (nk == 0) continue;
+                float kd = acc ? dd : INFINITY;
+                uint32_t kid = acc ? fid : 0xffffffffu;
+                warp_sort(kd, kid, lane);
+                __syncwarp();
+                nd[lane] = kd;
+                ni[lane] = kid;
+                __syncwarp();
+                const uint32_t m2 = min(ef, m + nk);
+                for (uint32_t i = lane; i < m; i += 32) {
+                    const float d0 = bd[i];
+                    const uint32_t i0 = bi[i];
+                    uint32_t lo = 0, hi = nk;
+                    while (lo < hi) {
+                        const uint32_t md = (lo + hi) >> 1;
+                        if (key_less(nd[md], ni[md], d0, i0 & IDM)) lo = md + 1;
+                        else hi = md;
+                    }
+                    if (i + lo < m2) {
+                        td[i + lo] = d0;
+                        ti[i + lo] = i0;
+                    }
+                }
+                uint32_t first = m2;
+                if (lane < nk) {
+                    uint32_t lo = 0, hi = m;
+                    while (lo < hi) {
+                        const uint32_t md = (lo + hi) >> 1;
+                        if (key_less(bd[md], bi[md] & IDM, kd, kid)) lo = md + 1;
+                        else hi = md;
+                    }
+                    if (lane + lo < m2) {
+                        td[lane + lo] = kd;
+                        ti[lane + lo] = kid;
+                    }
+                    first = lane + lo;
+                }
+                first = __shfl_sync(FULL, first, 0);
+                __syncwarp();
+                float* sd = bd;
+                bd = td;
+                td = sd;
+                uint32_t* si = bi;
+                bi = ti;
+                ti = si;
+                m = m2;
+                if (first < p) p = first;
+            }
+        }
+        // results: the first out_k entries
+        for (uint32_t t = lane; t < a.out_k; t += 32) {
+            const size_t o = (size_t)qi * a.out_k + t;
+            a.out_ids[o] = t < m ? (bi[t] & IDM) : 0xffffffffu;
+            if (a.out_d) a.out_d[o] = t < m ? bd[t] : 0.f;
+        }
+        // clear this query's visited bits
+        if (nvis <= FVCAP) {
+            for (uint32_t t = lane; t < nvis; t += 32) {
+                const uint32_t id = vl[t];
+                atomicAnd(&vis[id >> 5], ~(1u << (id & 31)));
+            }
+        } else {
+            for (uint32_t t = lane; t < a.words; t += 32) vis[t] = 0;
+        }
+        __syncwarp();
+    }
+    for (int o = 16; o > 0; o >>= 1) cmps += __shfl_xor_sync(FULL, cmps, o);
+    if (lane == 0) {
+        atomicAdd(a.ncmps, cmps / 32);
+        atomicAdd(a.nexp, nexp);
+    }
+}
+
+using ServeFn = void (*)(ServeArgs);
+template <int M>
+ServeFn pick_qv(uint32_t qv) {
+    return qv == 1 ? k_serve<M, 1> : (qv == 2 ? k_serve<M, 2> : k_serve<M, 4>);
+}
+}  // namespace
+
+int index_run_fast(Ctx& ctx, IndexDev& ix, const SearchReq& r) {
+    cudaStream_t st = ctx.stream;
+    if (ix.dp > FAST_MAX_DP) {
+        ctx.last_error = "fast search supports d <= 512";
+        return 1;
+    }
+    const uint32_t dp4 = ix.dp / 4;
+    const uint32_t qv = dp4 <= 32 ? 1 : (dp4 <= 64 ? 2 : 4);
+    const ServeFn fn = ix.metric == L2 ? pick_qv<L2>(qv) : (ix.metric == L1 ? pick_qv<L1>(qv) : pick_qv<CHI2>(qv));
+    const size_t smem = (size_t)FW * ((size_t)r.beam_max * 16 + 256);
+    NNM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int nsm = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx.device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FW * 32, smem);
+    const uint32_t blocks = (uint32_t)std::min(std::max(1, per_sm), 8) * (uint32_t)nsm;
+    const uint32_t words = (ix.n + 31) / 32;
+    const size_t slots = (size_t)blocks * FW;
+    if (ix.visited.bytes < slots * words * 4) {
+        NNM_CUDA_TRY(ix.visited.ensure(slots * words * 4));
+        NNM_CUDA_TRY(cudaMemsetAsync(ix.visited.p, 0, slots * words * 4, st));
+    }
+    NNM_CUDA_TRY(ix.vlist.ensure(slots * FVCAP * 4));
+    NNM_CUDA_TRY(cudaMemsetAsync(ix.ctr.p, 0, 64, st));
+    ServeArgs a{};
+    a.x = ix.x.as<float>();
+    a.dp4 = dp4;
+    a.L = ix.L;
+    for (uint32_t g = 0; g < ix.L; g++) {
+        a.off_base[g] = ix.off_base[g];
+        a.nrows[g] = ix.nrows[g];
+    }
+    a.off_all = ix.off.as<uint64_t>();
+    a.adj_all = ix.adj.as<uint32_t>();
+    a.q = r.q;
+    a.nq = r.nq;
+    a.beams = r.beams;
+    a.beam = r.beam;
+    a.cap = r.beam_max;
+    a.out_k = r.out_k;
+    a.entry = ix.entry;
+    a.probes = r.probes;
+    a.nprobe = r.nprobe;
+    a.g0 = r.g0;
+    a.out_ids = r.out_ids;
+    a.out_d = r.out_d;
+    a.visited = ix.visited.as<uint32_t>();
+    a.words = words;
+    a.vlist = ix.vlist.as<uint32_t>();
+    unsigned char* c = ix.ctr.as<unsigned char>();
+    a.next_q = reinterpret_cast<unsigned*>(c);
+    a.overflow = reinterpret_cast<unsigned*>(c + 4);
+    a.ncmps = reinterpret_cast<unsigned long long*>(c + 8);
+    a.nexp = reinterpret_cast<unsigned long long*>(c + 16);
+    fn<<<blocks, FW * 32, smem, st>>>(a); count_launch();
+    NNM_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace nnm

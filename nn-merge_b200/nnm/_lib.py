@@ -66,6 +66,34 @@ def _mlp_struct(m):
                m["w2"].ctypes.data, m["b2"].ctypes.data)
 
 
+class EntryMlp(ctypes.Structure):
+    _fields_ = [("d_in", ctypes.c_uint32), ("n_classes", ctypes.c_uint32), ("in_scale", ctypes.c_float),
+                ("in_shift", ctypes.c_float), ("w1", ctypes.c_void_p), ("b1", ctypes.c_void_p),
+                ("w2", ctypes.c_void_p), ("b2", ctypes.c_void_p)]
+
+
+class SearchStats(ctypes.Structure):
+    _fields_ = [("ncmps", ctypes.c_uint64), ("expansions", ctypes.c_uint64), ("device_ms", ctypes.c_double),
+                ("predict_ms", ctypes.c_double)]
+
+
+def entry_init(d, n_classes, seed=0, in_scale=1.0 / 64.0, in_shift=-1.0):
+    """A fresh entry-point network (He-initialised weights, zero biases) as a
+    dict of float32 arrays: w1 (256 x d), b1 (256), w2 (C x 256), b2 (C)."""
+    rng = np.random.default_rng(seed)
+    return dict(w1=(rng.standard_normal((MLP_HIDDEN, d)) * np.sqrt(2.0 / d)).astype(np.float32),
+                b1=np.zeros(MLP_HIDDEN, np.float32),
+                w2=(rng.standard_normal((n_classes, MLP_HIDDEN)) * np.sqrt(1.0 / MLP_HIDDEN)).astype(np.float32),
+                b2=np.zeros(n_classes, np.float32), in_scale=float(in_scale), in_shift=float(in_shift))
+
+
+def _entry_struct(m):
+    for k in ("w1", "b1", "w2", "b2"):
+        m[k] = np.ascontiguousarray(m[k], np.float32)
+    return EntryMlp(m["w1"].shape[1], m["w2"].shape[0], m["in_scale"], m["in_shift"], m["w1"].ctypes.data,
+                    m["b1"].ctypes.data, m["w2"].ctypes.data, m["b2"].ctypes.data)
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("ncmps", ctypes.c_uint64), ("sub_ncmps", ctypes.c_uint64), ("iterations", ctypes.c_uint32),
                 ("n_trace", ctypes.c_uint32), ("trace", ctypes.c_float * 256), ("device_ms", ctypes.c_double)]
@@ -108,6 +136,15 @@ def load():
         lib.nnm_mlp_grad.argtypes = [vp, vp, vp, u64, u32, vp, u32, ctypes.c_float, vp, vp]
         lib.nnm_mlp_codes.argtypes = [vp, vp, vp, u64, u32, vp, vp]
         lib.nnm_set_init_model.argtypes = [vp, vp]
+        lib.nnm_index_create.argtypes = [vp, vp, u64, u32, vp, u32, u32, ctypes.POINTER(ctypes.c_void_p)]
+        lib.nnm_index_free.argtypes = [vp]
+        for name in ("nnm_index_search", "nnm_index_search_dev"):
+            getattr(lib, name).argtypes = [vp, vp, u64, vp, u32, u32, u32, u32, vp, vp, vp]
+        lib.nnm_index_entry_layer.argtypes = [vp, vp, vp]
+        lib.nnm_entry_forward.argtypes = [vp, vp, vp, u64, u32, vp]
+        lib.nnm_entry_grad.argtypes = [vp, vp, vp, u64, u32, vp, vp, vp]
+        lib.nnm_entry_train.argtypes = [vp, vp, vp, vp]
+        lib.nnm_index_set_entry_model.argtypes = [vp, vp, u32]
         _lib = lib
     return _lib
 
@@ -301,16 +338,7 @@ class Context:
     def search(self, x, layers, q, topk, seed=0, metric="l2"):
         x = np.ascontiguousarray(x, np.float32)
         q = np.ascontiguousarray(q, np.float32)
-        lay = Layers()
-        lay.nlayers = len(layers)
-        keep = []
-        for g, (off, adj) in enumerate(layers):
-            off = np.ascontiguousarray(off, np.uint64)
-            adj = np.ascontiguousarray(adj if len(adj) else np.zeros(1, np.uint32), np.uint32)
-            keep += [off, adj]
-            lay.nrows[g] = len(off) - 1
-            lay.off[g] = off.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
-            lay.adj[g] = adj.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        lay, keep = _layers_struct(layers)
         nq = q.shape[0]
         ids = np.empty((nq, topk), np.uint32)
         ds = np.empty((nq, topk), np.float32)
@@ -319,3 +347,121 @@ class Context:
         self._check(self.lib.nnm_search(self.h, _ptr(x), x.shape[0], x.shape[1], ctypes.byref(lay), _ptr(q), nq,
                                         topk, ctypes.byref(o), _ptr(ids), _ptr(ds), ctypes.byref(nc)))
         return dict(ids=ids, dists=ds, ncmps=int(nc.value))
+
+    # -- serving ------------------------------------------------------------
+    def index(self, x, layers, seed=0, metric="l2"):
+        """A resident search index over x and its hierarchy (list of (off, adj))."""
+        return Index(self, x, layers, seed, metric)
+
+    def entry_forward(self, model, x):
+        x = np.ascontiguousarray(x, np.float32)
+        n, d = x.shape
+        ms = _entry_struct(model)
+        s = np.empty((n, ms.n_classes), np.float32)
+        self._check(self.lib.nnm_entry_forward(self.h, ctypes.byref(ms), _ptr(x), n, d, _ptr(s)))
+        return s
+
+    def entry_grad(self, model, x, labels):
+        x = np.ascontiguousarray(x, np.float32)
+        lab = np.ascontiguousarray(labels, np.uint32)
+        n, d = x.shape
+        grad = {k: np.zeros_like(np.asarray(model[k], np.float32)) for k in ("w1", "b1", "w2", "b2")}
+        grad.update(in_scale=model["in_scale"], in_shift=model["in_shift"])
+        ms, gs = _entry_struct(model), _entry_struct(grad)
+        loss = ctypes.c_float()
+        self._check(self.lib.nnm_entry_grad(self.h, ctypes.byref(ms), _ptr(x), n, d, _ptr(lab), ctypes.byref(loss),
+                                            ctypes.byref(gs)))
+        return float(loss.value), grad
+
+
+def _layers_struct(layers):
+    lay = Layers()
+    lay.nlayers = len(layers)
+    keep = []
+    for g, (off, adj) in enumerate(layers):
+        off = np.ascontiguousarray(off, np.uint64)
+        adj = np.ascontiguousarray(adj if len(adj) else np.zeros(1, np.uint32), np.uint32)
+        keep += [off, adj]
+        lay.nrows[g] = len(off) - 1
+        lay.off[g] = off.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        lay.adj[g] = adj.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+    return lay, keep
+
+
+SERVE_MODES = {"exact": 0, "fast": 1}
+ENTRY_MODES = {"default": 0, "learned": 1}
+
+
+class Index:
+    """nnm_index: vectors and hierarchy resident on the device, batched
+    LySearch with per-query beam widths and default or learned entries."""
+
+    def __init__(self, ctx, x, layers, seed=0, metric="l2"):
+        self.ctx = ctx
+        x = np.ascontiguousarray(x, np.float32)
+        self.n, self.d = x.shape
+        lay, keep = _layers_struct(layers)
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.nnm_index_create(ctx.h, _ptr(x), self.n, self.d, ctypes.byref(lay), seed,
+                                            METRICS[metric], ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.nnm_index_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def search(self, q, out_k=10, beams=None, beam=None, mode="fast", entry="default"):
+        q = np.ascontiguousarray(q, np.float32)
+        nq = q.shape[0]
+        b = None if beams is None else np.ascontiguousarray(beams, np.uint32)
+        if beam is None:
+            beam = out_k if b is None else int(b.max())
+        ids = np.empty((nq, out_k), np.uint32)
+        ds = np.empty((nq, out_k), np.float32)
+        st = SearchStats()
+        self.ctx._check(self.ctx.lib.nnm_index_search(self.h, _ptr(q), nq, _ptr(b), beam, out_k, SERVE_MODES[mode],
+                                                      ENTRY_MODES[entry], _ptr(ids), _ptr(ds), ctypes.byref(st)))
+        return dict(ids=ids, dists=ds, ncmps=int(st.ncmps), expansions=int(st.expansions),
+                    device_ms=float(st.device_ms), predict_ms=float(st.predict_ms))
+
+    def search_dev(self, q_ptr, nq, out_ids_ptr, out_d_ptr, out_k, beams_ptr=0, beam=None, mode="fast",
+                   entry="default"):
+        """Device-pointer form: q (nq x d float32), beams (nq uint32, `beam`
+        >= every width), out_ids / out_d (nq x out_k)."""
+        st = SearchStats()
+        self.ctx._check(self.ctx.lib.nnm_index_search_dev(self.h, ctypes.c_void_p(q_ptr), nq,
+                                                          ctypes.c_void_p(beams_ptr), beam, out_k, SERVE_MODES[mode],
+                                                          ENTRY_MODES[entry], ctypes.c_void_p(out_ids_ptr),
+                                                          ctypes.c_void_p(out_d_ptr), ctypes.byref(st)))
+        return dict(ncmps=int(st.ncmps), expansions=int(st.expansions), device_ms=float(st.device_ms),
+                    predict_ms=float(st.predict_ms))
+
+    def entry_layer(self):
+        layer, nc = ctypes.c_uint32(), ctypes.c_uint32()
+        self.ctx._check(self.ctx.lib.nnm_index_entry_layer(self.h, ctypes.byref(layer), ctypes.byref(nc)))
+        return int(layer.value), int(nc.value)
+
+    def entry_train(self, model, steps=1000, batch=2048, lr=2e-3, seed=0):
+        """Trains the entry network `model` (dict from entry_init) in place on
+        the index's rows; returns the per-step losses."""
+        o = TrainOpts()
+        self.ctx.lib.nnm_train_opts_default(ctypes.byref(o))
+        o.steps, o.batch, o.lr, o.seed = steps, batch, lr, seed
+        ms = _entry_struct(model)
+        loss = np.empty(steps, np.float32)
+        self.ctx._check(self.ctx.lib.nnm_entry_train(self.h, ctypes.byref(ms), ctypes.byref(o), _ptr(loss)))
+        return loss
+
+    def set_entry_model(self, model, probes=4):
+        if model is None:
+            self.ctx._check(self.ctx.lib.nnm_index_set_entry_model(self.h, None, 0))
+            return
+        ms = _entry_struct(model)
+        self.ctx._check(self.ctx.lib.nnm_index_set_entry_model(self.h, ctypes.byref(ms), probes))

@@ -897,8 +897,21 @@ static void pq_pop(pq_t *q) {
 int nno_search(const float *x, uint32_t n, uint32_t d, const nno_layers *layers,
                const float *q, uint32_t nq, uint32_t topk, int metric, uint32_t seed,
                uint32_t *out_ids, float *out_dists, uint64_t *ncmps, uint32_t *entry) {
-    if (!layers || layers->nlayers < 1 || topk == 0) return -1;
+    return nno_search_ex(x, n, d, layers, q, nq, NULL, topk, topk, NULL, 0, 0, metric, seed, out_ids, out_dists,
+                         ncmps, entry);
+}
+
+/* The serving form: query i searches with beam width beams[i] (or `beam`)
+ * and keeps its first out_k results; with probes (nq x nprobe rows of layer
+ * g0) a query starts at the first nearest of its probes, in probe order,
+ * and descends from layer g0 instead of from the global entry on layer 0. */
+int nno_search_ex(const float *x, uint32_t n, uint32_t d, const nno_layers *layers,
+                  const float *q, uint32_t nq, const uint32_t *beams, uint32_t beam, uint32_t out_k,
+                  const uint32_t *probes, uint32_t nprobe, uint32_t g0, int metric, uint32_t seed,
+                  uint32_t *out_ids, float *out_dists, uint64_t *ncmps, uint32_t *entry) {
+    if (!layers || layers->nlayers < 1 || beam == 0 || out_k == 0) return -1;
     const uint32_t L = layers->nlayers;
+    if (probes && (nprobe == 0 || g0 >= L)) return -1;
     grand_t rnd;
     grand_seed(&rnd, seed);
     uint32_t enter = (uint32_t)grand_next(&rnd) % layers->nrows[0];  /* lysearch.cpp:382 */
@@ -909,10 +922,24 @@ int nno_search(const float *x, uint32_t n, uint32_t d, const nno_layers *layers,
     uint64_t cmps = 0;
     for (uint32_t qi = 0; qi < nq; qi++) {
         const float *qv = q + (size_t)qi * d;
-        uint32_t cur = enter;
-        float cur_d = nno_dist(qv, 0, x, cur, d, metric);
-        cmps++;
-        for (uint32_t ir = 0; ir + 1 < L; ir++) {                    /* :397-420 */
+        const uint32_t topk = beams ? beams[qi] : beam;
+        uint32_t cur = enter, gstart = 0;
+        float cur_d;
+        if (probes) {
+            gstart = g0;
+            cur = probes[(size_t)qi * nprobe];
+            cur_d = nno_dist(qv, 0, x, cur, d, metric);
+            for (uint32_t j = 1; j < nprobe; j++) {
+                const uint32_t pj = probes[(size_t)qi * nprobe + j];
+                const float dj = nno_dist(qv, 0, x, pj, d, metric);
+                if (dj < cur_d) { cur_d = dj; cur = pj; }
+            }
+            cmps += nprobe;
+        } else {
+            cur_d = nno_dist(qv, 0, x, cur, d, metric);
+            cmps++;
+        }
+        for (uint32_t ir = gstart; ir + 1 < L; ir++) {                    /* :397-420 */
             const uint64_t *off = layers->off[ir];
             const uint32_t *adj = layers->adj[ir];
             int moved = 1;
@@ -956,13 +983,15 @@ int nno_search(const float *x, uint32_t n, uint32_t d, const nno_layers *layers,
                 }
             }
         }
-        for (uint32_t t = 0; t < topk; t++) {
-            out_ids[(size_t)qi * topk + t] = 0xffffffffu;
-            out_dists[(size_t)qi * topk + t] = 0.f;
+        for (uint32_t t = 0; t < out_k; t++) {
+            out_ids[(size_t)qi * out_k + t] = 0xffffffffu;
+            out_dists[(size_t)qi * out_k + t] = 0.f;
         }
         for (long loc = (long)top.n - 1; loc >= 0; loc--) {
-            out_ids[(size_t)qi * topk + loc] = top.a[0].second;
-            out_dists[(size_t)qi * topk + loc] = top.a[0].first;
+            if ((uint32_t)loc < out_k) {
+                out_ids[(size_t)qi * out_k + loc] = top.a[0].second;
+                out_dists[(size_t)qi * out_k + loc] = top.a[0].first;
+            }
             pq_pop(&top);
         }
         for (uint32_t t = 0; t < npts; t++) flags[pts[t]] = 0;

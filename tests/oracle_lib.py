@@ -117,6 +117,44 @@ class Oracle:
             raise RuntimeError("oracle search failed")
         return dict(ids=ids, dists=ds, ncmps=int(nc.value), entry=int(ent.value))
 
+    def search_ex(self, x, layers, q, out_k, seed, beams=None, beam=None, probes=None, g0=0, metric="l2"):
+        """Serving form: per-query beams, the first out_k results, optional
+        learned entries (probes: nq x P rows of layer g0)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        q = np.ascontiguousarray(q, dtype=np.float32)
+        lay = Layers()
+        lay.nlayers = len(layers)
+        keep = []
+        for g, (off, adj) in enumerate(layers):
+            off = np.ascontiguousarray(off, np.uint64)
+            adj = np.ascontiguousarray(adj if len(adj) else np.zeros(1, np.uint32), np.uint32)
+            keep += [off, adj]
+            lay.nrows[g] = len(off) - 1
+            lay.off[g] = _p(off, ctypes.c_uint64)
+            lay.adj[g] = _p(adj, ctypes.c_uint32)
+        nq = q.shape[0]
+        b = None if beams is None else np.ascontiguousarray(beams, np.uint32)
+        pr = None if probes is None else np.ascontiguousarray(probes, np.uint32)
+        if beam is None:
+            beam = out_k if b is None else int(b.max())
+        ids = np.zeros((nq, out_k), np.uint32)
+        ds = np.zeros((nq, out_k), np.float32)
+        nc = ctypes.c_uint64(0)
+        ent = ctypes.c_uint32(0)
+        nul = ctypes.POINTER(ctypes.c_uint32)()
+        rc = self.lib.nno_search_ex(_p(x, ctypes.c_float), ctypes.c_uint32(x.shape[0]),
+                                    ctypes.c_uint32(x.shape[1]), ctypes.byref(lay),
+                                    _p(q, ctypes.c_float), ctypes.c_uint32(nq),
+                                    nul if b is None else _p(b, ctypes.c_uint32), ctypes.c_uint32(beam),
+                                    ctypes.c_uint32(out_k), nul if pr is None else _p(pr, ctypes.c_uint32),
+                                    ctypes.c_uint32(0 if pr is None else pr.shape[1]), ctypes.c_uint32(g0),
+                                    ctypes.c_int(METRICS[metric]), ctypes.c_uint32(seed),
+                                    _p(ids, ctypes.c_uint32), _p(ds, ctypes.c_float),
+                                    ctypes.byref(nc), ctypes.byref(ent))
+        if rc:
+            raise RuntimeError("oracle search failed")
+        return dict(ids=ids, dists=ds, ncmps=int(nc.value), entry=int(ent.value))
+
     def glibc_rand(self, seed, count):
         out = np.zeros(count, np.int32)
         self.lib.nno_glibc_rand(ctypes.c_uint32(seed), ctypes.c_uint32(count), _p(out, ctypes.c_int32))
