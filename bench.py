@@ -26,6 +26,12 @@ Printed JSON (one line, rank 0):
   cpu_baseline the reference itself (oracle/_ref, built from its sources) on
               a bounded sample, extrapolated linearly to 1M rows.
 
+--workload search measures batched LySearch serving instead (one step = a
+batch of 100,000 queries, top-10, beam widths drawn from 32..512, through
+nnm_index_search_dev on the 1M-row H-Merge hierarchy): `value` is queries/s
+with the learned entry, beside the default entry and the learned entry at
+narrower beams down to the default's recall@10.
+
 --impl reference times the reference's CPU path instead (rank 0 only).
 Multi-GPU (torchrun, N > 1): every rank builds its own 1M graph from its own
 seeded data (independent replicas, weak scaling), timed as the max over ranks.
@@ -78,6 +84,11 @@ def parse():
                    help="initial graphs: random, or from the codes of a trained MLP (needs --path fast)")
     p.add_argument("--train-steps", type=int, default=400)
     p.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 path beside")
+    p.add_argument("--workload", default="build", choices=["build", "search"],
+                   help="build: the headline 1M graph build; search: batched LySearch serving on a 1M hierarchy")
+    p.add_argument("--queries", type=int, default=100_000)
+    p.add_argument("--probes", type=int, default=4)
+    p.add_argument("--entry-steps", type=int, default=1500)
     return p.parse_args()
 
 
@@ -228,13 +239,214 @@ def run_reference_arm(a, rank):
     print(json.dumps(line), flush=True)
 
 
+SEARCH_METRIC = ("LySearch queries/s, 1M×128 k=20 H-Merge hierarchy, 100K queries, top-10, beams U{32..512}: "
+                 "learned vs default entry at equal recall@10")
+
+
+def search_truth(x_t, q, torch, k=10):
+    """k-th exact neighbour distance of every query: FP32 GEMM candidates
+    (top 16, no TF32) re-ranked in float64."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        xn = (x_t * x_t).sum(1)
+        x_np = x_t.cpu().numpy()
+        kth = np.empty(len(q))
+        for i in range(0, len(q), 500):
+            qt = torch.from_numpy(q[i:i + 500]).cuda()
+            d = (qt * qt).sum(1)[:, None] + xn[None, :] - 2.0 * (qt @ x_t.T)
+            cand = torch.topk(d, 16, dim=1, largest=False).indices.cpu().numpy()
+            ex = ((x_np[cand].astype(np.float64) - q[i:i + 500, None, :]) ** 2).sum(-1)
+            kth[i:i + 500] = np.sort(ex, axis=1)[:, k - 1]
+        return kth
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
+def search_recall(ids, x, q, kth):
+    """Results whose exact distance is within the query's k-th exact distance."""
+    d = ((x[ids.astype(np.int64)].astype(np.float64) - q[:, None, :].astype(np.float64)) ** 2).sum(-1)
+    return float((d <= kth[:, None] + 1e-6).mean())
+
+
+def search_cpu(x, layers, q, beams, seed, sample):
+    """The oracle's restatement of LySearch (nno_search_ex: the reference's
+    heaps and float sums, one thread) on the first `sample` queries."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    o = Oracle()
+    t0 = time.perf_counter()
+    o.search_ex(x, layers, q[:sample], 10, seed, beams=beams[:sample])
+    return time.perf_counter() - t0
+
+
+def run_search(a, rank, world, local):
+    """Serving workload (one step = one batch of `queries` queries through
+    nnm_index_search_dev with the vectors, hierarchy and queries resident)."""
+    import torch
+    import nnm
+    from nnm.datasets import gaussian_mixture_u8, queries_like
+    from nnm.replicas import Replicas
+
+    torch.cuda.set_device(local)
+    reps = Replicas("nccl")
+    n, d, k, nq = a.n, a.d, a.k, a.queries
+    seed = reps.data_seed(a.seed)
+    x = gaussian_mixture_u8(n, d=d, n_centres=a.centres, seed=seed)
+    q = queries_like(nq, d=d, n_centres=a.centres, seed=seed, query_seed=seed + 77)
+    beams = np.random.default_rng(seed + 5).integers(32, 513, size=nq).astype(np.uint32)
+    ctx = nnm.Context(local)
+    t0 = time.perf_counter()
+    h = ctx.hmerge(x, k, 20, seed=a.seed, rng="fast", join="tensor")
+    ix = ctx.index(x, h["layers"], seed=a.seed)
+    layer, C = ix.entry_layer()
+    model = nnm.entry_init(d, C, seed=11)
+    losses = ix.entry_train(model, steps=a.entry_steps, batch=2048, lr=2e-3, seed=3)
+    ix.set_entry_model(model, probes=a.probes)
+    prep_s = time.perf_counter() - t0
+    x_t = torch.from_numpy(x).cuda()
+    q_dev = torch.from_numpy(q).cuda()
+    oi = torch.empty((nq, 10), dtype=torch.int32, device="cuda")
+    od = torch.empty((nq, 10), dtype=torch.float32, device="cuda")
+    nrec = min(nq, 10_000)
+    kth = search_truth(x_t, q[:nrec], torch)
+
+    def timed(entry, scale=1.0, steps=a.steps, warm=a.warmup):
+        b = np.maximum(10, np.round(beams * scale)).astype(np.uint32)
+        b_dev = torch.from_numpy(b.astype(np.int32)).cuda()
+        kw = dict(beams_ptr=b_dev.data_ptr(), beam=int(b.max()), mode="fast", entry=entry)
+        for _ in range(warm):
+            ix.search_dev(q_dev.data_ptr(), nq, oi.data_ptr(), od.data_ptr(), 10, **kw)
+        torch.cuda.synchronize()
+        tot = pred = 0.0
+        cm = ex = 0
+        l0 = ctx.launch_count()
+        reps.barrier()
+        for _ in range(steps):
+            st = ix.search_dev(q_dev.data_ptr(), nq, oi.data_ptr(), od.data_ptr(), 10, **kw)
+            tot += st["device_ms"]
+            pred += st["predict_ms"]
+            cm += st["ncmps"]
+            ex += st["expansions"]
+        reps.barrier()
+        ids = oi[:nrec].cpu().numpy().view(np.uint32)
+        return dict(ms=tot / steps, predict_ms=pred / steps, ncmps=cm / steps, expansions=ex / steps,
+                    launches=ctx.launch_count() - l0, recall=search_recall(ids, x, q[:nrec], kth), scale=scale)
+
+    with ClockSampler(local) as clocks:
+        learned = timed("learned")
+    default = timed("default")
+    # equal recall: the learned entry at narrower beams, down to the default's recall
+    sweep = []
+    for sc in (0.7, 0.5, 0.3, 0.2, 0.15, 0.1, 0.07, 0.05):
+        r = timed("learned", sc, steps=1, warm=1)
+        sweep.append({"scale": sc, "recall": r["recall"], "qps": nq / r["ms"] * 1e3})
+        if r["recall"] < default["recall"]:
+            break
+    eq = [s for s in sweep if s["recall"] >= default["recall"]]
+    ms = reps.max(learned["ms"])
+    value = world * nq / (ms / 1e3)
+
+    # end to end through the host C ABI: pinned queries and beams in, ids and distances out
+    e2e = None
+    if not a.no_e2e:
+        q_pin = torch.from_numpy(q).pin_memory().numpy()
+        b_pin = torch.from_numpy(beams.astype(np.int32)).pin_memory().numpy().view(np.uint32)
+        ix.search(q_pin, out_k=10, beams=b_pin, mode="fast", entry="learned")
+        reps.barrier()
+        t1 = time.perf_counter()
+        for _ in range(a.steps):
+            ix.search(q_pin, out_k=10, beams=b_pin, mode="fast", entry="learned")
+        e2e_s = reps.max((time.perf_counter() - t1) / a.steps)
+        e2e = {"value": world * nq / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": int(q.nbytes + beams.nbytes),
+               "d2h_bytes_per_step": int(nq * 10 * 8)}
+
+    hbm, peak_kind = peaks()
+    kern_ms = learned["ms"] - learned["predict_ms"]
+    row_bytes = ((d + 3) // 4) * 16
+    achieved = learned["ncmps"] * row_bytes / (kern_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": "k_serve<L2,1> (warp-per-query beam search, fast kernel)",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+            "traffic": None,
+            "algorithmic_bytes": "distance evaluations x %d B (one vector row each) per step" % row_bytes,
+            "kernel_ms": kern_ms, "predict_ms": learned["predict_ms"]}
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        sample = 2000
+        t = search_cpu(x, h["layers"], q, beams, a.seed, sample)
+        cpu = {"value": sample / t, "unit": "queries/s", "cores": 1, "kind": "port",
+               "sample": "the oracle's LySearch (nno_search_ex, reference heaps and sums) on the first %d queries "
+                         "with their beams, default entry, single thread (%.1f s)" % (sample, t)}
+    if rank == 0:
+        line = {
+            "metric": SEARCH_METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded %d-centre Gaussian mixture, integers 0-255; queries from the same mixture "
+                    "(fresh seed)" % a.centres,
+            "config": {"workload": "LySearch batch of %d queries, top-10, beams U{32..512}, fast kernel, learned "
+                                   "entry (probes %d), on the H-Merge hierarchy of %dx%d k=%d"
+                                   % (nq, a.probes, n, d, k),
+                       "n": n, "d": d, "k": k, "queries": nq, "layers": [len(o) - 1 for o, _ in h["layers"]],
+                       "entry_layer": layer, "classes": C, "entry_train_steps": a.entry_steps,
+                       "entry_loss_first": float(losses[:20].mean()), "entry_loss_last": float(losses[-20:].mean()),
+                       "prep_s": prep_s, "recall@10": learned["recall"], "recall_rows": nrec,
+                       "learned": learned, "default": default,
+                       "qps_default": nq / default["ms"] * 1e3,
+                       "equal_recall": {"default_recall": default["recall"], "sweep": sweep,
+                                        "learned_qps_at_default_recall": eq[-1]["qps"] if eq else None,
+                                        "speedup": (eq[-1]["qps"] / (nq / default["ms"] * 1e3)) if eq else None},
+                       "l2": "vectors (%d MB) larger than L2 (126 MB)" % (x.nbytes >> 20),
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": learned["launches"],
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ix.close()
+    ctx.close()
+    reps.close()
+
+
+def run_search_reference_arm(a, rank):
+    """The oracle's LySearch (the reference's steps, one thread) on a bounded
+    sample of the serving workload; the hierarchy is built by the library
+    (a CPU H-Merge of 1M rows does not fit the run)."""
+    if rank != 0:
+        return
+    import nnm
+    from nnm.datasets import gaussian_mixture_u8, queries_like
+    x = gaussian_mixture_u8(a.n, d=a.d, n_centres=a.centres, seed=a.seed)
+    q = queries_like(2000, d=a.d, n_centres=a.centres, seed=a.seed, query_seed=a.seed + 77)
+    beams = np.random.default_rng(a.seed + 5).integers(32, 513, size=len(q)).astype(np.uint32)
+    ctx = nnm.Context(0)
+    h = ctx.hmerge(x, a.k, 20, seed=a.seed, rng="fast", join="tensor")
+    ctx.close()
+    times = [search_cpu(x, h["layers"], q, beams, a.seed, 500) for _ in range(max(1, a.steps))]
+    v = 500 / statistics.median(times)
+    line = {"metric": SEARCH_METRIC, "impl": "reference", "value": v, "unit": "queries/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": statistics.median(times) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic, as the nnm arm", "config": {"workload": "500 queries per step, default entry",
+                                                           "n": a.n, "d": a.d, "k": a.k},
+            "cpu_baseline": {"value": v, "unit": "queries/s", "cores": 1, "kind": "port",
+                             "sample": "500 queries with their beams, single thread"},
+            "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
-        run_reference_arm(a, rank)
+        if a.workload == "search":
+            run_search_reference_arm(a, rank)
+        else:
+            run_reference_arm(a, rank)
+        return
+    if a.workload == "search":
+        run_search(a, rank, world, local)
         return
 
     import torch

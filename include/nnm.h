@@ -287,13 +287,21 @@ int nnm_index_search_dev(nnm_index *ix, const float *q_dev, uint64_t nq, const u
                          uint32_t beam, uint32_t out_k, uint32_t serve_mode, uint32_t entry_mode,
                          uint32_t *out_ids_dev, float *out_dists_dev, nnm_search_stats *stats);
 
+/* NNM_SERVE_FAST only: a step of a query with beam width ef expands its
+ * min(width, max(1, ef / 64)) nearest unexpanded beam entries together and
+ * reads their lists as one sequence, so their memory latencies overlap
+ * (1: strict best-first order, as the reference).  width is in 1..4,
+ * default 4; wider steps may expand a few more nodes. */
+int nnm_index_set_width(nnm_index *ix, uint32_t width);
+
 /* Entry-point network (no counterpart in the reference): its classes are
  * rows 0..C-1 of the data set (C <= NNM_ENTRY_MAX_CLASSES), and a learned
  * search starts its greedy descent on the first layer that holds them all.
  * nnm_index_entry_layer gives the default: the deepest layer with at most
  * NNM_ENTRY_MAX_CLASSES rows (C = its rows), else layer 0 with C = 4096.
  *   u = x * in_scale + in_shift,  h = relu(W1 u + b1),  s = W2 h + b2,
- * d_in (<= 256) -> 256 -> C, BF16-rounded weights, FP32 accumulation.
+ * d_in (<= 256) -> 256 -> C, BF16-rounded weights, FP32 accumulation
+ * (inference also rounds h to BF16, the tensor-core operand).
  * Training minimises the softmax cross-entropy of s against the nearest
  * class row (squared L2) of each training row, with Adam on FP32 master
  * weights.  w1 is 256 x d_in, w2 is C x 256 (row-major). */
@@ -305,9 +313,15 @@ typedef struct {
 } nnm_entry_mlp;
 
 int nnm_index_entry_layer(const nnm_index *ix, uint32_t *layer, uint32_t *n_classes);
-/* Scores (n x C) of x (n x d). */
+/* Scores (n x C) of x (n x d) as the search computes them: h rounded to
+ * BF16, s = W2 h + b2 on the tensor cores (BF16 operands, FP32 sums). */
 int nnm_entry_forward(nnm_ctx *ctx, const nnm_entry_mlp *model, const float *x, uint64_t n, uint32_t d,
                       float *scores);
+/* The probes a learned search takes for x: the classes of each row's
+ * `probes` (1..min(8, C)) largest scores, ties to the lower class, in
+ * descending order (n x probes). */
+int nnm_entry_probes(nnm_ctx *ctx, const nnm_entry_mlp *model, const float *x, uint64_t n, uint32_t d,
+                     uint32_t probes, uint32_t *out);
 /* Mean cross-entropy over the rows of x against labels (n classes) and its
  * gradients w.r.t. the BF16-rounded weights; grad has the model's shapes. */
 int nnm_entry_grad(nnm_ctx *ctx, const nnm_entry_mlp *model, const float *x, uint64_t n, uint32_t d,

@@ -589,12 +589,15 @@ int index_search_impl(nnm_index* h, const float* q, uint64_t nq, const uint32_t*
     r.out_k = out_k;
     r.out_ids = oi;
     r.out_d = od;
+    if ((rc = cu(cudaMemsetAsync(ix.ctr.p, 0, 64, st)))) return rc;
     cudaEvent_t ev[3];
     for (auto& e : ev) cudaEventCreate(&e);
     cudaEventRecord(ev[0], st);
     if (emode == NNM_ENTRY_LEARNED) {
         rc = cu(ix.probes.ensure((size_t)nq * ix.nprobe * 4));
-        if (!rc) rc = nnm::entry_predict(c, ix, qd, (uint32_t)nq, ix.probes.as<uint32_t>());
+        if (!rc)
+            rc = nnm::entry_predict(c, ix, qd, (uint32_t)nq, ix.probes.as<uint32_t>(),
+                                    reinterpret_cast<unsigned*>(ix.ctr.as<unsigned char>() + 4));
         r.probes = ix.probes.as<uint32_t>();
         r.nprobe = ix.nprobe;
         r.g0 = ix.entry_layer;
@@ -651,6 +654,13 @@ int nnm_index_search_dev(nnm_index* ix, const float* q, uint64_t nq, const uint3
     return index_search_impl(ix, q, nq, beams, beam, out_k, serve_mode, entry_mode, out_ids, out_dists, stats, true);
 }
 
+int nnm_index_set_width(nnm_index* h, uint32_t width) {
+    if (!h) return NNM_ERR_INVALID;
+    if (width < 1 || width > 4) return fail(h->ctx, NNM_ERR_INVALID, "width must be in [1, 4]");
+    h->ix.width = width;
+    return NNM_OK;
+}
+
 int nnm_index_entry_layer(const nnm_index* h, uint32_t* layer, uint32_t* n_classes) {
     if (!h || !layer || !n_classes) return NNM_ERR_INVALID;
     const nnm::IndexDev& ix = h->ix;
@@ -665,29 +675,56 @@ int nnm_index_entry_layer(const nnm_index* h, uint32_t* layer, uint32_t* n_class
     return NNM_OK;
 }
 
-int nnm_entry_forward(nnm_ctx* ctx, const nnm_entry_mlp* model, const float* x, uint64_t n, uint32_t d,
-                      float* scores) {
-    if (!ctx || !x || !scores || n == 0 || n >= (1ull << 30)) return NNM_ERR_INVALID;
-    if (!entry_ok(ctx, model, d)) return NNM_ERR_INVALID;
+namespace {
+// Scores (when scores is non-null) or probes of x through the inference kernels.
+int entry_infer_host(nnm_ctx* ctx, const nnm_entry_mlp* model, const float* x, uint64_t n, uint32_t d,
+                     float* scores, uint32_t P, uint32_t* probes) {
     Ctx& c = ctx->c;
     if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
     nnm::DevEntry m;
     GraphStore st;
     GraphDev g;
-    nnm::DevBuf hb, sb;
+    nnm::DevBuf hb, ob, eb;
+    const size_t out_bytes = scores ? n * model->n_classes * 4 : n * P * 4;
     int rc = nnm::entry_upload(c, m, *model);
     if (!rc) rc = upload_plain(c, st, g, x, n, d);
-    if (!rc && (hb.ensure(n * nnm::ENTRY_H * 4) != cudaSuccess || sb.ensure(n * model->n_classes * 4) != cudaSuccess))
+    if (!rc && (hb.ensure(n * nnm::ENTRY_H * 2) != cudaSuccess || ob.ensure(out_bytes) != cudaSuccess ||
+                eb.ensure(16) != cudaSuccess))
         rc = fail(ctx, NNM_ERR_OOM, "device allocation failed");
-    if (!rc) rc = nnm::entry_scores_dev(c, m, g.x, (uint32_t)n, g.dp, hb.as<float>(), sb.as<float>());
-    if (!rc && cudaStreamSynchronize(c.stream) != cudaSuccess) rc = fail(ctx, NNM_ERR_CUDA, "entry forward failed");
-    if (!rc && cudaMemcpy(scores, sb.p, n * model->n_classes * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (!rc && cudaMemsetAsync(eb.p, 0, 16, c.stream) != cudaSuccess) rc = NNM_ERR_CUDA;
+    if (!rc)
+        rc = nnm::entry_infer(c, m, g.x, (uint32_t)n, g.dp, hb.p, scores ? ob.as<float>() : nullptr, P,
+                              scores ? nullptr : ob.as<uint32_t>(), eb.as<unsigned>());
+    if (!rc && cudaStreamSynchronize(c.stream) != cudaSuccess) rc = fail(ctx, NNM_ERR_CUDA, "entry inference failed");
+    unsigned e = 0;
+    if (!rc && cudaMemcpy(&e, eb.p, 4, cudaMemcpyDeviceToHost) != cudaSuccess) rc = NNM_ERR_CUDA;
+    if (!rc && e) rc = fail(ctx, NNM_ERR_CAPACITY, "entry inference: a bounded wait ran out");
+    if (!rc && cudaMemcpy(scores ? (void*)scores : (void*)probes, ob.p, out_bytes, cudaMemcpyDeviceToHost) !=
+                   cudaSuccess)
         rc = NNM_ERR_CUDA;
     m.release();
     st.release();
     hb.release();
-    sb.release();
+    ob.release();
+    eb.release();
     return rc;
+}
+}  // namespace
+
+int nnm_entry_forward(nnm_ctx* ctx, const nnm_entry_mlp* model, const float* x, uint64_t n, uint32_t d,
+                      float* scores) {
+    if (!ctx || !x || !scores || n == 0 || n >= (1ull << 30)) return NNM_ERR_INVALID;
+    if (!entry_ok(ctx, model, d)) return NNM_ERR_INVALID;
+    return entry_infer_host(ctx, model, x, n, d, scores, 0, nullptr);
+}
+
+int nnm_entry_probes(nnm_ctx* ctx, const nnm_entry_mlp* model, const float* x, uint64_t n, uint32_t d,
+                     uint32_t probes, uint32_t* out) {
+    if (!ctx || !x || !out || n == 0 || n >= (1ull << 30)) return NNM_ERR_INVALID;
+    if (!entry_ok(ctx, model, d)) return NNM_ERR_INVALID;
+    if (probes == 0 || probes > (uint32_t)nnm::ENTRY_MAX_PROBES || probes > model->n_classes)
+        return fail(ctx, NNM_ERR_INVALID, "probes must be in [1, min(8, n_classes)]");
+    return entry_infer_host(ctx, model, x, n, d, nullptr, probes, out);
 }
 
 int nnm_entry_grad(nnm_ctx* ctx, const nnm_entry_mlp* model, const float* x, uint64_t n, uint32_t d,

@@ -25,13 +25,13 @@
 #include "nnm_entry.h"
 #include "nnm_launch.h"
 #include "nnm_learned.h"
+#include "nnm_tc.cuh"
 
 namespace nnm {
 namespace {
 using bf16 = __nv_bfloat16;
 constexpr uint32_t EH = ENTRY_H;
 constexpr uint32_t ERB = 32;          // rows per block
-constexpr uint32_t CHUNK = 16384;     // queries per inference chunk
 constexpr uint64_t STEP_KERNELS = 11; // kernels of one captured training step
 
 struct EView {
@@ -48,10 +48,16 @@ __device__ __forceinline__ float bf(bf16 v) { return __bfloat162float(v); }
 
 size_t hidden_smem(uint32_t d) { return (size_t)ERB * ((d + 3) & ~3u) * 4; }
 
+__device__ __forceinline__ void put(float* p, float v) { *p = v; }
+__device__ __forceinline__ void put(bf16* p, float v) { *p = __float2bfloat16_rn(v); }
+
 // h = relu(W1 u + b1) of ERB rows per block; row r is x row idx[r] (or r).
+// Training keeps h in FP32; inference rounds it to BF16, the tensor-core
+// operand of the score kernel.
+template <typename OutT>
 __global__ void __launch_bounds__(256) k_ent_hidden(EView v, const float* __restrict__ x, uint32_t dp,
                                                     const uint32_t* __restrict__ idx, uint32_t nrows,
-                                                    float* __restrict__ h) {
+                                                    OutT* __restrict__ h) {
     extern __shared__ __align__(16) float us[];
     const uint32_t d = v.d, dpad = (d + 3) & ~3u, tid = threadIdx.x, r0 = blockIdx.x * ERB;
     for (uint32_t i = tid; i < ERB * dpad; i += 256) {
@@ -84,7 +90,7 @@ __global__ void __launch_bounds__(256) k_ent_hidden(EView v, const float* __rest
     }
 #pragma unroll
     for (uint32_t r = 0; r < ERB; r++)
-        if (r0 + r < nrows) h[(size_t)(r0 + r) * EH + j] = fmaxf(acc[r], 0.f);
+        if (r0 + r < nrows) put(h + (size_t)(r0 + r) * EH + j, fmaxf(acc[r], 0.f));
 }
 
 // s = W2 h + b2: block (row tile, 256-class tile), thread = class.
@@ -329,17 +335,97 @@ __global__ void k_ent_sample(uint32_t* idx, uint32_t* lab, uint32_t B, const uin
 
 __global__ void k_ent_step_inc(uint32_t* step) { *step += 1; }
 
-__device__ __forceinline__ bool score_gt(float a, uint32_t ia, float b, uint32_t ib) {
-    return a > b || (a == b && ia < ib);
+// ---- inference on the tensor cores ----
+// Scores of 128 rows per CTA against the C classes in tiles of 128 classes:
+// D (128 x 128, FP32 in TMEM) = A (BF16 h, 128 x 256, K-major, resident in
+// shared memory) x B^T (BF16 W2 rows of the tile, 128 x 256, K-major), one
+// tcgen05.mma chain of 16 instructions (K = 16 each) per tile, issued by one
+// thread and committed to an mbarrier.  Two B buffers and two 128-column
+// accumulators: the MMA of tile j+1 runs while the epilogue reads tile j and
+// tile j+2 loads.  The epilogue (thread = row = TMEM lane) reads 32 scores
+// at a time with tcgen05.ld, adds the biases (all C of them staged in shared
+// memory, padded with -inf), and either writes the scores (MODE 0) or keeps
+// the row's ENTRY_MAX_PROBES largest in registers (MODE 1, ties to the lower
+// class; a chunk whose maximum cannot enter the list is skipped) -- the
+// probes, with no score written to HBM.  Operand layout: no swizzle, 8-row
+// groups of 32 K-chunks of 16 bytes (4096 bytes per group).
+constexpr uint32_t PT = 128;                  // rows (M) and classes (N) per tile
+constexpr uint32_t PROW = EH * 2;             // 512 bytes of K per row
+constexpr uint32_t PGRP = (PROW / 16) * 128;  // 4096 bytes per 8-row group
+constexpr uint32_t PTILE = PT * PROW;         // 64 KB per operand tile
+constexpr size_t PROBE_SMEM = 3 * (size_t)PTILE + (size_t)ENTRY_MAX_C * 4;
+constexpr uint32_t IDESC_E = (1u << 4) | (1u << 7) | (1u << 10) | ((PT >> 3) << 17) | ((PT >> 4) << 24);
+constexpr unsigned EERR_WAIT = 64u;           // an mbarrier wait ran out (search self-check code)
+
+__device__ __forceinline__ void st_shared_zero16(uint32_t addr) {
+    asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(addr), "r"(0u) : "memory");
 }
 
-// Warp per row: the P (<= ENTRY_MAX_PROBES) classes of largest score, ties
-// to the lower class, in descending order.
-__global__ void k_ent_topp(const float* __restrict__ s, uint32_t nrows, uint32_t C, uint32_t P,
-                           uint32_t* __restrict__ probes, uint32_t row0) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (row >= nrows) return;
+// Rows [r0, r0 + 128) of a (rows x 256 BF16, row-major) into the operand
+// layout at dst; rows past `rows` are zero.  Thread t copies chunk t % 32 of
+// rows t / 32 + 4i: 32 consecutive threads read one 512-byte row.
+__device__ __forceinline__ void load_tile(uint32_t dst, const bf16* __restrict__ src, uint32_t r0, uint32_t rows,
+                                          uint32_t tid) {
+    const uint32_t c = tid & 31, rt = tid >> 5;
+    const char* s0 = reinterpret_cast<const char*>(src) + (size_t)r0 * PROW + c * 16;
+#pragma unroll 8
+    for (uint32_t i = 0; i < PT / 4; i++) {
+        const uint32_t r = rt + 4 * i;
+        const uint32_t addr = dst + (r >> 3) * PGRP + c * 128 + (r & 7) * 16;
+        if (r0 + r < rows) cp_async16(addr, s0 + (size_t)r * PROW);
+        else st_shared_zero16(addr);
+    }
+}
+
+__device__ __forceinline__ void mma_tile(uint32_t tmem_acc, uint32_t a_s, uint32_t b_s, uint32_t bar) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll 1
+    for (uint32_t kk = 0; kk < PROW / 32; kk++) {  // 32 bytes of K per instruction
+        const uint64_t da = smem_desc(a_s + kk * 256, 128, PGRP);
+        const uint64_t db = smem_desc(b_s + kk * 256, 128, PGRP);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_acc),
+            "l"(da), "l"(db), "r"(IDESC_E), "r"(kk));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128, 1) k_ent_tc(const bf16* __restrict__ h, uint32_t nrows,
+                                                   const bf16* __restrict__ w2r, const float* __restrict__ b2,
+                                                   uint32_t C, float* __restrict__ scores, uint32_t P,
+                                                   uint32_t* __restrict__ probes, unsigned* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ uint64_t mma_bar[2];
+    __shared__ uint32_t tmem_base;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t a_s = smem_u32(smem), r0 = blockIdx.x * PT;
+    const uint32_t b_s0 = a_s + PTILE;  // B buffer x at b_s0 + x * PTILE
+    float* sbias = reinterpret_cast<float*>(smem + 3 * (size_t)PTILE);
+    const uint32_t nt = (C + PT - 1) / PT, row = r0 + tid;
+    if (tid == 0) {
+        for (int b = 0; b < 2; b++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mma_bar[b])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(2 * PT));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    for (uint32_t c = tid; c < nt * PT; c += 128) sbias[c] = c < C ? b2[c] : -INFINITY;
+    load_tile(a_s, h, r0, nrows, tid);
+    load_tile(b_s0, w2r, 0, C, tid);
+    if (nt > 1) load_tile(b_s0 + PTILE, w2r, PT, C, tid);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // cp.async writes -> tensor core reads
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+    const uint32_t bar0 = smem_u32(&mma_bar[0]);  // barrier x at bar0 + 8x
+    if (tid == 0) mma_tile(tmem, a_s, b_s0, bar0);
     constexpr int Q = ENTRY_MAX_PROBES;
     float lv[Q];
     uint32_t li[Q];
@@ -348,48 +434,88 @@ __global__ void k_ent_topp(const float* __restrict__ s, uint32_t nrows, uint32_t
         lv[q] = -INFINITY;
         li[q] = 0xffffffffu;
     }
-    const float* sr = s + (size_t)row * C;
-    for (uint32_t c = lane; c < C; c += 32) {
-        const float v = sr[c];
-        if (score_gt(v, c, lv[Q - 1], li[Q - 1])) {
-            lv[Q - 1] = v;
-            li[Q - 1] = c;
+    uint32_t phase = 0u, pending = 1u;  // bit x: accumulator x's next phase / MMA in flight
+    bool failed = false;
+    for (uint32_t j = 0; j < nt; j++) {
+        const uint32_t b = j & 1;
+        // MMA j+1: its B buffer was loaded before the last barrier, and its
+        // accumulator was last read by epilogue j-1, before that barrier
+        if (j + 1 < nt) {
+            if (tid == 0) mma_tile(tmem + (b ^ 1) * PT, a_s, b_s0 + (b ^ 1) * PTILE, bar0 + 8 * (b ^ 1));
+            pending |= 1u << (b ^ 1);
+        }
+        const bool ok = mbar_wait_bounded(bar0 + 8 * b, (phase >> b) & 1u);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        pending &= ~(1u << b);
+        phase ^= 1u << b;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (j + 2 < nt) load_tile(b_s0 + b * PTILE, w2r, (j + 2) * PT, C, tid);  // MMA j, its last reader, is complete
+        const uint32_t c0 = j * PT;
+#pragma unroll 1
+        for (uint32_t cc = 0; cc < PT; cc += 32) {
+            uint32_t v[32];
+            tmem_ld32(tmem + ((warp * 32u) << 16) + b * PT + cc, v);
+            float sc[32];
 #pragma unroll
-            for (int q = Q - 1; q > 0; q--)
-                if (score_gt(lv[q], li[q], lv[q - 1], li[q - 1])) {
-                    const float tv = lv[q];
-                    lv[q] = lv[q - 1];
-                    lv[q - 1] = tv;
-                    const uint32_t ti = li[q];
-                    li[q] = li[q - 1];
-                    li[q - 1] = ti;
+            for (int i = 0; i < 32; i += 4) {
+                const float4 bv = *reinterpret_cast<const float4*>(sbias + c0 + cc + i);
+                sc[i] = __uint_as_float(v[i]) + bv.x;
+                sc[i + 1] = __uint_as_float(v[i + 1]) + bv.y;
+                sc[i + 2] = __uint_as_float(v[i + 2]) + bv.z;
+                sc[i + 3] = __uint_as_float(v[i + 3]) + bv.w;
+            }
+            if (MODE == 0) {
+                if (row < nrows)
+#pragma unroll
+                    for (int i = 0; i < 32; i++)
+                        if (c0 + cc + i < C) scores[(size_t)row * C + c0 + cc + i] = sc[i];
+            } else {
+                float mx = sc[0];
+#pragma unroll
+                for (int i = 1; i < 32; i++) mx = fmaxf(mx, sc[i]);
+                if (mx > lv[Q - 1]) {
+#pragma unroll
+                    for (int i = 0; i < 32; i++) {
+                        if (sc[i] > lv[Q - 1]) {
+                            lv[Q - 1] = sc[i];
+                            li[Q - 1] = c0 + cc + i;
+#pragma unroll
+                            for (int q = Q - 1; q > 0; q--)
+                                if (lv[q] > lv[q - 1]) {
+                                    const float tv = lv[q];
+                                    lv[q] = lv[q - 1];
+                                    lv[q - 1] = tv;
+                                    const uint32_t ti = li[q];
+                                    li[q] = li[q - 1];
+                                    li[q - 1] = ti;
+                                }
+                        }
+                    }
                 }
+            }
         }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
     }
-    for (uint32_t t = 0; t < P; t++) {
-        float bv = lv[0];
-        uint32_t bi = li[0], bl = lane;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            const uint32_t oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            const uint32_t ol = __shfl_xor_sync(0xffffffffu, bl, o);
-            if (score_gt(ov, oi, bv, bi) || (ov == bv && oi == bi && ol < bl)) {
-                bv = ov;
-                bi = oi;
-                bl = ol;
-            }
-        }
-        if (lane == 0) probes[(size_t)(row0 + row) * P + t] = bi < C ? bi : 0u;
-        if (lane == bl) {
-#pragma unroll
-            for (int q = 0; q < Q - 1; q++) {
-                lv[q] = lv[q + 1];
-                li[q] = li[q + 1];
-            }
-            lv[Q - 1] = -INFINITY;
-            li[Q - 1] = 0xffffffffu;
-        }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (failed) {
+        if (tid == 0) atomicOr(err, EERR_WAIT);
+        for (uint32_t b = 0; b < 2; b++)
+            if ((pending >> b) & 1u) mbar_wait_bounded(bar0 + 8 * b, (phase >> b) & 1u);  // an MMA may still write TMEM
+    } else if (MODE == 1 && row < nrows) {
+        for (uint32_t t = 0; t < P; t++) probes[(size_t)row * P + t] = li[t] < C ? li[t] : 0u;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * PT));
     }
 }
 
@@ -422,7 +548,13 @@ EView view_of(const DevEntry& m) {
 }
 
 cudaError_t set_attrs(uint32_t d) {
-    cudaError_t e = cudaFuncSetAttribute(k_ent_hidden, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hidden_smem(d));
+    const int hs = (int)hidden_smem(d);
+    cudaError_t e = cudaFuncSetAttribute(k_ent_hidden<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, hs);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ent_hidden<bf16>, cudaFuncAttributeMaxDynamicSharedMemorySize, hs);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_ent_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PROBE_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_ent_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PROBE_SMEM);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_ent_labels, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)((LR + LC) * (d + 1) * 4));
@@ -479,7 +611,7 @@ EView pass_view(const EPass& p, const ELayout& L, const DevEntry& m) {
 
 void enqueue_pass(const EView& v, const float* x, uint32_t dp, uint32_t B, EPass& p, const ELayout& L,
                   const uint32_t* step, cudaStream_t st) {
-    k_ent_hidden<<<(B + ERB - 1) / ERB, 256, hidden_smem(v.d), st>>>(v, x, dp, p.idx.as<uint32_t>(), B,
+    k_ent_hidden<float><<<(B + ERB - 1) / ERB, 256, hidden_smem(v.d), st>>>(v, x, dp, p.idx.as<uint32_t>(), B,
                                                                     p.h.as<float>());
     k_ent_scores<<<dim3((B + ERB - 1) / ERB, (v.C + 255) / 256), 256, 0, st>>>(v, p.h.as<float>(), B, p.s.as<float>());
     const uint32_t nblk = (B + 7) / 8;
@@ -520,30 +652,28 @@ int entry_upload(Ctx& ctx, DevEntry& m, const nnm_entry_mlp& h) {
     return 0;
 }
 
-int entry_scores_dev(Ctx& ctx, const DevEntry& m, const float* x, uint32_t n, uint32_t dp, float* h, float* s) {
+int entry_infer(Ctx& ctx, const DevEntry& m, const float* x, uint32_t n, uint32_t dp, void* hbuf, float* scores,
+                uint32_t P, uint32_t* probes, unsigned* err) {
     NNM_CUDA_TRY(set_attrs(m.d));
     if (!n) return 0;
-    const EView v = view_of(m);
-    k_ent_hidden<<<(n + ERB - 1) / ERB, 256, hidden_smem(m.d), ctx.stream>>>(v, x, dp, nullptr, n, h); count_launch();
-    k_ent_scores<<<dim3((n + ERB - 1) / ERB, (m.C + 255) / 256), 256, 0, ctx.stream>>>(v, h, n, s); count_launch();
+    bf16* hb = static_cast<bf16*>(hbuf);
+    k_ent_hidden<bf16><<<(n + ERB - 1) / ERB, 256, hidden_smem(m.d), ctx.stream>>>(view_of(m), x, dp, nullptr, n,
+                                                                                  hb);
+    const uint32_t grid = (n + PT - 1) / PT;
+    if (scores)
+        k_ent_tc<0><<<grid, 128, PROBE_SMEM, ctx.stream>>>(hb, n, m.w2r.as<bf16>(), m.b2.as<float>(), m.C, scores, 0,
+                                                          nullptr, err);
+    else
+        k_ent_tc<1><<<grid, 128, PROBE_SMEM, ctx.stream>>>(hb, n, m.w2r.as<bf16>(), m.b2.as<float>(), m.C, nullptr, P,
+                                                          probes, err);
+    count_launch(2);
     NNM_CUDA_TRY(cudaGetLastError());
     return 0;
 }
 
-int entry_predict(Ctx& ctx, IndexDev& ix, const float* q, uint32_t nq, uint32_t* probes) {
-    const DevEntry& m = *ix.net;
-    const uint32_t C = m.C, chunk = std::min(nq, CHUNK);
-    NNM_CUDA_TRY(ix.hid.ensure((size_t)chunk * EH * 4));
-    NNM_CUDA_TRY(ix.scores.ensure((size_t)chunk * C * 4));
-    for (uint32_t q0 = 0; q0 < nq; q0 += CHUNK) {
-        const uint32_t cn = std::min(CHUNK, nq - q0);
-        int rc = entry_scores_dev(ctx, m, q + (size_t)q0 * ix.dp, cn, ix.dp, ix.hid.as<float>(), ix.scores.as<float>());
-        if (rc) return rc;
-        k_ent_topp<<<(cn + 7) / 8, 256, 0, ctx.stream>>>(ix.scores.as<float>(), cn, C, ix.nprobe, probes, q0);
-        count_launch();
-    }
-    NNM_CUDA_TRY(cudaGetLastError());
-    return 0;
+int entry_predict(Ctx& ctx, IndexDev& ix, const float* q, uint32_t nq, uint32_t* probes, unsigned* err) {
+    NNM_CUDA_TRY(ix.hid.ensure((size_t)nq * EH * 2));
+    return entry_infer(ctx, *ix.net, q, nq, ix.dp, ix.hid.p, nullptr, ix.nprobe, probes, err);
 }
 
 int entry_grad(Ctx& ctx, const nnm_entry_mlp& model, const float* x_dev, uint32_t n, uint32_t dp,

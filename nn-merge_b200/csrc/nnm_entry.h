@@ -26,10 +26,14 @@ struct DevEntry {
 };
 
 int entry_upload(Ctx& ctx, DevEntry& m, const nnm_entry_mlp& h);
-// Hidden activations (n x 256) and scores (n x C) of rows [0, n) of x (stride dp).
-int entry_scores_dev(Ctx& ctx, const DevEntry& m, const float* x, uint32_t n, uint32_t dp, float* h, float* s);
-// Probes (nq x ix.nprobe rows of the entry layer) of queries q (stride ix.dp), with ix.net.
-int entry_predict(Ctx& ctx, IndexDev& ix, const float* q, uint32_t nq, uint32_t* probes);
+// Inference of rows [0, n) of x (stride dp): BF16 hidden rows into hbuf
+// (n x 256 x 2 bytes), then either the scores (n x C, when scores is
+// non-null) or the P probes of every row (n x P) from the tensor-core
+// kernel.  A wait of that kernel that runs out sets 64 in *err.
+int entry_infer(Ctx& ctx, const DevEntry& m, const float* x, uint32_t n, uint32_t dp, void* hbuf, float* scores,
+                uint32_t P, uint32_t* probes, unsigned* err);
+// Probes (nq x ix.nprobe rows) of queries q (stride ix.dp), with ix.net.
+int entry_predict(Ctx& ctx, IndexDev& ix, const float* q, uint32_t nq, uint32_t* probes, unsigned* err);
 int entry_grad(Ctx& ctx, const nnm_entry_mlp& model, const float* x_dev, uint32_t n, uint32_t dp,
                const uint32_t* lab_host, float* loss, nnm_entry_mlp& grad);
 int entry_train(Ctx& ctx, IndexDev& ix, uint32_t layer, const nnm_train_opts& o, nnm_entry_mlp& model,

@@ -45,6 +45,7 @@ struct IndexDev {
     DevBuf qpad, beams, probes, hid, scores, out;  // per-call staging
     DevEntry* net = nullptr;                   // entry network, owned
     uint32_t nprobe = 0, entry_layer = 0, n_classes = 0;
+    uint32_t width = 4;  // fast kernel: most unexpanded entries expanded together
     void release();
 };
 
@@ -62,6 +63,8 @@ struct SearchReq {
 
 int index_upload(Ctx& ctx, IndexDev& ix, const float* x, uint64_t n, uint32_t d, const nnm_layers* layers,
                  uint32_t seed, uint32_t metric);
+// The caller zeroes ix.ctr (64 bytes: query counter, self-check flags,
+// distance and expansion counts) before a run.
 int index_run_exact(Ctx& ctx, IndexDev& ix, const SearchReq& r);
 int index_run_fast(Ctx& ctx, IndexDev& ix, const SearchReq& r);
 // Waits for the stream, reads the distance and expansion counts of the last

@@ -425,7 +425,6 @@ int index_run_exact(Ctx& ctx, IndexDev& ix, const SearchReq& r) {
     }
     NNM_CUDA_TRY(ix.vlist.ensure(slots * VCAP * 4));
     NNM_CUDA_TRY(ix.cand.ensure(slots * CCAP * sizeof(HP)));
-    NNM_CUDA_TRY(cudaMemsetAsync(ix.ctr.p, 0, 64, st));
     SearchArgs a{};
     a.x = ix.x.as<float>();
     a.dp = dp;
@@ -529,6 +528,7 @@ int search_host(Ctx& ctx, const float* x, uint64_t n, uint32_t d, const nnm_laye
     r.out_k = topk;
     r.out_ids = ib.as<uint32_t>();
     r.out_d = db.as<float>();
+    TRY_OR_FREE(cudaMemsetAsync(ix.ctr.p, 0, 64, st));
     if ((rc = index_run_exact(ctx, ix, r))) return fail(rc);
     TRY_OR_FREE(cudaMemcpyAsync(out_ids, ib.p, (size_t)nq * topk * 4, cudaMemcpyDeviceToHost, st));
     if (out_dists) TRY_OR_FREE(cudaMemcpyAsync(out_dists, db.p, (size_t)nq * topk * 4, cudaMemcpyDeviceToHost, st));

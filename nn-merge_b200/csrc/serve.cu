@@ -20,7 +20,12 @@
 //     `beam` entries in shared memory, sorted by (distance, id), with an
 //     "expanded" bit per entry: expand the first unexpanded entry, merge the
 //     accepted neighbours (distance below the worst entry, or the beam not
-//     full) into place, stop when every entry is expanded.
+//     full) into place (only the entries after the first new one move),
+//     stop when every entry is expanded.
+//   - width: a step expands the first min(width, beam / 64) unexpanded
+//     entries together, reading their lists as one sequence of 32-id chunks,
+//     so that the dependent loads (offsets, lists, visited bits, rows) of
+//     several nodes are in flight at once; width 1 is strict best-first.
 //   - visited set: one bitmap per warp slot in HBM, cleared after each query
 //     from the list of ids it set.
 #include <algorithm>
@@ -61,6 +66,7 @@ struct ServeArgs {
     uint32_t* visited;
     uint32_t words;
     uint32_t* vlist;
+    uint32_t width;  // most unexpanded entries expanded together (1..4)
     unsigned* next_q;
     unsigned* overflow;
     unsigned long long* ncmps;
@@ -89,6 +95,35 @@ template <int M, int QV>
 __device__ __forceinline__ float warp_dists(const float4 (&qr)[QV], const float4* __restrict__ x4, uint32_t dp4,
                                             uint32_t fid, uint32_t nf, uint32_t lane) {
     constexpr int NB = QV == 1 ? 8 : (QV == 2 ? 4 : 2);  // rows in flight per lane
+    if (nf <= (uint32_t)NB) {
+        // few rows: one xor-shuffle reduction per row.  Its sum tree pairs
+        // lanes l and l^s at width s = 16, 8, .., 1 exactly as the
+        // transposing butterfly below does, so the sums are the same bits.
+        float4 r[NB][QV];
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            const uint32_t id = __shfl_sync(FULL, fid, b);
+#pragma unroll
+            for (int t = 0; t < QV; t++) {
+                const uint32_t c4 = lane + 32u * t;
+                r[b][t] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if ((uint32_t)b < nf && c4 < dp4) r[b][t] = __ldg(x4 + (size_t)id * dp4 + c4);
+            }
+        }
+        float out = 0.f;
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            if ((uint32_t)b < nf) {
+                float sum = 0.f;
+#pragma unroll
+                for (int t = 0; t < QV; t++) sum = part4<M>(qr[t], r[b][t], sum);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL, sum, o);
+                if (lane == (uint32_t)b) out = sum;
+            }
+        }
+        return out;
+    }
     float v[32];
 #pragma unroll
     for (int j = 0; j < 32; j++) v[j] = 0.f;
@@ -148,15 +183,17 @@ __device__ __forceinline__ void warp_argmin(float d, uint32_t valid, uint32_t la
     ml = l;
 }
 
-// Bitonic sort of one (d, id) pair per lane, ascending by (d, id).
-__device__ __forceinline__ void warp_sort(float& d, uint32_t& id, uint32_t lane) {
+// Bitonic sort of one (d, id) pair per lane over lanes [0, w), w a power of
+// two (warp-uniform); ascending by (d, id).  Lanes >= w are left as they are.
+__device__ __forceinline__ void warp_sort(float& d, uint32_t& id, uint32_t lane, uint32_t w) {
 #pragma unroll
-    for (int k = 2; k <= 32; k <<= 1) {
+    for (uint32_t k = 2; k <= 32; k <<= 1) {
+        if (k > w) break;
 #pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
             const float od = __shfl_xor_sync(FULL, d, j);
             const uint32_t oi = __shfl_xor_sync(FULL, id, j);
-            const bool asc = (lane & k) == 0 || k == 32;
+            const bool asc = (lane & k) == 0 || k == w;
             const bool low = (lane & j) == 0;
             const bool other_less = key_less(od, oi, d, id);
             const bool other_more = key_less(d, id, od, oi);
@@ -195,6 +232,8 @@ __global__ void __launch_bounds__(FW * 32) k_serve(ServeArgs a) {
             if (lane == 0) atomicOr(a.overflow, FERR_BEAM_RANGE);
             ef = min(max(ef, a.out_k), a.cap);
         }
+        // expansions per step: wide beams take up to a.width, narrow ones 1
+        const uint32_t width = max(1u, min(a.width, ef / 64));
         float4 qr[QV];
 #pragma unroll
         for (int t = 0; t < QV; t++) {
@@ -277,33 +316,57 @@ __global__ void __launch_bounds__(FW * 32) k_serve(ServeArgs a) {
         __syncwarp();
         uint32_t expansions = 0;
         for (;;) {
-            __syncwarp();  // lane 0's expanded mark and the last merge are visible
-            uint32_t pos = m;
-            for (uint32_t s0 = p; s0 < m; s0 += 32) {
-                const bool un = s0 + lane < m && !(bi[s0 + lane] & EXP_BIT);
-                const unsigned bal = __ballot_sync(FULL, un);
-                if (bal) {
-                    pos = s0 + __ffs(bal) - 1;
-                    break;
+            __syncwarp();  // the expanded marks and the last merge are visible
+            // the first `width` unexpanded entries; lane e keeps the e-th one
+            uint32_t ne = 0, mine = 0, mypos = 0, last = 0;
+            for (uint32_t s0 = p; s0 < m && ne < width; s0 += 32) {
+                unsigned bal = __ballot_sync(FULL, s0 + lane < m && !(bi[s0 + lane] & EXP_BIT));
+                while (bal && ne < width) {
+                    last = s0 + __ffs(bal) - 1;
+                    bal &= bal - 1;
+                    if (lane == ne) {
+                        mine = bi[last] & IDM;
+                        mypos = last;
+                    }
+                    ne++;
                 }
             }
-            if (pos >= m) break;
-            if (++expansions > nlast) {
+            if (ne == 0) break;
+            expansions += ne;
+            if (expansions > nlast) {
                 if (lane == 0) atomicOr(a.overflow, FERR_LOOP);
                 break;
             }
-            p = pos + 1;
-            const uint32_t c = bi[pos] & IDM;
+            p = last + 1;
             __syncwarp();
-            if (lane == 0) bi[pos] = c | EXP_BIT;
-            nexp++;
-            const uint64_t b = off[c], e = off[c + 1];
-            for (uint64_t c0 = b; c0 < e; c0 += 32) {
-                const uint32_t cnt = (uint32_t)(e - c0 < 32 ? e - c0 : 32);
+            if (lane < ne) bi[mypos] = mine | EXP_BIT;
+            nexp += ne;
+            // the selected nodes' lists, read as one sequence of `total` ids:
+            // entry t belongs to list e when end_{e-1} <= t < end_e
+            uint64_t lb = 0, le = 0;
+            if (lane < ne) {
+                lb = off[mine];
+                le = off[mine + 1];
+            }
+            const uint32_t len = (uint32_t)(le - lb);
+            uint32_t pre = len;
+#pragma unroll
+            for (int o = 1; o < 4; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, pre, o);
+                if (lane >= (uint32_t)o) pre += v;
+            }
+            const uint32_t end0 = __shfl_sync(FULL, pre, 0), end1 = __shfl_sync(FULL, pre, 1),
+                           end2 = __shfl_sync(FULL, pre, 2), total = __shfl_sync(FULL, pre, 3);
+            const uint64_t base_l = lb - (pre - len);  // list e: adjacency index base_e + t
+            const uint64_t base0 = __shfl_sync(FULL, base_l, 0), base1 = __shfl_sync(FULL, base_l, 1),
+                           base2 = __shfl_sync(FULL, base_l, 2), base3 = __shfl_sync(FULL, base_l, 3);
+            for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+                const uint32_t t = t0 + lane;
                 bool fresh = false;
                 uint32_t nn = 0;
-                if (lane < cnt) {
-                    nn = a.adj_all[c0 + lane];
+                if (t < total) {
+                    const uint64_t bs = t < end0 ? base0 : (t < end1 ? base1 : (t < end2 ? base2 : base3));
+                    nn = a.adj_all[bs + t];
                     const uint32_t old = atomicOr(&vis[nn >> 5], 1u << (nn & 31));
                     fresh = !(old & (1u << (nn & 31)));
                 }
@@ -328,27 +391,18 @@ __global__ void __launch_bounds__(FW * 32) k_serve(ServeArgs a) {
                 if (nk == 0) continue;
                 float kd = acc ? dd : INFINITY;
                 uint32_t kid = acc ? fid : 0xffffffffu;
-                warp_sort(kd, kid, lane);
+                // the accepted entries are among lanes [0, nf): sort that many
+                uint32_t w = 1;
+                while (w < nf) w <<= 1;
+                warp_sort(kd, kid, lane, w);
                 __syncwarp();
                 nd[lane] = kd;
                 ni[lane] = kid;
-                __syncwarp();
+                // merge in place: entries before the first new one keep their
+                // slots; the suffix [lo0, m) is staged, then every entry of the
+                // merged range [lo0, m2) is written once
                 const uint32_t m2 = min(ef, m + nk);
-                for (uint32_t i = lane; i < m; i += 32) {
-                    const float d0 = bd[i];
-                    const uint32_t i0 = bi[i];
-                    uint32_t lo = 0, hi = nk;
-                    while (lo < hi) {
-                        const uint32_t md = (lo + hi) >> 1;
-                        if (key_less(nd[md], ni[md], d0, i0 & IDM)) lo = md + 1;
-                        else hi = md;
-                    }
-                    if (i + lo < m2) {
-                        td[i + lo] = d0;
-                        ti[i + lo] = i0;
-                    }
-                }
-                uint32_t first = m2;
+                uint32_t npos = 0;
                 if (lane < nk) {
                     uint32_t lo = 0, hi = m;
                     while (lo < hi) {
@@ -356,22 +410,35 @@ __global__ void __launch_bounds__(FW * 32) k_serve(ServeArgs a) {
                         if (key_less(bd[md], bi[md] & IDM, kd, kid)) lo = md + 1;
                         else hi = md;
                     }
-                    if (lane + lo < m2) {
-                        td[lane + lo] = kd;
-                        ti[lane + lo] = kid;
-                    }
-                    first = lane + lo;
+                    npos = lane + lo;
                 }
-                first = __shfl_sync(FULL, first, 0);
+                const uint32_t lo0 = __shfl_sync(FULL, npos, 0);
+                for (uint32_t i = lo0 + lane; i < m; i += 32) {
+                    td[i - lo0] = bd[i];
+                    ti[i - lo0] = bi[i];
+                }
                 __syncwarp();
-                float* sd = bd;
-                bd = td;
-                td = sd;
-                uint32_t* si = bi;
-                bi = ti;
-                ti = si;
+                for (uint32_t i = lo0 + lane; i < m; i += 32) {
+                    const float d0 = td[i - lo0];
+                    const uint32_t i0 = ti[i - lo0];
+                    uint32_t lo = 0, hi = nk;
+                    while (lo < hi) {
+                        const uint32_t md = (lo + hi) >> 1;
+                        if (key_less(nd[md], ni[md], d0, i0 & IDM)) lo = md + 1;
+                        else hi = md;
+                    }
+                    if (i + lo < m2) {
+                        bd[i + lo] = d0;
+                        bi[i + lo] = i0;
+                    }
+                }
+                if (lane < nk && npos < m2) {
+                    bd[npos] = kd;
+                    bi[npos] = kid;
+                }
+                __syncwarp();
                 m = m2;
-                if (first < p) p = first;
+                if (lo0 < p) p = lo0;
             }
         }
         // results: the first out_k entries
@@ -427,7 +494,6 @@ int index_run_fast(Ctx& ctx, IndexDev& ix, const SearchReq& r) {
         NNM_CUDA_TRY(cudaMemsetAsync(ix.visited.p, 0, slots * words * 4, st));
     }
     NNM_CUDA_TRY(ix.vlist.ensure(slots * FVCAP * 4));
-    NNM_CUDA_TRY(cudaMemsetAsync(ix.ctr.p, 0, 64, st));
     ServeArgs a{};
     a.x = ix.x.as<float>();
     a.dp4 = dp4;
@@ -453,6 +519,7 @@ int index_run_fast(Ctx& ctx, IndexDev& ix, const SearchReq& r) {
     a.visited = ix.visited.as<uint32_t>();
     a.words = words;
     a.vlist = ix.vlist.as<uint32_t>();
+    a.width = ix.width;
     unsigned char* c = ix.ctr.as<unsigned char>();
     a.next_q = reinterpret_cast<unsigned*>(c);
     a.overflow = reinterpret_cast<unsigned*>(c + 4);

@@ -141,7 +141,9 @@ def load():
         for name in ("nnm_index_search", "nnm_index_search_dev"):
             getattr(lib, name).argtypes = [vp, vp, u64, vp, u32, u32, u32, u32, vp, vp, vp]
         lib.nnm_index_entry_layer.argtypes = [vp, vp, vp]
+        lib.nnm_index_set_width.argtypes = [vp, u32]
         lib.nnm_entry_forward.argtypes = [vp, vp, vp, u64, u32, vp]
+        lib.nnm_entry_probes.argtypes = [vp, vp, vp, u64, u32, u32, vp]
         lib.nnm_entry_grad.argtypes = [vp, vp, vp, u64, u32, vp, vp, vp]
         lib.nnm_entry_train.argtypes = [vp, vp, vp, vp]
         lib.nnm_index_set_entry_model.argtypes = [vp, vp, u32]
@@ -361,6 +363,15 @@ class Context:
         self._check(self.lib.nnm_entry_forward(self.h, ctypes.byref(ms), _ptr(x), n, d, _ptr(s)))
         return s
 
+    def entry_probes(self, model, x, probes=4):
+        """The probes a learned search takes for the rows of x (n x probes)."""
+        x = np.ascontiguousarray(x, np.float32)
+        n, d = x.shape
+        ms = _entry_struct(model)
+        out = np.empty((n, probes), np.uint32)
+        self._check(self.lib.nnm_entry_probes(self.h, ctypes.byref(ms), _ptr(x), n, d, probes, _ptr(out)))
+        return out
+
     def entry_grad(self, model, x, labels):
         x = np.ascontiguousarray(x, np.float32)
         lab = np.ascontiguousarray(labels, np.uint32)
@@ -442,6 +453,9 @@ class Index:
                                                           ctypes.c_void_p(out_d_ptr), ctypes.byref(st)))
         return dict(ncmps=int(st.ncmps), expansions=int(st.expansions), device_ms=float(st.device_ms),
                     predict_ms=float(st.predict_ms))
+
+    def set_width(self, width):
+        self.ctx._check(self.ctx.lib.nnm_index_set_width(self.h, width))
 
     def entry_layer(self):
         layer, nc = ctypes.c_uint32(), ctypes.c_uint32()

@@ -8,6 +8,7 @@ documents it (include/nnm.h, "Entry-point network"):
 
     u = x * in_scale + in_shift
     h = relu(W1 u + b1),  s = W2 h + b2          (d -> 256 -> C)
+    inference rounds h to BF16 (the tensor-core operand) before W2
     loss = mean_b [ log sum_c exp(s_bc) - s_b,label_b ]
     label of a row = its nearest class row (rows 0..C-1), squared L2,
                      ties to the lower class
@@ -38,7 +39,16 @@ def forward(model, x, rounded=True):
 
 
 def scores(model, x):
+    """Scores with h in full precision (the training forward)."""
     return forward(model, x)[3]
+
+
+def infer_scores(model, x):
+    """Scores as inference computes them: h rounded to BF16 (after rounding
+    to float32, where the device accumulates it), s = W2 h + b2."""
+    _, _, w2, b2 = _weights(model)
+    h = bf16_round(forward(model, x)[2].astype(np.float32)).astype(np.float64)
+    return h @ w2.T + b2
 
 
 def loss_and_grad(model, x, labels, rounded=True):
