@@ -301,6 +301,22 @@ __device__ __forceinline__ uint32_t leaf_of_row(uint32_t id, const uint32_t* off
     return lo;
 }
 
+// (view, other-leaf index) of candidate pair q of a row.  When every
+// (view, other leaf) pair fits, all are taken; otherwise the row takes
+// npair / nview leaves spaced evenly over the other leaves, rotated by a
+// per-row draw, in each of nview views.
+__device__ __forceinline__ void cross_pair(uint32_t q, uint32_t nl1, uint32_t nview, uint32_t npair, uint32_t rot,
+                                           uint32_t& v, uint32_t& lo) {
+    if (nview * nl1 <= npair) {
+        v = q / nl1;
+        lo = q - v * nl1;
+    } else {
+        const uint32_t nj = npair / nview, j = q / nview;
+        v = q - j * nview;
+        lo = (uint32_t)(((unsigned long long)j * nl1 / nj + rot) % nl1);
+    }
+}
+
 __global__ void __launch_bounds__(IW * 32) k_learned_cross(CrossArgsL a) {
     __shared__ SortEnt ents[IW][NCAND + 32];
     __shared__ uint32_t cid[IW][NCAND];
@@ -320,9 +336,12 @@ __global__ void __launch_bounds__(IW * 32) k_learned_cross(CrossArgsL a) {
         a.cpdist[(size_t)row * K + lane] = e[keep + lane].dist;
     }
     __syncwarp();
-    // lane q < npair: lower bound of this row's key in (view q / nl1, other leaf q % nl1)
+    const uint32_t rot = bounded(Philox{a.seed, 0x6e6e6d05u}(row, a.phase, 0, 0).x, nl1);
+    // lane q < npair: lower bound of this row's key in its pair q
     if (lane < (int)npair) {
-        const uint32_t v = lane / nl1, lo = lane - v * nl1, l2 = lo < leaf ? lo : lo + 1;
+        uint32_t v, lo;
+        cross_pair(lane, nl1, a.nview, npair, rot, v, lo);
+        const uint32_t l2 = lo < leaf ? lo : lo + 1;
         const unsigned long long key = (unsigned long long)rotl(a.codes[row], 8 * v) << 32;
         const unsigned long long* seg = a.keys + (size_t)(v * a.nleaf + l2) * a.P;
         uint32_t b = 0, t = a.leaf_off[l2 + 1] - a.leaf_off[l2];
@@ -340,7 +359,9 @@ __global__ void __launch_bounds__(IW * 32) k_learned_cross(CrossArgsL a) {
         const uint32_t s = lane + 32 * h, per = 2 * a.win;
         if (s < npair * per) {
             const uint32_t q = s / per, off = s - q * per;
-            const uint32_t v = q / nl1, lo = q - v * nl1, l2 = lo < leaf ? lo : lo + 1;
+            uint32_t v, lo;
+            cross_pair(q, nl1, a.nview, npair, rot, v, lo);
+            const uint32_t l2 = lo < leaf ? lo : lo + 1;
             const uint32_t L = a.leaf_off[l2 + 1] - a.leaf_off[l2];
             const int64_t pp = (int64_t)cpos[w][q] + (int64_t)off - (int64_t)a.win;
             if (pp >= 0 && pp < (int64_t)L)
@@ -428,8 +449,9 @@ int learned_cross(Ctx& ctx, GraphDev& g, const CodeViews& vw, const uint32_t* d_
     NNM_CUDA_TRY(cudaMemsetAsync(ctx.ws.counters.p, 0, sizeof(IterCounters), ctx.stream));
     const uint32_t nl1 = vw.nleaf - 1;
     // (view, other leaf) pairs: all views of every other leaf while that is
-    // at most 32 pairs, else fewer views (view 0 of the first 32 leaves at
-    // the least); the 64 candidate slots are shared out evenly
+    // at most 32 pairs, else fewer views, and with more than 32 other leaves
+    // view 0 of 32 leaves spread over them (per row); the 64 candidate
+    // slots are shared out evenly
     const uint32_t nview = std::max<uint32_t>(1, std::min<uint32_t>(vw.V, 32 / nl1));
     const uint32_t npair = std::min<uint32_t>(nview * nl1, 32);
     const uint32_t win = std::max<uint32_t>(1, NCAND / (2 * npair));

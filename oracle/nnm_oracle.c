@@ -897,21 +897,30 @@ static void pq_pop(pq_t *q) {
 int nno_search(const float *x, uint32_t n, uint32_t d, const nno_layers *layers,
                const float *q, uint32_t nq, uint32_t topk, int metric, uint32_t seed,
                uint32_t *out_ids, float *out_dists, uint64_t *ncmps, uint32_t *entry) {
-    return nno_search_ex(x, n, d, layers, q, nq, NULL, topk, topk, NULL, 0, 0, metric, seed, out_ids, out_dists,
+    return nno_search_ex(x, n, d, layers, q, nq, NULL, topk, topk, NULL, 0, 0, 0, metric, seed, out_ids, out_dists,
                          ncmps, entry);
 }
 
 /* The serving form: query i searches with beam width beams[i] (or `beam`)
  * and keeps its first out_k results; with probes (nq x nprobe rows of layer
  * g0) a query starts at the first nearest of its probes, in probe order,
- * and descends from layer g0 instead of from the global entry on layer 0. */
+ * and descends from layer g0 instead of from the global entry on layer 0.
+ * flat: nndFlatSrch (lysearch.cpp:439-520) -- no descent; the beam starts
+ * with getRndSds(mt19937(seed), beam, rows of the last layer) pushed in
+ * draw order (the reference seeds a new generator from its clock per query,
+ * lysearch.cpp:455, so with the clock frozen every query draws the same). */
 int nno_search_ex(const float *x, uint32_t n, uint32_t d, const nno_layers *layers,
                   const float *q, uint32_t nq, const uint32_t *beams, uint32_t beam, uint32_t out_k,
-                  const uint32_t *probes, uint32_t nprobe, uint32_t g0, int metric, uint32_t seed,
+                  const uint32_t *probes, uint32_t nprobe, uint32_t g0, int flat, int metric, uint32_t seed,
                   uint32_t *out_ids, float *out_dists, uint64_t *ncmps, uint32_t *entry) {
     if (!layers || layers->nlayers < 1 || beam == 0 || out_k == 0) return -1;
     const uint32_t L = layers->nlayers;
     if (probes && (nprobe == 0 || g0 >= L)) return -1;
+    const uint32_t nlast = layers->nrows[L - 1];
+    if (flat)
+        for (uint32_t qi = 0; qi < nq; qi++)
+            if ((beams ? beams[qi] : beam) > nlast) return -1;
+    uint32_t *sds = flat ? malloc(sizeof(uint32_t) * (nlast + 1)) : NULL;
     grand_t rnd;
     grand_seed(&rnd, seed);
     uint32_t enter = (uint32_t)grand_next(&rnd) % layers->nrows[0];  /* lysearch.cpp:382 */
@@ -924,8 +933,12 @@ int nno_search_ex(const float *x, uint32_t n, uint32_t d, const nno_layers *laye
         const float *qv = q + (size_t)qi * d;
         const uint32_t topk = beams ? beams[qi] : beam;
         uint32_t cur = enter, gstart = 0;
-        float cur_d;
-        if (probes) {
+        float cur_d = 0.f;
+        if (flat) {
+            mt_t rng;
+            mt_seed(&rng, seed);
+            rnd_seeds(&rng, topk, sds, nlast);
+        } else if (probes) {
             gstart = g0;
             cur = probes[(size_t)qi * nprobe];
             cur_d = nno_dist(qv, 0, x, cur, d, metric);
@@ -939,7 +952,7 @@ int nno_search_ex(const float *x, uint32_t n, uint32_t d, const nno_layers *laye
             cur_d = nno_dist(qv, 0, x, cur, d, metric);
             cmps++;
         }
-        for (uint32_t ir = gstart; ir + 1 < L; ir++) {                    /* :397-420 */
+        for (uint32_t ir = gstart; !flat && ir + 1 < L; ir++) {           /* :397-420 */
             const uint64_t *off = layers->off[ir];
             const uint32_t *adj = layers->adj[ir];
             int moved = 1;
@@ -959,10 +972,22 @@ int nno_search_ex(const float *x, uint32_t n, uint32_t d, const nno_layers *laye
         const uint32_t *adj = layers->adj[L - 1];
         uint32_t npts = 0;
         top.n = cand.n = 0;
-        pq_push(&cand, -cur_d, cur);
-        pq_push(&top, cur_d, cur);
-        flags[cur] = 1;
-        pts[npts++] = cur;
+        if (flat) {
+            for (uint32_t i = 0; i < topk; i++) {  /* lysearch.cpp:462-472 */
+                const uint32_t s = sds[i];
+                const float ds = nno_dist(qv, 0, x, s, d, metric);
+                pq_push(&cand, -ds, s);
+                pq_push(&top, ds, s);
+                flags[s] = 1;
+                pts[npts++] = s;
+                cmps++;
+            }
+        } else {
+            pq_push(&cand, -cur_d, cur);
+            pq_push(&top, cur_d, cur);
+            flags[cur] = 1;
+            pts[npts++] = cur;
+        }
         float lwbnd = top.a[0].first;
         while (cand.n) {
             fpair c = cand.a[0];
@@ -1001,5 +1026,6 @@ int nno_search_ex(const float *x, uint32_t n, uint32_t d, const nno_layers *laye
     free(cand.a);
     free(flags);
     free(pts);
+    free(sds);
     return 0;
 }

@@ -63,10 +63,11 @@ int nno_search(const float *x, uint32_t n, uint32_t d, const nno_layers *layers,
                uint32_t *out_ids, float *out_dists, uint64_t *ncmps, uint32_t *entry);
 /* Serving form: per-query beam widths (beams, or `beam` for all), the first
  * out_k results of each query, and optional learned entries: the first
- * nearest of probes[i*nprobe ..] starts the greedy descent on layer g0. */
+ * nearest of probes[i*nprobe ..] starts the greedy descent on layer g0.
+ * flat != 0: nndFlatSrch (no descent, getRndSds seeds of the last layer). */
 int nno_search_ex(const float *x, uint32_t n, uint32_t d, const nno_layers *layers,
                   const float *q, uint32_t nq, const uint32_t *beams, uint32_t beam, uint32_t out_k,
-                  const uint32_t *probes, uint32_t nprobe, uint32_t g0, int metric, uint32_t seed,
+                  const uint32_t *probes, uint32_t nprobe, uint32_t g0, int flat, int metric, uint32_t seed,
                   uint32_t *out_ids, float *out_dists, uint64_t *ncmps, uint32_t *entry);
 
 /* Building blocks exposed for unit tests. */

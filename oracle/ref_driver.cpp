@@ -153,6 +153,31 @@ struct SearchProbe : public LySearch {
                 ds[(size_t)i * topk + r] = res[r].dst;
             }
         }
+        write(outp, nq, topk, enter, ids, ds);
+    }
+    /* LySearch::singleknnSearch's per-query step (lysearch.cpp:522-561): the
+     * reference's own nndFlatSrch on the last layer, which seeds each query
+     * with getRndSds(mt19937(time(NULL)), topk) (lysearch.cpp:455-460). */
+    void run_flat(const float *q, unsigned nq, unsigned dim, unsigned topk, const char *outp) {
+        flags = new unsigned short int[row];
+        std::memset(flags, 0, sizeof(unsigned short int) * row);
+        nCmps = 0;
+        std::vector<uint32_t> ids((size_t)nq * topk, 0xffffffffu);
+        std::vector<float> ds((size_t)nq * topk, 0.f);
+        std::vector<RTPair> res;
+        for (unsigned i = 0; i < nq; i++) {
+            crntQry = const_cast<float *>(q) + (size_t)i * dim;
+            res.clear();
+            nndFlatSrch(5, res, topk);
+            for (size_t r = 0; r < res.size() && r < topk; r++) {
+                ids[(size_t)i * topk + r] = res[r].id;
+                ds[(size_t)i * topk + r] = res[r].dst;
+            }
+        }
+        write(outp, nq, topk, 0, ids, ds);
+    }
+    void write(const char *outp, unsigned nq, unsigned topk, unsigned enter, const std::vector<uint32_t> &ids,
+               const std::vector<float> &ds) {
         FILE *f = std::fopen(outp, "wb");
         uint32_t hdr[3] = {nq, topk, enter};
         std::fwrite(hdr, 4, 3, f);
@@ -177,7 +202,7 @@ int usage() {
     std::fprintf(stderr,
         "usage: nnm_ref kgraph|smerge|jmerge <metric> <in.mat> <K> <seed> <out.graph>\n"
         "       nnm_ref hmerge <metric> <in.mat> <K> <M> <seed> <out.graph> <out_prefix>\n"
-        "       nnm_ref search <metric> <in.mat> <layers.txt> <queries.mat> <topk> <seed> <out.res>\n");
+        "       nnm_ref search|flatsearch <metric> <in.mat> <layers.txt> <queries.mat> <topk> <seed> <out.res>\n");
     return 2;
 }
 
@@ -239,7 +264,7 @@ int main(int argc, char **argv) {
         std::remove(grd.c_str());
         return 0;
     }
-    if (cmd == "search") {
+    if (cmd == "search" || cmd == "flatsearch") {
         if (argc != 9) return usage();
         SpaceInterface<float> *space = make_space(argv[2]);
         unsigned n, d, nq, qd;
@@ -252,7 +277,8 @@ int main(int argc, char **argv) {
         g_seed = (time_t)std::strtoll(argv[7], nullptr, 10);
         srand((unsigned)g_seed);
         auto *s = new SearchProbe(src.c_str(), argv[4], space);
-        s->run(q, nq, qd, topk, argv[8]);
+        if (cmd == "search") s->run(q, nq, qd, topk, argv[8]);
+        else s->run_flat(q, nq, qd, topk, argv[8]);
         std::remove(src.c_str());
         return 0;
     }

@@ -70,7 +70,10 @@ SEED = 20240601
 def main():
     if not ref_available():
         sys.exit("oracle/_ref/nnm_ref is missing: run `make -C oracle ref` first")
+    only = set(sys.argv[1:])  # optional: regenerate just these fixtures
     for name, cmd, make, k, extra in CASES:
+        if only and name not in only:
+            continue
         x = make()
         out = {"x_u8": x.astype(np.uint8), "k": k, "seed": SEED, "cmd": cmd,
                "metric": extra.get("metric", "l2")}
@@ -99,6 +102,11 @@ def main():
                         out["search%d_dists" % topk] = s["dists"]
                         out["search%d_ncmps" % topk] = s["ncmps"]
                         out["search%d_entry" % topk] = s["entry"]
+                        f = run_ref("flatsearch", x, None, SEED, td, metric=out["metric"],
+                                    layers_txt=os.path.join(td, "hier.txt"), queries=q, topk=topk)
+                        out["flat%d_ids" % topk] = f["ids"]
+                        out["flat%d_dists" % topk] = f["dists"]
+                        out["flat%d_ncmps" % topk] = f["ncmps"]
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **out)
         print("%-16s %-7s n=%-6d d=%-3d k=%-3d iters=%-3d ncmps=%d  %d bytes"

@@ -117,9 +117,11 @@ class Oracle:
             raise RuntimeError("oracle search failed")
         return dict(ids=ids, dists=ds, ncmps=int(nc.value), entry=int(ent.value))
 
-    def search_ex(self, x, layers, q, out_k, seed, beams=None, beam=None, probes=None, g0=0, metric="l2"):
+    def search_ex(self, x, layers, q, out_k, seed, beams=None, beam=None, probes=None, g0=0, flat=False,
+                  metric="l2"):
         """Serving form: per-query beams, the first out_k results, optional
-        learned entries (probes: nq x P rows of layer g0)."""
+        learned entries (probes: nq x P rows of layer g0) or the reference's
+        flat search (random seeds on the last layer, no descent)."""
         x = np.ascontiguousarray(x, dtype=np.float32)
         q = np.ascontiguousarray(q, dtype=np.float32)
         lay = Layers()
@@ -148,7 +150,8 @@ class Oracle:
                                     nul if b is None else _p(b, ctypes.c_uint32), ctypes.c_uint32(beam),
                                     ctypes.c_uint32(out_k), nul if pr is None else _p(pr, ctypes.c_uint32),
                                     ctypes.c_uint32(0 if pr is None else pr.shape[1]), ctypes.c_uint32(g0),
-                                    ctypes.c_int(METRICS[metric]), ctypes.c_uint32(seed),
+                                    ctypes.c_int(1 if flat else 0), ctypes.c_int(METRICS[metric]),
+                                    ctypes.c_uint32(seed),
                                     _p(ids, ctypes.c_uint32), _p(ds, ctypes.c_float),
                                     ctypes.byref(nc), ctypes.byref(ent))
         if rc:
@@ -239,7 +242,7 @@ def run_ref(cmd, x, k, seed, tmpdir, metric="l2", m=None, layers_txt=None, queri
     r = subprocess.run(argv, capture_output=True, text=True, cwd=tmpdir)
     if r.returncode != 0:
         raise RuntimeError("reference failed: %s %s" % (r.stdout[-2000:], r.stderr[-2000:]))
-    if cmd == "search":
+    if cmd in ("search", "flatsearch"):
         b = open(out, "rb").read()
         nq, tk, entry = struct.unpack("<III", b[:12])
         nc, = struct.unpack("<Q", b[12:20])

@@ -45,6 +45,17 @@ def test_oracle_search_matches_golden(oracle):
         assert got["entry"] == int(fx["search%d_entry" % topk])
 
 
+def test_oracle_flat_search_matches_golden(oracle):
+    """nndFlatSrch: the reference's own flat search (random seeds of the
+    last layer, no descent) against the oracle's restatement."""
+    fx = golden_lib.load("hmerge_search")
+    for topk in (1, 10, 40):
+        got = oracle.search_ex(fx["x"], fx["layers"], fx["q"], topk, fx["seed"], beam=topk, flat=True)
+        assert np.array_equal(got["ids"], fx["flat%d_ids" % topk])
+        assert np.array_equal(got["dists"], fx["flat%d_dists" % topk])
+        assert got["ncmps"] == int(fx["flat%d_ncmps" % topk])
+
+
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
 @pytest.mark.parametrize("cmd,n,k,seed", [("kgraph", 1500, 20, 1), ("kgraph", 900, 16, 123456),
                                           ("smerge", 1200, 20, 7), ("jmerge", 1300, 12, 99),
