@@ -89,6 +89,7 @@ def parse():
     p.add_argument("--queries", type=int, default=100_000)
     p.add_argument("--probes", type=int, default=4)
     p.add_argument("--entry-steps", type=int, default=1500)
+    p.add_argument("--no-flat", action="store_true", help="search: skip the flat k-NN graph measurement")
     return p.parse_args()
 
 
@@ -361,6 +362,30 @@ def run_search(a, rank, world, local):
         e2e = {"value": world * nq / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": int(q.nbytes + beams.nbytes),
                "d2h_bytes_per_step": int(nq * 10 * 8)}
 
+    # the same queries against the flat 1M k-NN graph of the headline build
+    # (one layer): the reference's flat search (random seeds) vs the
+    # learned entry
+    flat = None
+    if not a.no_flat:
+        k_ids = torch.empty((n, k), dtype=torch.int32, device="cuda")
+        k_ds = torch.empty((n, k), dtype=torch.float32, device="cuda")
+        ctx.merge_leaves_dev(x_t.data_ptr(), n, d, k, leaf_sizes(n, a.leaves), k_ids.data_ptr(), k_ds.data_ptr(), 0,
+                             seed=a.seed, rng="fast", join="tensor", init="random")
+        adj = k_ids.cpu().numpy().view(np.uint32).reshape(-1)
+        fx = ctx.index(x, [(np.arange(0, n * k + 1, k, dtype=np.uint64), adj)], seed=a.seed)
+        fl, fc = fx.entry_layer()
+        fm = nnm.entry_init(d, fc, seed=11)
+        fx.entry_train(fm, steps=a.entry_steps, batch=2048, lr=2e-3, seed=3)
+        fx.set_entry_model(fm, probes=a.probes)
+        flat = {}
+        for entry in ("flat", "learned"):
+            fx.search(q, out_k=10, beams=beams, mode="fast", entry=entry)
+            r = fx.search(q, out_k=10, beams=beams, mode="fast", entry=entry)
+            flat[entry] = {"qps": nq / r["device_ms"] * 1e3, "ms": r["device_ms"],
+                           "recall": search_recall(r["ids"][:nrec], x, q[:nrec], kth),
+                           "ncmps": r["ncmps"] / nq, "expansions": r["expansions"] / nq}
+        fx.close()
+
     hbm, peak_kind = peaks()
     kern_ms = learned["ms"] - learned["predict_ms"]
     row_bytes = ((d + 3) // 4) * 16
@@ -396,6 +421,7 @@ def run_search(a, rank, world, local):
                        "equal_recall": {"default_recall": default["recall"], "sweep": sweep,
                                         "learned_qps_at_default_recall": eq[-1]["qps"] if eq else None,
                                         "speedup": (eq[-1]["qps"] / (nq / default["ms"] * 1e3)) if eq else None},
+                       "flat_graph": flat,
                        "l2": "vectors (%d MB) larger than L2 (126 MB)" % (x.nbytes >> 20),
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": learned["launches"],

@@ -263,7 +263,14 @@ int nnm_set_init_model(nnm_ctx *ctx, const nnm_mlp *model);
 typedef struct nnm_index nnm_index;
 
 typedef enum { NNM_SERVE_EXACT = 0, NNM_SERVE_FAST = 1 } nnm_serve_mode;
-typedef enum { NNM_ENTRY_DEFAULT = 0, NNM_ENTRY_LEARNED = 1 } nnm_entry_mode;
+typedef enum {
+    NNM_ENTRY_DEFAULT = 0, /* LySearch::knnSearch: one global entry, greedy descent from layer 0 */
+    NNM_ENTRY_LEARNED = 1, /* the entry network's probes, descent from their layer */
+    NNM_ENTRY_FLAT = 2     /* LySearch::nndFlatSrch (lysearch.cpp:439-520): no descent; the beam starts
+                              with `beam` distinct rows of the last layer drawn by getRndSds from a fresh
+                              mt19937(seed) (the reference reseeds per query from its clock); every
+                              beam width must be at most the last layer's rows */
+} nnm_entry_mode;
 
 typedef struct {
     uint64_t ncmps;       /* distance evaluations, all queries (entry probes included) */

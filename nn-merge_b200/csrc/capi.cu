@@ -531,7 +531,7 @@ int index_search_impl(nnm_index* h, const float* q, uint64_t nq, const uint32_t*
     if (nq == 0) return NNM_OK;
     if (!q || !out_ids) return fail(ctx, NNM_ERR_INVALID, "q and out_ids are required");
     if (nq >= (1ull << 31)) return fail(ctx, NNM_ERR_INVALID, "nq must be below 2^31");
-    if (smode > NNM_SERVE_FAST || emode > NNM_ENTRY_LEARNED) return fail(ctx, NNM_ERR_INVALID, "unknown mode");
+    if (smode > NNM_SERVE_FAST || emode > NNM_ENTRY_FLAT) return fail(ctx, NNM_ERR_INVALID, "unknown mode");
     if (emode == NNM_ENTRY_LEARNED && !ix.net) return fail(ctx, NNM_ERR_INVALID, "no entry model set");
     if (out_k == 0) return fail(ctx, NNM_ERR_INVALID, "out_k must be positive");
     uint32_t bmax = beam;
@@ -601,6 +601,11 @@ int index_search_impl(nnm_index* h, const float* q, uint64_t nq, const uint32_t*
         r.probes = ix.probes.as<uint32_t>();
         r.nprobe = ix.nprobe;
         r.g0 = ix.entry_layer;
+    } else if (emode == NNM_ENTRY_FLAT) {
+        rc = nnm::index_flat_seeds(c, ix, bmax);
+        r.flat = 1;
+        r.flat_off = ix.flat_off.as<uint32_t>();
+        r.flat_pool = ix.flat_pool.as<uint32_t>();
     }
     cudaEventRecord(ev[1], st);
     if (!rc) rc = smode == NNM_SERVE_FAST ? nnm::index_run_fast(c, ix, r) : nnm::index_run_exact(c, ix, r);

@@ -43,6 +43,8 @@ struct IndexDev {
     DevBuf x, off, adj;
     DevBuf visited, vlist, cand, ctr;          // per-warp scratch and counters
     DevBuf qpad, beams, probes, hid, scores, out;  // per-call staging
+    DevBuf flat_off, flat_pool;                // flat-search seeds of every beam width <= flat_max
+    uint32_t flat_max = 0;
     DevEntry* net = nullptr;                   // entry network, owned
     uint32_t nprobe = 0, entry_layer = 0, n_classes = 0;
     uint32_t width = 4;  // fast kernel: most unexpanded entries expanded together
@@ -57,6 +59,9 @@ struct SearchReq {
     uint32_t beam, beam_max, out_k;
     const uint32_t* probes;   // nq x nprobe rows of layer g0, or null: default entry
     uint32_t nprobe, g0;
+    uint32_t flat;            // nndFlatSrch: getRndSds seeds of the last layer, no descent
+    const uint32_t* flat_off;
+    const uint32_t* flat_pool;
     uint32_t* out_ids;        // nq x out_k
     float* out_d;             // nq x out_k or null
 };
@@ -67,6 +72,8 @@ int index_upload(Ctx& ctx, IndexDev& ix, const float* x, uint64_t n, uint32_t d,
 // distance and expansion counts) before a run.
 int index_run_exact(Ctx& ctx, IndexDev& ix, const SearchReq& r);
 int index_run_fast(Ctx& ctx, IndexDev& ix, const SearchReq& r);
+// Seeds of nndFlatSrch for every beam width up to beam_max (cached).
+int index_flat_seeds(Ctx& ctx, IndexDev& ix, uint32_t beam_max);
 // Waits for the stream, reads the distance and expansion counts of the last
 // run and turns its self-check flags into an error.
 int index_counters(Ctx& ctx, IndexDev& ix, uint64_t* ncmps, uint64_t* nexp);

@@ -3,7 +3,8 @@
 // One warp per query, persistent warps pulling queries from a counter so
 // that queries of different beam widths balance.  Per query:
 //   - entry point: one global id, rand() % |layer 0| after srand(seed)
-//     (lysearch.cpp:382);
+//     (lysearch.cpp:382); or, for nndFlatSrch (lysearch.cpp:439-520), no
+//     descent and `topk` getRndSds seeds of the last layer in both heaps;
 //   - greedy 1-NN descent through layers 0..L-2 (lysearch.cpp:397-420): the
 //     distances of a node's neighbours are computed in parallel, one
 //     neighbour per lane, and the moves are then applied in list order, as
@@ -95,6 +96,9 @@ struct SearchArgs {
     uint32_t out_k;          // results written per query
     const uint32_t* probes;  // learned entries: nq x nprobe rows of layer g0, or null
     uint32_t nprobe, g0;
+    uint32_t flat;           // nndFlatSrch: random seeds of the last layer, no descent
+    const uint32_t* flat_off;   // seeds of beam width b at flat_pool + flat_off[b]
+    const uint32_t* flat_pool;
     uint32_t* out_ids;
     float* out_d;
     uint32_t* visited;  // per warp slot: ceil(n/32) words
@@ -143,8 +147,10 @@ __global__ void k_search(SearchArgs a) {
         for (uint32_t t = lane; t < a.dp; t += 32) qv[t] = a.q[(size_t)qi * a.dp + t];
         __syncwarp();
         uint32_t cur = a.entry, g0 = 0;
-        float cur_d;
-        if (a.probes) {
+        float cur_d = 0.f;
+        if (a.flat) {
+            g0 = a.L - 1;  // nndFlatSrch (lysearch.cpp:439-520): no descent
+        } else if (a.probes) {
             // learned entries: the first nearest of the probed rows of layer g0,
             // taken in probe order as the descent takes a list
             g0 = a.g0;
@@ -208,12 +214,44 @@ __global__ void k_search(SearchArgs a) {
         const uint64_t* off = a.off_all + a.off_base[a.L - 1];
         uint32_t ntop = 0, ncand = 0, nvis = 1;
         bool vis_overflow = false;
-        const bool start_ok = cur < a.nrows[a.L - 1];  // false only after a failed greedy check
-        if (lane == 0 && start_ok) {
-            heap_push(cand, ncand, HP{-cur_d, cur});
-            heap_push(top, ntop, HP{cur_d, cur});
-            atomicOr(&vis[cur >> 5], 1u << (cur & 31));
-            vl[0] = cur;
+        bool start_ok = true;
+        if (a.flat) {
+            // the getRndSds seeds of this beam width, pushed in draw order
+            // (lysearch.cpp:462-472); their distances in parallel first
+            const uint32_t* sd = a.flat_pool + a.flat_off[topk];
+            nvis = 0;
+            for (uint32_t c0 = 0; c0 < topk; c0 += 32) {
+                const uint32_t cnt = min(32u, topk - c0);
+                if (lane < cnt) {
+                    const uint32_t id = sd[c0 + lane];
+                    stage_i[lane] = id;
+                    stage_d[lane] = dist_seq_rt(a.metric, qv, a.x + (size_t)id * a.dp, a.dp);
+                    atomicOr(&vis[id >> 5], 1u << (id & 31));
+                    if (nvis + lane < VCAP) vl[nvis + lane] = id;
+                }
+                __syncwarp();
+                if (lane == 0)
+                    for (uint32_t r = 0; r < cnt; r++) {
+                        if (ncand >= CCAP) {
+                            atomicOr(a.overflow, SERR_HEAP);
+                            break;
+                        }
+                        heap_push(cand, ncand, HP{-stage_d[r], stage_i[r]});
+                        heap_push(top, ntop, HP{stage_d[r], stage_i[r]});
+                    }
+                __syncwarp();
+                nvis += cnt;
+                cmps += cnt;
+            }
+            if (nvis > VCAP) vis_overflow = true;
+        } else {
+            start_ok = cur < a.nrows[a.L - 1];  // false only after a failed greedy check
+            if (lane == 0 && start_ok) {
+                heap_push(cand, ncand, HP{-cur_d, cur});
+                heap_push(top, ntop, HP{cur_d, cur});
+                atomicOr(&vis[cur >> 5], 1u << (cur & 31));
+                vl[0] = cur;
+            }
         }
         ncand = __shfl_sync(FULL, ncand, 0);
         ntop = __shfl_sync(FULL, ntop, 0);
@@ -447,6 +485,9 @@ int index_run_exact(Ctx& ctx, IndexDev& ix, const SearchReq& r) {
     a.probes = r.probes;
     a.nprobe = r.nprobe;
     a.g0 = r.g0;
+    a.flat = r.flat;
+    a.flat_off = r.flat_off;
+    a.flat_pool = r.flat_pool;
     a.out_ids = r.out_ids;
     a.out_d = r.out_d;
     a.visited = ix.visited.as<uint32_t>();
@@ -460,6 +501,47 @@ int index_run_exact(Ctx& ctx, IndexDev& ix, const SearchReq& r) {
     a.nexp = reinterpret_cast<unsigned long long*>(c + 16);
     k_search<<<blocks, SWARPS * 32, smem, st>>>(a); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// getRndSds (lysearch.cpp:206-233) with a fresh std::mt19937(seed): k
+// distinct ids of [0, N) -- what nndFlatSrch draws per query with the clock
+// frozen at `seed`.
+static void rnd_seeds(uint32_t seed, uint32_t k, uint32_t N, uint32_t* out) {
+    if (N == k) {
+        for (uint32_t i = 0; i < k; i++) out[i] = i;
+        return;
+    }
+    std::vector<uint32_t> r(k + 1);
+    gen_mt19937(seed, k + 1, r.data());
+    for (uint32_t i = 0; i < k; i++) out[i] = r[i] % (N - k);
+    std::sort(out, out + k);
+    for (uint32_t i = 1; i < k; i++)
+        if (out[i] <= out[i - 1]) out[i] = out[i - 1] + 1;
+    const uint32_t off = r[k] % N;
+    for (uint32_t i = 0; i < k; i++) out[i] = (uint32_t)(((uint64_t)out[i] + off) % N);
+}
+
+int index_flat_seeds(Ctx& ctx, IndexDev& ix, uint32_t beam_max) {
+    const uint32_t N = ix.nrows[ix.L - 1];
+    if (beam_max > N) {
+        ctx.last_error = "flat search: a beam width is larger than the last layer";
+        return 1;
+    }
+    if (ix.flat_max >= beam_max) return 0;
+    // seeds of every beam width 1..beam_max, concatenated
+    std::vector<uint32_t> off(beam_max + 1, 0), pool;
+    pool.reserve((size_t)beam_max * (beam_max + 1) / 2);
+    for (uint32_t b = 1; b <= beam_max; b++) {
+        off[b] = (uint32_t)pool.size();
+        pool.resize(pool.size() + b);
+        rnd_seeds(ix.seed, b, N, pool.data() + off[b]);
+    }
+    NNM_CUDA_TRY(ix.flat_off.ensure(off.size() * 4));
+    NNM_CUDA_TRY(ix.flat_pool.ensure(std::max<size_t>(pool.size(), 1) * 4));
+    NNM_CUDA_TRY(cudaMemcpy(ix.flat_off.p, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+    NNM_CUDA_TRY(cudaMemcpy(ix.flat_pool.p, pool.data(), pool.size() * 4, cudaMemcpyHostToDevice));
+    ix.flat_max = beam_max;
     return 0;
 }
 
@@ -480,7 +562,8 @@ int index_counters(Ctx& ctx, IndexDev& ix, uint64_t* ncmps, uint64_t* nexp) {
 }
 
 void IndexDev::release() {
-    DevBuf* all[] = {&x, &off, &adj, &visited, &vlist, &cand, &ctr, &qpad, &beams, &probes, &hid, &scores, &out};
+    DevBuf* all[] = {&x,     &off,   &adj,  &visited, &vlist,  &cand,     &ctr,      &qpad,
+                     &beams, &probes, &hid, &scores,  &out,    &flat_off, &flat_pool};
     for (auto* b : all) b->release();
 }
 

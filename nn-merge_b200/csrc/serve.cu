@@ -67,6 +67,9 @@ struct ServeArgs {
     uint32_t words;
     uint32_t* vlist;
     uint32_t width;  // most unexpanded entries expanded together (1..4)
+    uint32_t flat;               // nndFlatSrch: random seeds, no descent
+    const uint32_t* flat_off;    // seeds of beam width b at flat_pool + flat_off[b]
+    const uint32_t* flat_pool;
     unsigned* next_q;
     unsigned* overflow;
     unsigned long long* ncmps;
@@ -242,9 +245,11 @@ __global__ void __launch_bounds__(FW * 32) k_serve(ServeArgs a) {
                                : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         // entry
-        uint32_t cur, g0;
-        float cur_d;
-        if (a.probes) {
+        uint32_t cur = 0, g0;
+        float cur_d = 0.f;
+        if (a.flat) {
+            g0 = a.L - 1;  // nndFlatSrch: no descent; the seeds start the beam
+        } else if (a.probes) {
             g0 = a.g0;
             uint32_t pid = 0;
             if (lane < a.nprobe) {
@@ -301,7 +306,80 @@ __global__ void __launch_bounds__(FW * 32) k_serve(ServeArgs a) {
         // beam on the last layer
         const uint64_t* off = a.off_all + a.off_base[a.L - 1];
         uint32_t m = 0, p = 0, nvis = 0;
-        if (cur < nlast) {
+        // Offers the fresh rows whose ids lanes [0, nf) hold: distances, the
+        // ones below the worst entry of a full beam sorted by a bitonic
+        // network over those lanes and merged in place -- entries before the
+        // first new one keep their slots; the suffix [lo0, m) is staged, then
+        // every entry of the merged range [lo0, m2) is written once.
+        auto offer = [&](uint32_t fid, uint32_t nf) {
+            cmps += nf;
+            const float dd = warp_dists<M, QV>(qr, x4, a.dp4, fid, nf, lane);
+            bool acc = lane < nf;
+            if (m >= ef) acc = acc && key_less(dd, fid, bd[m - 1], bi[m - 1] & IDM);
+            const uint32_t nk = __popc(__ballot_sync(FULL, acc));
+            if (nk == 0) return;
+            float kd = acc ? dd : INFINITY;
+            uint32_t kid = acc ? fid : 0xffffffffu;
+            uint32_t w = 1;
+            while (w < nf) w <<= 1;
+            warp_sort(kd, kid, lane, w);
+            __syncwarp();
+            nd[lane] = kd;
+            ni[lane] = kid;
+            const uint32_t m2 = min(ef, m + nk);
+            uint32_t npos = 0;
+            if (lane < nk) {
+                uint32_t lo = 0, hi = m;
+                while (lo < hi) {
+                    const uint32_t md = (lo + hi) >> 1;
+                    if (key_less(bd[md], bi[md] & IDM, kd, kid)) lo = md + 1;
+                    else hi = md;
+                }
+                npos = lane + lo;
+            }
+            const uint32_t lo0 = __shfl_sync(FULL, npos, 0);
+            for (uint32_t i = lo0 + lane; i < m; i += 32) {
+                td[i - lo0] = bd[i];
+                ti[i - lo0] = bi[i];
+            }
+            __syncwarp();
+            for (uint32_t i = lo0 + lane; i < m; i += 32) {
+                const float d0 = td[i - lo0];
+                const uint32_t i0 = ti[i - lo0];
+                uint32_t lo = 0, hi = nk;
+                while (lo < hi) {
+                    const uint32_t md = (lo + hi) >> 1;
+                    if (key_less(nd[md], ni[md], d0, i0 & IDM)) lo = md + 1;
+                    else hi = md;
+                }
+                if (i + lo < m2) {
+                    bd[i + lo] = d0;
+                    bi[i + lo] = i0;
+                }
+            }
+            if (lane < nk && npos < m2) {
+                bd[npos] = kd;
+                bi[npos] = kid;
+            }
+            __syncwarp();
+            m = m2;
+            if (lo0 < p) p = lo0;
+        };
+        if (a.flat) {
+            // nndFlatSrch (lysearch.cpp:455-472): the beam's getRndSds seeds
+            const uint32_t* sd = a.flat_pool + a.flat_off[ef];
+            for (uint32_t c0 = 0; c0 < ef; c0 += 32) {
+                const uint32_t cnt = min(32u, ef - c0);
+                uint32_t id = 0;
+                if (lane < cnt) {
+                    id = sd[c0 + lane];
+                    atomicOr(&vis[id >> 5], 1u << (id & 31));
+                    if (nvis + lane < FVCAP) vl[nvis + lane] = id;
+                }
+                nvis += cnt;
+                offer(id, cnt);
+            }
+        } else if (cur < nlast) {
             if (lane == 0) {
                 bd[0] = cur_d;
                 bi[0] = cur;
@@ -382,63 +460,8 @@ __global__ void __launch_bounds__(FW * 32) k_serve(ServeArgs a) {
                 __syncwarp();
                 const uint32_t fid = lane < nf ? ni[lane] : 0u;
                 nvis += nf;
-                cmps += nf;
-                const float dd = warp_dists<M, QV>(qr, x4, a.dp4, fid, nf, lane);
-                // accepted: below the worst entry of a full beam
-                bool acc = lane < nf;
-                if (m >= ef) acc = acc && key_less(dd, fid, bd[m - 1], bi[m - 1] & IDM);
-                const uint32_t nk = __popc(__ballot_sync(FULL, acc));
-                if (nk == 0) continue;
-                float kd = acc ? dd : INFINITY;
-                uint32_t kid = acc ? fid : 0xffffffffu;
-                // the accepted entries are among lanes [0, nf): sort that many
-                uint32_t w = 1;
-                while (w < nf) w <<= 1;
-                warp_sort(kd, kid, lane, w);
-                __syncwarp();
-                nd[lane] = kd;
-                ni[lane] = kid;
-                // merge in place: entries before the first new one keep their
-                // slots; the suffix [lo0, m) is staged, then every entry of the
-                // merged range [lo0, m2) is written once
-                const uint32_t m2 = min(ef, m + nk);
-                uint32_t npos = 0;
-                if (lane < nk) {
-                    uint32_t lo = 0, hi = m;
-                    while (lo < hi) {
-                        const uint32_t md = (lo + hi) >> 1;
-                        if (key_less(bd[md], bi[md] & IDM, kd, kid)) lo = md + 1;
-                        else hi = md;
-                    }
-                    npos = lane + lo;
-                }
-                const uint32_t lo0 = __shfl_sync(FULL, npos, 0);
-                for (uint32_t i = lo0 + lane; i < m; i += 32) {
-                    td[i - lo0] = bd[i];
-                    ti[i - lo0] = bi[i];
-                }
-                __syncwarp();
-                for (uint32_t i = lo0 + lane; i < m; i += 32) {
-                    const float d0 = td[i - lo0];
-                    const uint32_t i0 = ti[i - lo0];
-                    uint32_t lo = 0, hi = nk;
-                    while (lo < hi) {
-                        const uint32_t md = (lo + hi) >> 1;
-                        if (key_less(nd[md], ni[md], d0, i0 & IDM)) lo = md + 1;
-                        else hi = md;
-                    }
-                    if (i + lo < m2) {
-                        bd[i + lo] = d0;
-                        bi[i + lo] = i0;
-                    }
-                }
-                if (lane < nk && npos < m2) {
-                    bd[npos] = kd;
-                    bi[npos] = kid;
-                }
-                __syncwarp();
-                m = m2;
-                if (lo0 < p) p = lo0;
+                __syncwarp();  // every lane has read its id before offer() reuses ni
+                offer(fid, nf);
             }
         }
         // results: the first out_k entries
@@ -520,6 +543,9 @@ int index_run_fast(Ctx& ctx, IndexDev& ix, const SearchReq& r) {
     a.words = words;
     a.vlist = ix.vlist.as<uint32_t>();
     a.width = ix.width;
+    a.flat = r.flat;
+    a.flat_off = r.flat_off;
+    a.flat_pool = r.flat_pool;
     unsigned char* c = ix.ctr.as<unsigned char>();
     a.next_q = reinterpret_cast<unsigned*>(c);
     a.overflow = reinterpret_cast<unsigned*>(c + 4);

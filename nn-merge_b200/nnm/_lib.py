@@ -400,7 +400,7 @@ def _layers_struct(layers):
 
 
 SERVE_MODES = {"exact": 0, "fast": 1}
-ENTRY_MODES = {"default": 0, "learned": 1}
+ENTRY_MODES = {"default": 0, "learned": 1, "flat": 2}
 
 
 class Index:

@@ -92,6 +92,57 @@ def test_exact_learned_entries_match_oracle(ctx, oracle, hier, index):
     assert got["ncmps"] == exp["ncmps"]
 
 
+def test_exact_flat_search_matches_oracle(oracle, hier, index):
+    x, layers, q = hier
+    beams = np.random.default_rng(17).integers(10, 97, size=500).astype(np.uint32)
+    exp = oracle.search_ex(x, layers, q[:500], 10, 9, beams=beams, flat=True)
+    got = index.search(q[:500], out_k=10, beams=beams, mode="exact", entry="flat")
+    assert np.array_equal(got["ids"], exp["ids"])
+    assert np.array_equal(got["dists"].view(np.uint32), exp["dists"].view(np.uint32))
+    assert got["ncmps"] == exp["ncmps"]
+
+
+def test_flat_search_matches_reference_golden(ctx):
+    """nndFlatSrch as the reference itself ran it (tests/golden)."""
+    import golden_lib
+    fx = golden_lib.load("hmerge_search")
+    ix = ctx.index(fx["x"], fx["layers"], seed=int(fx["seed"]))
+    try:
+        for topk in (1, 10, 40):
+            got = ix.search(fx["q"], out_k=topk, beam=topk, mode="exact", entry="flat")
+            assert np.array_equal(got["ids"], fx["flat%d_ids" % topk])
+            assert np.array_equal(got["dists"], fx["flat%d_dists" % topk])
+            assert got["ncmps"] == int(fx["flat%d_ncmps" % topk])
+    finally:
+        ix.close()
+
+
+def test_fast_flat_search(hier, index):
+    x, _, q = hier
+    beams = np.random.default_rng(18).integers(32, 129, size=NQ).astype(np.uint32)
+    f = index.search(q, out_k=10, beams=beams, mode="fast", entry="flat")
+    e = index.search(q, out_k=10, beams=beams, mode="exact", entry="flat")
+    assert (np.diff(f["dists"], axis=1) >= 0).all() and all(len(set(r)) == 10 for r in f["ids"])
+    _, gt_d = truth(x, q)
+    rf, re = recall(f["ids"], gt_d, x, q), recall(e["ids"], gt_d, x, q)
+    print("flat recall fast %.4f exact %.4f" % (rf, re))
+    assert rf >= re - 0.01
+
+
+def test_flat_beam_larger_than_layer_is_rejected(ctx):
+    x = gaussian_mixture_u8(200, d=16, seed=3)
+    off = np.arange(0, 201 * 4, 4, dtype=np.uint64)
+    adj = np.random.default_rng(0).integers(0, 200, size=800).astype(np.uint32)
+    ix = ctx.index(x, [(off, adj)], seed=1)
+    try:
+        with pytest.raises(NnmError):
+            ix.search(x[:5], out_k=10, beam=300, mode="fast", entry="flat")
+        r = ix.search(x[:5], out_k=10, beam=200, mode="exact", entry="flat")
+        assert (r["ids"][:, 0] == np.arange(5)).all()  # every row is a seed: exact search
+    finally:
+        ix.close()
+
+
 def test_fast_results_are_exact_distances_and_recall_holds(hier, index):
     x, _, q = hier
     rng = np.random.default_rng(8)
