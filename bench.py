@@ -84,6 +84,8 @@ def parse():
                    help="initial graphs: random, or from the codes of a trained MLP (needs --path fast)")
     p.add_argument("--train-steps", type=int, default=400)
     p.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 path beside")
+    p.add_argument("--no-tune", action="store_true",
+                   help="skip the autotuner (sample cap and convergence threshold from --smpl/--delta)")
     p.add_argument("--workload", default="build", choices=["build", "search"],
                    help="build: the headline 1M graph build; search: batched LySearch serving on a 1M hierarchy")
     p.add_argument("--queries", type=int, default=100_000)
@@ -513,6 +515,19 @@ def main():
                  "loss_first": float(losses[:10].mean()), "loss_last": float(losses[-10:].mean())}
         ctx.set_init_model(model)
 
+    # autotuner (untimed, like the training): sample cap and convergence
+    # threshold from trial builds on the whole set (a smaller sample reads a
+    # higher recall than the full build), scored on the device on 2,000 rows
+    # against recall@10 >= 0.95 + 0.005
+    tune = None
+    if not a.no_tune and a.path == "fast":
+        t0 = time.perf_counter()
+        chosen, trials = ctx.autotune_merge_leaves_dev(x_dev.data_ptr(), n, d, k, sizes, sample_rows=n,
+                                                       eval_rows=2000, repeats=2, **bkw)
+        bkw.update(chosen)
+        tune = {"chosen": chosen, "s": time.perf_counter() - t0, "sample_rows": n, "eval_rows": 2000,
+                "trials": trials}
+
     rng_rows = np.random.default_rng(7)
     rows = np.sort(rng_rows.choice(n, min(a.recall_rows, n), replace=False))
 
@@ -619,8 +634,8 @@ def main():
                                       if (a.path, a.join, a.init) == ("exact", "fp32", "random")
                                       else "%s init, %s draws, %s join" % (a.init, a.path, a.join)),
                        "n": n, "d": d, "k": k, "leaves": a.leaves,
-                       "path": a.path, "init": a.init, "train": train,
-                       "delta": bkw["delta"], "smpl": a.smpl, "join": a.join,
+                       "path": a.path, "init": a.init, "train": train, "tune": tune,
+                       "delta": bkw["delta"], "smpl": bkw["sample_cap"], "join": a.join,
                        "join_rows": prof["rows"],
                        "recall@10": rec, "iterations": st["iterations"], "ncmps_merge": st["ncmps"],
                        "ncmps_leaves": st["sub_ncmps"],

@@ -342,6 +342,53 @@ int nnm_entry_train(nnm_index *ix, nnm_entry_mlp *model, const nnm_train_opts *o
  * 1..min(8, C); NULL clears it. */
 int nnm_index_set_entry_model(nnm_index *ix, const nnm_entry_mlp *model, uint32_t probes);
 
+/* Recall@atop of a k-NN graph (Evaluator::getKGraphRecall,
+ * evaluator.cpp:258-295, with the ground truth computed on the device): for
+ * each of the `nrows` listed rows, the share of its first atop ids (atop
+ * <= 16) whose distance is at most the row's atop-th exact nearest distance
+ * (brute force over all other rows, the reference's FP32 sums; rows tied at
+ * that distance count as hits).  x: n x d, ids: n x k, rows: nrows, all host.
+ * d <= 512. */
+int nnm_graph_recall(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, const uint32_t *ids, uint32_t k,
+                     const uint32_t *rows, uint32_t nrows, uint32_t atop, double *recall);
+
+/* Autotuner (no counterpart in the reference) for nnm_merge_leaves_dev:
+ * trial builds on the first sample_rows rows of x (leaf sizes scaled to
+ * the sample) over a grid of reverse-sample caps (smplNum) and convergence
+ * thresholds, each scored with nnm_graph_recall on eval_rows seeded rows
+ * and timed with CUDA events; the chosen setting is the fastest whose
+ * sample recall@10 is at least target_recall + margin (else the one of the
+ * highest recall).  `tuned` is `base` with sample_cap and delta replaced.
+ * A sample smaller than the data set usually reads a higher recall than the
+ * full build reaches (its clusters are sparser); sample_rows = n tunes on
+ * the build itself. */
+typedef struct {
+    float target_recall;  /* 0.95 */
+    float margin;         /* 0.005: the sample's recall is read above the full build's */
+    uint32_t sample_rows; /* 200000 (at most n) */
+    uint32_t eval_rows;   /* 1000 */
+    uint32_t repeats;     /* timed builds per setting, the fastest kept: 2 */
+    uint32_t reserved[7];
+} nnm_tune_opts;
+
+#define NNM_TUNE_MAX_TRIALS 32
+typedef struct {
+    uint32_t sample_cap;
+    float delta;
+    float recall; /* on the sample */
+    double ms;    /* device time of the sample build */
+} nnm_tune_trial;
+
+typedef struct {
+    uint32_t ntrials, chosen; /* trials run; index of the chosen one */
+    nnm_tune_trial trials[NNM_TUNE_MAX_TRIALS];
+} nnm_tune_result;
+
+void nnm_tune_opts_default(nnm_tune_opts *o);
+int nnm_autotune_merge_leaves(nnm_ctx *ctx, const float *x_dev, uint64_t n, uint32_t d, uint32_t k,
+                              const uint32_t *leaf_sizes, uint32_t nleaf, const nnm_opts *base,
+                              const nnm_tune_opts *topts, nnm_opts *tuned, nnm_tune_result *result);
+
 /* Profiling (no counterpart in the reference, which times whole builds with
  * boost::timer): while enabled, the engine records CUDA events around its
  * local-join and top-K merge kernels and accumulates their device time and

@@ -2,11 +2,14 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <random>
 #include <string>
+#include <vector>
 
 #include "../../include/nnm.h"
 #include "nnm_builders.h"
 #include "nnm_entry.h"
+#include "nnm_eval.h"
 #include "nnm_hier.h"
 #include "nnm_launch.h"
 #include "nnm_learned.h"
@@ -481,6 +484,133 @@ int nnm_search(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, const nnm_l
     Ctx& c = ctx->c;
     if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
     return nnm::search_host(c, x, n, d, layers, q, nq, topk, o.seed, (int)o.metric, out_ids, out_dists, ncmps);
+}
+
+int nnm_graph_recall(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, const uint32_t* ids, uint32_t k,
+                     const uint32_t* rows, uint32_t nrows, uint32_t atop, double* recall) {
+    if (!ctx || !x || !ids || !recall || (nrows && !rows) || n < 2 || n >= (1ull << 30) || d == 0 || d > 512 ||
+        k == 0 || atop == 0 || atop > (uint32_t)nnm::EVAL_MAX_ATOP || atop > k)
+        return ctx ? fail(ctx, NNM_ERR_INVALID, "recall: bad arguments (atop <= min(16, k), d <= 512)")
+                   : NNM_ERR_INVALID;
+    for (uint32_t i = 0; i < nrows; i++)
+        if (rows[i] >= n) return fail(ctx, NNM_ERR_INVALID, "recall: row out of range");
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    GraphStore st;
+    GraphDev g;
+    nnm::DevBuf ib, rb;
+    int rc = upload_plain(c, st, g, x, n, d);
+    if (!rc && (ib.ensure(n * k * 4) != cudaSuccess || rb.ensure((size_t)nrows * 4 + 4) != cudaSuccess))
+        rc = fail(ctx, NNM_ERR_OOM, "device allocation failed");
+    if (!rc && (cudaMemcpy(ib.p, ids, n * k * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+                (nrows && cudaMemcpy(rb.p, rows, (size_t)nrows * 4, cudaMemcpyHostToDevice) != cudaSuccess)))
+        rc = NNM_ERR_CUDA;
+    if (!rc)
+        rc = nnm::graph_recall_dev(c, g.x, (uint32_t)n, g.dp, NNM_METRIC_L2, ib.as<uint32_t>(), k, rb.as<uint32_t>(),
+                                   nrows, atop, recall);
+    st.release();
+    ib.release();
+    rb.release();
+    return rc;
+}
+
+void nnm_tune_opts_default(nnm_tune_opts* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->target_recall = 0.95f;
+    o->margin = 0.005f;
+    o->sample_rows = 200000;
+    o->eval_rows = 1000;
+    o->repeats = 2;
+}
+
+int nnm_autotune_merge_leaves(nnm_ctx* ctx, const float* x_dev, uint64_t n, uint32_t d, uint32_t k,
+                              const uint32_t* leaf_sizes, uint32_t nleaf, const nnm_opts* base,
+                              const nnm_tune_opts* topts, nnm_opts* tuned, nnm_tune_result* result) {
+    if (!ctx || !x_dev || !leaf_sizes || !tuned || nleaf < 2 || n < 2 || d == 0 || d > 512 || k < 10)
+        return ctx ? fail(ctx, NNM_ERR_INVALID, "autotune: bad arguments (k >= 10, d <= 512)") : NNM_ERR_INVALID;
+    nnm_opts b;
+    if (base) b = *base;
+    else nnm_opts_default(&b);
+    nnm_tune_opts t;
+    if (topts) t = *topts;
+    else nnm_tune_opts_default(&t);
+    if (t.repeats == 0) t.repeats = 1;
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    // the sample: the first ns rows, leaves scaled to it
+    const uint32_t ns = (uint32_t)std::min<uint64_t>(n, std::max<uint32_t>(t.sample_rows, 1000));
+    std::vector<uint32_t> ls(nleaf);
+    uint64_t acc = 0, tot = 0;
+    for (uint32_t l = 0; l < nleaf; l++) tot += leaf_sizes[l];
+    if (tot != n) return fail(ctx, NNM_ERR_INVALID, "leaf sizes must sum to n");
+    for (uint32_t l = 0; l < nleaf; l++) {
+        acc += leaf_sizes[l];
+        ls[l] = (uint32_t)(acc * ns / n);
+    }
+    for (uint32_t l = nleaf - 1; l > 0; l--) ls[l] -= ls[l - 1];
+    for (uint32_t l = 0; l < nleaf; l++)
+        if (ls[l] < k + 2) return fail(ctx, NNM_ERR_INVALID, "autotune: a sampled leaf is too small");
+    const uint32_t ne = std::min(t.eval_rows, ns);
+    std::vector<uint32_t> rows(ne);
+    {
+        // seeded distinct rows: a stride walk from a seeded start
+        std::mt19937 rng(b.seed + 77u);
+        const uint64_t step = ns / ne, start = rng() % std::max<uint64_t>(step, 1);
+        for (uint32_t i = 0; i < ne; i++) rows[i] = (uint32_t)(start + (uint64_t)i * step);
+    }
+    nnm::DevBuf ib, rb, xp;
+    auto done = [&](int rc) {
+        ib.release();
+        rb.release();
+        xp.release();
+        return rc;
+    };
+    const uint32_t dp = (d + 3) & ~3u;
+    if (ib.ensure((size_t)ns * k * 4) != cudaSuccess || rb.ensure((size_t)ne * 4) != cudaSuccess ||
+        (dp != d && xp.ensure((size_t)ns * dp * 4) != cudaSuccess))
+        return done(fail(ctx, NNM_ERR_OOM, "device allocation failed"));
+    if (cudaMemcpy(rb.p, rows.data(), (size_t)ne * 4, cudaMemcpyHostToDevice) != cudaSuccess) return done(NNM_ERR_CUDA);
+    const float* xe = x_dev;
+    if (dp != d) {
+        if (cudaMemset2D(xp.p, dp * 4, 0, dp * 4, ns) != cudaSuccess ||
+            cudaMemcpy2D(xp.p, dp * 4, x_dev, d * 4, d * 4, ns, cudaMemcpyDeviceToDevice) != cudaSuccess)
+            return done(NNM_ERR_CUDA);
+        xe = xp.as<float>();
+    }
+    // the reference's cap (100) and convergence threshold (0.002) first
+    static const uint32_t caps[] = {100, 88, 76, 64, 48};
+    static const float deltas[] = {0.002f, 0.008f, 0.016f};
+    nnm_tune_result res;
+    std::memset(&res, 0, sizeof(res));
+    int best = -1, best_rec = 0;
+    for (uint32_t cap : caps)
+        for (float dl : deltas) {
+            nnm_opts o = b;
+            o.sample_cap = cap;
+            o.delta = dl;
+            double ms = 1e30;
+            for (uint32_t r = 0; r < t.repeats; r++) {
+                nnm_stats stt;
+                int rc = nnm_merge_leaves_dev(ctx, x_dev, ns, d, k, ls.data(), nleaf, &o, ib.as<uint32_t>(), nullptr,
+                                              nullptr, &stt);
+                if (rc) return done(rc);
+                ms = std::min(ms, stt.device_ms);
+            }
+            double rec = 0.0;
+            int rc = nnm::graph_recall_dev(c, xe, ns, dp, (int)o.metric, ib.as<uint32_t>(), k, rb.as<uint32_t>(), ne,
+                                           10, &rec);
+            if (rc) return done(rc);
+            const uint32_t i = res.ntrials++;
+            res.trials[i] = nnm_tune_trial{cap, dl, (float)rec, ms};
+            if (rec >= (double)(t.target_recall + t.margin) && (best < 0 || ms < res.trials[best].ms)) best = (int)i;
+            if (rec > res.trials[best_rec].recall) best_rec = (int)i;
+        }
+    res.chosen = best >= 0 ? (uint32_t)best : (uint32_t)best_rec;
+    *tuned = b;
+    tuned->sample_cap = res.trials[res.chosen].sample_cap;
+    tuned->delta = res.trials[res.chosen].delta;
+    if (result) *result = res;
+    return done(0);
 }
 
 int nnm_index_create(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, const nnm_layers* layers, uint32_t seed,

@@ -94,6 +94,20 @@ def _entry_struct(m):
                     m["b1"].ctypes.data, m["w2"].ctypes.data, m["b2"].ctypes.data)
 
 
+class TuneOpts(ctypes.Structure):
+    _fields_ = [("target_recall", ctypes.c_float), ("margin", ctypes.c_float), ("sample_rows", ctypes.c_uint32),
+                ("eval_rows", ctypes.c_uint32), ("repeats", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 7)]
+
+
+class TuneTrial(ctypes.Structure):
+    _fields_ = [("sample_cap", ctypes.c_uint32), ("delta", ctypes.c_float), ("recall", ctypes.c_float),
+                ("ms", ctypes.c_double)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("ntrials", ctypes.c_uint32), ("chosen", ctypes.c_uint32), ("trials", TuneTrial * 32)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("ncmps", ctypes.c_uint64), ("sub_ncmps", ctypes.c_uint64), ("iterations", ctypes.c_uint32),
                 ("n_trace", ctypes.c_uint32), ("trace", ctypes.c_float * 256), ("device_ms", ctypes.c_double)]
@@ -136,6 +150,9 @@ def load():
         lib.nnm_mlp_grad.argtypes = [vp, vp, vp, u64, u32, vp, u32, ctypes.c_float, vp, vp]
         lib.nnm_mlp_codes.argtypes = [vp, vp, vp, u64, u32, vp, vp]
         lib.nnm_set_init_model.argtypes = [vp, vp]
+        lib.nnm_graph_recall.argtypes = [vp, vp, u64, u32, vp, u32, vp, u32, u32, vp]
+        lib.nnm_tune_opts_default.argtypes = [vp]
+        lib.nnm_autotune_merge_leaves.argtypes = [vp, vp, u64, u32, u32, vp, u32, vp, vp, vp, vp]
         lib.nnm_index_create.argtypes = [vp, vp, u64, u32, vp, u32, u32, ctypes.POINTER(ctypes.c_void_p)]
         lib.nnm_index_free.argtypes = [vp]
         for name in ("nnm_index_search", "nnm_index_search_dev"):
@@ -349,6 +366,38 @@ class Context:
         self._check(self.lib.nnm_search(self.h, _ptr(x), x.shape[0], x.shape[1], ctypes.byref(lay), _ptr(q), nq,
                                         topk, ctypes.byref(o), _ptr(ids), _ptr(ds), ctypes.byref(nc)))
         return dict(ids=ids, dists=ds, ncmps=int(nc.value))
+
+    # -- evaluation and tuning -----------------------------------------------
+    def graph_recall(self, x, ids, rows, atop=10):
+        """Recall@atop of the graph `ids` (n x k) on the listed rows against
+        exact brute force on the device (ties at the atop-th distance count)."""
+        x = np.ascontiguousarray(x, np.float32)
+        ids = np.ascontiguousarray(ids, np.uint32)
+        rows = np.ascontiguousarray(rows, np.uint32)
+        r = ctypes.c_double()
+        self._check(self.lib.nnm_graph_recall(self.h, _ptr(x), x.shape[0], x.shape[1], _ptr(ids), ids.shape[1],
+                                              _ptr(rows), len(rows), atop, ctypes.byref(r)))
+        return float(r.value)
+
+    def autotune_merge_leaves_dev(self, x_ptr, n, d, k, leaf_sizes, target_recall=0.95, margin=0.005,
+                                  sample_rows=200_000, eval_rows=1000, repeats=2, **kw):
+        """Chooses sample_cap and delta for nnm_merge_leaves_dev on the
+        device-resident x; returns (options for merge_leaves*, trials)."""
+        sizes = np.ascontiguousarray(leaf_sizes, np.uint32)
+        o = make_opts(**kw)
+        t = TuneOpts()
+        self.lib.nnm_tune_opts_default(ctypes.byref(t))
+        t.target_recall, t.margin, t.sample_rows, t.eval_rows, t.repeats = (target_recall, margin, sample_rows,
+                                                                           eval_rows, repeats)
+        tuned = Opts()
+        res = TuneResult()
+        self._check(self.lib.nnm_autotune_merge_leaves(self.h, ctypes.c_void_p(x_ptr), n, d, k, _ptr(sizes),
+                                                       len(sizes), ctypes.byref(o), ctypes.byref(t),
+                                                       ctypes.byref(tuned), ctypes.byref(res)))
+        trials = [dict(sample_cap=int(res.trials[i].sample_cap), delta=float(res.trials[i].delta),
+                       recall=float(res.trials[i].recall), ms=float(res.trials[i].ms)) for i in range(res.ntrials)]
+        chosen = trials[res.chosen]
+        return dict(sample_cap=chosen["sample_cap"], delta=chosen["delta"]), trials
 
     # -- serving ------------------------------------------------------------
     def index(self, x, layers, seed=0, metric="l2"):
