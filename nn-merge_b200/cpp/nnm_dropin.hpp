@@ -344,17 +344,23 @@ protected:
         }
     }
 
-public:
-    LySearch(const char *Rsrc, const char *Gsrc, SpaceInterface<float> *func) : metric(func->nnm_metric()) {
-        mat = nnm_dropin::load_refSet(Rsrc, col, row);
-        loadGraphs(Gsrc);
+    nnm_index *ix_ = nullptr;
+
+    // The data set and hierarchy go to the device once (nnm_index_create);
+    // the clock value seeds the entry point, as knnSearch's rand() does.
+    nnm_index *index() {
+        if (!ix_) {
+            nnm_opts o = nnm_dropin::opts(metric);
+            nnm_dropin::check(nnm_index_create(nnm_dropin::context(), mat, row, col, &layers, o.seed, o.metric, &ix_));
+        }
+        return ix_;
     }
-    virtual ~LySearch() { delete[] mat; }
-    // knnSearch (lysearch.cpp:363-437): beams 60 .. 2; writes "query id dist"
-    // of each query's nearest result to dstFn and "beam recall time
-    // distances/query" lines to record; recall@1 against grdFn ("query id"
-    // pairs) when it can be read.
-    int knnSearch(const char *qryFn, const char *dstFn, const char *grdFn, const char *record) {
+
+    // The sweep both searches share (lysearch.cpp:380-436, :530-561): beam
+    // widths 60 .. 2; "query id dist" of each query's nearest result to
+    // dstFn, "beam recall time distances/query" lines to record; recall@1
+    // against grdFn ("query id" pairs) when it can be read.
+    int sweep(const char *qryFn, const char *dstFn, const char *grdFn, const char *record, uint32_t entry) {
         unsigned qd = 0, nq = 0;
         float *q = nnm_dropin::load_refSet(qryFn, qd, nq);
         if (qd != col) {
@@ -369,15 +375,14 @@ public:
         }
         std::ofstream rec(record);
         static const unsigned beams[17] = {60, 50, 40, 36, 32, 28, 24, 20, 18, 15, 14, 12, 10, 8, 6, 4, 2};
-        nnm_opts o = nnm_dropin::opts(metric);
         for (unsigned t = 0; t < 17; t++) {
             const unsigned topk = beams[t];
             std::vector<uint32_t> ids((size_t)nq * topk);
             std::vector<float> ds((size_t)nq * topk);
-            uint64_t ncmps = 0;
+            nnm_search_stats st;
             auto t0 = std::chrono::steady_clock::now();
-            nnm_dropin::check(nnm_search(nnm_dropin::context(), mat, row, col, &layers, q, nq, topk, &o, ids.data(),
-                                         ds.data(), &ncmps));
+            nnm_dropin::check(nnm_index_search(index(), q, nq, nullptr, topk, topk, NNM_SERVE_EXACT, entry,
+                                               ids.data(), ds.data(), &st));
             double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             std::ofstream out(dstFn);
             unsigned hits = 0;
@@ -387,12 +392,33 @@ public:
                 if (it != grd.end() && it->second == ids[(size_t)i * topk]) hits++;
             }
             float r = grd.empty() ? 0.f : (float)hits / (float)grd.size();
-            std::cout << "Top-1 : " << r << "\t" << ncmps / nq << "\t" << secs << std::endl;
-            rec << topk << "\t" << r << "\t" << secs << "\t" << ncmps / nq << std::endl;
+            const uint64_t per_q = nq ? st.ncmps / nq : 0;
+            std::cout << "Top-1 : " << r << "\t" << per_q << "\t" << secs << std::endl;
+            rec << topk << "\t" << r << "\t" << secs << "\t" << per_q << std::endl;
             if (r == 1) break;
         }
         delete[] q;
         return 0;
+    }
+
+public:
+    LySearch(const char *Rsrc, const char *Gsrc, SpaceInterface<float> *func) : metric(func->nnm_metric()) {
+        mat = nnm_dropin::load_refSet(Rsrc, col, row);
+        loadGraphs(Gsrc);
+    }
+    virtual ~LySearch() {
+        if (ix_) nnm_index_free(ix_);
+        delete[] mat;
+    }
+    // knnSearch (lysearch.cpp:363-437): one global entry, greedy descent
+    // through the upper layers, best-first beam on the last.
+    int knnSearch(const char *qryFn, const char *dstFn, const char *grdFn, const char *record) {
+        return sweep(qryFn, dstFn, grdFn, record, NNM_ENTRY_DEFAULT);
+    }
+    // singleknnSearch (lysearch.cpp:522-561) with nndFlatSrch (:439-520):
+    // the beam starts from `beam` random rows of the last layer.
+    int singleknnSearch(const char *qryFn, const char *dstFn, const char *grdFn, const char *record) {
+        return sweep(qryFn, dstFn, grdFn, record, NNM_ENTRY_FLAT);
     }
 };
 

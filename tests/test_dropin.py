@@ -57,3 +57,30 @@ def test_dropin_matches_oracle(oracle, cmd):
         got = read_knn(dst)
     exp = getattr(oracle, cmd)(x, 20, 4242)
     assert np.array_equal(got, exp["ids"])
+
+
+@needs_gxx
+@pytest.mark.gpu
+@pytest.mark.parametrize("cmd", ["search", "flatsearch"])
+def test_dropin_search_matches_oracle(oracle, cmd):
+    """LyNNDescent::buildhgraph then LySearch::knnSearch / singleknnSearch
+    through the drop-in classes: the last beam of the sweep (2, with no
+    ground truth) against the oracle's search at that beam."""
+    from nnm.datasets import queries_like
+    x = gaussian_mixture_u8(34000, d=16, seed=9)
+    q = queries_like(300, d=16, seed=9, query_seed=4)
+    with tempfile.TemporaryDirectory() as td:
+        exe = build(td)
+        src, qp = os.path.join(td, "x.fvecs"), os.path.join(td, "q.fvecs")
+        write_fvecs(src, x)
+        write_fvecs(qp, q)
+        env = dict(os.environ, NNM_SEED="77")
+        pre = os.path.join(td, "h")
+        subprocess.run([exe, "hmerge", src, "10", "10", pre], check=True, env=env, capture_output=True)
+        out, rec = os.path.join(td, "s.txt"), os.path.join(td, "r.txt")
+        subprocess.run([exe, cmd, src, pre + ".txt", qp, out, rec], check=True, env=env, capture_output=True)
+        got = np.array([int(l.split()[1]) for l in open(out).read().strip().split("\n")], np.uint32)
+        assert len(open(rec).read().strip().split("\n")) == 17
+    h = oracle.hmerge(x, 10, 10, 77)
+    exp = oracle.search_ex(x, h["layers"], q, 2, 77, beam=2, flat=(cmd == "flatsearch"))
+    assert np.array_equal(got, exp["ids"][:, 0])
