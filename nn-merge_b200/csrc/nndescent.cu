@@ -234,6 +234,7 @@ struct ShufArgs {
     IterCounters* ctr;
     uint32_t fast, seed, phase;  // fast tier: Philox sample instead of std::random_shuffle
     uint32_t tc_max_s;    // rows with S up to this go to the tensor-core join (no stored pairs)
+    int max_staged;       // highest FP32 tier whose vectors fit in shared memory (-1: none); larger lists go unstaged
 };
 
 __global__ void k_rand_count(const uint64_t* roff_new, const uint64_t* roff_old, uint32_t n, uint32_t* out) {
@@ -395,7 +396,8 @@ __global__ void k_shuffle_append(ShufArgs a) {
         const uint32_t S = nl + ol;
         a.npairs[t] = nl && S > a.tc_max_s ? nl * (nl - 1) / 2 + nl * ol : 0u;
         if (nl) {
-            const int tier = tier_of(S);
+            int tier = tier_of(S);
+            if (tier < NTIER - 1 && S > a.tc_max_s && tier > a.max_staged) tier = NTIER - 1;
             a.tier_rows[(size_t)tier * a.n + atomicAdd(&a.ctr->ntier[tier], 1u)] = t;
         }
     }
@@ -858,17 +860,28 @@ static size_t pairs_smem(uint32_t R, uint32_t dp, bool staged) {
     return (size_t)R * 16 + (staged ? ((size_t)R * vstride + R / 4 + 1) * 16 : 0) + 64;
 }
 
+// Highest list-size tier whose staged vectors fit in a CTA's shared memory
+// at this dimension (3: all; lower at large d, -1 for none -- those rows
+// take the unstaged kernel of the last tier, with the same sums).
+static int max_staged_tier(uint32_t dp, int device) {
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    int t = 0;
+    while (t < NTIER - 1 && pairs_smem(TIER_CAP[t], dp, true) <= (size_t)optin) t++;
+    return t - 1;
+}
+
 template <int M>
-static cudaError_t prep_pairs(uint32_t caps, uint32_t dp, size_t emit_smem) {
+static cudaError_t prep_pairs(uint32_t caps, uint32_t dp, size_t emit_smem, int max_staged) {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_pairs<M, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)pairs_smem(TIER_CAP[0], dp, true))) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_pairs<M, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)pairs_smem(TIER_CAP[1], dp, true))) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_pairs<M, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)pairs_smem(TIER_CAP[2], dp, true))) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_pairs<M, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)pairs_smem(TIER_CAP[3], dp, true))) != cudaSuccess) return e;
+    if (max_staged >= 0 && (e = cudaFuncSetAttribute(k_pairs<M, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)pairs_smem(TIER_CAP[0], dp, true))) != cudaSuccess) return e;
+    if (max_staged >= 1 && (e = cudaFuncSetAttribute(k_pairs<M, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)pairs_smem(TIER_CAP[1], dp, true))) != cudaSuccess) return e;
+    if (max_staged >= 2 && (e = cudaFuncSetAttribute(k_pairs<M, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)pairs_smem(TIER_CAP[2], dp, true))) != cudaSuccess) return e;
+    if (max_staged >= 3 && (e = cudaFuncSetAttribute(k_pairs<M, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)pairs_smem(TIER_CAP[3], dp, true))) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_pairs<M, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)pairs_smem(caps, dp, false))) != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)emit_smem);
@@ -939,9 +952,10 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     IterCounters* ctr = P<IterCounters>(ws.counters);
 
     const size_t emit_smem = (size_t)EMIT_WARPS * caps * 24 + 64;
-    cudaError_t ae = g.metric == L2 ? prep_pairs<L2>(caps, g.dp, emit_smem)
-                     : g.metric == L1 ? prep_pairs<L1>(caps, g.dp, emit_smem)
-                                      : prep_pairs<CHI2>(caps, g.dp, emit_smem);
+    const int max_staged = max_staged_tier(g.dp, ctx.device);
+    cudaError_t ae = g.metric == L2 ? prep_pairs<L2>(caps, g.dp, emit_smem, max_staged)
+                     : g.metric == L1 ? prep_pairs<L1>(caps, g.dp, emit_smem, max_staged)
+                                      : prep_pairs<CHI2>(caps, g.dp, emit_smem, max_staged);
     NNM_CUDA_TRY(ae);
     NNM_CUDA_TRY(ws.npairs.ensure(n1 * 4));
     NNM_CUDA_TRY(ws.poff.ensure(n1 * 8));
@@ -1004,7 +1018,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
                     track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
                     P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, g.phase++,
-                    tc ? TC_MAX_S : 0u};
+                    tc ? TC_MAX_S : 0u, max_staged};
         k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh); count_launch();
         NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.npairs), P<uint64_t>(ws.poff), n, scan_tmp,
                                     reinterpret_cast<uint64_t*>(&ctr->pairs), st));

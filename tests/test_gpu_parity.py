@@ -125,3 +125,13 @@ def test_cuda_matches_golden(ctx, name):
             assert np.array_equal(s["ids"], fx["search%d_ids" % topk])
             assert np.array_equal(s["dists"], fx["search%d_dists" % topk])
             assert s["ncmps"] == int(fx["search%d_ncmps" % topk])
+
+
+@pytest.mark.parametrize("join", ["fp32", "auto"])
+def test_kgraph_wide_vectors(ctx, oracle, join):
+    """d = 600: the staged FP32 join kernels do not fit shared memory for the
+    larger list sizes, whose rows take the unstaged kernel -- same sums."""
+    x = gaussian_mixture_u8(1200, d=600, seed=81)
+    exp = oracle.kgraph(x, 16, 9)
+    got = ctx.kgraph(x, 16, seed=9, exact_trace=True, join=join)
+    assert_same_graph(got, exp)

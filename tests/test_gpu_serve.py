@@ -286,3 +286,97 @@ def test_learned_entries_in_fast_search(hier, index, trained):
     assert rl >= rd - 0.005
     assert lr["ncmps"] < df["ncmps"]
     assert lr["predict_ms"] > 0
+
+
+# ---- edge cases of the serving kernels -------------------------------------
+
+def small_index(ctx, n, d, metric="l2", seed=1):
+    x = gaussian_mixture_u8(n, d=d, seed=seed)
+    h = ctx.hmerge(x, 10, 10, seed=3, metric=metric)
+    return x, h["layers"], ctx.index(x, h["layers"], seed=5, metric=metric)
+
+
+def exact_dist(x, q, ids, metric):
+    a = q[:, None, :].astype(np.float64)
+    b = x[ids.astype(np.int64)].astype(np.float64)
+    if metric == "l2":
+        return ((a - b) ** 2).sum(-1)
+    if metric == "l1":
+        return np.abs(a - b).sum(-1)
+    s = a + b
+    return np.where(s != 0, (a - b) ** 2 / np.where(s != 0, s, 1), 0).sum(-1)
+
+
+def test_empty_batch(ctx):
+    _, _, ix = small_index(ctx, 3000, 16)
+    try:
+        r = ix.search(np.zeros((0, 16), np.float32), out_k=10, beam=32)
+        assert r["ids"].shape == (0, 10) and r["ncmps"] == 0
+    finally:
+        ix.close()
+
+
+@pytest.mark.parametrize("d", [1, 13, 200, 512])
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_dimensions(ctx, oracle, d, mode):
+    x, layers, ix = small_index(ctx, 3000, d, seed=d)
+    try:
+        q = gaussian_mixture_u8(50, d=d, seed=d + 1)
+        r = ix.search(q, out_k=5, beam=24, mode=mode)
+        ids = r["ids"]
+        assert (ids < 3000).all() and (np.diff(r["dists"], axis=1) >= 0).all()
+        ref = exact_dist(x, q, ids, "l2")
+        assert np.abs(ref - r["dists"]).max() <= 1e-5 * max(ref.max(), 1.0)
+        if mode == "exact":
+            e = oracle.search_ex(x, layers, q, 5, 5, beam=24)
+            assert np.array_equal(ids, e["ids"])
+    finally:
+        ix.close()
+
+
+@pytest.mark.parametrize("metric", ["l1", "chi2"])
+def test_fast_kernel_other_metrics(ctx, oracle, metric):
+    x, layers, ix = small_index(ctx, 4000, 32, metric=metric, seed=11)
+    try:
+        q = gaussian_mixture_u8(200, d=32, seed=12)
+        f = ix.search(q, out_k=10, beam=64, mode="fast")
+        e = ix.search(q, out_k=10, beam=64, mode="exact")
+        o = oracle.search_ex(x, layers, q, 10, 5, beam=64, metric=metric)
+        assert np.array_equal(e["ids"], o["ids"])
+        ref = exact_dist(x, q, f["ids"], metric)
+        assert np.abs(ref - f["dists"]).max() <= 1e-5 * ref.max()
+        # the fast kernel finds (nearly) the exact kernel's results
+        same = np.mean([len(set(a) & set(b)) / 10 for a, b in zip(f["ids"], e["ids"])])
+        assert same >= 0.95, same
+    finally:
+        ix.close()
+
+
+def test_widest_beam(ctx, oracle):
+    x, layers, ix = small_index(ctx, 3000, 16, seed=13)
+    try:
+        q = gaussian_mixture_u8(40, d=16, seed=14)
+        for mode in ("exact", "fast"):
+            r = ix.search(q, out_k=16, beam=1024, mode=mode)
+            ref = exact_dist(x, q, np.arange(3000)[None, :].repeat(40, 0), "l2")
+            kth = np.sort(ref, axis=1)[:, 15:16]
+            # a 1024-wide beam over 3,000 rows finds the exact 16 nearest
+            assert (exact_dist(x, q, r["ids"], "l2") <= kth).mean() >= 0.99, mode
+        e = oracle.search_ex(x, layers, q, 16, 5, beam=1024)
+        assert np.array_equal(ix.search(q, out_k=16, beam=1024, mode="exact")["ids"], e["ids"])
+        with pytest.raises(NnmError):
+            ix.search(q, out_k=16, beam=1025, mode="fast")
+    finally:
+        ix.close()
+
+
+def test_out_k_equal_to_small_beams(ctx):
+    _, _, ix = small_index(ctx, 2000, 16, seed=15)
+    try:
+        q = gaussian_mixture_u8(30, d=16, seed=16)
+        beams = np.full(30, 10, np.uint32)
+        for mode in ("exact", "fast"):
+            r = ix.search(q, out_k=10, beams=beams, mode=mode)
+            assert (r["ids"] != 0xFFFFFFFF).all()
+    finally:
+        ix.close()
