@@ -235,6 +235,8 @@ struct ShufArgs {
     uint32_t fast, seed, phase;  // fast tier: Philox sample instead of std::random_shuffle
     uint32_t tc_max_s;    // rows with S up to this go to the tensor-core join (no stored pairs)
     int max_staged;       // highest FP32 tier whose vectors fit in shared memory (-1: none); larger lists go unstaged
+    uint32_t *rscr_new, *rscr_old;  // scratch of the reverse lists' sizes (fast tier: duplicate removal)
+    uint32_t dedupe;      // fast tier, first iteration of an H-Merge level: carried + new lists may repeat ids
 };
 
 __global__ void k_rand_count(const uint64_t* roff_new, const uint64_t* roff_old, uint32_t n, uint32_t* out) {
@@ -339,6 +341,36 @@ __device__ void hash_sample(uint32_t* seg, uint32_t len, uint32_t keep, const Ph
     }
 }
 
+// Removes repeated ids from seg[0, len): an id's copies keep the larger word
+// (a set group bit wins), identical copies the first; the kept entries go to
+// scr in list order and back to seg.  The kept set does not depend on the
+// order of the list (which, in the fast tier, is the order of atomics), so
+// the hash sample after it is deterministic.  Returns the new length.
+__device__ uint32_t dedupe_ids(uint32_t* seg, uint32_t len, uint32_t* scr) {
+    const int lane = threadIdx.x & 31;
+    uint32_t out = 0;
+    for (uint32_t j0 = 0; j0 < len; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        bool keep = false;
+        uint32_t v = 0;
+        if (j < len) {
+            v = seg[j];
+            keep = true;
+            for (uint32_t i = 0; i < len && keep; i++) {
+                const uint32_t u = seg[i];
+                if (i != j && (u & LID_MASK) == (v & LID_MASK) && (u > v || (u == v && i < j))) keep = false;
+            }
+        }
+        const unsigned m = __ballot_sync(FULL, keep);
+        if (keep) scr[out + __popc(m & ((1u << lane) - 1u))] = v;
+        out += __popc(m);
+    }
+    __syncwarp();
+    for (uint32_t j = lane; j < out; j += 32) seg[j] = scr[j];
+    __syncwarp();
+    return out;
+}
+
 // One warp per row: lane 0 shuffles in shared memory, the warp appends.
 __global__ void k_shuffle_append(ShufArgs a) {
     __shared__ uint32_t stage[8][SHUF_SMEM];
@@ -352,6 +384,7 @@ __global__ void k_shuffle_append(ShufArgs a) {
         uint64_t lo = l ? a.roff_old[t] : a.roff_new[t];
         uint32_t len = (uint32_t)((l ? a.roff_old[t + 1] : a.roff_new[t + 1]) - lo);
         uint32_t* seg = (l ? a.rseg_old : a.rseg_new) + lo;
+        if (a.dedupe && len > 1) len = dedupe_ids(seg, len, (l ? a.rscr_old : a.rscr_new) + lo);
         uint32_t keep = min(len, a.smpl);
         uint32_t* sh = stage[w];
         bool staged = len <= SHUF_SMEM;
@@ -1018,7 +1051,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
                     track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
                     P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, g.phase++,
-                    tc ? TC_MAX_S : 0u, max_staged};
+                    tc ? TC_MAX_S : 0u, max_staged, rscr_new, rscr_old, (g.fast && carry_now) ? 1u : 0u};
         k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh); count_launch();
         NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.npairs), P<uint64_t>(ws.poff), n, scan_tmp,
                                     reinterpret_cast<uint64_t*>(&ctr->pairs), st));

@@ -42,6 +42,8 @@ constexpr uint32_t FVCAP = 65536;        // visited ids recorded per warp slot
 constexpr uint32_t EXP_BIT = 1u << 31;   // beam entry already expanded
 constexpr uint32_t IDM = 0x7fffffffu;
 constexpr uint32_t FAST_MAX_DP = 512;    // 4 float4 per lane
+constexpr uint32_t GROUP = 4;            // 32-id chunks of a step whose loads and atomics overlap
+constexpr uint32_t WARP_EXTRA = 256 + GROUP * 32 * 4;  // nd, ni and fr after the two beam arrays
 
 // self-check codes, shared with the exact kernel's report
 enum : unsigned { FERR_LOOP = 4u, FERR_BAD_ID = 8u, FERR_BEAM_RANGE = 32u };
@@ -213,13 +215,14 @@ __global__ void __launch_bounds__(FW * 32) k_serve(ServeArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t slot = blockIdx.x * FW + w;
-    unsigned char* base = smem + (size_t)w * ((size_t)a.cap * 16 + 256);
+    unsigned char* base = smem + (size_t)w * ((size_t)a.cap * 16 + WARP_EXTRA);
     float* bd = reinterpret_cast<float*>(base);
     uint32_t* bi = reinterpret_cast<uint32_t*>(bd + a.cap);
     float* td = reinterpret_cast<float*>(bi + a.cap);
     uint32_t* ti = reinterpret_cast<uint32_t*>(td + a.cap);
     float* nd = reinterpret_cast<float*>(ti + a.cap);
     uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 32);
+    uint32_t* fr = ni + 32;  // fresh ids of one group of a step
     uint32_t* vis = a.visited + (size_t)slot * a.words;
     uint32_t* vl = a.vlist + (size_t)slot * FVCAP;
     const float4* x4 = reinterpret_cast<const float4*>(a.x);
@@ -438,30 +441,49 @@ __global__ void __launch_bounds__(FW * 32) k_serve(ServeArgs a) {
             const uint64_t base_l = lb - (pre - len);  // list e: adjacency index base_e + t
             const uint64_t base0 = __shfl_sync(FULL, base_l, 0), base1 = __shfl_sync(FULL, base_l, 1),
                            base2 = __shfl_sync(FULL, base_l, 2), base3 = __shfl_sync(FULL, base_l, 3);
-            for (uint32_t t0 = 0; t0 < total; t0 += 32) {
-                const uint32_t t = t0 + lane;
-                bool fresh = false;
-                uint32_t nn = 0;
-                if (t < total) {
-                    const uint64_t bs = t < end0 ? base0 : (t < end1 ? base1 : (t < end2 ? base2 : base3));
-                    nn = a.adj_all[bs + t];
-                    const uint32_t old = atomicOr(&vis[nn >> 5], 1u << (nn & 31));
-                    fresh = !(old & (1u << (nn & 31)));
+            // the step's ids GROUP x 32 at a time: every list load, then every
+            // visited-bit atomic, is in flight at once; the fresh ids are
+            // gathered in list order and offered 32 at a time (the beam after
+            // a step is the best of the union whatever the order of offers)
+            for (uint32_t t0 = 0; t0 < total; t0 += 32 * GROUP) {
+                uint32_t nn[GROUP];
+                bool fresh[GROUP];
+#pragma unroll
+                for (uint32_t c = 0; c < GROUP; c++) {
+                    const uint32_t t = t0 + 32 * c + lane;
+                    nn[c] = 0;
+                    if (t < total) {
+                        const uint64_t bs = t < end0 ? base0 : (t < end1 ? base1 : (t < end2 ? base2 : base3));
+                        nn[c] = a.adj_all[bs + t];
+                    }
                 }
-                const unsigned fb = __ballot_sync(FULL, fresh);
-                const uint32_t nf = __popc(fb);
-                if (nf == 0) continue;
-                __syncwarp();
-                if (fresh) {
-                    const uint32_t r = __popc(fb & ((1u << lane) - 1u));
-                    ni[r] = nn;
-                    if (nvis + r < FVCAP) vl[nvis + r] = nn;
+#pragma unroll
+                for (uint32_t c = 0; c < GROUP; c++) {
+                    fresh[c] = false;
+                    if (t0 + 32 * c + lane < total) {
+                        const uint32_t old = atomicOr(&vis[nn[c] >> 5], 1u << (nn[c] & 31));
+                        fresh[c] = !(old & (1u << (nn[c] & 31)));
+                    }
                 }
-                __syncwarp();
-                const uint32_t fid = lane < nf ? ni[lane] : 0u;
+                uint32_t nf = 0;
+                __syncwarp();  // the last offer() has finished with fr
+#pragma unroll
+                for (uint32_t c = 0; c < GROUP; c++) {
+                    const unsigned fb = __ballot_sync(FULL, fresh[c]);
+                    if (fresh[c]) {
+                        const uint32_t r = nf + __popc(fb & ((1u << lane) - 1u));
+                        fr[r] = nn[c];
+                        if (nvis + r < FVCAP) vl[nvis + r] = nn[c];
+                    }
+                    nf += __popc(fb);
+                }
                 nvis += nf;
-                __syncwarp();  // every lane has read its id before offer() reuses ni
-                offer(fid, nf);
+                __syncwarp();
+                for (uint32_t f0 = 0; f0 < nf; f0 += 32) {
+                    const uint32_t cnt = min(32u, nf - f0);
+                    const uint32_t fid = lane < cnt ? fr[f0 + lane] : 0u;
+                    offer(fid, cnt);
+                }
             }
         }
         // results: the first out_k entries
@@ -504,7 +526,7 @@ int index_run_fast(Ctx& ctx, IndexDev& ix, const SearchReq& r) {
     const uint32_t dp4 = ix.dp / 4;
     const uint32_t qv = dp4 <= 32 ? 1 : (dp4 <= 64 ? 2 : 4);
     const ServeFn fn = ix.metric == L2 ? pick_qv<L2>(qv) : (ix.metric == L1 ? pick_qv<L1>(qv) : pick_qv<CHI2>(qv));
-    const size_t smem = (size_t)FW * ((size_t)r.beam_max * 16 + 256);
+    const size_t smem = (size_t)FW * ((size_t)r.beam_max * 16 + WARP_EXTRA);
     NNM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int nsm = 148, per_sm = 1;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx.device);

@@ -60,3 +60,14 @@ def test_fast_tier_hmerge_layers(ctx):
     g = ctx.hmerge(x, 16, 16, seed=2, rng="fast")
     check_pools(x, g)
     assert [len(o) - 1 for o, _ in g["layers"]] == [64, 512, 4096, 5000]
+
+
+@pytest.mark.parametrize("join", ["fp32", "tensor"])
+def test_hmerge_fast_is_deterministic(ctx, join):
+    x = gaussian_mixture_u8(40_000, n_centres=64, seed=91)
+    a = ctx.hmerge(x, 20, 20, seed=3, rng="fast", join=join)
+    b = ctx.hmerge(x, 20, 20, seed=3, rng="fast", join=join)
+    diff = [g for g, ((ao, aa), (bo, ba)) in enumerate(zip(a["layers"], b["layers"]))
+            if not (np.array_equal(ao, bo) and np.array_equal(aa, ba))]
+    assert np.array_equal(a["ids"], b["ids"]) and np.array_equal(a["dists"], b["dists"]), "pools differ"
+    assert not diff, "layers differ: %s" % diff
