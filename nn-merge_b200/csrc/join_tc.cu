@@ -368,13 +368,13 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                             if (pa) {
                                 const unsigned long long slot = S.base[av] + base + __popc(m & ((1u << lane) - 1u));
                                 a.bucket[slot] = Prop{
-                                    dd, e_b, prop_key(a.fast_key, row_b, pidx, e_b & LID_MASK, outer == q_a ? 0u : 1u)};
+                                    dd, e_b, prop_key(a.fast_key, row_b, pidx, e_b, outer == q_a ? 0u : 1u)};
                             }
                         }
                         if (ok && dd < kth_b) {
                             const unsigned long long slot = S.base[tid] + atomicAdd(&S.cnt[tid], 1u);
                             a.bucket[slot] = Prop{
-                                dd, e_a, prop_key(a.fast_key, row_b, pidx, e_a & LID_MASK, outer == q_b ? 0u : 1u)};
+                                dd, e_a, prop_key(a.fast_key, row_b, pidx, e_a, outer == q_b ? 0u : 1u)};
                         }
                     }
                 }

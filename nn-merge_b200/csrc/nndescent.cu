@@ -605,11 +605,11 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
             const uint32_t pidx = outer * S + inner;
             if (dd < s_kth[outer]) {
                 unsigned long long slot = s_base[outer] + atomicAdd(&s_cur[outer], 1u);
-                a.bucket[slot] = Prop{dd, s_ids[inner], prop_key(a.fast_key, row, pidx, s_ids[inner] & LID_MASK, 0)};
+                a.bucket[slot] = Prop{dd, s_ids[inner], prop_key(a.fast_key, row, pidx, s_ids[inner], 0)};
             }
             if (dd < s_kth[inner]) {
                 unsigned long long slot = s_base[inner] + atomicAdd(&s_cur[inner], 1u);
-                a.bucket[slot] = Prop{dd, s_ids[outer], prop_key(a.fast_key, row, pidx, s_ids[outer] & LID_MASK, 1)};
+                a.bucket[slot] = Prop{dd, s_ids[outer], prop_key(a.fast_key, row, pidx, s_ids[outer], 1)};
             }
         }
     }

@@ -54,11 +54,17 @@ struct JoinArgs {
 // `row`.  Exact tier: the reference's sequential insert order (the pair's
 // index in join order, then the side: 0 = into the outer element's pool).
 // Fast tier: the other element's id in place of the pair index, so that the
-// graphs do not depend on the order of the sample lists.
+// graphs do not depend on the order of the sample lists, and in place of
+// the side (which a pair listed once does not need) the other list entry's
+// group bit, set first: when a row's lists hold an id twice with different
+// group bits, the two copies' proposals then order by key rather than by
+// their arrival in the bucket, and the merge keeps the first.
 __device__ __forceinline__ unsigned long long prop_key(uint32_t fast, uint32_t row, uint32_t pair_idx,
-                                                       uint32_t other_id, uint32_t side) {
+                                                       uint32_t other_word, uint32_t side) {
+    const uint32_t other_id = other_word & 0x7fffffffu;
+    const uint32_t tie = fast ? ((other_word >> 31) ^ 1u) : side;
     return (1ull << 63) | ((unsigned long long)row << 32) |
-           ((unsigned long long)(fast ? other_id : pair_idx) << 1) | side;
+           ((unsigned long long)(fast ? other_id : pair_idx) << 1) | tie;
 }
 
 __device__ __forceinline__ uint32_t leaf_of(uint32_t id, const uint32_t* off, uint32_t nleaf) {
