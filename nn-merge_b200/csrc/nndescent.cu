@@ -1003,61 +1003,143 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     const unsigned tblocks = (unsigned)((n + 255) / 256);
     std::vector<uint8_t> h_nflag;
 
+    // Fast tier: an iteration's sampling segment -- list clears through the
+    // pair-count scan and the counter read-back -- launches the same kernels
+    // with the same arguments in every iteration but the first of a carried
+    // H-Merge level, except the draw phase of k_shuffle_append.  It is
+    // captured once per call as a CUDA graph and replayed, the phase set on
+    // the instantiated graph's node before each replay.  (The join and the
+    // merge follow host reads of tile, pair and proposal counts.)
+    struct SegGraph {
+        cudaGraph_t graph = nullptr;  // kept while exec lives: its node handle names the node to update
+        cudaGraphExec_t exec = nullptr;
+        cudaGraphNode_t shuf = nullptr;
+        cudaKernelNodeParams kp{};
+        uint64_t launches = 0;
+        bool disabled = false;
+        ~SegGraph() {
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+        }
+    } seg;
     for (uint32_t it = 0;; it++) {
         const bool carry_now = (it == 0) && g.carry && track;
-        if (!carry_now) {
-            k_clear_lists<<<tblocks, 256, 0, st>>>(g.newlen, g.oldlen,
-                                                   track ? g.rnewTlen : nullptr,
-                                                   track ? g.roldTlen : nullptr, n); count_launch();
-        }
-        NNM_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(IterCounters), st));
-        // reverse counts and cursors start at the carried lengths
-        k_set_u32<<<tblocks, 256, 0, st>>>(rcnt_new, track ? g.rnewTlen : nullptr, n); count_launch();
-        k_set_u32<<<tblocks, 256, 0, st>>>(rcnt_old, track ? g.roldTlen : nullptr, n); count_launch();
-        k_set_u32<<<tblocks, 256, 0, st>>>(rcur_new, track ? g.rnewTlen : nullptr, n); count_launch();
-        k_set_u32<<<tblocks, 256, 0, st>>>(rcur_old, track ? g.roldTlen : nullptr, n); count_launch();
-        SampleArgs sa{g.pid, g.pdist, n, K, (uint32_t)mode, split,
-                      rcnt_new, rcnt_old, rcur_new, rcur_old, roff_new, roff_old, rseg_new, rseg_old,
-                      g.newL, g.oldL, g.newlen, g.oldlen,
-                      g.capn, g.capo,
-                      carry_now ? g.rnewT : nullptr, carry_now ? g.roldT : nullptr,
-                      carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr,
-                      g.smpl, ctr};
-        k_sample_count<<<warp_blocks, 256, 0, st>>>(sa); count_launch();
-        NNM_CUDA_TRY(exclusive_scan(rcnt_new, roff_new, n, scan_tmp, nullptr, st));
-        NNM_CUDA_TRY(exclusive_scan(rcnt_old, roff_old, n, scan_tmp, nullptr, st));
-        k_sample_fill<<<warp_blocks, 256, 0, st>>>(sa); count_launch();
-        RevSortArgs ra{{roff_new, roff_old}, {rseg_new, rseg_old}, {rscr_new, rscr_old},
-                       {carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr},
-                       n, P<uint32_t>(ws.bigrev), ctr};
-        // reverse lists in ascending source order, as the reference pushes
-        // them; the fast tier keeps them in the (arbitrary) order the atomics
-        // left: its samples and tie-break keys do not depend on list order
-        if (!g.fast) {
-            k_rev_sort_small<<<dim3(warp_blocks, 2), 256, 0, st>>>(ra); count_launch();
-            k_rev_sort_big<<<nsm * 2, 512, 0, st>>>(ra); count_launch();
-        }
-        if (!g.fast) {
-            // std::rand() draws of this iteration's shuffles
-            k_rand_count<<<tblocks, 256, 0, st>>>(roff_new, roff_old, n, P<uint32_t>(ws.rcount)); count_launch();
-            NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.rcount), P<uint64_t>(ws.rofs), n, scan_tmp, d_tot, st));
-            NNM_CUDA_TRY(glibc_stream_generate(P<int32_t>(ws.rbuf), g.gbase, g.gpos, d_tot, rev_cap * 2, st));
+        const uint32_t phase = g.phase++;
+        auto shuf_args = [&]() {
+            return ShufArgs{roff_new, roff_old, rseg_new, rseg_old, P<uint64_t>(ws.rofs), P<int32_t>(ws.rbuf),
+                            g.newL, g.oldL, g.newlen, g.oldlen,
+                            g.capn, g.capo, n, g.smpl,
+                            track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
+                            track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
+                            P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, phase,
+                            tc ? TC_MAX_S : 0u, max_staged, rscr_new, rscr_old, (g.fast && carry_now) ? 1u : 0u};
+        };
+        // the segment; its first failing call's error is returned
+        auto seg_a = [&]() -> cudaError_t {
+            cudaError_t e = cudaSuccess;
+            auto chk = [&](cudaError_t x) {
+                if (e == cudaSuccess) e = x;
+            };
+            if (!carry_now) {
+                k_clear_lists<<<tblocks, 256, 0, st>>>(g.newlen, g.oldlen,
+                                                       track ? g.rnewTlen : nullptr,
+                                                       track ? g.roldTlen : nullptr, n); count_launch();
+            }
+            chk(cudaMemsetAsync(ctr, 0, sizeof(IterCounters), st));
+            // reverse counts and cursors start at the carried lengths
+            k_set_u32<<<tblocks, 256, 0, st>>>(rcnt_new, track ? g.rnewTlen : nullptr, n); count_launch();
+            k_set_u32<<<tblocks, 256, 0, st>>>(rcnt_old, track ? g.roldTlen : nullptr, n); count_launch();
+            k_set_u32<<<tblocks, 256, 0, st>>>(rcur_new, track ? g.rnewTlen : nullptr, n); count_launch();
+            k_set_u32<<<tblocks, 256, 0, st>>>(rcur_old, track ? g.roldTlen : nullptr, n); count_launch();
+            SampleArgs sa{g.pid, g.pdist, n, K, (uint32_t)mode, split,
+                          rcnt_new, rcnt_old, rcur_new, rcur_old, roff_new, roff_old, rseg_new, rseg_old,
+                          g.newL, g.oldL, g.newlen, g.oldlen,
+                          g.capn, g.capo,
+                          carry_now ? g.rnewT : nullptr, carry_now ? g.roldT : nullptr,
+                          carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr,
+                          g.smpl, ctr};
+            k_sample_count<<<warp_blocks, 256, 0, st>>>(sa); count_launch();
+            chk(exclusive_scan(rcnt_new, roff_new, n, scan_tmp, nullptr, st));
+            chk(exclusive_scan(rcnt_old, roff_old, n, scan_tmp, nullptr, st));
+            k_sample_fill<<<warp_blocks, 256, 0, st>>>(sa); count_launch();
+            RevSortArgs ra{{roff_new, roff_old}, {rseg_new, rseg_old}, {rscr_new, rscr_old},
+                           {carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr},
+                           n, P<uint32_t>(ws.bigrev), ctr};
+            // reverse lists in ascending source order, as the reference pushes
+            // them; the fast tier keeps them in the (arbitrary) order the atomics
+            // left: its samples and tie-break keys do not depend on list order
+            if (!g.fast) {
+                k_rev_sort_small<<<dim3(warp_blocks, 2), 256, 0, st>>>(ra); count_launch();
+                k_rev_sort_big<<<nsm * 2, 512, 0, st>>>(ra); count_launch();
+                // std::rand() draws of this iteration's shuffles
+                k_rand_count<<<tblocks, 256, 0, st>>>(roff_new, roff_old, n, P<uint32_t>(ws.rcount)); count_launch();
+                chk(exclusive_scan(P<uint32_t>(ws.rcount), P<uint64_t>(ws.rofs), n, scan_tmp, d_tot, st));
+                chk(glibc_stream_generate(P<int32_t>(ws.rbuf), g.gbase, g.gpos, d_tot, rev_cap * 2, st));
+            } else {
+                chk(cudaMemsetAsync(d_tot, 0, 8, st));
+            }
+            const ShufArgs sh = shuf_args();
+            k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh); count_launch();
+            chk(exclusive_scan(P<uint32_t>(ws.npairs), P<uint64_t>(ws.poff), n, scan_tmp,
+                               reinterpret_cast<uint64_t*>(&ctr->pairs), st));
+            chk(cudaMemsetAsync(ws.bcnt.p, 0, n1 * 4, st));
+            chk(cudaMemsetAsync(ws.bcur.p, 0, n1 * 4, st));
+            chk(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
+            chk(cudaGetLastError());
+            return e;
+        };
+        const bool graphable = g.fast && !carry_now && !seg.disabled;
+        if (graphable && seg.exec) {
+            ShufArgs sh = shuf_args();
+            void* kargs[] = {&sh};
+            cudaKernelNodeParams kp = seg.kp;
+            kp.kernelParams = kargs;
+            kp.extra = nullptr;
+            cudaError_t e = cudaGraphExecKernelNodeSetParams(seg.exec, seg.shuf, &kp);
+            if (e == cudaSuccess) e = cudaGraphLaunch(seg.exec, st);
+            NNM_CUDA_TRY(e);
+            count_launch(seg.launches);
+        } else if (graphable) {
+            const uint64_t c0 = launch_counter().load();
+            cudaGraph_t& graph = seg.graph;
+            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                const cudaError_t e1 = seg_a();
+                const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+                e = e1 != cudaSuccess ? e1 : e2;
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&seg.exec, graph, 0);
+            if (e == cudaSuccess) {
+                size_t nn = 0;
+                cudaGraphGetNodes(graph, nullptr, &nn);
+                std::vector<cudaGraphNode_t> nodes(nn);
+                cudaGraphGetNodes(graph, nodes.data(), &nn);
+                for (cudaGraphNode_t nd : nodes) {
+                    cudaGraphNodeType ty;
+                    cudaKernelNodeParams kp{};
+                    if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel &&
+                        cudaGraphKernelNodeGetParams(nd, &kp) == cudaSuccess &&
+                        kp.func == reinterpret_cast<void*>(k_shuffle_append)) {
+                        seg.shuf = nd;
+                        seg.kp = kp;
+                    }
+                }
+            }
+            seg.launches = launch_counter().load() - c0;
+            if (e == cudaSuccess && seg.shuf) e = cudaGraphLaunch(seg.exec, st);  // capture counted its kernels
+            if (e != cudaSuccess || !seg.shuf) {
+                // no graph: this call launches the segment directly
+                cudaGetLastError();
+                if (seg.exec) cudaGraphExecDestroy(seg.exec);
+                if (seg.graph) cudaGraphDestroy(seg.graph);
+                seg.exec = nullptr;
+                seg.graph = nullptr;
+                seg.disabled = true;
+                NNM_CUDA_TRY(seg_a());
+            }
         } else {
-            NNM_CUDA_TRY(cudaMemsetAsync(d_tot, 0, 8, st));
+            NNM_CUDA_TRY(seg_a());
         }
-        ShufArgs sh{roff_new, roff_old, rseg_new, rseg_old, P<uint64_t>(ws.rofs), P<int32_t>(ws.rbuf),
-                    g.newL, g.oldL, g.newlen, g.oldlen,
-                    g.capn, g.capo, n, g.smpl,
-                    track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
-                    track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
-                    P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, g.phase++,
-                    tc ? TC_MAX_S : 0u, max_staged, rscr_new, rscr_old, (g.fast && carry_now) ? 1u : 0u};
-        k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh); count_launch();
-        NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.npairs), P<uint64_t>(ws.poff), n, scan_tmp,
-                                    reinterpret_cast<uint64_t*>(&ctr->pairs), st));
-        NNM_CUDA_TRY(cudaMemsetAsync(ws.bcnt.p, 0, n1 * 4, st));
-        NNM_CUDA_TRY(cudaMemsetAsync(ws.bcur.p, 0, n1 * 4, st));
-        NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
         NNM_CUDA_TRY(cudaStreamSynchronize(st));
         if (ctx.h_counters->error) {
             ctx.last_error = "device capacity check failed (code " + std::to_string(ctx.h_counters->error) + ")";
