@@ -594,6 +594,12 @@ def main():
     # quality: recall@10 on a seeded row sample vs exact brute force
     build_dev()
     rec = recall_now()
+    # distance error of the returned distances against FP64 on the same rows
+    ids_s = ids_dev[torch.as_tensor(rows, device="cuda")].cpu().numpy().view(np.uint32).astype(np.int64)
+    ds_s = dists_dev[torch.as_tensor(rows, device="cuda")].cpu().numpy().astype(np.float64)
+    ref_s = ((x[rows][:, None, :].astype(np.float64) - x[ids_s].astype(np.float64)) ** 2).sum(-1)
+    rel = np.abs(ds_s - ref_s) / np.maximum(ref_s, 1e-30)
+    dist_err = {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()), "rows": len(rows)}
 
     hbm, peak_kind = peaks()
     names = {"join": ("local-join count pass: k_join_tc<0> (u8 Gram tiles on tcgen05) + FP32 k_pairs for lists > 128"
@@ -637,7 +643,8 @@ def main():
                        "path": a.path, "init": a.init, "train": train, "tune": tune,
                        "delta": bkw["delta"], "smpl": bkw["sample_cap"], "join": a.join,
                        "join_rows": prof["rows"],
-                       "recall@10": rec, "iterations": st["iterations"], "ncmps_merge": st["ncmps"],
+                       "recall@10": rec, "dist_err_vs_fp64": dist_err, "iterations": st["iterations"],
+                       "ncmps_merge": st["ncmps"],
                        "ncmps_leaves": st["sub_ncmps"],
                        "l2": "inputs (%d MB) larger than L2 (126 MB)" % (x.nbytes >> 20),
                        "parallelism": "replicas" if world > 1 else "single"},
