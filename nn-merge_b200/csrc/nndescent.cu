@@ -733,7 +733,10 @@ __device__ __forceinline__ void warp_sort_ment(uint32_t& pd, unsigned long long&
 // collected in a 32-entry buffer; a full buffer (and the rest at the end)
 // is sorted and merged into the pool, which lowers the K-th entry for the
 // proposals still to come.
-__global__ void __launch_bounds__(MERGE_WARPS * 32) k_merge(MergeArgs a) {
+// Eight blocks (64 warps) per SM, registers capped at 32: the merge waits on
+// scattered bucket and pool reads, and the added warps hide more of that
+// latency -- the 1M build is 2.4 % faster than at the uncapped 48 registers.
+__global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
     __shared__ MEnt sm[MERGE_WARPS][64];
     __shared__ MEnt kept[MERGE_WARPS][32];
     __shared__ MEnt buf[MERGE_WARPS][32];
