@@ -306,6 +306,8 @@ def run_search(a, rank, world, local):
     model = nnm.entry_init(d, C, seed=11)
     losses = ix.entry_train(model, steps=a.entry_steps, batch=2048, lr=2e-3, seed=3)
     ix.set_entry_model(model, probes=a.probes)
+    # autotuner (untimed): the fast kernel's width, timed on 10,000 of the queries
+    width, width_ms = ix.tune_width(q[:10_000], out_k=10, beams=beams[:10_000], entry="learned")
     prep_s = time.perf_counter() - t0
     x_t = torch.from_numpy(x).cuda()
     q_dev = torch.from_numpy(q).cuda()
@@ -411,11 +413,12 @@ def run_search(a, rank, world, local):
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded %d-centre Gaussian mixture, integers 0-255; queries from the same mixture "
                     "(fresh seed)" % a.centres,
-            "config": {"workload": "LySearch batch of %d queries, top-10, beams U{32..512}, fast kernel, learned "
-                                   "entry (probes %d), on the H-Merge hierarchy of %dx%d k=%d"
+            "config": {"workload": "LySearch batch of %d queries, top-10, beams U{32..512}, fast kernel (tuned width), "
+                                   "learned entry (probes %d), on the H-Merge hierarchy of %dx%d k=%d"
                                    % (nq, a.probes, n, d, k),
                        "n": n, "d": d, "k": k, "queries": nq, "layers": [len(o) - 1 for o, _ in h["layers"]],
                        "entry_layer": layer, "classes": C, "entry_train_steps": a.entry_steps,
+                       "width": width, "width_ms_10k": [round(float(v), 3) for v in width_ms],
                        "entry_loss_first": float(losses[:20].mean()), "entry_loss_last": float(losses[-20:].mean()),
                        "prep_s": prep_s, "recall@10": learned["recall"], "recall_rows": nrec,
                        "learned": learned, "default": default,

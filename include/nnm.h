@@ -300,6 +300,12 @@ int nnm_index_search_dev(nnm_index *ix, const float *q_dev, uint64_t nq, const u
  * (1: strict best-first order, as the reference).  width is in 1..4,
  * default 4; wider steps may expand a few more nodes. */
 int nnm_index_set_width(nnm_index *ix, uint32_t width);
+/* Autotuner of the width: times NNM_SERVE_FAST on the sample queries (host
+ * arrays, as nnm_index_search takes them) at widths 1..4, `repeats` times
+ * each (the fastest kept), sets the fastest and returns it in *width;
+ * ms (4 entries, may be NULL) gets each width's device time. */
+int nnm_index_tune_width(nnm_index *ix, const float *q, uint64_t nq, const uint32_t *beams, uint32_t beam,
+                         uint32_t out_k, uint32_t entry_mode, uint32_t repeats, uint32_t *width, double *ms);
 
 /* Entry-point network (no counterpart in the reference): its classes are
  * rows 0..C-1 of the data set (C <= NNM_ENTRY_MAX_CLASSES), and a learned

@@ -796,6 +796,38 @@ int nnm_index_set_width(nnm_index* h, uint32_t width) {
     return NNM_OK;
 }
 
+int nnm_index_tune_width(nnm_index* h, const float* q, uint64_t nq, const uint32_t* beams, uint32_t beam,
+                         uint32_t out_k, uint32_t entry_mode, uint32_t repeats, uint32_t* width, double* ms) {
+    if (!h || !width || nq == 0) return h ? fail(h->ctx, NNM_ERR_INVALID, "tune: queries and width are required")
+                                          : NNM_ERR_INVALID;
+    std::vector<uint32_t> ids((size_t)nq * out_k);
+    const uint32_t keep = h->ix.width;
+    double best = 1e300;
+    uint32_t bw = keep;
+    for (uint32_t w = 1; w <= 4; w++) {
+        h->ix.width = w;
+        double t = 1e300;
+        for (uint32_t r = 0; r < std::max(1u, repeats); r++) {
+            nnm_search_stats st;
+            int rc = index_search_impl(h, q, nq, beams, beam, out_k, NNM_SERVE_FAST, entry_mode, ids.data(), nullptr,
+                                       &st, false);
+            if (rc) {
+                h->ix.width = keep;
+                return rc;
+            }
+            t = std::min(t, st.device_ms - st.predict_ms);
+        }
+        if (ms) ms[w - 1] = t;
+        if (t < best) {
+            best = t;
+            bw = w;
+        }
+    }
+    h->ix.width = bw;
+    *width = bw;
+    return NNM_OK;
+}
+
 int nnm_index_entry_layer(const nnm_index* h, uint32_t* layer, uint32_t* n_classes) {
     if (!h || !layer || !n_classes) return NNM_ERR_INVALID;
     const nnm::IndexDev& ix = h->ix;

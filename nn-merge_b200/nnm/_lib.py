@@ -159,6 +159,7 @@ def load():
             getattr(lib, name).argtypes = [vp, vp, u64, vp, u32, u32, u32, u32, vp, vp, vp]
         lib.nnm_index_entry_layer.argtypes = [vp, vp, vp]
         lib.nnm_index_set_width.argtypes = [vp, u32]
+        lib.nnm_index_tune_width.argtypes = [vp, vp, u64, vp, u32, u32, u32, u32, vp, vp]
         lib.nnm_entry_forward.argtypes = [vp, vp, vp, u64, u32, vp]
         lib.nnm_entry_probes.argtypes = [vp, vp, vp, u64, u32, u32, vp]
         lib.nnm_entry_grad.argtypes = [vp, vp, vp, u64, u32, vp, vp, vp]
@@ -505,6 +506,19 @@ class Index:
 
     def set_width(self, width):
         self.ctx._check(self.ctx.lib.nnm_index_set_width(self.h, width))
+
+    def tune_width(self, q, out_k=10, beams=None, beam=None, entry="default", repeats=2):
+        """Times the fast kernel at widths 1..4 on these queries, keeps the
+        fastest; returns (width, ms per width)."""
+        q = np.ascontiguousarray(q, np.float32)
+        b = None if beams is None else np.ascontiguousarray(beams, np.uint32)
+        if beam is None:
+            beam = out_k if b is None else int(b.max())
+        w = ctypes.c_uint32()
+        ms = np.zeros(4, np.float64)
+        self.ctx._check(self.ctx.lib.nnm_index_tune_width(self.h, _ptr(q), q.shape[0], _ptr(b), beam, out_k,
+                                                          ENTRY_MODES[entry], repeats, ctypes.byref(w), _ptr(ms)))
+        return int(w.value), ms
 
     def entry_layer(self):
         layer, nc = ctypes.c_uint32(), ctypes.c_uint32()

@@ -380,3 +380,17 @@ def test_out_k_equal_to_small_beams(ctx):
             assert (r["ids"] != 0xFFFFFFFF).all()
     finally:
         ix.close()
+
+
+def test_width_tuner(hier, index):
+    """The width autotuner times widths 1..4 and keeps the fastest; the
+    search then runs at it, with the results of that width."""
+    _, _, q = hier
+    beams = np.random.default_rng(31).integers(32, 257, size=1000).astype(np.uint32)
+    w, ms = index.tune_width(q[:1000], out_k=10, beams=beams, repeats=2)
+    assert 1 <= w <= 4 and (ms > 0).all() and ms[w - 1] == ms.min()
+    a = index.search(q[:300], out_k=10, beams=beams[:300], mode="fast")
+    index.set_width(w)
+    b = index.search(q[:300], out_k=10, beams=beams[:300], mode="fast")
+    assert np.array_equal(a["ids"], b["ids"])
+    index.set_width(4)
