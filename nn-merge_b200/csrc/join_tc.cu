@@ -320,6 +320,12 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             const uint32_t nrm_b = S.nrm[tid], grp_b = S.grp[tid];
             const uint32_t blk = tid & ~(B - 1);
             uint32_t cb = 0;
+            // Rows of at most 32 slots lie inside one warp, so every proposal
+            // to slot s of such a tile comes from the warp holding s: its
+            // counter lives in a register of lane s % 32 (read by shuffle)
+            // instead of shared memory (an atomic round trip per pair).
+            const bool wl = lgB <= 5;
+            uint32_t cnt_r = 0;
             const uint32_t c_first = B >= 32 ? ((warp * 32) & ~(B - 1)) : warp * 32;
             for (uint32_t c0 = c_first; c0 <= warp * 32; c0 += 32) {
                 // columns a of a pair are new-list entries: a < blk + nn_b; the
@@ -327,59 +333,82 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                 const int lim = valid_b ? (int)(blk + nn_b) - (int)c0 : 0;
                 const uint32_t jend = (uint32_t)__reduce_max_sync(0xffffffffu, lim < 0 ? 0 : (lim > 32 ? 32 : lim));
                 if (jend == 0) continue;
-                uint32_t v[32];
-                tmem_ld32(tmem + ((warp * 32) << 16) + c0, v);
+                // 16 columns per TMEM load keeps the epilogue within 64 registers
+                for (uint32_t h = 0; h < jend; h += 16) {
+                    uint32_t v[16];
+                    tmem_ld16(tmem + ((warp * 32) << 16) + c0 + h, v);
 #pragma unroll
-                for (uint32_t jj = 0; jj < 32; jj++) {
-                    if (jj >= jend) break;
-                    const uint32_t av = c0 + jj;
-                    const uint32_t q_a = av & (B - 1);
-                    const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
-                    const uint32_t e_a = S.ids[av];
-                    float dd;
-                    if (KIND == 0) {
-                        dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[jj]);
-                    } else {
-                        // approximate distance; pairs it cannot rule out get
-                        // the reference's exact sum
-                        const float ns = __uint_as_float(S.nrm[av]) + __uint_as_float(nrm_b);
-                        dd = ns - 2.f * __uint_as_float(v[jj]);
-                        if (pv && dd - a.err_c * ns < fmaxf(S.kth[av], kth_b))
-                            dd = exact_l2(a.x, a.dp, e_a & LID_MASK, e_b & LID_MASK);
-                    }
-                    uint32_t outer = 0, inner = 0;
-                    const bool ok =
-                        pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, S.grp[av], grp_b, outer, inner);
-                    const float kth_a = S.kth[av];
-                    if (PASS == 0) {
-                        cmps += ok;
-                        cb += (ok && dd < kth_b);
-                        const unsigned m = __ballot_sync(0xffffffffu, ok && dd < kth_a);
-                        if (m && lane == 0) atomicAdd(&S.cnt[av], (uint32_t)__popc(m));
-                    } else {
-                        const uint32_t pidx = outer * S_b + inner;
-                        const bool pa = ok && dd < kth_a;
-                        const unsigned m = __ballot_sync(0xffffffffu, pa);
-                        if (m) {
-                            const uint32_t leader = __ffs(m) - 1;
-                            uint32_t base = 0;
-                            if (lane == leader) base = atomicAdd(&S.cnt[av], (uint32_t)__popc(m));
-                            base = __shfl_sync(0xffffffffu, base, leader);
-                            if (pa) {
-                                const unsigned long long slot = S.base[av] + base + __popc(m & ((1u << lane) - 1u));
-                                a.bucket[slot] = Prop{
-                                    dd, e_b, prop_key(a.fast_key, row_b, pidx, e_b, outer == q_a ? 0u : 1u)};
-                            }
+                    for (uint32_t j16 = 0; j16 < 16; j16++) {
+                        const uint32_t jj = h + j16;
+                        if (jj >= jend) break;
+                        const uint32_t av = c0 + jj;
+                        const uint32_t q_a = av & (B - 1);
+                        const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
+                        const uint32_t e_a = S.ids[av];
+                        float dd;
+                        if (KIND == 0) {
+                            dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[j16]);
+                        } else {
+                            // approximate distance; pairs it cannot rule out get
+                            // the reference's exact sum
+                            const float ns = __uint_as_float(S.nrm[av]) + __uint_as_float(nrm_b);
+                            dd = ns - 2.f * __uint_as_float(v[j16]);
+                            if (pv && dd - a.err_c * ns < fmaxf(S.kth[av], kth_b))
+                                dd = exact_l2(a.x, a.dp, e_a & LID_MASK, e_b & LID_MASK);
                         }
-                        if (ok && dd < kth_b) {
-                            const unsigned long long slot = S.base[tid] + atomicAdd(&S.cnt[tid], 1u);
-                            a.bucket[slot] = Prop{
-                                dd, e_a, prop_key(a.fast_key, row_b, pidx, e_a, outer == q_b ? 0u : 1u)};
+                        uint32_t outer = 0, inner = 0;
+                        const bool ok =
+                            pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, S.grp[av], grp_b, outer, inner);
+                        const float kth_a = S.kth[av];
+                        if (PASS == 0) {
+                            cmps += ok;
+                            cb += (ok && dd < kth_b);
+                            const unsigned m = __ballot_sync(0xffffffffu, ok && dd < kth_a);
+                            if (wl) {
+                                if (lane == (av & 31)) cnt_r += __popc(m);
+                            } else if (m && lane == 0) {
+                                atomicAdd(&S.cnt[av], (uint32_t)__popc(m));
+                            }
+                        } else {
+                            const uint32_t pidx = outer * S_b + inner;
+                            const bool pa = ok && dd < kth_a;
+                            const unsigned m = __ballot_sync(0xffffffffu, pa);
+                            if (m) {
+                                uint32_t base;
+                                if (wl) {
+                                    // the owner of slot av is lane av % 32; its own
+                                    // pair with av is not a pair (q_a == q_b), so it
+                                    // takes no b-side proposal in this step
+                                    base = __shfl_sync(0xffffffffu, cnt_r, av & 31);
+                                    if (lane == (av & 31)) cnt_r += __popc(m);
+                                } else {
+                                    const uint32_t leader = __ffs(m) - 1;
+                                    base = 0;
+                                    if (lane == leader) base = atomicAdd(&S.cnt[av], (uint32_t)__popc(m));
+                                    base = __shfl_sync(0xffffffffu, base, leader);
+                                }
+                                if (pa) {
+                                    const unsigned long long slot = S.base[av] + base + __popc(m & ((1u << lane) - 1u));
+                                    a.bucket[slot] = Prop{
+                                        dd, e_b, prop_key(a.fast_key, row_b, pidx, e_b, outer == q_a ? 0u : 1u)};
+                                }
+                            }
+                            if (ok && dd < kth_b) {
+                                const uint32_t pos = wl ? cnt_r++ : atomicAdd(&S.cnt[tid], 1u);
+                                const unsigned long long slot = S.base[tid] + pos;
+                                a.bucket[slot] = Prop{
+                                    dd, e_a, prop_key(a.fast_key, row_b, pidx, e_a, outer == q_b ? 0u : 1u)};
+                            }
                         }
                     }
                 }
             }
-            if (PASS == 0 && cb) atomicAdd(&S.cnt[tid], cb);
+            if (PASS == 0) {
+                if (wl)
+                    S.cnt[tid] = cnt_r + cb;
+                else if (cb)
+                    atomicAdd(&S.cnt[tid], cb);
+            }
             asm volatile("tcgen05.fence::before_thread_sync;");
             group_sync(BAR_CONS);
             if (PASS == 0) {
