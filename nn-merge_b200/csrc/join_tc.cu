@@ -333,13 +333,13 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                 const int lim = valid_b ? (int)(blk + nn_b) - (int)c0 : 0;
                 const uint32_t jend = (uint32_t)__reduce_max_sync(0xffffffffu, lim < 0 ? 0 : (lim > 32 ? 32 : lim));
                 if (jend == 0) continue;
-                // 16 columns per TMEM load keeps the epilogue within 64 registers
-                for (uint32_t h = 0; h < jend; h += 16) {
-                    uint32_t v[16];
-                    tmem_ld16(tmem + ((warp * 32) << 16) + c0 + h, v);
+                // 8 columns per TMEM load: no spills at 64 registers, a short unrolled body
+                for (uint32_t h = 0; h < jend; h += 8) {
+                    uint32_t v[8];
+                    tmem_ld8(tmem + ((warp * 32) << 16) + c0 + h, v);
 #pragma unroll
-                    for (uint32_t j16 = 0; j16 < 16; j16++) {
-                        const uint32_t jj = h + j16;
+                    for (uint32_t j8 = 0; j8 < 8; j8++) {
+                        const uint32_t jj = h + j8;
                         if (jj >= jend) break;
                         const uint32_t av = c0 + jj;
                         const uint32_t q_a = av & (B - 1);
@@ -347,12 +347,12 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                         const uint32_t e_a = S.ids[av];
                         float dd;
                         if (KIND == 0) {
-                            dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[j16]);
+                            dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[j8]);
                         } else {
                             // approximate distance; pairs it cannot rule out get
                             // the reference's exact sum
                             const float ns = __uint_as_float(S.nrm[av]) + __uint_as_float(nrm_b);
-                            dd = ns - 2.f * __uint_as_float(v[j16]);
+                            dd = ns - 2.f * __uint_as_float(v[j8]);
                             if (pv && dd - a.err_c * ns < fmaxf(S.kth[av], kth_b))
                                 dd = exact_l2(a.x, a.dp, e_a & LID_MASK, e_b & LID_MASK);
                         }
