@@ -449,17 +449,27 @@ __global__ void k_shuffle_append(ShufArgs a) {
 // of neighbouring threads (q = 4t + i for consecutive t) fall in different
 // bank groups.
 __device__ __forceinline__ uint32_t vrow(uint32_t q, uint32_t vstride) { return q * vstride + (q >> 2); }
+__host__ __device__ __forceinline__ uint32_t vec_stride(uint32_t units) { return ((units + 7) & ~7u) + 1; }
 
-template <int M, bool STAGED>
+// Where pairs_row reads a row's vectors: FP32 from global memory (L2), FP32
+// staged in shared memory, or the u8 operand copy of the tensor-core join
+// staged in shared memory.  The u8 form is used only when every component
+// is an integer in [0, 255]: d(a, b) = |a|^2 + |b|^2 - 2 a.b is then an
+// exact integer below 2^24, the value of the reference's sequential float
+// sum of the same terms, so all three give the same distances.
+constexpr int VEC_GLOBAL = 0, VEC_F32 = 1, VEC_U8 = 2;
+
+template <int M, int VEC>
 __device__ void pairs_row(const JoinArgs& a, uint32_t row, unsigned char* smem, uint32_t R) {
     const uint32_t nn = a.newlen[row], no = a.oldlen[row], S = nn + no;
     uint32_t* s_ids = reinterpret_cast<uint32_t*>(smem);
     float* s_kth = reinterpret_cast<float*>(s_ids + R);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_kth + R);
     uint32_t* s_grp = s_cnt + R;
-    float4* s_vec = reinterpret_cast<float4*>(s_grp + R);  // 16R bytes before it
-    const uint32_t dq = a.dp >> 2, vstride = ((dq + 7) & ~7u) + 1;
-    const float4* x4 = reinterpret_cast<const float4*>(a.x);
+    uint32_t* s_nrm = s_grp + R;  // VEC_U8 only
+    float4* s_vec = reinterpret_cast<float4*>(VEC == VEC_U8 ? s_nrm + ((R + 3) & ~3u) : s_grp + R);
+    const uint32_t dq = VEC == VEC_U8 ? a.kq >> 4 : a.dp >> 2, vstride = vec_stride(dq);
+    const float4* x4 = reinterpret_cast<const float4*>(VEC == VEC_U8 ? (const void*)a.xq : (const void*)a.x);
 
     for (uint32_t q = threadIdx.x; q < S; q += blockDim.x) {
         uint32_t e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
@@ -468,9 +478,10 @@ __device__ void pairs_row(const JoinArgs& a, uint32_t row, unsigned char* smem, 
         s_kth[q] = a.pdist[(size_t)id * a.K + a.K - 1];
         s_cnt[q] = 0;
         s_grp[q] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
+        if (VEC == VEC_U8) s_nrm[q] = a.nrm[id];
     }
     __syncthreads();
-    if (STAGED) {
+    if (VEC != VEC_GLOBAL) {
         for (uint32_t i = threadIdx.x; i < S * dq; i += blockDim.x) {
             uint32_t q = i / dq, c = i - q * dq;
             s_vec[vrow(q, vstride) + c] = x4[(size_t)(s_ids[q] & LID_MASK) * dq + c];
@@ -494,30 +505,62 @@ __device__ void pairs_row(const JoinArgs& a, uint32_t row, unsigned char* smem, 
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             uint32_t ai = min(ta * 4 + i, nn - 1), bj = min(tb * 4 + i, S - 1);
-            pa[i] = STAGED ? s_vec + vrow(ai, vstride) : x4 + (size_t)(s_ids[ai] & LID_MASK) * dq;
-            pb[i] = STAGED ? s_vec + vrow(bj, vstride) : x4 + (size_t)(s_ids[bj] & LID_MASK) * dq;
+            pa[i] = VEC != VEC_GLOBAL ? s_vec + vrow(ai, vstride) : x4 + (size_t)(s_ids[ai] & LID_MASK) * dq;
+            pb[i] = VEC != VEC_GLOBAL ? s_vec + vrow(bj, vstride) : x4 + (size_t)(s_ids[bj] & LID_MASK) * dq;
         }
         float acc[4][4];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
-        for (uint32_t c = 0; c < dq; c++) {
-            float4 A[4], B[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                A[i] = pa[i][c];
-                B[i] = pb[i][c];
-            }
+        if (VEC == VEC_U8) {
+            uint32_t dot[4][4];
 #pragma unroll
             for (int i = 0; i < 4; i++)
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    acc[i][j] = dist_step<M>(acc[i][j], A[i].x, B[j].x);
-                    acc[i][j] = dist_step<M>(acc[i][j], A[i].y, B[j].y);
-                    acc[i][j] = dist_step<M>(acc[i][j], A[i].z, B[j].z);
-                    acc[i][j] = dist_step<M>(acc[i][j], A[i].w, B[j].w);
+                for (int j = 0; j < 4; j++) dot[i][j] = 0u;
+            for (uint32_t c = 0; c < dq; c++) {  // 16 components per step
+                uint4 A[4], B[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    A[i] = reinterpret_cast<const uint4*>(pa[i])[c];
+                    B[i] = reinterpret_cast<const uint4*>(pb[i])[c];
                 }
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        dot[i][j] = __dp4a(A[i].x, B[j].x, dot[i][j]);
+                        dot[i][j] = __dp4a(A[i].y, B[j].y, dot[i][j]);
+                        dot[i][j] = __dp4a(A[i].z, B[j].z, dot[i][j]);
+                        dot[i][j] = __dp4a(A[i].w, B[j].w, dot[i][j]);
+                    }
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t na = s_nrm[min(ta * 4 + i, nn - 1)];
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    acc[i][j] = (float)((int)(na + s_nrm[min(tb * 4 + j, S - 1)]) - 2 * (int)dot[i][j]);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+            for (uint32_t c = 0; c < dq; c++) {
+                float4 A[4], B[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    A[i] = pa[i][c];
+                    B[i] = pb[i][c];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        acc[i][j] = dist_step<M>(acc[i][j], A[i].x, B[j].x);
+                        acc[i][j] = dist_step<M>(acc[i][j], A[i].y, B[j].y);
+                        acc[i][j] = dist_step<M>(acc[i][j], A[i].z, B[j].z);
+                        acc[i][j] = dist_step<M>(acc[i][j], A[i].w, B[j].w);
+                    }
+            }
         }
 #pragma unroll
         for (int i = 0; i < 4; i++) {
@@ -554,7 +597,17 @@ __global__ void __launch_bounds__(TIER_THREADS[TIER]) k_pairs(JoinArgs a, uint32
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t cnt = a.ctr->ntier[TIER];
     const uint32_t* rows = a.tier_rows + (size_t)TIER * a.n;
-    for (uint32_t b = blockIdx.x; b < cnt; b += gridDim.x) pairs_row<M, (TIER < NTIER - 1)>(a, rows[b], smem, R);
+    for (uint32_t b = blockIdx.x; b < cnt; b += gridDim.x)
+        pairs_row<M, (TIER < NTIER - 1 ? VEC_F32 : VEC_GLOBAL)>(a, rows[b], smem, R);
+}
+
+// Rows of the last tier (S > 128) next to the u8 tensor-core join: the u8
+// vectors staged in shared memory, integer dot products (dp4a).
+__global__ void __launch_bounds__(TIER_THREADS[NTIER - 1]) k_pairs_u8(JoinArgs a, uint32_t R) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t cnt = a.ctr->ntier[NTIER - 1];
+    const uint32_t* rows = a.tier_rows + (size_t)(NTIER - 1) * a.n;
+    for (uint32_t b = blockIdx.x; b < cnt; b += gridDim.x) pairs_row<L2, VEC_U8>(a, rows[b], smem, R);
 }
 
 // One warp per row: proposals from the stored pair distances.  With the
@@ -892,8 +945,14 @@ int graph_alloc(Ctx& ctx, GraphStore& s, GraphDev& g, bool with_carry) {
 // Shared memory of a k_pairs block: member arrays (16 B per list slot) and,
 // for the staged tiers, the swizzled vectors.
 static size_t pairs_smem(uint32_t R, uint32_t dp, bool staged) {
-    const uint32_t dq = dp / 4, vstride = ((dq + 7) & ~7u) + 1;
+    const uint32_t vstride = vec_stride(dp / 4);
     return (size_t)R * 16 + (staged ? ((size_t)R * vstride + R / 4 + 1) * 16 : 0) + 64;
+}
+
+// k_pairs_u8: the member arrays, the norms, then kq bytes a row.
+static size_t pairs_smem_u8(uint32_t R, uint32_t kq) {
+    const uint32_t vstride = vec_stride(kq / 16);
+    return (size_t)R * 16 + (size_t)((R + 3) & ~3u) * 4 + ((size_t)R * vstride + R / 4 + 1) * 16 + 64;
 }
 
 // Highest list-size tier whose staged vectors fit in a CTA's shared memory
@@ -927,7 +986,7 @@ static cudaError_t prep_pairs(uint32_t caps, uint32_t dp, size_t emit_smem, int 
 // join takes the others.
 template <int M>
 static void launch_pairs(const JoinArgs& ja, const unsigned* ntier, uint32_t caps, uint32_t dp, int nsm,
-                         bool last_only, cudaStream_t st) {
+                         bool last_only, bool u8_last, cudaStream_t st) {
     if (!last_only) {
         if (ntier[0]) { k_pairs<M, 0><<<ntier[0], TIER_THREADS[0], pairs_smem(TIER_CAP[0], dp, true), st>>>(ja, TIER_CAP[0]); count_launch(); }
         if (ntier[1]) { k_pairs<M, 1><<<ntier[1], TIER_THREADS[1], pairs_smem(TIER_CAP[1], dp, true), st>>>(ja, TIER_CAP[1]); count_launch(); }
@@ -936,7 +995,12 @@ static void launch_pairs(const JoinArgs& ja, const unsigned* ntier, uint32_t cap
     }
     if (ntier[4]) {
         unsigned g = std::min<unsigned>(ntier[4], (unsigned)nsm * 4);
-        k_pairs<M, 4><<<g, TIER_THREADS[4], pairs_smem(caps, dp, false), st>>>(ja, caps); count_launch();
+        if (u8_last) {
+            k_pairs_u8<<<g, TIER_THREADS[4], pairs_smem_u8(caps, ja.kq), st>>>(ja, caps);
+        } else {
+            k_pairs<M, 4><<<g, TIER_THREADS[4], pairs_smem(caps, dp, false), st>>>(ja, caps);
+        }
+        count_launch();
     }
 }
 
@@ -997,9 +1061,16 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     NNM_CUDA_TRY(ws.poff.ensure(n1 * 8));
     NNM_CUDA_TRY(ws.tiers.ensure((size_t)n * NTIER * 4 + 16));
     const bool tc = g.xq != nullptr;
+    bool u8_last = false;  // rows of S > 128 on k_pairs_u8 (u8 join, staged vectors fit)
     if (tc) {
         NNM_CUDA_TRY(tc_set_attributes(g.kq, g.tc_kind));
         NNM_CUDA_TRY(ws.erows.ensure((size_t)n * 4 * 4 + 16));
+        int optin = 0;
+        NNM_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx.device));
+        const size_t u8_smem = pairs_smem_u8(caps, g.kq);
+        u8_last = g.tc_kind == 0 && g.metric == L2 && u8_smem <= (size_t)optin;
+        if (u8_last)
+            NNM_CUDA_TRY(cudaFuncSetAttribute(k_pairs_u8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u8_smem));
     }
 
     const unsigned warp_blocks = (unsigned)((n + 7) / 8);
@@ -1161,9 +1232,9 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     g.fast ? 1u : 0u, g.tc_kind, g.err_c};
         if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
         if (tc) NNM_CUDA_TRY(launch_join_tc(0, ja, ntier, nsm, st));
-        if (g.metric == L2) launch_pairs<L2>(ja, ntier, caps, g.dp, nsm, tc, st);
-        else if (g.metric == L1) launch_pairs<L1>(ja, ntier, caps, g.dp, nsm, tc, st);
-        else launch_pairs<CHI2>(ja, ntier, caps, g.dp, nsm, tc, st);
+        if (g.metric == L2) launch_pairs<L2>(ja, ntier, caps, g.dp, nsm, tc, u8_last, st);
+        else if (g.metric == L1) launch_pairs<L1>(ja, ntier, caps, g.dp, nsm, tc, false, st);
+        else launch_pairs<CHI2>(ja, ntier, caps, g.dp, nsm, tc, false, st);
         if (ctx.prof) cudaEventRecord(ctx.ev[1], st);
         NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff), n, scan_tmp,
                                     reinterpret_cast<uint64_t*>(&ctr->proposals), st));
@@ -1221,8 +1292,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                                      : (hc.ntier[0] > 0) + (hc.ntier[1] > 0) + (hc.ntier[2] > 0) +
                                            (hc.ntier[3] > 0) + (hc.ntier[4] > 0);
             ctx.kjoin.ms += t01;
-            ctx.kjoin.bytes += s_f32 * ((double)g.dp * 4.0 + 10.0) + s_tc * ((double)g.kq + 14.0) +
-                               (double)hc.pairs * 4.0;
+            const double f32_slot = u8_last ? (double)g.kq + 14.0 : (double)g.dp * 4.0 + 10.0;
+            ctx.kjoin.bytes += s_f32 * f32_slot + s_tc * ((double)g.kq + 14.0) + (double)hc.pairs * 4.0;
             ctx.kjoin.flops += (double)hc.pairs * (double)g.d * 3.0;
             ctx.kemit.launches += tc ? 1 + (hc.ntier[4] > 0) : 1;
             ctx.kemit.ms += t23;

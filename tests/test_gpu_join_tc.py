@@ -67,10 +67,13 @@ def test_hmerge(ctx):
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
-def test_all_tiers_and_big_lists(ctx):
+@pytest.mark.parametrize("d", [128, 300])
+def test_all_tiers_and_big_lists(ctx, d):
     # k=32 with a large sample cap gives lists of 17..128 entries and rows
-    # above 128 that stay on the FP32 kernel; k=6 gives lists of <= 16
-    x = gaussian_mixture_u8(4000, seed=36, n_centres=8)
+    # above 128, which take the staged u8 pair kernel (d=128) or, when the
+    # staged vectors do not fit in shared memory (d=300, lists up to 864),
+    # the unstaged FP32 one; k=6 gives lists of <= 16
+    x = gaussian_mixture_u8(4000, d=d, seed=36, n_centres=8)
     t, f, big = both(ctx, ctx.kgraph, x, 32, seed=11, sample_cap=400)
     same(t, f)
     t, f, small = both(ctx, ctx.kgraph, x, 6, seed=11)
