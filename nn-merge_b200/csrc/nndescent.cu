@@ -721,11 +721,9 @@ __device__ __forceinline__ void merge_round(uint32_t pd, unsigned long long pk, 
                                             uint32_t& cd, uint32_t& ce, unsigned long long& ck, MEnt* sm,
                                             MEnt* kept) {
     const int lane = threadIdx.x & 31;
-    if (lane < (int)K) {
-        uint32_t pos = lane + count_less(pd, pk, m, cd, ck);
-        sm[pos] = MEnt{cd, ce, ck};
-    } else {
-        count_less(pd, pk, m, cd, ck);
+    {
+        const uint32_t pos = lane + count_less(pd, pk, m, cd, ck);  // every lane takes part in the shuffles
+        if (lane < (int)K) sm[pos] = MEnt{cd, ce, ck};
     }
     {
         uint32_t pos = lane + count_less(cd, ck, K, pd, pk, true);
@@ -789,6 +787,10 @@ __device__ __forceinline__ void warp_sort_ment(uint32_t& pd, unsigned long long&
 // Eight blocks (64 warps) per SM, registers capped at 32: the merge waits on
 // scattered bucket and pool reads, and the added warps hide more of that
 // latency -- the 1M build is 2.4 % faster than at the uncapped 48 registers.
+// The kernel is bound by instruction fetch (the GPC instruction cache ran at
+// 96 % of its request rate with the flush inlined twice), so the flush and
+// the pool-side binary search each have a single inlined copy: 9 % off the
+// 1M build.
 __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
     __shared__ MEnt sm[MERGE_WARPS][64];
     __shared__ MEnt kept[MERGE_WARPS][32];
@@ -828,35 +830,45 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
                 kk = __shfl_sync(FULL, ck, K - 1);
                 nb = 0;
             };
-            for (uint32_t b0 = 0; b0 < c; b0 += 32) {
+            // One call site of flush (its sort and merge are long): a full
+            // buffer flushes inside the loop, the last partial one after the
+            // final chunk, at the same points of the proposal stream as
+            // before.
+            for (uint32_t b0 = 0;; b0 += 32) {
                 uint32_t pd = 0xffffffffu, pe = 0;
                 unsigned long long pk = ~0ull;
-                bool valid = false;
-                if (b0 + lane < c) {
-                    Prop p = bp[b0 + lane];
-                    pd = __float_as_uint(p.dist);
-                    pk = p.key;
-                    pe = (p.idg & LID_MASK) | ((p.idg >> 31) << 30) | FLAG_BIT;
-                    valid = mless(pd, pk, kd, kk);
-                }
-                unsigned vb = __ballot_sync(FULL, valid);
-                if (!vb) continue;
-                const uint32_t take = min((uint32_t)__popc(vb), 32u - nb);
-                const uint32_t rank = __popc(vb & lt);
-                if (valid && rank < take) buf[w][nb + rank] = MEnt{pd, pe, pk};
-                __syncwarp();
-                nb += take;
-                if (nb == 32) {
-                    flush();
-                    // the rest of this chunk, against the new K-th entry
-                    valid = valid && rank >= take && mless(pd, pk, kd, kk);
-                    vb = __ballot_sync(FULL, valid);
-                    if (valid) buf[w][__popc(vb & lt)] = MEnt{pd, pe, pk};
+                bool rest = false;
+                const bool last = b0 >= c;
+                if (last) {
+                    if (nb == 0) break;
+                } else {
+                    bool valid = false;
+                    if (b0 + lane < c) {
+                        Prop p = bp[b0 + lane];
+                        pd = __float_as_uint(p.dist);
+                        pk = p.key;
+                        pe = (p.idg & LID_MASK) | ((p.idg >> 31) << 30) | FLAG_BIT;
+                        valid = mless(pd, pk, kd, kk);
+                    }
+                    const unsigned vb = __ballot_sync(FULL, valid);
+                    if (!vb) continue;
+                    const uint32_t take = min((uint32_t)__popc(vb), 32u - nb);
+                    const uint32_t rank = __popc(vb & lt);
+                    if (valid && rank < take) buf[w][nb + rank] = MEnt{pd, pe, pk};
                     __syncwarp();
-                    nb = __popc(vb);
+                    nb += take;
+                    if (nb < 32) continue;
+                    rest = valid && rank >= take;
                 }
+                flush();
+                if (last) break;
+                // the rest of this chunk, against the new K-th entry
+                rest = rest && mless(pd, pk, kd, kk);
+                const unsigned rb = __ballot_sync(FULL, rest);
+                if (rest) buf[w][__popc(rb & lt)] = MEnt{pd, pe, pk};
+                __syncwarp();
+                nb = __popc(rb);
             }
-            if (nb) flush();
             if (lane < (int)K) {
                 a.pid[(size_t)t * K + lane] = ce;
                 a.pdist[(size_t)t * K + lane] = __uint_as_float(cd);
