@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 
 #include <cuda_bf16.h>
 
@@ -324,87 +325,96 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             // to slot s of such a tile comes from the warp holding s: its
             // counter lives in a register of lane s % 32 (read by shuffle)
             // instead of shared memory (an atomic round trip per pair).
-            const bool wl = lgB <= 5;
+            const bool wl_tile = lgB <= 5;
             uint32_t cnt_r = 0;
             const uint32_t c_first = B >= 32 ? ((warp * 32) & ~(B - 1)) : warp * 32;
-            for (uint32_t c0 = c_first; c0 <= warp * 32; c0 += 32) {
-                // columns a of a pair are new-list entries: a < blk + nn_b; the
-                // bound is made warp-uniform (lanes of different rows take the max)
-                const int lim = valid_b ? (int)(blk + nn_b) - (int)c0 : 0;
-                const uint32_t jend = (uint32_t)__reduce_max_sync(0xffffffffu, lim < 0 ? 0 : (lim > 32 ? 32 : lim));
-                if (jend == 0) continue;
-                // 8 columns per TMEM load: no spills at 64 registers, a short unrolled body
-                for (uint32_t h = 0; h < jend; h += 8) {
-                    uint32_t v[8];
-                    tmem_ld8(tmem + ((warp * 32) << 16) + c0 + h, v);
+            // the loop specialised for the tile's counter kind, so that the
+            // one running holds no code of the other (the emit pass is
+            // bound by instruction fetch)
+            auto pairs = [&](auto wl_kind) {
+                constexpr bool wl = decltype(wl_kind)::value;
+                for (uint32_t c0 = c_first; c0 <= warp * 32; c0 += 32) {
+                    // columns a of a pair are new-list entries: a < blk + nn_b; the
+                    // bound is made warp-uniform (lanes of different rows take the max)
+                    const int lim = valid_b ? (int)(blk + nn_b) - (int)c0 : 0;
+                    const uint32_t jend = (uint32_t)__reduce_max_sync(0xffffffffu, lim < 0 ? 0 : (lim > 32 ? 32 : lim));
+                    if (jend == 0) continue;
+                    // 8 columns per TMEM load: no spills at 64 registers, a short unrolled body
+                    for (uint32_t h = 0; h < jend; h += 8) {
+                        uint32_t v[8];
+                        tmem_ld8(tmem + ((warp * 32) << 16) + c0 + h, v);
 #pragma unroll
-                    for (uint32_t j8 = 0; j8 < 8; j8++) {
-                        const uint32_t jj = h + j8;
-                        if (jj >= jend) break;
-                        const uint32_t av = c0 + jj;
-                        const uint32_t q_a = av & (B - 1);
-                        const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
-                        const uint32_t e_a = S.ids[av];
-                        float dd;
-                        if (KIND == 0) {
-                            dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[j8]);
-                        } else {
-                            // approximate distance; pairs it cannot rule out get
-                            // the reference's exact sum
-                            const float ns = __uint_as_float(S.nrm[av]) + __uint_as_float(nrm_b);
-                            dd = ns - 2.f * __uint_as_float(v[j8]);
-                            if (pv && dd - a.err_c * ns < fmaxf(S.kth[av], kth_b))
-                                dd = exact_l2(a.x, a.dp, e_a & LID_MASK, e_b & LID_MASK);
-                        }
-                        uint32_t outer = 0, inner = 0;
-                        const bool ok =
-                            pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, S.grp[av], grp_b, outer, inner);
-                        const float kth_a = S.kth[av];
-                        if (PASS == 0) {
-                            cmps += ok;
-                            cb += (ok && dd < kth_b);
-                            const unsigned m = __ballot_sync(0xffffffffu, ok && dd < kth_a);
-                            if (wl) {
-                                if (lane == (av & 31)) cnt_r += __popc(m);
-                            } else if (m && lane == 0) {
-                                atomicAdd(&S.cnt[av], (uint32_t)__popc(m));
+                        for (uint32_t j8 = 0; j8 < 8; j8++) {
+                            const uint32_t jj = h + j8;
+                            if (jj >= jend) break;
+                            const uint32_t av = c0 + jj;
+                            const uint32_t q_a = av & (B - 1);
+                            const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
+                            const uint32_t e_a = S.ids[av];
+                            float dd;
+                            if (KIND == 0) {
+                                dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[j8]);
+                            } else {
+                                // approximate distance; pairs it cannot rule out get
+                                // the reference's exact sum
+                                const float ns = __uint_as_float(S.nrm[av]) + __uint_as_float(nrm_b);
+                                dd = ns - 2.f * __uint_as_float(v[j8]);
+                                if (pv && dd - a.err_c * ns < fmaxf(S.kth[av], kth_b))
+                                    dd = exact_l2(a.x, a.dp, e_a & LID_MASK, e_b & LID_MASK);
                             }
-                        } else {
-                            const uint32_t pidx = outer * S_b + inner;
-                            const bool pa = ok && dd < kth_a;
-                            const unsigned m = __ballot_sync(0xffffffffu, pa);
-                            if (m) {
-                                uint32_t base;
+                            uint32_t outer = 0, inner = 0;
+                            const bool ok = pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, S.grp[av],
+                                                             grp_b, outer, inner);
+                            const float kth_a = S.kth[av];
+                            if (PASS == 0) {
+                                cmps += ok;
+                                cb += (ok && dd < kth_b);
+                                const unsigned m = __ballot_sync(0xffffffffu, ok && dd < kth_a);
                                 if (wl) {
-                                    // the owner of slot av is lane av % 32; its own
-                                    // pair with av is not a pair (q_a == q_b), so it
-                                    // takes no b-side proposal in this step
-                                    base = __shfl_sync(0xffffffffu, cnt_r, av & 31);
                                     if (lane == (av & 31)) cnt_r += __popc(m);
-                                } else {
-                                    const uint32_t leader = __ffs(m) - 1;
-                                    base = 0;
-                                    if (lane == leader) base = atomicAdd(&S.cnt[av], (uint32_t)__popc(m));
-                                    base = __shfl_sync(0xffffffffu, base, leader);
+                                } else if (m && lane == 0) {
+                                    atomicAdd(&S.cnt[av], (uint32_t)__popc(m));
                                 }
-                                if (pa) {
-                                    const unsigned long long slot = S.base[av] + base + __popc(m & ((1u << lane) - 1u));
+                            } else {
+                                const uint32_t pidx = outer * S_b + inner;
+                                const bool pa = ok && dd < kth_a;
+                                const unsigned m = __ballot_sync(0xffffffffu, pa);
+                                if (m) {
+                                    uint32_t base;
+                                    if (wl) {
+                                        // the owner of slot av is lane av % 32; its own
+                                        // pair with av is not a pair (q_a == q_b), so it
+                                        // takes no b-side proposal in this step
+                                        base = __shfl_sync(0xffffffffu, cnt_r, av & 31);
+                                        if (lane == (av & 31)) cnt_r += __popc(m);
+                                    } else {
+                                        const uint32_t leader = __ffs(m) - 1;
+                                        base = 0;
+                                        if (lane == leader) base = atomicAdd(&S.cnt[av], (uint32_t)__popc(m));
+                                        base = __shfl_sync(0xffffffffu, base, leader);
+                                    }
+                                    if (pa) {
+                                        const uint32_t before = __popc(m & ((1u << lane) - 1u));
+                                        const unsigned long long slot = S.base[av] + base + before;
+                                        a.bucket[slot] = Prop{
+                                            dd, e_b, prop_key(a.fast_key, row_b, pidx, e_b, outer == q_a ? 0u : 1u)};
+                                    }
+                                }
+                                if (ok && dd < kth_b) {
+                                    const uint32_t pos = wl ? cnt_r++ : atomicAdd(&S.cnt[tid], 1u);
+                                    const unsigned long long slot = S.base[tid] + pos;
                                     a.bucket[slot] = Prop{
-                                        dd, e_b, prop_key(a.fast_key, row_b, pidx, e_b, outer == q_a ? 0u : 1u)};
+                                        dd, e_a, prop_key(a.fast_key, row_b, pidx, e_a, outer == q_b ? 0u : 1u)};
                                 }
-                            }
-                            if (ok && dd < kth_b) {
-                                const uint32_t pos = wl ? cnt_r++ : atomicAdd(&S.cnt[tid], 1u);
-                                const unsigned long long slot = S.base[tid] + pos;
-                                a.bucket[slot] = Prop{
-                                    dd, e_a, prop_key(a.fast_key, row_b, pidx, e_a, outer == q_b ? 0u : 1u)};
                             }
                         }
                     }
                 }
-            }
+            };
+            if (wl_tile) pairs(std::true_type{});
+            else pairs(std::false_type{});
             if (PASS == 0) {
-                if (wl)
+                if (wl_tile)
                     S.cnt[tid] = cnt_r + cb;
                 else if (cb)
                     atomicAdd(&S.cnt[tid], cb);
