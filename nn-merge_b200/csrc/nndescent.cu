@@ -614,42 +614,55 @@ __global__ void __launch_bounds__(TIER_THREADS[NTIER - 1]) k_pairs_u8(JoinArgs a
 // tensor-core join active, only the rows of the last tier have stored pairs.
 constexpr int EMIT_WARPS = 4;
 
-__global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t idx = blockIdx.x * EMIT_WARPS + w;
-    uint32_t row = idx;
-    if (a.tc) {
-        if (idx >= a.ctr->ntier[NTIER - 1]) return;
-        row = a.tier_rows[(size_t)(NTIER - 1) * a.n + idx];
-    } else if (row >= a.n) {
-        return;
-    }
-    const uint32_t nn = a.newlen[row], no = a.oldlen[row], S = nn + no;
-    if (nn == 0) return;
-    const uint32_t R = a.caps;
-    unsigned char* base = smem + (size_t)w * R * 24;
-    unsigned long long* s_base = reinterpret_cast<unsigned long long*>(base);
-    uint32_t* s_ids = reinterpret_cast<uint32_t*>(s_base + R);
-    float* s_kth = reinterpret_cast<float*>(s_ids + R);
-    uint32_t* s_cur = reinterpret_cast<uint32_t*>(s_kth + R);
-    uint32_t* s_grp = s_cur + R;
+// Members of one row (bucket bases, ids, K-th distances, cursors, groups)
+// in shared memory, 24 bytes a list slot; false when no pair of the row
+// passed the filter.  `first`/`step` split the slots over the threads.
+struct EmitRow {
+    unsigned long long* base;
+    uint32_t *ids, *cur, *grp;
+    float* kth;
+};
+
+__device__ __forceinline__ EmitRow emit_row_smem(unsigned char* p, uint32_t R) {
+    EmitRow m;
+    m.base = reinterpret_cast<unsigned long long*>(p);
+    m.ids = reinterpret_cast<uint32_t*>(m.base + R);
+    m.kth = reinterpret_cast<float*>(m.ids + R);
+    m.cur = reinterpret_cast<uint32_t*>(m.kth + R);
+    m.grp = m.cur + R;
+    return m;
+}
+
+__device__ __forceinline__ bool emit_load_row(const JoinArgs& a, uint32_t row, uint32_t nn, uint32_t S,
+                                              EmitRow m, uint32_t first, uint32_t step) {
     bool any_c = false;
-    for (uint32_t q = lane; q < S; q += 32) {
+    for (uint32_t q = first; q < S; q += step) {
         uint32_t e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
         uint32_t id = e & LID_MASK;
-        s_ids[q] = e;
-        s_kth[q] = a.pdist[(size_t)id * a.K + a.K - 1];
-        s_cur[q] = 0;
-        s_grp[q] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
+        m.ids[q] = e;
+        m.kth[q] = a.pdist[(size_t)id * a.K + a.K - 1];
+        m.cur[q] = 0;
+        m.grp[q] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
         uint32_t c = a.cntpos[(size_t)row * a.caps + q];
-        if (c) s_base[q] = a.boff[id] + atomicAdd(&a.bcur[id], c);
+        if (c) m.base[q] = a.boff[id] + atomicAdd(&a.bcur[id], c);
         any_c |= c != 0;
     }
-    if (!__any_sync(FULL, any_c)) return;  // no pair of this row passed the filter
-    __syncwarp();
+    return any_c;
+}
+
+// Proposals of the pairs (av, bv) of a row with av = av0, av0 + av_step, ...
+// (a warp's share), lanes over bv.
+__device__ __forceinline__ void emit_pairs(const JoinArgs& a, uint32_t row, uint32_t nn, uint32_t no,
+                                           EmitRow m, uint32_t av0, uint32_t av_step) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t S = nn + no;
+    const unsigned long long* s_base = m.base;
+    const uint32_t* s_ids = m.ids;
+    const float* s_kth = m.kth;
+    uint32_t* s_cur = m.cur;
+    const uint32_t* s_grp = m.grp;
     const float* pd = a.pd + a.poff[row];
-    for (uint32_t av = 0; av < nn; av++) {
+    for (uint32_t av = av0; av < nn; av += av_step) {
         for (uint32_t bv = av + 1 + lane; bv < S; bv += 32) {
             uint32_t outer, inner;
             if (!pair_order(a.mode, a.verse, av, bv, nn, s_ids[av], s_ids[bv], s_grp[av], s_grp[bv], outer, inner))
@@ -666,6 +679,37 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
             }
         }
     }
+}
+
+// FP32 join: a warp per row.
+__global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t row = blockIdx.x * EMIT_WARPS + w;
+    if (row >= a.n) return;
+    const uint32_t nn = a.newlen[row], no = a.oldlen[row];
+    if (nn == 0) return;
+    const EmitRow m = emit_row_smem(smem + (size_t)w * a.caps * 24, a.caps);
+    if (!__any_sync(FULL, emit_load_row(a, row, nn, nn + no, m, lane, 32))) return;
+    __syncwarp();
+    emit_pairs(a, row, nn, no, m, 0, 1);
+}
+
+// Rows of the last tier next to the tensor-core join (lists of more than
+// 128 entries, up to caps^2 / 2 pairs each, a few thousand rows): a block
+// per row, its warps taking the outer entries in turn, so that no row is a
+// single warp's long chain of loads.
+constexpr int EMIT_ROW_WARPS = 8;
+
+__global__ void __launch_bounds__(EMIT_ROW_WARPS * 32) k_emit_rows(JoinArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (blockIdx.x >= a.ctr->ntier[NTIER - 1]) return;
+    const uint32_t row = a.tier_rows[(size_t)(NTIER - 1) * a.n + blockIdx.x];
+    const uint32_t nn = a.newlen[row], no = a.oldlen[row];
+    if (nn == 0) return;
+    const EmitRow m = emit_row_smem(smem, a.caps);
+    if (!__syncthreads_or(emit_load_row(a, row, nn, nn + no, m, threadIdx.x, blockDim.x))) return;
+    emit_pairs(a, row, nn, no, m, threadIdx.x >> 5, EMIT_ROW_WARPS);
 }
 
 // ---------------------------------------------------------------------------
@@ -991,6 +1035,9 @@ static cudaError_t prep_pairs(uint32_t caps, uint32_t dp, size_t emit_smem, int 
                                                      (int)pairs_smem(TIER_CAP[3], dp, true))) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_pairs<M, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)pairs_smem(caps, dp, false))) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_emit_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(caps * 24 + 64))) !=
+        cudaSuccess)
+        return e;
     return cudaFuncSetAttribute(k_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)emit_smem);
 }
 
@@ -1261,9 +1308,13 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         // stored distances
         if (ctx.prof) cudaEventRecord(ctx.ev[2], st);
         if (tc) NNM_CUDA_TRY(launch_join_tc(1, ja, ntier, nsm, st));
-        const unsigned emit_rows = tc ? ntier[NTIER - 1] : n;
-        if (emit_rows) {
-            k_emit<<<(emit_rows + EMIT_WARPS - 1) / EMIT_WARPS, EMIT_WARPS * 32, emit_smem, st>>>(ja); count_launch();
+        if (tc ? ntier[NTIER - 1] > 0 : n > 0) {
+            if (tc) {
+                k_emit_rows<<<ntier[NTIER - 1], EMIT_ROW_WARPS * 32, (size_t)caps * 24 + 64, st>>>(ja);
+            } else {
+                k_emit<<<(n + EMIT_WARPS - 1) / EMIT_WARPS, EMIT_WARPS * 32, emit_smem, st>>>(ja);
+            }
+            count_launch();
         }
         MergeArgs ma{g.pid, g.pdist, n, K, P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff),
                      P<Prop>(ws.bucket), P<uint8_t>(ws.nflag), ctr};
