@@ -607,7 +607,7 @@ def main():
     hbm, peak_kind = peaks()
     names = {"join": ("local-join count pass: k_join_tc<0> (u8 Gram tiles on tcgen05) + FP32 k_pairs for lists > 128"
                       if a.join != "fp32" else "local-join pair distances (FP32 k_pairs, all tiers)"),
-             "emit": ("local-join emit pass: k_join_tc<1> + k_emit" if a.join != "fp32" else "proposal emit (k_emit)"),
+             "emit": ("local-join emit pass: k_join_tc<1> + k_emit_rows" if a.join != "fp32" else "proposal emit (k_emit)"),
              "merge": "top-K merge (k_merge)"}
     dom = max(("join", "emit", "merge"), key=lambda c: prof[c]["ms"])
     j = prof[dom]
