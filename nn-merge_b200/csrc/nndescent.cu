@@ -615,8 +615,7 @@ __global__ void __launch_bounds__(TIER_THREADS[NTIER - 1]) k_pairs_u8(JoinArgs a
 constexpr int EMIT_WARPS = 4;
 
 // Members of one row (bucket bases, ids, K-th distances, cursors, groups)
-// in shared memory, 24 bytes a list slot; false when no pair of the row
-// passed the filter.  `first`/`step` split the slots over the threads.
+// in shared memory, 24 bytes a list slot.
 struct EmitRow {
     unsigned long long* base;
     uint32_t *ids, *cur, *grp;
@@ -633,6 +632,8 @@ __device__ __forceinline__ EmitRow emit_row_smem(unsigned char* p, uint32_t R) {
     return m;
 }
 
+// Loads the members of list slots first, first + step, ... and reserves
+// their bucket ranges; false when no pair of the row passed the filter.
 __device__ __forceinline__ bool emit_load_row(const JoinArgs& a, uint32_t row, uint32_t nn, uint32_t S,
                                               EmitRow m, uint32_t first, uint32_t step) {
     bool any_c = false;
