@@ -82,6 +82,32 @@ def test_all_tiers_and_big_lists(ctx, d):
     assert big["tiers"][4] > 0 and small["tiers"][0] > 0
 
 
+@pytest.mark.parametrize("rng", ["exact", "fast"])
+def test_big_lists_in_merges(ctx, rng):
+    # lists above 128 entries in the merge builders: their group and verse
+    # filters on the staged u8 pair kernel and the block-per-row emit
+    x = gaussian_mixture_u8(4000, seed=41, n_centres=8)
+    t, f, rows = both(ctx, ctx.merge_leaves, x, 32, [1000] * 4, seed=5, rng=rng, sample_cap=400)
+    same(t, f)
+    assert rows["tiers"][4] > 0
+    t, f, rows = both(ctx, ctx.jmerge, x, 32, seed=6, rng=rng, sample_cap=400)
+    same(t, f)
+    assert rows["tiers"][4] > 0
+
+
+def test_big_lists_in_hmerge(ctx):
+    x = gaussian_mixture_u8(4000, seed=42, n_centres=8)
+    ctx.profile(True)
+    t = ctx.hmerge(x, 16, 8, seed=9, join="tensor", sample_cap=400)
+    rows = ctx.profile_stats()["rows"]
+    ctx.profile(False)
+    f = ctx.hmerge(x, 16, 8, seed=9, join="fp32", sample_cap=400)
+    same(t, f)
+    assert rows["tiers"][4] > 0
+    for a, b in zip(t["layers"], f["layers"]):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
 @pytest.mark.parametrize("d", [1, 8, 37, 96, 200])
 def test_ragged_dims(ctx, d):
     x = gaussian_mixture_u8(3000, d=d, seed=37 + d)
