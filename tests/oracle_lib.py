@@ -174,6 +174,13 @@ class Oracle:
                                ctypes.c_uint32(n), _p(out, ctypes.c_uint32))
         return out
 
+    def dist(self, x, i, j, metric="l2"):
+        """The reference's distance of rows i and j of x (its sequential float sum)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        self.lib.nno_dist.restype = ctypes.c_float
+        return self.lib.nno_dist(_p(x, ctypes.c_float), ctypes.c_uint64(i), _p(x, ctypes.c_float),
+                                 ctypes.c_uint64(j), ctypes.c_uint32(x.shape[1]), ctypes.c_int(METRICS[metric]))
+
     def sort_pool(self, ids, dists, flags):
         ids = np.ascontiguousarray(ids, np.uint32).copy()
         dists = np.ascontiguousarray(dists, np.float32).copy()
