@@ -146,7 +146,9 @@ __device__ __forceinline__ bool group_any(uint32_t id, bool p) {
 // So the loads of tile k+1 overlap the MMA and epilogue of tile k.  Every
 // mbarrier wait is bounded; a group decides to stop with a barrier-OR over
 // its threads, and the other group then times out on its next wait.
-template <int PASS, int KIND>
+// PASS 0 counts, PASS 1 writes the proposals (FAST: the fast tier's 8-byte
+// form); KIND 0: u8 operands, 1: BF16 with the exact recheck.
+template <int PASS, int KIND, bool FAST>
 __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ TcShared sh;
@@ -396,15 +398,13 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                                     if (pa) {
                                         const uint32_t before = __popc(m & ((1u << lane) - 1u));
                                         const unsigned long long slot = S.base[av] + base + before;
-                                        a.bucket[slot] = Prop{
-                                            dd, e_b, prop_key(a.fast_key, row_b, pidx, e_b, outer == q_a ? 0u : 1u)};
+                                        put_prop<FAST>(a.bucket, slot, dd, e_b, row_b, pidx, outer == q_a ? 0u : 1u);
                                     }
                                 }
                                 if (ok && dd < kth_b) {
                                     const uint32_t pos = wl ? cnt_r++ : atomicAdd(&S.cnt[tid], 1u);
                                     const unsigned long long slot = S.base[tid] + pos;
-                                    a.bucket[slot] = Prop{
-                                        dd, e_a, prop_key(a.fast_key, row_b, pidx, e_a, outer == q_b ? 0u : 1u)};
+                                    put_prop<FAST>(a.bucket, slot, dd, e_a, row_b, pidx, outer == q_b ? 0u : 1u);
                                 }
                             }
                         }
@@ -597,14 +597,13 @@ int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
 cudaError_t tc_set_attributes(uint32_t kq, uint32_t kind) {
     const int bytes = (int)std::max<size_t>(tc_smem_bytes(kq), TC_SMEM_FLOOR);
     cudaError_t e;
-    if (kind == 0) {
-        e = cudaFuncSetAttribute(k_join_tc<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        if (e != cudaSuccess) return e;
-        return cudaFuncSetAttribute(k_join_tc<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    }
-    e = cudaFuncSetAttribute(k_join_tc<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_join_tc<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    const void* fns[2][3] = {{(const void*)k_join_tc<0, 0, false>, (const void*)k_join_tc<1, 0, false>,
+                              (const void*)k_join_tc<1, 0, true>},
+                             {(const void*)k_join_tc<0, 1, false>, (const void*)k_join_tc<1, 1, false>,
+                              (const void*)k_join_tc<1, 1, true>}};
+    for (const void* f : fns[kind ? 1 : 0])
+        if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
+    return cudaSuccess;
 }
 
 cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, int nsm, cudaStream_t st) {
@@ -613,12 +612,15 @@ cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, 
     if (!tiles) return cudaSuccess;
     const unsigned grid = std::min<unsigned>(tiles, (unsigned)nsm * 4);
     const size_t bytes = std::max<size_t>(tc_smem_bytes(ja.kq), TC_SMEM_FLOOR);
+    const bool fast = ja.fast_key != 0;
     if (ja.tc_kind == 0) {
-        if (pass == 0) k_join_tc<0, 0><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else k_join_tc<1, 0><<<grid, TC_THREADS, bytes, st>>>(ja);
+        if (pass == 0) k_join_tc<0, 0, false><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else if (fast) k_join_tc<1, 0, true><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else k_join_tc<1, 0, false><<<grid, TC_THREADS, bytes, st>>>(ja);
     } else {
-        if (pass == 0) k_join_tc<0, 1><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else k_join_tc<1, 1><<<grid, TC_THREADS, bytes, st>>>(ja);
+        if (pass == 0) k_join_tc<0, 1, false><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else if (fast) k_join_tc<1, 1, true><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else k_join_tc<1, 1, false><<<grid, TC_THREADS, bytes, st>>>(ja);
     }
     count_launch();
     return cudaGetLastError();

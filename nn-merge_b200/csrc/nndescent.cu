@@ -652,7 +652,8 @@ __device__ __forceinline__ bool emit_load_row(const JoinArgs& a, uint32_t row, u
 }
 
 // Proposals of the pairs (av, bv) of a row with av = av0, av0 + av_step, ...
-// (a warp's share), lanes over bv.
+// (a warp's share), lanes over bv; FAST: the fast tier's 8-byte form.
+template <bool FAST>
 __device__ __forceinline__ void emit_pairs(const JoinArgs& a, uint32_t row, uint32_t nn, uint32_t no,
                                            EmitRow m, uint32_t av0, uint32_t av_step) {
     const int lane = threadIdx.x & 31;
@@ -672,11 +673,11 @@ __device__ __forceinline__ void emit_pairs(const JoinArgs& a, uint32_t row, uint
             const uint32_t pidx = outer * S + inner;
             if (dd < s_kth[outer]) {
                 unsigned long long slot = s_base[outer] + atomicAdd(&s_cur[outer], 1u);
-                a.bucket[slot] = Prop{dd, s_ids[inner], prop_key(a.fast_key, row, pidx, s_ids[inner], 0)};
+                put_prop<FAST>(a.bucket, slot, dd, s_ids[inner], row, pidx, 0);
             }
             if (dd < s_kth[inner]) {
                 unsigned long long slot = s_base[inner] + atomicAdd(&s_cur[inner], 1u);
-                a.bucket[slot] = Prop{dd, s_ids[outer], prop_key(a.fast_key, row, pidx, s_ids[outer], 1)};
+                put_prop<FAST>(a.bucket, slot, dd, s_ids[outer], row, pidx, 1);
             }
         }
     }
@@ -693,7 +694,8 @@ __global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
     const EmitRow m = emit_row_smem(smem + (size_t)w * a.caps * 24, a.caps);
     if (!__any_sync(FULL, emit_load_row(a, row, nn, nn + no, m, lane, 32))) return;
     __syncwarp();
-    emit_pairs(a, row, nn, no, m, 0, 1);
+    if (a.fast_key) emit_pairs<true>(a, row, nn, no, m, 0, 1);
+    else emit_pairs<false>(a, row, nn, no, m, 0, 1);
 }
 
 // Rows of the last tier next to the tensor-core join (lists of more than
@@ -710,7 +712,8 @@ __global__ void __launch_bounds__(EMIT_ROW_WARPS * 32) k_emit_rows(JoinArgs a) {
     if (nn == 0) return;
     const EmitRow m = emit_row_smem(smem, a.caps);
     if (!__syncthreads_or(emit_load_row(a, row, nn, nn + no, m, threadIdx.x, blockDim.x))) return;
-    emit_pairs(a, row, nn, no, m, threadIdx.x >> 5, EMIT_ROW_WARPS);
+    if (a.fast_key) emit_pairs<true>(a, row, nn, no, m, threadIdx.x >> 5, EMIT_ROW_WARPS);
+    else emit_pairs<false>(a, row, nn, no, m, threadIdx.x >> 5, EMIT_ROW_WARPS);
 }
 
 // ---------------------------------------------------------------------------
@@ -721,7 +724,7 @@ struct MergeArgs {
     uint32_t n, K;
     const uint32_t* bcnt;
     const uint64_t* boff;
-    const Prop* bucket;
+    const void* bucket;  // Prop (exact tier) or Prop8 (fast tier) entries
     uint8_t* nflag;
     IterCounters* ctr;
 };
@@ -856,7 +859,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
             }
             uint32_t kd = __shfl_sync(FULL, cd, K - 1);
             unsigned long long kk = __shfl_sync(FULL, ck, K - 1);
-            const Prop* bp = a.bucket + a.boff[t];
+            const unsigned long long b_first = a.boff[t];
             const unsigned lt = (1u << lane) - 1u;
             uint32_t nb = 0;  // entries in buf
             auto flush = [&]() {
@@ -889,7 +892,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
                 } else {
                     bool valid = false;
                     if (b0 + lane < c) {
-                        Prop p = bp[b0 + lane];
+                        const Prop p = reinterpret_cast<const Prop*>(a.bucket)[b_first + b0 + lane];
                         pd = __float_as_uint(p.dist);
                         pk = p.key;
                         pe = (p.idg & LID_MASK) | ((p.idg >> 31) << 30) | FLAG_BIT;
@@ -922,6 +925,156 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
         }
         if (lane == 0) a.nflag[t] = (uint8_t)nfl;
     }
+}
+
+// Fast-tier merge.  A fast-tier key is a function of the entry (fast_key),
+// so an entry and its order fit one 64-bit word:
+//   dist bits (63..32) | id (31..2) | new flag (1) | group bit ^ 1 (0)
+// and the words order as (distance, id, ...) (distances are non-negative,
+// so their bits order as the floats).  Copies of an entry -- the same id at
+// the same distance -- are adjacent in sorted order, one already in the pool
+// (flag 0) before a proposal, proposals of group 1 before group 0 (as
+// fast_key orders them); the first copy is kept.  The start pool is keyed
+// the same way: entries of equal distance order by id, not by their
+// previous position, and a proposal equal in distance to a pool entry of a
+// larger id precedes it -- deterministic, as the tier requires.
+__device__ __forceinline__ unsigned long long fm_word(uint32_t dist_bits, uint32_t pool_word) {
+    return ((unsigned long long)dist_bits << 32) | ((pool_word & ID_MASK) << 2) | ((pool_word >> 31) << 1) |
+           (((pool_word >> 30) & 1u) ^ 1u);
+}
+
+__device__ __forceinline__ uint32_t fm_pool_word(unsigned long long v) {
+    const uint32_t lo = (uint32_t)v;
+    return ((lo >> 2) & ID_MASK) | (((lo & 1u) ^ 1u) << 30) | (((lo >> 1) & 1u) << 31);
+}
+
+// Ascending bitonic sort of one word per lane.
+__device__ __forceinline__ unsigned long long fm_sort32(unsigned long long v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(FULL, v, j);
+            const bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
+            v = take_min ? min(v, o) : max(v, o);
+        }
+    return v;
+}
+
+// Ascending order of a bitonic sequence of one word per lane.
+__device__ __forceinline__ unsigned long long fm_bitonic_merge32(unsigned long long v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(FULL, v, j);
+        v = (lane & j) ? max(v, o) : min(v, o);
+    }
+    return v;
+}
+
+constexpr unsigned long long FM_EMPTY = ~0ull;
+
+// The pool (sorted words in lanes < K, FM_EMPTY above) merged with a buffer
+// of up to 32 proposal words (FM_EMPTY padded): the K smallest distinct
+// entries of both.  `stage` is the warp's 64-word shared scratch.
+__device__ __forceinline__ unsigned long long fm_flush(unsigned long long pool, unsigned long long buf, uint32_t K,
+                                                       unsigned long long* stage) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    buf = fm_sort32(buf);
+    const unsigned long long br = __shfl_sync(FULL, buf, 31 - lane);
+    // lo: the 32 smallest words of both (a bitonic sequence), hi: the rest
+    unsigned long long lo = min(pool, br), hi = max(pool, br);
+    lo = fm_bitonic_merge32(lo);
+    unsigned long long prev = __shfl_up_sync(FULL, lo, 1);
+    const bool keep = lo != FM_EMPTY && (lane == 0 || (prev >> 2) != (lo >> 2));
+    const unsigned m = __ballot_sync(FULL, keep);
+    const uint32_t r = __popc(m & lt);
+    if (keep && r < K) stage[r] = lo;
+    uint32_t got = __popc(m);
+    if (got < K) {  // copies among the 32 smallest: take entries of hi too
+        hi = fm_bitonic_merge32(hi);
+        const unsigned long long last_lo = __shfl_sync(FULL, lo, 31);
+        prev = __shfl_up_sync(FULL, hi, 1);
+        if (lane == 0) prev = last_lo;
+        const bool keep2 = hi != FM_EMPTY && (prev >> 2) != (hi >> 2);
+        const unsigned m2 = __ballot_sync(FULL, keep2);
+        const uint32_t r2 = got + __popc(m2 & lt);
+        if (keep2 && r2 < K) stage[r2] = hi;
+        got += __popc(m2);
+    }
+    __syncwarp();
+    const unsigned long long out = (lane < (int)K && (uint32_t)lane < got) ? stage[lane] : FM_EMPTY;
+    __syncwarp();
+    return out;
+}
+
+// One warp per target, as k_merge, on the fast tier's 8-byte proposals.
+__global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a) {
+    __shared__ unsigned long long buf[MERGE_WARPS][32];
+    __shared__ unsigned long long stage[MERGE_WARPS][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t t = blockIdx.x * MERGE_WARPS + w;
+    if (t >= a.n) return;
+    const uint32_t K = a.K;
+    const uint32_t c = a.bcnt[t];
+    uint32_t nfl = 0;
+    if (c) {
+        unsigned long long pool = FM_EMPTY;
+        if (lane < (int)K)
+            pool = fm_word(__float_as_uint(a.pdist[(size_t)t * K + lane]), a.pid[(size_t)t * K + lane]);
+        // the start pool in word order (entries of equal distance by id);
+        // a pool the previous merge wrote is in that order already
+        const unsigned long long pprev = __shfl_up_sync(FULL, pool, 1);
+        if (!__all_sync(FULL, lane == 0 || pprev <= pool)) pool = fm_sort32(pool);
+        unsigned long long kth = __shfl_sync(FULL, pool, K - 1);
+        const uint2* bp = reinterpret_cast<const uint2*>(a.bucket) + a.boff[t];
+        const unsigned lt = (1u << lane) - 1u;
+        uint32_t nb = 0;
+        for (uint32_t b0 = 0;; b0 += 32) {
+            unsigned long long v = FM_EMPTY;
+            bool rest = false;
+            const bool last = b0 >= c;
+            if (last) {
+                if (nb == 0) break;
+            } else {
+                bool valid = false;
+                if (b0 + lane < c) {
+                    const uint2 p = bp[b0 + lane];
+                    // a new entry: flag 1, group bit from the list entry
+                    v = ((unsigned long long)p.x << 32) | ((p.y & ID_MASK) << 2) | 2u | ((p.y >> 31) ^ 1u);
+                    valid = v < kth;
+                }
+                const unsigned vb = __ballot_sync(FULL, valid);
+                if (!vb) continue;
+                const uint32_t take = min((uint32_t)__popc(vb), 32u - nb);
+                const uint32_t rank = __popc(vb & lt);
+                if (valid && rank < take) buf[w][nb + rank] = v;
+                __syncwarp();
+                nb += take;
+                if (nb < 32) continue;
+                rest = valid && rank >= take;
+            }
+            const unsigned long long bv = lane < (int)nb ? buf[w][lane] : FM_EMPTY;
+            __syncwarp();
+            pool = fm_flush(pool, bv, K, stage[w]);
+            kth = __shfl_sync(FULL, pool, K - 1);
+            nb = 0;
+            if (last) break;
+            rest = rest && v < kth;  // the rest of this chunk, against the new K-th entry
+            const unsigned rb = __ballot_sync(FULL, rest);
+            if (rest) buf[w][__popc(rb & lt)] = v;
+            __syncwarp();
+            nb = __popc(rb);
+        }
+        if (lane < (int)K) {
+            a.pid[(size_t)t * K + lane] = fm_pool_word(pool);
+            a.pdist[(size_t)t * K + lane] = __uint_as_float((uint32_t)(pool >> 32));
+        }
+        nfl = __popc(__ballot_sync(FULL, lane < (int)K && (pool & 2ull)));
+    }
+    if (lane == 0) a.nflag[t] = (uint8_t)nfl;
 }
 
 // Total of the per-row flag counts (the warps of k_merge finish unevenly, so
@@ -1100,7 +1253,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     NNM_CUDA_TRY(ws.nflag.ensure(n1));
     NNM_CUDA_TRY(ws.scan_tmp.ensure((scan_temp_elems(n1) + 8) * 8));
     NNM_CUDA_TRY(ws.counters.ensure(sizeof(IterCounters) + 64));
-    if (ws.bucket.bytes < (size_t)n * K * 4 * sizeof(Prop)) NNM_CUDA_TRY(ws.bucket.ensure((size_t)n * K * 4 * sizeof(Prop)));
+    const size_t prop_bytes = g.fast ? sizeof(Prop8) : sizeof(Prop);  // the tier's proposal format
+    if (ws.bucket.bytes < (size_t)n * K * 4 * prop_bytes) NNM_CUDA_TRY(ws.bucket.ensure((size_t)n * K * 4 * prop_bytes));
 
     uint32_t *rcnt_new = P<uint32_t>(ws.rcnt), *rcnt_old = rcnt_new + n1;
     uint32_t *rcur_new = P<uint32_t>(ws.rcur), *rcur_old = rcur_new + n1;
@@ -1287,7 +1441,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         JoinArgs ja{g.x, g.dp, K, n, g.pdist, g.newL, g.oldL, g.newlen, g.oldlen, g.capn, g.capo, caps,
                     (uint32_t)mode, verse, d_leaf_off, nleaf, P<uint32_t>(ws.tiers), P<uint64_t>(ws.poff),
                     P<float>(ws.pd), P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
-                    P<uint64_t>(ws.boff), P<Prop>(ws.bucket), ctr,
+                    P<uint64_t>(ws.boff), ws.bucket.p, ctr,
                     g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error, tc ? P<uint32_t>(ws.erows) : nullptr,
                     g.fast ? 1u : 0u, g.tc_kind, g.err_c};
         if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
@@ -1301,9 +1455,9 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
         NNM_CUDA_TRY(cudaStreamSynchronize(st));
         const uint64_t nprop = ctx.h_counters->proposals;
-        if (nprop * sizeof(Prop) > ws.bucket.bytes) {
-            NNM_CUDA_TRY(ws.bucket.ensure((size_t)(nprop * 1.25 + 1024) * sizeof(Prop)));
-            ja.bucket = P<Prop>(ws.bucket);
+        if (nprop * prop_bytes > ws.bucket.bytes) {
+            NNM_CUDA_TRY(ws.bucket.ensure((size_t)(nprop * 1.25 + 1024) * prop_bytes));
+            ja.bucket = ws.bucket.p;
         }
         // pass 2: proposals, recomputed on the tensor cores or read from the
         // stored distances
@@ -1318,9 +1472,11 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             count_launch();
         }
         MergeArgs ma{g.pid, g.pdist, n, K, P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff),
-                     P<Prop>(ws.bucket), P<uint8_t>(ws.nflag), ctr};
+                     ws.bucket.p, P<uint8_t>(ws.nflag), ctr};
         if (ctx.prof) cudaEventRecord(ctx.ev[3], st);
-        k_merge<<<(n + MERGE_WARPS - 1) / MERGE_WARPS, MERGE_WARPS * 32, 0, st>>>(ma); count_launch();
+        if (g.fast) k_merge_fast<<<(n + MERGE_WARPS - 1) / MERGE_WARPS, MERGE_WARPS * 32, 0, st>>>(ma);
+        else k_merge<<<(n + MERGE_WARPS - 1) / MERGE_WARPS, MERGE_WARPS * 32, 0, st>>>(ma);
+        count_launch();
         k_sum_flags<<<std::min<unsigned>((n + 255) / 256, (unsigned)nsm * 4), 256, 0, st>>>(P<uint8_t>(ws.nflag), n, ctr); count_launch();
         if (ctx.prof) cudaEventRecord(ctx.ev[4], st);
         NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
@@ -1362,10 +1518,10 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             ctx.kemit.launches += tc ? 1 + (hc.ntier[4] > 0) : 1;
             ctx.kemit.ms += t23;
             ctx.kemit.bytes += (double)hc.pairs * 4.0 + s_f32 * 18.0 + s_tc * ((double)g.kq + 22.0) +
-                               (double)hc.proposals * 16.0;
+                               (double)hc.proposals * (double)prop_bytes;
             ctx.kmerge.launches += 1;
             ctx.kmerge.ms += t34;
-            ctx.kmerge.bytes += (double)n * K * 16.0 + (double)hc.proposals * 16.0 + (double)n * 13.0;
+            ctx.kmerge.bytes += (double)n * K * 16.0 + (double)hc.proposals * (double)prop_bytes + (double)n * 13.0;
         }
         g.gpos += hc.rand_draws;
         g.ncmps += hc.ncmps;

@@ -35,7 +35,7 @@ struct JoinArgs {
     uint16_t* cntpos;
     uint32_t *bcnt, *bcur;
     const uint64_t* boff;
-    Prop* bucket;
+    void* bucket;               // Prop (exact tier) or Prop8 (fast tier) entries
     IterCounters* ctr;
     // tensor-core join: the operand copy of the vectors (kq bytes a row,
     // zero padded; u8 or BF16 by tc_kind) and their squared norms (u32
@@ -50,21 +50,27 @@ struct JoinArgs {
     float err_c;          // BF16: |approx - reference distance| <= err_c * (|a|^2 + |b|^2)
 };
 
-// Tie-break key of the proposal "target gets `other`" from the join of
-// `row`.  Exact tier: the reference's sequential insert order (the pair's
-// index in join order, then the side: 0 = into the outer element's pool).
-// Fast tier: the other element's id in place of the pair index, so that the
-// graphs do not depend on the order of the sample lists, and in place of
-// the side (which a pair listed once does not need) the other list entry's
-// group bit, set first: when a row's lists hold an id twice with different
-// group bits, the two copies' proposals then order by key rather than by
-// their arrival in the bucket, and the merge keeps the first.
-__device__ __forceinline__ unsigned long long prop_key(uint32_t fast, uint32_t row, uint32_t pair_idx,
-                                                       uint32_t other_word, uint32_t side) {
-    const uint32_t other_id = other_word & 0x7fffffffu;
-    const uint32_t tie = fast ? ((other_word >> 31) ^ 1u) : side;
-    return (1ull << 63) | ((unsigned long long)row << 32) |
-           ((unsigned long long)(fast ? other_id : pair_idx) << 1) | tie;
+// Tie-break key of the exact tier's proposal "target gets the other entry"
+// from the join of `row`: the reference's sequential insert order (the
+// row, the pair's index in join order, then the side: 0 = into the outer
+// element's pool).  The fast tier's key (fast_key, nnm_nnd.h) is the other
+// entry's id and group bit alone, so that the graphs do not depend on the
+// order of the sample lists nor on which row proposed a pair: copies of a
+// proposal are equal in (distance, key) and the merge keeps one; when a
+// row's lists hold an id twice with different group bits, the copies order
+// by the group bit rather than by their arrival in the bucket.
+__device__ __forceinline__ unsigned long long prop_key(uint32_t row, uint32_t pair_idx, uint32_t side) {
+    return (1ull << 63) | ((unsigned long long)row << 32) | ((unsigned long long)pair_idx << 1) | side;
+}
+
+// Writes proposal number `slot` of the bucket array in the tier's format.
+template <bool FAST>
+__device__ __forceinline__ void put_prop(void* bucket, unsigned long long slot, float dist, uint32_t idg,
+                                         uint32_t row, uint32_t pair_idx, uint32_t side) {
+    if (FAST)
+        reinterpret_cast<uint2*>(bucket)[slot] = make_uint2(__float_as_uint(dist), idg);
+    else
+        reinterpret_cast<Prop*>(bucket)[slot] = Prop{dist, idg, prop_key(row, pair_idx, side)};
 }
 
 __device__ __forceinline__ uint32_t leaf_of(uint32_t id, const uint32_t* off, uint32_t nleaf) {

@@ -19,12 +19,28 @@ enum JoinMode : uint32_t {
 // A proposal "insert id into target's pool with distance dist", ordered by
 // (dist, key); key = 2^63 | row << 32 | pair index << 1 | side reproduces the
 // reference's sequential insert order (row ascending, pairs in join order,
-// first insert into the outer element's pool, then the inner's).
+// first insert into the outer element's pool, then the inner's).  Exact tier.
 struct __align__(16) Prop {
     float dist;
     uint32_t idg;  // id | group bit << 31
     unsigned long long key;
 };
+
+// The fast tier's proposal, 8 bytes: its tie-break key depends only on the
+// proposed entry (fast_key below), so the bucket holds (dist, idg) and the
+// merge derives the key -- half the bytes written by the join and read by
+// the merge.
+struct __align__(8) Prop8 {
+    float dist;
+    uint32_t idg;
+};
+
+// Key of a fast-tier proposal of list entry `idg`: the entry's id, then its
+// group bit with group 1 first; bit 63 set so that the start pool's entries
+// (keys 0..K-1) precede every proposal of equal distance.
+__host__ __device__ __forceinline__ unsigned long long fast_key(uint32_t idg) {
+    return (1ull << 63) | ((unsigned long long)(idg & 0x7fffffffu) << 1) | ((idg >> 31) ^ 1u);
+}
 
 // Per-iteration statistics read back by the host.
 struct IterCounters {
