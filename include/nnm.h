@@ -136,6 +136,53 @@ int nnm_jmerge(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, uint32_t k,
                const nnm_opts *opts, uint32_t *ids, float *dists, uint8_t *flags,
                nnm_stats *stats);
 
+/* Staged merge: the steps of Smerge::buildKGraph (smerge.cpp:46-91) and
+ * Jmerge::buildKGraph (jmerge.cpp:43-80) as separate calls on one session,
+ * for callers that drive AbstractMerge's interface (abstractmerge.h:25-37)
+ * step by step.  The session holds the vectors and the pools (the
+ * reference's MergeType egraph) on the device and behaves as one reference
+ * process: the std::rand() stream starts from srand(opts.seed) at
+ * nnm_merge_create and continues across the steps; each phase the
+ * reference seeds with time(NULL) draws from mt19937(opts.seed).  Run in
+ * the reference's order, the steps give the graphs of nnm_smerge /
+ * nnm_jmerge bit for bit.  Reference streams only (opts.rng_mode
+ * NNM_RNG_EXACT); opts.join_kernel selects the join kernel as elsewhere. */
+typedef struct nnm_merge nnm_merge;
+
+/* Which reference class's local join (and initial graph) a step runs. */
+typedef enum {
+    NNM_MERGE_SMERGE = 1, /* Smerge::localJoin (smerge.cpp:212-235): groups differ */
+    NNM_MERGE_JMERGE = 2  /* Jmerge::localJoin (jmerge.cpp:178-203): groups differ or either is 1 */
+} nnm_merge_kind;
+
+/* AbstractMerge::InitialMemory(mata, k, n, d) (abstractmerge.cpp:25-35):
+ * x is n x d row-major host memory, copied to the device. */
+int nnm_merge_create(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, uint32_t k,
+                     const nnm_opts *opts, nnm_merge **out);
+/* KGraph::buildKGraph on cutMat(mata, b, e) (smerge.cpp:56-68): NN-Descent
+ * on rows [b, e) alone, continuing the session's std::rand() stream.
+ * graph (host, may be NULL): (e - b) x k ids local to the sub-range, as the
+ * reference's buildKGraph returns them; ncmps (may be NULL): its distance
+ * evaluations. */
+int nnm_merge_subgraph(nnm_merge *m, uint32_t b, uint32_t e, uint32_t *graph, uint64_t *ncmps);
+/* AbstractMerge::InitSGraph(b, graph, gid, size) (abstractmerge.cpp:55-76):
+ * rows [b, b + size) take the host graph's local ids + b in its order,
+ * flagged new with group id gid (0 or 1), distances recomputed. */
+int nnm_merge_init_sgraph(nnm_merge *m, uint32_t b, const uint32_t *graph, uint32_t gid, uint32_t size);
+/* Smerge::InitialGraph (smerge.cpp:94-209) or Jmerge::InitialGraph
+ * (jmerge.cpp:83-176) with preSize = pre. */
+int nnm_merge_initial_graph(nnm_merge *m, uint32_t kind, uint32_t pre);
+/* AbstractMerge::nnDescent (abstractmerge.cpp:78-192) with the local join of
+ * `kind`, until the reference's convergence test passes (or opts.max_iter).
+ * stats (may be NULL): the step's distance evaluations (ncmps), its
+ * iterations and convergence means. */
+int nnm_merge_nndescent(nnm_merge *m, uint32_t kind, uint32_t pre, nnm_stats *stats);
+/* AbstractMerge::merge2one(sz) (abstractmerge.cpp:232-277): rows [0, sz). */
+int nnm_merge_merge2one(nnm_merge *m, uint32_t sz);
+/* The pools (n x k; any output may be NULL), host memory. */
+int nnm_merge_read(nnm_merge *m, uint32_t *ids, float *dists, uint8_t *flags);
+int nnm_merge_free(nnm_merge *m);
+
 /* S-Merge over `nleaf` consecutive leaves of the given sizes (sum = n): every
  * leaf is built with NN-Descent, every row keeps its best k - k/2 entries
  * and samples k/2 ids from the other leaves, and the join pairs only rows of
@@ -190,9 +237,17 @@ typedef struct {
  * (NNM_ERR_INVALID beyond them); a query needing more than 12288 candidate
  * heap entries fails the call with NNM_ERR_CAPACITY.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) and
- * caches it, so make that first call before any stream capture.  All calls
- * share the one array: calls that overlap on the GPU race and must not be
- * issued.  The call waits for its stream before returning. */
+ * caches it; under lazy module loading that first call is also where the
+ * ~16 MiB are claimed on the device, so a process with a fixed memory
+ * budget should make one warm-up call at start-up.  Every call ends by
+ * copying its counters to the host and waiting for its stream, so no call
+ * may be made while its stream is being captured into a CUDA graph.  All
+ * calls share the one array: calls that overlap on the GPU race and must
+ * not be issued.  The hierarchy is read as given and is not checked: off[g]
+ * must be non-decreasing with off[g][nrows[g]] within adj[g], and every id
+ * in adj[g] below nrows[g] (ids out of range end the call with
+ * NNM_ERR_CAPACITY after partial output; offsets out of range read out of
+ * bounds). */
 int nnm_search_noalloc(const float *x_dev, uint64_t n, uint32_t d, const nnm_dev_layers *layers,
                        const float *q_dev, uint64_t nq, uint32_t topk, uint32_t seed, uint32_t metric,
                        uint32_t *out_ids_dev, float *out_dists_dev, uint64_t *ncmps, void *stream);

@@ -5,6 +5,8 @@
 // interface follow the reference:
 //   AbstractGraph    abstractgraph.h:21-45
 //   KGraph           kgraph.h:126-150   (buildKGraph returns new unsigned[n*k])
+//   AbstractMerge    abstractmerge.h:16-40 (InitSGraph, InitialGraph,
+//                    nnDescent, localJoin, merge2one, cutMat, EvaluateDelta)
 //   Smerge, Jmerge   smerge.h:8-23, jmerge.h:7-22 (buildKGraph returns 0)
 //   LyNNDescent      lynndescent.h:19-86 (buildhgraph(src, dst, grd, K, M))
 //   LySearch         lysearch.h:23-91   (knnSearch is public here)
@@ -216,44 +218,211 @@ public:
     }
 };
 
+// One entry of a pool as the reference's merges keep it (pvetex.h:18-30).
+struct Neighbor {
+    unsigned id = 0;
+    float dist = 0.f;
+    bool flag = false;
+    unsigned gd = 0;
+};
+typedef std::vector<Neighbor> Neighbors;
+
+// AbstractMerge (abstractmerge.h:16-40) over a device session (nnm_merge_*):
+// the pools and compensation lists -- the reference's egraph -- live on the
+// device from InitialMemory on, and every step below is one call of the
+// session, in the reference's order giving the reference's graph.
+//
+// The local join runs inside nnDescent() on the device with the filter that
+// join_filter() names: Smerge's and Jmerge's (groups differ; or either
+// group is 1).  A subclass whose localJoin() is its own host code cannot
+// run on the device: its nnDescent() ends with NNM_ERR_INVALID unless it
+// also overrides join_filter() to pick one of the device filters.
 class AbstractMerge : public AbstractGraph {
+protected:
+    nnm_merge *egraph = nullptr;
+    unsigned preSize = 0;
+
+    // NNM_MERGE_SMERGE / NNM_MERGE_JMERGE, or -1: no device filter
+    virtual int join_filter() const { return -1; }
+
+    nnm_opts session_opts() const { return nnm_dropin::opts(metric); }
+
 public:
     AbstractMerge() {}
     explicit AbstractMerge(SpaceInterface<float> *func) : AbstractGraph(func) {}
+    ~AbstractMerge() override {
+        if (egraph) nnm_merge_free(egraph);
+    }
+    // AbstractMerge::InitialMemory (abstractmerge.cpp:25-35): the matrix to
+    // the device, empty pools.
+    unsigned InitialMemory(float *mata, const unsigned k, const unsigned n, const unsigned d) override {
+        AbstractGraph::InitialMemory(mata, k, n, d);
+        if (egraph) nnm_merge_free(egraph);
+        egraph = nullptr;
+        nnm_opts o = session_opts();
+        nnm_dropin::check(nnm_merge_create(nnm_dropin::context(), mata, n, d, k, &o, &egraph));
+        return 0;
+    }
+    unsigned InitialGraph() override = 0;
+    unsigned *buildKGraph(float *mata, const unsigned K, const unsigned N, const unsigned D) override = 0;
+    // abstractmerge.cpp:278-291, from the device pools
+    void saveKGraph(const char *dst) override {
+        if (egraph) {
+            ids_.resize((size_t)row * K0);
+            nnm_dropin::check(nnm_merge_read(egraph, ids_.data(), nullptr, nullptr));
+        }
+        AbstractGraph::saveKGraph(dst);
+    }
+    // AbstractMerge::nnDescent (abstractmerge.cpp:78-192): sampling,
+    // shuffles, this class's local join and the convergence test, repeated
+    // on the device until the reference's test passes.
+    virtual unsigned nnDescent() {
+        const int f = join_filter();
+        if (f < 0) {
+            std::cout << "nnm: this class's localJoin() has no device form (override join_filter())" << std::endl;
+            nnm_dropin::check(NNM_ERR_INVALID);
+        }
+        nnm_stats st;
+        nnm_dropin::check(nnm_merge_nndescent(egraph, (uint32_t)f, preSize, &st));
+        nCmps += st.ncmps;
+        return 0;
+    }
+    // The local join of one iteration runs inside nnDescent() (the only
+    // place the reference calls it, abstractmerge.cpp:168); called on its
+    // own there are no sample lists to join and it returns 0.
+    virtual unsigned localJoin() = 0;
+    void setdisfunc(SpaceInterface<float> *func) override = 0;
+    // AbstractMerge::EvaluateDelta (abstractmerge.cpp:194-202): the share
+    // of new entries among the first K of a pool.
+    float EvaluateDelta(Neighbors &pool, unsigned K) {
+        unsigned c = 0, N = K;
+        if (pool.size() < N) N = (unsigned)pool.size();
+        for (unsigned i = 0; i < N; ++i)
+            if (pool[i].flag) ++c;
+        return float(c) / K;
+    }
+    // AbstractMerge::InitSGraph (abstractmerge.cpp:55-76): rows [b_idx,
+    // b_idx + size_data) take `graph` (local ids) with group id Gid.
+    void InitSGraph(const unsigned b_idx, unsigned *graph, unsigned Gid, unsigned size_data) {
+        nnm_dropin::check(nnm_merge_init_sgraph(egraph, b_idx, graph, Gid, size_data));
+    }
+    // KGraph::buildKGraph on rows [b_idx, l_idx) inside this merge (the
+    // reference builds a KGraph on cutMat(mata, b_idx, l_idx)): the same
+    // graph, with the merge's std::rand() stream continuing through it as
+    // the reference's process-wide stream does.  Returns new unsigned[]
+    // of local ids, as KGraph::buildKGraph.
+    unsigned *subGraph(const unsigned b_idx, const unsigned l_idx) {
+        unsigned *g = new unsigned[(size_t)(l_idx - b_idx) * K0];
+        uint64_t c = 0;
+        nnm_dropin::check(nnm_merge_subgraph(egraph, b_idx, l_idx, g, &c));
+        nCmps += c;
+        return g;
+    }
+    // AbstractMerge::merge2one (abstractmerge.cpp:232-277)
+    unsigned merge2one(const unsigned sz) {
+        nnm_dropin::check(nnm_merge_merge2one(egraph, sz));
+        return 1;
+    }
+    // AbstractMerge::cutMat (abstractmerge.cpp:37-53): rows [b_idx, l_idx)
+    // copied into new float[].
+    float *cutMat(float *mata, const unsigned b_idx, const unsigned l_idx) {
+        const size_t n = (size_t)(l_idx - b_idx) * col;
+        float *c = new float[n];
+        std::memcpy(c, mata + (size_t)b_idx * col, n * sizeof(float));
+        return c;
+    }
+    // The pools as Neighbors (the reference's egraph->knnGraph[i].pool).
+    Neighbors pool(const unsigned i) {
+        std::vector<uint32_t> ids((size_t)row * K0);
+        std::vector<float> ds((size_t)row * K0);
+        std::vector<uint8_t> fl((size_t)row * K0);
+        nnm_dropin::check(nnm_merge_read(egraph, ids.data(), ds.data(), fl.data()));
+        Neighbors p(K0);
+        for (unsigned j = 0; j < K0; j++) {
+            p[j].id = ids[(size_t)i * K0 + j];
+            p[j].dist = ds[(size_t)i * K0 + j];
+            p[j].flag = fl[(size_t)i * K0 + j] != 0;
+        }
+        return p;
+    }
 };
 
+// Smerge (smerge.h:8-23): Smerge::buildKGraph (smerge.cpp:46-91) step by step.
 class Smerge : public AbstractMerge {
+protected:
+    int join_filter() const override { return NNM_MERGE_SMERGE; }
+
 public:
     Smerge() {}
     explicit Smerge(SpaceInterface<float> *func) : AbstractMerge(func) {}
     unsigned *buildKGraph(float *mata, const unsigned K, const unsigned N, const unsigned D) override {
+        std::cout << "1. Two Sub graphs are prepared..................k = " << K << std::endl;
         InitialMemory(mata, K, N, D);
-        nnm_opts o = nnm_dropin::opts(metric);
-        nnm_stats st;
-        ids_.resize((size_t)N * K);
-        nnm_dropin::check(nnm_smerge(nnm_dropin::context(), mata, N, D, K, &o, ids_.data(), nullptr, nullptr, &st));
-        nCmps = st.ncmps;
+        preSize = row * 5 / 10;
+        unsigned *one = subGraph(0, preSize);
+        unsigned *two = subGraph(preSize, row);
+        nCmps = 0;
+        std::cout << "2. Symmetric Merge process.....................:" << std::endl;
+        auto t0 = std::chrono::steady_clock::now();
+        InitSGraph(0, one, 0, preSize);
+        InitSGraph(preSize, two, 1, row - preSize);
+        delete[] one;
+        delete[] two;
+        InitialGraph();
+        nnDescent();
+        merge2one(row);
+        std::cout << "Merge time .....................................times = "
+                  << std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() << std::endl;
         std::cout << "Merge-Scanning rate:............................rate  = "
                   << nCmps / ((row / 2.0) * (row - 1.0)) << std::endl;
         return 0;
     }
+    // Smerge::InitialGraph (smerge.cpp:94-209): cross samples of the other half.
+    unsigned InitialGraph() override {
+        nnm_dropin::check(nnm_merge_initial_graph(egraph, NNM_MERGE_SMERGE, preSize));
+        nCmps += (unsigned long)row * (K0 * 1 / 2);
+        return 1;
+    }
+    unsigned localJoin() override { return 0; }
+    void setdisfunc(SpaceInterface<float> *func) override { metric = func->nnm_metric(); }
 };
 
+// Jmerge (jmerge.h:7-22): Jmerge::buildKGraph (jmerge.cpp:43-80) step by step.
 class Jmerge : public AbstractMerge {
+protected:
+    int join_filter() const override { return NNM_MERGE_JMERGE; }
+
 public:
     Jmerge() {}
     explicit Jmerge(SpaceInterface<float> *func) : AbstractMerge(func) {}
     unsigned *buildKGraph(float *mata, const unsigned K, const unsigned N, const unsigned D) override {
+        std::cout << "1. One Sub graph are prepared...................k = " << K << std::endl;
         InitialMemory(mata, K, N, D);
-        nnm_opts o = nnm_dropin::opts(metric);
-        nnm_stats st;
-        ids_.resize((size_t)N * K);
-        nnm_dropin::check(nnm_jmerge(nnm_dropin::context(), mata, N, D, K, &o, ids_.data(), nullptr, nullptr, &st));
-        nCmps = st.ncmps;
+        preSize = row * 5 / 10;
+        unsigned *one = subGraph(0, preSize);
+        std::cout << "2. Joint Merge process.........................:" << std::endl;
+        nCmps = 0;
+        auto t0 = std::chrono::steady_clock::now();
+        InitSGraph(0, one, 0, preSize);
+        delete[] one;
+        InitialGraph();
+        nnDescent();
+        merge2one(preSize);
+        std::cout << "Merge time .....................................times = "
+                  << std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() << std::endl;
         std::cout << "Merge-Scanning rate:............................rate  = "
                   << nCmps / ((row / 2.0) * (row - 1.0)) << std::endl;
         return 0;
     }
+    // Jmerge::InitialGraph (jmerge.cpp:83-176): cross samples of the raw
+    // rows for the built ones, random pools for the raw ones.
+    unsigned InitialGraph() override {
+        nnm_dropin::check(nnm_merge_initial_graph(egraph, NNM_MERGE_JMERGE, preSize));
+        nCmps += (unsigned long)preSize * (K0 * 3 / 6) + (unsigned long)(row - preSize) * K0;
+        return 1;
+    }
+    unsigned localJoin() override { return 0; }
+    void setdisfunc(SpaceInterface<float> *func) override { metric = func->nnm_metric(); }
 };
 
 class LyNNDescent {

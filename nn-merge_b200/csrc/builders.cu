@@ -319,6 +319,20 @@ __global__ void k_rebase(uint32_t* pid, size_t count, uint32_t add, uint32_t gd)
     pid[t] = ((pid[t] & ID_MASK) + add) | (gd ? GD_BIT : 0u) | FLAG_BIT;
 }
 
+// AbstractMerge::InitSGraph (abstractmerge.cpp:55-76) from a caller's
+// graph: rows [b, b + rows) take the graph's local ids + b, in the graph's
+// order, flagged new with group id `gd`, distances recomputed (a warp per
+// row, a lane per entry).
+__global__ void k_init_sgraph(const float* x, uint32_t dp, int metric, uint32_t K, const uint32_t* graph, uint32_t b,
+                              uint32_t rows, uint32_t gd, uint32_t* pid, float* pdist) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t i = blockIdx.x * WPB + w;
+    if (i >= rows || lane >= (int)K) return;
+    const uint32_t row = b + i, id = graph[(size_t)i * K + lane] + b;
+    pid[(size_t)row * K + lane] = id | (gd ? GD_BIT : 0u) | FLAG_BIT;
+    pdist[(size_t)row * K + lane] = dist_seq_rt(metric, x + (size_t)row * dp, x + (size_t)id * dp, dp);
+}
+
 // setflag (lynndescent.cpp:717-732): all group ids to 0.
 __global__ void k_clear_gd(uint32_t* pid, size_t count) {
     size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -521,6 +535,67 @@ static void absorb(GraphDev& p, const GraphDev& s) {
     p.trace.insert(p.trace.end(), s.trace.begin(), s.trace.end());
 }
 
+// Smerge::InitialGraph (smerge.cpp:94-209) over G leaves, reference
+// streams: one mt19937(seed) for all rows in order, getRndSds(2 cut) over the
+// rows outside the row's leaf, the worst `cut` entries to the compensation
+// list.  d_leaf_off: the leaf boundaries on the device.
+static int cross_sample_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off,
+                               const uint32_t* d_leaf_off) {
+    const uint32_t K = g.K, n = g.n, nleaf = (uint32_t)leaf_off.size() - 1;
+    int rc;
+    g.cut = K * 1 / 2;
+    size_t total = 0;
+    std::vector<uint32_t> per(nleaf);
+    for (uint32_t l = 0; l < nleaf; l++) {
+        uint32_t range = n - (leaf_off[l + 1] - leaf_off[l]);
+        per[l] = sds_draws(2 * g.cut, range);
+        total += (size_t)(leaf_off[l + 1] - leaf_off[l]) * per[l];
+    }
+    std::vector<uint32_t> h(total);
+    gen_mt19937(g.seed, total, h.data());
+    if ((rc = upload_draws(ctx, g.seed, h, total))) return rc;
+    if ((rc = reset_counters(ctx))) return rc;
+    size_t off = 0;
+    for (uint32_t l = 0; l < nleaf; l++) {
+        uint32_t r0 = leaf_off[l], r1 = leaf_off[l + 1];
+        CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist,
+                     ctx.ws.draws.as<uint32_t>() + off, per[l], 2 * g.cut, g.cut, r0, r1,
+                     d_leaf_off, nleaf, 0, 0, nleaf == 2 ? (l == 0 ? 1u : 0u) : 0u,
+                     ctx.ws.counters.as<IterCounters>()};
+        k_cross_sample<<<blocks_for(r1 - r0, WPB), WPB * 32, 0, ctx.stream>>>(ca); count_launch();
+        off += (size_t)(r1 - r0) * per[l];
+    }
+    NNM_CUDA_TRY(cudaGetLastError());
+    if ((rc = check_counters(ctx))) return rc;
+    g.ncmps += (uint64_t)n * g.cut;
+    return 0;
+}
+
+// Jmerge::InitialGraph (jmerge.cpp:83-176), reference streams: the built
+// rows [0, pre) cross-sample `cut` ids of the raw rows, the raw rows [pre, n)
+// take K random ids of all rows; one mt19937(seed), built rows first.
+static int jmerge_initial_exact(Ctx& ctx, GraphDev& g, uint32_t pre) {
+    const uint32_t K = g.K, n = g.n;
+    int rc;
+    g.cut = K * 3 / 6;  // jmerge.cpp:87
+    const uint32_t per_old = sds_draws(2 * g.cut, n - pre), per_new = sds_draws(K + 1, n);
+    size_t total = (size_t)pre * per_old + (size_t)(n - pre) * per_new;
+    std::vector<uint32_t> h(total);
+    gen_mt19937(g.seed, total, h.data());
+    if ((rc = upload_draws(ctx, g.seed, h, total))) return rc;
+    if ((rc = reset_counters(ctx))) return rc;
+    CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist, ctx.ws.draws.as<uint32_t>(), per_old,
+                 2 * g.cut, g.cut, 0, pre, nullptr, 0, pre, n - pre, 1, ctx.ws.counters.as<IterCounters>()};
+    k_cross_sample<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(ca); count_launch();
+    InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>() + (size_t)pre * per_old,
+                per_new, K + 1, n, pre, n, pre, ctx.ws.counters.as<IterCounters>()};
+    k_init_rows<<<blocks_for(n - pre, WPB), WPB * 32, 0, ctx.stream>>>(ia); count_launch();
+    NNM_CUDA_TRY(cudaGetLastError());
+    if ((rc = check_counters(ctx))) return rc;
+    g.ncmps += (uint64_t)pre * g.cut + (uint64_t)(n - pre) * K;
+    return 0;
+}
+
 int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, uint64_t* sub_ncmps) {
     const uint32_t K = g.K, n = g.n, nleaf = (uint32_t)leaf_off.size() - 1;
     int rc;
@@ -584,41 +659,12 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
         NNM_CUDA_TRY(cudaGetLastError());
         return 0;
     }
-    std::vector<uint32_t> h;
-    h.reserve((size_t)n * (2 * g.cut + 1));
-    {
-        std::vector<uint32_t> all;
-        size_t total = 0;
-        std::vector<uint32_t> per(nleaf);
-        for (uint32_t l = 0; l < nleaf; l++) {
-            uint32_t range = n - (leaf_off[l + 1] - leaf_off[l]);
-            per[l] = sds_draws(2 * g.cut, range);
-            total += (size_t)(leaf_off[l + 1] - leaf_off[l]) * per[l];
-        }
-        h.resize(total);
-        gen_mt19937(g.seed, total, h.data());
-        if ((rc = upload_draws(ctx, g.seed, h, total))) return rc;
-        DevBuf& lo = ctx.ws.misc;
-        NNM_CUDA_TRY(lo.ensure(leaf_off.size() * 4 + 64));
-        NNM_CUDA_TRY(cudaMemcpyAsync(lo.p, leaf_off.data(), leaf_off.size() * 4, cudaMemcpyHostToDevice, ctx.stream));
-        if ((rc = reset_counters(ctx))) return rc;
-        size_t off = 0;
-        for (uint32_t l = 0; l < nleaf; l++) {
-            uint32_t r0 = leaf_off[l], r1 = leaf_off[l + 1];
-            CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist,
-                         ctx.ws.draws.as<uint32_t>() + off, per[l], 2 * g.cut, g.cut, r0, r1,
-                         lo.as<uint32_t>(), nleaf, 0, 0, nleaf == 2 ? (l == 0 ? 1u : 0u) : 0u,
-                         ctx.ws.counters.as<IterCounters>()};
-            k_cross_sample<<<blocks_for(r1 - r0, WPB), WPB * 32, 0, ctx.stream>>>(ca); count_launch();
-            off += (size_t)(r1 - r0) * per[l];
-        }
-        NNM_CUDA_TRY(cudaGetLastError());
-        if ((rc = check_counters(ctx))) return rc;
-        g.ncmps += (uint64_t)n * g.cut;
-        // 3. NN-Descent with the cross-group join, 4. merge2one
-        rc = run_nndescent(ctx, g, MODE_SMERGE, leaf_off[1], 0, lo.as<uint32_t>(), nleaf);
-        if (rc) return rc;
-    }
+    DevBuf& lo = ctx.ws.misc;
+    NNM_CUDA_TRY(lo.ensure(leaf_off.size() * 4 + 64));
+    NNM_CUDA_TRY(cudaMemcpyAsync(lo.p, leaf_off.data(), leaf_off.size() * 4, cudaMemcpyHostToDevice, ctx.stream));
+    if ((rc = cross_sample_leaves(ctx, g, leaf_off, lo.as<uint32_t>()))) return rc;
+    // 3. NN-Descent with the cross-group join, 4. merge2one
+    if ((rc = run_nndescent(ctx, g, MODE_SMERGE, leaf_off[1], 0, lo.as<uint32_t>(), nleaf))) return rc;
     k_merge2one<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, n, g.fast ? 1u : 0u); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return 0;
@@ -642,21 +688,7 @@ int jmerge_build(Ctx& ctx, GraphDev& g, uint64_t* sub_ncmps) {
         NNM_CUDA_TRY(cudaGetLastError());
         return 0;
     }
-    const uint32_t per_old = sds_draws(2 * g.cut, n - pre), per_new = sds_draws(K + 1, n);
-    size_t total = (size_t)pre * per_old + (size_t)(n - pre) * per_new;
-    std::vector<uint32_t> h(total);
-    gen_mt19937(g.seed, total, h.data());
-    if ((rc = upload_draws(ctx, g.seed, h, total))) return rc;
-    if ((rc = reset_counters(ctx))) return rc;
-    CrossArgs ca{g.x, g.dp, K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist, ctx.ws.draws.as<uint32_t>(), per_old,
-                 2 * g.cut, g.cut, 0, pre, nullptr, 0, pre, n - pre, 1, ctx.ws.counters.as<IterCounters>()};
-    k_cross_sample<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(ca); count_launch();
-    InitArgs ia{g.x, g.dp, K, g.metric, g.pid, g.pdist, ctx.ws.draws.as<uint32_t>() + (size_t)pre * per_old,
-                per_new, K + 1, n, pre, n, pre, ctx.ws.counters.as<IterCounters>()};
-    k_init_rows<<<blocks_for(n - pre, WPB), WPB * 32, 0, ctx.stream>>>(ia); count_launch();
-    NNM_CUDA_TRY(cudaGetLastError());
-    if ((rc = check_counters(ctx))) return rc;
-    g.ncmps += (uint64_t)pre * g.cut + (uint64_t)(n - pre) * K;
+    if ((rc = jmerge_initial_exact(ctx, g, pre))) return rc;
     if ((rc = run_nndescent(ctx, g, MODE_JMERGE, pre, 0, nullptr, 0))) return rc;
     k_merge2one<<<blocks_for(pre, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, pre, g.fast ? 1u : 0u); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
@@ -732,6 +764,45 @@ int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer) {
             k_clear_gd<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid, cnt); count_launch();  // setflag
         }
     }
+    NNM_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Staged merge: the steps of Smerge/Jmerge::buildKGraph as separate calls on
+// one graph (reference streams).  The graph is one reference process: the
+// std::rand() stream continues from step to step, each phase that the
+// reference seeds with time(NULL) draws from mt19937(seed).
+
+int stage_subgraph(Ctx& ctx, GraphDev& g, uint32_t b, uint32_t e, uint64_t* ncmps) {
+    GraphDev s = sub_view(g, b, e);
+    int rc = kgraph_build(ctx, s);
+    if (rc) return rc;
+    if (ncmps) *ncmps = s.ncmps;
+    absorb(g, s);
+    return 0;
+}
+
+int stage_init_sgraph(Ctx& ctx, GraphDev& g, uint32_t b, const uint32_t* d_graph, uint32_t gid, uint32_t rows) {
+    k_init_sgraph<<<blocks_for(rows, WPB), WPB * 32, 0, ctx.stream>>>(g.x, g.dp, g.metric, g.K, d_graph, b, rows,
+                                                                   gid, g.pid, g.pdist); count_launch();
+    NNM_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int stage_initial_graph(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t pre, const uint32_t* d_leaf_off) {
+    if (mode == MODE_SMERGE) return cross_sample_leaves(ctx, g, {0u, pre, g.n}, d_leaf_off);
+    return jmerge_initial_exact(ctx, g, pre);
+}
+
+int stage_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t pre, const uint32_t* d_leaf_off) {
+    if (mode == MODE_SMERGE) return run_nndescent(ctx, g, MODE_SMERGE, pre, 0, d_leaf_off, 2);
+    return run_nndescent(ctx, g, MODE_JMERGE, pre, 0, nullptr, 0);
+}
+
+int stage_merge2one(Ctx& ctx, GraphDev& g, uint32_t sz) {
+    k_merge2one<<<blocks_for(sz, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, g.K, g.cut, sz,
+                                                                 g.fast ? 1u : 0u); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return 0;
 }

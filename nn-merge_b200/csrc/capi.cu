@@ -23,6 +23,15 @@ struct nnm_index {
     nnm::IndexDev ix;
 };
 
+// A staged merge: its own graph arrays (the reference's egraph), so that
+// other calls on the context between the steps leave it alone.
+struct nnm_merge {
+    nnm_ctx* ctx;
+    nnm::GraphStore store;
+    nnm::GraphDev g;
+    nnm::DevBuf leaf_off, graph;  // {0, pre, n}; a caller's graph for InitSGraph
+};
+
 namespace {
 
 using nnm::Ctx;
@@ -184,6 +193,32 @@ int upload_plain(Ctx& c, GraphStore& st, GraphDev& g, const float* x, uint64_t n
     return nnm::upload_vectors(c, st, g, x, false);
 }
 
+// Runs one step of a staged merge: sets the device, returns the step's
+// status after its work has finished.
+template <class F>
+int merge_step(nnm_merge* m, F&& step) {
+    if (!m) return NNM_ERR_INVALID;
+    Ctx& c = m->ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(m->ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    int rc = step(c);
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(c.stream);
+        if (e != cudaSuccess) rc = fail(m->ctx, NNM_ERR_CUDA, cudaGetErrorString(e));
+    }
+    return rc;
+}
+
+bool merge_kind_ok(nnm_merge* m, uint32_t kind, uint32_t pre) {
+    if (kind != NNM_MERGE_SMERGE && kind != NNM_MERGE_JMERGE) {
+        fail(m->ctx, NNM_ERR_INVALID, "kind must be NNM_MERGE_SMERGE or NNM_MERGE_JMERGE");
+        return false;
+    }
+    if (pre < m->g.K + 2 || pre >= m->g.n || (kind == NNM_MERGE_SMERGE && m->g.n - pre < m->g.K + 2)) {
+        fail(m->ctx, NNM_ERR_INVALID, "pre must leave at least k+2 rows on its built side(s)");
+        return false;
+    }
+    return true;
+}
 }  // namespace
 
 extern "C" {
@@ -278,6 +313,140 @@ int nnm_merge_leaves_dev(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, u
                          const uint32_t* leaf_sizes, uint32_t nleaf, const nnm_opts* opts, uint32_t* ids,
                          float* dists, uint8_t* flags, nnm_stats* stats) {
     return build_common(ctx, KIND_LEAVES, x, true, n, d, k, leaf_sizes, nleaf, opts, ids, dists, flags, stats);
+}
+
+int nnm_merge_create(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint32_t k, const nnm_opts* opts,
+                     nnm_merge** out) {
+    if (!ctx) return NNM_ERR_INVALID;
+    if (!out) return fail(ctx, NNM_ERR_INVALID, "out must be non-null");
+    *out = nullptr;
+    if (!x || n == 0 || d == 0) return fail(ctx, NNM_ERR_INVALID, "x must be non-null with n, d > 0");
+    if (k == 0 || k > (uint32_t)nnm::MAXK) return fail(ctx, NNM_ERR_INVALID, "k must be in [1, 32]");
+    if (n >= (1ull << 30)) return fail(ctx, NNM_ERR_INVALID, "n must be below 2^30");
+    if (n < k + 2) return fail(ctx, NNM_ERR_INVALID, "n must be at least k+2");
+    nnm_opts o;
+    if (opts) o = *opts;
+    else nnm_opts_default(&o);
+    int rc;
+    if (!opts_ok(ctx, &o, &rc)) return rc;
+    if (o.rng_mode != NNM_RNG_EXACT)
+        return fail(ctx, NNM_ERR_INVALID, "the staged merge runs the reference's streams (NNM_RNG_EXACT)");
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    std::unique_ptr<nnm_merge> m(new nnm_merge());
+    m->ctx = ctx;
+    setup_graph(m->g, o, n, d, k);
+    rc = nnm::upload_vectors(c, m->store, m->g, x, false);
+    if (!rc) rc = nnm::graph_alloc(c, m->store, m->g, false);
+    if (!rc) {
+        cudaError_t e = m->leaf_off.ensure(64);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+        if (e != cudaSuccess) rc = fail(ctx, NNM_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (rc) {
+        m->store.release();
+        m->leaf_off.release();
+        return rc;
+    }
+    *out = m.release();
+    return NNM_OK;
+}
+
+
+int nnm_merge_subgraph(nnm_merge* m, uint32_t b, uint32_t e, uint32_t* graph, uint64_t* ncmps) {
+    if (!m) return NNM_ERR_INVALID;
+    if (b >= e || e > m->g.n || e - b < m->g.K + 2)
+        return fail(m->ctx, NNM_ERR_INVALID, "need 0 <= b < e <= n with at least k+2 rows");
+    return merge_step(m, [&](Ctx& ctx) {
+        uint64_t nc = 0;
+        int rc = nnm::stage_subgraph(ctx, m->g, b, e, &nc);
+        if (!rc && graph) {
+            nnm::GraphDev s = m->g;
+            s.n = e - b;
+            s.pid = m->g.pid + (size_t)b * m->g.K;
+            s.pdist = m->g.pdist + (size_t)b * m->g.K;
+            rc = nnm::export_graph(ctx, s, graph, nullptr, nullptr, true);
+        }
+        if (!rc && ncmps) *ncmps = nc;
+        return rc;
+    });
+}
+
+int nnm_merge_init_sgraph(nnm_merge* m, uint32_t b, const uint32_t* graph, uint32_t gid, uint32_t size) {
+    if (!m) return NNM_ERR_INVALID;
+    const uint32_t K = m->g.K;
+    if (!graph || size == 0 || (uint64_t)b + size > m->g.n)
+        return fail(m->ctx, NNM_ERR_INVALID, "need a graph and 0 < size with b + size <= n");
+    if (gid > 1) return fail(m->ctx, NNM_ERR_INVALID, "gid must be 0 or 1");
+    for (size_t t = 0; t < (size_t)size * K; t++)
+        if (graph[t] >= size) return fail(m->ctx, NNM_ERR_INVALID, "graph ids must be local to the sub-range");
+    return merge_step(m, [&](Ctx& ctx) {
+        const size_t bytes = (size_t)size * K * 4;
+        NNM_CUDA_TRY(m->graph.ensure(bytes));
+        NNM_CUDA_TRY(cudaMemcpyAsync(m->graph.p, graph, bytes, cudaMemcpyHostToDevice, ctx.stream));
+        return nnm::stage_init_sgraph(ctx, m->g, b, m->graph.as<uint32_t>(), gid, size);
+    });
+}
+
+int nnm_merge_initial_graph(nnm_merge* m, uint32_t kind, uint32_t pre) {
+    if (!m) return NNM_ERR_INVALID;
+    if (!merge_kind_ok(m, kind, pre)) return NNM_ERR_INVALID;
+    return merge_step(m, [&](Ctx& ctx) {
+        const uint32_t off[3] = {0u, pre, m->g.n};
+        NNM_CUDA_TRY(cudaMemcpyAsync(m->leaf_off.p, off, sizeof(off), cudaMemcpyHostToDevice, ctx.stream));
+        NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));  // off lives on this stack
+        return nnm::stage_initial_graph(ctx, m->g, kind == NNM_MERGE_SMERGE ? nnm::MODE_SMERGE : nnm::MODE_JMERGE, pre,
+                                        m->leaf_off.as<uint32_t>());
+    });
+}
+
+int nnm_merge_nndescent(nnm_merge* m, uint32_t kind, uint32_t pre, nnm_stats* stats) {
+    if (!m) return NNM_ERR_INVALID;
+    if (!merge_kind_ok(m, kind, pre)) return NNM_ERR_INVALID;
+    return merge_step(m, [&](Ctx& ctx) {
+        const uint32_t off[3] = {0u, pre, m->g.n};
+        NNM_CUDA_TRY(cudaMemcpyAsync(m->leaf_off.p, off, sizeof(off), cudaMemcpyHostToDevice, ctx.stream));
+        NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+        GraphDev& g = m->g;
+        const uint64_t c0 = g.ncmps;
+        const uint32_t it0 = g.iters;
+        const size_t t0 = g.trace.size();
+        EventTimer tm(ctx.stream);
+        int rc = nnm::stage_nndescent(ctx, g, kind == NNM_MERGE_SMERGE ? nnm::MODE_SMERGE : nnm::MODE_JMERGE, pre,
+                                      m->leaf_off.as<uint32_t>());
+        const float ms = tm.stop();
+        if (!rc && stats) {
+            GraphDev part;
+            part.ncmps = g.ncmps - c0;
+            part.iters = g.iters - it0;
+            part.trace.assign(g.trace.begin() + t0, g.trace.end());
+            fill_stats(stats, part, 0, ms);
+        }
+        return rc;
+    });
+}
+
+int nnm_merge_merge2one(nnm_merge* m, uint32_t sz) {
+    if (!m) return NNM_ERR_INVALID;
+    if (sz == 0 || sz > m->g.n) return fail(m->ctx, NNM_ERR_INVALID, "sz must be in [1, n]");
+    if (m->g.cut == 0) return fail(m->ctx, NNM_ERR_INVALID, "merge2one needs an initial graph (its compensation lists)");
+    return merge_step(m, [&](Ctx& ctx) { return nnm::stage_merge2one(ctx, m->g, sz); });
+}
+
+int nnm_merge_read(nnm_merge* m, uint32_t* ids, float* dists, uint8_t* flags) {
+    if (!m) return NNM_ERR_INVALID;
+    return merge_step(m, [&](Ctx& ctx) { return nnm::export_graph(ctx, m->g, ids, dists, flags, true); });
+}
+
+int nnm_merge_free(nnm_merge* m) {
+    if (!m) return NNM_OK;
+    cudaSetDevice(m->ctx->c.device);
+    cudaStreamSynchronize(m->ctx->c.stream);
+    m->store.release();
+    m->leaf_off.release();
+    m->graph.release();
+    delete m;
+    return NNM_OK;
 }
 
 int nnm_hmerge_build(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint32_t k, uint32_t m,

@@ -28,4 +28,20 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
 int jmerge_build(Ctx& ctx, GraphDev& g, uint64_t* sub_ncmps);
 int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer);
 
+// Staged merge (reference streams): the steps of Smerge::buildKGraph
+// (smerge.cpp:46-91) and Jmerge::buildKGraph (jmerge.cpp:43-80) as separate
+// calls on one graph, its std::rand() stream continuing across them.
+//   stage_subgraph      KGraph::buildKGraph on rows [b, e), in place (local ids)
+//   stage_init_sgraph   AbstractMerge::InitSGraph from a device graph of local ids
+//   stage_initial_graph Smerge::InitialGraph (MODE_SMERGE, halves split at pre)
+//                       or Jmerge::InitialGraph (MODE_JMERGE, built rows [0, pre))
+//   stage_nndescent     AbstractMerge::nnDescent with that class's localJoin filter
+//   stage_merge2one     AbstractMerge::merge2one(sz)
+// d_leaf_off: {0, pre, n} on the device (MODE_SMERGE).
+int stage_subgraph(Ctx& ctx, GraphDev& g, uint32_t b, uint32_t e, uint64_t* ncmps);
+int stage_init_sgraph(Ctx& ctx, GraphDev& g, uint32_t b, const uint32_t* d_graph, uint32_t gid, uint32_t rows);
+int stage_initial_graph(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t pre, const uint32_t* d_leaf_off);
+int stage_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t pre, const uint32_t* d_leaf_off);
+int stage_merge2one(Ctx& ctx, GraphDev& g, uint32_t sz);
+
 }  // namespace nnm

@@ -18,6 +18,8 @@ EXPORTED = (
     "nnm_merge_leaves_dev", "nnm_hmerge_build", "nnm_layers_free", "nnm_search",
     "nnm_profile_enable", "nnm_profile_get", "nnm_launch_count",
     "nnm_train_opts_default", "nnm_mlp_train", "nnm_mlp_grad", "nnm_mlp_codes", "nnm_set_init_model",
+    "nnm_merge_create", "nnm_merge_subgraph", "nnm_merge_init_sgraph", "nnm_merge_initial_graph",
+    "nnm_merge_nndescent", "nnm_merge_merge2one", "nnm_merge_read", "nnm_merge_free",
 )
 MLP_HIDDEN, MLP_OUT = 256, 32
 
@@ -165,6 +167,14 @@ def load():
         lib.nnm_entry_grad.argtypes = [vp, vp, vp, u64, u32, vp, vp, vp]
         lib.nnm_entry_train.argtypes = [vp, vp, vp, vp]
         lib.nnm_index_set_entry_model.argtypes = [vp, vp, u32]
+        lib.nnm_merge_create.argtypes = [vp, vp, u64, u32, u32, vp, ctypes.POINTER(ctypes.c_void_p)]
+        lib.nnm_merge_subgraph.argtypes = [vp, u32, u32, vp, vp]
+        lib.nnm_merge_init_sgraph.argtypes = [vp, u32, vp, u32, u32]
+        lib.nnm_merge_initial_graph.argtypes = [vp, u32, u32]
+        lib.nnm_merge_nndescent.argtypes = [vp, u32, u32, vp]
+        lib.nnm_merge_merge2one.argtypes = [vp, u32]
+        lib.nnm_merge_read.argtypes = [vp, vp, vp, vp]
+        lib.nnm_merge_free.argtypes = [vp]
         _lib = lib
     return _lib
 
@@ -355,6 +365,10 @@ class Context:
         self.lib.nnm_layers_free(ctypes.byref(lay))
         return dict(ids=ids, dists=dists, flags=flags, layers=layers, **_stats_dict(st))
 
+    def merge_session(self, x, k, **kw):
+        """A staged merge (nnm_merge_*): AbstractMerge's steps as calls."""
+        return Merge(self, x, k, **kw)
+
     def search(self, x, layers, q, topk, seed=0, metric="l2"):
         x = np.ascontiguousarray(x, np.float32)
         q = np.ascontiguousarray(q, np.float32)
@@ -433,6 +447,65 @@ class Context:
         self._check(self.lib.nnm_entry_grad(self.h, ctypes.byref(ms), _ptr(x), n, d, _ptr(lab), ctypes.byref(loss),
                                             ctypes.byref(gs)))
         return float(loss.value), grad
+
+
+MERGE_KINDS = {"smerge": 1, "jmerge": 2}
+
+
+class Merge:
+    """AbstractMerge (abstractmerge.h:16-40) step by step on the device:
+    InitialMemory at construction, then subgraph (KGraph::buildKGraph on a
+    row range, continuing the merge's std::rand() stream), init_sgraph
+    (InitSGraph), initial_graph (Smerge/Jmerge::InitialGraph), nndescent
+    (nnDescent with that class's localJoin), merge2one and read (the
+    pools).  Reference streams only."""
+
+    def __init__(self, ctx, x, k, **kw):
+        self.ctx, self.k = ctx, k
+        x = np.ascontiguousarray(x, np.float32)
+        self.n, self.d = x.shape
+        self.h = ctypes.c_void_p()
+        o = make_opts(**kw)
+        ctx._check(ctx.lib.nnm_merge_create(ctx.h, _ptr(x), self.n, self.d, k, ctypes.byref(o), ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.nnm_merge_free(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def subgraph(self, b, e):
+        g = np.empty((e - b, self.k), np.uint32)
+        c = ctypes.c_uint64()
+        self.ctx._check(self.ctx.lib.nnm_merge_subgraph(self.h, b, e, _ptr(g), ctypes.byref(c)))
+        return g, int(c.value)
+
+    def init_sgraph(self, b, graph, gid):
+        graph = np.ascontiguousarray(graph, np.uint32)
+        self.ctx._check(self.ctx.lib.nnm_merge_init_sgraph(self.h, b, _ptr(graph), gid, graph.shape[0]))
+
+    def initial_graph(self, kind, pre):
+        self.ctx._check(self.ctx.lib.nnm_merge_initial_graph(self.h, MERGE_KINDS[kind], pre))
+
+    def nndescent(self, kind, pre):
+        st = Stats()
+        self.ctx._check(self.ctx.lib.nnm_merge_nndescent(self.h, MERGE_KINDS[kind], pre, ctypes.byref(st)))
+        return _stats_dict(st)
+
+    def merge2one(self, sz):
+        self.ctx._check(self.ctx.lib.nnm_merge_merge2one(self.h, sz))
+
+    def read(self):
+        ids = np.empty((self.n, self.k), np.uint32)
+        dists = np.empty((self.n, self.k), np.float32)
+        flags = np.empty((self.n, self.k), np.uint8)
+        self.ctx._check(self.ctx.lib.nnm_merge_read(self.h, _ptr(ids), _ptr(dists), _ptr(flags)))
+        return dict(ids=ids, dists=dists, flags=flags)
 
 
 def _layers_struct(layers):
