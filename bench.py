@@ -24,7 +24,12 @@ Printed JSON (one line, rank 0):
   roofline    the dominant kernel (the local join) from the library's own
               CUDA-event timing and algorithmic byte count;
   cpu_baseline the reference itself (oracle/_ref, built from its sources) on
-              a bounded sample, extrapolated linearly to 1M rows.
+              the first 40,000 and 100,000 rows of the same set,
+              extrapolated to 1M rows by the power law through both times;
+  cfg1        the 100,000-row plain S-Merge (64-centre mixture): the
+              reference and the plain FP32 and exact u8 device paths on the
+              same rows (same configuration, same graphs);
+  search      the serving workload below, measured in the same run.
 
 --workload search measures batched LySearch serving instead (one step = a
 batch of 100,000 queries, top-10, beam widths drawn from 32..512, through
@@ -70,6 +75,11 @@ def parse():
     p.add_argument("--seed", type=int, default=1234)
     p.add_argument("--recall-rows", type=int, default=2000)
     p.add_argument("--cpu-sample", type=int, default=40_000)
+    p.add_argument("--fit-rows", type=int, default=100_000,
+                   help="second size of the reference's timing, for the exponent of its extrapolation")
+    p.add_argument("--no-cfg1", action="store_true",
+                   help="skip the 100,000-row plain S-Merge timed on the reference and the GPU")
+    p.add_argument("--no-search", action="store_true", help="build workload: skip the embedded serving measurement")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--path", default="fast", choices=["exact", "fast"],
@@ -167,18 +177,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def recall_at(ids, x_t, rows, atop, torch):
+def recall_at(ids, x_t, rows, atop, torch, both=False):
     """Recall@atop of the graph rows `rows` against exact brute force
-    (FP32 squared L2 without TF32: exact for integer data), counting an
-    entry as a hit when its exact distance is within the atop-th exact
-    distance (ties counted as hits)."""
+    (FP32 squared L2 without TF32: exact for integer data).  The first
+    figure counts an entry as a hit when its exact distance is within the
+    atop-th exact distance (ties counted as hits); with both=True the second
+    is Evaluator::getKGraphRecall's (evaluator.cpp:258-295): the graph's
+    first atop ids intersected with the atop exact neighbours, ties at the
+    atop-th distance broken by id."""
     prev = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = False
     try:
         q = x_t[rows]
         qn = (q * q).sum(1, keepdim=True)
         xn = (x_t * x_t).sum(1)
-        hits = 0
+        hits = ihits = 0
         for b in range(0, len(rows), 256):
             qb, qnb = q[b:b + 256], qn[b:b + 256]
             d = qnb + xn[None, :] - 2.0 * (qb @ x_t.T)
@@ -186,14 +199,24 @@ def recall_at(ids, x_t, rows, atop, torch):
             kth = torch.topk(d, atop, dim=1, largest=False).values[:, -1:]
             g = torch.as_tensor(ids[b:b + 256, :atop].astype(np.int64), device=d.device)
             hits += int((torch.gather(d, 1, g) <= kth).sum())
-        return hits / (len(rows) * atop)
+            if both:
+                # exact neighbours with ties by id: the atop smallest of (distance, id)
+                cand = torch.topk(d, atop + 16, dim=1, largest=False)
+                cd, ci = cand.values.cpu().numpy(), cand.indices.cpu().numpy()
+                for r in range(len(qb)):
+                    order = np.lexsort((ci[r], cd[r]))[:atop]
+                    ihits += len(np.intersect1d(ci[r][order], ids[b + r, :atop].astype(np.int64)))
+        rec = hits / (len(rows) * atop)
+        return (rec, ihits / (len(rows) * atop)) if both else rec
     finally:
         torch.backends.cuda.matmul.allow_tf32 = prev
 
 
-def reference_cpu(x, k, seed, sample):
+def reference_cpu(x, k, seed, sample, want_graph=False):
     """Times the reference on the first `sample` rows: S-Merge with its own
-    split (smerge.cpp:53).  Returns (seconds, kind, cores, note)."""
+    split (smerge.cpp:53), one thread (the reference has no threading).
+    Returns (seconds, kind, cores) -- and the graph's ids with want_graph.
+    The time includes the reference process reading its input."""
     ref = os.path.join(ROOT, "oracle", "_ref", "nnm_ref")
     xs = np.ascontiguousarray(x[:sample])
     if os.path.exists(ref):
@@ -202,41 +225,68 @@ def reference_cpu(x, k, seed, sample):
             with open(mat, "wb") as f:
                 f.write(np.array(xs.shape, np.uint32).tobytes())
                 f.write(xs.tobytes())
+            out = os.path.join(td, "out")
             t0 = time.perf_counter()
-            subprocess.run([ref, "smerge", "l2", mat, str(k), str(seed), os.path.join(td, "out")],
-                           check=True, capture_output=True, cwd=td)
-            return time.perf_counter() - t0, "reference", 1
+            subprocess.run([ref, "smerge", "l2", mat, str(k), str(seed), out], check=True, capture_output=True, cwd=td)
+            t = time.perf_counter() - t0
+            ids = None
+            if want_graph:
+                b = open(out, "rb").read()
+                n, kk = np.frombuffer(b, np.uint32, 2)
+                ids = np.frombuffer(b, np.uint32, int(n) * int(kk), 8).reshape(int(n), int(kk)).copy()
+            return (t, "reference", 1, ids) if want_graph else (t, "reference", 1)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_lib import Oracle
     o = Oracle()
     t0 = time.perf_counter()
-    o.smerge(xs, k, seed)
-    return time.perf_counter() - t0, "port", 1
+    r = o.smerge(xs, k, seed)
+    t = time.perf_counter() - t0
+    return (t, "port", 1, r["ids"]) if want_graph else (t, "port", 1)
+
+
+def cpu_fit(x, k, seed, s1, s2, n):
+    """The reference's S-Merge timed at two sizes of the same rows; the
+    power law t = t1 (m / s1)^alpha through both points extrapolates it to
+    n rows (NN-Descent is slightly super-linear in the row count)."""
+    t1, kind, cores = reference_cpu(x, k, seed, s1)
+    t2, _, _ = reference_cpu(x, k, seed, s2)
+    alpha = float(np.log(t2 / t1) / np.log(s2 / s1))
+    return {"t_small": t1, "t_large": t2, "rows": [s1, s2], "alpha": alpha,
+            "value": t2 * (n / s2) ** alpha, "kind": kind, "cores": cores}
 
 
 def run_reference_arm(a, rank):
+    """The reference's S-Merge (oracle/_ref: its own sources) on the first
+    cpu_sample rows of the same 1M set the GPU arm builds, each step one
+    run; one run on the first fit_rows rows fixes the power-law exponent
+    that scales the per-step median to the full row count."""
     if rank != 0:
         return
     from nnm.datasets import gaussian_mixture_u8
-    x = gaussian_mixture_u8(a.n if a.cpu_sample > a.n else a.cpu_sample, d=a.d, n_centres=a.centres, seed=a.seed)
+    x = gaussian_mixture_u8(a.n, d=a.d, n_centres=a.centres, seed=a.seed)
     times = []
     kind = "reference"
     for step in range(min(a.warmup, 1) + a.steps):
         t, kind, cores = reference_cpu(x, a.k, a.seed, a.cpu_sample)
         if step >= min(a.warmup, 1):
             times.append(t)
-    scale = a.n / a.cpu_sample
-    v = statistics.median(times) * scale
+    t_med = statistics.median(times)
+    t_fit, _, _ = reference_cpu(x, a.k, a.seed, a.fit_rows)
+    alpha = float(np.log(t_fit / t_med) / np.log(a.fit_rows / a.cpu_sample))
+    v = t_fit * (a.n / a.fit_rows) ** alpha
     line = {
         "metric": METRIC, "impl": "reference", "value": v, "unit": "s", "n_gpus": a.gpus, "steps": a.steps,
-        "warmup": a.warmup, "ms_per_step": statistics.median(times) * 1e3, "higher_is_better": False,
+        "warmup": a.warmup, "ms_per_step": t_med * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: seeded %d-centre Gaussian mixture, integers 0-255" % a.centres,
-        "config": {"workload": "S-Merge (smerge.cpp:46-91) of the first %d rows, seconds scaled by %.1f to %d rows "
-                               "(linear in n: a lower bound for NN-Descent)" % (a.cpu_sample, scale, a.n),
-                   "n": a.n, "d": a.d, "k": a.k},
+        "data": "synthetic: seeded %d-centre Gaussian mixture, integers 0-255 (the GPU arm's rows)" % a.centres,
+        "config": {"workload": "S-Merge (smerge.cpp:46-91) of the first %d rows per step; seconds extrapolated to "
+                               "%d rows by t = t(%d) (n / %d)^alpha, alpha = %.3f from the %d- and %d-row times"
+                               % (a.cpu_sample, a.n, a.fit_rows, a.fit_rows, alpha, a.cpu_sample, a.fit_rows),
+                   "n": a.n, "d": a.d, "k": a.k, "t_sample_s": t_med, "t_fit_rows_s": t_fit, "alpha": alpha,
+                   "fit_rows": a.fit_rows, "sample_rows": a.cpu_sample},
         "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": kind,
-                         "sample": "%d rows, S-Merge, single thread (the reference has no threading)" % a.cpu_sample},
+                         "sample": "%d rows per step (%d for the exponent), S-Merge, single thread (the reference "
+                                   "has no threading)" % (a.cpu_sample, a.fit_rows)},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -283,16 +333,20 @@ def search_cpu(x, layers, q, beams, seed, sample):
     return time.perf_counter() - t0
 
 
-def run_search(a, rank, world, local):
+def run_search(a, rank, world, local, reps=None, embedded=False):
     """Serving workload (one step = one batch of `queries` queries through
-    nnm_index_search_dev with the vectors, hierarchy and queries resident)."""
+    nnm_index_search_dev with the vectors, hierarchy and queries resident).
+    embedded: measured inside the build bench -- returns the line's fields
+    (rank 0) instead of printing, and skips the flat-graph comparison."""
     import torch
     import nnm
     from nnm.datasets import gaussian_mixture_u8, queries_like
     from nnm.replicas import Replicas
 
     torch.cuda.set_device(local)
-    reps = Replicas("nccl")
+    own_reps = reps is None
+    if own_reps:
+        reps = Replicas("nccl")
     n, d, k, nq = a.n, a.d, a.k, a.queries
     seed = reps.data_seed(a.seed)
     x = gaussian_mixture_u8(n, d=d, n_centres=a.centres, seed=seed)
@@ -370,7 +424,7 @@ def run_search(a, rank, world, local):
     # (one layer): the reference's flat search (random seeds) vs the
     # learned entry
     flat = None
-    if not a.no_flat:
+    if not a.no_flat and not embedded:
         k_ids = torch.empty((n, k), dtype=torch.int32, device="cuda")
         k_ds = torch.empty((n, k), dtype=torch.float32, device="cuda")
         ctx.merge_leaves_dev(x_t.data_ptr(), n, d, k, leaf_sizes(n, a.leaves), k_ids.data_ptr(), k_ds.data_ptr(), 0,
@@ -432,10 +486,16 @@ def run_search(a, rank, world, local):
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": learned["launches"],
             "clocks": clocks.summary(),
         }
-        print(json.dumps(line), flush=True)
+        if not embedded:
+            print(json.dumps(line), flush=True)
     ix.close()
     ctx.close()
-    reps.close()
+    if own_reps:
+        reps.close()
+    if embedded and rank == 0:
+        return {key: line[key] for key in ("metric", "value", "unit", "ms_per_step", "config", "roofline",
+                                           "cpu_baseline", "e2e", "gpu_launches", "clocks")}
+    return None
 
 
 def run_search_reference_arm(a, rank):
@@ -463,6 +523,32 @@ def run_search_reference_arm(a, rank):
                              "sample": "500 queries with their beams, single thread"},
             "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_cfg1(ctx, torch, seed):
+    """100,000 x 128 from the 64-centre mixture, S-Merge of the halves, k=20
+    (Smerge::buildKGraph, smerge.cpp:46-91): the reference's own process on
+    one host core, and the plain FP32 and exact u8 device paths (reference
+    streams) through the host C ABI on the same rows.  Returns the times,
+    whether the device graphs equal the reference's, and recall@10 of both."""
+    from nnm.datasets import gaussian_mixture_u8
+    x = gaussian_mixture_u8(100_000, d=128, n_centres=64, seed=1234)
+    t_ref, kind, cores, ref_ids = reference_cpu(x, 20, seed, len(x), want_graph=True)
+    out = {"workload": "100000x128 (64-centre mixture) S-Merge of the halves, k=20, reference streams",
+           "reference_s": t_ref, "reference_kind": kind, "reference_cores": cores}
+    for name, join in (("plain_fp32", "fp32"), ("exact_u8", "tensor")):
+        ctx.smerge(x, 20, seed=seed, join=join)  # warm-up
+        t0 = time.perf_counter()
+        r = ctx.smerge(x, 20, seed=seed, join=join)
+        t = time.perf_counter() - t0
+        out[name] = {"s_host_api": t, "device_ms": r["device_ms"], "iterations": r["iterations"],
+                     "same_graph_as_reference": bool(np.array_equal(r["ids"], ref_ids)),
+                     "ratio_reference_over_device": t_ref / t}
+    x_t = torch.from_numpy(x).cuda()
+    rows = np.sort(np.random.default_rng(7).choice(len(x), 2000, replace=False))
+    out["recall@10_reference"] = recall_at(ref_ids[rows], x_t, rows, 10, torch, both=True)
+    out["recall@10_device"] = recall_at(r["ids"][rows], x_t, rows, 10, torch, both=True)
+    return out
 
 
 def main():
@@ -524,19 +610,24 @@ def main():
     # against recall@10 >= 0.95 + 0.005
     tune = None
     if not a.no_tune and a.path == "fast":
+        # tuned on a held-out set of the same generator and size (another
+        # seed), so that the timed set's recall is measured, not fitted
         t0 = time.perf_counter()
-        chosen, trials = ctx.autotune_merge_leaves_dev(x_dev.data_ptr(), n, d, k, sizes, sample_rows=n,
+        xh = torch.from_numpy(gaussian_mixture_u8(n, d=d, n_centres=a.centres,
+                                                  seed=reps.data_seed(a.seed) + 50_000)).cuda()
+        chosen, trials = ctx.autotune_merge_leaves_dev(xh.data_ptr(), n, d, k, sizes, sample_rows=n,
                                                        eval_rows=2000, repeats=2, **bkw)
+        del xh
         bkw.update(chosen)
         tune = {"chosen": chosen, "s": time.perf_counter() - t0, "sample_rows": n, "eval_rows": 2000,
-                "trials": trials}
+                "held_out_seed": reps.data_seed(a.seed) + 50_000, "trials": trials}
 
     rng_rows = np.random.default_rng(7)
     rows = np.sort(rng_rows.choice(n, min(a.recall_rows, n), replace=False))
 
-    def recall_now():
+    def recall_now(both=False):
         ids_np = ids_dev[torch.as_tensor(rows, device="cuda")].cpu().numpy().view(np.uint32)
-        return recall_at(ids_np, x_dev, rows, 10, torch)
+        return recall_at(ids_np, x_dev, rows, 10, torch, both=both)
 
     # the plain FP32 GPU path (reference streams, FP32 join, random init),
     # timed the same way, for the speed-up of the default path
@@ -552,8 +643,9 @@ def main():
             pst = build_dev(**pkw)
         e1.record()
         torch.cuda.synchronize()
-        plain = {"s": e0.elapsed_time(e1) / 2 / 1e3, "recall@10": recall_now(), "iterations": pst["iterations"],
-                 "steps": 2}
+        prec, pirec = recall_now(both=True)
+        plain = {"s": e0.elapsed_time(e1) / 2 / 1e3, "recall@10": prec, "recall@10_ids": pirec,
+                 "iterations": pst["iterations"], "steps": 2}
 
     for _ in range(a.warmup):
         st = build_dev()
@@ -596,7 +688,7 @@ def main():
 
     # quality: recall@10 on a seeded row sample vs exact brute force
     build_dev()
-    rec = recall_now()
+    rec, rec_ids = recall_now(both=True)
     # distance error of the returned distances against FP64 on the same rows
     ids_s = ids_dev[torch.as_tensor(rows, device="cuda")].cpu().numpy().view(np.uint32).astype(np.int64)
     ds_s = dists_dev[torch.as_tensor(rows, device="cuda")].cpu().numpy().astype(np.float64)
@@ -625,10 +717,26 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        t, kind, cores = reference_cpu(x, k, build_seed, a.cpu_sample)
-        cpu = {"value": t * n / a.cpu_sample, "unit": "s", "cores": cores, "kind": kind,
-               "sample": "S-Merge of the first %d rows (%.1f s measured), scaled linearly to %d rows"
-                         % (a.cpu_sample, t, n)}
+        f = cpu_fit(x, k, build_seed, a.cpu_sample, a.fit_rows, n)
+        cpu = {"value": f["value"], "unit": "s", "cores": f["cores"], "kind": f["kind"],
+               "sample": "S-Merge of the first %d and %d rows of this set (%.1f s, %.1f s), extrapolated to %d rows "
+                         "by the power law through both (exponent %.3f)"
+                         % (f["rows"][0], f["rows"][1], f["t_small"], f["t_large"], n, f["alpha"]),
+               "fit": f}
+
+    # the 100,000-row plain S-Merge (the reference's CPU-runnable workload):
+    # the reference on the host next to the plain FP32 and exact u8 device
+    # paths on the same rows -- a same-configuration ratio
+    cfg1 = None
+    if rank == 0 and world == 1 and not a.no_cfg1:
+        cfg1 = run_cfg1(ctx, torch, build_seed)
+
+    # serving on the same kind of data (LySearch on a 1M hierarchy)
+    search = None
+    if not a.no_search:
+        ctx.close()
+        ctx = None
+        search = run_search(a, rank, world, local, reps=reps, embedded=True)
 
     if rank == 0:
         line = {
@@ -646,7 +754,10 @@ def main():
                        "path": a.path, "init": a.init, "train": train, "tune": tune,
                        "delta": bkw["delta"], "smpl": bkw["sample_cap"], "join": a.join,
                        "join_rows": prof["rows"],
-                       "recall@10": rec, "dist_err_vs_fp64": dist_err, "iterations": st["iterations"],
+                       "recall@10": rec, "recall@10_ids": rec_ids,
+                       "recall_note": "recall@10 counts ties at the 10th exact distance; recall@10_ids intersects ids "
+                                      "(Evaluator::getKGraphRecall)",
+                       "dist_err_vs_fp64": dist_err, "iterations": st["iterations"],
                        "ncmps_merge": st["ncmps"],
                        "ncmps_leaves": st["sub_ncmps"],
                        "l2": "inputs (%d MB) larger than L2 (126 MB)" % (x.nbytes >> 20),
@@ -654,10 +765,11 @@ def main():
             "plain_fp32": plain,
             "speedup_vs_plain_fp32": (plain["s"] / (ms / 1e3)) if plain else None,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks.summary(),
+            "clocks": clocks.summary(), "cfg1": cfg1, "search": search,
         }
         print(json.dumps(line), flush=True)
-    ctx.close()
+    if ctx is not None:
+        ctx.close()
     reps.close()
 
 
