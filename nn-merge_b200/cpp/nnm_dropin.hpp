@@ -30,6 +30,11 @@
 #include <string>
 #include <vector>
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include "../../include/nnm.h"
 
 template <typename MTYPE>
@@ -102,11 +107,43 @@ inline nnm_opts opts(int metric) {
     return o;
 }
 
-// IODelegator::load_refSet (iodelegator.cpp:159-182): .fvecs, .bvecs, .txt.
+inline bool ends_with(const char *fn, const char *e) {
+    const size_t a = std::strlen(fn), l = std::strlen(e);
+    return a >= l && std::strcmp(fn + a - l, e) == 0;
+}
+
+// A read-only memory map of a whole file (the fast path of the binary
+// readers: no stream buffering, one copy out of the page cache).
+struct MappedFile {
+    const unsigned char *p = nullptr;
+    size_t size = 0;
+    explicit MappedFile(const char *fn) {
+        const int fd = ::open(fn, O_RDONLY);
+        if (fd < 0) return;
+        struct stat st;
+        if (::fstat(fd, &st) == 0 && st.st_size > 0) {
+            void *m = ::mmap(nullptr, (size_t)st.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+            if (m != MAP_FAILED) {
+                p = static_cast<const unsigned char *>(m);
+                size = (size_t)st.st_size;
+                ::madvise(m, size, MADV_SEQUENTIAL);
+            }
+        }
+        ::close(fd);
+    }
+    ~MappedFile() {
+        if (p) ::munmap(const_cast<unsigned char *>(p), size);
+    }
+    MappedFile(const MappedFile &) = delete;
+    MappedFile &operator=(const MappedFile &) = delete;
+};
+
+// IODelegator::load_refSet (iodelegator.cpp:159-182): .fvecs
+// (load_fvecs, :222-265), .bvecs (loadBvec10m, :319-385: at most 10^7
+// rows, bytes to floats) and .txt ("rows cols" then the values, loadMatrix
+// :186-220).  The binary formats are read through a memory map.
 inline float *load_refSet(const char *fn, unsigned &d, unsigned &r) {
-    std::string s(fn);
-    auto ends = [&](const char *e) { size_t l = std::strlen(e); return s.size() >= l && s.compare(s.size() - l, l, e) == 0; };
-    if (ends(".txt")) {
+    if (ends_with(fn, ".txt")) {
         std::ifstream in(fn);
         if (!in) { std::cout << "Fail to read " << fn << std::endl; std::exit(0); }
         float a, b;
@@ -117,30 +154,31 @@ inline float *load_refSet(const char *fn, unsigned &d, unsigned &r) {
         for (size_t i = 0; i < (size_t)r * d; i++) in >> m[i];
         return m;
     }
-    const bool bytes = ends(".bvecs");
-    if (!bytes && !ends(".fvecs")) { std::cout << "unknown format " << fn << std::endl; std::exit(0); }
-    std::ifstream in(fn, std::ios::binary);
-    if (!in) { std::cout << "File '" << fn << "' cannot open for read!" << std::endl; std::exit(0); }
+    const bool bytes = ends_with(fn, ".bvecs");
+    if (!bytes && !ends_with(fn, ".fvecs")) { std::cout << "unknown format " << fn << std::endl; std::exit(0); }
+    MappedFile f(fn);
+    if (!f.p || f.size < 4) { std::cout << "File '" << fn << "' cannot open for read!" << std::endl; std::exit(0); }
     uint32_t dim = 0;
-    in.read(reinterpret_cast<char *>(&dim), 4);
-    in.seekg(0, std::ios::end);
+    std::memcpy(&dim, f.p, 4);
     const size_t rec = 4 + (size_t)dim * (bytes ? 1 : 4);
-    r = (unsigned)((size_t)in.tellg() / rec);
+    size_t rows = f.size / rec;
+    if (bytes && rows > 10000000) rows = 10000000;
+    r = (unsigned)rows;
     d = dim;
-    in.seekg(0);
     float *m = new float[(size_t)r * d];
-    std::vector<unsigned char> buf(rec);
-    for (unsigned i = 0; i < r; i++) {
-        in.read(reinterpret_cast<char *>(buf.data()), rec);
-        for (unsigned j = 0; j < d; j++) {
-            if (bytes) m[(size_t)i * d + j] = (float)buf[4 + j];
-            else std::memcpy(&m[(size_t)i * d + j], &buf[4 + 4 * (size_t)j], 4);
-        }
+    for (size_t i = 0; i < rows; i++) {
+        const unsigned char *src = f.p + i * rec + 4;
+        if (bytes)
+            for (unsigned j = 0; j < d; j++) m[i * d + j] = (float)src[j];
+        else
+            std::memcpy(m + i * d, src, (size_t)d * 4);
     }
     return m;
 }
 
-// The k-NN graph text format (abstractmerge.cpp:278-291, kgraph.cpp:247-261).
+// The k-NN graph text format (abstractmerge.cpp:278-291, kgraph.cpp:247-261),
+// read back by the reference's IODelegator::loadKNNGraph
+// (iodelegator.cpp:65-102).
 inline void save_knn(const char *dst, const std::vector<uint32_t> &ids, unsigned n, unsigned k) {
     std::ofstream out(dst);
     out << n << " " << k << std::endl;
@@ -149,6 +187,55 @@ inline void save_knn(const char *dst, const std::vector<uint32_t> &ids, unsigned
         for (unsigned j = 0; j < k; j++) out << ids[(size_t)i * k + j] << " ";
         out << std::endl;
     }
+}
+
+// Binary k-NN graph (no counterpart in the reference; for graphs whose text
+// form would dominate the build time): the bytes "NNMK", u32 version 1,
+// u32 n, u32 k, then n x k u32 ids, row-major, little endian.
+constexpr char KNN_MAGIC[4] = {'N', 'N', 'M', 'K'};
+
+inline void save_knn_bin(const char *dst, const std::vector<uint32_t> &ids, unsigned n, unsigned k) {
+    FILE *f = std::fopen(dst, "wb");
+    if (!f) { std::cout << "File '" << dst << "' cannot open for write!" << std::endl; std::exit(0); }
+    const uint32_t hdr[3] = {1u, n, k};
+    std::fwrite(KNN_MAGIC, 1, 4, f);
+    std::fwrite(hdr, 4, 3, f);
+    std::fwrite(ids.data(), 4, (size_t)n * k, f);
+    std::fclose(f);
+}
+
+// Either form, told apart by the magic: returns new unsigned[n * k] as
+// IODelegator::loadKNNGraph returns its array (topk = k).
+inline unsigned *load_knn(const char *fn, unsigned &n, unsigned &k) {
+    {
+        MappedFile f(fn);
+        if (f.p && f.size >= 16 && std::memcmp(f.p, KNN_MAGIC, 4) == 0) {
+            uint32_t hdr[3];
+            std::memcpy(hdr, f.p + 4, 12);
+            n = hdr[1];
+            k = hdr[2];
+            if (hdr[0] != 1 || f.size < 16 + (size_t)n * k * 4) {
+                std::cout << "File '" << fn << "' is not a version-1 graph" << std::endl;
+                std::exit(0);
+            }
+            unsigned *g = new unsigned[(size_t)n * k];
+            std::memcpy(g, f.p + 16, (size_t)n * k * 4);
+            return g;
+        }
+    }
+    std::ifstream in(fn);
+    if (!in) { std::cout << "File '" << fn << "' cannot open for read!" << std::endl; std::exit(0); }
+    in >> n >> k;
+    unsigned *g = new unsigned[(size_t)n * k]();
+    for (unsigned i = 0; i < n && in; i++) {
+        unsigned idx, num, v;
+        in >> idx >> num;
+        for (unsigned j = 0; j < num; j++) {
+            in >> v;
+            if (j < k) g[(size_t)i * k + j] = v;
+        }
+    }
+    return g;
 }
 
 }  // namespace nnm_dropin
@@ -194,7 +281,12 @@ public:
     }
     virtual unsigned InitialGraph() { return 0; }  // part of the device build
     virtual unsigned *buildKGraph(float *mata, const unsigned K, const unsigned N, const unsigned D) = 0;
-    virtual void saveKGraph(const char *dst) { nnm_dropin::save_knn(dst, ids_, row, K0); }
+    // The reference's text format; a name ending in ".knng" gets the
+    // binary form instead.
+    virtual void saveKGraph(const char *dst) {
+        if (nnm_dropin::ends_with(dst, ".knng")) nnm_dropin::save_knn_bin(dst, ids_, row, K0);
+        else nnm_dropin::save_knn(dst, ids_, row, K0);
+    }
     virtual void setdisfunc(SpaceInterface<float> *func) { metric = func->nnm_metric(); }
 };
 

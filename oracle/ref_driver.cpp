@@ -17,6 +17,10 @@
  *               in call order)
  *   search out: u32 nq, u32 topk, u32 entry point, u64 nCmps,
  *               nq*topk u32 ids, nq*topk f32 dists  (ascending)
+ *   loadknn   : the reference's own reader of the k-NN graph text
+ *               (IODelegator::loadKNNGraph) -> u32 n, u32 k, n*k u32 ids
+ *   loadvecs  : the reference's own reader of .fvecs/.bvecs/.txt vectors
+ *               (IODelegator::load_refSet) -> matrix format above
  */
 #include "kgraph.h"
 #include "smerge.h"
@@ -24,6 +28,7 @@
 #include "lynndescent.h"
 #include "lysearch.h"
 #include "space_lp.h"
+#include "iodelegator.h"
 
 #include <cstdint>
 #include <cstdio>
@@ -202,7 +207,9 @@ int usage() {
     std::fprintf(stderr,
         "usage: nnm_ref kgraph|smerge|jmerge <metric> <in.mat> <K> <seed> <out.graph>\n"
         "       nnm_ref hmerge <metric> <in.mat> <K> <M> <seed> <out.graph> <out_prefix>\n"
-        "       nnm_ref search|flatsearch <metric> <in.mat> <layers.txt> <queries.mat> <topk> <seed> <out.res>\n");
+        "       nnm_ref search|flatsearch <metric> <in.mat> <layers.txt> <queries.mat> <topk> <seed> <out.res>\n"
+        "       nnm_ref loadknn <graph.txt> <K> <out.ids>\n"
+        "       nnm_ref loadvecs <in.fvecs|.bvecs|.txt> <out.mat>\n");
     return 2;
 }
 
@@ -262,6 +269,30 @@ int main(int argc, char **argv) {
         write_graph(argv[7], n, k, pools, h->cmps());
         std::remove(src.c_str());
         std::remove(grd.c_str());
+        return 0;
+    }
+    if (cmd == "loadknn") {
+        if (argc != 5) return usage();
+        unsigned n = 0, k = 0;
+        unsigned *g = IODelegator::loadKNNGraph(argv[2], n, k, (unsigned)std::atoi(argv[3]));
+        FILE *f = std::fopen(argv[4], "wb");
+        std::fwrite(&n, 4, 1, f);
+        std::fwrite(&k, 4, 1, f);
+        std::fwrite(g, 4, (size_t)n * k, f);
+        std::fclose(f);
+        std::free(g);
+        return 0;
+    }
+    if (cmd == "loadvecs") {
+        if (argc != 4) return usage();
+        unsigned n = 0, d = 0;
+        float *m = IODelegator::load_refSet(argv[2], d, n);
+        FILE *f = std::fopen(argv[3], "wb");
+        std::fwrite(&n, 4, 1, f);
+        std::fwrite(&d, 4, 1, f);
+        std::fwrite(m, 4, (size_t)n * d, f);
+        std::fclose(f);
+        delete[] m;
         return 0;
     }
     if (cmd == "search" || cmd == "flatsearch") {

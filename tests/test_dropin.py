@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from nnm.datasets import gaussian_mixture_u8
+from oracle_lib import ref_available, run_ref
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 needs_gxx = pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
@@ -84,3 +85,34 @@ def test_dropin_search_matches_oracle(oracle, cmd):
     h = oracle.hmerge(x, 10, 10, 77)
     exp = oracle.search_ex(x, h["layers"], q, 2, 77, beam=2, flat=(cmd == "flatsearch"))
     assert np.array_equal(got, exp["ids"][:, 0])
+
+
+@needs_gxx
+@pytest.mark.gpu
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref/nnm_ref (the reference compiled from its sources) not built")
+def test_reference_reads_the_dropin_hierarchy(oracle):
+    """LyNNDescent::buildhgraph of the drop-in writes <dst>.txt; the
+    reference's own LySearch::loadGraphs (lysearch.cpp:112-186) reads it and
+    searches: its results equal the oracle's search on the layers as this
+    package parses them (so both read the file alike), and those layers are
+    the reference's own H-Merge hierarchy."""
+    from nnm import io as nio
+    from nnm.datasets import queries_like
+    x = gaussian_mixture_u8(6000, d=16, seed=12)
+    q = queries_like(200, d=16, seed=12, query_seed=5)
+    with tempfile.TemporaryDirectory() as td:
+        exe = build(td)
+        src = os.path.join(td, "x.fvecs")
+        write_fvecs(src, x)
+        pre = os.path.join(td, "h")
+        subprocess.run([exe, "hmerge", src, "10", "10", pre], check=True, capture_output=True,
+                       env=dict(os.environ, NNM_SEED="31"))
+        layers = nio.read_layers_text(pre + ".txt")
+        ref = run_ref("search", x, 10, 31, td, layers_txt=pre + ".txt", queries=q, topk=10)
+    exp = oracle.search(x, layers, q, 10, 31)
+    assert np.array_equal(ref["ids"], exp["ids"]) and np.array_equal(ref["dists"], exp["dists"])
+    assert ref["ncmps"] == exp["ncmps"]
+    h = oracle.hmerge(x, 10, 10, 31)
+    assert len(h["layers"]) == len(layers)
+    for (a, b), (c, e) in zip(h["layers"], layers):
+        assert np.array_equal(a, c) and np.array_equal(b, e)
