@@ -50,16 +50,23 @@ typedef enum {
 } nnm_rng_mode;
 
 /* Kernel of the local join's distance evaluations.  All give the same
-   graphs bit for bit.  The tensor-core join needs the L2 metric; for data
-   whose components are all integers in [0, 255] it computes u8 Gram matrices
-   exactly (every squared distance stays below 2^24, where the reference's
-   float sum is exact); for other finite data (|components| in [2^-60, 2^50],
-   d <= 384) it computes BF16 Gram matrices, rules pairs out with a rigorous
-   error bound and gives every other pair the reference's exact FP32 sum. */
+   graphs bit for bit.  The tensor-core joins need the L2 metric.  For data
+   whose components are all integers in [0, 255] the u8 join computes Gram
+   matrices exactly (every squared distance stays below 2^24, where the
+   reference's float sum is exact).  The reduced-precision joins (other
+   finite data, |components| in [2^-60, 2^50]) compute d~ = |a|^2 + |b|^2 -
+   2 G~ from split operands -- BF16: each vector as hi + lo parts, three
+   MMAs (d <= 192); FP8: each vector scaled by a power of two and written as
+   E4M3 parts hi + mid + lo, six MMAs (d <= 256) -- with a stated bound
+   |d~ - d| <= err_c (|a|^2 + |b|^2) against the reference's FP32 distance
+   d; a pair side is proposed when its lower bound passes the target's
+   filter, and the merge computes the exact FP32 distance of every proposal
+   that can still enter the top K, so the graphs equal the FP32 join's. */
 typedef enum {
     NNM_JOIN_AUTO = 0,   /* u8 tensor cores for integer data, else FP32 */
     NNM_JOIN_FP32 = 1,   /* FP32 CUDA cores: the reference's sequential sums */
-    NNM_JOIN_TENSOR = 2  /* tensor cores (u8, else BF16 with the FP32 recheck); NNM_ERR_INVALID when neither applies */
+    NNM_JOIN_TENSOR = 2, /* tensor cores: u8, else BF16 hi + lo; NNM_ERR_INVALID when neither applies */
+    NNM_JOIN_FP8 = 3     /* tensor cores, FP8 (E4M3) hi + mid + lo with per-vector power-of-two scales */
 } nnm_join_kernel;
 
 /* Initial graphs.  NNM_INIT_LEARNED (no counterpart in the reference) needs
@@ -82,7 +89,10 @@ typedef struct {
     uint32_t exact_trace; /* nonzero: record the reference's float mean every iteration */
     uint32_t join_kernel; /* nnm_join_kernel */
     uint32_t init;        /* nnm_init_mode */
-    uint32_t reserved[7];
+    uint32_t audit;       /* nonzero: the reduced-precision joins also compute every pair's exact
+                             distance and fail the call (NNM_ERR_CAPACITY) if one lies outside
+                             the stated bound -- a test of the bound, slow */
+    uint32_t reserved[6];
 } nnm_opts;
 
 typedef struct {

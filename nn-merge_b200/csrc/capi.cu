@@ -56,7 +56,7 @@ bool opts_ok(nnm_ctx* ctx, const nnm_opts* o, int* rc) {
         *rc = fail(ctx, NNM_ERR_INVALID, "sample_cap must be in [1, 4096]");
         return false;
     }
-    if (o->join_kernel > NNM_JOIN_TENSOR) {
+    if (o->join_kernel > NNM_JOIN_FP8) {
         *rc = fail(ctx, NNM_ERR_INVALID, "unknown join_kernel");
         return false;
     }
@@ -85,6 +85,7 @@ void setup_graph(GraphDev& g, const nnm_opts& o, uint64_t n, uint32_t d, uint32_
     g.exact_trace = o.exact_trace != 0;
     g.fast = o.rng_mode == NNM_RNG_FAST;
     g.join_kernel = o.join_kernel;
+    g.audit = o.audit != 0;
     g.init = o.init;
     g.phase = 0;
 }

@@ -38,6 +38,8 @@
 #include <type_traits>
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
 
 #include "../../include/nnm.h"
 #include "nnm_engine.h"
@@ -61,10 +63,25 @@ constexpr uint32_t IDESC_U8 = (2u << 4) | ((TC_SLOTS >> 3) << 17) | ((TC_SLOTS >
 // Instruction descriptor of kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16
 // (bits 7-9 = 1, 10-12 = 1), both K-major.
 constexpr uint32_t IDESC_BF16 = (1u << 4) | (1u << 7) | (1u << 10) | ((TC_SLOTS >> 3) << 17) | ((TC_SLOTS >> 4) << 24);
+// Instruction descriptor of kind::f8f6f4: D = F32 (bits 4-5 = 1), A = B =
+// E4M3 (bits 7-9 = 0, 10-12 = 0), both K-major.
+constexpr uint32_t IDESC_E4M3 = (1u << 4) | ((TC_SLOTS >> 3) << 17) | ((TC_SLOTS >> 4) << 24);
 
-// The reference's sequential FP32 distance of rows i and j: the BF16 tier's
-// recheck, one non-inlined copy for every call site.
-__device__ __noinline__ float exact_l2(const float* x, uint32_t dp, uint32_t i, uint32_t j) {
+// Operand kinds of the join (JoinArgs::tc_kind):
+//   KIND_U8    u8 vectors, kind::i8, exact integer Gram matrices;
+//   KIND_BF16  each row as BF16 parts hi + lo (lo = the rounding residual),
+//              G = hi.hi + hi.lo + lo.hi in three kind::f16 MMAs per K step;
+//   KIND_FP8   each row scaled by a power of two to |x| <= 448 and written as
+//              E4M3 parts hi + mid + lo (successive rounding residuals),
+//              G = hh + hm + mh + hl + lh + mm in six kind::f8f6f4 MMAs per
+//              K step, unscaled exactly by the two powers of two.
+// The reduced-precision kinds give d~ with |d~ - d| <= err_c (|a|^2 + |b|^2)
+// against the reference's FP32 distance d.
+constexpr uint32_t KIND_U8 = 0, KIND_BF16 = 1, KIND_FP8 = 2;
+
+// The reference's sequential FP32 distance of rows i and j (the audit of
+// the reduced-precision bound), one non-inlined copy.
+__device__ __noinline__ float audit_l2(const float* x, uint32_t dp, uint32_t i, uint32_t j) {
     return dist_seq<L2>(x + (size_t)i * dp, x + (size_t)j * dp, (int)dp);
 }
 
@@ -86,7 +103,7 @@ struct TcShared {
 // per-slot arrays.  Two buffers.
 __host__ __device__ constexpr size_t tc_vec_bytes(uint32_t kq) { return (size_t)TC_SLOTS * kq; }
 __host__ __device__ constexpr size_t tc_buf_bytes(uint32_t kq) {
-    return (tc_vec_bytes(kq) + (size_t)TC_SLOTS * (5 * 4 + 8) + 1023) & ~(size_t)1023;
+    return (tc_vec_bytes(kq) + (size_t)TC_SLOTS * (7 * 4 + 8) + 1023) & ~(size_t)1023;
 }
 __host__ __device__ constexpr size_t tc_smem_bytes(uint32_t kq) { return 2 * tc_buf_bytes(kq) + 1024; }
 
@@ -97,6 +114,8 @@ struct SlotBuf {
     uint32_t* nrm;
     uint32_t* cnt;  // pass 0: counts; pass 1: bucket cursors
     uint32_t* grp;
+    uint32_t* lim;  // pass 1: the slot's reserved bucket range (its pass-0 count)
+    float* scl;     // KIND_FP8: the row's inverse scale 2^-e
     unsigned long long* base;
 };
 
@@ -109,7 +128,9 @@ __device__ __forceinline__ SlotBuf slot_buf(unsigned char* smem, uint32_t kq, ui
     s.nrm = reinterpret_cast<uint32_t*>(s.kth + TC_SLOTS);
     s.cnt = s.nrm + TC_SLOTS;
     s.grp = s.cnt + TC_SLOTS;
-    s.base = reinterpret_cast<unsigned long long*>(s.grp + TC_SLOTS);
+    s.lim = s.grp + TC_SLOTS;
+    s.scl = reinterpret_cast<float*>(s.lim + TC_SLOTS);
+    s.base = reinterpret_cast<unsigned long long*>(s.scl + TC_SLOTS);
     return s;
 }
 
@@ -147,7 +168,16 @@ __device__ __forceinline__ bool group_any(uint32_t id, bool p) {
 // mbarrier wait is bounded; a group decides to stop with a barrier-OR over
 // its threads, and the other group then times out on its next wait.
 // PASS 0 counts, PASS 1 writes the proposals (FAST: the fast tier's 8-byte
-// form); KIND 0: u8 operands, 1: BF16 with the exact recheck.
+// form); KIND: the operand kind (KIND_U8, KIND_BF16, KIND_FP8).
+//
+// Reduced-precision kinds: a pair side passes when its lower bound
+// d~ - err_c (|a|^2 + |b|^2) is below the target's K-th distance -- every
+// side the FP32 join passes, and a few more, which the merge drops after
+// computing their exact distances.  The proposal carries d~ and APPROX_BIT.
+// Both passes then run the same tiles (all joined rows, not only those with
+// proposals), so every pair's d~ comes from the same MMA position and the
+// two passes decide alike; pass 1 still writes no proposal beyond the range
+// pass 0 reserved, and records DERR_TC_WAIT if a slot's count differs.
 template <int PASS, int KIND, bool FAST>
 __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -175,9 +205,10 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
     const uint32_t tmem = sh.tmem;
 
     // pass 0 joins every row of tiers 0-3; pass 1 only the rows that pass 0
-    // found to have proposals
-    const uint32_t* rcount = PASS == 0 ? a.ctr->ntier : a.ctr->nemit;
-    const uint32_t* rlist = PASS == 0 ? a.tier_rows : a.emit_rows;
+    // found to have proposals (reduced-precision kinds: every row again)
+    constexpr bool APPROX = KIND != KIND_U8;
+    const uint32_t* rcount = (PASS == 0 || APPROX) ? a.ctr->ntier : a.ctr->nemit;
+    const uint32_t* rlist = (PASS == 0 || APPROX) ? a.tier_rows : a.emit_rows;
     uint32_t nt[4];
     uint32_t total = 0;
 #pragma unroll
@@ -236,10 +267,12 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                     const uint32_t id = e & LID_MASK;
                     S.kth[ptid] = a.pdist[(size_t)id * a.K + a.K - 1];
                     S.nrm[ptid] = a.nrm[id];
+                    if (KIND == KIND_FP8) S.scl[ptid] = a.scl[id];
                     S.grp[ptid] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
                     S.cnt[ptid] = 0;
                     if (PASS == 1) {
                         const uint32_t c = a.cntpos[(size_t)row * a.caps + q];
+                        S.lim[ptid] = c;
                         S.base[ptid] = c ? a.boff[id] + atomicAdd(&a.bcur[id], c) : 0ull;
                     }
                 }
@@ -283,22 +316,47 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             if (tid == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint32_t vbase = smem_u32(S.vec);
-                for (uint32_t kk = 0; kk < nchunk / 2; kk++) {  // 32 bytes of K per instruction
-                    const uint64_t desc = smem_desc(vbase + kk * 256, 128, gbytes);
-                    if (KIND == 0)
+                // 32 bytes of K per instruction; the parts of a row lie one
+                // after another along K (cpp chunks of 16 bytes each)
+                const uint32_t nparts = KIND == KIND_U8 ? 1u : KIND == KIND_BF16 ? 2u : 3u;
+                const uint32_t cpp = nchunk / nparts;
+                auto desc_of = [&](uint32_t part, uint32_t kk) {
+                    return smem_desc(vbase + (part * cpp + 2 * kk) * 128, 128, gbytes);
+                };
+                for (uint32_t kk = 0; kk < cpp / 2; kk++) {
+                    if (KIND == KIND_U8) {
+                        const uint64_t desc = desc_of(0, kk);
                         asm volatile(
                             "{\n\t.reg .pred p;\n\t"
                             "setp.ne.b32 p, %4, 0;\n\t"
                             "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
                                 tmem),
                             "l"(desc), "l"(desc), "r"(IDESC_U8), "r"(kk), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-                    else
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\t"
-                            "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-                                tmem),
-                            "l"(desc), "l"(desc), "r"(IDESC_BF16), "r"(kk), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                    } else {
+                        // (A part, B part) products: BF16 hi.hi, hi.lo, lo.hi;
+                        // FP8 hh, hm, mh, hl, lh, mm
+                        constexpr uint32_t NPROD = KIND == KIND_BF16 ? 3u : 6u;
+                        constexpr uint32_t PA[6] = {0, 0, 1, 0, 2, 1}, PB[6] = {0, 1, 0, 2, 0, 1};
+#pragma unroll
+                        for (uint32_t pr = 0; pr < NPROD; pr++) {
+                            const uint64_t da = desc_of(PA[pr], kk), db = desc_of(PB[pr], kk);
+                            const uint32_t acc = (kk | pr) != 0;
+                            if (KIND == KIND_BF16)
+                                asm volatile(
+                                    "{\n\t.reg .pred p;\n\t"
+                                    "setp.ne.b32 p, %4, 0;\n\t"
+                                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                        tmem),
+                                    "l"(da), "l"(db), "r"(IDESC_BF16), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                            else
+                                asm volatile(
+                                    "{\n\t.reg .pred p;\n\t"
+                                    "setp.ne.b32 p, %4, 0;\n\t"
+                                    "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                        tmem),
+                                    "l"(da), "l"(db), "r"(IDESC_E4M3), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                        }
+                    }
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  mma_bar)
@@ -321,6 +379,9 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             const uint32_t row_b = valid_b ? H.row[r_b] : 0u;
             const float kth_b = S.kth[tid];
             const uint32_t nrm_b = S.nrm[tid], grp_b = S.grp[tid];
+            const float scl_b = KIND == KIND_FP8 ? S.scl[tid] : 1.f;
+            const uint32_t lim_b = (PASS == 1 && APPROX) ? S.lim[tid] : 0u;
+            bool over = false;  // pass 1, reduced precision: a write beyond a reserved range
             const uint32_t blk = tid & ~(B - 1);
             uint32_t cb = 0;
             // Rows of at most 32 slots lie inside one warp, so every proposal
@@ -353,25 +414,31 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                             const uint32_t q_a = av & (B - 1);
                             const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
                             const uint32_t e_a = S.ids[av];
-                            float dd;
-                            if (KIND == 0) {
+                            float dd, lb;
+                            if (KIND == KIND_U8) {
                                 dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[j8]);
+                                lb = dd;
                             } else {
-                                // approximate distance; pairs it cannot rule out get
-                                // the reference's exact sum
+                                // d~ and its lower bound (distances are >= 0)
                                 const float ns = __uint_as_float(S.nrm[av]) + __uint_as_float(nrm_b);
-                                dd = ns - 2.f * __uint_as_float(v[j8]);
-                                if (pv && dd - a.err_c * ns < fmaxf(S.kth[av], kth_b))
-                                    dd = exact_l2(a.x, a.dp, e_a & LID_MASK, e_b & LID_MASK);
+                                float gd = __uint_as_float(v[j8]);
+                                if (KIND == KIND_FP8) gd *= S.scl[av] * scl_b;
+                                dd = fmaxf(ns - 2.f * gd, 0.f);
+                                lb = dd - a.err_c * ns;
+                                if (PASS == 0 && a.audit && pv) {  // the bound against the exact distance
+                                    const float ex = audit_l2(a.x, a.dp, e_a & LID_MASK, e_b & LID_MASK);
+                                    if (!(ex >= lb && ex <= dd + a.err_c * ns)) atomicOr(a.tc_err, (unsigned)DERR_BOUND);
+                                }
                             }
+                            const uint32_t axb = APPROX ? APPROX_BIT : 0u;
                             uint32_t outer = 0, inner = 0;
                             const bool ok = pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, S.grp[av],
                                                              grp_b, outer, inner);
                             const float kth_a = S.kth[av];
                             if (PASS == 0) {
                                 cmps += ok;
-                                cb += (ok && dd < kth_b);
-                                const unsigned m = __ballot_sync(0xffffffffu, ok && dd < kth_a);
+                                cb += (ok && lb < kth_b);
+                                const unsigned m = __ballot_sync(0xffffffffu, ok && lb < kth_a);
                                 if (wl) {
                                     if (lane == (av & 31)) cnt_r += __popc(m);
                                 } else if (m && lane == 0) {
@@ -379,7 +446,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                                 }
                             } else {
                                 const uint32_t pidx = outer * S_b + inner;
-                                const bool pa = ok && dd < kth_a;
+                                const bool pa = ok && lb < kth_a;
                                 const unsigned m = __ballot_sync(0xffffffffu, pa);
                                 if (m) {
                                     uint32_t base;
@@ -398,13 +465,20 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                                     if (pa) {
                                         const uint32_t before = __popc(m & ((1u << lane) - 1u));
                                         const unsigned long long slot = S.base[av] + base + before;
-                                        put_prop<FAST>(a.bucket, slot, dd, e_b, row_b, pidx, outer == q_a ? 0u : 1u);
+                                        if (!APPROX || base + before < S.lim[av])
+                                            put_prop<FAST>(a.bucket, slot, dd, e_b | axb, row_b, pidx,
+                                                           outer == q_a ? 0u : 1u);
+                                        else
+                                            over = true;
                                     }
                                 }
-                                if (ok && dd < kth_b) {
+                                if (ok && lb < kth_b) {
                                     const uint32_t pos = wl ? cnt_r++ : atomicAdd(&S.cnt[tid], 1u);
                                     const unsigned long long slot = S.base[tid] + pos;
-                                    put_prop<FAST>(a.bucket, slot, dd, e_a, row_b, pidx, outer == q_b ? 0u : 1u);
+                                    if (!APPROX || pos < lim_b)
+                                        put_prop<FAST>(a.bucket, slot, dd, e_a | axb, row_b, pidx, outer == q_b ? 0u : 1u);
+                                    else
+                                        over = true;
                                 }
                             }
                         }
@@ -421,6 +495,10 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
             group_sync(BAR_CONS);
+            if (PASS == 1 && APPROX) {  // every reserved range filled exactly
+                const uint32_t got = wl_tile ? cnt_r : S.cnt[tid];
+                if (over || (valid_b && got != lim_b)) atomicOr(a.tc_err, (unsigned)DERR_TC_RANGE);
+            }
             if (PASS == 0) {
                 if (valid_b) {
                     const uint32_t c = S.cnt[tid];
@@ -488,27 +566,31 @@ __global__ void k_quantize(const float* x, uint32_t n, uint32_t d, uint32_t dp, 
     }
 }
 
-// Warp per vector: the BF16 copy (round to nearest even, zero padded to kq
-// bytes) and the squared norm (double sum, rounded to float).  Flags rows
-// the BF16 bound does not cover: non-finite components, or nonzero ones
-// outside [2^-60, 2^50] (products must stay normal and sums finite).
-__global__ void k_to_bf16(const float* x, uint32_t n, uint32_t d, uint32_t dp, uint32_t kq, __nv_bfloat16* xb,
-                          uint32_t* nrm, unsigned* bad) {
+// Warp per vector: the BF16 parts hi = bf16(x) and lo = bf16(x - hi)
+// (round to nearest even), stored one after the other along K (each part
+// dpad = d rounded up to 16 elements, zero padded), and the squared norm
+// (double sum, rounded to float).  Flags rows the bound does not cover:
+// non-finite components, or nonzero ones outside [2^-60, 2^50] (products of
+// parts must stay normal and sums finite).
+__global__ void k_to_bf16x2(const float* x, uint32_t n, uint32_t d, uint32_t dp, uint32_t dpad, __nv_bfloat16* xb,
+                            uint32_t* nrm, unsigned* bad) {
     const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const uint32_t lane = threadIdx.x & 31;
     if (row >= n) return;
     const float* src = x + (size_t)row * dp;
-    __nv_bfloat16* dst = xb + (size_t)row * (kq / 2);
+    __nv_bfloat16* dst = xb + (size_t)row * 2 * dpad;
     double s = 0.0;
     bool ok = true;
-    for (uint32_t k = lane; k < kq / 2; k += 32) {
+    for (uint32_t k = lane; k < dpad; k += 32) {
         float v = 0.f;
         if (k < d) {
             v = src[k];
             const float m = fabsf(v);
             if (!(m <= 0x1p50f) || (m != 0.f && m < 0x1p-60f)) ok = false;
         }
-        dst[k] = __float2bfloat16_rn(v);
+        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+        dst[k] = hi;
+        dst[dpad + k] = __float2bfloat16_rn(v - __bfloat162float(hi));
         s += (double)v * (double)v;
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -519,11 +601,102 @@ __global__ void k_to_bf16(const float* x, uint32_t n, uint32_t d, uint32_t dp, u
     }
 }
 
+__device__ __forceinline__ float e4m3_value(__nv_fp8_storage_t q) {
+    return __half2float(__half(__nv_cvt_fp8_to_halfraw(q, __NV_E4M3)));
+}
+
+// Warp per vector: the FP8 (E4M3) parts.  The row is scaled by 2^e, the
+// power of two that brings its largest magnitude into (224, 448] (448 is
+// E4M3's largest finite value; scaling by a power of two is exact), then
+// hi = e4m3(x 2^e), mid = e4m3(x 2^e - hi), lo = e4m3(x 2^e - hi - mid),
+// round to nearest even, the residuals exact in FP32.  Parts one after the
+// other along K (each dpad = d rounded up to 32 bytes, zero padded); scl =
+// 2^-e; squared norm as for BF16.  Flags rows with non-finite components or
+// a nonzero largest magnitude outside [2^-60, 2^50].
+__global__ void k_to_fp8x3(const float* x, uint32_t n, uint32_t d, uint32_t dp, uint32_t dpad, uint8_t* xq,
+                           uint32_t* nrm, float* scl, unsigned* bad) {
+    const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float* src = x + (size_t)row * dp;
+    uint8_t* dst = xq + (size_t)row * 3 * dpad;
+    float mx = 0.f;
+    bool ok = true;
+    double s = 0.0;
+    for (uint32_t k = lane; k < d; k += 32) {
+        const float v = src[k];
+        if (!(fabsf(v) <= 0x1p50f)) ok = false;
+        mx = fmaxf(mx, fabsf(v));
+        s += (double)v * (double)v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    }
+    if (mx != 0.f && mx < 0x1p-60f) ok = false;
+    // 2^e with mx 2^e in (224, 448]: e = floor(log2(448 / mx))
+    int e = 0;
+    if (mx > 0.f) {
+        int ex;
+        frexpf(mx, &ex);  // mx = f 2^ex, f in [0.5, 1)
+        e = 8 - ex;       // mx 2^e in [128, 256)
+        if (ldexpf(mx, e + 1) <= 448.f) e++;
+    }
+    for (uint32_t k = lane; k < dpad; k += 32) {
+        const float v = k < d ? ldexpf(src[k], e) : 0.f;
+        const __nv_fp8_storage_t h = __nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
+        const float r1 = v - e4m3_value(h);
+        const __nv_fp8_storage_t m = __nv_cvt_float_to_fp8(r1, __NV_SATFINITE, __NV_E4M3);
+        const float r2 = r1 - e4m3_value(m);
+        dst[k] = h;
+        dst[dpad + k] = m;
+        dst[2 * dpad + k] = __nv_cvt_float_to_fp8(r2, __NV_SATFINITE, __NV_E4M3);
+    }
+    const bool all_ok = __all_sync(0xffffffffu, ok);
+    if (lane == 0) {
+        nrm[row] = __float_as_uint((float)s);
+        scl[row] = ldexpf(1.f, -e);
+        if (!all_ok) atomicOr(bad, 1u);
+    }
+}
+
 }  // namespace
+
+// err_c of the reduced-precision kinds: |d~ - d| <= err_c (|a|^2 + |b|^2)
+// for d~ = |a|^2 + |b|^2 - 2 G~ against the reference's FP32 distance d,
+// with |a||b| <= (|a|^2 + |b|^2) / 2 (so 2 |G~ - a.b| <= c (|a|^2 + |b|^2)
+// when |G~ - a.b| <= c |a||b|):
+//   parts      BF16 (unit roundoff u = 2^-8): a = hi + lo + e, |e| <= u^2 |a|,
+//              the dropped lo.lo and e terms <= 3.1 u^2 |a_i||b_i| a component;
+//              FP8 E4M3 (u = 2^-4, subnormal spacing 2^-9 after the 2^e
+//              scaling): the dropped ml, lm, ll and residual terms <= 4.1 u^3
+//              |a_i||b_i| + 3 2^-9 (|a_i| + |b_i|) scaled, i.e. + 6 sqrt(d)
+//              2^-9 / 224 |a||b| after unscaling (the scale puts each row's
+//              largest component above 224);
+//   accumulate FP32 adds of all products, truncation allowed: 1.02 (P d + P)
+//              2^-23 (P products per component), plus an allowance for the
+//              MMA's internal grouping of 2^-16 (BF16) and 1.1 2^-13 (FP8);
+//   norms      float of a double sum: 2^-24; final add and subtract: 2^-23;
+//   reference  its own sequential FP32 sum: (d + 1) 2^-23 of a distance
+//              <= 2 (|a|^2 + |b|^2);
+// times a 1.25 safety factor.  Tests run the joins with every pair's exact
+// distance checked against this bound (nnm_opts.audit).
+static double err_coef(uint32_t kind, uint32_t d) {
+    const double dd = (double)d, e23 = std::ldexp(1.0, -23);
+    const double tail = std::ldexp(1.0, -24) + e23 + (dd + 1) * e23;
+    if (kind == KIND_BF16) {
+        const double u = std::ldexp(1.0, -8);
+        return 1.25 * (3.1 * u * u + 1.02 * (3 * dd + 3) * e23 + std::ldexp(1.0, -16) + tail);
+    }
+    const double u = std::ldexp(1.0, -4);
+    return 1.25 * (4.1 * u * u * u + 6.0 * std::sqrt(dd) * std::ldexp(1.0, -9) / 224.0 +
+                   1.1 * std::ldexp(1.0, -13) + 1.02 * (6 * dd + 6) * e23 + tail);
+}
 
 int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
     g.xq = nullptr;
     g.nrm = nullptr;
+    g.scl = nullptr;
     g.kq = 0;
     if (g.join_kernel == NNM_JOIN_FP32) return 0;
     const uint32_t kq = (g.d + 31) & ~31u;
@@ -531,63 +704,82 @@ int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
     if (g.metric != L2) why = "the tensor-core join needs the L2 metric";
     else if (kq > TC_MAX_KQ) why = "the tensor-core join takes d <= 768";
     if (!why) {
-        NNM_CUDA_TRY(s.xq.ensure((size_t)g.n_cap * kq));
         NNM_CUDA_TRY(s.nrm.ensure((size_t)g.n_cap * 4));
         DevBuf& m = ctx.ws.misc;
         NNM_CUDA_TRY(m.ensure(64));
-        NNM_CUDA_TRY(cudaMemsetAsync(m.p, 0, 16, ctx.stream));
         unsigned* flags = m.as<unsigned>();
-        k_quantize<<<(g.n_cap + 7) / 8, 256, 0, ctx.stream>>>(g.x, g.n_cap, g.d, g.dp, kq, s.xq.as<uint8_t>(),
-                                                              s.nrm.as<uint32_t>(), flags, flags + 1); count_launch();
         unsigned h[2] = {0, 0};
-        NNM_CUDA_TRY(cudaMemcpyAsync(h, flags, 8, cudaMemcpyDeviceToHost, ctx.stream));
-        NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
-        // every squared distance is at most |a|^2 + |b|^2 for non-negative vectors
-        if (!h[0] && 2ull * h[1] < (1ull << 24)) {
-            g.xq = s.xq.as<uint8_t>();
-            g.nrm = s.nrm.as<uint32_t>();
-            g.kq = kq;
-            g.tc_kind = 0;
-            return 0;
-        }
-        // other data: BF16 Gram matrices with the FP32 recheck, on request
-        // only -- the rigorous BF16 bound (about 2^-8 of |a|^2 + |b|^2)
-        // leaves most candidate pairs inside the recheck band, and the
-        // per-pair exact sums then cost more than the FP32 join (measured
-        // 3-4x slower per iteration on unit-norm 96-d data)
-        const uint32_t kqb = 2 * ((g.d + 15) & ~15u);
-        if (g.join_kernel != NNM_JOIN_TENSOR) {
-            why = "auto: FP32 join for non-integer data";
-        } else if (kqb > TC_MAX_KQ) {
-            why = "the BF16 tensor-core join takes d <= 384";
-        } else {
-            NNM_CUDA_TRY(s.xq.ensure((size_t)g.n_cap * kqb));
+        if (g.join_kernel != NNM_JOIN_FP8) {
+            NNM_CUDA_TRY(s.xq.ensure((size_t)g.n_cap * kq));
             NNM_CUDA_TRY(cudaMemsetAsync(m.p, 0, 16, ctx.stream));
-            k_to_bf16<<<(g.n_cap + 7) / 8, 256, 0, ctx.stream>>>(g.x, g.n_cap, g.d, g.dp, kqb,
-                                                                 s.xq.as<__nv_bfloat16>(), s.nrm.as<uint32_t>(), flags); count_launch();
-            NNM_CUDA_TRY(cudaMemcpyAsync(h, flags, 4, cudaMemcpyDeviceToHost, ctx.stream));
+            k_quantize<<<(g.n_cap + 7) / 8, 256, 0, ctx.stream>>>(g.x, g.n_cap, g.d, g.dp, kq, s.xq.as<uint8_t>(),
+                                                                  s.nrm.as<uint32_t>(), flags, flags + 1); count_launch();
+            NNM_CUDA_TRY(cudaMemcpyAsync(h, flags, 8, cudaMemcpyDeviceToHost, ctx.stream));
             NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
-            if (h[0]) {
-                why = "the BF16 tensor-core join needs finite components with magnitudes in [2^-60, 2^50]";
-            } else {
+            // every squared distance is at most |a|^2 + |b|^2 for non-negative vectors
+            if (!h[0] && 2ull * h[1] < (1ull << 24)) {
                 g.xq = s.xq.as<uint8_t>();
                 g.nrm = s.nrm.as<uint32_t>();
-                g.kq = kqb;
-                g.tc_kind = 1;
-                // |computed - reference| <= err_c (|a|^2 + |b|^2): BF16 inputs
-                // (2 x 2^-9 relative per product), FP32 accumulation of d
-                // terms (d 2^-22, truncating adds allowed), the float norms
-                // and the final two operations (2^-21), and the reference's
-                // own sequential sum ((d + 2) 2^-23 of a distance <= 2(|a|^2 +
-                // |b|^2)); |a||b| <= (|a|^2 + |b|^2) / 2; a 1.25 safety factor
-                const double dd = (double)g.d;
-                g.err_c = (float)(1.25 * (std::ldexp(1.0, -8) + std::ldexp(1.0, -18) + (2 * dd + 4) * std::ldexp(1.0, -22) +
-                                          std::ldexp(1.0, -21)));
+                g.kq = kq;
+                g.tc_kind = KIND_U8;
                 return 0;
             }
         }
+        // other data: BF16 (hi + lo) Gram matrices on request; FP8 (E4M3
+        // hi + mid + lo, per-row power-of-two scales) on request for any data
+        if (g.join_kernel == NNM_JOIN_AUTO) {
+            why = "auto: FP32 join for non-integer data";
+        } else if (g.join_kernel == NNM_JOIN_TENSOR) {
+            const uint32_t dpad = (g.d + 15) & ~15u, kqb = 4 * dpad;
+            if (kqb > TC_MAX_KQ) {
+                why = "the BF16 tensor-core join takes d <= 192";
+            } else {
+                NNM_CUDA_TRY(s.xq.ensure((size_t)g.n_cap * kqb));
+                NNM_CUDA_TRY(cudaMemsetAsync(m.p, 0, 16, ctx.stream));
+                k_to_bf16x2<<<(g.n_cap + 7) / 8, 256, 0, ctx.stream>>>(g.x, g.n_cap, g.d, g.dp, dpad,
+                                                                       s.xq.as<__nv_bfloat16>(),
+                                                                       s.nrm.as<uint32_t>(), flags); count_launch();
+                NNM_CUDA_TRY(cudaMemcpyAsync(h, flags, 4, cudaMemcpyDeviceToHost, ctx.stream));
+                NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+                if (h[0]) {
+                    why = "the BF16 tensor-core join needs finite components with magnitudes in [2^-60, 2^50]";
+                } else {
+                    g.xq = s.xq.as<uint8_t>();
+                    g.nrm = s.nrm.as<uint32_t>();
+                    g.kq = kqb;
+                    g.tc_kind = KIND_BF16;
+                    g.err_c = (float)err_coef(KIND_BF16, g.d);
+                    return 0;
+                }
+            }
+        } else {  // NNM_JOIN_FP8
+            const uint32_t dpad = (g.d + 31) & ~31u, kq8 = 3 * dpad;
+            if (kq8 > TC_MAX_KQ) {
+                why = "the FP8 tensor-core join takes d <= 256";
+            } else {
+                NNM_CUDA_TRY(s.xq.ensure((size_t)g.n_cap * kq8));
+                NNM_CUDA_TRY(s.scl.ensure((size_t)g.n_cap * 4));
+                NNM_CUDA_TRY(cudaMemsetAsync(m.p, 0, 16, ctx.stream));
+                k_to_fp8x3<<<(g.n_cap + 7) / 8, 256, 0, ctx.stream>>>(g.x, g.n_cap, g.d, g.dp, dpad, s.xq.as<uint8_t>(),
+                                                                      s.nrm.as<uint32_t>(), s.scl.as<float>(),
+                                                                      flags); count_launch();
+                NNM_CUDA_TRY(cudaMemcpyAsync(h, flags, 4, cudaMemcpyDeviceToHost, ctx.stream));
+                NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+                if (h[0]) {
+                    why = "the FP8 tensor-core join needs finite components with magnitudes in [2^-60, 2^50]";
+                } else {
+                    g.xq = s.xq.as<uint8_t>();
+                    g.nrm = s.nrm.as<uint32_t>();
+                    g.scl = s.scl.as<float>();
+                    g.kq = kq8;
+                    g.tc_kind = KIND_FP8;
+                    g.err_c = (float)err_coef(KIND_FP8, g.d);
+                    return 0;
+                }
+            }
+        }
     }
-    if (why && g.join_kernel == NNM_JOIN_TENSOR) {
+    if (why && (g.join_kernel == NNM_JOIN_TENSOR || g.join_kernel == NNM_JOIN_FP8)) {
         ctx.last_error = why;
         return 1;  // NNM_ERR_INVALID
     }
@@ -597,11 +789,13 @@ int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
 cudaError_t tc_set_attributes(uint32_t kq, uint32_t kind) {
     const int bytes = (int)std::max<size_t>(tc_smem_bytes(kq), TC_SMEM_FLOOR);
     cudaError_t e;
-    const void* fns[2][3] = {{(const void*)k_join_tc<0, 0, false>, (const void*)k_join_tc<1, 0, false>,
-                              (const void*)k_join_tc<1, 0, true>},
-                             {(const void*)k_join_tc<0, 1, false>, (const void*)k_join_tc<1, 1, false>,
-                              (const void*)k_join_tc<1, 1, true>}};
-    for (const void* f : fns[kind ? 1 : 0])
+    const void* fns[3][3] = {{(const void*)k_join_tc<0, KIND_U8, false>, (const void*)k_join_tc<1, KIND_U8, false>,
+                              (const void*)k_join_tc<1, KIND_U8, true>},
+                             {(const void*)k_join_tc<0, KIND_BF16, false>, (const void*)k_join_tc<1, KIND_BF16, false>,
+                              (const void*)k_join_tc<1, KIND_BF16, true>},
+                             {(const void*)k_join_tc<0, KIND_FP8, false>, (const void*)k_join_tc<1, KIND_FP8, false>,
+                              (const void*)k_join_tc<1, KIND_FP8, true>}};
+    for (const void* f : fns[kind < 3 ? kind : 0])
         if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
     return cudaSuccess;
 }
@@ -613,14 +807,18 @@ cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, 
     const unsigned grid = std::min<unsigned>(tiles, (unsigned)nsm * 4);
     const size_t bytes = std::max<size_t>(tc_smem_bytes(ja.kq), TC_SMEM_FLOOR);
     const bool fast = ja.fast_key != 0;
-    if (ja.tc_kind == 0) {
-        if (pass == 0) k_join_tc<0, 0, false><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else if (fast) k_join_tc<1, 0, true><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else k_join_tc<1, 0, false><<<grid, TC_THREADS, bytes, st>>>(ja);
+    if (ja.tc_kind == KIND_U8) {
+        if (pass == 0) k_join_tc<0, KIND_U8, false><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else if (fast) k_join_tc<1, KIND_U8, true><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else k_join_tc<1, KIND_U8, false><<<grid, TC_THREADS, bytes, st>>>(ja);
+    } else if (ja.tc_kind == KIND_BF16) {
+        if (pass == 0) k_join_tc<0, KIND_BF16, false><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else if (fast) k_join_tc<1, KIND_BF16, true><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else k_join_tc<1, KIND_BF16, false><<<grid, TC_THREADS, bytes, st>>>(ja);
     } else {
-        if (pass == 0) k_join_tc<0, 1, false><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else if (fast) k_join_tc<1, 1, true><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else k_join_tc<1, 1, false><<<grid, TC_THREADS, bytes, st>>>(ja);
+        if (pass == 0) k_join_tc<0, KIND_FP8, false><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else if (fast) k_join_tc<1, KIND_FP8, true><<<grid, TC_THREADS, bytes, st>>>(ja);
+        else k_join_tc<1, KIND_FP8, false><<<grid, TC_THREADS, bytes, st>>>(ja);
     }
     count_launch();
     return cudaGetLastError();

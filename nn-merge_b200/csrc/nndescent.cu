@@ -727,7 +727,38 @@ struct MergeArgs {
     const void* bucket;  // Prop (exact tier) or Prop8 (fast tier) entries
     uint8_t* nflag;
     IterCounters* ctr;
+    // reduced-precision joins: proposals flagged APPROX_BIT carry d~; the
+    // exact distance is the sequential FP32 sum of the rows of x, and
+    // |d~ - d| <= err_c * (nrm[t] + nrm[u]) (float norms)
+    const float* x;
+    uint32_t dp;
+    const uint32_t* nrm;
+    float err_c;
 };
+
+// Proposal number i of the bucket array: distance bits and list entry (and,
+// exact tier, the key).
+template <bool FAST>
+__device__ __forceinline__ void load_prop(const void* bucket, unsigned long long i, uint32_t& dbits, uint32_t& idg,
+                                          unsigned long long& key) {
+    if (FAST) {
+        const uint2 p = reinterpret_cast<const uint2*>(bucket)[i];
+        dbits = p.x;
+        idg = p.y;
+        key = fast_key(idg);
+    } else {
+        const Prop p = reinterpret_cast<const Prop*>(bucket)[i];
+        dbits = __float_as_uint(p.dist);
+        idg = p.idg;
+        key = p.key;
+    }
+}
+
+// The reference's FP32 distance of rows t and u (the reduced-precision
+// joins' exact value), one non-inlined copy.
+__device__ __noinline__ float merge_exact_l2(const float* x, uint32_t dp, uint32_t t, uint32_t u) {
+    return dist_seq<L2>(x + (size_t)t * dp, x + (size_t)u * dp, (int)dp);
+}
 
 struct MEnt {
     uint32_t d;
@@ -828,105 +859,6 @@ __device__ __forceinline__ void warp_sort_ment(uint32_t& pd, unsigned long long&
         }
 }
 
-// One warp per target.  Proposals that pass the current K-th entry are
-// collected in a 32-entry buffer; a full buffer (and the rest at the end)
-// is sorted and merged into the pool, which lowers the K-th entry for the
-// proposals still to come.
-// Eight blocks (64 warps) per SM, registers capped at 32: the merge waits on
-// scattered bucket and pool reads, and the added warps hide more of that
-// latency -- the 1M build is 2.4 % faster than at the uncapped 48 registers.
-// The kernel is bound by instruction fetch (the GPC instruction cache ran at
-// 96 % of its request rate with the flush inlined twice), so the flush and
-// the pool-side binary search each have a single inlined copy: 9 % off the
-// 1M build.
-__global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
-    __shared__ MEnt sm[MERGE_WARPS][64];
-    __shared__ MEnt kept[MERGE_WARPS][32];
-    __shared__ MEnt buf[MERGE_WARPS][32];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t t = blockIdx.x * MERGE_WARPS + w;
-    uint32_t nfl = 0;
-    if (t < a.n) {
-        const uint32_t K = a.K;
-        const uint32_t c = a.bcnt[t];
-        if (c) {
-            uint32_t cd = 0xffffffffu, ce = 0;
-            unsigned long long ck = ~0ull;
-            if (lane < (int)K) {
-                ce = a.pid[(size_t)t * K + lane];
-                cd = __float_as_uint(a.pdist[(size_t)t * K + lane]);
-                ck = (unsigned long long)lane;  // start entries precede every proposal of equal distance
-            }
-            uint32_t kd = __shfl_sync(FULL, cd, K - 1);
-            unsigned long long kk = __shfl_sync(FULL, ck, K - 1);
-            const unsigned long long b_first = a.boff[t];
-            const unsigned lt = (1u << lane) - 1u;
-            uint32_t nb = 0;  // entries in buf
-            auto flush = [&]() {
-                uint32_t pd = 0xffffffffu, pe = 0;
-                unsigned long long pk = ~0ull;
-                if (lane < (int)nb) {
-                    const MEnt me = buf[w][lane];
-                    pd = me.d;
-                    pe = me.e;
-                    pk = me.k;
-                }
-                __syncwarp();
-                warp_sort_ment(pd, pk, pe);
-                merge_round(pd, pk, pe, nb, K, cd, ce, ck, sm[w], kept[w]);
-                kd = __shfl_sync(FULL, cd, K - 1);
-                kk = __shfl_sync(FULL, ck, K - 1);
-                nb = 0;
-            };
-            // One call site of flush (its sort and merge are long): a full
-            // buffer flushes inside the loop, the last partial one after the
-            // final chunk, at the same points of the proposal stream as
-            // before.
-            for (uint32_t b0 = 0;; b0 += 32) {
-                uint32_t pd = 0xffffffffu, pe = 0;
-                unsigned long long pk = ~0ull;
-                bool rest = false;
-                const bool last = b0 >= c;
-                if (last) {
-                    if (nb == 0) break;
-                } else {
-                    bool valid = false;
-                    if (b0 + lane < c) {
-                        const Prop p = reinterpret_cast<const Prop*>(a.bucket)[b_first + b0 + lane];
-                        pd = __float_as_uint(p.dist);
-                        pk = p.key;
-                        pe = (p.idg & LID_MASK) | ((p.idg >> 31) << 30) | FLAG_BIT;
-                        valid = mless(pd, pk, kd, kk);
-                    }
-                    const unsigned vb = __ballot_sync(FULL, valid);
-                    if (!vb) continue;
-                    const uint32_t take = min((uint32_t)__popc(vb), 32u - nb);
-                    const uint32_t rank = __popc(vb & lt);
-                    if (valid && rank < take) buf[w][nb + rank] = MEnt{pd, pe, pk};
-                    __syncwarp();
-                    nb += take;
-                    if (nb < 32) continue;
-                    rest = valid && rank >= take;
-                }
-                flush();
-                if (last) break;
-                // the rest of this chunk, against the new K-th entry
-                rest = rest && mless(pd, pk, kd, kk);
-                const unsigned rb = __ballot_sync(FULL, rest);
-                if (rest) buf[w][__popc(rb & lt)] = MEnt{pd, pe, pk};
-                __syncwarp();
-                nb = __popc(rb);
-            }
-            if (lane < (int)K) {
-                a.pid[(size_t)t * K + lane] = ce;
-                a.pdist[(size_t)t * K + lane] = __uint_as_float(cd);
-            }
-            nfl = __popc(__ballot_sync(FULL, lane < (int)K && (ce & FLAG_BIT)));
-        }
-        if (lane == 0) a.nflag[t] = (uint8_t)nfl;
-    }
-}
-
 // Fast-tier merge.  A fast-tier key is a function of the entry (fast_key),
 // so an entry and its order fit one 64-bit word:
 //   dist bits (63..32) | id (31..2) | new flag (1) | group bit ^ 1 (0)
@@ -975,6 +907,209 @@ __device__ __forceinline__ unsigned long long fm_bitonic_merge32(unsigned long l
 
 constexpr unsigned long long FM_EMPTY = ~0ull;
 
+// Reduced-precision joins: an upper bound (float bits) of the K-th exact
+// distance the merge will leave -- the K-th smallest of the start pool's
+// exact distances and, for each id proposed and not in the pool, one upper
+// bound of its distance (d~ + err_c (|t|^2 + |u|^2), or the exact value).
+// Any set of K distinct ids bounds the final K-th entry from above, so a
+// proposal whose lower bound exceeds it cannot enter the pool.  The 32
+// smallest upper bounds are kept by a buffered warp sort, then ids already
+// in the pool or repeated among them are dropped.  pool_d / pool_id: the
+// start pool in lanes < K, ascending distances; scratch: 32 words.
+template <bool FAST>
+__device__ uint32_t approx_bound(const MergeArgs& a, unsigned long long b_first, uint32_t c, uint32_t K,
+                                 uint32_t pool_d, uint32_t pool_id, float nt, unsigned long long* scratch) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    constexpr unsigned long long EMPTY = ~0ull;
+    unsigned long long kept = EMPTY, klast = EMPTY;
+    uint32_t nb = 0;
+    for (uint32_t b0 = 0;; b0 += 32) {
+        const bool last = b0 >= c;
+        unsigned long long v = EMPTY;
+        bool rest = false;
+        if (last) {
+            if (nb == 0) break;
+        } else {
+            bool valid = false;
+            if (b0 + lane < c) {
+                uint32_t dbits, idg;
+                unsigned long long key;
+                load_prop<FAST>(a.bucket, b_first + b0 + lane, dbits, idg, key);
+                const uint32_t id = idg & ID_MASK;
+                float ub = __uint_as_float(dbits);
+                if (idg & APPROX_BIT) ub += a.err_c * (nt + __uint_as_float(a.nrm[id]));
+                v = ((unsigned long long)__float_as_uint(ub) << 32) | id;
+                valid = v < klast;
+            }
+            const unsigned vb = __ballot_sync(FULL, valid);
+            if (!vb) continue;
+            const uint32_t take = min((uint32_t)__popc(vb), 32u - nb);
+            const uint32_t rank = __popc(vb & lt);
+            if (valid && rank < take) scratch[nb + rank] = v;
+            __syncwarp();
+            nb += take;
+            if (nb < 32) continue;
+            rest = valid && rank >= take;
+        }
+        unsigned long long bv = lane < (int)nb ? scratch[lane] : EMPTY;
+        __syncwarp();
+        // the 32 smallest of kept and the buffer
+        bv = fm_sort32(bv);
+        kept = fm_bitonic_merge32(min(kept, __shfl_sync(FULL, bv, 31 - lane)));
+        klast = __shfl_sync(FULL, kept, 31);
+        nb = 0;
+        if (last) break;
+        rest = rest && v < klast;
+        const unsigned rb = __ballot_sync(FULL, rest);
+        if (rest) scratch[__popc(rb & lt)] = v;
+        __syncwarp();
+        nb = __popc(rb);
+    }
+    // one value per id: drop ids of the pool and repeats (kept is sorted by
+    // value, so the first copy of an id is its smallest bound)
+    const uint32_t kid = (uint32_t)kept;
+    bool drop = kept == EMPTY;
+    for (uint32_t j = 0; j < K; j++) drop |= (__shfl_sync(FULL, pool_id, j) & ID_MASK) == kid;
+    for (int j = 0; j < 31; j++) {
+        const uint32_t o = __shfl_sync(FULL, kid, j);
+        if (j < lane && o == kid) drop = true;
+    }
+    unsigned long long kv = drop ? EMPTY : (kept & 0xffffffff00000000ull) | 0xffffffffull;
+    kv = fm_sort32(kv);
+    const unsigned long long pw = lane < (int)K ? (((unsigned long long)pool_d << 32) | (uint32_t)lane) : EMPTY;
+    const unsigned long long lo = fm_bitonic_merge32(min(pw, __shfl_sync(FULL, kv, 31 - lane)));
+    return (uint32_t)(__shfl_sync(FULL, lo, K - 1) >> 32);
+}
+
+// One warp per target.  Proposals that pass the current K-th entry are
+// collected in a 32-entry buffer; a full buffer (and the rest at the end)
+// is sorted and merged into the pool, which lowers the K-th entry for the
+// proposals still to come.
+// Eight blocks (64 warps) per SM, registers capped at 32: the merge waits on
+// scattered bucket and pool reads, and the added warps hide more of that
+// latency -- the 1M build is 2.4 % faster than at the uncapped 48 registers.
+// The kernel is bound by instruction fetch (the GPC instruction cache ran at
+// 96 % of its request rate with the flush inlined twice), so the flush and
+// the pool-side binary search each have a single inlined copy: 9 % off the
+// 1M build.
+// APPROX: proposals may carry the reduced-precision joins' d~ (APPROX_BIT);
+// a first pass bounds the final K-th distance, the second buffers only the
+// proposals whose lower bound d~ - err_c (|t|^2 + |u|^2) reaches it and
+// computes their exact distances at the flush -- so the pool gets what the
+// FP32 join's proposals would give it.
+template <bool APPROX>
+__global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
+    __shared__ MEnt sm[MERGE_WARPS][64];
+    __shared__ MEnt kept[MERGE_WARPS][32];
+    __shared__ MEnt buf[MERGE_WARPS][32];
+    __shared__ uint8_t bufax[APPROX ? MERGE_WARPS : 1][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t t = blockIdx.x * MERGE_WARPS + w;
+    uint32_t nfl = 0;
+    if (t < a.n) {
+        const uint32_t K = a.K;
+        const uint32_t c = a.bcnt[t];
+        if (c) {
+            uint32_t cd = 0xffffffffu, ce = 0;
+            unsigned long long ck = ~0ull;
+            if (lane < (int)K) {
+                ce = a.pid[(size_t)t * K + lane];
+                cd = __float_as_uint(a.pdist[(size_t)t * K + lane]);
+                ck = (unsigned long long)lane;  // start entries precede every proposal of equal distance
+            }
+            uint32_t kd = __shfl_sync(FULL, cd, K - 1);
+            unsigned long long kk = __shfl_sync(FULL, ck, K - 1);
+            const unsigned long long b_first = a.boff[t];
+            const unsigned lt = (1u << lane) - 1u;
+            float nt = 0.f;
+            uint32_t bound = 0xffffffffu;
+            if (APPROX) {
+                nt = __uint_as_float(a.nrm[t]);
+                bound = approx_bound<false>(a, b_first, c, K, cd, ce, nt,
+                                            reinterpret_cast<unsigned long long*>(&sm[w][0]));
+            }
+            uint32_t nb = 0;  // entries in buf
+            auto flush = [&]() {
+                uint32_t pd = 0xffffffffu, pe = 0;
+                unsigned long long pk = ~0ull;
+                if (lane < (int)nb) {
+                    const MEnt me = buf[w][lane];
+                    pd = me.d;
+                    pe = me.e;
+                    pk = me.k;
+                    if (APPROX && bufax[w][lane])
+                        pd = __float_as_uint(merge_exact_l2(a.x, a.dp, t, pe & ID_MASK));
+                }
+                __syncwarp();
+                warp_sort_ment(pd, pk, pe);
+                merge_round(pd, pk, pe, nb, K, cd, ce, ck, sm[w], kept[w]);
+                kd = __shfl_sync(FULL, cd, K - 1);
+                kk = __shfl_sync(FULL, ck, K - 1);
+                nb = 0;
+            };
+            // One call site of flush (its sort and merge are long): a full
+            // buffer flushes inside the loop, the last partial one after the
+            // final chunk, at the same points of the proposal stream as
+            // before.
+            for (uint32_t b0 = 0;; b0 += 32) {
+                uint32_t pd = 0xffffffffu, pe = 0;
+                unsigned long long pk = ~0ull;
+                bool rest = false, ax = false;
+                float lb = 0.f;
+                const bool last = b0 >= c;
+                if (last) {
+                    if (nb == 0) break;
+                } else {
+                    bool valid = false;
+                    if (b0 + lane < c) {
+                        const Prop p = reinterpret_cast<const Prop*>(a.bucket)[b_first + b0 + lane];
+                        pd = __float_as_uint(p.dist);
+                        pk = p.key;
+                        pe = (p.idg & ID_MASK) | ((p.idg >> 31) << 30) | FLAG_BIT;
+                        if (APPROX && (p.idg & APPROX_BIT)) {
+                            ax = true;
+                            lb = p.dist - a.err_c * (nt + __uint_as_float(a.nrm[p.idg & ID_MASK]));
+                            valid = lb <= __uint_as_float(bound) && lb <= __uint_as_float(kd);
+                        } else {
+                            valid = mless(pd, pk, kd, kk);
+                        }
+                    }
+                    const unsigned vb = __ballot_sync(FULL, valid);
+                    if (!vb) continue;
+                    const uint32_t take = min((uint32_t)__popc(vb), 32u - nb);
+                    const uint32_t rank = __popc(vb & lt);
+                    if (valid && rank < take) {
+                        buf[w][nb + rank] = MEnt{pd, pe, pk};
+                        if (APPROX) bufax[w][nb + rank] = ax;
+                    }
+                    __syncwarp();
+                    nb += take;
+                    if (nb < 32) continue;
+                    rest = valid && rank >= take;
+                }
+                flush();
+                if (last) break;
+                // the rest of this chunk, against the new K-th entry
+                rest = rest && (ax ? lb <= __uint_as_float(kd) : mless(pd, pk, kd, kk));
+                const unsigned rb = __ballot_sync(FULL, rest);
+                if (rest) {
+                    buf[w][__popc(rb & lt)] = MEnt{pd, pe, pk};
+                    if (APPROX) bufax[w][__popc(rb & lt)] = ax;
+                }
+                __syncwarp();
+                nb = __popc(rb);
+            }
+            if (lane < (int)K) {
+                a.pid[(size_t)t * K + lane] = ce;
+                a.pdist[(size_t)t * K + lane] = __uint_as_float(cd);
+            }
+            nfl = __popc(__ballot_sync(FULL, lane < (int)K && (ce & FLAG_BIT)));
+        }
+        if (lane == 0) a.nflag[t] = (uint8_t)nfl;
+    }
+}
+
 // The pool (sorted words in lanes < K, FM_EMPTY above) merged with a buffer
 // of up to 32 proposal words (FM_EMPTY padded): the K smallest distinct
 // entries of both.  `stage` is the warp's 64-word shared scratch.
@@ -1010,10 +1145,13 @@ __device__ __forceinline__ unsigned long long fm_flush(unsigned long long pool, 
     return out;
 }
 
-// One warp per target, as k_merge, on the fast tier's 8-byte proposals.
+// One warp per target, as k_merge, on the fast tier's 8-byte proposals;
+// APPROX as there.
+template <bool APPROX>
 __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a) {
     __shared__ unsigned long long buf[MERGE_WARPS][32];
     __shared__ unsigned long long stage[MERGE_WARPS][32];
+    __shared__ uint8_t bufax[APPROX ? MERGE_WARPS : 1][32];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t t = blockIdx.x * MERGE_WARPS + w;
     if (t >= a.n) return;
@@ -1029,12 +1167,20 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a)
         const unsigned long long pprev = __shfl_up_sync(FULL, pool, 1);
         if (!__all_sync(FULL, lane == 0 || pprev <= pool)) pool = fm_sort32(pool);
         unsigned long long kth = __shfl_sync(FULL, pool, K - 1);
-        const uint2* bp = reinterpret_cast<const uint2*>(a.bucket) + a.boff[t];
+        const unsigned long long b_first = a.boff[t];
+        const uint2* bp = reinterpret_cast<const uint2*>(a.bucket) + b_first;
         const unsigned lt = (1u << lane) - 1u;
+        float nt = 0.f;
+        uint32_t bound = 0xffffffffu;
+        if (APPROX) {
+            nt = __uint_as_float(a.nrm[t]);
+            bound = approx_bound<true>(a, b_first, c, K, (uint32_t)(pool >> 32), (uint32_t)(pool >> 2), nt, stage[w]);
+        }
         uint32_t nb = 0;
         for (uint32_t b0 = 0;; b0 += 32) {
             unsigned long long v = FM_EMPTY;
-            bool rest = false;
+            bool rest = false, ax = false;
+            float lb = 0.f;
             const bool last = b0 >= c;
             if (last) {
                 if (nb == 0) break;
@@ -1044,27 +1190,46 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a)
                     const uint2 p = bp[b0 + lane];
                     // a new entry: flag 1, group bit from the list entry
                     v = ((unsigned long long)p.x << 32) | ((p.y & ID_MASK) << 2) | 2u | ((p.y >> 31) ^ 1u);
-                    valid = v < kth;
+                    if (APPROX && (p.y & APPROX_BIT)) {
+                        ax = true;
+                        lb = __uint_as_float(p.x) - a.err_c * (nt + __uint_as_float(a.nrm[p.y & ID_MASK]));
+                        valid = lb <= __uint_as_float(bound) && lb <= __uint_as_float((uint32_t)(kth >> 32));
+                    } else {
+                        valid = v < kth;
+                    }
                 }
                 const unsigned vb = __ballot_sync(FULL, valid);
                 if (!vb) continue;
                 const uint32_t take = min((uint32_t)__popc(vb), 32u - nb);
                 const uint32_t rank = __popc(vb & lt);
-                if (valid && rank < take) buf[w][nb + rank] = v;
+                if (valid && rank < take) {
+                    buf[w][nb + rank] = v;
+                    if (APPROX) bufax[w][nb + rank] = ax;
+                }
                 __syncwarp();
                 nb += take;
                 if (nb < 32) continue;
                 rest = valid && rank >= take;
             }
-            const unsigned long long bv = lane < (int)nb ? buf[w][lane] : FM_EMPTY;
+            unsigned long long bv = FM_EMPTY;
+            if (lane < (int)nb) {
+                bv = buf[w][lane];
+                if (APPROX && bufax[w][lane])  // the exact distance replaces d~
+                    bv = ((unsigned long long)__float_as_uint(merge_exact_l2(a.x, a.dp, t, (uint32_t)(bv >> 2) & ID_MASK))
+                          << 32) | (uint32_t)bv;
+            }
             __syncwarp();
             pool = fm_flush(pool, bv, K, stage[w]);
             kth = __shfl_sync(FULL, pool, K - 1);
             nb = 0;
             if (last) break;
-            rest = rest && v < kth;  // the rest of this chunk, against the new K-th entry
+            // the rest of this chunk, against the new K-th entry
+            rest = rest && (ax ? lb <= __uint_as_float((uint32_t)(kth >> 32)) : v < kth);
             const unsigned rb = __ballot_sync(FULL, rest);
-            if (rest) buf[w][__popc(rb & lt)] = v;
+            if (rest) {
+                buf[w][__popc(rb & lt)] = v;
+                if (APPROX) bufax[w][__popc(rb & lt)] = ax;
+            }
             __syncwarp();
             nb = __popc(rb);
         }
@@ -1275,6 +1440,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     NNM_CUDA_TRY(ws.poff.ensure(n1 * 8));
     NNM_CUDA_TRY(ws.tiers.ensure((size_t)n * NTIER * 4 + 16));
     const bool tc = g.xq != nullptr;
+    // reduced-precision joins (BF16, FP8) emit approximate distances
+    const bool approx = tc && g.tc_kind != 0;
     bool u8_last = false;  // rows of S > 128 on k_pairs_u8 (u8 join, staged vectors fit)
     if (tc) {
         NNM_CUDA_TRY(tc_set_attributes(g.kq, g.tc_kind));
@@ -1443,7 +1610,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     P<float>(ws.pd), P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
                     P<uint64_t>(ws.boff), ws.bucket.p, ctr,
                     g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error, tc ? P<uint32_t>(ws.erows) : nullptr,
-                    g.fast ? 1u : 0u, g.tc_kind, g.err_c};
+                    g.fast ? 1u : 0u, g.tc_kind, g.err_c, g.scl, g.audit ? 1u : 0u};
         if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
         if (tc) NNM_CUDA_TRY(launch_join_tc(0, ja, ntier, nsm, st));
         if (g.metric == L2) launch_pairs<L2>(ja, ntier, caps, g.dp, nsm, tc, u8_last, st);
@@ -1472,10 +1639,16 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             count_launch();
         }
         MergeArgs ma{g.pid, g.pdist, n, K, P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff),
-                     ws.bucket.p, P<uint8_t>(ws.nflag), ctr};
+                     ws.bucket.p, P<uint8_t>(ws.nflag), ctr, g.x, g.dp, g.nrm, g.err_c};
         if (ctx.prof) cudaEventRecord(ctx.ev[3], st);
-        if (g.fast) k_merge_fast<<<(n + MERGE_WARPS - 1) / MERGE_WARPS, MERGE_WARPS * 32, 0, st>>>(ma);
-        else k_merge<<<(n + MERGE_WARPS - 1) / MERGE_WARPS, MERGE_WARPS * 32, 0, st>>>(ma);
+        const unsigned mgrid = (n + MERGE_WARPS - 1) / MERGE_WARPS;
+        if (g.fast) {
+            if (approx) k_merge_fast<true><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
+            else k_merge_fast<false><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
+        } else {
+            if (approx) k_merge<true><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
+            else k_merge<false><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
+        }
         count_launch();
         k_sum_flags<<<std::min<unsigned>((n + 255) / 256, (unsigned)nsm * 4), 256, 0, st>>>(P<uint8_t>(ws.nflag), n, ctr); count_launch();
         if (ctx.prof) cudaEventRecord(ctx.ev[4], st);

@@ -52,11 +52,12 @@ struct Workspace {
 // Device storage of a graph under construction (owned buffers).
 struct GraphStore {
     DevBuf pid, pdist, cpid, cpdist, newL, oldL, newlen, oldlen, rnewT, roldT, rnewTlen, roldTlen, x;
-    DevBuf xq, nrm;  // u8 copy of the vectors and their squared norms (tensor-core join)
+    DevBuf xq, nrm;  // operand copy of the vectors and their squared norms (tensor-core join)
+    DevBuf scl;      // FP8 operands: per-row inverse scales
     DevBuf codes, vkeys, vpos, voff;  // learned codes and their sorted views
     void release() {
         DevBuf* all[] = {&pid, &pdist, &cpid, &cpdist, &newL, &oldL, &newlen, &oldlen,
-                         &rnewT, &roldT, &rnewTlen, &roldTlen, &x, &xq, &nrm,
+                         &rnewT, &roldT, &rnewTlen, &roldTlen, &x, &xq, &nrm, &scl,
                          &codes, &vkeys, &vpos, &voff};
         for (auto* b : all) b->release();
     }
@@ -109,8 +110,9 @@ struct GraphDev {
     const uint8_t* xq = nullptr;
     const uint32_t* nrm = nullptr;
     uint32_t kq = 0;
-    uint32_t tc_kind = 0;  // 0: u8 copy (exact); 1: BF16 copy, float norms, FP32 recheck
-    float err_c = 0.f;     // BF16 distance error bound coefficient
+    uint32_t tc_kind = 0;  // 0: u8 copy (exact); 1: BF16 hi + lo parts; 2: FP8 hi + mid + lo parts
+    float err_c = 0.f;     // reduced precision: |d~ - d| <= err_c (|a|^2 + |b|^2)
+    const float* scl = nullptr;  // FP8: per-row inverse scales 2^-e
     uint32_t join_kernel = 0;       // nnm_join_kernel
     // Learned initialisation: codes of rows [0, n_cap) and, inside a merge,
     // the parent's code views with this graph's leaf index.
@@ -134,6 +136,7 @@ struct GraphDev {
     float delta = 0.002f;
     uint32_t max_iter = 0;     // 0: iterate until the reference's convergence test passes
     bool exact_trace = false;  // record the reference's float mean every iteration
+    bool audit = false;        // reduced-precision joins: check every pair against its bound
     // Fast tier: counter-based random draws (Philox keyed by the seed) in
     // place of the reference's sequential streams, so the initial graphs and
     // samples are drawn on the device and reverse lists need no ordering.

@@ -46,8 +46,10 @@ struct JoinArgs {
     unsigned* tc_err;
     uint32_t* emit_rows;  // 4 lists of n rows: rows of tiers 0-3 that have proposals
     uint32_t fast_key;    // tie-break keys from ids instead of list positions (fast tier)
-    uint32_t tc_kind;     // 0: u8 (exact), 1: BF16 with the FP32 recheck
-    float err_c;          // BF16: |approx - reference distance| <= err_c * (|a|^2 + |b|^2)
+    uint32_t tc_kind;     // 0: u8 (exact), 1: BF16 hi + lo, 2: FP8 hi + mid + lo (join_tc.cu)
+    float err_c;          // reduced precision: |d~ - reference distance| <= err_c * (|a|^2 + |b|^2)
+    const float* scl;     // FP8: per-row inverse scales
+    uint32_t audit;       // reduced precision: check every pair's d~ against its exact distance
 };
 
 // Tie-break key of the exact tier's proposal "target gets the other entry"

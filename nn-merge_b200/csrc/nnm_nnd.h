@@ -35,11 +35,17 @@ struct __align__(8) Prop8 {
     uint32_t idg;
 };
 
+// Bit 30 of a proposal's idg (ids stay below 2^30): its distance is the
+// reduced-precision join's approximation d~, within err_c * (|t|^2 + |u|^2)
+// of the exact FP32 distance; the merge computes the exact value of those
+// proposals that can still reach the top K.
+constexpr uint32_t APPROX_BIT = 1u << 30;
+
 // Key of a fast-tier proposal of list entry `idg`: the entry's id, then its
 // group bit with group 1 first; bit 63 set so that the start pool's entries
 // (keys 0..K-1) precede every proposal of equal distance.
 __host__ __device__ __forceinline__ unsigned long long fast_key(uint32_t idg) {
-    return (1ull << 63) | ((unsigned long long)(idg & 0x7fffffffu) << 1) | ((idg >> 31) ^ 1u);
+    return (1ull << 63) | ((unsigned long long)(idg & 0x3fffffffu) << 1) | ((idg >> 31) ^ 1u);
 }
 
 // Per-iteration statistics read back by the host.
@@ -65,6 +71,8 @@ enum DevError : unsigned int {
     DERR_LIST_CAP = 1,      // a sample list overflowed its row capacity
     DERR_CROSS_SAMPLE = 2,  // a merge found fewer new ids than it needs
     DERR_TC_WAIT = 4,       // a tensor-core join wait ran out (the kernel gave up)
+    DERR_TC_RANGE = 8,      // a reduced-precision emit pass filled a reserved bucket range differently
+    DERR_BOUND = 16,        // audit: a pair's reduced-precision distance lay outside its stated bound
 };
 
 }  // namespace nnm

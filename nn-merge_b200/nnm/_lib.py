@@ -36,7 +36,7 @@ class Opts(ctypes.Structure):
     _fields_ = [("seed", ctypes.c_uint32), ("rng_mode", ctypes.c_uint32), ("metric", ctypes.c_uint32),
                 ("sample_cap", ctypes.c_uint32), ("delta", ctypes.c_float), ("max_iter", ctypes.c_uint32),
                 ("exact_trace", ctypes.c_uint32), ("join_kernel", ctypes.c_uint32),
-                ("init", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 7)]
+                ("init", ctypes.c_uint32), ("audit", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
 
 
 class Mlp(ctypes.Structure):
@@ -186,12 +186,12 @@ def _ptr(a):
 RNG_MODES = {"exact": 0, "fast": 1}
 
 
-JOIN_KERNELS = {"auto": 0, "fp32": 1, "tensor": 2}
+JOIN_KERNELS = {"auto": 0, "fp32": 1, "tensor": 2, "bf16": 2, "fp8": 3}
 INITS = {"random": 0, "learned": 1}
 
 
 def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exact_trace=False, rng="exact",
-              join="auto", init="random"):
+              join="auto", init="random", audit=False):
     lib = load()
     o = Opts()
     lib.nnm_opts_default(ctypes.byref(o))
@@ -204,6 +204,7 @@ def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exac
     o.exact_trace = 1 if exact_trace else 0
     o.join_kernel = JOIN_KERNELS[join]
     o.init = INITS[init]
+    o.audit = 1 if audit else 0
     return o
 
 

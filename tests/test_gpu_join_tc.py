@@ -21,9 +21,9 @@ def same(a, b):
     assert a["iterations"] == b["iterations"]
 
 
-def both(ctx, fn, *args, **kw):
+def both(ctx, fn, *args, tjoin="tensor", **kw):
     ctx.profile(True)
-    t = fn(*args, join="tensor", **kw)
+    t = fn(*args, join=tjoin, **kw)
     rows = ctx.profile_stats()["rows"]
     f = fn(*args, join="fp32", **kw)
     ctx.profile(False)
@@ -144,33 +144,70 @@ def float_mixture(n, d, seed, unit=False):
     return x.astype(np.float32)
 
 
+@pytest.mark.parametrize("kern", ["tensor", "fp8"])
 @pytest.mark.parametrize("unit", [False, True])
 @pytest.mark.parametrize("rng", ["exact", "fast"])
-def test_bf16_tier_matches_fp32(ctx, unit, rng):
+def test_reduced_precision_matches_fp32(ctx, kern, unit, rng):
+    """BF16 (hi + lo) and FP8 (E4M3 hi + mid + lo) Gram matrices: the same
+    graphs as the FP32 join, bit for bit."""
     x = float_mixture(5000, 96, 50 + unit, unit)
-    t, f, rows = both(ctx, ctx.kgraph, x, 16, seed=3, rng=rng)
+    t, f, rows = both(ctx, ctx.kgraph, x, 16, seed=3, rng=rng, tjoin=kern)
     same(t, f)
     assert rows["tensor"] > 0
 
 
-def test_bf16_tier_merges_match_fp32(ctx):
+@pytest.mark.parametrize("kern", ["tensor", "fp8"])
+def test_reduced_precision_merges_match_fp32(ctx, kern):
     x = float_mixture(6000, 64, 61) * 37.0
-    t, f, _ = both(ctx, ctx.merge_leaves, x, 20, [1500] * 4, seed=5)
+    t, f, _ = both(ctx, ctx.merge_leaves, x, 20, [1500] * 4, seed=5, tjoin=kern)
     same(t, f)
-    t, f, _ = both(ctx, ctx.jmerge, x[:4000], 12, seed=6)
+    t, f, _ = both(ctx, ctx.merge_leaves, x, 20, [1500] * 4, seed=5, rng="fast", tjoin=kern)
     same(t, f)
-    t = ctx.hmerge(x[:3000], 10, 8, seed=9, join="tensor")
+    t, f, _ = both(ctx, ctx.jmerge, x[:4000], 12, seed=6, tjoin=kern)
+    same(t, f)
+    t = ctx.hmerge(x[:3000], 10, 8, seed=9, join=kern)
     f = ctx.hmerge(x[:3000], 10, 8, seed=9, join="fp32")
     same(t, f)
 
 
-def test_bf16_tier_ties_and_scales(ctx):
+@pytest.mark.parametrize("kern", ["tensor", "fp8"])
+def test_reduced_precision_ties_and_scales(ctx, kern):
     # many exact ties (few distinct values) and mixed magnitudes
     rng = np.random.default_rng(62)
     x = (rng.integers(-3, 4, size=(4000, 40)) * 0.25).astype(np.float32)
     x[::7] *= 1e3
-    t, f, _ = both(ctx, ctx.kgraph, x, 12, seed=7)
+    t, f, _ = both(ctx, ctx.kgraph, x, 12, seed=7, tjoin=kern)
     same(t, f)
+
+
+def test_fp8_on_integer_data_matches_fp32(ctx):
+    # FP8 when asked for, even where the u8 join would be exact
+    x = gaussian_mixture_u8(5000, seed=71)
+    t, f, rows = both(ctx, ctx.kgraph, x, 20, seed=3, tjoin="fp8")
+    same(t, f)
+    assert rows["tensor"] > 0
+
+
+@pytest.mark.parametrize("kern", ["tensor", "fp8"])
+@pytest.mark.parametrize("data", ["unit", "scaled", "ties", "spread", "sparse"])
+def test_reduced_precision_bound_holds(ctx, kern, data):
+    """Every joined pair's d~ within err_c (|a|^2 + |b|^2) of its exact FP32
+    distance (the audit computes them all and fails the call otherwise)."""
+    rng = np.random.default_rng(80)
+    if data == "unit":
+        x = float_mixture(3000, 96, 81, True)
+    elif data == "scaled":
+        x = float_mixture(3000, 128, 82) * 1e-3
+    elif data == "ties":
+        x = (rng.integers(-3, 4, size=(3000, 40)) * 0.25).astype(np.float32)
+    elif data == "spread":  # components over many binades within a row
+        x = (rng.standard_normal((3000, 64)) * np.exp2(rng.integers(-20, 20, size=(3000, 64)))).astype(np.float32)
+    else:  # mostly zeros, a few large components
+        x = np.zeros((3000, 96), np.float32)
+        m = rng.random((3000, 96)) < 0.05
+        x[m] = rng.standard_normal(int(m.sum())).astype(np.float32) * 100
+    ctx.kgraph(x, 12, seed=4, join=kern, audit=True)
+    ctx.kgraph(x, 12, seed=4, join=kern, audit=True, rng="fast")
 
 
 @pytest.mark.parametrize("bad", ["nan", "inf", "huge", "tiny", "wide"])
@@ -185,7 +222,7 @@ def test_forced_tensor_rejects_uncovered_data(ctx, bad):
     elif bad == "tiny":
         x[9, 0] = 2.0 ** -70
     else:
-        x = float_mixture(2000, 400, 41)  # BF16 tier: d <= 384
+        x = float_mixture(2000, 400, 41)  # BF16 tier: d <= 192
     with pytest.raises(NnmError) as e:
         ctx.kgraph(x, 10, seed=1, join="tensor")
     assert e.value.status == 1
