@@ -96,8 +96,11 @@ def parse():
     p.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 path beside")
     p.add_argument("--no-tune", action="store_true",
                    help="skip the autotuner (sample cap and convergence threshold from --smpl/--delta)")
-    p.add_argument("--workload", default="build", choices=["build", "search"],
-                   help="build: the headline 1M graph build; search: batched LySearch serving on a 1M hierarchy")
+    p.add_argument("--workload", default="build", choices=["build", "search", "vmf"],
+                   help="build: the headline 1M graph build; search: batched LySearch serving on a 1M hierarchy; "
+                        "vmf: 10M x 96 unit vectors, log-uniform leaves merged, FP32 / BF16 / FP8 joins")
+    p.add_argument("--vmf-n", type=int, default=10_000_000)
+    p.add_argument("--vmf-tiers", default="fp32,tensor,fp8")
     p.add_argument("--queries", type=int, default=100_000)
     p.add_argument("--probes", type=int, default=4)
     p.add_argument("--entry-steps", type=int, default=1500)
@@ -525,6 +528,97 @@ def run_search_reference_arm(a, rank):
     print(json.dumps(line), flush=True)
 
 
+VMF_METRIC = "10M×96 k=16 vMF build s, log-uniform leaves merged: FP32 vs BF16 vs FP8 join"
+
+
+def loguniform_leaves(n, lo, hi, seed):
+    """Leaf sizes drawn log-uniformly from [lo, hi] until they cover n rows
+    (the last leaf takes the rest, or joins its predecessor when below lo)."""
+    rng = np.random.default_rng(seed)
+    sizes, tot = [], 0
+    while tot < n:
+        sz = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+        sz = min(sz, n - tot)
+        if sz < lo and sizes:
+            sizes[-1] += sz
+        else:
+            sizes.append(sz)
+        tot += sz
+    return sizes
+
+
+def run_vmf(a, rank, world, local):
+    """10M x 96 unit-norm vectors from the 1024-centre vMF-like mixture
+    (kappa 50), leaves of log-uniform sizes in [5,000, 200,000], k = 16, all
+    leaves built and merged in one multi-way merge (fast draws, random
+    initial graphs), once per join tier: FP32 (the reference's sums), BF16
+    (hi + lo) and FP8 (E4M3 hi + mid + lo).  The reduced-precision tiers
+    give the FP32 tier's graph bit for bit; value = the BF16 tier's seconds."""
+    import torch
+    import nnm
+    from nnm.datasets import vmf_mixture
+    from nnm.replicas import Replicas
+
+    torch.cuda.set_device(local)
+    reps = Replicas("nccl")
+    n, d, k = a.vmf_n, 96, 16
+    t0 = time.perf_counter()
+    x = vmf_mixture(n, d=d, n_centres=1024, kappa=50.0, seed=reps.data_seed(4321))
+    gen_s = time.perf_counter() - t0
+    sizes = loguniform_leaves(n, 5_000, 200_000, 17)
+    x_dev = torch.from_numpy(x).cuda()
+    ids_dev = torch.empty((n, k), dtype=torch.int32, device="cuda")
+    dists_dev = torch.empty((n, k), dtype=torch.float32, device="cuda")
+    ctx = nnm.Context(local)
+    rows = np.sort(np.random.default_rng(7).choice(n, 2000, replace=False))
+    tiers, ref_ids = {}, None
+    for tier in a.vmf_tiers.split(","):
+        kw = dict(seed=a.seed, rng="fast", join=tier, init="random")
+        ctx.merge_leaves_dev(x_dev.data_ptr(), n, d, k, sizes, ids_dev.data_ptr(), dists_dev.data_ptr(), 0, **kw)
+        ctx.profile(True)
+        times = []
+        for _ in range(max(1, a.steps)):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            st = ctx.merge_leaves_dev(x_dev.data_ptr(), n, d, k, sizes, ids_dev.data_ptr(), dists_dev.data_ptr(), 0,
+                                      **kw)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+        prof = ctx.profile_stats()
+        ctx.profile(False)
+        ids = ids_dev.cpu().numpy().view(np.uint32)
+        rec, rec_ids = recall_at(ids[rows], x_dev, rows, 10, torch, both=True)
+        ids_s = ids[rows].astype(np.int64)
+        ds_s = dists_dev[torch.as_tensor(rows, device="cuda")].cpu().numpy().astype(np.float64)
+        ref_s = ((x[rows][:, None, :].astype(np.float64) - x[ids_s].astype(np.float64)) ** 2).sum(-1)
+        rel = np.abs(ds_s - ref_s) / np.maximum(ref_s, 1e-30)
+        same = None
+        if ref_ids is None:
+            ref_ids = ids.copy()
+        else:
+            same = bool(np.array_equal(ids, ref_ids))
+        tiers[tier] = {"s": statistics.median(times), "times": times, "iterations": st["iterations"],
+                       "recall@10": rec, "recall@10_ids": rec_ids,
+                       "dist_err_vs_fp64": {"max_rel": float(rel.max()), "mean_rel": float(rel.mean())},
+                       "same_graph_as_first_tier": same,
+                       "join_ms": prof["join"]["ms"], "emit_ms": prof["emit"]["ms"], "merge_ms": prof["merge"]["ms"],
+                       "proposals": int(sum(L[3] for L in prof["iters"]))}
+    ms = reps.max(tiers.get("tensor", next(iter(tiers.values())))["s"] * 1e3)
+    if rank == 0:
+        line = {"metric": VMF_METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": a.steps,
+                "warmup": 1, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "bf16", "data": "synthetic: seeded 1024-centre vMF-like mixture (kappa 50), unit norm",
+                "config": {"workload": "%dx%d k=%d, %d log-uniform leaves (%d..%d rows) built and merged, fast draws, "
+                                       "random init" % (n, d, k, len(sizes), min(sizes), max(sizes)),
+                           "n": n, "d": d, "k": k, "leaves": len(sizes), "gen_s": gen_s, "tiers": tiers},
+                "cpu_baseline": None, "e2e": None}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    reps.close()
+
+
 def run_cfg1(ctx, torch, seed):
     """100,000 x 128 from the 64-centre mixture, S-Merge of the halves, k=20
     (Smerge::buildKGraph, smerge.cpp:46-91): the reference's own process on
@@ -564,6 +658,9 @@ def main():
         return
     if a.workload == "search":
         run_search(a, rank, world, local)
+        return
+    if a.workload == "vmf":
+        run_vmf(a, rank, world, local)
         return
 
     import torch

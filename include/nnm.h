@@ -79,6 +79,16 @@ typedef enum {
     NNM_INIT_LEARNED = 1 /* candidates bucketed by the learned codes */
 } nnm_init_mode;
 
+/* How nnm_merge_leaves merges its built leaves (no counterpart in the
+   reference, which merges two sub-graphs).  ALL: one multi-way merge, every
+   row taking cross samples from all other leaves.  TREE (needs
+   NNM_RNG_FAST): bottom-up pairwise S-Merges, leaf 2i with leaf 2i + 1, level
+   after level, all pairs of a level batched into one NN-Descent run. */
+typedef enum {
+    NNM_MERGE_ALL = 0,
+    NNM_MERGE_TREE = 1
+} nnm_merge_order;
+
 typedef struct {
     uint32_t seed;        /* clock value the reference's time(NULL) seeding is frozen at */
     uint32_t rng_mode;    /* nnm_rng_mode */
@@ -92,7 +102,8 @@ typedef struct {
     uint32_t audit;       /* nonzero: the reduced-precision joins also compute every pair's exact
                              distance and fail the call (NNM_ERR_CAPACITY) if one lies outside
                              the stated bound -- a test of the bound, slow */
-    uint32_t reserved[6];
+    uint32_t merge_order; /* nnm_merge_order (nnm_merge_leaves) */
+    uint32_t reserved[5];
 } nnm_opts;
 
 typedef struct {

@@ -204,6 +204,8 @@ struct FastArgs {
     uint32_t gd_split;
     uint32_t seed, phase;
     IterCounters* ctr;
+    uint32_t partner;          // with leaf_off: draw from the partner leaf (leaf ^ 1) only; a row
+                               // whose leaf has no partner keeps its pool
 };
 
 __global__ void k_fast_rows(FastArgs a) {
@@ -212,13 +214,21 @@ __global__ void k_fast_rows(FastArgs a) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t row = a.row0 + blockIdx.x * WPB + w;
     if (row >= a.row1) return;
-    const uint32_t K = a.K, need = K - a.keep;
+    const uint32_t K = a.K;
+    uint32_t need = K - a.keep;
     uint32_t lo = a.base, span = 0, range = a.range;
     if (a.leaf_off) {
         uint32_t g = leaf_index(row, a.leaf_off, a.nleaf);
-        lo = a.leaf_off[g];
-        span = a.leaf_off[g + 1] - lo;
-        range = a.leaf_off[a.nleaf] - span;
+        if (a.partner) {  // ids lo + [0, range) of the partner leaf
+            const uint32_t p = g ^ 1u;
+            if (p >= a.nleaf) return;  // unpaired at this level: the pool stays
+            lo = a.leaf_off[p];
+            range = a.leaf_off[p + 1] - lo;
+        } else {
+            lo = a.leaf_off[g];
+            span = a.leaf_off[g + 1] - lo;
+            range = a.leaf_off[a.nleaf] - span;
+        }
     }
     if (lane < (int)K && a.keep) ents[w][lane] = SortEnt{a.pdist[(size_t)row * K + lane], a.pid[(size_t)row * K + lane]};
     __syncwarp();
@@ -230,7 +240,7 @@ __global__ void k_fast_rows(FastArgs a) {
     uint32_t taken = 0;
     for (uint32_t round = 0; taken < need && round < 64; round++) {
         const uint32_t s = bounded(ph(row, a.phase, round, (uint32_t)lane).x, range);
-        const uint32_t id = a.leaf_off ? (s < lo ? s : s + span) : s + a.base;
+        const uint32_t id = (a.leaf_off && !a.partner) ? (s < lo ? s : s + span) : s + (a.leaf_off ? lo : a.base);
         bool ok = id != row;
         for (uint32_t l = 0; l < K && ok; l++)
             if (a.keep && (ents[w][l].id & ID_MASK) == id) ok = false;
@@ -455,11 +465,12 @@ int export_graph(Ctx& ctx, const GraphDev& g, uint32_t* ids, float* dists, uint8
 
 // KGraph on rows [0, g.n) of g (x, pid, pdist already offset by the caller).
 static int fast_rows(Ctx& ctx, GraphDev& g, uint32_t row0, uint32_t row1, uint32_t keep, uint32_t range,
-                     uint32_t base, const uint32_t* leaf_off, uint32_t nleaf, uint32_t gd_new, uint32_t gd_split) {
+                     uint32_t base, const uint32_t* leaf_off, uint32_t nleaf, uint32_t gd_new, uint32_t gd_split,
+                     uint32_t partner = 0) {
     int rc;
     if ((rc = reset_counters(ctx))) return rc;
     FastArgs fa{g.x, g.dp, g.K, g.metric, g.pid, g.pdist, g.cpid, g.cpdist, row0, row1, keep, range, base,
-                leaf_off, nleaf, gd_new, gd_split, g.seed, g.phase++, ctx.ws.counters.as<IterCounters>()};
+                leaf_off, nleaf, gd_new, gd_split, g.seed, g.phase++, ctx.ws.counters.as<IterCounters>(), partner};
     k_fast_rows<<<blocks_for(row1 - row0, WPB), WPB * 32, 0, ctx.stream>>>(fa); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return check_counters(ctx);
@@ -596,6 +607,39 @@ static int jmerge_initial_exact(Ctx& ctx, GraphDev& g, uint32_t pre) {
     return 0;
 }
 
+// Bottom-up pairwise merge of built leaves (fast tier): at each level leaf
+// 2i is S-Merged with leaf 2i + 1 (an odd last leaf waits for the next
+// level), and all pairs of a level share one NN-Descent run -- every row's
+// cross samples come from its partner leaf only, so no list mixes pairs --
+// then merge2one; the merged pairs are the next level's leaves.  On entry
+// the leaves hold their graphs (global ids).
+static int merge_tree_levels(Ctx& ctx, GraphDev& g, std::vector<uint32_t> off) {
+    const uint32_t K = g.K;
+    int rc;
+    g.cut = K * 1 / 2;
+    DevBuf& lo = ctx.ws.misc;
+    NNM_CUDA_TRY(lo.ensure(off.size() * 4 + 64));
+    while (off.size() > 2) {
+        const uint32_t nl = (uint32_t)off.size() - 1;
+        const uint32_t pend = (nl & 1u) ? off[nl - 1] : off[nl];  // rows of paired leaves
+        NNM_CUDA_TRY(cudaMemcpyAsync(lo.p, off.data(), off.size() * 4, cudaMemcpyHostToDevice, ctx.stream));
+        // InitSGraph of both sub-graphs of every pair: all entries new
+        k_rebase<<<blocks_for((size_t)pend * K, 256), 256, 0, ctx.stream>>>(g.pid, (size_t)pend * K, 0u, 0u); count_launch();
+        if ((rc = fast_rows(ctx, g, 0, pend, K - g.cut, 0, 0, lo.as<uint32_t>(), nl, 0, 0, 1))) return rc;
+        g.ncmps += (uint64_t)pend * g.cut;
+        if ((rc = run_nndescent(ctx, g, MODE_SMERGE, off[1], 0, lo.as<uint32_t>(), nl))) return rc;
+        k_merge2one<<<blocks_for(pend, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut,
+                                                                       pend, 1u); count_launch();
+        NNM_CUDA_TRY(cudaGetLastError());
+        std::vector<uint32_t> nxt;
+        for (size_t i = 0; i < off.size(); i += 2) nxt.push_back(off[i]);
+        if (nxt.back() != off.back()) nxt.push_back(off.back());
+        off.swap(nxt);
+        NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));  // `off` on the host changes before the next copy
+    }
+    return 0;
+}
+
 int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, uint64_t* sub_ncmps) {
     const uint32_t K = g.K, n = g.n, nleaf = (uint32_t)leaf_off.size() - 1;
     int rc;
@@ -644,6 +688,7 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
         k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(s.pid, cnt, leaf_off[l], nleaf == 2 ? l : 0u); count_launch();
     }
     if (sub_ncmps) *sub_ncmps = subc;
+    if (g.fast && g.merge_tree) return merge_tree_levels(ctx, g, leaf_off);
     // 2. cross sampling (smerge.cpp:94-209)
     g.cut = K * 1 / 2;
     if (g.fast) {

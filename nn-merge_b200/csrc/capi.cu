@@ -64,6 +64,14 @@ bool opts_ok(nnm_ctx* ctx, const nnm_opts* o, int* rc) {
         *rc = fail(ctx, NNM_ERR_INVALID, "unknown init");
         return false;
     }
+    if (o->merge_order > NNM_MERGE_TREE) {
+        *rc = fail(ctx, NNM_ERR_INVALID, "unknown merge_order");
+        return false;
+    }
+    if (o->merge_order == NNM_MERGE_TREE && o->rng_mode != NNM_RNG_FAST) {
+        *rc = fail(ctx, NNM_ERR_INVALID, "NNM_MERGE_TREE needs rng_mode NNM_RNG_FAST");
+        return false;
+    }
     if (o->init == NNM_INIT_LEARNED && o->rng_mode != NNM_RNG_FAST) {
         *rc = fail(ctx, NNM_ERR_INVALID, "NNM_INIT_LEARNED needs rng_mode NNM_RNG_FAST");
         return false;
@@ -86,6 +94,7 @@ void setup_graph(GraphDev& g, const nnm_opts& o, uint64_t n, uint32_t d, uint32_
     g.fast = o.rng_mode == NNM_RNG_FAST;
     g.join_kernel = o.join_kernel;
     g.audit = o.audit != 0;
+    g.merge_tree = o.merge_order == NNM_MERGE_TREE;
     g.init = o.init;
     g.phase = 0;
 }

@@ -137,6 +137,7 @@ struct GraphDev {
     uint32_t max_iter = 0;     // 0: iterate until the reference's convergence test passes
     bool exact_trace = false;  // record the reference's float mean every iteration
     bool audit = false;        // reduced-precision joins: check every pair against its bound
+    bool merge_tree = false;   // multi-leaf merges: bottom-up pairwise levels instead of all at once
     // Fast tier: counter-based random draws (Philox keyed by the seed) in
     // place of the reference's sequential streams, so the initial graphs and
     // samples are drawn on the device and reverse lists need no ordering.

@@ -36,7 +36,8 @@ class Opts(ctypes.Structure):
     _fields_ = [("seed", ctypes.c_uint32), ("rng_mode", ctypes.c_uint32), ("metric", ctypes.c_uint32),
                 ("sample_cap", ctypes.c_uint32), ("delta", ctypes.c_float), ("max_iter", ctypes.c_uint32),
                 ("exact_trace", ctypes.c_uint32), ("join_kernel", ctypes.c_uint32),
-                ("init", ctypes.c_uint32), ("audit", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
+                ("init", ctypes.c_uint32), ("audit", ctypes.c_uint32), ("merge_order", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 5)]
 
 
 class Mlp(ctypes.Structure):
@@ -191,7 +192,7 @@ INITS = {"random": 0, "learned": 1}
 
 
 def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exact_trace=False, rng="exact",
-              join="auto", init="random", audit=False):
+              join="auto", init="random", audit=False, merge_order="all"):
     lib = load()
     o = Opts()
     lib.nnm_opts_default(ctypes.byref(o))
@@ -205,6 +206,7 @@ def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exac
     o.join_kernel = JOIN_KERNELS[join]
     o.init = INITS[init]
     o.audit = 1 if audit else 0
+    o.merge_order = {"all": 0, "tree": 1}[merge_order]
     return o
 
 

@@ -71,3 +71,28 @@ def test_hmerge_fast_is_deterministic(ctx, join):
             if not (np.array_equal(ao, bo) and np.array_equal(aa, ba))]
     assert np.array_equal(a["ids"], b["ids"]) and np.array_equal(a["dists"], b["dists"]), "pools differ"
     assert not diff, "layers differ: %s" % diff
+
+
+@pytest.mark.parametrize("join", ["auto", "tensor"])
+def test_merge_tree_of_uneven_leaves(ctx, join):
+    """Bottom-up pairwise merge (NNM_MERGE_TREE) of leaves of uneven sizes and
+    an odd count: deterministic, well formed, recall as the multi-way merge."""
+    x = gaussian_mixture_u8(14000, d=64, n_centres=48, seed=21)
+    sizes = [1200, 3300, 2500, 900, 4000, 2100]  # 6 leaves -> 3 -> 2 (one waits) -> 1
+    sizes[-1] += len(x) - sum(sizes)
+    a = ctx.merge_leaves(x, 16, sizes, seed=3, rng="fast", join=join, merge_order="tree")
+    b = ctx.merge_leaves(x, 16, sizes, seed=3, rng="fast", join=join, merge_order="tree")
+    assert np.array_equal(a["ids"], b["ids"]) and a["ncmps"] == b["ncmps"]
+    check_pools(x, a)
+    m = ctx.merge_leaves(x, 16, sizes, seed=3, rng="fast", join=join)
+    assert recall(x, a) >= recall(x, m) - 0.02 and recall(x, a) >= 0.93
+    odd = ctx.merge_leaves(x, 16, sizes[:4] + [sizes[4] + sizes[5]], seed=3, rng="fast", merge_order="tree")
+    check_pools(x, odd)
+    assert recall(x, odd) >= 0.93
+
+
+def test_merge_tree_needs_fast_draws(ctx):
+    from nnm import NnmError
+    x = gaussian_mixture_u8(3000, d=16, seed=22)
+    with pytest.raises(NnmError):
+        ctx.merge_leaves(x, 10, [1000, 1000, 1000], seed=1, merge_order="tree")
