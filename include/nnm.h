@@ -102,7 +102,7 @@ typedef struct {
     uint32_t audit;       /* nonzero: the reduced-precision joins also compute every pair's exact
                              distance and fail the call (NNM_ERR_CAPACITY) if one lies outside
                              the stated bound -- a test of the bound, slow */
-    uint32_t merge_order; /* nnm_merge_order (nnm_merge_leaves) */
+    uint32_t merge_order; /* an nnm_merge_order, read by nnm_merge_leaves */
     uint32_t reserved[5];
 } nnm_opts;
 
