@@ -108,6 +108,9 @@ def parse():
     return p.parse_args()
 
 
+BF16_FALLBACK = 1590.0  # TFLOP/s
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -115,6 +118,31 @@ def peaks():
         return float(m["hbm_gbs"]), "measured"
     except Exception:
         return HBM_FALLBACK, "fallback"
+
+
+def tensor_peak():
+    """Dense BF16 tensor TFLOP/s as measured (burst), else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return BF16_FALLBACK, "fallback"
+
+
+# DRAM bytes per launch measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) on a 200,000-row build, as a ratio to the library's
+# algorithmic bytes of the same launch; the full-size launch's traffic is
+# estimated by that ratio times its algorithmic bytes (traffic grows with the
+# rows and proposals a launch processes).  Keyed by (kernel class, tensor
+# join); empty until a capture of the current kernels gives the ratio.
+NCU_TRAFFIC_RATIO = {}
+
+
+def traffic_per_launch(kind, stat, a):
+    r = NCU_TRAFFIC_RATIO.get((kind, a.join != "fp32"))
+    if r is None or not stat["launches"]:
+        return None
+    return r * stat["bytes"] / stat["launches"]
 
 
 def leaf_sizes(n, leaves):
@@ -805,9 +833,17 @@ def main():
         per_ms = j["ms"] / j["launches"]
         per_bytes = j["bytes"] / j["launches"]
         achieved = per_bytes / (per_ms * 1e-3) / 1e9
+        # tensor pipe: the 8-bit MMAs run at twice the BF16 rate, so their
+        # peak is twice the measured BF16 figure
+        tpk, tpk_kind = tensor_peak()
+        t_ops = j.get("tensor_ops", 0.0) / j["launches"]
+        tpeak = tpk * (2.0 if a.join != "fp32" else 1.0)
         roof = {"bound": "hbm", "kernel": names[dom],
                 "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "peak_kind": peak_kind, "traffic": None,
+                "peak_kind": peak_kind, "traffic": traffic_per_launch(dom, j, a),
+                "tensor_tflops": t_ops / (per_ms * 1e-3) / 1e12,
+                "tensor_frac": (t_ops / (per_ms * 1e-3) / 1e12) / tpeak,
+                "tensor_peak": tpeak, "tensor_peak_kind": tpk_kind + " (bf16, x2 for 8-bit operands)",
                 "join_share_of_step": prof["join"]["ms"] / (ms * a.steps),
                 "emit_share_of_step": prof["emit"]["ms"] / (ms * a.steps),
                 "merge_share_of_step": prof["merge"]["ms"] / (ms * a.steps)}

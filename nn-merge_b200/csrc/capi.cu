@@ -514,11 +514,11 @@ int nnm_profile_get(const nnm_ctx* ctx, char* buf, uint64_t buflen) {
     std::string js;
     char tmp[512];
     std::snprintf(tmp, sizeof tmp,
-                  "{\"join\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f, \"flops\": %.1f}, "
-                  "\"emit\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}, "
+                  "{\"join\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f, \"flops\": %.1f, \"tensor_ops\": %.1f}, "
+                  "\"emit\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f, \"tensor_ops\": %.1f}, "
                   "\"merge\": {\"launches\": %llu, \"ms\": %.6f, \"bytes\": %.1f}, ",
-                  (unsigned long long)c.kjoin.launches, c.kjoin.ms, c.kjoin.bytes, c.kjoin.flops,
-                  (unsigned long long)c.kemit.launches, c.kemit.ms, c.kemit.bytes,
+                  (unsigned long long)c.kjoin.launches, c.kjoin.ms, c.kjoin.bytes, c.kjoin.flops, c.kjoin.tensor_ops,
+                  (unsigned long long)c.kemit.launches, c.kemit.ms, c.kemit.bytes, c.kemit.tensor_ops,
                   (unsigned long long)c.kmerge.launches, c.kmerge.ms, c.kmerge.bytes);
     js += tmp;
     std::snprintf(tmp, sizeof tmp, "\"rows\": {\"tiers\": [%llu, %llu, %llu, %llu, %llu], \"tensor\": %llu}, \"iters\": [",

@@ -1692,6 +1692,20 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             ctx.kemit.ms += t23;
             ctx.kemit.bytes += (double)hc.pairs * 4.0 + s_f32 * 18.0 + s_tc * ((double)g.kq + 22.0) +
                                (double)hc.proposals * (double)prop_bytes;
+            if (tc) {
+                // every MMA chain fills a 128 x 128 tile over the padded row:
+                // kq K elements (u8), 3 products of kq/4 (BF16 hi + lo), 6 of
+                // kq/3 (FP8 hi + mid + lo)
+                const double kel = g.tc_kind == 0 ? (double)g.kq : g.tc_kind == 1 ? 3.0 * g.kq / 4.0 : 6.0 * g.kq / 3.0;
+                const double per_tile = 2.0 * 128.0 * 128.0 * kel;
+                double t0n = 0, t1n = 0;
+                for (int t = 0; t < 4; t++) {
+                    t0n += (double)((hc.ntier[t] + (8u >> t) - 1) >> (3 - t));
+                    t1n += (double)(((approx ? hc.ntier[t] : hc.nemit[t]) + (8u >> t) - 1) >> (3 - t));
+                }
+                ctx.kjoin.tensor_ops += t0n * per_tile;
+                ctx.kemit.tensor_ops += t1n * per_tile;
+            }
             ctx.kmerge.launches += 1;
             ctx.kmerge.ms += t34;
             ctx.kmerge.bytes += (double)n * K * 16.0 + (double)hc.proposals * (double)prop_bytes + (double)n * 13.0;

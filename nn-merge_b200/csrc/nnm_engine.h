@@ -68,6 +68,7 @@ struct GraphStore {
 struct KStat {
     uint64_t launches = 0;
     double ms = 0.0, bytes = 0.0, flops = 0.0;
+    double tensor_ops = 0.0;  // multiply-adds x 2 issued to the tensor cores (whole 128 x 128 tiles)
 };
 
 struct DevMlp;
