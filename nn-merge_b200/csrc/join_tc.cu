@@ -182,6 +182,7 @@ template <int PASS, int KIND, bool FAST>
 __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ TcShared sh;
+    if (a.ctr->overflow) return;  // a buffer sized ahead was too small: the host reruns
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t kq = a.kq, nchunk = kq >> 4, gbytes = nchunk * 128;
     const uint32_t mma_bar = smem_u32(&sh.mma_bar);
@@ -801,10 +802,14 @@ cudaError_t tc_set_attributes(uint32_t kq, uint32_t kind) {
 }
 
 cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, int nsm, cudaStream_t st) {
-    unsigned tiles = 0;
-    for (int t = 0; t < 4; t++) tiles += (ntier[t] + (8u >> t) - 1) >> (3 - t);
-    if (!tiles) return cudaSuccess;
-    const unsigned grid = std::min<unsigned>(tiles, (unsigned)nsm * 4);
+    // ntier null: the counts are on the device only -- every SM's four CTAs
+    unsigned grid = (unsigned)nsm * 4;
+    if (ntier) {
+        unsigned tiles = 0;
+        for (int t = 0; t < 4; t++) tiles += (ntier[t] + (8u >> t) - 1) >> (3 - t);
+        if (!tiles) return cudaSuccess;
+        grid = std::min<unsigned>(tiles, grid);
+    }
     const size_t bytes = std::max<size_t>(tc_smem_bytes(ja.kq), TC_SMEM_FLOOR);
     const bool fast = ja.fast_key != 0;
     if (ja.tc_kind == KIND_U8) {

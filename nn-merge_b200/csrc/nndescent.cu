@@ -595,6 +595,7 @@ __device__ void pairs_row(const JoinArgs& a, uint32_t row, unsigned char* smem, 
 template <int M, int TIER>
 __global__ void __launch_bounds__(TIER_THREADS[TIER]) k_pairs(JoinArgs a, uint32_t R) {
     extern __shared__ __align__(16) unsigned char smem[];
+    if (a.ctr->overflow) return;
     const uint32_t cnt = a.ctr->ntier[TIER];
     const uint32_t* rows = a.tier_rows + (size_t)TIER * a.n;
     for (uint32_t b = blockIdx.x; b < cnt; b += gridDim.x)
@@ -605,6 +606,7 @@ __global__ void __launch_bounds__(TIER_THREADS[TIER]) k_pairs(JoinArgs a, uint32
 // vectors staged in shared memory, integer dot products (dp4a).
 __global__ void __launch_bounds__(TIER_THREADS[NTIER - 1]) k_pairs_u8(JoinArgs a, uint32_t R) {
     extern __shared__ __align__(16) unsigned char smem[];
+    if (a.ctr->overflow) return;
     const uint32_t cnt = a.ctr->ntier[NTIER - 1];
     const uint32_t* rows = a.tier_rows + (size_t)(NTIER - 1) * a.n;
     for (uint32_t b = blockIdx.x; b < cnt; b += gridDim.x) pairs_row<L2, VEC_U8>(a, rows[b], smem, R);
@@ -686,6 +688,7 @@ __device__ __forceinline__ void emit_pairs(const JoinArgs& a, uint32_t row, uint
 // FP32 join: a warp per row.
 __global__ void __launch_bounds__(EMIT_WARPS * 32) k_emit(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
+    if (a.ctr->overflow) return;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t row = blockIdx.x * EMIT_WARPS + w;
     if (row >= a.n) return;
@@ -706,14 +709,20 @@ constexpr int EMIT_ROW_WARPS = 8;
 
 __global__ void __launch_bounds__(EMIT_ROW_WARPS * 32) k_emit_rows(JoinArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    if (blockIdx.x >= a.ctr->ntier[NTIER - 1]) return;
-    const uint32_t row = a.tier_rows[(size_t)(NTIER - 1) * a.n + blockIdx.x];
-    const uint32_t nn = a.newlen[row], no = a.oldlen[row];
-    if (nn == 0) return;
-    const EmitRow m = emit_row_smem(smem, a.caps);
-    if (!__syncthreads_or(emit_load_row(a, row, nn, nn + no, m, threadIdx.x, blockDim.x))) return;
-    if (a.fast_key) emit_pairs<true>(a, row, nn, no, m, threadIdx.x >> 5, EMIT_ROW_WARPS);
-    else emit_pairs<false>(a, row, nn, no, m, threadIdx.x >> 5, EMIT_ROW_WARPS);
+    if (a.ctr->overflow) return;
+    const uint32_t cnt = a.ctr->ntier[NTIER - 1];
+    for (uint32_t b = blockIdx.x; b < cnt; b += gridDim.x) {  // a block per row
+        const uint32_t row = a.tier_rows[(size_t)(NTIER - 1) * a.n + b];
+        const uint32_t nn = a.newlen[row], no = a.oldlen[row];
+        if (nn == 0) continue;
+        const EmitRow m = emit_row_smem(smem, a.caps);
+        const bool any = __syncthreads_or(emit_load_row(a, row, nn, nn + no, m, threadIdx.x, blockDim.x));
+        if (any) {
+            if (a.fast_key) emit_pairs<true>(a, row, nn, no, m, threadIdx.x >> 5, EMIT_ROW_WARPS);
+            else emit_pairs<false>(a, row, nn, no, m, threadIdx.x >> 5, EMIT_ROW_WARPS);
+        }
+        __syncthreads();  // the row's members in shared memory are read before the next row's load
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1004,6 +1013,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
     __shared__ MEnt kept[MERGE_WARPS][32];
     __shared__ MEnt buf[MERGE_WARPS][32];
     __shared__ uint8_t bufax[APPROX ? MERGE_WARPS : 1][32];
+    if (a.ctr->overflow) return;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t t = blockIdx.x * MERGE_WARPS + w;
     uint32_t nfl = 0;
@@ -1152,6 +1162,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a)
     __shared__ unsigned long long buf[MERGE_WARPS][32];
     __shared__ unsigned long long stage[MERGE_WARPS][32];
     __shared__ uint8_t bufax[APPROX ? MERGE_WARPS : 1][32];
+    if (a.ctr->overflow) return;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t t = blockIdx.x * MERGE_WARPS + w;
     if (t >= a.n) return;
@@ -1246,6 +1257,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a)
 // they do not meet at a block barrier to add them up).
 __global__ void k_sum_flags(const uint8_t* nflag, uint32_t n, IterCounters* ctr) {
     __shared__ unsigned int part[8];
+    if (ctr->overflow) return;
     unsigned int s = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += nflag[i];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
@@ -1259,6 +1271,12 @@ __global__ void k_sum_flags(const uint8_t* nflag, uint32_t n, IterCounters* ctr)
 }
 
 // ---------------------------------------------------------------------------
+// Sets `bit` of the overflow word when *total exceeds cap.
+__global__ void k_check_cap(IterCounters* ctr, const unsigned long long* total, unsigned long long cap,
+                            unsigned int bit) {
+    if (threadIdx.x == 0 && *total > cap) atomicOr(&ctr->overflow, bit);
+}
+
 __global__ void k_clear_lists(uint32_t* newlen, uint32_t* oldlen, uint32_t* tn, uint32_t* to, uint32_t n) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
@@ -1365,14 +1383,16 @@ static cudaError_t prep_pairs(uint32_t caps, uint32_t dp, size_t emit_smem, int 
 template <int M>
 static void launch_pairs(const JoinArgs& ja, const unsigned* ntier, uint32_t caps, uint32_t dp, int nsm,
                          bool last_only, bool u8_last, cudaStream_t st) {
-    if (!last_only) {
+    if (!last_only && ntier) {
         if (ntier[0]) { k_pairs<M, 0><<<ntier[0], TIER_THREADS[0], pairs_smem(TIER_CAP[0], dp, true), st>>>(ja, TIER_CAP[0]); count_launch(); }
         if (ntier[1]) { k_pairs<M, 1><<<ntier[1], TIER_THREADS[1], pairs_smem(TIER_CAP[1], dp, true), st>>>(ja, TIER_CAP[1]); count_launch(); }
         if (ntier[2]) { k_pairs<M, 2><<<ntier[2], TIER_THREADS[2], pairs_smem(TIER_CAP[2], dp, true), st>>>(ja, TIER_CAP[2]); count_launch(); }
         if (ntier[3]) { k_pairs<M, 3><<<ntier[3], TIER_THREADS[3], pairs_smem(TIER_CAP[3], dp, true), st>>>(ja, TIER_CAP[3]); count_launch(); }
     }
-    if (ntier[4]) {
-        unsigned g = std::min<unsigned>(ntier[4], (unsigned)nsm * 4);
+    // ntier null (the tensor-core join takes tiers 0-3): the count of the
+    // last tier is on the device only, the blocks loop over its rows
+    if (!ntier || ntier[4]) {
+        unsigned g = ntier ? std::min<unsigned>(ntier[4], (unsigned)nsm * 4) : (unsigned)nsm * 4;
         if (u8_last) {
             k_pairs_u8<<<g, TIER_THREADS[4], pairs_smem_u8(caps, ja.kq), st>>>(ja, caps);
         } else {
@@ -1477,6 +1497,40 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             if (graph) cudaGraphDestroy(graph);
         }
     } seg;
+    // The whole-iteration graph of the fast tier on the tensor cores.
+    struct WholeGraph {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraphNode_t shuf = nullptr;
+        cudaKernelNodeParams kp{};
+        uint64_t launches = 0;
+        bool disabled = false;
+        void reset() {
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+            exec = nullptr;
+            graph = nullptr;
+            shuf = nullptr;
+        }
+        ~WholeGraph() { reset(); }
+    } whole_g;
+    // the node of kernel `fn` in a captured graph, and its parameters
+    auto find_kernel_node = [](cudaGraph_t graph, void* fn, cudaKernelNodeParams& out) -> cudaGraphNode_t {
+        size_t nn = 0;
+        cudaGraphGetNodes(graph, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        cudaGraphGetNodes(graph, nodes.data(), &nn);
+        for (cudaGraphNode_t nd : nodes) {
+            cudaGraphNodeType ty;
+            cudaKernelNodeParams kp{};
+            if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel &&
+                cudaGraphKernelNodeGetParams(nd, &kp) == cudaSuccess && kp.func == fn) {
+                out = kp;
+                return nd;
+            }
+        }
+        return nullptr;
+    };
     for (uint32_t it = 0;; it++) {
         const bool carry_now = (it == 0) && g.carry && track;
         const uint32_t phase = g.phase++;
@@ -1489,8 +1543,10 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                             P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, phase,
                             tc ? TC_MAX_S : 0u, max_staged, rscr_new, rscr_old, (g.fast && carry_now) ? 1u : 0u};
         };
-        // the segment; its first failing call's error is returned
-        auto seg_a = [&]() -> cudaError_t {
+        // the segment; its first failing call's error is returned.  copy:
+        // read the counters back at its end (the whole-iteration graph reads
+        // them once, after the merge)
+        auto seg_a = [&](bool copy = true) -> cudaError_t {
             cudaError_t e = cudaSuccess;
             auto chk = [&](cudaError_t x) {
                 if (e == cudaSuccess) e = x;
@@ -1539,122 +1595,230 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                                reinterpret_cast<uint64_t*>(&ctr->pairs), st));
             chk(cudaMemsetAsync(ws.bcnt.p, 0, n1 * 4, st));
             chk(cudaMemsetAsync(ws.bcur.p, 0, n1 * 4, st));
-            chk(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
+            if (copy) chk(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
             chk(cudaGetLastError());
             return e;
         };
-        const bool graphable = g.fast && !carry_now && !seg.disabled;
-        if (graphable && seg.exec) {
-            ShufArgs sh = shuf_args();
-            void* kargs[] = {&sh};
-            cudaKernelNodeParams kp = seg.kp;
-            kp.kernelParams = kargs;
-            kp.extra = nullptr;
-            cudaError_t e = cudaGraphExecKernelNodeSetParams(seg.exec, seg.shuf, &kp);
-            if (e == cudaSuccess) e = cudaGraphLaunch(seg.exec, st);
-            NNM_CUDA_TRY(e);
-            count_launch(seg.launches);
-        } else if (graphable) {
-            const uint64_t c0 = launch_counter().load();
-            cudaGraph_t& graph = seg.graph;
-            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-            if (e == cudaSuccess) {
-                const cudaError_t e1 = seg_a();
-                const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
-                e = e1 != cudaSuccess ? e1 : e2;
-            }
-            if (e == cudaSuccess) e = cudaGraphInstantiate(&seg.exec, graph, 0);
-            if (e == cudaSuccess) {
-                size_t nn = 0;
-                cudaGraphGetNodes(graph, nullptr, &nn);
-                std::vector<cudaGraphNode_t> nodes(nn);
-                cudaGraphGetNodes(graph, nodes.data(), &nn);
-                for (cudaGraphNode_t nd : nodes) {
-                    cudaGraphNodeType ty;
-                    cudaKernelNodeParams kp{};
-                    if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel &&
-                        cudaGraphKernelNodeGetParams(nd, &kp) == cudaSuccess &&
-                        kp.func == reinterpret_cast<void*>(k_shuffle_append)) {
-                        seg.shuf = nd;
-                        seg.kp = kp;
-                    }
-                }
-            }
-            seg.launches = launch_counter().load() - c0;
-            if (e == cudaSuccess && seg.shuf) e = cudaGraphLaunch(seg.exec, st);  // capture counted its kernels
-            if (e != cudaSuccess || !seg.shuf) {
-                // no graph: this call launches the segment directly
-                cudaGetLastError();
-                if (seg.exec) cudaGraphExecDestroy(seg.exec);
-                if (seg.graph) cudaGraphDestroy(seg.graph);
-                seg.exec = nullptr;
-                seg.graph = nullptr;
-                seg.disabled = true;
-                NNM_CUDA_TRY(seg_a());
-            }
-        } else {
-            NNM_CUDA_TRY(seg_a());
-        }
-        NNM_CUDA_TRY(cudaStreamSynchronize(st));
-        if (ctx.h_counters->error) {
-            ctx.last_error = "device capacity check failed (code " + std::to_string(ctx.h_counters->error) + ")";
-            return 6;
-        }
-        unsigned ntier[NTIER];
-        for (int t = 0; t < NTIER; t++) ntier[t] = ctx.h_counters->ntier[t];
-        NNM_CUDA_TRY(ws.pd.ensure(std::max<uint64_t>(ctx.h_counters->pairs, 1) * 4));
+        // Event records inside a capture become graph nodes (external events)
+        // so that the profile reads the replayed kernels' times.
+        auto rec = [&](int i) {
+            if (!ctx.prof) return;
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            cudaStreamIsCapturing(st, &cs);
+            if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(ctx.ev[i], st, cudaEventRecordExternal);
+            else cudaEventRecord(ctx.ev[i], st);
+        };
+        auto make_ja = [&]() {
+            return JoinArgs{g.x, g.dp, K, n, g.pdist, g.newL, g.oldL, g.newlen, g.oldlen, g.capn, g.capo, caps,
+                            (uint32_t)mode, verse, d_leaf_off, nleaf, P<uint32_t>(ws.tiers), P<uint64_t>(ws.poff),
+                            P<float>(ws.pd), P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
+                            P<uint64_t>(ws.boff), ws.bucket.p, ctr,
+                            g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error, tc ? P<uint32_t>(ws.erows) : nullptr,
+                            g.fast ? 1u : 0u, g.tc_kind, g.err_c, g.scl, g.audit ? 1u : 0u};
+        };
         // local join, pass 1: per-target proposal counts (and, on the FP32
-        // path, the stored pair distances)
-        JoinArgs ja{g.x, g.dp, K, n, g.pdist, g.newL, g.oldL, g.newlen, g.oldlen, g.capn, g.capo, caps,
-                    (uint32_t)mode, verse, d_leaf_off, nleaf, P<uint32_t>(ws.tiers), P<uint64_t>(ws.poff),
-                    P<float>(ws.pd), P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
-                    P<uint64_t>(ws.boff), ws.bucket.p, ctr,
-                    g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error, tc ? P<uint32_t>(ws.erows) : nullptr,
-                    g.fast ? 1u : 0u, g.tc_kind, g.err_c, g.scl, g.audit ? 1u : 0u};
-        if (ctx.prof) cudaEventRecord(ctx.ev[0], st);
-        if (tc) NNM_CUDA_TRY(launch_join_tc(0, ja, ntier, nsm, st));
-        if (g.metric == L2) launch_pairs<L2>(ja, ntier, caps, g.dp, nsm, tc, u8_last, st);
-        else if (g.metric == L1) launch_pairs<L1>(ja, ntier, caps, g.dp, nsm, tc, false, st);
-        else launch_pairs<CHI2>(ja, ntier, caps, g.dp, nsm, tc, false, st);
-        if (ctx.prof) cudaEventRecord(ctx.ev[1], st);
-        NNM_CUDA_TRY(exclusive_scan(P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff), n, scan_tmp,
-                                    reinterpret_cast<uint64_t*>(&ctr->proposals), st));
-        NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
-        NNM_CUDA_TRY(cudaStreamSynchronize(st));
-        const uint64_t nprop = ctx.h_counters->proposals;
-        if (nprop * prop_bytes > ws.bucket.bytes) {
-            NNM_CUDA_TRY(ws.bucket.ensure((size_t)(nprop * 1.25 + 1024) * prop_bytes));
-            ja.bucket = ws.bucket.p;
-        }
+        // path, the stored pair distances), then the bucket offsets.  nt:
+        // rows per tier read by the host, or null (grids of every SM; the
+        // kernels read the counts on the device).
+        auto part0 = [&](const JoinArgs& ja, const unsigned* nt) -> cudaError_t {
+            cudaError_t e = cudaSuccess;
+            rec(0);
+            if (tc) e = launch_join_tc(0, ja, nt, nsm, st);
+            if (e == cudaSuccess) {
+                if (g.metric == L2) launch_pairs<L2>(ja, nt, caps, g.dp, nsm, tc, u8_last, st);
+                else if (g.metric == L1) launch_pairs<L1>(ja, nt, caps, g.dp, nsm, tc, false, st);
+                else launch_pairs<CHI2>(ja, nt, caps, g.dp, nsm, tc, false, st);
+                rec(1);
+                e = exclusive_scan(P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff), n, scan_tmp,
+                                   reinterpret_cast<uint64_t*>(&ctr->proposals), st);
+            }
+            return e != cudaSuccess ? e : cudaGetLastError();
+        };
         // pass 2: proposals, recomputed on the tensor cores or read from the
-        // stored distances
-        if (ctx.prof) cudaEventRecord(ctx.ev[2], st);
-        if (tc) NNM_CUDA_TRY(launch_join_tc(1, ja, ntier, nsm, st));
-        if (tc ? ntier[NTIER - 1] > 0 : n > 0) {
+        // stored distances; the top-K merge and the flag total
+        auto part1 = [&](const JoinArgs& ja, const unsigned* nt) -> cudaError_t {
+            cudaError_t e = cudaSuccess;
+            rec(2);
+            if (tc) e = launch_join_tc(1, ja, nt, nsm, st);
+            if (e != cudaSuccess) return e;
             if (tc) {
-                k_emit_rows<<<ntier[NTIER - 1], EMIT_ROW_WARPS * 32, (size_t)caps * 24 + 64, st>>>(ja);
+                const unsigned rows4 = nt ? nt[NTIER - 1] : (unsigned)nsm * 2;
+                if (rows4) {
+                    k_emit_rows<<<rows4, EMIT_ROW_WARPS * 32, (size_t)caps * 24 + 64, st>>>(ja); count_launch();
+                }
+            } else if (n > 0) {
+                k_emit<<<(n + EMIT_WARPS - 1) / EMIT_WARPS, EMIT_WARPS * 32, emit_smem, st>>>(ja); count_launch();
+            }
+            MergeArgs ma{g.pid, g.pdist, n, K, P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff),
+                         ja.bucket, P<uint8_t>(ws.nflag), ctr, g.x, g.dp, g.nrm, g.err_c};
+            rec(3);
+            const unsigned mgrid = (n + MERGE_WARPS - 1) / MERGE_WARPS;
+            if (g.fast) {
+                if (approx) k_merge_fast<true><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
+                else k_merge_fast<false><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
             } else {
-                k_emit<<<(n + EMIT_WARPS - 1) / EMIT_WARPS, EMIT_WARPS * 32, emit_smem, st>>>(ja);
+                if (approx) k_merge<true><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
+                else k_merge<false><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
             }
             count_launch();
+            k_sum_flags<<<std::min<unsigned>((n + 255) / 256, (unsigned)nsm * 4), 256, 0, st>>>(P<uint8_t>(ws.nflag), n, ctr); count_launch();
+            rec(4);
+            return cudaGetLastError();
+        };
+        auto copy_back = [&]() -> cudaError_t {
+            cudaError_t e = cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(&ctx.h_counters->rand_draws, d_tot, 8, cudaMemcpyDeviceToHost, st);
+            return e;
+        };
+        // Fast tier on the tensor cores, after the first iteration of the
+        // call has sized the pair and bucket buffers: the whole iteration --
+        // sampling, both join passes, merge, counters -- is one CUDA graph,
+        // replayed with the draw phase set on its shuffle node, and the host
+        // reads the counters once.  The buffers are sized from earlier
+        // iterations (with headroom) and checked on the device; on overflow
+        // the join and merge kernels do nothing, and the host grows the
+        // buffer and reruns the skipped part directly.
+        const bool whole = g.fast && tc && !carry_now && !whole_g.disabled && it > 0;
+        bool done = false;
+        if (whole) {
+            if (!whole_g.exec) {
+                const uint64_t c0 = launch_counter().load();
+                cudaGraph_t graph = nullptr;
+                cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+                if (e == cudaSuccess) {
+                    const JoinArgs ja = make_ja();
+                    cudaError_t e1 = seg_a(false);
+                    if (e1 == cudaSuccess) {
+                        k_check_cap<<<1, 32, 0, st>>>(ctr, reinterpret_cast<const unsigned long long*>(&ctr->pairs),
+                                                      (unsigned long long)(ws.pd.bytes / 4), OVF_PAIRS); count_launch();
+                        e1 = part0(ja, nullptr);
+                    }
+                    if (e1 == cudaSuccess) {
+                        k_check_cap<<<1, 32, 0, st>>>(ctr, reinterpret_cast<const unsigned long long*>(&ctr->proposals),
+                                                      (unsigned long long)(ws.bucket.bytes / prop_bytes),
+                                                      OVF_PROPOSALS); count_launch();
+                        e1 = part1(ja, nullptr);
+                    }
+                    if (e1 == cudaSuccess) e1 = copy_back();
+                    const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+                    e = e1 != cudaSuccess ? e1 : e2;
+                }
+                if (e == cudaSuccess) e = cudaGraphInstantiate(&whole_g.exec, graph, 0);
+                if (e == cudaSuccess) whole_g.shuf = find_kernel_node(graph, reinterpret_cast<void*>(k_shuffle_append),
+                                                                      whole_g.kp);
+                whole_g.graph = graph;
+                whole_g.launches = launch_counter().load() - c0;
+                if (e != cudaSuccess || !whole_g.shuf) {  // no graph: this call launches directly
+                    cudaGetLastError();
+                    whole_g.reset();
+                    whole_g.disabled = true;
+                }
+            } else {
+                count_launch(whole_g.launches);
+            }
+            if (whole_g.exec) {
+                ShufArgs sh = shuf_args();
+                void* kargs[] = {&sh};
+                cudaKernelNodeParams kp = whole_g.kp;
+                kp.kernelParams = kargs;
+                kp.extra = nullptr;
+                cudaError_t e = cudaGraphExecKernelNodeSetParams(whole_g.exec, whole_g.shuf, &kp);
+                if (e == cudaSuccess) e = cudaGraphLaunch(whole_g.exec, st);
+                NNM_CUDA_TRY(e);
+                NNM_CUDA_TRY(cudaStreamSynchronize(st));
+                IterCounters& h = *ctx.h_counters;
+                if (h.error) {
+                    ctx.last_error = "device capacity check failed (code " + std::to_string(h.error) + ")";
+                    return 6;
+                }
+                if (h.overflow) {
+                    // grow what was short (the graph names the old buffers:
+                    // it is captured again next iteration) and rerun what the
+                    // kernels skipped
+                    whole_g.reset();
+                    unsigned nt[NTIER];
+                    for (int t = 0; t < NTIER; t++) nt[t] = h.ntier[t];
+                    const unsigned ovf = h.overflow;
+                    NNM_CUDA_TRY(cudaMemsetAsync(&ctr->overflow, 0, 4, st));
+                    if (ovf & OVF_PAIRS) {
+                        NNM_CUDA_TRY(ws.pd.ensure((size_t)(std::max<uint64_t>(h.pairs, 1) * 1.5 + 1024) * 4));
+                        NNM_CUDA_TRY(part0(make_ja(), nt));
+                        NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
+                        NNM_CUDA_TRY(cudaStreamSynchronize(st));
+                    }
+                    const uint64_t nprop = ctx.h_counters->proposals;
+                    if (nprop * prop_bytes > ws.bucket.bytes)
+                        NNM_CUDA_TRY(ws.bucket.ensure((size_t)(nprop * 1.5 + 1024) * prop_bytes));
+                    NNM_CUDA_TRY(part1(make_ja(), nt));
+                    NNM_CUDA_TRY(copy_back());
+                    NNM_CUDA_TRY(cudaStreamSynchronize(st));
+                }
+                done = true;
+            }
         }
-        MergeArgs ma{g.pid, g.pdist, n, K, P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff),
-                     ws.bucket.p, P<uint8_t>(ws.nflag), ctr, g.x, g.dp, g.nrm, g.err_c};
-        if (ctx.prof) cudaEventRecord(ctx.ev[3], st);
-        const unsigned mgrid = (n + MERGE_WARPS - 1) / MERGE_WARPS;
-        if (g.fast) {
-            if (approx) k_merge_fast<true><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
-            else k_merge_fast<false><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
-        } else {
-            if (approx) k_merge<true><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
-            else k_merge<false><<<mgrid, MERGE_WARPS * 32, 0, st>>>(ma);
+        if (!done) {
+            const bool graphable = g.fast && !carry_now && !seg.disabled && !tc;
+            if (graphable && seg.exec) {
+                ShufArgs sh = shuf_args();
+                void* kargs[] = {&sh};
+                cudaKernelNodeParams kp = seg.kp;
+                kp.kernelParams = kargs;
+                kp.extra = nullptr;
+                cudaError_t e = cudaGraphExecKernelNodeSetParams(seg.exec, seg.shuf, &kp);
+                if (e == cudaSuccess) e = cudaGraphLaunch(seg.exec, st);
+                NNM_CUDA_TRY(e);
+                count_launch(seg.launches);
+            } else if (graphable) {
+                const uint64_t c0 = launch_counter().load();
+                cudaGraph_t& graph = seg.graph;
+                cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+                if (e == cudaSuccess) {
+                    const cudaError_t e1 = seg_a();
+                    const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+                    e = e1 != cudaSuccess ? e1 : e2;
+                }
+                if (e == cudaSuccess) e = cudaGraphInstantiate(&seg.exec, graph, 0);
+                if (e == cudaSuccess) seg.shuf = find_kernel_node(graph, reinterpret_cast<void*>(k_shuffle_append), seg.kp);
+                seg.launches = launch_counter().load() - c0;
+                if (e == cudaSuccess && seg.shuf) e = cudaGraphLaunch(seg.exec, st);  // capture counted its kernels
+                if (e != cudaSuccess || !seg.shuf) {
+                    // no graph: this call launches the segment directly
+                    cudaGetLastError();
+                    if (seg.exec) cudaGraphExecDestroy(seg.exec);
+                    if (seg.graph) cudaGraphDestroy(seg.graph);
+                    seg.exec = nullptr;
+                    seg.graph = nullptr;
+                    seg.disabled = true;
+                    NNM_CUDA_TRY(seg_a());
+                }
+            } else {
+                NNM_CUDA_TRY(seg_a());
+            }
+            NNM_CUDA_TRY(cudaStreamSynchronize(st));
+            if (ctx.h_counters->error) {
+                ctx.last_error = "device capacity check failed (code " + std::to_string(ctx.h_counters->error) + ")";
+                return 6;
+            }
+            unsigned ntier[NTIER];
+            for (int t = 0; t < NTIER; t++) ntier[t] = ctx.h_counters->ntier[t];
+            // headroom for the iterations the whole-iteration graph runs
+            const double room = (g.fast && tc) ? 1.5 : 1.0;
+            const size_t pd_need = (size_t)(std::max<uint64_t>(ctx.h_counters->pairs, 1) * room) * 4;
+            if (pd_need > ws.pd.bytes) NNM_CUDA_TRY(ws.pd.ensure(pd_need + 4096));
+            JoinArgs ja = make_ja();
+            NNM_CUDA_TRY(part0(ja, ntier));
+            NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
+            NNM_CUDA_TRY(cudaStreamSynchronize(st));
+            const uint64_t nprop = ctx.h_counters->proposals;
+            if (nprop * prop_bytes > ws.bucket.bytes) {
+                NNM_CUDA_TRY(ws.bucket.ensure((size_t)(nprop * (g.fast && tc ? 1.5 : 1.25) + 1024) * prop_bytes));
+                ja.bucket = ws.bucket.p;
+            }
+            NNM_CUDA_TRY(part1(ja, ntier));
+            NNM_CUDA_TRY(copy_back());
+            NNM_CUDA_TRY(cudaStreamSynchronize(st));
         }
-        count_launch();
-        k_sum_flags<<<std::min<unsigned>((n + 255) / 256, (unsigned)nsm * 4), 256, 0, st>>>(P<uint8_t>(ws.nflag), n, ctr); count_launch();
-        if (ctx.prof) cudaEventRecord(ctx.ev[4], st);
-        NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, st));
-        NNM_CUDA_TRY(cudaMemcpyAsync(&ctx.h_counters->rand_draws, d_tot, 8, cudaMemcpyDeviceToHost, st));
-        NNM_CUDA_TRY(cudaStreamSynchronize(st));
         NNM_CUDA_TRY(cudaGetLastError());
         const IterCounters hc = *ctx.h_counters;
         if (hc.error) {

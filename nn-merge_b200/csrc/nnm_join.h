@@ -122,6 +122,8 @@ struct GraphDev;
 int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g);
 cudaError_t tc_set_attributes(uint32_t kq, uint32_t kind);
 // pass 0: per-slot proposal counts; pass 1: proposals into the buckets.
+// ntier: rows per tier as the host read them, or null (grid of every SM's
+// CTAs, the kernel reads the counts on the device).
 cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, int nsm, cudaStream_t st);
 
 }  // namespace nnm

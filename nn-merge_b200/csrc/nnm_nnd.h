@@ -56,7 +56,8 @@ struct IterCounters {
     unsigned long long rand_draws; // std::rand() calls of the shuffles
     unsigned int error;            // nonzero: a capacity or input check failed
     unsigned int nbig_rev;         // reverse lists longer than one warp
-    unsigned int unused;
+    unsigned int overflow;         // a buffer sized ahead of the counts was too small (OVF_*): the
+                                   // join and merge kernels did nothing, the host grows it and reruns
     unsigned int pad;
     unsigned long long sum_s;      // sum over joined rows of |new| + |old|
     unsigned long long pairs;      // pair-distance slots of this iteration
@@ -65,6 +66,11 @@ struct IterCounters {
     unsigned long long sum_s_tc;   // the part of sum_s joined on the tensor cores
     unsigned int nemit[4];         // rows of tiers 0-3 with at least one proposal (tensor-core emit pass)
 };
+
+// IterCounters::overflow bits (the whole-iteration graph sizes its buffers
+// from earlier iterations and checks them on the device).
+constexpr unsigned int OVF_PAIRS = 1;      // stored pair distances beyond the pair buffer
+constexpr unsigned int OVF_PROPOSALS = 2;  // proposals beyond the bucket array
 
 enum DevError : unsigned int {
     DERR_NONE = 0,
