@@ -791,6 +791,18 @@ def main():
     launches = ctx.launch_count() - l0
     prof = ctx.profile_stats()
     ctx.profile(False)
+    # the same build with every kernel launched directly (no iteration graphs)
+    direct = None
+    if a.path == "fast":
+        build_dev(**dict(bkw, graph=False))
+        torch.cuda.synchronize()
+        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        d0.record(stream)
+        for _ in range(3):
+            build_dev(**dict(bkw, graph=False))
+        d1.record(stream)
+        torch.cuda.synchronize()
+        direct = {"s": d0.elapsed_time(d1) / 3 / 1e3, "steps": 3}
     # builds run on the library's stream and synchronize before returning, so
     # the events on torch's stream bracket them
     ms = ev0.elapsed_time(ev1) / a.steps
@@ -896,6 +908,7 @@ def main():
                        "l2": "inputs (%d MB) larger than L2 (126 MB)" % (x.nbytes >> 20),
                        "parallelism": "replicas" if world > 1 else "single"},
             "plain_fp32": plain,
+            "direct_launches": direct,
             "speedup_vs_plain_fp32": (plain["s"] / (ms / 1e3)) if plain else None,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks.summary(), "cfg1": cfg1, "search": search,

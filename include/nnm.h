@@ -103,7 +103,9 @@ typedef struct {
                              distance and fail the call (NNM_ERR_CAPACITY) if one lies outside
                              the stated bound -- a test of the bound, slow */
     uint32_t merge_order; /* an nnm_merge_order, read by nnm_merge_leaves */
-    uint32_t reserved[5];
+    uint32_t no_graph;    /* nonzero: launch every kernel directly; zero: the fast tier replays
+                             each NN-Descent iteration as a CUDA graph where it can */
+    uint32_t reserved[4];
 } nnm_opts;
 
 typedef struct {

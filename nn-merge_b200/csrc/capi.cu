@@ -95,6 +95,7 @@ void setup_graph(GraphDev& g, const nnm_opts& o, uint64_t n, uint32_t d, uint32_
     g.join_kernel = o.join_kernel;
     g.audit = o.audit != 0;
     g.merge_tree = o.merge_order == NNM_MERGE_TREE;
+    g.no_graph = o.no_graph != 0;
     g.init = o.init;
     g.phase = 0;
 }

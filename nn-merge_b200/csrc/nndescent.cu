@@ -1679,7 +1679,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         // iterations (with headroom) and checked on the device; on overflow
         // the join and merge kernels do nothing, and the host grows the
         // buffer and reruns the skipped part directly.
-        const bool whole = g.fast && tc && !carry_now && !whole_g.disabled && it > 0;
+        const bool whole = g.fast && tc && !carry_now && !whole_g.disabled && !g.no_graph && it > 0;
         bool done = false;
         if (whole) {
             if (!whole_g.exec) {
@@ -1758,7 +1758,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             }
         }
         if (!done) {
-            const bool graphable = g.fast && !carry_now && !seg.disabled && !tc;
+            const bool graphable = g.fast && !carry_now && !seg.disabled && !tc && !g.no_graph;
             if (graphable && seg.exec) {
                 ShufArgs sh = shuf_args();
                 void* kargs[] = {&sh};

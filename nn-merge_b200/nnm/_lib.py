@@ -37,7 +37,7 @@ class Opts(ctypes.Structure):
                 ("sample_cap", ctypes.c_uint32), ("delta", ctypes.c_float), ("max_iter", ctypes.c_uint32),
                 ("exact_trace", ctypes.c_uint32), ("join_kernel", ctypes.c_uint32),
                 ("init", ctypes.c_uint32), ("audit", ctypes.c_uint32), ("merge_order", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 5)]
+                ("no_graph", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 4)]
 
 
 class Mlp(ctypes.Structure):
@@ -192,7 +192,7 @@ INITS = {"random": 0, "learned": 1}
 
 
 def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exact_trace=False, rng="exact",
-              join="auto", init="random", audit=False, merge_order="all"):
+              join="auto", init="random", audit=False, merge_order="all", graph=True):
     lib = load()
     o = Opts()
     lib.nnm_opts_default(ctypes.byref(o))
@@ -207,6 +207,7 @@ def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exac
     o.init = INITS[init]
     o.audit = 1 if audit else 0
     o.merge_order = {"all": 0, "tree": 1}[merge_order]
+    o.no_graph = 0 if graph else 1
     return o
 
 

@@ -96,3 +96,21 @@ def test_merge_tree_needs_fast_draws(ctx):
     x = gaussian_mixture_u8(3000, d=16, seed=22)
     with pytest.raises(NnmError):
         ctx.merge_leaves(x, 10, [1000, 1000, 1000], seed=1, merge_order="tree")
+
+
+@pytest.mark.parametrize("join", ["tensor", "fp8"])
+def test_iteration_graph_matches_direct_launches(ctx, join):
+    """The whole-iteration CUDA graph (one counter read per iteration,
+    buffers sized ahead and checked on the device) gives the graph of direct
+    launches, bit for bit, with learned and random initial graphs."""
+    x = gaussian_mixture_u8(20000, d=64, n_centres=40, seed=5)
+    if join == "fp8":
+        x = x / 17.0 + 0.25
+    for kw in (dict(init="random"), dict(init="random", merge_order="tree")):
+        a = ctx.merge_leaves(x, 16, [5000] * 4, seed=2, rng="fast", join=join, **kw)
+        b = ctx.merge_leaves(x, 16, [5000] * 4, seed=2, rng="fast", join=join, graph=False, **kw)
+        assert np.array_equal(a["ids"], b["ids"]) and np.array_equal(a["dists"], b["dists"])
+        assert a["iterations"] == b["iterations"] and a["ncmps"] == b["ncmps"]
+    k = ctx.kgraph(x[:6000], 20, seed=4, rng="fast", join=join)
+    kd = ctx.kgraph(x[:6000], 20, seed=4, rng="fast", join=join, graph=False)
+    assert np.array_equal(k["ids"], kd["ids"]) and k["iterations"] == kd["iterations"]
