@@ -159,6 +159,25 @@ int nnm_jmerge(nnm_ctx *ctx, const float *x, uint64_t n, uint32_t d, uint32_t k,
                const nnm_opts *opts, uint32_t *ids, float *dists, uint8_t *flags,
                nnm_stats *stats);
 
+/* The two halves of nnm_merge_leaves_dev on the fast tier (rng_mode
+ * NNM_RNG_FAST), for a build whose leaves are split over several GPUs (no
+ * counterpart in the reference).  nnm_build_leaves_dev: NN-Descent on
+ * nleaf consecutive leaves of x (sizes summing to n) as nnm_merge_leaves
+ * builds them, without the merge; leaf0 is the index of the first of these
+ * leaves among all leaves of the whole build (it fixes their random draws);
+ * ids are local to x's rows.  nnm_merge_prebuilt_dev: the merge of
+ * nnm_merge_leaves over leaves whose graphs are given (n x k ids of x's rows,
+ * distances; ids outside [0, n) are rejected).  Building all leaves in one
+ * call and merging them gives nnm_merge_leaves_dev's graph bit for bit.
+ * All pointers are device pointers. */
+int nnm_build_leaves_dev(nnm_ctx *ctx, const float *x_dev, uint64_t n, uint32_t d, uint32_t k,
+                         const uint32_t *leaf_sizes, uint32_t nleaf, uint32_t leaf0, const nnm_opts *opts,
+                         uint32_t *ids_dev, float *dists_dev, nnm_stats *stats);
+int nnm_merge_prebuilt_dev(nnm_ctx *ctx, const float *x_dev, uint64_t n, uint32_t d, uint32_t k,
+                           const uint32_t *leaf_sizes, uint32_t nleaf, const nnm_opts *opts,
+                           const uint32_t *ids_in_dev, const float *dists_in_dev, uint32_t *ids_dev,
+                           float *dists_dev, uint8_t *flags_dev, nnm_stats *stats);
+
 /* Staged merge: the steps of Smerge::buildKGraph (smerge.cpp:46-91) and
  * Jmerge::buildKGraph (jmerge.cpp:43-80) as separate calls on one session,
  * for callers that drive AbstractMerge's interface (abstractmerge.h:25-37)

@@ -640,47 +640,125 @@ static int merge_tree_levels(Ctx& ctx, GraphDev& g, std::vector<uint32_t> off) {
     return 0;
 }
 
-int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, uint64_t* sub_ncmps) {
+// Fast tier, step 1 of a multi-leaf build: NN-Descent on every leaf, in
+// place (smerge.cpp:56-68), all leaves in one run: each leaf's initial graph
+// holds only rows of that leaf and reverse lists come from the pools, so no
+// list ever mixes leaves -- one launch sequence for leaves of any sizes.
+// leaf0: the index of the first leaf among all leaves of the build (the
+// leaves' initial draws).  Pools end with ids of g's rows.
+static int fast_leaf_builds(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, uint32_t leaf0,
+                            const CodeViews* vw, uint64_t* subc) {
+    const uint32_t K = g.K, nleaf = (uint32_t)leaf_off.size() - 1;
+    int rc;
+    for (uint32_t l = 0; l < nleaf; l++) {
+        GraphDev s = sub_view(g, leaf_off[l], leaf_off[l + 1]);
+        if (vw) {
+            s.views = vw;
+            s.view_leaf = l;
+        }
+        s.phase = g.phase + leaf0 + l;  // independent draws per leaf
+        if ((rc = fast_init(ctx, s))) return rc;
+        *subc += s.ncmps;
+        const size_t cnt = (size_t)s.n * K;
+        k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(s.pid, cnt, leaf_off[l], 0u); count_launch();
+    }
+    g.phase = LEAF_PHASE0;  // the leaf run's draws do not depend on how the leaves were split
+    const uint64_t before = g.ncmps;
+    if ((rc = run_nndescent(ctx, g, MODE_KGRAPH, 0, 0, nullptr, 0))) return rc;
+    *subc += g.ncmps - before;
+    g.ncmps = before;
+    return 0;
+}
+
+// Fast tier, steps 2-4 of a multi-leaf build on leaves whose graphs are in
+// g's pools (ids of g's rows): InitSGraph (all entries new, group ids),
+// cross sampling from the other leaves (learned or random), NN-Descent with
+// the cross-leaf join, merge2one -- or the bottom-up tree.  The merge's
+// draws start at a fixed phase, so they do not depend on the leaf runs.
+static int fast_merge_phase(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, const CodeViews* vw) {
     const uint32_t K = g.K, n = g.n, nleaf = (uint32_t)leaf_off.size() - 1;
+    int rc;
+    g.phase = MERGE_PHASE0;
+    for (uint32_t l = 0; l < nleaf; l++) {
+        const size_t cnt = (size_t)(leaf_off[l + 1] - leaf_off[l]) * K;
+        k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid + (size_t)leaf_off[l] * K, cnt, 0u,
+                                                              nleaf == 2 ? l : 0u); count_launch();
+    }
+    if (g.merge_tree) return merge_tree_levels(ctx, g, leaf_off);
+    g.cut = K * 1 / 2;
+    DevBuf& lo = ctx.ws.misc;
+    NNM_CUDA_TRY(lo.ensure(leaf_off.size() * 4 + 64));
+    NNM_CUDA_TRY(cudaMemcpyAsync(lo.p, leaf_off.data(), leaf_off.size() * 4, cudaMemcpyHostToDevice, ctx.stream));
+    rc = vw ? learned_cross(ctx, g, *vw, lo.as<uint32_t>())
+            : fast_rows(ctx, g, 0, n, K - g.cut, 0, 0, lo.as<uint32_t>(), nleaf, 0, 0);
+    if (rc) return rc;
+    g.ncmps += (uint64_t)n * g.cut;
+    if ((rc = run_nndescent(ctx, g, MODE_SMERGE, leaf_off[1], 0, lo.as<uint32_t>(), nleaf))) return rc;
+    k_merge2one<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, n, 1u); count_launch();
+    NNM_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int build_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, uint32_t leaf0, uint64_t* ncmps) {
+    CodeViews vw;
+    const bool learned = g.init == NNM_INIT_LEARNED;
+    int rc;
+    if (learned && (rc = views_build(ctx, g, leaf_off, vw))) return rc;
+    uint64_t c = 0;
+    if ((rc = fast_leaf_builds(ctx, g, leaf_off, leaf0, learned ? &vw : nullptr, &c))) return rc;
+    if (ncmps) *ncmps = c;
+    return 0;
+}
+
+// Pools from a caller's device arrays (n x K ids of g's rows, distances);
+// ids outside [0, n) fail with DERR_CROSS_SAMPLE's status.
+__global__ void k_check_ids(const uint32_t* ids, size_t count, uint32_t n, IterCounters* ctr) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count && ids[t] >= n) atomicOr(&ctr->error, (unsigned)DERR_LIST_CAP);
+}
+
+int load_pools(Ctx& ctx, GraphDev& g, const uint32_t* ids_dev, const float* dists_dev) {
+    const size_t cnt = (size_t)g.n * g.K;
+    int rc;
+    if ((rc = reset_counters(ctx))) return rc;
+    k_check_ids<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(ids_dev, cnt, g.n, ctx.ws.counters.as<IterCounters>()); count_launch();
+    NNM_CUDA_TRY(cudaGetLastError());
+    IterCounters* ctr = ctx.ws.counters.as<IterCounters>();
+    NNM_CUDA_TRY(cudaMemcpyAsync(ctx.h_counters, ctr, sizeof(IterCounters), cudaMemcpyDeviceToHost, ctx.stream));
+    NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+    if (ctx.h_counters->error) {
+        ctx.last_error = "leaf graph ids must lie in [0, n)";
+        return 1;
+    }
+    NNM_CUDA_TRY(cudaMemcpyAsync(g.pid, ids_dev, cnt * 4, cudaMemcpyDeviceToDevice, ctx.stream));
+    NNM_CUDA_TRY(cudaMemcpyAsync(g.pdist, dists_dev, cnt * 4, cudaMemcpyDeviceToDevice, ctx.stream));
+    return 0;
+}
+
+int merge_prebuilt(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off) {
+    CodeViews vw;
+    const bool learned = g.init == NNM_INIT_LEARNED;
+    int rc;
+    if (learned && (rc = views_build(ctx, g, leaf_off, vw))) return rc;
+    return fast_merge_phase(ctx, g, leaf_off, learned ? &vw : nullptr);
+}
+
+int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, uint64_t* sub_ncmps) {
+    const uint32_t K = g.K;
     int rc;
     uint64_t subc = 0;
     CodeViews vw;
     const bool learned = g.fast && g.init == NNM_INIT_LEARNED;
     if (learned && (rc = views_build(ctx, g, leaf_off, vw))) return rc;
-    // 1. NN-Descent on every leaf, in place (smerge.cpp:56-68).  The fast
-    // tier runs all leaves in one NN-Descent: each leaf's initial graph holds
-    // only rows of that leaf, reverse lists come from the pools, so no list
-    // ever mixes leaves -- one launch sequence for leaves of any sizes.
     if (g.fast) {
-        for (uint32_t l = 0; l < nleaf; l++) {
-            GraphDev s = sub_view(g, leaf_off[l], leaf_off[l + 1]);
-            if (learned) {
-                s.views = &vw;
-                s.view_leaf = l;
-            }
-            s.phase = g.phase + l;  // independent draws per leaf
-            if ((rc = fast_init(ctx, s))) return rc;
-            subc += s.ncmps;
-            const size_t cnt = (size_t)s.n * K;
-            k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(s.pid, cnt, leaf_off[l], 0u); count_launch();
-        }
-        g.phase += nleaf;
-        const uint64_t before = g.ncmps;
-        if ((rc = run_nndescent(ctx, g, MODE_KGRAPH, 0, 0, nullptr, 0))) return rc;
-        subc += g.ncmps - before;
-        g.ncmps = before;
-        for (uint32_t l = 0; l < nleaf; l++) {  // InitSGraph: all entries new, group ids
-            const size_t cnt = (size_t)(leaf_off[l + 1] - leaf_off[l]) * K;
-            k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(g.pid + (size_t)leaf_off[l] * K, cnt, 0u,
-                                                                  nleaf == 2 ? l : 0u); count_launch();
-        }
+        if ((rc = fast_leaf_builds(ctx, g, leaf_off, 0, learned ? &vw : nullptr, &subc))) return rc;
+        if (sub_ncmps) *sub_ncmps = subc;
+        return fast_merge_phase(ctx, g, leaf_off, learned ? &vw : nullptr);
     }
-    for (uint32_t l = 0; l < nleaf && !g.fast; l++) {
+    // reference streams: one KGraph per leaf, the std::rand() stream running on
+    const uint32_t n = g.n, nleaf = (uint32_t)leaf_off.size() - 1;
+    for (uint32_t l = 0; l < nleaf; l++) {
         GraphDev s = sub_view(g, leaf_off[l], leaf_off[l + 1]);
-        if (learned) {
-            s.views = &vw;
-            s.view_leaf = l;
-        }
         if ((rc = kgraph_build(ctx, s))) return rc;
         subc += s.ncmps;
         absorb(g, s);
@@ -688,22 +766,8 @@ int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, u
         k_rebase<<<blocks_for(cnt, 256), 256, 0, ctx.stream>>>(s.pid, cnt, leaf_off[l], nleaf == 2 ? l : 0u); count_launch();
     }
     if (sub_ncmps) *sub_ncmps = subc;
-    if (g.fast && g.merge_tree) return merge_tree_levels(ctx, g, leaf_off);
     // 2. cross sampling (smerge.cpp:94-209)
     g.cut = K * 1 / 2;
-    if (g.fast) {
-        DevBuf& lo = ctx.ws.misc;
-        NNM_CUDA_TRY(lo.ensure(leaf_off.size() * 4 + 64));
-        NNM_CUDA_TRY(cudaMemcpyAsync(lo.p, leaf_off.data(), leaf_off.size() * 4, cudaMemcpyHostToDevice, ctx.stream));
-        rc = learned ? learned_cross(ctx, g, vw, lo.as<uint32_t>())
-                     : fast_rows(ctx, g, 0, n, K - g.cut, 0, 0, lo.as<uint32_t>(), nleaf, 0, 0);
-        if (rc) return rc;
-        g.ncmps += (uint64_t)n * g.cut;
-        if ((rc = run_nndescent(ctx, g, MODE_SMERGE, leaf_off[1], 0, lo.as<uint32_t>(), nleaf))) return rc;
-        k_merge2one<<<blocks_for(n, WPB), WPB * 32, 0, ctx.stream>>>(g.pid, g.pdist, g.cpid, g.cpdist, K, g.cut, n, g.fast ? 1u : 0u); count_launch();
-        NNM_CUDA_TRY(cudaGetLastError());
-        return 0;
-    }
     DevBuf& lo = ctx.ws.misc;
     NNM_CUDA_TRY(lo.ensure(leaf_off.size() * 4 + 64));
     NNM_CUDA_TRY(cudaMemcpyAsync(lo.p, leaf_off.data(), leaf_off.size() * 4, cudaMemcpyHostToDevice, ctx.stream));

@@ -326,6 +326,75 @@ int nnm_merge_leaves_dev(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, u
     return build_common(ctx, KIND_LEAVES, x, true, n, d, k, leaf_sizes, nleaf, opts, ids, dists, flags, stats);
 }
 
+namespace {
+// The two halves of a fast-tier multi-leaf build on device arrays.
+int leaves_common(nnm_ctx* ctx, bool merge, const float* x, uint64_t n, uint32_t d, uint32_t k,
+                  const uint32_t* leaf_sizes, uint32_t nleaf, uint32_t leaf0, const nnm_opts* opts,
+                  const uint32_t* ids_in, const float* dists_in, uint32_t* ids, float* dists, uint8_t* flags,
+                  nnm_stats* stats) {
+    if (!ctx) return NNM_ERR_INVALID;
+    if (!x || n == 0 || d == 0) return fail(ctx, NNM_ERR_INVALID, "x must be non-null with n, d > 0");
+    if (k == 0 || k > (uint32_t)nnm::MAXK) return fail(ctx, NNM_ERR_INVALID, "k must be in [1, 32]");
+    if (n >= (1ull << 30)) return fail(ctx, NNM_ERR_INVALID, "n must be below 2^30");
+    if (merge && (!ids_in || !dists_in)) return fail(ctx, NNM_ERR_INVALID, "the leaves' graphs must be given");
+    nnm_opts o;
+    if (opts) o = *opts;
+    else nnm_opts_default(&o);
+    int rc;
+    if (!opts_ok(ctx, &o, &rc)) return rc;
+    if (o.rng_mode != NNM_RNG_FAST) return fail(ctx, NNM_ERR_INVALID, "split leaf builds need rng_mode NNM_RNG_FAST");
+    if (!leaf_sizes || nleaf < (merge ? 2u : 1u) || nleaf > 1024) return fail(ctx, NNM_ERR_INVALID, "bad leaf count");
+    std::vector<uint32_t> off(1, 0);
+    for (uint32_t l = 0; l < nleaf; l++) {
+        if (leaf_sizes[l] < k + 2) return fail(ctx, NNM_ERR_INVALID, "every leaf needs at least k+2 rows");
+        off.push_back(off.back() + leaf_sizes[l]);
+    }
+    if (off.back() != n) return fail(ctx, NNM_ERR_INVALID, "leaf sizes must sum to n");
+    Ctx& c = ctx->c;
+    if (cudaSetDevice(c.device) != cudaSuccess) return fail(ctx, NNM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    GraphDev g;
+    setup_graph(g, o, n, d, k);
+    uint64_t sub = 0;
+    EventTimer tm(c.stream);
+    rc = nnm::upload_vectors(c, c.store, g, x, true);
+    if (!rc) rc = nnm::graph_alloc(c, c.store, g, false);
+    if (!rc) {
+        if (merge) {
+            rc = nnm::load_pools(c, g, ids_in, dists_in);
+            if (!rc) rc = nnm::merge_prebuilt(c, g, off);
+        } else {
+            rc = nnm::build_leaves(c, g, off, leaf0, &sub);
+        }
+    }
+    if (!rc) rc = nnm::export_graph(c, g, ids, dists, flags, false);
+    float ms = tm.stop();
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(c.stream);
+        if (e != cudaSuccess) rc = fail(ctx, NNM_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (!rc) {
+        if (!merge) g.ncmps = 0;
+        fill_stats(stats, g, sub, ms);
+    }
+    return rc;
+}
+}  // namespace
+
+int nnm_build_leaves_dev(nnm_ctx* ctx, const float* x_dev, uint64_t n, uint32_t d, uint32_t k,
+                         const uint32_t* leaf_sizes, uint32_t nleaf, uint32_t leaf0, const nnm_opts* opts,
+                         uint32_t* ids_dev, float* dists_dev, nnm_stats* stats) {
+    return leaves_common(ctx, false, x_dev, n, d, k, leaf_sizes, nleaf, leaf0, opts, nullptr, nullptr, ids_dev,
+                         dists_dev, nullptr, stats);
+}
+
+int nnm_merge_prebuilt_dev(nnm_ctx* ctx, const float* x_dev, uint64_t n, uint32_t d, uint32_t k,
+                           const uint32_t* leaf_sizes, uint32_t nleaf, const nnm_opts* opts,
+                           const uint32_t* ids_in_dev, const float* dists_in_dev, uint32_t* ids_dev,
+                           float* dists_dev, uint8_t* flags_dev, nnm_stats* stats) {
+    return leaves_common(ctx, true, x_dev, n, d, k, leaf_sizes, nleaf, 0, opts, ids_in_dev, dists_in_dev, ids_dev,
+                         dists_dev, flags_dev, stats);
+}
+
 int nnm_merge_create(nnm_ctx* ctx, const float* x, uint64_t n, uint32_t d, uint32_t k, const nnm_opts* opts,
                      nnm_merge** out) {
     if (!ctx) return NNM_ERR_INVALID;
@@ -506,6 +575,7 @@ int nnm_profile_enable(nnm_ctx* ctx, int on) {
     for (auto& r : ctx->c.join_rows) r = 0;
     ctx->c.join_rows_tc = 0;
     ctx->c.iter_log.clear();
+    ctx->c.audit_max = ctx->c.audit_err_c = 0.f;
     return NNM_OK;
 }
 
@@ -521,6 +591,9 @@ int nnm_profile_get(const nnm_ctx* ctx, char* buf, uint64_t buflen) {
                   (unsigned long long)c.kjoin.launches, c.kjoin.ms, c.kjoin.bytes, c.kjoin.flops, c.kjoin.tensor_ops,
                   (unsigned long long)c.kemit.launches, c.kemit.ms, c.kemit.bytes, c.kemit.tensor_ops,
                   (unsigned long long)c.kmerge.launches, c.kmerge.ms, c.kmerge.bytes);
+    js += tmp;
+    std::snprintf(tmp, sizeof tmp, "\"audit\": {\"max_rel\": %.9g, \"err_c\": %.9g}, ", (double)c.audit_max,
+                  (double)c.audit_err_c);
     js += tmp;
     std::snprintf(tmp, sizeof tmp, "\"rows\": {\"tiers\": [%llu, %llu, %llu, %llu, %llu], \"tensor\": %llu}, \"iters\": [",
                   (unsigned long long)c.join_rows[0], (unsigned long long)c.join_rows[1],

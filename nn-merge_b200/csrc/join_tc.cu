@@ -429,6 +429,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                                 if (PASS == 0 && a.audit && pv) {  // the bound against the exact distance
                                     const float ex = audit_l2(a.x, a.dp, e_a & LID_MASK, e_b & LID_MASK);
                                     if (!(ex >= lb && ex <= dd + a.err_c * ns)) atomicOr(a.tc_err, (unsigned)DERR_BOUND);
+                                    if (ns > 0.f) atomicMax(&a.ctr->audit_max, __float_as_uint(fabsf(ex - dd) / ns));
                                 }
                             }
                             const uint32_t axb = APPROX ? APPROX_BIT : 0u;

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "nnm_engine.h"
@@ -1824,6 +1825,12 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         if (hc.error) {
             ctx.last_error = "device capacity check failed (code " + std::to_string(hc.error) + ")";
             return 6;
+        }
+        if (ctx.prof && g.audit) {
+            float am;
+            std::memcpy(&am, &hc.audit_max, 4);
+            ctx.audit_max = std::max(ctx.audit_max, am);
+            ctx.audit_err_c = g.err_c;
         }
         if (ctx.prof) {
             float t01 = 0.f, t23 = 0.f, t34 = 0.f;

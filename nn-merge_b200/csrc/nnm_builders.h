@@ -26,6 +26,13 @@ int kgraph_build(Ctx& ctx, GraphDev& g);
 // with two leaves split at n*5/10 this is Smerge::buildKGraph.
 int merge_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, uint64_t* sub_ncmps);
 int jmerge_build(Ctx& ctx, GraphDev& g, uint64_t* sub_ncmps);
+// Fast tier, the two halves of merge_leaves: the leaf builds alone (leaf0:
+// the index of the first leaf among all leaves of the build; pools end with
+// ids of g's rows), and the merge of leaves whose graphs are in g's pools.
+int build_leaves(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off, uint32_t leaf0, uint64_t* ncmps);
+int merge_prebuilt(Ctx& ctx, GraphDev& g, const std::vector<uint32_t>& leaf_off);
+// Copies a caller's n x K device pools (ids of g's rows, distances) into g.
+int load_pools(Ctx& ctx, GraphDev& g, const uint32_t* ids_dev, const float* dists_dev);
 int hmerge_build(Ctx& ctx, GraphDev& g, const LayerHook& on_layer);
 
 // Staged merge (reference streams): the steps of Smerge::buildKGraph

@@ -89,6 +89,9 @@ struct Ctx {
         float ms_join, ms_emit, ms_merge;
     };
     std::vector<IterLog> iter_log;
+    // audit of the reduced-precision joins (while profiling): the largest
+    // |d~ - d| / (|a|^2 + |b|^2) seen and the bound coefficient it is held to
+    float audit_max = 0.f, audit_err_c = 0.f;
     cudaEvent_t ev[8] = {};
     cudaStream_t stream = nullptr;
     Workspace ws;
@@ -149,6 +152,13 @@ struct GraphDev {
     uint32_t iters = 0;
     std::vector<float> trace;
 };
+
+// Philox phases of the fast tier's multi-leaf build: the leaves' initial
+// draws use phases 0 .. nleaf - 1, the leaf run's iterations start at
+// LEAF_PHASE0, the merge's draws at MERGE_PHASE0 -- so that the merge does
+// not depend on how the leaves were built (one run or one per rank).
+constexpr uint32_t LEAF_PHASE0 = 1u << 24;
+constexpr uint32_t MERGE_PHASE0 = 1u << 28;
 
 #define NNM_CUDA_TRY(expr)                                                         \
     do {                                                                           \

@@ -58,7 +58,7 @@ struct IterCounters {
     unsigned int nbig_rev;         // reverse lists longer than one warp
     unsigned int overflow;         // a buffer sized ahead of the counts was too small (OVF_*): the
                                    // join and merge kernels did nothing, the host grows it and reruns
-    unsigned int pad;
+    unsigned int audit_max;        // audit: largest |d~ - d| / (|a|^2 + |b|^2) seen (float bits)
     unsigned long long sum_s;      // sum over joined rows of |new| + |old|
     unsigned long long pairs;      // pair-distance slots of this iteration
     unsigned int ntier[5];         // rows per join tier (by list size)

@@ -20,6 +20,7 @@ EXPORTED = (
     "nnm_train_opts_default", "nnm_mlp_train", "nnm_mlp_grad", "nnm_mlp_codes", "nnm_set_init_model",
     "nnm_merge_create", "nnm_merge_subgraph", "nnm_merge_init_sgraph", "nnm_merge_initial_graph",
     "nnm_merge_nndescent", "nnm_merge_merge2one", "nnm_merge_read", "nnm_merge_free",
+    "nnm_build_leaves_dev", "nnm_merge_prebuilt_dev",
 )
 MLP_HIDDEN, MLP_OUT = 256, 32
 
@@ -176,6 +177,8 @@ def load():
         lib.nnm_merge_merge2one.argtypes = [vp, u32]
         lib.nnm_merge_read.argtypes = [vp, vp, vp, vp]
         lib.nnm_merge_free.argtypes = [vp]
+        lib.nnm_build_leaves_dev.argtypes = [vp, vp, u64, u32, u32, vp, u32, u32, vp, vp, vp, vp]
+        lib.nnm_merge_prebuilt_dev.argtypes = [vp, vp, u64, u32, u32, vp, u32, vp, vp, vp, vp, vp, vp, vp]
         _lib = lib
     return _lib
 
@@ -323,6 +326,30 @@ class Context:
                                                   ctypes.byref(o), ctypes.c_void_p(ids_ptr),
                                                   ctypes.c_void_p(dists_ptr), ctypes.c_void_p(flags_ptr),
                                                   ctypes.byref(st)))
+        return _stats_dict(st)
+
+    def build_leaves_dev(self, x_ptr, n, d, k, leaf_sizes, ids_ptr, dists_ptr, leaf0=0, **kw):
+        """The leaf builds of merge_leaves_dev alone (fast tier): ids local
+        to the rows at x_ptr; leaf0 = index of the first leaf in the build."""
+        sizes = np.ascontiguousarray(leaf_sizes, np.uint32)
+        st = Stats()
+        o = make_opts(**kw)
+        self._check(self.lib.nnm_build_leaves_dev(self.h, ctypes.c_void_p(x_ptr), n, d, k, _ptr(sizes), len(sizes),
+                                                  leaf0, ctypes.byref(o), ctypes.c_void_p(ids_ptr),
+                                                  ctypes.c_void_p(dists_ptr), ctypes.byref(st)))
+        return _stats_dict(st)
+
+    def merge_prebuilt_dev(self, x_ptr, n, d, k, leaf_sizes, ids_in_ptr, dists_in_ptr, ids_ptr, dists_ptr,
+                           flags_ptr=0, **kw):
+        """The merge of merge_leaves_dev over leaves whose graphs are given."""
+        sizes = np.ascontiguousarray(leaf_sizes, np.uint32)
+        st = Stats()
+        o = make_opts(**kw)
+        self._check(self.lib.nnm_merge_prebuilt_dev(self.h, ctypes.c_void_p(x_ptr), n, d, k, _ptr(sizes), len(sizes),
+                                                    ctypes.byref(o), ctypes.c_void_p(ids_in_ptr),
+                                                    ctypes.c_void_p(dists_in_ptr), ctypes.c_void_p(ids_ptr),
+                                                    ctypes.c_void_p(dists_ptr), ctypes.c_void_p(flags_ptr),
+                                                    ctypes.byref(st)))
         return _stats_dict(st)
 
     def merge_leaves_into(self, x, k, leaf_sizes, ids, dists=None, flags=None, **kw):

@@ -95,10 +95,12 @@ def test_reference_reads_the_dropin_hierarchy(oracle):
     reference's own LySearch::loadGraphs (lysearch.cpp:112-186) reads it and
     searches: its results equal the oracle's search on the layers as this
     package parses them (so both read the file alike), and those layers are
-    the reference's own H-Merge hierarchy."""
+    the reference's own H-Merge hierarchy.  The reference's search walks
+    five layers (lysearch.cpp:393-421), so the set has more than 32,768
+    rows."""
     from nnm import io as nio
     from nnm.datasets import queries_like
-    x = gaussian_mixture_u8(6000, d=16, seed=12)
+    x = gaussian_mixture_u8(34000, d=16, seed=12)
     q = queries_like(200, d=16, seed=12, query_seed=5)
     with tempfile.TemporaryDirectory() as td:
         exe = build(td)
