@@ -105,7 +105,10 @@ typedef struct {
     uint32_t merge_order; /* an nnm_merge_order, read by nnm_merge_leaves */
     uint32_t no_graph;    /* nonzero: launch every kernel directly; zero: the fast tier replays
                              each NN-Descent iteration as a CUDA graph where it can */
-    uint32_t reserved[4];
+    uint32_t tile_rows;   /* u8 tensor-core join: the longest sample lists (entries of a row's
+                             new + old lists) joined in tensor-core tiles, 32, 64 or 128 (0: 128);
+                             longer lists go to the dp4a pair kernel.  Same graphs either way. */
+    uint32_t reserved[3];
 } nnm_opts;
 
 typedef struct {
@@ -478,8 +481,9 @@ typedef struct {
 typedef struct {
     uint32_t sample_cap;
     float delta;
-    float recall; /* on the sample */
-    double ms;    /* device time of the sample build */
+    float recall;       /* on the sample */
+    uint32_t tile_rows; /* nnm_opts.tile_rows of the trial */
+    double ms;          /* device time of the sample build */
 } nnm_tune_trial;
 
 typedef struct {

@@ -64,6 +64,10 @@ bool opts_ok(nnm_ctx* ctx, const nnm_opts* o, int* rc) {
         *rc = fail(ctx, NNM_ERR_INVALID, "unknown init");
         return false;
     }
+    if (o->tile_rows != 0 && o->tile_rows != 32 && o->tile_rows != 64 && o->tile_rows != 128) {
+        *rc = fail(ctx, NNM_ERR_INVALID, "tile_rows must be 0, 32, 64 or 128");
+        return false;
+    }
     if (o->merge_order > NNM_MERGE_TREE) {
         *rc = fail(ctx, NNM_ERR_INVALID, "unknown merge_order");
         return false;
@@ -96,6 +100,7 @@ void setup_graph(GraphDev& g, const nnm_opts& o, uint64_t n, uint32_t d, uint32_
     g.audit = o.audit != 0;
     g.merge_tree = o.merge_order == NNM_MERGE_TREE;
     g.no_graph = o.no_graph != 0;
+    g.tile_rows = o.tile_rows ? o.tile_rows : 128u;
     g.init = o.init;
     g.phase = 0;
 }
@@ -854,14 +859,34 @@ int nnm_autotune_merge_leaves(nnm_ctx* ctx, const float* x_dev, uint64_t n, uint
                                            10, &rec);
             if (rc) return done(rc);
             const uint32_t i = res.ntrials++;
-            res.trials[i] = nnm_tune_trial{cap, dl, (float)rec, ms};
+            res.trials[i] = nnm_tune_trial{cap, dl, (float)rec, b.tile_rows ? b.tile_rows : 128u, ms};
             if (rec >= (double)(t.target_recall + t.margin) && (best < 0 || ms < res.trials[best].ms)) best = (int)i;
             if (rec > res.trials[best_rec].recall) best_rec = (int)i;
         }
     res.chosen = best >= 0 ? (uint32_t)best : (uint32_t)best_rec;
+    // then the tile shape at the chosen cap and threshold: the longest lists
+    // joined in tensor-core tiles (the graphs are the same; only time decides)
+    for (uint32_t tr : {64u, 32u}) {
+        nnm_opts o = b;
+        o.sample_cap = res.trials[res.chosen].sample_cap;
+        o.delta = res.trials[res.chosen].delta;
+        o.tile_rows = tr;
+        double ms = 1e30;
+        for (uint32_t r = 0; r < t.repeats; r++) {
+            nnm_stats stt;
+            int rc = nnm_merge_leaves_dev(ctx, x_dev, ns, d, k, ls.data(), nleaf, &o, ib.as<uint32_t>(), nullptr,
+                                          nullptr, &stt);
+            if (rc) return done(rc);
+            ms = std::min(ms, stt.device_ms);
+        }
+        const uint32_t i = res.ntrials++;
+        res.trials[i] = nnm_tune_trial{o.sample_cap, o.delta, res.trials[res.chosen].recall, tr, ms};
+        if (ms < res.trials[res.chosen].ms) res.chosen = i;
+    }
     *tuned = b;
     tuned->sample_cap = res.trials[res.chosen].sample_cap;
     tuned->delta = res.trials[res.chosen].delta;
+    tuned->tile_rows = res.trials[res.chosen].tile_rows;
     if (result) *result = res;
     return done(0);
 }

@@ -431,7 +431,9 @@ __global__ void k_shuffle_append(ShufArgs a) {
         a.npairs[t] = nl && S > a.tc_max_s ? nl * (nl - 1) / 2 + nl * ol : 0u;
         if (nl) {
             int tier = tier_of(S);
-            if (tier < NTIER - 1 && S > a.tc_max_s && tier > a.max_staged) tier = NTIER - 1;
+            // next to the tensor-core join (tc_max_s != 0) longer lists take the
+            // pair kernel; without it, tiers whose staged vectors do not fit
+            if (tier < NTIER - 1 && S > a.tc_max_s && (a.tc_max_s != 0 || tier > a.max_staged)) tier = NTIER - 1;
             a.tier_rows[(size_t)tier * a.n + atomicAdd(&a.ctr->ntier[tier], 1u)] = t;
         }
     }
@@ -1542,7 +1544,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                             track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
                             track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
                             P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, phase,
-                            tc ? TC_MAX_S : 0u, max_staged, rscr_new, rscr_old, (g.fast && carry_now) ? 1u : 0u};
+                            tc ? (g.tc_kind == 0 ? g.tile_rows : TC_MAX_S) : 0u, max_staged, rscr_new, rscr_old,
+                            (g.fast && carry_now) ? 1u : 0u};
         };
         // the segment; its first failing call's error is returned.  copy:
         // read the counters back at its end (the whole-iteration graph reads

@@ -143,6 +143,7 @@ struct GraphDev {
     bool audit = false;        // reduced-precision joins: check every pair against its bound
     bool merge_tree = false;   // multi-leaf merges: bottom-up pairwise levels instead of all at once
     bool no_graph = false;     // launch every kernel directly (no CUDA graphs)
+    uint32_t tile_rows = 128;  // u8 tensor-core join: longest lists in tensor-core tiles (32, 64, 128)
     // Fast tier: counter-based random draws (Philox keyed by the seed) in
     // place of the reference's sequential streams, so the initial graphs and
     // samples are drawn on the device and reverse lists need no ordering.

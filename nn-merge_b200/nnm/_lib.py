@@ -38,7 +38,7 @@ class Opts(ctypes.Structure):
                 ("sample_cap", ctypes.c_uint32), ("delta", ctypes.c_float), ("max_iter", ctypes.c_uint32),
                 ("exact_trace", ctypes.c_uint32), ("join_kernel", ctypes.c_uint32),
                 ("init", ctypes.c_uint32), ("audit", ctypes.c_uint32), ("merge_order", ctypes.c_uint32),
-                ("no_graph", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 4)]
+                ("no_graph", ctypes.c_uint32), ("tile_rows", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3)]
 
 
 class Mlp(ctypes.Structure):
@@ -105,7 +105,7 @@ class TuneOpts(ctypes.Structure):
 
 class TuneTrial(ctypes.Structure):
     _fields_ = [("sample_cap", ctypes.c_uint32), ("delta", ctypes.c_float), ("recall", ctypes.c_float),
-                ("ms", ctypes.c_double)]
+                ("tile_rows", ctypes.c_uint32), ("ms", ctypes.c_double)]
 
 
 class TuneResult(ctypes.Structure):
@@ -195,7 +195,7 @@ INITS = {"random": 0, "learned": 1}
 
 
 def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exact_trace=False, rng="exact",
-              join="auto", init="random", audit=False, merge_order="all", graph=True):
+              join="auto", init="random", audit=False, merge_order="all", graph=True, tile_rows=0):
     lib = load()
     o = Opts()
     lib.nnm_opts_default(ctypes.byref(o))
@@ -211,6 +211,7 @@ def make_opts(seed=0, metric="l2", sample_cap=100, delta=0.002, max_iter=0, exac
     o.audit = 1 if audit else 0
     o.merge_order = {"all": 0, "tree": 1}[merge_order]
     o.no_graph = 0 if graph else 1
+    o.tile_rows = tile_rows
     return o
 
 
@@ -441,9 +442,10 @@ class Context:
                                                        len(sizes), ctypes.byref(o), ctypes.byref(t),
                                                        ctypes.byref(tuned), ctypes.byref(res)))
         trials = [dict(sample_cap=int(res.trials[i].sample_cap), delta=float(res.trials[i].delta),
-                       recall=float(res.trials[i].recall), ms=float(res.trials[i].ms)) for i in range(res.ntrials)]
+                       recall=float(res.trials[i].recall), tile_rows=int(res.trials[i].tile_rows),
+                       ms=float(res.trials[i].ms)) for i in range(res.ntrials)]
         chosen = trials[res.chosen]
-        return dict(sample_cap=chosen["sample_cap"], delta=chosen["delta"]), trials
+        return dict(sample_cap=chosen["sample_cap"], delta=chosen["delta"], tile_rows=chosen["tile_rows"]), trials
 
     # -- serving ------------------------------------------------------------
     def index(self, x, layers, seed=0, metric="l2"):

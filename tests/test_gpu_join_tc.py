@@ -232,3 +232,20 @@ def test_forced_tensor_rejects_other_metrics(ctx):
     x = gaussian_mixture_u8(2000, d=32, seed=41)
     with pytest.raises(NnmError):
         ctx.kgraph(x, 10, seed=1, metric="l1", join="tensor")
+
+
+@pytest.mark.parametrize("rng", ["exact", "fast"])
+def test_tile_rows_give_the_same_graph(ctx, rng):
+    """Lists longer than tile_rows go from the tensor-core tiles to the dp4a
+    pair kernel: both exact, the same graph for every boundary."""
+    x = gaussian_mixture_u8(6000, seed=91)
+    ref = ctx.kgraph(x, 20, seed=3, rng=rng, join="tensor")
+    for tr in (32, 64):
+        ctx.profile(True)
+        g = ctx.kgraph(x, 20, seed=3, rng=rng, join="tensor", tile_rows=tr)
+        rows = ctx.profile_stats()["rows"]
+        ctx.profile(False)
+        same(g, ref)
+        assert rows["tensor"] > 0 and rows["tiers"][4] > 0
+    with pytest.raises(NnmError):
+        ctx.kgraph(x, 20, seed=3, join="tensor", tile_rows=48)
