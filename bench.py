@@ -657,7 +657,7 @@ def run_cfg1(ctx, torch, seed):
     x = gaussian_mixture_u8(100_000, d=128, n_centres=64, seed=1234)
     t_ref, kind, cores, ref_ids = reference_cpu(x, 20, seed, len(x), want_graph=True)
     out = {"workload": "100000x128 (64-centre mixture) S-Merge of the halves, k=20, reference streams",
-           "reference_s": t_ref, "reference_kind": kind, "reference_cores": cores}
+           "reference_s": t_ref, "reference_kind": kind, "reference_cores": cores, "host_cpus": os.cpu_count()}
     for name, join in (("plain_fp32", "fp32"), ("exact_u8", "tensor")):
         ctx.smerge(x, 20, seed=seed, join=join)  # warm-up
         t0 = time.perf_counter()
@@ -863,7 +863,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         f = cpu_fit(x, k, build_seed, a.cpu_sample, a.fit_rows, n)
-        cpu = {"value": f["value"], "unit": "s", "cores": f["cores"], "kind": f["kind"],
+        cpu = {"value": f["value"], "unit": "s", "cores": f["cores"], "kind": f["kind"], "host_cpus": os.cpu_count(),
                "sample": "S-Merge of the first %d and %d rows of this set (%.1f s, %.1f s), extrapolated to %d rows "
                          "by the power law through both (exponent %.3f)"
                          % (f["rows"][0], f["rows"][1], f["t_small"], f["t_large"], n, f["alpha"]),
