@@ -528,6 +528,7 @@ static GraphDev sub_view(const GraphDev& p, uint32_t b, uint32_t e) {
     if (p.xq) {
         s.xq = p.xq + (size_t)b * p.kq;
         s.nrm = p.nrm + b;
+        if (p.scl) s.scl = p.scl + b;  // FP8 operands: the rows' scales with their rows
     }
     s.pid = p.pid + (size_t)b * p.K;
     s.pdist = p.pdist + (size_t)b * p.K;

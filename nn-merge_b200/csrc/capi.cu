@@ -286,6 +286,8 @@ int nnm_ctx_destroy(nnm_ctx* ctx) {
     cudaStreamSynchronize(ctx->c.stream);
     for (auto& e : ctx->c.ev)
         if (e) cudaEventDestroy(e);
+    for (auto& ig : ctx->c.iter_graph)
+        if (ig.exec) cudaGraphExecDestroy(ig.exec);
     ctx->c.ws.release_all();
     ctx->c.store.release();
     if (ctx->c.init_model) {

@@ -238,6 +238,7 @@ struct ShufArgs {
     int max_staged;       // highest FP32 tier whose vectors fit in shared memory (-1: none); larger lists go unstaged
     uint32_t *rscr_new, *rscr_old;  // scratch of the reverse lists' sizes (fast tier: duplicate removal)
     uint32_t dedupe;      // fast tier, first iteration of an H-Merge level: carried + new lists may repeat ids
+    const uint32_t* phase_dev;  // non-null: the draw phase is read here (an iteration graph's replays)
 };
 
 __global__ void k_rand_count(const uint64_t* roff_new, const uint64_t* roff_old, uint32_t n, uint32_t* out) {
@@ -391,7 +392,9 @@ __global__ void k_shuffle_append(ShufArgs a) {
         bool staged = len <= SHUF_SMEM;
         if (a.fast) {
             // a uniform random subset of smplNum entries, chosen by id
-            if (len > a.smpl) hash_sample(seg, len, keep, Philox{a.seed, 0x6e6e6d01u}, t, a.phase, (uint32_t)l, hist[w]);
+            if (len > a.smpl)
+                hash_sample(seg, len, keep, Philox{a.seed, 0x6e6e6d01u}, t, a.phase_dev ? *a.phase_dev : a.phase,
+                            (uint32_t)l, hist[w]);
             __syncwarp();
             sh = seg;
         } else if (staged) {
@@ -1500,23 +1503,17 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             if (graph) cudaGraphDestroy(graph);
         }
     } seg;
-    // The whole-iteration graph of the fast tier on the tensor cores.
-    struct WholeGraph {
-        cudaGraph_t graph = nullptr;
+    // The whole-iteration graph of the fast tier on the tensor cores: the
+    // context's executable graph of this join mode, once it holds this
+    // call's iteration (owned by the context).
+    struct {
         cudaGraphExec_t exec = nullptr;
-        cudaGraphNode_t shuf = nullptr;
-        cudaKernelNodeParams kp{};
-        uint64_t launches = 0;
         bool disabled = false;
-        void reset() {
-            if (exec) cudaGraphExecDestroy(exec);
-            if (graph) cudaGraphDestroy(graph);
-            exec = nullptr;
-            graph = nullptr;
-            shuf = nullptr;
-        }
-        ~WholeGraph() { reset(); }
     } whole_g;
+    // the draw phase of the replays: a device word past the counters and its
+    // pinned host source past the host counters
+    uint32_t* phase_dev = reinterpret_cast<uint32_t*>(ctr + 1);
+    uint32_t* h_phase = reinterpret_cast<uint32_t*>(ctx.h_counters + 1);
     // the node of kernel `fn` in a captured graph, and its parameters
     auto find_kernel_node = [](cudaGraph_t graph, void* fn, cudaKernelNodeParams& out) -> cudaGraphNode_t {
         size_t nn = 0;
@@ -1545,12 +1542,12 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                             track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
                             P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, phase,
                             tc ? (g.tc_kind == 0 ? g.tile_rows : TC_MAX_S) : 0u, max_staged, rscr_new, rscr_old,
-                            (g.fast && carry_now) ? 1u : 0u};
+                            (g.fast && carry_now) ? 1u : 0u, nullptr};
         };
         // the segment; its first failing call's error is returned.  copy:
         // read the counters back at its end (the whole-iteration graph reads
         // them once, after the merge)
-        auto seg_a = [&](bool copy = true) -> cudaError_t {
+        auto seg_a = [&](bool copy = true, const uint32_t* phase_dev = nullptr) -> cudaError_t {
             cudaError_t e = cudaSuccess;
             auto chk = [&](cudaError_t x) {
                 if (e == cudaSuccess) e = x;
@@ -1593,7 +1590,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             } else {
                 chk(cudaMemsetAsync(d_tot, 0, 8, st));
             }
-            const ShufArgs sh = shuf_args();
+            ShufArgs sh = shuf_args();
+            sh.phase_dev = phase_dev;
             k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh); count_launch();
             chk(exclusive_scan(P<uint32_t>(ws.npairs), P<uint64_t>(ws.poff), n, scan_tmp,
                                reinterpret_cast<uint64_t*>(&ctr->pairs), st));
@@ -1686,13 +1684,19 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         const bool whole = g.fast && tc && !carry_now && !whole_g.disabled && !g.no_graph && it > 0;
         bool done = false;
         if (whole) {
+            // The graph is captured at the call's first whole iteration and
+            // applied to the context's executable graph of this join mode
+            // (cudaGraphExecUpdate: no new instantiation while the shape of
+            // the iteration is the same); the draw phase is read from a
+            // device word, written before each replay.
+            Ctx::IterGraph& ig = ctx.iter_graph[(int)mode & 3];
             if (!whole_g.exec) {
                 const uint64_t c0 = launch_counter().load();
                 cudaGraph_t graph = nullptr;
                 cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
                 if (e == cudaSuccess) {
                     const JoinArgs ja = make_ja();
-                    cudaError_t e1 = seg_a(false);
+                    cudaError_t e1 = seg_a(false, phase_dev);
                     if (e1 == cudaSuccess) {
                         k_check_cap<<<1, 32, 0, st>>>(ctr, reinterpret_cast<const unsigned long long*>(&ctr->pairs),
                                                       (unsigned long long)(ws.pd.bytes / 4), OVF_PAIRS); count_launch();
@@ -1708,28 +1712,32 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
                     e = e1 != cudaSuccess ? e1 : e2;
                 }
-                if (e == cudaSuccess) e = cudaGraphInstantiate(&whole_g.exec, graph, 0);
-                if (e == cudaSuccess) whole_g.shuf = find_kernel_node(graph, reinterpret_cast<void*>(k_shuffle_append),
-                                                                      whole_g.kp);
-                whole_g.graph = graph;
-                whole_g.launches = launch_counter().load() - c0;
-                if (e != cudaSuccess || !whole_g.shuf) {  // no graph: this call launches directly
+                if (e == cudaSuccess && ig.exec) {
+                    cudaGraphExecUpdateResultInfo info;
+                    if (cudaGraphExecUpdate(ig.exec, graph, &info) != cudaSuccess) {
+                        cudaGetLastError();
+                        cudaGraphExecDestroy(ig.exec);
+                        ig.exec = nullptr;
+                    }
+                }
+                if (e == cudaSuccess && !ig.exec) e = cudaGraphInstantiate(&ig.exec, graph, 0);
+                if (graph) cudaGraphDestroy(graph);
+                ig.launches = launch_counter().load() - c0;
+                if (e != cudaSuccess) {  // no graph: this call launches directly
                     cudaGetLastError();
-                    whole_g.reset();
+                    if (ig.exec) cudaGraphExecDestroy(ig.exec);
+                    ig.exec = nullptr;
                     whole_g.disabled = true;
+                } else {
+                    whole_g.exec = ig.exec;
                 }
             } else {
-                count_launch(whole_g.launches);
+                count_launch(ig.launches);
             }
             if (whole_g.exec) {
-                ShufArgs sh = shuf_args();
-                void* kargs[] = {&sh};
-                cudaKernelNodeParams kp = whole_g.kp;
-                kp.kernelParams = kargs;
-                kp.extra = nullptr;
-                cudaError_t e = cudaGraphExecKernelNodeSetParams(whole_g.exec, whole_g.shuf, &kp);
-                if (e == cudaSuccess) e = cudaGraphLaunch(whole_g.exec, st);
-                NNM_CUDA_TRY(e);
+                *h_phase = phase;  // pinned; the copy is enqueued before the replay
+                NNM_CUDA_TRY(cudaMemcpyAsync(phase_dev, h_phase, 4, cudaMemcpyHostToDevice, st));
+                NNM_CUDA_TRY(cudaGraphLaunch(whole_g.exec, st));
                 NNM_CUDA_TRY(cudaStreamSynchronize(st));
                 IterCounters& h = *ctx.h_counters;
                 if (h.error) {
@@ -1740,7 +1748,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                     // grow what was short (the graph names the old buffers:
                     // it is captured again next iteration) and rerun what the
                     // kernels skipped
-                    whole_g.reset();
+                    whole_g.exec = nullptr;
                     unsigned nt[NTIER];
                     for (int t = 0; t < NTIER; t++) nt[t] = h.ntier[t];
                     const unsigned ovf = h.overflow;

@@ -93,6 +93,12 @@ struct Ctx {
     // |d~ - d| / (|a|^2 + |b|^2) seen and the bound coefficient it is held to
     float audit_max = 0.f, audit_err_c = 0.f;
     cudaEvent_t ev[8] = {};
+    // executable whole-iteration graphs of the fast tier, one per join mode,
+    // refreshed by cudaGraphExecUpdate at each NN-Descent call
+    struct IterGraph {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t launches = 0;
+    } iter_graph[4];
     cudaStream_t stream = nullptr;
     Workspace ws;
     IterCounters* h_counters = nullptr;  // pinned
