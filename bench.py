@@ -101,6 +101,8 @@ def parse():
                         "vmf: 10M x 96 unit vectors, log-uniform leaves merged, FP32 / BF16 / FP8 joins")
     p.add_argument("--vmf-n", type=int, default=10_000_000)
     p.add_argument("--vmf-tiers", default="fp32,tensor,fp8")
+    p.add_argument("--vmf-tree-tiers", default="tensor,fp8",
+                   help="vmf: join tiers also timed with the bottom-up pairwise merge of the leaves")
     p.add_argument("--queries", type=int, default=100_000)
     p.add_argument("--probes", type=int, default=4)
     p.add_argument("--entry-steps", type=int, default=1500)
@@ -600,8 +602,9 @@ def run_vmf(a, rank, world, local):
     ctx = nnm.Context(local)
     rows = np.sort(np.random.default_rng(7).choice(n, 2000, replace=False))
     tiers, ref_ids = {}, None
-    for tier in a.vmf_tiers.split(","):
-        kw = dict(seed=a.seed, rng="fast", join=tier, init="random")
+    runs = [(t, "all") for t in a.vmf_tiers.split(",") if t] + [(t, "tree") for t in a.vmf_tree_tiers.split(",") if t]
+    for tier, order in runs:
+        kw = dict(seed=a.seed, rng="fast", join=tier, init="random", merge_order=order)
         ctx.merge_leaves_dev(x_dev.data_ptr(), n, d, k, sizes, ids_dev.data_ptr(), dists_dev.data_ptr(), 0, **kw)
         ctx.profile(True)
         times = []
@@ -623,11 +626,14 @@ def run_vmf(a, rank, world, local):
         ref_s = ((x[rows][:, None, :].astype(np.float64) - x[ids_s].astype(np.float64)) ** 2).sum(-1)
         rel = np.abs(ds_s - ref_s) / np.maximum(ref_s, 1e-30)
         same = None
-        if ref_ids is None:
-            ref_ids = ids.copy()
-        else:
-            same = bool(np.array_equal(ids, ref_ids))
-        tiers[tier] = {"s": statistics.median(times), "times": times, "iterations": st["iterations"],
+        if order == "all":
+            if ref_ids is None:
+                ref_ids = ids.copy()
+            else:
+                same = bool(np.array_equal(ids, ref_ids))
+        tiers[tier if order == "all" else tier + "/tree"] = {
+                       "s": statistics.median(times), "times": times, "iterations": st["iterations"],
+                       "merge_order": order,
                        "recall@10": rec, "recall@10_ids": rec_ids,
                        "dist_err_vs_fp64": {"max_rel": float(rel.max()), "mean_rel": float(rel.mean())},
                        "same_graph_as_first_tier": same,
