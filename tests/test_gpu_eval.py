@@ -59,11 +59,16 @@ def test_autotune_meets_its_target(ctx):
     kw = dict(seed=3, rng="fast", join="tensor", init="random")
     chosen, trials = ctx.autotune_merge_leaves_dev(xd.data_ptr(), n, 128, k, sizes, target_recall=0.93,
                                                    sample_rows=30_000, eval_rows=500, repeats=1, **kw)
-    assert len(trials) == 15 and all(0 < t["recall"] <= 1 and t["ms"] > 0 for t in trials)
-    ok = [t for t in trials if t["recall"] >= 0.935]
-    pick = [t for t in trials if t["sample_cap"] == chosen["sample_cap"] and t["delta"] == chosen["delta"]][0]
+    # 15 trials of sample cap x threshold, then the tile shape at the chosen pair
+    assert len(trials) == 17 and all(0 < t["recall"] <= 1 and t["ms"] > 0 for t in trials)
+    grid, tiles = trials[:15], trials[15:]
+    ok = [t for t in grid if t["recall"] >= 0.935]
+    pick = [t for t in grid if t["sample_cap"] == chosen["sample_cap"] and t["delta"] == chosen["delta"]][0]
     if ok:
         assert pick["recall"] >= 0.935 and pick["ms"] == min(t["ms"] for t in ok)
+    assert [t["tile_rows"] for t in tiles] == [64, 32] and pick["tile_rows"] == 128
+    assert all(t["sample_cap"] == pick["sample_cap"] and t["delta"] == pick["delta"] for t in tiles)
+    assert chosen["tile_rows"] == min([pick] + tiles, key=lambda t: t["ms"])["tile_rows"]
     # the tuned build on the whole set stays near the target
     kw.update(chosen)
     g = ctx.merge_leaves(x, k, sizes, **kw)
