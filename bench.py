@@ -22,7 +22,9 @@ Printed JSON (one line, rank 0):
   e2e         the same through the host C ABI (nnm_merge_leaves): pinned
               host vectors copied in, the graph (ids) copied back, per step;
   roofline    the dominant kernel (the local join) from the library's own
-              CUDA-event timing and algorithmic byte count;
+              CUDA-event timing and algorithmic byte count, over a second
+              run of the same K steps with those events on (the timed
+              steps run without them);
   cpu_baseline the reference itself (oracle/_ref, built from its sources) on
               the first 40,000 and 100,000 rows of the same set,
               extrapolated to 1M rows by the power law through both times;
@@ -80,6 +82,7 @@ def parse():
     p.add_argument("--no-cfg1", action="store_true",
                    help="skip the 100,000-row plain S-Merge timed on the reference and the GPU")
     p.add_argument("--no-search", action="store_true", help="build workload: skip the embedded serving measurement")
+    p.add_argument("--dump-iters", default=None, help="write the profiled steps' per-iteration counters (JSON)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--path", default="fast", choices=["exact", "fast"],
@@ -781,7 +784,6 @@ def main():
     for _ in range(a.warmup):
         st = build_dev()
     torch.cuda.synchronize()
-    ctx.profile(True)
     l0 = ctx.launch_count()
     stream = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -795,8 +797,23 @@ def main():
         torch.cuda.synchronize()
         barrier()
     launches = ctx.launch_count() - l0
+    # the same K steps again with the library's per-kernel CUDA events on
+    # (the roofline's kernel times and byte counts come from this run)
+    ctx.profile(True)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for _ in range(a.steps):
+        build_dev()
+    p1.record(stream)
+    torch.cuda.synchronize()
     prof = ctx.profile_stats()
     ctx.profile(False)
+    prof_ms = p0.elapsed_time(p1) / a.steps
+    if a.dump_iters:
+        with open(a.dump_iters, "w") as f:
+            json.dump({"iters": prof["iters"], "kq": (d + 31) // 32 * 32, "steps": a.steps,
+                       "columns": ["n", "rows_per_tier", "pairs", "proposals", "flags", "ncmps", "sum_s",
+                                   "ms_join", "ms_emit", "ms_merge"]}, f)
     # the same build with every kernel launched directly (no iteration graphs)
     direct = None
     if a.path == "fast":
@@ -862,9 +879,10 @@ def main():
                 "tensor_tflops": t_ops / (per_ms * 1e-3) / 1e12,
                 "tensor_frac": (t_ops / (per_ms * 1e-3) / 1e12) / tpeak,
                 "tensor_peak": tpeak, "tensor_peak_kind": tpk_kind + " (bf16, x2 for 8-bit operands)",
-                "join_share_of_step": prof["join"]["ms"] / (ms * a.steps),
-                "emit_share_of_step": prof["emit"]["ms"] / (ms * a.steps),
-                "merge_share_of_step": prof["merge"]["ms"] / (ms * a.steps)}
+                "join_share_of_step": prof["join"]["ms"] / (prof_ms * a.steps),
+                "emit_share_of_step": prof["emit"]["ms"] / (prof_ms * a.steps),
+                "merge_share_of_step": prof["merge"]["ms"] / (prof_ms * a.steps),
+                "profiled_ms_per_step": prof_ms}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
