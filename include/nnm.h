@@ -284,7 +284,10 @@ typedef struct {
  * device looks up the array's device address (cudaGetSymbolAddress) and
  * caches it; under lazy module loading that first call is also where the
  * ~16 MiB are claimed on the device, so a process with a fixed memory
- * budget should make one warm-up call at start-up.  Every call ends by
+ * budget should make one warm-up call at start-up.  That first call also
+ * zeroes the visited bitmaps (8 MiB); later calls zero only the 256-byte
+ * counters, since every query clears the bits it set, unless the previous
+ * call on the device returned before its kernel finished.  Every call ends by
  * copying its counters to the host and waiting for its stream, so no call
  * may be made while its stream is being captured into a CUDA graph.  All
  * calls share the one array: calls that overlap on the GPU race and must

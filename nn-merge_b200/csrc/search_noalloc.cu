@@ -302,6 +302,12 @@ __global__ void k_search_noalloc(NaArgs a) {
 // Device address of g_noalloc_scratch, fetched once per device.
 std::mutex g_addr_mu;
 unsigned char* g_addr[64] = {};
+// Whether a device's visited bitmaps are known to be all zero.  Every query clears
+// the bits it set before its warp takes the next one (error paths included),
+// so a call whose kernel ran to completion leaves them all zero; they are
+// cleared on the first call on a device and after a call that did not reach
+// its final synchronize.
+bool g_bits_clean[64] = {};
 
 cudaError_t scratch_address(int dev, unsigned char** out) {
     std::lock_guard<std::mutex> lk(g_addr_mu);
@@ -363,11 +369,15 @@ extern "C" int nnm_search_noalloc(const float* x_dev, uint64_t n, uint32_t d, co
     unsigned char* scratch = nullptr;
     if (scratch_address(dev, &scratch) != cudaSuccess) return NNM_ERR_CUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // clear what must start at zero: the counters and the visited bitmaps
+    // clear what must start at zero: the counters on every call, the visited
+    // bitmaps (64 slots x 128 KiB) only when an earlier call may have left bits
     if (cudaMemsetAsync(scratch, 0, NA_HEADER, st) != cudaSuccess) return NNM_ERR_CUDA;
-    const size_t words = ((size_t)layers->nrows[L - 1] + 31) / 32;
-    if (cudaMemset2DAsync(scratch + NA_HEADER, sizeof(NaSlot), 0, words * 4, NA_SLOTS, st) != cudaSuccess)
-        return NNM_ERR_CUDA;
+    if (!g_bits_clean[dev]) {
+        if (cudaMemset2DAsync(scratch + NA_HEADER, sizeof(NaSlot), 0, sizeof(uint32_t) * NA_WORDS, NA_SLOTS, st) !=
+            cudaSuccess)
+            return NNM_ERR_CUDA;
+    }
+    g_bits_clean[dev] = false;
     NaArgs a{};
     a.x = x_dev;
     a.dp = d;
@@ -396,6 +406,7 @@ extern "C" int nnm_search_noalloc(const float* x_dev, uint64_t n, uint32_t d, co
     NaHeader h;
     if (cudaMemcpyAsync(&h, scratch, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess) return NNM_ERR_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return NNM_ERR_CUDA;
+    g_bits_clean[dev] = true;  // the kernel finished: every query cleared its bits
     if (ncmps) *ncmps = h.ncmps;
     if (h.err) return NNM_ERR_CAPACITY;
     return NNM_OK;

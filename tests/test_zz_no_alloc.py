@@ -116,3 +116,39 @@ def test_noalloc_rejects_sizes_beyond_its_maximum():
     assert lib.nnm_search_noalloc(x_d.data_ptr(), x.shape[0], 4097, ctypes.byref(lay), q_d.data_ptr(),
                                   len(q), 10, seed, 0, ids.data_ptr(), None, None, None) == 1
     del keep
+
+
+def test_noalloc_after_a_failed_call():
+    """A call that the kernel's own id checks fail (adjacency ids past the
+    last layer) returns an error; the next call on well-formed layers still
+    returns exactly nnm_search's result (the visited bitmaps are cleared only
+    when a call may have left bits set, so this checks that a failed call
+    leaves none)."""
+    import torch
+    lib = bind()
+    fx = golden_lib.load("hmerge_search")
+    x, q, seed = fx["x"], fx["q"], fx["seed"]
+    ctx = nnm.Context(0)
+    try:
+        exp = ctx.search(x, fx["layers"], q, 10, seed=seed)
+    finally:
+        ctx.close()
+    x_d = torch.from_numpy(x).cuda()
+    q_d = torch.from_numpy(q).cuda()
+    good, keep = device_layers(torch, fx["layers"])
+    off, adj = fx["layers"][-1]
+    nlast = len(off) - 1
+    bad_adj = adj.astype(np.int64).copy()
+    bad_adj[::7] = nlast + 3  # every 7th neighbour out of range: the kernel skips it and records the error
+    bad, keep2 = device_layers(torch, fx["layers"][:-1] + [(off, bad_adj)])
+    ids = torch.empty((len(q), 10), dtype=torch.int32, device="cuda")
+    for lay, want_ok in ((good, True), (bad, False), (good, True), (bad, False), (bad, False), (good, True)):
+        ids.fill_(-7)
+        rc = lib.nnm_search_noalloc(x_d.data_ptr(), x.shape[0], x.shape[1], ctypes.byref(lay), q_d.data_ptr(),
+                                    len(q), 10, seed, 0, ids.data_ptr(), None, None, None)
+        if want_ok:
+            assert rc == 0, lib.nnm_status_string(rc)
+            assert np.array_equal(ids.cpu().numpy().view(np.uint32), exp["ids"])
+        else:
+            assert rc != 0
+    del keep, keep2
