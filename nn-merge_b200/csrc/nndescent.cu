@@ -1396,16 +1396,32 @@ static void launch_pairs(const JoinArgs& ja, const unsigned* ntier, uint32_t cap
         if (ntier[3]) { k_pairs<M, 3><<<ntier[3], TIER_THREADS[3], pairs_smem(TIER_CAP[3], dp, true), st>>>(ja, TIER_CAP[3]); count_launch(); }
     }
     // ntier null (the tensor-core join takes tiers 0-3): the count of the
-    // last tier is on the device only, the blocks loop over its rows
+    // last tier is on the device only, the blocks loop over its rows; the
+    // grid is every block that fits on the SMs at once
     if (!ntier || ntier[4]) {
-        unsigned g = ntier ? std::min<unsigned>(ntier[4], (unsigned)nsm * 4) : (unsigned)nsm * 4;
+        const size_t smem = u8_last ? pairs_smem_u8(caps, ja.kq) : pairs_smem(caps, dp, false);
+        int per_sm = 0;
+        if (u8_last)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs_u8, TIER_THREADS[4], smem);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs<M, 4>, TIER_THREADS[4], smem);
+        const unsigned full = (unsigned)nsm * (unsigned)std::max(per_sm, 1);
+        const unsigned g = ntier ? std::min<unsigned>(ntier[4], full) : full;
         if (u8_last) {
-            k_pairs_u8<<<g, TIER_THREADS[4], pairs_smem_u8(caps, ja.kq), st>>>(ja, caps);
+            k_pairs_u8<<<g, TIER_THREADS[4], smem, st>>>(ja, caps);
         } else {
-            k_pairs<M, 4><<<g, TIER_THREADS[4], pairs_smem(caps, dp, false), st>>>(ja, caps);
+            k_pairs<M, 4><<<g, TIER_THREADS[4], smem, st>>>(ja, caps);
         }
         count_launch();
     }
+}
+
+// Grid of k_emit_rows when the row count is on the device only: every
+// block that fits on the SMs at once.
+static unsigned emit_rows_grid(uint32_t caps, int nsm) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_emit_rows, EMIT_ROW_WARPS * 32, (size_t)caps * 24 + 64);
+    return (unsigned)nsm * (unsigned)std::max(per_sm, 1);
 }
 
 // Sequential float mean of the per-row deltas, as the reference computes it
@@ -1644,7 +1660,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             if (tc) e = launch_join_tc(1, ja, nt, nsm, st);
             if (e != cudaSuccess) return e;
             if (tc) {
-                const unsigned rows4 = nt ? nt[NTIER - 1] : (unsigned)nsm * 2;
+                const unsigned rows4 = nt ? nt[NTIER - 1] : emit_rows_grid(caps, nsm);
                 if (rows4) {
                     k_emit_rows<<<rows4, EMIT_ROW_WARPS * 32, (size_t)caps * 24 + 64, st>>>(ja); count_launch();
                 }
