@@ -642,7 +642,11 @@ def run_vmf(a, rank, world, local):
                        "dist_err_vs_fp64": {"max_rel": float(rel.max()), "mean_rel": float(rel.mean())},
                        "same_graph_as_first_tier": same,
                        "join_ms": prof["join"]["ms"], "emit_ms": prof["emit"]["ms"], "merge_ms": prof["merge"]["ms"],
-                       "proposals": int(sum(L[3] for L in prof["iters"]))}
+                       "proposals": int(sum(L[3] for L in prof["iters"])),
+                       # reduced precision: proposals carrying d~, and the share the merge recomputed exactly
+                       "approx_proposals": prof["approx"]["proposals"],
+                       "recheck_rate": (prof["approx"]["rechecks"] / prof["approx"]["proposals"]
+                                        if prof["approx"]["proposals"] else None)}
     ms = reps.max(tiers.get("tensor", next(iter(tiers.values())))["s"] * 1e3)
     if rank == 0:
         line = {"metric": VMF_METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": a.steps,

@@ -583,6 +583,7 @@ int nnm_profile_enable(nnm_ctx* ctx, int on) {
     ctx->c.join_rows_tc = 0;
     ctx->c.iter_log.clear();
     ctx->c.audit_max = ctx->c.audit_err_c = 0.f;
+    ctx->c.approx_props = ctx->c.rechecks = 0;
     return NNM_OK;
 }
 
@@ -599,8 +600,11 @@ int nnm_profile_get(const nnm_ctx* ctx, char* buf, uint64_t buflen) {
                   (unsigned long long)c.kemit.launches, c.kemit.ms, c.kemit.bytes, c.kemit.tensor_ops,
                   (unsigned long long)c.kmerge.launches, c.kmerge.ms, c.kmerge.bytes);
     js += tmp;
-    std::snprintf(tmp, sizeof tmp, "\"audit\": {\"max_rel\": %.9g, \"err_c\": %.9g}, ", (double)c.audit_max,
-                  (double)c.audit_err_c);
+    std::snprintf(tmp, sizeof tmp,
+                  "\"audit\": {\"max_rel\": %.9g, \"err_c\": %.9g}, "
+                  "\"approx\": {\"proposals\": %llu, \"rechecks\": %llu}, ",
+                  (double)c.audit_max, (double)c.audit_err_c, (unsigned long long)c.approx_props,
+                  (unsigned long long)c.rechecks);
     js += tmp;
     std::snprintf(tmp, sizeof tmp, "\"rows\": {\"tiers\": [%llu, %llu, %llu, %llu, %llu], \"tensor\": %llu}, \"iters\": [",
                   (unsigned long long)c.join_rows[0], (unsigned long long)c.join_rows[1],

@@ -103,17 +103,14 @@ struct TcShared {
 // per-slot arrays.  Two buffers.
 __host__ __device__ constexpr size_t tc_vec_bytes(uint32_t kq) { return (size_t)TC_SLOTS * kq; }
 __host__ __device__ constexpr size_t tc_buf_bytes(uint32_t kq) {
-    return (tc_vec_bytes(kq) + (size_t)TC_SLOTS * (7 * 4 + 8) + 1023) & ~(size_t)1023;
+    return (tc_vec_bytes(kq) + (size_t)TC_SLOTS * (16 + 3 * 4 + 8) + 1023) & ~(size_t)1023;
 }
 __host__ __device__ constexpr size_t tc_smem_bytes(uint32_t kq) { return 2 * tc_buf_bytes(kq) + 1024; }
 
 struct SlotBuf {
     unsigned char* vec;
-    uint32_t* ids;
-    float* kth;
-    uint32_t* nrm;
+    uint4* info;    // per slot: list entry, K-th distance (bits), norm, group -- one 16-byte read
     uint32_t* cnt;  // pass 0: counts; pass 1: bucket cursors
-    uint32_t* grp;
     uint32_t* lim;  // pass 1: the slot's reserved bucket range (its pass-0 count)
     float* scl;     // KIND_FP8: the row's inverse scale 2^-e
     unsigned long long* base;
@@ -123,12 +120,9 @@ __device__ __forceinline__ SlotBuf slot_buf(unsigned char* smem, uint32_t kq, ui
     unsigned char* p = smem + b * tc_buf_bytes(kq);
     SlotBuf s;
     s.vec = p;
-    s.ids = reinterpret_cast<uint32_t*>(p + tc_vec_bytes(kq));
-    s.kth = reinterpret_cast<float*>(s.ids + TC_SLOTS);
-    s.nrm = reinterpret_cast<uint32_t*>(s.kth + TC_SLOTS);
-    s.cnt = s.nrm + TC_SLOTS;
-    s.grp = s.cnt + TC_SLOTS;
-    s.lim = s.grp + TC_SLOTS;
+    s.info = reinterpret_cast<uint4*>(p + tc_vec_bytes(kq));
+    s.cnt = reinterpret_cast<uint32_t*>(s.info + TC_SLOTS);
+    s.lim = s.cnt + TC_SLOTS;
     s.scl = reinterpret_cast<float*>(s.lim + TC_SLOTS);
     s.base = reinterpret_cast<unsigned long long*>(s.scl + TC_SLOTS);
     return s;
@@ -222,8 +216,57 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
 
     if (warp >= 4) {
         // ---------------- producers ----------------
+        // One thread per slot.  The slot's metadata (its row, list entry,
+        // K-th distance, norm, group; pass 1: its bucket range) is a chain
+        // of dependent reads; it is fetched into registers for tile k+1
+        // while the vector copies of tile k are in flight, and stored into
+        // the buffer once that buffer is released.
         const uint32_t ptid = tid - 128;
         unsigned long long sum_s = 0;
+        struct SlotMeta {
+            uint32_t t, lgB, nrows, row, nn, S, e, nrm, grp, lim;
+            float kth, scl;
+            unsigned long long base;
+        };
+        auto fetch = [&](uint32_t tile, SlotMeta& m) {
+            uint32_t t = 0, lt = tile;
+            while (t < 3 && lt >= nt[t]) {
+                lt -= nt[t];
+                t++;
+            }
+            const uint32_t lgB = 4 + t, B = 1u << lgB, RT = 8u >> t;
+            const uint32_t first = lt * RT;
+            m.t = t;
+            m.lgB = lgB;
+            m.nrows = min(RT, rcount[t] - first);
+            m.e = NO_SLOT;
+            m.row = m.nn = m.S = 0;
+            const uint32_t r = ptid >> lgB, q = ptid & (B - 1);
+            if (r < m.nrows) {
+                const uint32_t row = rlist[(size_t)t * a.n + first + r];
+                const uint32_t nn = a.newlen[row], Sr = nn + a.oldlen[row];
+                m.row = row;
+                m.nn = nn;
+                m.S = Sr;
+                if (q < Sr) {
+                    const uint32_t e =
+                        q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
+                    const uint32_t id = e & LID_MASK;
+                    m.e = e;
+                    m.kth = a.pdist[(size_t)id * a.K + a.K - 1];
+                    m.nrm = a.nrm[id];
+                    m.scl = KIND == KIND_FP8 ? a.scl[id] : 1.f;
+                    m.grp = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
+                    if (PASS == 1) {
+                        const uint32_t c = a.cntpos[(size_t)row * a.caps + q];
+                        m.lim = c;
+                        m.base = c ? a.boff[id] + atomicAdd(&a.bcur[id], c) : 0ull;
+                    }
+                }
+            }
+        };
+        SlotMeta cur{};
+        if (blockIdx.x < total) fetch(blockIdx.x, cur);
         for (uint32_t k = 0;; k++) {
             const uint32_t tile = blockIdx.x + k * gridDim.x;
             if (tile >= total) break;
@@ -235,59 +278,43 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                     break;
                 }
             }
-            uint32_t t = 0, lt = tile;
-            while (t < 3 && lt >= nt[t]) {
-                lt -= nt[t];
-                t++;
-            }
-            const uint32_t lgB = 4 + t, B = 1u << lgB, RT = 8u >> t;
-            const uint32_t first = lt * RT, nrows = min(RT, rcount[t] - first);
             TileHdr& H = sh.hdr[b];
             const SlotBuf S = slot_buf(smem, kq, b);
+            const uint32_t B = 1u << cur.lgB, r = ptid >> cur.lgB, q = ptid & (B - 1);
             if (ptid == 0) {
-                H.t = t;
-                H.lgB = lgB;
-                H.nrows = nrows;
+                H.t = cur.t;
+                H.lgB = cur.lgB;
+                H.nrows = cur.nrows;
             }
             if (ptid < 8) H.any[ptid] = 0;
-            if (ptid < nrows) {
-                const uint32_t row = rlist[(size_t)t * a.n + first + ptid];
-                const uint32_t nn = a.newlen[row], Sr = nn + a.oldlen[row];
-                H.row[ptid] = row;
-                H.nn[ptid] = nn;
-                H.S[ptid] = Sr;
-                sum_s += Sr;
+            if (q == 0 && r < cur.nrows) {
+                H.row[r] = cur.row;
+                H.nn[r] = cur.nn;
+                H.S[r] = cur.S;
+                sum_s += cur.S;
             }
-            group_sync(BAR_PROD);
-            {  // slot metadata, ptid = slot
-                const uint32_t r = ptid >> lgB, q = ptid & (B - 1);
-                uint32_t e = NO_SLOT;
-                if (r < nrows && q < H.S[r]) {
-                    const uint32_t row = H.row[r], nn = H.nn[r];
-                    e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
-                    const uint32_t id = e & LID_MASK;
-                    S.kth[ptid] = a.pdist[(size_t)id * a.K + a.K - 1];
-                    S.nrm[ptid] = a.nrm[id];
-                    if (KIND == KIND_FP8) S.scl[ptid] = a.scl[id];
-                    S.grp[ptid] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
-                    S.cnt[ptid] = 0;
-                    if (PASS == 1) {
-                        const uint32_t c = a.cntpos[(size_t)row * a.caps + q];
-                        S.lim[ptid] = c;
-                        S.base[ptid] = c ? a.boff[id] + atomicAdd(&a.bcur[id], c) : 0ull;
-                    }
+            S.info[ptid] = cur.e != NO_SLOT ? make_uint4(cur.e, __float_as_uint(cur.kth), cur.nrm, cur.grp)
+                                            : make_uint4(NO_SLOT, 0u, 0u, 0u);
+            if (cur.e != NO_SLOT) {
+                if (KIND == KIND_FP8) S.scl[ptid] = cur.scl;
+                S.cnt[ptid] = 0;
+                if (PASS == 1) {
+                    S.lim[ptid] = cur.lim;
+                    S.base[ptid] = cur.base;
                 }
-                S.ids[ptid] = e;
             }
             group_sync(BAR_PROD);
             // gather: 16-byte chunk c of slot s -> group s/8, core matrix c, row s%8
             const uint32_t vbase = smem_u32(S.vec);
             for (uint32_t i = ptid; i < TC_SLOTS * nchunk; i += 128) {
                 const uint32_t r8 = i & 7, rest = i >> 3, c = rest % nchunk, g = rest / nchunk, sl = g * 8 + r8;
-                const uint32_t e = S.ids[sl];
+                const uint32_t e = S.info[sl].x;
                 if (e != NO_SLOT)
                     cp_async16(vbase + g * gbytes + c * 128 + r8 * 16, a.xq + (size_t)(e & LID_MASK) * kq + c * 16);
             }
+            // the next tile's metadata while these copies land
+            const uint32_t nxt = tile + gridDim.x;
+            if (nxt < total) fetch(nxt, cur);
             asm volatile("cp.async.wait_all;" ::: "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // cp.async writes -> tensor core reads
             mbar_arrive(smem_u32(&sh.full[b]));
@@ -373,13 +400,14 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             asm volatile("tcgen05.fence::after_thread_sync;");
 
             // epilogue: this thread is slot b = tid (TMEM lane tid)
-            const uint32_t e_b = S.ids[tid];
+            const uint4 info_b = S.info[tid];
+            const uint32_t e_b = info_b.x;
             const bool valid_b = e_b != NO_SLOT;
             const uint32_t r_b = tid >> lgB, q_b = tid & (B - 1);
             const uint32_t nn_b = valid_b ? H.nn[r_b] : 0u, S_b = valid_b ? H.S[r_b] : 0u;
             const uint32_t row_b = valid_b ? H.row[r_b] : 0u;
-            const float kth_b = S.kth[tid];
-            const uint32_t nrm_b = S.nrm[tid], grp_b = S.grp[tid];
+            const float kth_b = __uint_as_float(info_b.y);
+            const uint32_t nrm_b = info_b.z, grp_b = info_b.w;
             const float scl_b = KIND == KIND_FP8 ? S.scl[tid] : 1.f;
             const uint32_t lim_b = (PASS == 1 && APPROX) ? S.lim[tid] : 0u;
             bool over = false;  // pass 1, reduced precision: a write beyond a reserved range
@@ -414,14 +442,15 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                             const uint32_t av = c0 + jj;
                             const uint32_t q_a = av & (B - 1);
                             const bool pv = valid_b && (av & ~(B - 1)) == blk && q_a < q_b && q_a < nn_b;
-                            const uint32_t e_a = S.ids[av];
+                            const uint4 info_a = S.info[av];
+                            const uint32_t e_a = info_a.x;
                             float dd, lb;
                             if (KIND == KIND_U8) {
-                                dd = (float)((int)(S.nrm[av] + nrm_b) - 2 * (int)v[j8]);
+                                dd = (float)((int)(info_a.z + nrm_b) - 2 * (int)v[j8]);
                                 lb = dd;
                             } else {
                                 // d~ and its lower bound (distances are >= 0)
-                                const float ns = __uint_as_float(S.nrm[av]) + __uint_as_float(nrm_b);
+                                const float ns = __uint_as_float(info_a.z) + __uint_as_float(nrm_b);
                                 float gd = __uint_as_float(v[j8]);
                                 if (KIND == KIND_FP8) gd *= S.scl[av] * scl_b;
                                 dd = fmaxf(ns - 2.f * gd, 0.f);
@@ -434,9 +463,9 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                             }
                             const uint32_t axb = APPROX ? APPROX_BIT : 0u;
                             uint32_t outer = 0, inner = 0;
-                            const bool ok = pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, S.grp[av],
+                            const bool ok = pv && pair_order(a.mode, a.verse, q_a, q_b, nn_b, e_a, e_b, info_a.w,
                                                              grp_b, outer, inner);
-                            const float kth_a = S.kth[av];
+                            const float kth_a = __uint_as_float(info_a.y);
                             if (PASS == 0) {
                                 cmps += ok;
                                 cb += (ok && lb < kth_b);

@@ -749,6 +749,7 @@ struct MergeArgs {
     uint32_t dp;
     const uint32_t* nrm;
     float err_c;
+    uint32_t count_approx;  // count the approximate proposals and their exact rechecks (profiling)
 };
 
 // Proposal number i of the bucket array: distance bits and list entry (and,
@@ -1046,6 +1047,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
                                             reinterpret_cast<unsigned long long*>(&sm[w][0]));
             }
             uint32_t nb = 0;  // entries in buf
+            uint32_t nrc = 0, nax = 0;  // rechecks, approximate proposals (count_approx)
             auto flush = [&]() {
                 uint32_t pd = 0xffffffffu, pe = 0;
                 unsigned long long pk = ~0ull;
@@ -1057,6 +1059,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
                     if (APPROX && bufax[w][lane])
                         pd = __float_as_uint(merge_exact_l2(a.x, a.dp, t, pe & ID_MASK));
                 }
+                if (APPROX && a.count_approx) nrc += __popc(__ballot_sync(FULL, lane < (int)nb && bufax[w][lane]));
                 __syncwarp();
                 warp_sort_ment(pd, pk, pe);
                 merge_round(pd, pk, pe, nb, K, cd, ce, ck, sm[w], kept[w]);
@@ -1091,6 +1094,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
                             valid = mless(pd, pk, kd, kk);
                         }
                     }
+                    if (APPROX && a.count_approx) nax += __popc(__ballot_sync(FULL, ax));
                     const unsigned vb = __ballot_sync(FULL, valid);
                     if (!vb) continue;
                     const uint32_t take = min((uint32_t)__popc(vb), 32u - nb);
@@ -1119,6 +1123,10 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
             if (lane < (int)K) {
                 a.pid[(size_t)t * K + lane] = ce;
                 a.pdist[(size_t)t * K + lane] = __uint_as_float(cd);
+            }
+            if (APPROX && a.count_approx && lane == 0 && nax) {
+                atomicAdd(&a.ctr->approx_props, (unsigned long long)nax);
+                atomicAdd(&a.ctr->rechecks, (unsigned long long)nrc);
             }
             nfl = __popc(__ballot_sync(FULL, lane < (int)K && (ce & FLAG_BIT)));
         }
@@ -1194,6 +1202,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a)
             bound = approx_bound<true>(a, b_first, c, K, (uint32_t)(pool >> 32), (uint32_t)(pool >> 2), nt, stage[w]);
         }
         uint32_t nb = 0;
+        uint32_t nrc = 0, nax = 0;  // rechecks, approximate proposals (count_approx)
         for (uint32_t b0 = 0;; b0 += 32) {
             unsigned long long v = FM_EMPTY;
             bool rest = false, ax = false;
@@ -1215,6 +1224,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a)
                         valid = v < kth;
                     }
                 }
+                if (APPROX && a.count_approx) nax += __popc(__ballot_sync(FULL, ax));
                 const unsigned vb = __ballot_sync(FULL, valid);
                 if (!vb) continue;
                 const uint32_t take = min((uint32_t)__popc(vb), 32u - nb);
@@ -1235,6 +1245,7 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a)
                     bv = ((unsigned long long)__float_as_uint(merge_exact_l2(a.x, a.dp, t, (uint32_t)(bv >> 2) & ID_MASK))
                           << 32) | (uint32_t)bv;
             }
+            if (APPROX && a.count_approx) nrc += __popc(__ballot_sync(FULL, lane < (int)nb && bufax[w][lane]));
             __syncwarp();
             pool = fm_flush(pool, bv, K, stage[w]);
             kth = __shfl_sync(FULL, pool, K - 1);
@@ -1253,6 +1264,10 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a)
         if (lane < (int)K) {
             a.pid[(size_t)t * K + lane] = fm_pool_word(pool);
             a.pdist[(size_t)t * K + lane] = __uint_as_float((uint32_t)(pool >> 32));
+        }
+        if (APPROX && a.count_approx && lane == 0 && nax) {
+            atomicAdd(&a.ctr->approx_props, (unsigned long long)nax);
+            atomicAdd(&a.ctr->rechecks, (unsigned long long)nrc);
         }
         nfl = __popc(__ballot_sync(FULL, lane < (int)K && (pool & 2ull)));
     }
@@ -1668,7 +1683,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                 k_emit<<<(n + EMIT_WARPS - 1) / EMIT_WARPS, EMIT_WARPS * 32, emit_smem, st>>>(ja); count_launch();
             }
             MergeArgs ma{g.pid, g.pdist, n, K, P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff),
-                         ja.bucket, P<uint8_t>(ws.nflag), ctr, g.x, g.dp, g.nrm, g.err_c};
+                         ja.bucket, P<uint8_t>(ws.nflag), ctr, g.x, g.dp, g.nrm, g.err_c, ctx.prof ? 1u : 0u};
             rec(3);
             const unsigned mgrid = (n + MERGE_WARPS - 1) / MERGE_WARPS;
             if (g.fast) {
@@ -1870,7 +1885,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             // 2-byte count per list slot; the FP32 path also writes one
             // distance per pair.  The emit pass gathers the same members
             // again on the tensor cores (or reads the stored distances) and
-            // writes every proposal (16 B).
+            // writes every proposal (16 B in the exact tier, 8 B in the fast tier).
             for (int t = 0; t < NTIER; t++) ctx.join_rows[t] += hc.ntier[t];
             if (ctx.iter_log.size() < 4096) {
                 Ctx::IterLog L{n, {hc.ntier[0], hc.ntier[1], hc.ntier[2], hc.ntier[3], hc.ntier[4]},
@@ -1904,6 +1919,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                 ctx.kjoin.tensor_ops += t0n * per_tile;
                 ctx.kemit.tensor_ops += t1n * per_tile;
             }
+            ctx.approx_props += hc.approx_props;
+            ctx.rechecks += hc.rechecks;
             ctx.kmerge.launches += 1;
             ctx.kmerge.ms += t34;
             ctx.kmerge.bytes += (double)n * K * 16.0 + (double)hc.proposals * (double)prop_bytes + (double)n * 13.0;

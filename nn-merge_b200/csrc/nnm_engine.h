@@ -92,6 +92,9 @@ struct Ctx {
     // audit of the reduced-precision joins (while profiling): the largest
     // |d~ - d| / (|a|^2 + |b|^2) seen and the bound coefficient it is held to
     float audit_max = 0.f, audit_err_c = 0.f;
+    // reduced-precision joins (while profiling): proposals carrying d~, and
+    // those the merge computed exactly
+    uint64_t approx_props = 0, rechecks = 0;
     cudaEvent_t ev[8] = {};
     // executable whole-iteration graphs of the fast tier, one per join mode,
     // refreshed by cudaGraphExecUpdate at each NN-Descent call

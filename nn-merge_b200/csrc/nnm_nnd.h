@@ -65,6 +65,10 @@ struct IterCounters {
     unsigned int pad2;
     unsigned long long sum_s_tc;   // the part of sum_s joined on the tensor cores
     unsigned int nemit[4];         // rows of tiers 0-3 with at least one proposal (tensor-core emit pass)
+    // reduced-precision joins, counted while profiling: proposals that carry
+    // d~, and those of them whose exact distance the merge computed
+    unsigned long long approx_props;
+    unsigned long long rechecks;
 };
 
 // IterCounters::overflow bits (the whole-iteration graph sizes its buffers
