@@ -171,8 +171,10 @@ __device__ __forceinline__ bool group_any(uint32_t id, bool p) {
 // Both passes then run the same tiles (all joined rows, not only those with
 // proposals), so every pair's d~ comes from the same MMA position and the
 // two passes decide alike; pass 1 still writes no proposal beyond the range
-// pass 0 reserved, and records DERR_TC_WAIT if a slot's count differs.
-template <int PASS, int KIND, bool FAST>
+// pass 0 reserved, and records DERR_TC_RANGE if a slot's count differs.
+// AUDIT (pass 0 of the reduced-precision kinds): every pair's d~ is also
+// checked against its exact distance.
+template <int PASS, int KIND, bool FAST, bool AUDIT = false>
 __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ TcShared sh;
@@ -455,7 +457,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                                 if (KIND == KIND_FP8) gd *= S.scl[av] * scl_b;
                                 dd = fmaxf(ns - 2.f * gd, 0.f);
                                 lb = dd - a.err_c * ns;
-                                if (PASS == 0 && a.audit && pv) {  // the bound against the exact distance
+                                if (PASS == 0 && AUDIT && pv) {  // the bound against the exact distance
                                     const float ex = audit_l2(a.x, a.dp, e_a & LID_MASK, e_b & LID_MASK);
                                     if (!(ex >= lb && ex <= dd + a.err_c * ns)) atomicOr(a.tc_err, (unsigned)DERR_BOUND);
                                     if (ns > 0.f) atomicMax(&a.ctr->audit_max, __float_as_uint(fabsf(ex - dd) / ns));
@@ -820,41 +822,50 @@ int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
 cudaError_t tc_set_attributes(uint32_t kq, uint32_t kind) {
     const int bytes = (int)std::max<size_t>(tc_smem_bytes(kq), TC_SMEM_FLOOR);
     cudaError_t e;
-    const void* fns[3][3] = {{(const void*)k_join_tc<0, KIND_U8, false>, (const void*)k_join_tc<1, KIND_U8, false>,
-                              (const void*)k_join_tc<1, KIND_U8, true>},
+    const void* fns[3][4] = {{(const void*)k_join_tc<0, KIND_U8, false>, (const void*)k_join_tc<1, KIND_U8, false>,
+                              (const void*)k_join_tc<1, KIND_U8, true>, (const void*)k_join_tc<0, KIND_U8, false>},
                              {(const void*)k_join_tc<0, KIND_BF16, false>, (const void*)k_join_tc<1, KIND_BF16, false>,
-                              (const void*)k_join_tc<1, KIND_BF16, true>},
+                              (const void*)k_join_tc<1, KIND_BF16, true>, (const void*)k_join_tc<0, KIND_BF16, false, true>},
                              {(const void*)k_join_tc<0, KIND_FP8, false>, (const void*)k_join_tc<1, KIND_FP8, false>,
-                              (const void*)k_join_tc<1, KIND_FP8, true>}};
+                              (const void*)k_join_tc<1, KIND_FP8, true>, (const void*)k_join_tc<0, KIND_FP8, false, true>}};
     for (const void* f : fns[kind < 3 ? kind : 0])
         if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
+// One launch of a join variant: a persistent grid of the CTAs that fit on
+// the SMs at once (four per SM when the tile buffers allow, fewer for wide
+// operand rows), or fewer when the host knows the tile count.
+template <int PASS, int KIND, bool FAST, bool AUDIT = false>
+static void launch_tc(const JoinArgs& ja, unsigned tiles, int nsm, size_t bytes, cudaStream_t st) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_join_tc<PASS, KIND, FAST, AUDIT>, TC_THREADS, bytes);
+    const unsigned grid = std::min<unsigned>(tiles, (unsigned)nsm * (unsigned)std::max(per_sm, 1));
+    k_join_tc<PASS, KIND, FAST, AUDIT><<<grid, TC_THREADS, bytes, st>>>(ja);
+}
+
+template <int KIND>
+static void launch_tc_kind(int pass, const JoinArgs& ja, unsigned tiles, int nsm, size_t bytes, cudaStream_t st) {
+    // the audit (reduced-precision kinds) in its own count-pass variant, so
+    // that the unaudited one holds no code of it
+    if (pass == 0 && KIND != KIND_U8 && ja.audit) launch_tc<0, KIND, false, KIND != KIND_U8>(ja, tiles, nsm, bytes, st);
+    else if (pass == 0) launch_tc<0, KIND, false>(ja, tiles, nsm, bytes, st);
+    else if (ja.fast_key) launch_tc<1, KIND, true>(ja, tiles, nsm, bytes, st);
+    else launch_tc<1, KIND, false>(ja, tiles, nsm, bytes, st);
+}
+
 cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, int nsm, cudaStream_t st) {
-    // ntier null: the counts are on the device only -- every SM's four CTAs
-    unsigned grid = (unsigned)nsm * 4;
+    // ntier null: the counts are on the device only -- the full grid
+    unsigned tiles = ~0u;
     if (ntier) {
-        unsigned tiles = 0;
+        tiles = 0;
         for (int t = 0; t < 4; t++) tiles += (ntier[t] + (8u >> t) - 1) >> (3 - t);
         if (!tiles) return cudaSuccess;
-        grid = std::min<unsigned>(tiles, grid);
     }
     const size_t bytes = std::max<size_t>(tc_smem_bytes(ja.kq), TC_SMEM_FLOOR);
-    const bool fast = ja.fast_key != 0;
-    if (ja.tc_kind == KIND_U8) {
-        if (pass == 0) k_join_tc<0, KIND_U8, false><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else if (fast) k_join_tc<1, KIND_U8, true><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else k_join_tc<1, KIND_U8, false><<<grid, TC_THREADS, bytes, st>>>(ja);
-    } else if (ja.tc_kind == KIND_BF16) {
-        if (pass == 0) k_join_tc<0, KIND_BF16, false><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else if (fast) k_join_tc<1, KIND_BF16, true><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else k_join_tc<1, KIND_BF16, false><<<grid, TC_THREADS, bytes, st>>>(ja);
-    } else {
-        if (pass == 0) k_join_tc<0, KIND_FP8, false><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else if (fast) k_join_tc<1, KIND_FP8, true><<<grid, TC_THREADS, bytes, st>>>(ja);
-        else k_join_tc<1, KIND_FP8, false><<<grid, TC_THREADS, bytes, st>>>(ja);
-    }
+    if (ja.tc_kind == KIND_U8) launch_tc_kind<KIND_U8>(pass, ja, tiles, nsm, bytes, st);
+    else if (ja.tc_kind == KIND_BF16) launch_tc_kind<KIND_BF16>(pass, ja, tiles, nsm, bytes, st);
+    else launch_tc_kind<KIND_FP8>(pass, ja, tiles, nsm, bytes, st);
     count_launch();
     return cudaGetLastError();
 }

@@ -1037,6 +1037,10 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
             }
             uint32_t kd = __shfl_sync(FULL, cd, K - 1);
             unsigned long long kk = __shfl_sync(FULL, ck, K - 1);
+            // the K-th distance the join filtered against: an approximate
+            // proposal whose exact distance is not below it is one the FP32
+            // join would not have made (a tie at the K-th distance)
+            const uint32_t kd0 = kd;
             const unsigned long long b_first = a.boff[t];
             const unsigned lt = (1u << lane) - 1u;
             float nt = 0.f;
@@ -1056,8 +1060,14 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge(MergeArgs a) {
                     pd = me.d;
                     pe = me.e;
                     pk = me.k;
-                    if (APPROX && bufax[w][lane])
+                    if (APPROX && bufax[w][lane]) {
                         pd = __float_as_uint(merge_exact_l2(a.x, a.dp, t, pe & ID_MASK));
+                        if (pd >= kd0) {
+                            pd = 0xffffffffu;
+                            pe = 0;
+                            pk = ~0ull;
+                        }
+                    }
                 }
                 if (APPROX && a.count_approx) nrc += __popc(__ballot_sync(FULL, lane < (int)nb && bufax[w][lane]));
                 __syncwarp();
@@ -1192,6 +1202,8 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a)
         const unsigned long long pprev = __shfl_up_sync(FULL, pool, 1);
         if (!__all_sync(FULL, lane == 0 || pprev <= pool)) pool = fm_sort32(pool);
         unsigned long long kth = __shfl_sync(FULL, pool, K - 1);
+        // the K-th distance the join filtered against (as in k_merge)
+        const uint32_t kd0 = (uint32_t)(kth >> 32);
         const unsigned long long b_first = a.boff[t];
         const uint2* bp = reinterpret_cast<const uint2*>(a.bucket) + b_first;
         const unsigned lt = (1u << lane) - 1u;
@@ -1241,9 +1253,10 @@ __global__ void __launch_bounds__(MERGE_WARPS * 32, 8) k_merge_fast(MergeArgs a)
             unsigned long long bv = FM_EMPTY;
             if (lane < (int)nb) {
                 bv = buf[w][lane];
-                if (APPROX && bufax[w][lane])  // the exact distance replaces d~
-                    bv = ((unsigned long long)__float_as_uint(merge_exact_l2(a.x, a.dp, t, (uint32_t)(bv >> 2) & ID_MASK))
-                          << 32) | (uint32_t)bv;
+                if (APPROX && bufax[w][lane]) {  // the exact distance replaces d~
+                    const uint32_t ex = __float_as_uint(merge_exact_l2(a.x, a.dp, t, (uint32_t)(bv >> 2) & ID_MASK));
+                    bv = ex < kd0 ? ((unsigned long long)ex << 32) | (uint32_t)bv : FM_EMPTY;
+                }
             }
             if (APPROX && a.count_approx) nrc += __popc(__ballot_sync(FULL, lane < (int)nb && bufax[w][lane]));
             __syncwarp();
