@@ -87,7 +87,8 @@ __device__ __noinline__ float audit_l2(const float* x, uint32_t dp, uint32_t i, 
 
 // Tile header of one buffer, written by the producers, read by the consumers.
 struct TileHdr {
-    uint32_t t, lgB, nrows, pad;
+    uint32_t t, lgB, nrows, done;  // done: no more tiles (the consumers stop)
+    uint32_t next;                 // the tile the producers load after this one
     uint32_t row[8], nn[8], S[8], any[8];
 };
 
@@ -267,11 +268,14 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                 }
             }
         };
+        // Tiles: a CTA's first is its block index, every later one is
+        // claimed from the launch's counter (tiles differ in cost; the CTAs
+        // that finish early take more).  After the last tile the producers
+        // hand the consumers a buffer marked done.
         SlotMeta cur{};
-        if (blockIdx.x < total) fetch(blockIdx.x, cur);
+        uint32_t tile = blockIdx.x;
+        if (tile < total) fetch(tile, cur);
         for (uint32_t k = 0;; k++) {
-            const uint32_t tile = blockIdx.x + k * gridDim.x;
-            if (tile >= total) break;
             const uint32_t b = k & 1, use = k >> 1;
             if (use > 0) {
                 const bool ok = mbar_wait_bounded(smem_u32(&sh.empty[b]), (use - 1) & 1);
@@ -281,6 +285,15 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                 }
             }
             TileHdr& H = sh.hdr[b];
+            if (tile >= total) {
+                if (ptid == 0) H.done = 1;
+                mbar_arrive(smem_u32(&sh.full[b]));  // the arrive releases the header write
+                break;
+            }
+            if (ptid == 0) {
+                H.done = 0;
+                H.next = gridDim.x + atomicAdd(&a.ctr->tc_next[PASS], 1u);
+            }
             const SlotBuf S = slot_buf(smem, kq, b);
             const uint32_t B = 1u << cur.lgB, r = ptid >> cur.lgB, q = ptid & (B - 1);
             if (ptid == 0) {
@@ -315,11 +328,12 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                     cp_async16(vbase + g * gbytes + c * 128 + r8 * 16, a.xq + (size_t)(e & LID_MASK) * kq + c * 16);
             }
             // the next tile's metadata while these copies land
-            const uint32_t nxt = tile + gridDim.x;
+            const uint32_t nxt = H.next;
             if (nxt < total) fetch(nxt, cur);
             asm volatile("cp.async.wait_all;" ::: "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // cp.async writes -> tensor core reads
             mbar_arrive(smem_u32(&sh.full[b]));
+            tile = nxt;
         }
         if (PASS == 0) {
             for (int o = 16; o > 0; o >>= 1) sum_s += __shfl_xor_sync(0xffffffffu, sum_s, o);
@@ -332,8 +346,6 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
         // ---------------- consumers ----------------
         uint32_t cmps = 0;
         for (uint32_t k = 0;; k++) {
-            const uint32_t tile = blockIdx.x + k * gridDim.x;
-            if (tile >= total) break;
             const uint32_t b = k & 1, use = k >> 1;
             const bool okf = mbar_wait_bounded(smem_u32(&sh.full[b]), use & 1);
             if (group_any(BAR_CONS, !okf)) {
@@ -341,6 +353,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                 break;
             }
             const TileHdr& H = sh.hdr[b];
+            if (H.done) break;
             const SlotBuf S = slot_buf(smem, kq, b);
             const uint32_t t = H.t, lgB = H.lgB, nrows = H.nrows, B = 1u << lgB;
             if (tid == 0) {
@@ -833,14 +846,27 @@ cudaError_t tc_set_attributes(uint32_t kq, uint32_t kind) {
     return cudaSuccess;
 }
 
-// One launch of a join variant: a persistent grid of the CTAs that fit on
-// the SMs at once (four per SM when the tile buffers allow, fewer for wide
-// operand rows), or fewer when the host knows the tile count.
+// One launch of a join variant: a persistent grid of the CTAs that are
+// resident on the SMs at once, or fewer when the host knows the tile count.
+// Residency is at most four CTAs per SM (TMEM: 512 columns, 128 a CTA; the
+// registers of __launch_bounds__ allow four), fewer when the tile buffers of
+// wide operand rows fill the shared memory (two for BF16 rows of d = 96).
+// It is counted here from the shared-memory sizes: the occupancy query
+// knows nothing of TMEM and reported half these counts, and a grid sized
+// larger than the residency leaves a second wave of persistent CTAs whose
+// tiles all run last.
+constexpr int TC_TMEM_CTAS = 512 / TC_COLS;
 template <int PASS, int KIND, bool FAST, bool AUDIT = false>
 static void launch_tc(const JoinArgs& ja, unsigned tiles, int nsm, size_t bytes, cudaStream_t st) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_join_tc<PASS, KIND, FAST, AUDIT>, TC_THREADS, bytes);
-    const unsigned grid = std::min<unsigned>(tiles, (unsigned)nsm * (unsigned)std::max(per_sm, 1));
+    int dev = 0, smem_sm = 0, reserved = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k_join_tc<PASS, KIND, FAST, AUDIT>);
+    const int per_sm_smem = (int)((size_t)smem_sm / (bytes + fa.sharedSizeBytes + (size_t)reserved));
+    const int per_sm = std::min(std::max(per_sm_smem, 1), TC_TMEM_CTAS);
+    const unsigned grid = std::min<unsigned>(tiles, (unsigned)nsm * (unsigned)per_sm);
     k_join_tc<PASS, KIND, FAST, AUDIT><<<grid, TC_THREADS, bytes, st>>>(ja);
 }
 

@@ -69,6 +69,7 @@ struct IterCounters {
     // d~, and those of them whose exact distance the merge computed
     unsigned long long approx_props;
     unsigned long long rechecks;
+    unsigned int tc_next[2];       // tiles claimed by the tensor-core join's CTAs, per pass
 };
 
 // IterCounters::overflow bits (the whole-iteration graph sizes its buffers

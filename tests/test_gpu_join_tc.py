@@ -171,12 +171,19 @@ def test_reduced_precision_merges_match_fp32(ctx, kern):
 
 
 @pytest.mark.parametrize("kern", ["tensor", "fp8"])
-def test_reduced_precision_ties_and_scales(ctx, kern):
-    # many exact ties (few distinct values) and mixed magnitudes
+@pytest.mark.parametrize("rng_tier", ["exact", "fast"])
+def test_reduced_precision_ties_and_scales(ctx, kern, rng_tier):
+    """Many exact ties (few distinct values) and mixed magnitudes.  In the
+    fast tier a proposal at exactly the K-th distance and of a smaller id
+    would displace the K-th entry; the FP32 join never proposes it (its
+    filter is strict), so neither may the reduced-precision join's merge."""
     rng = np.random.default_rng(62)
     x = (rng.integers(-3, 4, size=(4000, 40)) * 0.25).astype(np.float32)
     x[::7] *= 1e3
-    t, f, _ = both(ctx, ctx.kgraph, x, 12, seed=7, tjoin=kern)
+    t, f, _ = both(ctx, ctx.kgraph, x, 12, seed=7, rng=rng_tier, tjoin=kern)
+    same(t, f)
+    y = (rng.integers(0, 3, size=(6000, 24)) * 0.5).astype(np.float32)  # every distance a multiple of 0.25
+    t, f, _ = both(ctx, ctx.merge_leaves, y, 16, [1500] * 4, seed=8, rng=rng_tier, tjoin=kern)
     same(t, f)
 
 
