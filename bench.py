@@ -139,9 +139,10 @@ def tensor_peak():
 # (1,000,000 x 128, four leaves, the untuned sample cap), as a ratio to the
 # library's algorithmic bytes of the same launches; the bench reports that
 # ratio times the live run's algorithmic bytes per launch.  Keyed by (kernel
-# class, tensor join).  emit: k_join_tc<1> + k_emit_rows, 54.24 GB measured
-# per build against 49.03 GB algorithmic.
-NCU_TRAFFIC_RATIO = {("emit", True): 1.106}
+# class, tensor join).  Per build, measured against algorithmic: join
+# (k_join_tc<0> + k_pairs_u8) 29.21 / 41.33 GB, emit (k_join_tc<1> +
+# k_emit_rows) 49.93 / 49.03 GB, merge (k_merge_fast) 9.68 / 11.00 GB.
+NCU_TRAFFIC_RATIO = {("join", True): 0.707, ("emit", True): 1.018, ("merge", True): 0.880}
 
 
 def traffic_per_launch(kind, stat, a):
@@ -887,7 +888,11 @@ def main():
                 "join_share_of_step": prof["join"]["ms"] / (prof_ms * a.steps),
                 "emit_share_of_step": prof["emit"]["ms"] / (prof_ms * a.steps),
                 "merge_share_of_step": prof["merge"]["ms"] / (prof_ms * a.steps),
-                "profiled_ms_per_step": prof_ms}
+                "profiled_ms_per_step": prof_ms,
+                # per class and step: launches, device ms, algorithmic bytes (the ncu
+                # traffic ratios are measured against these)
+                "classes": {c: {"launches": prof[c]["launches"] / a.steps, "ms": prof[c]["ms"] / a.steps,
+                                "bytes": prof[c]["bytes"] / a.steps} for c in ("join", "emit", "merge")}}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

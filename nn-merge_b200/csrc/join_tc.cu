@@ -425,6 +425,9 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             const uint32_t nrm_b = info_b.z, grp_b = info_b.w;
             const float scl_b = KIND == KIND_FP8 ? S.scl[tid] : 1.f;
             const uint32_t lim_b = (PASS == 1 && APPROX) ? S.lim[tid] : 0u;
+            // this slot's bucket range start, read once (the proposal stores
+            // are generic and would make the compiler reload it)
+            const unsigned long long base_b = PASS == 1 ? S.base[tid] : 0ull;
             bool over = false;  // pass 1, reduced precision: a write beyond a reserved range
             const uint32_t blk = tid & ~(B - 1);
             uint32_t cb = 0;
@@ -520,7 +523,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                                 }
                                 if (ok && lb < kth_b) {
                                     const uint32_t pos = wl ? cnt_r++ : atomicAdd(&S.cnt[tid], 1u);
-                                    const unsigned long long slot = S.base[tid] + pos;
+                                    const unsigned long long slot = base_b + pos;
                                     if (!APPROX || pos < lim_b)
                                         put_prop<FAST>(a.bucket, slot, dd, e_a | axb, row_b, pidx, outer == q_b ? 0u : 1u);
                                     else
