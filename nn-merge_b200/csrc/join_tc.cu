@@ -50,7 +50,12 @@
 namespace nnm {
 namespace {
 
-constexpr int TC_THREADS = 256;                // consumers (warps 0-3) + producers (warps 4-7)
+// Consumer threads per CTA: the emit pass runs two warps per TMEM lane
+// quarter (warps 0-7), the count pass one (warps 0-3); the producers are
+// the next four warps, one thread per tile slot.
+constexpr int TC_PROD = 128;
+__host__ __device__ constexpr int tc_cons(int pass) { return pass == 1 ? 256 : 128; }
+__host__ __device__ constexpr int tc_threads(int pass) { return tc_cons(pass) + TC_PROD; }
 constexpr uint32_t TC_SLOTS = 128;             // M = N = 128: one TMEM lane and one column per slot
 constexpr uint32_t TC_COLS = 128;              // TMEM columns held by a CTA
 constexpr uint32_t TC_SMEM_FLOOR = 50 * 1024;  // keeps residency at <= 4 CTAs per SM (4 x 128 columns)
@@ -129,36 +134,41 @@ __device__ __forceinline__ SlotBuf slot_buf(unsigned char* smem, uint32_t kq, ui
     return s;
 }
 
-// Barriers of one 128-thread group (producers: 1, consumers: 2).
+// Barriers of one thread group (producers: 1, consumers: 2).
 constexpr uint32_t BAR_PROD = 1, BAR_CONS = 2;
 
-__device__ __forceinline__ void group_sync(uint32_t id) {
-    asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory");
+__device__ __forceinline__ void group_sync(uint32_t id, uint32_t nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
 // Barrier of the group that also ORs a predicate over its 128 threads, so
 // that a decision taken after per-thread bounded waits is the same in every
 // thread of the group.
-__device__ __forceinline__ bool group_any(uint32_t id, bool p) {
+__device__ __forceinline__ bool group_any(uint32_t id, bool p, uint32_t nthreads) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}\n"
         : "=r"(r)
-        : "r"((uint32_t)p), "r"(id)
+        : "r"((uint32_t)p), "r"(id), "r"(nthreads)
         : "memory");
     return r != 0;
 }
 
-// Persistent CTAs of 256 threads in two groups over two tile buffers:
-//   producers (warps 4-7): for tile k, wait until buffer k%2 is released,
+// Persistent CTAs in two groups over two tile buffers:
+//   producers (the last four warps): for tile k, wait until buffer k%2 is released,
 //     write its header and slot metadata, gather the slot vectors with
 //     cp.async, then arrive on full[k%2];
-//   consumers (warps 0-3, TMEM lanes 0-127): wait for full[k%2], run the
-//     MMA chain (thread 0) and the epilogue, write the counts, then arrive on
-//     empty[k%2].
+//   consumers (warps 0-3; in the emit pass warps 0-7, warps w and w + 4
+//     reading TMEM lanes 32 (w % 4) .. + 31 and sharing their columns in
+//     8-column blocks): wait for full[k%2], run the MMA chain (thread 0) and
+//     the epilogue, write the counts, then arrive on empty[k%2].
+// The emit pass takes two warps per lane quarter because its epilogue is
+// latency-bound (under one eligible warp per scheduler with one): 9 % off
+// the pass, at three CTAs per SM instead of four (registers); the count
+// pass, with less to do per pair, measured 6 % slower that way.
 // So the loads of tile k+1 overlap the MMA and epilogue of tile k.  Every
 // mbarrier wait is bounded; a group decides to stop with a barrier-OR over
 // its threads, and the other group then times out on its next wait.
@@ -176,9 +186,10 @@ __device__ __forceinline__ bool group_any(uint32_t id, bool p) {
 // AUDIT (pass 0 of the reduced-precision kinds): every pair's d~ is also
 // checked against its exact distance.
 template <int PASS, int KIND, bool FAST, bool AUDIT = false>
-__global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
+__global__ void __launch_bounds__(tc_threads(PASS), PASS == 0 ? 4 : KIND == KIND_U8 ? 3 : 2) k_join_tc(JoinArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ TcShared sh;
+    constexpr uint32_t CONS = tc_cons(PASS), HALVES = CONS / 128;
     if (a.ctr->overflow) return;  // a buffer sized ahead was too small: the host reruns
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t kq = a.kq, nchunk = kq >> 4, gbytes = nchunk * 128;
@@ -187,8 +198,8 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mma_bar));
         for (int b = 0; b < 2; b++) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(smem_u32(&sh.full[b])));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(smem_u32(&sh.empty[b])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&sh.full[b])), "r"(TC_PROD));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&sh.empty[b])), "r"(CONS));
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -217,14 +228,14 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
     bool failed = false, mma_pending = false;
     uint32_t mma_phase = 0;
 
-    if (warp >= 4) {
+    if (warp >= CONS / 32) {
         // ---------------- producers ----------------
         // One thread per slot.  The slot's metadata (its row, list entry,
         // K-th distance, norm, group; pass 1: its bucket range) is a chain
         // of dependent reads; it is fetched into registers for tile k+1
         // while the vector copies of tile k are in flight, and stored into
         // the buffer once that buffer is released.
-        const uint32_t ptid = tid - 128;
+        const uint32_t ptid = tid - CONS;
         unsigned long long sum_s = 0;
         struct SlotMeta {
             uint32_t t, lgB, nrows, row, nn, S, e, nrm, grp, lim;
@@ -279,7 +290,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             const uint32_t b = k & 1, use = k >> 1;
             if (use > 0) {
                 const bool ok = mbar_wait_bounded(smem_u32(&sh.empty[b]), (use - 1) & 1);
-                if (group_any(BAR_PROD, !ok)) {
+                if (group_any(BAR_PROD, !ok, TC_PROD)) {
                     failed = true;
                     break;
                 }
@@ -318,7 +329,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                     S.base[ptid] = cur.base;
                 }
             }
-            group_sync(BAR_PROD);
+            group_sync(BAR_PROD, TC_PROD);
             // gather: 16-byte chunk c of slot s -> group s/8, core matrix c, row s%8
             const uint32_t vbase = smem_u32(S.vec);
             for (uint32_t i = ptid; i < TC_SLOTS * nchunk; i += 128) {
@@ -348,7 +359,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
         for (uint32_t k = 0;; k++) {
             const uint32_t b = k & 1, use = k >> 1;
             const bool okf = mbar_wait_bounded(smem_u32(&sh.full[b]), use & 1);
-            if (group_any(BAR_CONS, !okf)) {
+            if (group_any(BAR_CONS, !okf, CONS)) {
                 failed = true;
                 break;
             }
@@ -406,7 +417,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                              : "memory");
             }
             const bool okm = mbar_wait_bounded(mma_bar, mma_phase);
-            if (group_any(BAR_CONS, !okm)) {
+            if (group_any(BAR_CONS, !okm, CONS)) {
                 failed = true;
                 mma_pending = true;
                 break;
@@ -414,36 +425,42 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             mma_phase ^= 1u;
             asm volatile("tcgen05.fence::after_thread_sync;");
 
-            // epilogue: this thread is slot b = tid (TMEM lane tid)
-            const uint4 info_b = S.info[tid];
+            // epilogue: this thread is slot b = tid % 128 (TMEM lane b); warps
+            // w and w + 4 (half 0 and 1) read the same lanes and take
+            // alternate 8-column blocks
+            const uint32_t slot = tid & (TC_SLOTS - 1), quarter = warp & 3, half = warp >> 2;
+            const uint4 info_b = S.info[slot];
             const uint32_t e_b = info_b.x;
             const bool valid_b = e_b != NO_SLOT;
-            const uint32_t r_b = tid >> lgB, q_b = tid & (B - 1);
+            const uint32_t r_b = slot >> lgB, q_b = slot & (B - 1);
             const uint32_t nn_b = valid_b ? H.nn[r_b] : 0u, S_b = valid_b ? H.S[r_b] : 0u;
             const uint32_t row_b = valid_b ? H.row[r_b] : 0u;
             const float kth_b = __uint_as_float(info_b.y);
             const uint32_t nrm_b = info_b.z, grp_b = info_b.w;
-            const float scl_b = KIND == KIND_FP8 ? S.scl[tid] : 1.f;
-            const uint32_t lim_b = (PASS == 1 && APPROX) ? S.lim[tid] : 0u;
+            const float scl_b = KIND == KIND_FP8 ? S.scl[slot] : 1.f;
+            const uint32_t lim_b = PASS == 1 ? S.lim[slot] : 0u;
             // this slot's bucket range start, read once (the proposal stores
             // are generic and would make the compiler reload it)
-            const unsigned long long base_b = PASS == 1 ? S.base[tid] : 0ull;
+            const unsigned long long base_b = PASS == 1 ? S.base[slot] : 0ull;
             bool over = false;  // pass 1, reduced precision: a write beyond a reserved range
-            const uint32_t blk = tid & ~(B - 1);
+            const uint32_t blk = slot & ~(B - 1);
             uint32_t cb = 0;
-            // Rows of at most 32 slots lie inside one warp, so every proposal
-            // to slot s of such a tile comes from the warp holding s: its
-            // counter lives in a register of lane s % 32 (read by shuffle)
-            // instead of shared memory (an atomic round trip per pair).
+            // Rows of at most 32 slots lie inside one lane quarter, so every
+            // proposal to slot s of such a tile comes from the two warps
+            // holding s: each keeps its counter in a register of lane s % 32
+            // (read by shuffle) instead of shared memory (an atomic round trip
+            // per pair).  In the emit pass half 0 fills the slot's reserved
+            // range from its start, half 1 from its end.
             const bool wl_tile = lgB <= 5;
             uint32_t cnt_r = 0;
-            const uint32_t c_first = B >= 32 ? ((warp * 32) & ~(B - 1)) : warp * 32;
+            const uint32_t c_first = B >= 32 ? ((quarter * 32) & ~(B - 1)) : quarter * 32;
             // the loop specialised for the tile's counter kind, so that the
             // one running holds no code of the other (the emit pass is
             // bound by instruction fetch)
             auto pairs = [&](auto wl_kind) {
                 constexpr bool wl = decltype(wl_kind)::value;
-                for (uint32_t c0 = c_first; c0 <= warp * 32; c0 += 32) {
+                uint32_t blocks = 0;  // 8-column blocks of this lane quarter so far
+                for (uint32_t c0 = c_first; c0 <= quarter * 32; c0 += 32) {
                     // columns a of a pair are new-list entries: a < blk + nn_b; the
                     // bound is made warp-uniform (lanes of different rows take the max)
                     const int lim = valid_b ? (int)(blk + nn_b) - (int)c0 : 0;
@@ -451,8 +468,12 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                     if (jend == 0) continue;
                     // 8 columns per TMEM load: no spills at 64 registers, a short unrolled body
                     for (uint32_t h = 0; h < jend; h += 8) {
+                        // blocks 0, 3, 4, 7, ... to half 0 and 1, 2, 5, 6, ... to
+                        // half 1: early columns hold more pairs (a < b)
+                        const uint32_t bi = blocks++;
+                        if (HALVES == 2 && ((bi + (bi >> 1)) & 1u) != half) continue;
                         uint32_t v[8];
-                        tmem_ld8(tmem + ((warp * 32) << 16) + c0 + h, v);
+                        tmem_ld8(tmem + ((quarter * 32) << 16) + c0 + h, v);
 #pragma unroll
                         for (uint32_t j8 = 0; j8 < 8; j8++) {
                             const uint32_t jj = h + j8;
@@ -505,6 +526,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                                         // takes no b-side proposal in this step
                                         base = __shfl_sync(0xffffffffu, cnt_r, av & 31);
                                         if (lane == (av & 31)) cnt_r += __popc(m);
+                                        if (half) base = S.lim[av] - base - __popc(m);  // from the range's end
                                     } else {
                                         const uint32_t leader = __ffs(m) - 1;
                                         base = 0;
@@ -513,19 +535,20 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
                                     }
                                     if (pa) {
                                         const uint32_t before = __popc(m & ((1u << lane) - 1u));
-                                        const unsigned long long slot = S.base[av] + base + before;
+                                        const unsigned long long at = S.base[av] + base + before;
                                         if (!APPROX || base + before < S.lim[av])
-                                            put_prop<FAST>(a.bucket, slot, dd, e_b | axb, row_b, pidx,
+                                            put_prop<FAST>(a.bucket, at, dd, e_b | axb, row_b, pidx,
                                                            outer == q_a ? 0u : 1u);
                                         else
                                             over = true;
                                     }
                                 }
                                 if (ok && lb < kth_b) {
-                                    const uint32_t pos = wl ? cnt_r++ : atomicAdd(&S.cnt[tid], 1u);
-                                    const unsigned long long slot = base_b + pos;
+                                    const uint32_t pos =
+                                        wl ? (half ? lim_b - 1u - cnt_r++ : cnt_r++) : atomicAdd(&S.cnt[slot], 1u);
+                                    const unsigned long long at = base_b + pos;
                                     if (!APPROX || pos < lim_b)
-                                        put_prop<FAST>(a.bucket, slot, dd, e_a | axb, row_b, pidx, outer == q_b ? 0u : 1u);
+                                        put_prop<FAST>(a.bucket, at, dd, e_a | axb, row_b, pidx, outer == q_b ? 0u : 1u);
                                     else
                                         over = true;
                                 }
@@ -537,27 +560,25 @@ __global__ void __launch_bounds__(TC_THREADS, 4) k_join_tc(JoinArgs a) {
             if (wl_tile) pairs(std::true_type{});
             else pairs(std::false_type{});
             if (PASS == 0) {
-                if (wl_tile)
-                    S.cnt[tid] = cnt_r + cb;
-                else if (cb)
-                    atomicAdd(&S.cnt[tid], cb);
+                if (wl_tile ? (cnt_r + cb) != 0 : cb != 0) atomicAdd(&S.cnt[slot], wl_tile ? cnt_r + cb : cb);
             }
+            if (PASS == 1 && APPROX && wl_tile && cnt_r) atomicAdd(&S.cnt[slot], cnt_r);
+            if (PASS == 1 && APPROX && over) atomicOr(a.tc_err, (unsigned)DERR_TC_RANGE);
             asm volatile("tcgen05.fence::before_thread_sync;");
-            group_sync(BAR_CONS);
-            if (PASS == 1 && APPROX) {  // every reserved range filled exactly
-                const uint32_t got = wl_tile ? cnt_r : S.cnt[tid];
-                if (over || (valid_b && got != lim_b)) atomicOr(a.tc_err, (unsigned)DERR_TC_RANGE);
+            group_sync(BAR_CONS, CONS);
+            if (PASS == 1 && APPROX && half == 0) {  // every reserved range filled exactly
+                if (valid_b && S.cnt[slot] != lim_b) atomicOr(a.tc_err, (unsigned)DERR_TC_RANGE);
             }
             if (PASS == 0) {
-                if (valid_b) {
-                    const uint32_t c = S.cnt[tid];
+                if (half == 0 && valid_b) {
+                    const uint32_t c = S.cnt[slot];
                     a.cntpos[(size_t)row_b * a.caps + q_b] = (uint16_t)c;
                     if (c) {
                         atomicAdd(&a.bcnt[e_b & LID_MASK], c);
                         sh.hdr[b].any[r_b] = 1;
                     }
                 }
-                group_sync(BAR_CONS);
+                group_sync(BAR_CONS, CONS);
                 if (warp == 0) {  // rows with proposals go to the emit pass's list
                     const bool has = lane < nrows && H.any[lane];
                     const unsigned m = __ballot_sync(0xffffffffu, has);
@@ -851,13 +872,13 @@ cudaError_t tc_set_attributes(uint32_t kq, uint32_t kind) {
 
 // One launch of a join variant: a persistent grid of the CTAs that are
 // resident on the SMs at once, or fewer when the host knows the tile count.
-// Residency is at most four CTAs per SM (TMEM: 512 columns, 128 a CTA; the
-// registers of __launch_bounds__ allow four), fewer when the tile buffers of
-// wide operand rows fill the shared memory (two for BF16 rows of d = 96).
-// It is counted here from the shared-memory sizes: the occupancy query
-// knows nothing of TMEM and reported half these counts, and a grid sized
-// larger than the residency leaves a second wave of persistent CTAs whose
-// tiles all run last.
+// Residency is at most four CTAs per SM (TMEM: 512 columns, 128 a CTA),
+// three for the u8 emit pass by registers (384 threads of 56), fewer when the
+// tile buffers of wide operand rows fill the shared memory (two for BF16
+// rows of d = 96).  It is counted here from the registers and shared-memory
+// sizes: the occupancy query knows nothing of TMEM and reported half these
+// counts, and a grid sized larger than the residency leaves a second wave of
+// persistent CTAs whose tiles run last.
 constexpr int TC_TMEM_CTAS = 512 / TC_COLS;
 template <int PASS, int KIND, bool FAST, bool AUDIT = false>
 static void launch_tc(const JoinArgs& ja, unsigned tiles, int nsm, size_t bytes, cudaStream_t st) {
@@ -868,9 +889,12 @@ static void launch_tc(const JoinArgs& ja, unsigned tiles, int nsm, size_t bytes,
     cudaFuncAttributes fa{};
     cudaFuncGetAttributes(&fa, k_join_tc<PASS, KIND, FAST, AUDIT>);
     const int per_sm_smem = (int)((size_t)smem_sm / (bytes + fa.sharedSizeBytes + (size_t)reserved));
-    const int per_sm = std::min(std::max(per_sm_smem, 1), TC_TMEM_CTAS);
+    int regs_sm = 65536;
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    const int per_sm_regs = regs_sm / (((fa.numRegs + 7) & ~7) * tc_threads(PASS));
+    const int per_sm = std::min(std::max(std::min(per_sm_smem, per_sm_regs), 1), TC_TMEM_CTAS);
     const unsigned grid = std::min<unsigned>(tiles, (unsigned)nsm * (unsigned)per_sm);
-    k_join_tc<PASS, KIND, FAST, AUDIT><<<grid, TC_THREADS, bytes, st>>>(ja);
+    k_join_tc<PASS, KIND, FAST, AUDIT><<<grid, tc_threads(PASS), bytes, st>>>(ja);
 }
 
 template <int KIND>
