@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(tc_threads(PASS), PASS == 0 ? 4 : KIND == KIND
                         q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
                     const uint32_t id = e & LID_MASK;
                     m.e = e;
-                    m.kth = a.pdist[(size_t)id * a.K + a.K - 1];
+                    m.kth = a.kthv[id];
                     m.nrm = a.nrm[id];
                     m.scl = KIND == KIND_FP8 ? a.scl[id] : 1.f;
                     m.grp = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);

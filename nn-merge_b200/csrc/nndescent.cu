@@ -58,7 +58,16 @@ struct SampleArgs {
     const uint32_t *rnewT, *roldT, *rnewTlen, *roldTlen;  // carried reverse lists (or null)
     uint32_t smpl;
     IterCounters* ctr;
+    const float* kth;  // every row's K-th distance (k_kth_gather)
 };
+
+// Every row's K-th distance, gathered once per iteration: the sampling and
+// the join read it for random rows, and the 4-byte array stays in L2 where
+// the pools' last entries (a sector per row) do not.
+__global__ void k_kth_gather(const float* pdist, uint32_t K, uint32_t n, float* kth) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) kth[t] = pdist[(size_t)t * K + K - 1];
+}
 
 __global__ void k_sample_count(SampleArgs a) {
     uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -68,7 +77,7 @@ __global__ void k_sample_count(SampleArgs a) {
     uint32_t e = a.pid[o];
     float d = a.pdist[o];
     uint32_t id = e & ID_MASK;
-    float kth = a.pdist[(size_t)id * a.K + a.K - 1];
+    float kth = a.kth[id];
     if (kth < d) atomicAdd((e & FLAG_BIT) ? &a.rcnt_new[id] : &a.rcnt_old[id], 1u);
 }
 
@@ -95,7 +104,7 @@ __global__ void k_sample_fill(SampleArgs a) {
         unsigned lt = (1u << lane) - 1u;
         if (isnew) a.newL[(size_t)row * a.capn + base_n + __popc(bal & lt)] = entry;
         else a.oldL[(size_t)row * a.capo + base_o + __popc(~bal & actmask & lt)] = entry;
-        float kth = a.pdist[(size_t)id * a.K + a.K - 1];
+        float kth = a.kth[id];
         if (kth < d) {
             uint32_t rg = (a.mode == MODE_KGRAPH) ? 0u : (row >= a.split ? 1u : 0u);
             uint32_t v = row | (rg << 31);
@@ -267,16 +276,23 @@ __device__ __forceinline__ void shuffle_seg(uint32_t* seg, uint32_t len, const i
 // the ids, not on their order.  The keep-th smallest hash is found by an
 // 8-bit radix select (4 rounds over a 256-bin histogram), ties on it by the
 // smallest ids.  Warp-wide; hist is this warp's 256-entry shared scratch.
+// hc (len entries of shared memory, or null): the hashes, computed once --
+// a Philox draw is 10 rounds, and the select reads every hash five times.
 __device__ void hash_sample(uint32_t* seg, uint32_t len, uint32_t keep, const Philox& ph, uint32_t t,
-                            uint32_t phase, uint32_t l, uint32_t* hist) {
+                            uint32_t phase, uint32_t l, uint32_t* hist, uint32_t* hc) {
     const int lane = threadIdx.x & 31;
     uint32_t prefix = 0, need = keep;
+    if (hc) {
+        for (uint32_t j = lane; j < len; j += 32) hc[j] = ph(t, phase, l, seg[j] & LID_MASK).x;
+        __syncwarp();
+    }
+    auto hash = [&](uint32_t j) { return hc ? hc[j] : ph(t, phase, l, seg[j] & LID_MASK).x; };
     for (int byte = 3; byte >= 0; byte--) {
         for (uint32_t i = lane; i < 256; i += 32) hist[i] = 0;
         __syncwarp();
         const uint32_t hi_mask = byte == 3 ? 0u : (0xffffffffu << (8 * (byte + 1)));
         for (uint32_t j = lane; j < len; j += 32) {
-            const uint32_t h = ph(t, phase, l, seg[j] & LID_MASK).x;
+            const uint32_t h = hash(j);
             if ((h & hi_mask) == prefix) atomicAdd(&hist[(h >> (8 * byte)) & 255u], 1u);
         }
         __syncwarp();
@@ -320,7 +336,7 @@ __device__ void hash_sample(uint32_t* seg, uint32_t len, uint32_t keep, const Ph
         uint32_t mn = 0xffffffffu;
         for (uint32_t j = lane; j < len; j += 32) {
             const uint32_t id = seg[j] & LID_MASK;
-            if ((r == 0 || id > idT) && id < mn && ph(t, phase, l, id).x == T) mn = id;
+            if ((r == 0 || id > idT) && id < mn && hash(j) == T) mn = id;
         }
         idT = __reduce_min_sync(FULL, mn);
     }
@@ -331,7 +347,7 @@ __device__ void hash_sample(uint32_t* seg, uint32_t len, uint32_t keep, const Ph
         bool sel = false;
         if (j < len) {
             v = seg[j];
-            const uint32_t id = v & LID_MASK, h = ph(t, phase, l, id).x;
+            const uint32_t id = v & LID_MASK, h = hash(j);
             sel = h < T || (h == T && id <= idT);
         }
         __syncwarp();
@@ -394,7 +410,7 @@ __global__ void k_shuffle_append(ShufArgs a) {
             // a uniform random subset of smplNum entries, chosen by id
             if (len > a.smpl)
                 hash_sample(seg, len, keep, Philox{a.seed, 0x6e6e6d01u}, t, a.phase_dev ? *a.phase_dev : a.phase,
-                            (uint32_t)l, hist[w]);
+                            (uint32_t)l, hist[w], staged ? stage[w] : nullptr);
             __syncwarp();
             sh = seg;
         } else if (staged) {
@@ -481,7 +497,7 @@ __device__ void pairs_row(const JoinArgs& a, uint32_t row, unsigned char* smem, 
         uint32_t e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
         uint32_t id = e & LID_MASK;
         s_ids[q] = e;
-        s_kth[q] = a.pdist[(size_t)id * a.K + a.K - 1];
+        s_kth[q] = a.kthv[id];
         s_cnt[q] = 0;
         s_grp[q] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
         if (VEC == VEC_U8) s_nrm[q] = a.nrm[id];
@@ -649,7 +665,7 @@ __device__ __forceinline__ bool emit_load_row(const JoinArgs& a, uint32_t row, u
         uint32_t e = q < nn ? a.newL[(size_t)row * a.capn + q] : a.oldL[(size_t)row * a.capo + q - nn];
         uint32_t id = e & LID_MASK;
         m.ids[q] = e;
-        m.kth[q] = a.pdist[(size_t)id * a.K + a.K - 1];
+        m.kth[q] = a.kthv[id];
         m.cur[q] = 0;
         m.grp[q] = a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e >> 31);
         uint32_t c = a.cntpos[(size_t)row * a.caps + q];
@@ -1486,6 +1502,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     NNM_CUDA_TRY(ws.boff.ensure(n1 * 8));
     NNM_CUDA_TRY(ws.bigrev.ensure(n1 * 2 * 4));
     NNM_CUDA_TRY(ws.nflag.ensure(n1));
+    NNM_CUDA_TRY(ws.kth.ensure(n1 * 4));
     NNM_CUDA_TRY(ws.scan_tmp.ensure((scan_temp_elems(n1) + 8) * 8));
     NNM_CUDA_TRY(ws.counters.ensure(sizeof(IterCounters) + 64));
     const size_t prop_bytes = g.fast ? sizeof(Prop8) : sizeof(Prop);  // the tier's proposal format
@@ -1613,7 +1630,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                           g.capn, g.capo,
                           carry_now ? g.rnewT : nullptr, carry_now ? g.roldT : nullptr,
                           carry_now ? g.rnewTlen : nullptr, carry_now ? g.roldTlen : nullptr,
-                          g.smpl, ctr};
+                          g.smpl, ctr, P<float>(ws.kth)};
+            k_kth_gather<<<tblocks, 256, 0, st>>>(g.pdist, K, n, P<float>(ws.kth)); count_launch();
             k_sample_count<<<warp_blocks, 256, 0, st>>>(sa); count_launch();
             chk(exclusive_scan(rcnt_new, roff_new, n, scan_tmp, nullptr, st));
             chk(exclusive_scan(rcnt_old, roff_old, n, scan_tmp, nullptr, st));
@@ -1660,7 +1678,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                             P<float>(ws.pd), P<uint16_t>(ws.cntpos), P<uint32_t>(ws.bcnt), P<uint32_t>(ws.bcur),
                             P<uint64_t>(ws.boff), ws.bucket.p, ctr,
                             g.xq, g.nrm, g.kq, tc ? 1u : 0u, &ctr->error, tc ? P<uint32_t>(ws.erows) : nullptr,
-                            g.fast ? 1u : 0u, g.tc_kind, g.err_c, g.scl, g.audit ? 1u : 0u};
+                            g.fast ? 1u : 0u, g.tc_kind, g.err_c, g.scl, g.audit ? 1u : 0u, P<float>(ws.kth)};
         };
         // local join, pass 1: per-target proposal counts (and, on the FP32
         // path, the stored pair distances), then the bucket offsets.  nt:

@@ -40,11 +40,12 @@ struct Workspace {
     DevBuf rcnt, rcur, rtot, roff, rseg, rscr, rcount, rofs, rbuf;
     DevBuf cntpos, bcnt, bcur, boff, bucket, bigrev, nflag, scan_tmp;
     DevBuf npairs, poff, pd, tiers, erows;
+    DevBuf kth;  // every row's K-th distance, gathered per iteration
     DevBuf draws, counters, misc;
     void release_all() {
         DevBuf* all[] = {&rcnt, &rcur, &rtot, &roff, &rseg, &rscr, &rcount, &rofs, &rbuf, &cntpos, &bcnt, &bcur,
-                         &boff, &bucket, &bigrev, &nflag, &scan_tmp, &npairs, &poff, &pd, &tiers, &erows, &draws,
-                         &counters, &misc};
+                         &boff, &bucket, &bigrev, &nflag, &scan_tmp, &npairs, &poff, &pd, &tiers, &erows, &kth,
+                         &draws, &counters, &misc};
         for (auto* b : all) b->release();
     }
 };

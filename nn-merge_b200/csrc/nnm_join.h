@@ -50,6 +50,7 @@ struct JoinArgs {
     float err_c;          // reduced precision: |d~ - reference distance| <= err_c * (|a|^2 + |b|^2)
     const float* scl;     // FP8: per-row inverse scales
     uint32_t audit;       // reduced precision: check every pair's d~ against its exact distance
+    const float* kthv;    // every row's K-th distance at the iteration's start (compact copy of pdist's)
 };
 
 // Tie-break key of the exact tier's proposal "target gets the other entry"
