@@ -104,10 +104,13 @@ struct TcShared {
     TileHdr hdr[2];
 };
 
-// Shared memory of one tile buffer: the slot vectors (128 x kq bytes,
-// canonical K-major layout: 8-slot groups of kq/16 core matrices), then the
-// per-slot arrays.  Two buffers.
-__host__ __device__ constexpr size_t tc_vec_bytes(uint32_t kq) { return (size_t)TC_SLOTS * kq; }
+// Shared memory of one tile buffer: the slot vectors in the 128-byte swizzle
+// K-major layout -- per 128-byte column of the operand row (kq rounded up
+// to 128), 128 slot rows of 128 bytes (16 KB, 8-row atoms of 1024 bytes) --
+// then the per-slot arrays.  Two buffers.
+constexpr uint32_t TC_COL_BYTES = TC_SLOTS * 128;  // one 128-byte column of every slot
+__host__ __device__ constexpr uint32_t tc_cols(uint32_t kq) { return (kq + 127) / 128; }
+__host__ __device__ constexpr size_t tc_vec_bytes(uint32_t kq) { return (size_t)tc_cols(kq) * TC_COL_BYTES; }
 __host__ __device__ constexpr size_t tc_buf_bytes(uint32_t kq) {
     return (tc_vec_bytes(kq) + (size_t)TC_SLOTS * (16 + 3 * 4 + 8) + 1023) & ~(size_t)1023;
 }
@@ -192,7 +195,7 @@ __global__ void __launch_bounds__(tc_threads(PASS), PASS == 0 ? 4 : KIND == KIND
     constexpr uint32_t CONS = tc_cons(PASS), HALVES = CONS / 128;
     if (a.ctr->overflow) return;  // a buffer sized ahead was too small: the host reruns
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t kq = a.kq, nchunk = kq >> 4, gbytes = nchunk * 128;
+    const uint32_t kq = a.kq, nchunk = kq >> 4;
     const uint32_t mma_bar = smem_u32(&sh.mma_bar);
 
     if (tid == 0) {
@@ -330,13 +333,16 @@ __global__ void __launch_bounds__(tc_threads(PASS), PASS == 0 ? 4 : KIND == KIND
                 }
             }
             group_sync(BAR_PROD, TC_PROD);
-            // gather: 16-byte chunk c of slot s -> group s/8, core matrix c, row s%8
+            // gather: 16-byte chunk c of slot s -> column c / 8, row s, chunk
+            // (c % 8) ^ (s % 8) (the 128-byte swizzle); a row's chunks by
+            // consecutive threads
             const uint32_t vbase = smem_u32(S.vec);
             for (uint32_t i = ptid; i < TC_SLOTS * nchunk; i += 128) {
-                const uint32_t r8 = i & 7, rest = i >> 3, c = rest % nchunk, g = rest / nchunk, sl = g * 8 + r8;
+                const uint32_t sl = i / nchunk, c = i - sl * nchunk;
                 const uint32_t e = S.info[sl].x;
                 if (e != NO_SLOT)
-                    cp_async16(vbase + g * gbytes + c * 128 + r8 * 16, a.xq + (size_t)(e & LID_MASK) * kq + c * 16);
+                    cp_async16(vbase + (c >> 3) * TC_COL_BYTES + sl * 128 + (((c & 7) ^ (sl & 7)) << 4),
+                               a.xq + (size_t)(e & LID_MASK) * kq + c * 16);
             }
             // the next tile's metadata while these copies land
             const uint32_t nxt = H.next;
@@ -375,7 +381,8 @@ __global__ void __launch_bounds__(tc_threads(PASS), PASS == 0 ? 4 : KIND == KIND
                 const uint32_t nparts = KIND == KIND_U8 ? 1u : KIND == KIND_BF16 ? 2u : 3u;
                 const uint32_t cpp = nchunk / nparts;
                 auto desc_of = [&](uint32_t part, uint32_t kk) {
-                    return smem_desc(vbase + (part * cpp + 2 * kk) * 128, 128, gbytes);
+                    const uint32_t koff = (part * cpp + 2 * kk) * 16;  // bytes into the operand row
+                    return smem_desc_sw128(vbase + (koff >> 7) * TC_COL_BYTES + (koff & 127));
                 };
                 for (uint32_t kk = 0; kk < cpp / 2; kk++) {
                     if (KIND == KIND_U8) {

@@ -27,6 +27,18 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
            ((uint64_t)((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
 }
 
+// Shared-memory matrix descriptor of a K-major operand in the 128-byte
+// swizzle layout (the one TMA writes with CU_TENSOR_MAP_SWIZZLE_128B): rows
+// of 128 bytes, 8-row atoms of 1024 bytes (SBO), the 16-byte chunk j of row
+// r stored at chunk j ^ (r % 8); LBO is unused for it (1); layout type 2 at
+// bits 61-63.  `addr` may point into a row (a K offset of a multiple of 32
+// bytes within the 128): the swizzle is applied to the absolute address, so
+// the atoms must be 1024-byte aligned.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3fffu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
+}
+
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
