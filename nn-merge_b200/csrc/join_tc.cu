@@ -614,32 +614,58 @@ __global__ void __launch_bounds__(tc_threads(PASS), PASS == 0 ? 4 : KIND == KIND
 
 // Warp per vector: checks that every component is an integer in [0, 255],
 // writes the u8 copy (zero padded to kq bytes) and the squared norm, and
-// tracks the largest norm.
-__global__ void k_quantize(const float* x, uint32_t n, uint32_t d, uint32_t dp, uint32_t kq, uint8_t* xq,
-                           uint32_t* nrm, unsigned* bad, unsigned* maxnrm) {
-    const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const uint32_t lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const float* src = x + (size_t)row * dp;
-    uint8_t* dst = xq + (size_t)row * kq;
-    uint32_t s = 0;
-    bool ok = true;
-    for (uint32_t k = lane; k < kq; k += 32) {
-        uint32_t u = 0;
-        if (k < d) {
-            const float v = src[k];
-            if (v >= 0.f && v <= 255.f && v == truncf(v)) u = (uint32_t)v;
-            else ok = false;
+// tracks the largest norm.  Four components per lane and step (rows are
+// dp floats, dp a multiple of 4; kq a multiple of 32).  Warps stride over
+// the rows; the largest norm and the check go to global memory once per
+// block (an atomic per row on one word serialised the kernel).
+__global__ void __launch_bounds__(256) k_quantize(const float* x, uint32_t n, uint32_t d, uint32_t dp, uint32_t kq,
+                                                  uint8_t* xq, uint32_t* nrm, unsigned* bad, unsigned* maxnrm) {
+    __shared__ unsigned bmax, bbad;
+    const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    if (threadIdx.x == 0) bmax = bbad = 0;
+    __syncthreads();
+    unsigned wmax = 0;
+    bool wok = true;
+    for (uint32_t row = blockIdx.x * wpb + (threadIdx.x >> 5); row < n; row += gridDim.x * wpb) {
+        const float* src = x + (size_t)row * dp;
+        uint8_t* dst = xq + (size_t)row * kq;
+        uint32_t s = 0;
+        bool ok = true;
+        for (uint32_t k = lane * 4; k < kq; k += 128) {
+            float v[4] = {0.f, 0.f, 0.f, 0.f};
+            if (k < dp) {
+                const float4 f = *reinterpret_cast<const float4*>(src + k);
+                v[0] = f.x;
+                v[1] = f.y;
+                v[2] = f.z;
+                v[3] = f.w;
+            }
+            uint32_t packed = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < 4; j++) {
+                uint32_t u = 0;
+                if (k + j < d) {
+                    if (v[j] >= 0.f && v[j] <= 255.f && v[j] == truncf(v[j])) u = (uint32_t)v[j];
+                    else ok = false;
+                }
+                packed |= u << (8 * j);
+                s += u * u;
+            }
+            *reinterpret_cast<uint32_t*>(dst + k) = packed;
         }
-        dst[k] = (uint8_t)u;
-        s += u * u;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        wok = wok && __all_sync(0xffffffffu, ok);
+        if (lane == 0) nrm[row] = s;
+        wmax = max(wmax, s);
     }
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    const bool all_ok = __all_sync(0xffffffffu, ok);
     if (lane == 0) {
-        nrm[row] = s;
-        if (!all_ok) atomicOr(bad, 1u);
-        atomicMax(maxnrm, s);
+        atomicMax(&bmax, wmax);
+        if (!wok) bbad = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (bbad) atomicOr(bad, 1u);
+        if (bmax) atomicMax(maxnrm, bmax);
     }
 }
 
@@ -789,7 +815,10 @@ int tc_prepare(Ctx& ctx, GraphStore& s, GraphDev& g) {
         if (g.join_kernel != NNM_JOIN_FP8) {
             NNM_CUDA_TRY(s.xq.ensure((size_t)g.n_cap * kq));
             NNM_CUDA_TRY(cudaMemsetAsync(m.p, 0, 16, ctx.stream));
-            k_quantize<<<(g.n_cap + 7) / 8, 256, 0, ctx.stream>>>(g.x, g.n_cap, g.d, g.dp, kq, s.xq.as<uint8_t>(),
+            int nsm = 148;
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx.device);
+            k_quantize<<<std::min<uint32_t>((g.n_cap + 7) / 8, (uint32_t)nsm * 8), 256, 0, ctx.stream>>>(
+                g.x, g.n_cap, g.d, g.dp, kq, s.xq.as<uint8_t>(),
                                                                   s.nrm.as<uint32_t>(), flags, flags + 1); count_launch();
             NNM_CUDA_TRY(cudaMemcpyAsync(h, flags, 8, cudaMemcpyDeviceToHost, ctx.stream));
             NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));

@@ -240,7 +240,6 @@ struct ShufArgs {
     uint32_t capn, capo, n, smpl;
     uint32_t *rnewT, *roldT, *rnewTlen, *roldTlen;
     uint32_t* npairs;     // pair-distance slots per row
-    uint32_t* tier_rows;  // NTIER lists of n rows: joined rows binned by list size
     IterCounters* ctr;
     uint32_t fast, seed, phase;  // fast tier: Philox sample instead of std::random_shuffle
     uint32_t tc_max_s;    // rows with S up to this go to the tensor-core join (no stored pairs)
@@ -248,6 +247,7 @@ struct ShufArgs {
     uint32_t *rscr_new, *rscr_old;  // scratch of the reverse lists' sizes (fast tier: duplicate removal)
     uint32_t dedupe;      // fast tier, first iteration of an H-Merge level: carried + new lists may repeat ids
     const uint32_t* phase_dev;  // non-null: the draw phase is read here (an iteration graph's replays)
+    uint8_t* rtier;       // each row's join tier (0xff: no new entries, not joined); k_tier_lists bins them
 };
 
 __global__ void k_rand_count(const uint64_t* roff_new, const uint64_t* roff_old, uint32_t n, uint32_t* out) {
@@ -398,9 +398,40 @@ __global__ void k_shuffle_append(ShufArgs a) {
     if (t >= a.n) return;
     const int32_t* draws = a.fast ? nullptr : a.rbuf + a.rofs[t];
     uint32_t nl = a.newlen[t], ol = a.oldlen[t];
+    // both lists' segments read up front (independent loads in flight together)
+    const uint64_t lo_n = a.roff_new[t], hi_n = a.roff_new[t + 1], lo_o = a.roff_old[t], hi_o = a.roff_old[t + 1];
+    // Fast tier, the common row: both reverse lists of at most 32 entries
+    // and within the sample cap -- kept whole, in list order -- copied with
+    // one load of each list, in flight together.
+    if (a.fast && !a.dedupe && hi_n - lo_n <= min(32u, a.smpl) && hi_o - lo_o <= min(32u, a.smpl)) {
+        const uint32_t ln = (uint32_t)(hi_n - lo_n), lk = (uint32_t)(hi_o - lo_o);
+        const uint32_t vn = lane < (int)ln ? a.rseg_new[lo_n + lane] : 0u;
+        const uint32_t vo = lane < (int)lk ? a.rseg_old[lo_o + lane] : 0u;
+        if (nl + ln > a.capn || ol + lk > a.capo) {
+            if (lane == 0) {
+                atomicOr(&a.ctr->error, (unsigned)DERR_LIST_CAP);
+                a.rtier[t] = 0xff;
+            }
+            return;
+        }
+        if (lane < (int)ln) {
+            a.newL[(size_t)t * a.capn + nl + lane] = vn;
+            if (a.rnewT) a.rnewT[(size_t)t * a.smpl + lane] = vn;
+        }
+        if (lane < (int)lk) {
+            a.oldL[(size_t)t * a.capo + ol + lane] = vo;
+            if (a.roldT) a.roldT[(size_t)t * a.smpl + lane] = vo;
+        }
+        if (lane == 0 && a.rnewT) {
+            a.rnewTlen[t] = ln;
+            a.roldTlen[t] = lk;
+        }
+        nl += ln;
+        ol += lk;
+    } else
     for (int l = 0; l < 2; l++) {
-        uint64_t lo = l ? a.roff_old[t] : a.roff_new[t];
-        uint32_t len = (uint32_t)((l ? a.roff_old[t + 1] : a.roff_new[t + 1]) - lo);
+        uint64_t lo = l ? lo_o : lo_n;
+        uint32_t len = (uint32_t)((l ? hi_o : hi_n) - lo);
         uint32_t* seg = (l ? a.rseg_old : a.rseg_new) + lo;
         if (a.dedupe && len > 1) len = dedupe_ids(seg, len, (l ? a.rscr_old : a.rscr_new) + lo);
         uint32_t keep = min(len, a.smpl);
@@ -429,7 +460,10 @@ __global__ void k_shuffle_append(ShufArgs a) {
         uint32_t cap = l ? a.capo : a.capn;
         uint32_t* T = l ? a.roldT : a.rnewT;
         if (base + keep > cap) {
-            if (lane == 0) atomicOr(&a.ctr->error, (unsigned)DERR_LIST_CAP);
+            if (lane == 0) {
+                atomicOr(&a.ctr->error, (unsigned)DERR_LIST_CAP);
+                a.rtier[t] = 0xff;
+            }
             return;
         }
         for (uint32_t j = lane; j < keep; j += 32) {
@@ -448,13 +482,42 @@ __global__ void k_shuffle_append(ShufArgs a) {
         // stored pairs of the local join: new x new above the diagonal, new x old
         const uint32_t S = nl + ol;
         a.npairs[t] = nl && S > a.tc_max_s ? nl * (nl - 1) / 2 + nl * ol : 0u;
+        int tier = 0xff;
         if (nl) {
-            int tier = tier_of(S);
+            tier = tier_of(S);
             // next to the tensor-core join (tc_max_s != 0) longer lists take the
             // pair kernel; without it, tiers whose staged vectors do not fit
             if (tier < NTIER - 1 && S > a.tc_max_s && (a.tc_max_s != 0 || tier > a.max_staged)) tier = NTIER - 1;
-            a.tier_rows[(size_t)tier * a.n + atomicAdd(&a.ctr->ntier[tier], 1u)] = t;
         }
+        a.rtier[t] = (uint8_t)tier;
+    }
+}
+
+// The tier lists from the rows' tiers: a block per chunk of rows counts its
+// rows per tier in shared memory, reserves each tier's range with one
+// global atomic, then places its rows.  (An atomic per row on the five tier
+// counters serialised the shuffle kernel.)  The order within a tier is free:
+// the joins and the merge do not depend on it.
+constexpr uint32_t TIER_CHUNK = 2048;
+__global__ void __launch_bounds__(256) k_tier_lists(const uint8_t* rtier, uint32_t n, uint32_t* tier_rows,
+                                                    IterCounters* ctr) {
+    __shared__ uint32_t cnt[NTIER], base[NTIER];
+    const uint32_t c0 = blockIdx.x * TIER_CHUNK, c1 = min(n, c0 + TIER_CHUNK);
+    if (threadIdx.x < NTIER) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t r = c0 + threadIdx.x; r < c1; r += blockDim.x) {
+        const uint32_t t = rtier[r];
+        if (t < NTIER) atomicAdd(&cnt[t], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < NTIER) {
+        base[threadIdx.x] = cnt[threadIdx.x] ? atomicAdd(&ctr->ntier[threadIdx.x], cnt[threadIdx.x]) : 0u;
+        cnt[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    for (uint32_t r = c0 + threadIdx.x; r < c1; r += blockDim.x) {
+        const uint32_t t = rtier[r];
+        if (t < NTIER) tier_rows[(size_t)t * n + base[t] + atomicAdd(&cnt[t], 1u)] = r;
     }
 }
 
@@ -1503,6 +1566,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     NNM_CUDA_TRY(ws.bigrev.ensure(n1 * 2 * 4));
     NNM_CUDA_TRY(ws.nflag.ensure(n1));
     NNM_CUDA_TRY(ws.kth.ensure(n1 * 4));
+    NNM_CUDA_TRY(ws.rtier.ensure(n1));
     NNM_CUDA_TRY(ws.scan_tmp.ensure((scan_temp_elems(n1) + 8) * 8));
     NNM_CUDA_TRY(ws.counters.ensure(sizeof(IterCounters) + 64));
     const size_t prop_bytes = g.fast ? sizeof(Prop8) : sizeof(Prop);  // the tier's proposal format
@@ -1601,9 +1665,9 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                             g.capn, g.capo, n, g.smpl,
                             track ? g.rnewT : nullptr, track ? g.roldT : nullptr,
                             track ? g.rnewTlen : nullptr, track ? g.roldTlen : nullptr,
-                            P<uint32_t>(ws.npairs), P<uint32_t>(ws.tiers), ctr, g.fast ? 1u : 0u, g.seed, phase,
+                            P<uint32_t>(ws.npairs), ctr, g.fast ? 1u : 0u, g.seed, phase,
                             tc ? (g.tc_kind == 0 ? g.tile_rows : TC_MAX_S) : 0u, max_staged, rscr_new, rscr_old,
-                            (g.fast && carry_now) ? 1u : 0u, nullptr};
+                            (g.fast && carry_now) ? 1u : 0u, nullptr, P<uint8_t>(ws.rtier)};
         };
         // the segment; its first failing call's error is returned.  copy:
         // read the counters back at its end (the whole-iteration graph reads
@@ -1655,6 +1719,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             ShufArgs sh = shuf_args();
             sh.phase_dev = phase_dev;
             k_shuffle_append<<<warp_blocks, 256, 0, st>>>(sh); count_launch();
+            k_tier_lists<<<(n + TIER_CHUNK - 1) / TIER_CHUNK, 256, 0, st>>>(P<uint8_t>(ws.rtier), n,
+                                                                           P<uint32_t>(ws.tiers), ctr); count_launch();
             chk(exclusive_scan(P<uint32_t>(ws.npairs), P<uint64_t>(ws.poff), n, scan_tmp,
                                reinterpret_cast<uint64_t*>(&ctr->pairs), st));
             chk(cudaMemsetAsync(ws.bcnt.p, 0, n1 * 4, st));

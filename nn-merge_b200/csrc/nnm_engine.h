@@ -41,10 +41,11 @@ struct Workspace {
     DevBuf cntpos, bcnt, bcur, boff, bucket, bigrev, nflag, scan_tmp;
     DevBuf npairs, poff, pd, tiers, erows;
     DevBuf kth;  // every row's K-th distance, gathered per iteration
+    DevBuf rtier;  // every row's join tier (k_shuffle_append), binned by k_tier_lists
     DevBuf draws, counters, misc;
     void release_all() {
         DevBuf* all[] = {&rcnt, &rcur, &rtot, &roff, &rseg, &rscr, &rcount, &rofs, &rbuf, &cntpos, &bcnt, &bcur,
-                         &boff, &bucket, &bigrev, &nflag, &scan_tmp, &npairs, &poff, &pd, &tiers, &erows, &kth,
+                         &boff, &bucket, &bigrev, &nflag, &scan_tmp, &npairs, &poff, &pd, &tiers, &erows, &kth, &rtier,
                          &draws, &counters, &misc};
         for (auto* b : all) b->release();
     }
