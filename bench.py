@@ -863,7 +863,8 @@ def main():
     dist_err = {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()), "rows": len(rows)}
 
     hbm, peak_kind = peaks()
-    names = {"join": ("local-join count pass: k_join_tc<0> (u8 Gram tiles on tcgen05) + FP32 k_pairs for lists > 128"
+    names = {"join": ("local-join count pass: k_join_tc<0> (u8 Gram tiles on tcgen05) + k_pairs_tc (lists > 128, "
+                      "128-slot blocks on tcgen05)"
                       if a.join != "fp32" else "local-join pair distances (FP32 k_pairs, all tiers)"),
              "emit": ("local-join emit pass: k_join_tc<1> + k_emit_rows" if a.join != "fp32" else "proposal emit (k_emit)"),
              "merge": "top-K merge (k_merge)"}

@@ -612,6 +612,306 @@ __global__ void __launch_bounds__(tc_threads(PASS), PASS == 0 ? 4 : KIND == KIND
     }
 }
 
+// Rows of the last tier (S > the tile's list cap) of the u8 join, count
+// pass, on the tensor cores.  A row's S slots lie in blocks of 128 (the
+// 128-byte swizzle K-major layout of a tile buffer, one block after
+// another); per block pair (p, q), p <= q, one kind::i8 MMA chain
+// D = X_q X_p^T (M = N = 128) into the CTA's 128 TMEM columns: TMEM lane m
+// is slot b = 128 q + m, column c is slot a = 128 p + c.  Consumer lane m
+// takes the pairs (a, b), a < b, a in the new list, column by column, so a
+// warp's 32 lanes hold 32 consecutive b of one a: each stored pair distance
+// (the slots of `pair_slot`, read by k_emit_rows) is one coalesced 128-byte
+// write, b's count a register, a's a ballot.  The outputs are k_pairs_u8's:
+// the distances (exact integers), the per-slot counts and the bucket
+// totals.  Recomputing the MMA in the emit pass instead of storing the
+// distances was measured slower (the emit epilogue costs more than reading
+// 4 bytes a pair back).
+//
+// Persistent CTAs of 320 threads over two row buffers, as the tiled join:
+// producers (warps 8-9) load a row's members and gather its vectors with
+// cp.async into buffer k % 2 while the consumers (warps 0-7, two per TMEM
+// lane quarter, alternate 8-column blocks) run the MMAs and the epilogue of
+// the other; full / empty mbarriers per buffer, every wait bounded, a
+// group's stop decided by a barrier-OR over its threads; a CTA that stops
+// records DERR_TC_WAIT, waits (bounded) once more for its MMA, frees its
+// TMEM and returns.
+constexpr int PT_CONS = 256, PT_PROD = 64, PT_THREADS = PT_CONS + PT_PROD;
+__host__ __device__ constexpr uint32_t pt_blocks(uint32_t R) { return (R + TC_SLOTS - 1) / TC_SLOTS; }
+// Rows of the last block: R's remainder rounded up to an 8-row swizzle atom.
+// Its columns are that many rows apart; an MMA reads 128 rows from a column
+// start all the same, the rows past the block's from whatever follows (slots
+// >= R, never read back).
+__host__ __device__ constexpr uint32_t pt_rows_last(uint32_t R) {
+    return ((R - TC_SLOTS * (pt_blocks(R) - 1)) + 7) & ~7u;
+}
+__host__ __device__ constexpr uint32_t pt_col_stride(uint32_t R, uint32_t blk) {
+    return (blk + 1 < pt_blocks(R) ? TC_SLOTS : pt_rows_last(R)) * 128;
+}
+__host__ __device__ constexpr size_t pt_vec_bytes(uint32_t R, uint32_t kq) {
+    return (size_t)((pt_blocks(R) - 1) * TC_SLOTS + pt_rows_last(R)) * 128 * tc_cols(kq);
+}
+// the members of one row buffer: per slot the 16-byte record {entry, K-th
+// distance bits, norm, group} and the count (4 B)
+__host__ __device__ constexpr size_t pt_mem_bytes(uint32_t R) { return ((size_t)R * 20 + 15) & ~(size_t)15; }
+// both buffers' vector blocks (1024-byte aligned), then both buffers'
+// members, and at least the 128 rows an MMA reads from the last column start
+__host__ __device__ constexpr size_t pt_smem_bytes(uint32_t R, uint32_t kq) {
+    return 2 * pt_vec_bytes(R, kq) + (2 * pt_mem_bytes(R) > (size_t)(TC_SLOTS - pt_rows_last(R)) * 128
+                                          ? 2 * pt_mem_bytes(R)
+                                          : (size_t)(TC_SLOTS - pt_rows_last(R)) * 128);
+}
+
+struct PtHdr {
+    uint32_t row, nn, S, done;
+    unsigned long long poff;  // the row's stored pair distances
+};
+
+__global__ void __launch_bounds__(PT_THREADS, 3) k_pairs_tc(JoinArgs a, uint32_t R) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ uint64_t mma_bar_s, full_s[2], empty_s[2];
+    __shared__ uint32_t tmem_s;
+    __shared__ PtHdr hdr[2];
+    if (a.ctr->overflow) return;  // a buffer sized ahead was too small: the host reruns
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t kq = a.kq, nchunk = kq >> 4, ncol = tc_cols(kq);
+    const size_t vbytes = pt_vec_bytes(R, kq), mbytes = pt_mem_bytes(R);
+    const uint32_t mma_bar = smem_u32(&mma_bar_s);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mma_bar));
+        for (int b = 0; b < 2; b++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full_s[b])), "r"(PT_PROD));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&empty_s[b])), "r"(PT_CONS));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_s)),
+                     "r"(TC_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_s;
+    const uint32_t cnt = a.ctr->ntier[NTIER - 1];
+    const uint32_t* rows = a.tier_rows + (size_t)(NTIER - 1) * a.n;
+    bool failed = false, mma_pending = false;
+    uint32_t mma_phase = 0;
+
+    if (warp >= PT_CONS / 32) {
+        // ---------------- producers ----------------
+        const uint32_t ptid = tid - PT_CONS;
+        uint32_t bi = blockIdx.x;
+        uint32_t pf_bi = ~0u, pf_row = 0, pf_nn = 0, pf_S = 0;  // a row header fetched ahead
+        unsigned long long sum_s = 0;
+        for (uint32_t k = 0;; k++) {
+            const uint32_t b = k & 1, use = k >> 1;
+            if (use > 0) {
+                const bool ok = mbar_wait_bounded(smem_u32(&empty_s[b]), (use - 1) & 1);
+                if (group_any(BAR_PROD, !ok, PT_PROD)) {
+                    failed = true;
+                    break;
+                }
+            }
+            unsigned char* buf = smem + b * vbytes;
+            uint4* info = reinterpret_cast<uint4*>(smem + 2 * vbytes + b * mbytes);
+            uint32_t* cur = reinterpret_cast<uint32_t*>(info + R);
+            // the next row with new entries; its header may have been
+            // fetched while the last row's vectors landed
+            uint32_t row = 0, nn = 0, S = 0;
+            for (; bi < cnt; bi += gridDim.x) {
+                if (pf_bi == bi) {
+                    row = pf_row;
+                    nn = pf_nn;
+                    S = pf_S;
+                } else {
+                    row = rows[bi];
+                    nn = a.newlen[row];
+                    S = nn + a.oldlen[row];
+                }
+                if (nn) break;
+                for (uint32_t q = ptid; q < S; q += PT_PROD) a.cntpos[(size_t)row * a.caps + q] = 0;  // no pairs
+            }
+            PtHdr& H = hdr[b];
+            if (bi >= cnt) {
+                if (ptid == 0) H.done = 1;
+                mbar_arrive(smem_u32(&full_s[b]));  // the arrive releases the header write
+                break;
+            }
+            // the members, four slots a thread at a time: each step's loads
+            // (entries; then K-th distances and norms; then groups) issued
+            // together
+            for (uint32_t q0 = ptid; q0 < S; q0 += 4 * PT_PROD) {
+                uint32_t e[4], nr[4];
+                float kt[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const uint32_t q = q0 + i * PT_PROD;
+                    e[i] = q < nn ? a.newL[(size_t)row * a.capn + q]
+                                  : (q < S ? a.oldL[(size_t)row * a.capo + q - nn] : 0u);
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const uint32_t q = q0 + i * PT_PROD, id = e[i] & LID_MASK;
+                    kt[i] = q < S ? a.kthv[id] : 0.f;
+                    nr[i] = q < S ? a.nrm[id] : 0u;
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const uint32_t q = q0 + i * PT_PROD, id = e[i] & LID_MASK;
+                    if (q < S) {
+                        info[q] = make_uint4(e[i], __float_as_uint(kt[i]), nr[i],
+                                             a.mode == MODE_SMERGE ? leaf_of(id, a.leaf_off, a.nleaf) : (e[i] >> 31));
+                        cur[q] = 0;
+                    }
+                }
+            }
+            sum_s += S;
+            if (ptid == 0) {
+                H.row = row;
+                H.nn = nn;
+                H.S = S;
+                H.done = 0;
+                H.poff = a.poff[row];
+            }
+            group_sync(BAR_PROD, PT_PROD);  // the members, before the gather reads them
+            bi += gridDim.x;
+            // gather: chunk c of slot s -> block s / 128, column c / 8, row
+            // s % 128, chunk (c % 8) ^ (s % 8)
+            const uint32_t vbase = smem_u32(buf);
+            for (uint32_t i = ptid; i < S * nchunk; i += PT_PROD) {
+                const uint32_t sl = i / nchunk, c = i - sl * nchunk, ls = sl & (TC_SLOTS - 1);
+                const uint32_t blk = sl >> 7;
+                cp_async16(vbase + blk * ncol * TC_COL_BYTES + (c >> 3) * pt_col_stride(R, blk) + ls * 128 +
+                               (((c & 7) ^ (ls & 7)) << 4),
+                           a.xq + (size_t)(info[sl].x & LID_MASK) * kq + c * 16);
+            }
+            if (bi < cnt) {  // the next row's header while these copies land
+                pf_bi = bi;
+                pf_row = rows[bi];
+                pf_nn = a.newlen[pf_row];
+                pf_S = pf_nn + a.oldlen[pf_row];
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // cp.async writes -> tensor core reads
+            mbar_arrive(smem_u32(&full_s[b]));
+        }
+        if (ptid == 0 && sum_s) atomicAdd(&a.ctr->sum_s, sum_s);  // every producer holds the total
+    } else {
+        // ---------------- consumers ----------------
+        uint32_t cmps = 0;
+        const uint32_t quarter = warp & 3, half = warp >> 2;
+        const uint32_t tlane = tmem + ((quarter * 32) << 16);
+        for (uint32_t k = 0;; k++) {
+            const uint32_t b = k & 1, use = k >> 1;
+            const bool okf = mbar_wait_bounded(smem_u32(&full_s[b]), use & 1);
+            if (group_any(BAR_CONS, !okf, PT_CONS)) {
+                failed = true;
+                break;
+            }
+            const PtHdr& H = hdr[b];
+            if (H.done) break;
+            const uint32_t row = H.row, nn = H.nn, S = H.S, no = S - nn;
+            float* pd = a.pd + H.poff;
+            const uint4* info = reinterpret_cast<const uint4*>(smem + 2 * vbytes + b * mbytes);
+            uint32_t* cur = const_cast<uint32_t*>(reinterpret_cast<const uint32_t*>(info + R));
+            const uint32_t vbase = smem_u32(smem + b * vbytes);
+            for (uint32_t p = 0; p * TC_SLOTS < nn && !failed; p++) {
+                for (uint32_t q = p; q * TC_SLOTS < S; q++) {
+                    if (tid == 0) {
+                        asm volatile("tcgen05.fence::after_thread_sync;");
+                        const uint32_t ab = vbase + q * ncol * TC_COL_BYTES, bb = vbase + p * ncol * TC_COL_BYTES;
+                        const uint32_t as = pt_col_stride(R, q), bs = pt_col_stride(R, p);
+                        for (uint32_t kk = 0; kk < kq / 32; kk++) {
+                            const uint32_t koff = kk * 32;  // bytes into the operand row
+                            const uint64_t da = smem_desc_sw128(ab + (koff >> 7) * as + (koff & 127));
+                            const uint64_t db = smem_desc_sw128(bb + (koff >> 7) * bs + (koff & 127));
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                                    tmem),
+                                "l"(da), "l"(db), "r"(IDESC_U8), "r"(kk), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                        }
+                        asm volatile(
+                            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                mma_bar)
+                            : "memory");
+                    }
+                    const bool okm = mbar_wait_bounded(mma_bar, mma_phase);
+                    if (group_any(BAR_CONS, !okm, PT_CONS)) {
+                        failed = true;
+                        mma_pending = true;
+                        break;
+                    }
+                    mma_phase ^= 1u;
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+                    // this lane: slot b = 128 q + 32 quarter + lane; columns a = 128 p + c
+                    // with a < nn and (diagonal block) a < the quarter's last b
+                    const uint32_t bv = q * TC_SLOTS + quarter * 32 + lane;
+                    if (q * TC_SLOTS + quarter * 32 < S) {
+                        const bool in_b = bv < S;
+                        const uint4 ib = info[in_b ? bv : 0];
+                        const uint32_t eb = ib.x, gb = ib.w, nb = ib.z;
+                        const float kth_b = __uint_as_float(ib.y);
+                        uint32_t cnt_b = 0;
+                        const uint32_t a0 = p * TC_SLOTS;
+                        uint32_t ncols = min(TC_SLOTS, nn - a0);
+                        if (p == q) ncols = min(ncols, quarter * 32 + 32);
+                        // 8-column blocks 0, 3, 4, 7, ... to half 0, 1, 2, 5, 6, ... to
+                        // half 1 (early columns of a diagonal block hold more pairs)
+                        for (uint32_t c0 = 0; c0 < ncols; c0 += 8) {
+                            const uint32_t bk = c0 >> 3;
+                            if (((bk + (bk >> 1)) & 1u) != half) continue;
+                            uint32_t v[8];
+                            tmem_ld8(tlane + c0, v);
+                            const uint32_t jn = min(8u, ncols - c0);
+#pragma unroll
+                            for (uint32_t j = 0; j < 8; j++) {
+                                if (j < jn) {
+                                    const uint32_t av = a0 + c0 + j;
+                                    const uint4 ia = info[av];
+                                    const float dd = (float)((int)(ia.z + nb) - 2 * (int)v[j]);
+                                    if (in_b && bv > av)  // lanes: consecutive b of one a
+                                        pd[(bv < nn ? av * nn - av * (av + 1) / 2 - av - 1
+                                                    : nn * (nn - 1) / 2 + av * no - nn) + bv] = dd;
+                                    uint32_t outer, inner;
+                                    const bool pr = in_b && bv > av &&
+                                                    pair_order(a.mode, a.verse, av, bv, nn, ia.x, eb, ia.w, gb, outer, inner);
+                                    cmps += pr;
+                                    cnt_b += pr && dd < kth_b;
+                                    const unsigned bal = __ballot_sync(0xffffffffu, pr && dd < __uint_as_float(ia.y));
+                                    if (lane == 0 && bal) atomicAdd(&cur[av], (uint32_t)__popc(bal));
+                                }
+                            }
+                        }
+                        if (cnt_b) atomicAdd(&cur[bv], cnt_b);
+                    }
+                    asm volatile("tcgen05.fence::before_thread_sync;");
+                    group_sync(BAR_CONS, PT_CONS);  // TMEM read and counts done before the next MMA
+                }
+            }
+            if (failed) break;
+            for (uint32_t q = tid; q < S; q += PT_CONS) {
+                const uint32_t c = cur[q];
+                a.cntpos[(size_t)row * a.caps + q] = (uint16_t)c;
+                if (c) atomicAdd(&a.bcnt[info[q].x & LID_MASK], c);
+            }
+            mbar_arrive(smem_u32(&empty_s[b]));
+        }
+        for (int o = 16; o > 0; o >>= 1) cmps += __shfl_xor_sync(0xffffffffu, cmps, o);
+        if (lane == 0 && cmps) atomicAdd(&a.ctr->ncmps, (unsigned long long)cmps);
+    }
+    if (failed && (tid & 127) == 0) atomicOr(a.tc_err, (unsigned)DERR_TC_WAIT);
+    if (mma_pending) mbar_wait_bounded(mma_bar, mma_phase);  // the MMA may still write TMEM
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_COLS));
+    }
+}
+
 // Warp per vector: checks that every component is an integer in [0, 255],
 // writes the u8 copy (zero padded to kq bytes) and the squared norm, and
 // tracks the largest norm.  Four components per lane and step (rows are
@@ -955,6 +1255,36 @@ cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, 
     if (ja.tc_kind == KIND_U8) launch_tc_kind<KIND_U8>(pass, ja, tiles, nsm, bytes, st);
     else if (ja.tc_kind == KIND_BF16) launch_tc_kind<KIND_BF16>(pass, ja, tiles, nsm, bytes, st);
     else launch_tc_kind<KIND_FP8>(pass, ja, tiles, nsm, bytes, st);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// k_pairs_tc: two row buffers; at least TC_SMEM_FLOOR, so that at most
+// four CTAs (4 x 128 TMEM columns) share an SM.
+size_t pairs_tc_smem(uint32_t R, uint32_t kq) { return std::max<size_t>(pt_smem_bytes(R, kq), TC_SMEM_FLOOR); }
+
+cudaError_t pairs_tc_set_attributes(uint32_t R, uint32_t kq) {
+    return cudaFuncSetAttribute(k_pairs_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pairs_tc_smem(R, kq));
+}
+
+// Residency counted as for the tiled join (shared memory, registers, the
+// TMEM cap).
+cudaError_t launch_pairs_tc(const JoinArgs& ja, uint32_t R, const unsigned* ntier, int nsm, cudaStream_t st) {
+    if (ntier && !ntier[NTIER - 1]) return cudaSuccess;
+    const size_t bytes = pairs_tc_smem(R, ja.kq);
+    int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 65536;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, k_pairs_tc);
+    const int per_sm_smem = (int)((size_t)smem_sm / (bytes + fa.sharedSizeBytes + (size_t)reserved));
+    const int per_sm_regs = regs_sm / (((fa.numRegs + 7) & ~7) * PT_THREADS);
+    const int per_sm = std::min(std::max(std::min(per_sm_smem, per_sm_regs), 1), TC_TMEM_CTAS);
+    const unsigned full = (unsigned)nsm * (unsigned)per_sm;
+    const unsigned grid = ntier ? std::min<unsigned>(ntier[NTIER - 1], full) : full;
+    k_pairs_tc<<<grid, PT_THREADS, bytes, st>>>(ja, R);
     count_launch();
     return cudaGetLastError();
 }

@@ -1495,7 +1495,7 @@ static cudaError_t prep_pairs(uint32_t caps, uint32_t dp, size_t emit_smem, int 
 // join takes the others.
 template <int M>
 static void launch_pairs(const JoinArgs& ja, const unsigned* ntier, uint32_t caps, uint32_t dp, int nsm,
-                         bool last_only, bool u8_last, cudaStream_t st) {
+                         bool last_only, bool u8_last, bool u8_tc, cudaStream_t st) {
     if (!last_only && ntier) {
         if (ntier[0]) { k_pairs<M, 0><<<ntier[0], TIER_THREADS[0], pairs_smem(TIER_CAP[0], dp, true), st>>>(ja, TIER_CAP[0]); count_launch(); }
         if (ntier[1]) { k_pairs<M, 1><<<ntier[1], TIER_THREADS[1], pairs_smem(TIER_CAP[1], dp, true), st>>>(ja, TIER_CAP[1]); count_launch(); }
@@ -1505,6 +1505,10 @@ static void launch_pairs(const JoinArgs& ja, const unsigned* ntier, uint32_t cap
     // ntier null (the tensor-core join takes tiers 0-3): the count of the
     // last tier is on the device only, the blocks loop over its rows; the
     // grid is every block that fits on the SMs at once
+    if (u8_tc) {  // the last tier on the tensor cores
+        launch_pairs_tc(ja, caps, ntier, nsm, st);
+        return;
+    }
     if (!ntier || ntier[4]) {
         const size_t smem = u8_last ? pairs_smem_u8(caps, ja.kq) : pairs_smem(caps, dp, false);
         int per_sm = 0;
@@ -1593,7 +1597,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
     const bool tc = g.xq != nullptr;
     // reduced-precision joins (BF16, FP8) emit approximate distances
     const bool approx = tc && g.tc_kind != 0;
-    bool u8_last = false;  // rows of S > 128 on k_pairs_u8 (u8 join, staged vectors fit)
+    bool u8_last = false;  // rows of S > 128 on the u8 vectors (staged vectors fit)
+    bool u8_tc = false;    // ... on the tensor cores (k_pairs_tc), else k_pairs_u8
     if (tc) {
         NNM_CUDA_TRY(tc_set_attributes(g.kq, g.tc_kind));
         NNM_CUDA_TRY(ws.erows.ensure((size_t)n * 4 * 4 + 16));
@@ -1603,6 +1608,8 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
         u8_last = g.tc_kind == 0 && g.metric == L2 && u8_smem <= (size_t)optin;
         if (u8_last)
             NNM_CUDA_TRY(cudaFuncSetAttribute(k_pairs_u8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u8_smem));
+        u8_tc = u8_last && pairs_tc_smem(caps, g.kq) <= (size_t)optin;
+        if (u8_tc) NNM_CUDA_TRY(pairs_tc_set_attributes(caps, g.kq));
     }
 
     const unsigned warp_blocks = (unsigned)((n + 7) / 8);
@@ -1755,9 +1762,9 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
             rec(0);
             if (tc) e = launch_join_tc(0, ja, nt, nsm, st);
             if (e == cudaSuccess) {
-                if (g.metric == L2) launch_pairs<L2>(ja, nt, caps, g.dp, nsm, tc, u8_last, st);
-                else if (g.metric == L1) launch_pairs<L1>(ja, nt, caps, g.dp, nsm, tc, false, st);
-                else launch_pairs<CHI2>(ja, nt, caps, g.dp, nsm, tc, false, st);
+                if (g.metric == L2) launch_pairs<L2>(ja, nt, caps, g.dp, nsm, tc, u8_last, u8_tc, st);
+                else if (g.metric == L1) launch_pairs<L1>(ja, nt, caps, g.dp, nsm, tc, false, false, st);
+                else launch_pairs<CHI2>(ja, nt, caps, g.dp, nsm, tc, false, false, st);
                 rec(1);
                 e = exclusive_scan(P<uint32_t>(ws.bcnt), P<uint64_t>(ws.boff), n, scan_tmp,
                                    reinterpret_cast<uint64_t*>(&ctr->proposals), st);
@@ -1989,7 +1996,7 @@ int run_nndescent(Ctx& ctx, GraphDev& g, JoinMode mode, uint32_t split, uint32_t
                                hc.pairs, hc.proposals, hc.flags, hc.ncmps, hc.sum_s, t01, t23, t34};
                 ctx.iter_log.push_back(L);
             }
-            if (tc) ctx.join_rows_tc += hc.ntier[0] + hc.ntier[1] + hc.ntier[2] + hc.ntier[3];
+            if (tc) ctx.join_rows_tc += hc.ntier[0] + hc.ntier[1] + hc.ntier[2] + hc.ntier[3] + (u8_tc ? hc.ntier[4] : 0u);
             const double s_tc = (double)hc.sum_s_tc, s_f32 = (double)(hc.sum_s - hc.sum_s_tc);
             ctx.kjoin.launches += tc ? 1 + (hc.ntier[4] > 0)
                                      : (hc.ntier[0] > 0) + (hc.ntier[1] > 0) + (hc.ntier[2] > 0) +

@@ -126,5 +126,13 @@ cudaError_t tc_set_attributes(uint32_t kq, uint32_t kind);
 // ntier: rows per tier as the host read them, or null (grid of every SM's
 // CTAs, the kernel reads the counts on the device).
 cudaError_t launch_join_tc(int pass, const JoinArgs& ja, const unsigned* ntier, int nsm, cudaStream_t st);
+// Rows of the last tier (lists longer than a tile's) of the u8 join on the
+// tensor cores, count pass: their stored pair distances, per-slot counts and
+// bucket totals, as k_pairs_u8 computes them (k_emit_rows then writes the
+// proposals).  R: the longest list (new + old caps); applies when
+// pairs_tc_smem(R, kq) fits a CTA's shared memory.
+size_t pairs_tc_smem(uint32_t R, uint32_t kq);
+cudaError_t pairs_tc_set_attributes(uint32_t R, uint32_t kq);
+cudaError_t launch_pairs_tc(const JoinArgs& ja, uint32_t R, const unsigned* ntier, int nsm, cudaStream_t st);
 
 }  // namespace nnm

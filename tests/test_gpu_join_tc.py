@@ -35,7 +35,9 @@ def test_kgraph(ctx, rng):
     x = gaussian_mixture_u8(6000, seed=31)
     t, f, rows = both(ctx, ctx.kgraph, x, 20, seed=3, rng=rng)
     same(t, f)
-    assert rows["tensor"] > 0 and rows["tensor"] == sum(rows["tiers"][:4])
+    # every joined row on the tensor cores: the tiles, and the lists longer
+    # than a tile on the tensor-core pair kernel
+    assert rows["tensor"] > 0 and rows["tensor"] == sum(rows["tiers"])
 
 
 @pytest.mark.parametrize("rng", ["exact", "fast"])
@@ -67,30 +69,36 @@ def test_hmerge(ctx):
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
-@pytest.mark.parametrize("d", [128, 300])
-def test_all_tiers_and_big_lists(ctx, d):
+@pytest.mark.parametrize("d,cap", [(128, 150), (128, 400), (160, 400), (300, 400)])
+def test_all_tiers_and_big_lists(ctx, d, cap):
     # k=32 with a large sample cap gives lists of 17..128 entries and rows
-    # above 128, which take the staged u8 pair kernel (d=128) or, when the
-    # staged vectors do not fit in shared memory (d=300, lists up to 864),
-    # the unstaged FP32 one; k=6 gives lists of <= 16
+    # above 128, which take the tensor-core pair kernel when two buffers of
+    # their 128-slot blocks fit in shared memory (d=128, lists up
+    # to 364: three blocks), else the staged u8 dp4a one (lists up to 864 at
+    # d=128 and 160), or the unstaged FP32 one (d=300); k=6 gives lists of
+    # <= 16
     x = gaussian_mixture_u8(4000, d=d, seed=36, n_centres=8)
-    t, f, big = both(ctx, ctx.kgraph, x, 32, seed=11, sample_cap=400)
+    t, f, big = both(ctx, ctx.kgraph, x, 32, seed=11, sample_cap=cap)
     same(t, f)
+    on_tc = d == 128 and cap == 150
+    assert (big["tensor"] == sum(big["tiers"])) == on_tc, big
     t, f, small = both(ctx, ctx.kgraph, x, 6, seed=11)
     same(t, f)
     assert all(a + b > 0 for a, b in zip(big["tiers"], small["tiers"])), (big, small)
     assert big["tiers"][4] > 0 and small["tiers"][0] > 0
 
 
+@pytest.mark.parametrize("cap", [150, 400])
 @pytest.mark.parametrize("rng", ["exact", "fast"])
-def test_big_lists_in_merges(ctx, rng):
+def test_big_lists_in_merges(ctx, rng, cap):
     # lists above 128 entries in the merge builders: their group and verse
-    # filters on the staged u8 pair kernel and the block-per-row emit
+    # filters on the tensor-core pair kernel (cap 150) or the staged u8 pair
+    # kernel (cap 400), and the block-per-row emit
     x = gaussian_mixture_u8(4000, seed=41, n_centres=8)
-    t, f, rows = both(ctx, ctx.merge_leaves, x, 32, [1000] * 4, seed=5, rng=rng, sample_cap=400)
+    t, f, rows = both(ctx, ctx.merge_leaves, x, 32, [1000] * 4, seed=5, rng=rng, sample_cap=cap)
     same(t, f)
     assert rows["tiers"][4] > 0
-    t, f, rows = both(ctx, ctx.jmerge, x, 32, seed=6, rng=rng, sample_cap=400)
+    t, f, rows = both(ctx, ctx.jmerge, x, 32, seed=6, rng=rng, sample_cap=cap)
     same(t, f)
     assert rows["tiers"][4] > 0
 
@@ -243,8 +251,8 @@ def test_forced_tensor_rejects_other_metrics(ctx):
 
 @pytest.mark.parametrize("rng", ["exact", "fast"])
 def test_tile_rows_give_the_same_graph(ctx, rng):
-    """Lists longer than tile_rows go from the tensor-core tiles to the dp4a
-    pair kernel: both exact, the same graph for every boundary."""
+    """Lists longer than tile_rows go from the tensor-core tiles to the
+    tensor-core pair kernel: both exact, the same graph for every boundary."""
     x = gaussian_mixture_u8(6000, seed=91)
     ref = ctx.kgraph(x, 20, seed=3, rng=rng, join="tensor")
     for tr in (32, 64):
