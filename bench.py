@@ -140,9 +140,9 @@ def tensor_peak():
 # library's algorithmic bytes of the same launches; the bench reports that
 # ratio times the live run's algorithmic bytes per launch.  Keyed by (kernel
 # class, tensor join).  Per build, measured against algorithmic: join
-# (k_join_tc<0> + k_pairs_u8) 21.29 / 41.33 GB, emit (k_join_tc<1> +
-# k_emit_rows) 43.36 / 49.03 GB, merge (k_merge_fast) 9.68 / 11.00 GB.
-NCU_TRAFFIC_RATIO = {("join", True): 0.515, ("emit", True): 0.884, ("merge", True): 0.880}
+# (k_join_tc<0> + k_pairs_tc) 21.80 / 41.33 GB, emit (k_join_tc<1> +
+# k_emit_rows) 44.03 / 49.03 GB, merge (k_merge_fast) 9.68 / 11.00 GB.
+NCU_TRAFFIC_RATIO = {("join", True): 0.527, ("emit", True): 0.898, ("merge", True): 0.880}
 
 
 def traffic_per_launch(kind, stat, a):
