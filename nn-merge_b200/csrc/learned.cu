@@ -21,6 +21,7 @@
 
 #include "nnm_launch.h"
 #include "nnm_learned.h"
+#include "nnm_tc.cuh"
 
 namespace nnm {
 namespace {
@@ -112,6 +113,215 @@ __global__ void __launch_bounds__(FWD_THREADS) k_mlp_fwd(MlpView m, const float*
                 if (z_out) z_out[(size_t)gr * MLP_O + o] = z;
             }
         }
+    }
+}
+
+// Inference on the tensor cores (d <= 128): a CTA per SM, 128 rows per
+// tile.  Layer 1 is one tcgen05 kind::f16 MMA chain D = U W1^T (M = 128
+// rows, N = 256 hidden units, FP32 accumulators in 256 TMEM columns) over
+// u = x * scale + shift split into three BF16 parts u = hi + mid + lo
+// (successive rounding residuals; a float's 24 significant bits in three
+// 8-bit parts): W1 is BF16 and every product of BF16 values is exact in
+// FP32, so layer 1 is the FP32 dot product of the CUDA-core kernel up to
+// the order of its sums.  The epilogue reads the row's hidden accumulators
+// (TMEM lane = row), adds b1, applies relu and accumulates layer 2 in FP32
+// on the CUDA cores (W2 in shared memory, read as broadcasts); the two warps
+// of a TMEM lane quarter take 128 hidden units each and add their partial
+// outputs through shared memory.  Operands in the 128-byte swizzle K-major
+// layout: W1 (256 rows) staged once per CTA, the three parts of U per tile.
+// The MMA wait is bounded; when it runs out the CTA records the failure,
+// waits (bounded) once more, frees its TMEM and returns.
+constexpr uint32_t MT_ROWS = 128, MT_THREADS = 256, MT_MAX_D = 128;
+// Instruction descriptor of kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16
+// (bits 7-9 = 1, 10-12 = 1), both K-major, N = 256 (N >> 3 at bit 17),
+// M = 128 (M >> 4 at bit 24).
+constexpr uint32_t MT_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((MLP_H >> 3) << 17) | ((MT_ROWS >> 4) << 24);
+
+__host__ __device__ constexpr uint32_t mt_dk(uint32_t d) { return (d + 15) & ~15u; }    // K: 16 per MMA
+__host__ __device__ constexpr uint32_t mt_cols(uint32_t d) { return (mt_dk(d) + 63) / 64; }  // 128-B columns
+__host__ __device__ constexpr size_t mt_w1_bytes(uint32_t d) { return (size_t)mt_cols(d) * MLP_H * 128; }
+__host__ __device__ constexpr size_t mt_part_bytes(uint32_t d) { return (size_t)mt_cols(d) * MT_ROWS * 128; }
+// W1, the three parts of U, W2 (FP32), b1, b2, the partial outputs (128 rows
+// of 33 floats)
+__host__ __device__ constexpr size_t mt_smem_bytes(uint32_t d) {
+    return mt_w1_bytes(d) + 3 * mt_part_bytes(d) + (size_t)MLP_H * MLP_O * 4 + MLP_H * 4 + MLP_O * 4 +
+           (size_t)MT_ROWS * 33 * 4;
+}
+
+// Byte offset of 16-byte chunk `kc` (elements 8 kc .. 8 kc + 7) of row r in
+// a swizzled K-major operand of `rows` rows.
+__device__ __forceinline__ uint32_t mt_chunk(uint32_t r, uint32_t kc, uint32_t rows) {
+    return (kc >> 3) * rows * 128 + r * 128 + (((kc & 7) ^ (r & 7)) << 4);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__global__ void __launch_bounds__(MT_THREADS, 1) k_mlp_tc(MlpView m, const float* __restrict__ x, uint32_t dp,
+                                                          uint32_t nrows, uint32_t* __restrict__ codes,
+                                                          float* __restrict__ z_out, unsigned* err) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ uint64_t mma_bar_s;
+    __shared__ uint32_t tmem_s;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t d = m.d, dk = mt_dk(d), nkc = dk / 8;
+    unsigned char* w1s = smem;
+    unsigned char* us = w1s + mt_w1_bytes(d);
+    float* w2s = reinterpret_cast<float*>(us + 3 * mt_part_bytes(d));
+    float* b1s = w2s + MLP_H * MLP_O;
+    float* b2s = b1s + MLP_H;
+    float* zp = b2s + MLP_O;
+    const uint32_t mma_bar = smem_u32(&mma_bar_s);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mma_bar));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_s)),
+                     "r"(MLP_H));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    // the weights, once: W1 row j (hidden unit) = column j of w1t, zero past d
+    for (uint32_t i = tid; i < MLP_H * nkc; i += MT_THREADS) {
+        const uint32_t j = i % MLP_H, kc = i / MLP_H;
+        uint32_t w[4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const uint32_t k = kc * 8 + 2 * t;
+            const float a = k < d ? bf(m.w1t[(size_t)k * MLP_H + j]) : 0.f;
+            const float b = k + 1 < d ? bf(m.w1t[(size_t)(k + 1) * MLP_H + j]) : 0.f;
+            w[t] = pack_bf16(a, b);  // exact: the values are BF16
+        }
+        *reinterpret_cast<uint4*>(w1s + mt_chunk(j, kc, MLP_H)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    for (uint32_t i = tid; i < MLP_H * MLP_O; i += MT_THREADS) w2s[i] = bf(m.w2t[i]);
+    for (uint32_t i = tid; i < MLP_H; i += MT_THREADS) b1s[i] = m.b1[i];
+    if (tid < MLP_O) b2s[tid] = m.b2[tid];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor core reads
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_s;
+    uint32_t phase = 0;
+    bool failed = false;
+    const uint32_t ntiles = (nrows + MT_ROWS - 1) / MT_ROWS;
+    for (uint32_t t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
+        const uint32_t r0 = t * MT_ROWS;
+        // U's three parts: chunk kc of row r from two float4 of x (zero past d
+        // and past the last row)
+        for (uint32_t i = tid; i < MT_ROWS * nkc; i += MT_THREADS) {
+            const uint32_t r = i / nkc, kc = i - r * nkc, k0 = kc * 8;
+            float u[8];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (r0 + r < nrows && k0 + 4 * h < d)
+                    v = __ldg(reinterpret_cast<const float4*>(x + (size_t)(r0 + r) * dp + k0 + 4 * h));
+                const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const uint32_t k = k0 + 4 * h + c;
+                    u[4 * h + c] = (r0 + r < nrows && k < d) ? fmaf(e[c], m.scale, m.shift) : 0.f;
+                }
+            }
+            uint32_t ph[4], pm[4], pl[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                float hi[2], mi[2], lo[2];
+#pragma unroll
+                for (int s = 0; s < 2; s++) {
+                    const float v = u[2 * c + s];
+                    hi[s] = __bfloat162float(__float2bfloat16_rn(v));
+                    const float r1 = v - hi[s];
+                    mi[s] = __bfloat162float(__float2bfloat16_rn(r1));
+                    lo[s] = r1 - mi[s];
+                }
+                ph[c] = pack_bf16(hi[0], hi[1]);
+                pm[c] = pack_bf16(mi[0], mi[1]);
+                pl[c] = pack_bf16(lo[0], lo[1]);
+            }
+            const uint32_t off = mt_chunk(r, kc, MT_ROWS);
+            *reinterpret_cast<uint4*>(us + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+            *reinterpret_cast<uint4*>(us + mt_part_bytes(d) + off) = make_uint4(pm[0], pm[1], pm[2], pm[3]);
+            *reinterpret_cast<uint4*>(us + 2 * mt_part_bytes(d) + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> tensor core reads
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t wb = smem_u32(w1s), ub = smem_u32(us);
+            for (uint32_t part = 0; part < 3; part++)
+                for (uint32_t kk = 0; kk < dk / 16; kk++) {
+                    const uint32_t koff = kk * 32;  // bytes into the operand row
+                    const uint64_t da = smem_desc_sw128(ub + part * (uint32_t)mt_part_bytes(d) +
+                                                        (koff >> 7) * MT_ROWS * 128 + (koff & 127));
+                    const uint64_t db = smem_desc_sw128(wb + (koff >> 7) * MLP_H * 128 + (koff & 127));
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                        "l"(da), "l"(db), "r"(MT_IDESC), "r"(part | kk), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mma_bar)
+                         : "memory");
+        }
+        const bool ok = mbar_wait_bounded(mma_bar, phase);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // epilogue: row r0 + 32 quarter + lane, hidden units [128 half, + 128)
+        const uint32_t quarter = warp & 3, half = warp >> 2, rl = quarter * 32 + lane;
+        float z[MLP_O];
+#pragma unroll
+        for (uint32_t o = 0; o < MLP_O; o++) z[o] = 0.f;
+        for (uint32_t c0 = 0; c0 < MLP_H / 2; c0 += 8) {
+            const uint32_t j0 = half * (MLP_H / 2) + c0;
+            uint32_t v[8];
+            tmem_ld8(tmem + ((quarter * 32) << 16) + j0, v);
+#pragma unroll
+            for (uint32_t jj = 0; jj < 8; jj++) {
+                const float h = fmaxf(__uint_as_float(v[jj]) + b1s[j0 + jj], 0.f);
+                const float4* w = reinterpret_cast<const float4*>(w2s + (j0 + jj) * MLP_O);
+#pragma unroll
+                for (uint32_t o4 = 0; o4 < MLP_O / 4; o4++) {
+                    const float4 wv = w[o4];
+                    z[4 * o4] = fmaf(h, wv.x, z[4 * o4]);
+                    z[4 * o4 + 1] = fmaf(h, wv.y, z[4 * o4 + 1]);
+                    z[4 * o4 + 2] = fmaf(h, wv.z, z[4 * o4 + 2]);
+                    z[4 * o4 + 3] = fmaf(h, wv.w, z[4 * o4 + 3]);
+                }
+            }
+        }
+        if (half == 1)
+#pragma unroll
+            for (uint32_t o = 0; o < MLP_O; o++) zp[rl * 33 + o] = z[o];
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();  // partial outputs written; TMEM and U read before the next tile's MMA
+        if (half == 0 && r0 + rl < nrows) {
+            uint32_t code = 0;
+#pragma unroll
+            for (uint32_t o = 0; o < MLP_O; o++) {
+                const float zo = z[o] + zp[rl * 33 + o] + b2s[o];
+                code |= (zo > 0.f ? 1u : 0u) << o;
+                if (z_out) z_out[(size_t)(r0 + rl) * MLP_O + o] = zo;
+            }
+            codes[r0 + rl] = code;
+        }
+    }
+    if (failed) {
+        if (tid == 0) atomicOr(err, 1u);
+        mbar_wait_bounded(mma_bar, phase);  // the MMA may still write TMEM
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(MLP_H));
     }
 }
 

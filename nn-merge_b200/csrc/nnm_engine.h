@@ -43,10 +43,11 @@ struct Workspace {
     DevBuf kth;  // every row's K-th distance, gathered per iteration
     DevBuf rtier;  // every row's join tier (k_shuffle_append), binned by k_tier_lists
     DevBuf draws, counters, misc;
+    DevBuf mlp_err;  // the code network's tensor-core inference: a wait that ran out
     void release_all() {
         DevBuf* all[] = {&rcnt, &rcur, &rtot, &roff, &rseg, &rscr, &rcount, &rofs, &rbuf, &cntpos, &bcnt, &bcur,
                          &boff, &bucket, &bigrev, &nflag, &scan_tmp, &npairs, &poff, &pd, &tiers, &erows, &kth, &rtier,
-                         &draws, &counters, &misc};
+                         &draws, &counters, &misc, &mlp_err};
         for (auto* b : all) b->release();
     }
 };
