@@ -575,9 +575,31 @@ int mlp_upload(Ctx& ctx, DevMlp& m, const nnm_mlp& h) {
     return 0;
 }
 
+// Inference: on the tensor cores (k_mlp_tc) for d <= 128 when its shared
+// memory fits, else the CUDA-core forward.
 int mlp_codes_dev(Ctx& ctx, const DevMlp& m, const float* x, uint32_t n, uint32_t dp, uint32_t* codes, float* z) {
     NNM_CUDA_TRY(set_fwd_attrs(m.d));
     if (!n) return 0;
+    int optin = 0, nsm = 148;
+    NNM_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx.device));
+    NNM_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx.device));
+    if (m.d <= MT_MAX_D && mt_smem_bytes(m.d) <= (size_t)optin) {
+        NNM_CUDA_TRY(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mt_smem_bytes(m.d)));
+        NNM_CUDA_TRY(ctx.ws.mlp_err.ensure(64));
+        NNM_CUDA_TRY(cudaMemsetAsync(ctx.ws.mlp_err.p, 0, 4, ctx.stream));
+        const uint32_t tiles = (n + MT_ROWS - 1) / MT_ROWS;
+        k_mlp_tc<<<std::min<uint32_t>(tiles, (uint32_t)nsm), MT_THREADS, mt_smem_bytes(m.d), ctx.stream>>>(
+            view_of(m), x, dp, n, codes, z, ctx.ws.mlp_err.as<unsigned>()); count_launch();
+        NNM_CUDA_TRY(cudaGetLastError());
+        unsigned err = 0;
+        NNM_CUDA_TRY(cudaMemcpyAsync(&err, ctx.ws.mlp_err.p, 4, cudaMemcpyDeviceToHost, ctx.stream));
+        NNM_CUDA_TRY(cudaStreamSynchronize(ctx.stream));
+        if (err) {
+            ctx.last_error = "the code network's tensor-core wait ran out";
+            return 6;
+        }
+        return 0;
+    }
     k_mlp_fwd<false><<<(n + RB - 1) / RB, FWD_THREADS, fwd_smem(m.d), ctx.stream>>>(view_of(m), x, dp, nullptr, n,
                                                                                   nullptr, nullptr, codes, z); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
