@@ -289,6 +289,7 @@ struct CrossArgsL {
     uint32_t seed, phase;
     IterCounters* ctr;
     DistSrc ds;
+    const unsigned long long* fence;  // every VFENCE-th key of each segment (P / VFENCE a segment)
 };
 
 __device__ __forceinline__ uint32_t leaf_of_row(uint32_t id, const uint32_t* off, uint32_t nleaf) {
@@ -344,7 +345,20 @@ __global__ void __launch_bounds__(IW * 32) k_learned_cross(CrossArgsL a) {
         const uint32_t l2 = lo < leaf ? lo : lo + 1;
         const unsigned long long key = (unsigned long long)rotl(a.codes[row], 8 * v) << 32;
         const unsigned long long* seg = a.keys + (size_t)(v * a.nleaf + l2) * a.P;
-        uint32_t b = 0, t = a.leaf_off[l2 + 1] - a.leaf_off[l2];
+        const uint32_t L = a.leaf_off[l2 + 1] - a.leaf_off[l2];
+        // the fences (keys VFENCE i < L, read through L1) narrow the search
+        // to one window of VFENCE keys: the first fence >= key is at fi, so
+        // the lower bound lies in ((fi - 1) VFENCE, fi VFENCE], or past the
+        // last fence when fi is the count
+        const unsigned long long* fs = a.fence + (size_t)(v * a.nleaf + l2) * (a.P / VFENCE);
+        const uint32_t nfv = (L + VFENCE - 1) / VFENCE;
+        uint32_t fb = 0, ft = nfv;
+        while (fb < ft) {
+            const uint32_t mid = (fb + ft) >> 1;
+            if (__ldg(fs + mid) < key) fb = mid + 1;
+            else ft = mid;
+        }
+        uint32_t b = fb == 0 ? 0u : (fb - 1) * VFENCE + 1, t = fb == nfv ? L : fb * VFENCE;
         while (b < t) {
             const uint32_t mid = (b + t) >> 1;
             if (seg[mid] < key) b = mid + 1;
@@ -391,6 +405,13 @@ __global__ void __launch_bounds__(IW * 32) k_learned_cross(CrossArgsL a) {
     }
 }
 
+// fence[i] = keys[VFENCE i]: segments are P keys long, P a multiple of
+// VFENCE, so fence i / (P / VFENCE) of segment (i * VFENCE) / P.
+__global__ void k_view_fences(const unsigned long long* keys, size_t nfence, unsigned long long* fence) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nfence) fence[i] = keys[i * VFENCE];
+}
+
 uint32_t pow2_at_least(uint32_t v) {
     uint32_t p = 1;
     while (p < v) p <<= 1;
@@ -430,6 +451,12 @@ int views_build(Ctx& ctx, const GraphDev& g, const std::vector<uint32_t>& leaf_o
     out.leaf_off = leaf_off;
     out.keys = keys;
     out.pos = s.vpos.as<uint32_t>();
+    // the fences: key VFENCE i of every segment
+    const size_t nfence = total / VFENCE;
+    NNM_CUDA_TRY(s.vfence.ensure(nfence * 8));
+    k_view_fences<<<blocks_for(nfence, 256), 256, 0, st>>>(keys, nfence, s.vfence.as<unsigned long long>()); count_launch();
+    NNM_CUDA_TRY(cudaGetLastError());
+    out.fence = s.vfence.as<unsigned long long>();
     return 0;
 }
 
@@ -457,7 +484,8 @@ int learned_cross(Ctx& ctx, GraphDev& g, const CodeViews& vw, const uint32_t* d_
     const uint32_t win = std::max<uint32_t>(1, NCAND / (2 * npair));
     CrossArgsL ca{g.x, g.dp, g.K, g.metric, g.pid, g.cpid, g.pdist, g.cpdist, g.n, g.K - g.cut, g.codes, vw.keys,
                   d_leaf_off, vw.P, vw.nleaf, nview, npair, win, g.seed, g.phase++,
-                  ctx.ws.counters.as<IterCounters>(), DistSrc{g.x, g.dp, g.metric, g.tc_kind == 0 ? g.xq : nullptr, g.nrm, g.kq}};
+                  ctx.ws.counters.as<IterCounters>(), DistSrc{g.x, g.dp, g.metric, g.tc_kind == 0 ? g.xq : nullptr, g.nrm, g.kq},
+                  vw.fence};
     k_learned_cross<<<blocks_for(g.n, IW), IW * 32, 0, ctx.stream>>>(ca); count_launch();
     NNM_CUDA_TRY(cudaGetLastError());
     return check_counters(ctx);

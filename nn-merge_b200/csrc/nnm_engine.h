@@ -58,10 +58,11 @@ struct GraphStore {
     DevBuf xq, nrm;  // operand copy of the vectors and their squared norms (tensor-core join)
     DevBuf scl;      // FP8 operands: per-row inverse scales
     DevBuf codes, vkeys, vpos, voff;  // learned codes and their sorted views
+    DevBuf vfence;                    // every 256th key of each sorted view segment
     void release() {
         DevBuf* all[] = {&pid, &pdist, &cpid, &cpdist, &newL, &oldL, &newlen, &oldlen,
                          &rnewT, &roldT, &rnewTlen, &roldTlen, &x, &xq, &nrm, &scl,
-                         &codes, &vkeys, &vpos, &voff};
+                         &codes, &vkeys, &vpos, &voff, &vfence};
         for (auto* b : all) b->release();
     }
 };

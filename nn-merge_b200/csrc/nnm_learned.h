@@ -63,7 +63,9 @@ struct CodeViews {
     std::vector<uint32_t> leaf_off;
     const unsigned long long* keys = nullptr;  // V*nleaf*P sorted (key << 32 | row)
     const uint32_t* pos = nullptr;             // V x n: position of each row in its leaf's segment
+    const unsigned long long* fence = nullptr; // V*nleaf*(P / VFENCE): key VFENCE*i of each segment
 };
+constexpr uint32_t VFENCE = 256;
 int views_build(Ctx& ctx, const GraphDev& g, const std::vector<uint32_t>& leaf_off, CodeViews& out);
 // Initial pools of rows [0, s.n) of the leaf sub-graph s (leaf `leaf` of vw).
 int learned_rows(Ctx& ctx, GraphDev& s, const CodeViews& vw, uint32_t leaf);
