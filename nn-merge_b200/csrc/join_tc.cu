@@ -18,6 +18,8 @@
 // b (slot b) with tcgen05.ld; by symmetry column a of that lane is G(a, b),
 // so lane b evaluates the pairs (a, b), a < b, of its row: a thread per
 // "inner" slot, all lanes of a warp on the same "outer" column at a time.
+// Longer lists (the last tier) take k_pairs_tc below: a row's slots in
+// several 128-slot blocks, one MMA chain per pair of blocks.
 //
 // Two passes, as the FP32 path: pass 0 counts, per list slot, the proposals
 // that pass the K-th-distance filter (the bucket sizes); pass 1 recomputes
